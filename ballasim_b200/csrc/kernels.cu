@@ -1,0 +1,552 @@
+// The device kernels of the path (sm_100a): sensor init, the pixel model over CSR sample runs (the
+// SensorModel::advance_device boundary, src/sensor/sensor_model.h:157-167), the window sampler writing CSR runs
+// (sample_window, src/engine/bindings/engine_module.cpp:311-355), and the fused engine that samples and senses
+// every window of every sensor with each pixel's state in registers (the reference's Camera::sample_and_sense,
+// src/engine/engine_impl.h:1253-1357, without the runs ever reaching HBM).
+//
+// Events leave through warp-aggregated atomics: the lanes that emit together take one slot range with one atomic
+// (coalesced group rank), and a call whose events exceed the buffer is re-run from its unchanged input state.
+#include <cooperative_groups.h>
+
+#include "device.h"
+
+namespace cg = cooperative_groups;
+
+namespace bs {
+
+namespace {
+
+struct GlobalSink {
+  EventBuf ev;
+  unsigned long long* count;
+  __device__ __forceinline__ void push(const RawEvent& e) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    unsigned long long base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(count, static_cast<unsigned long long>(g.size()));
+    base = g.shfl(base, 0);
+    const unsigned long long i = base + g.thread_rank();
+    if (i < ev.capacity) {
+      const uint4* src = reinterpret_cast<const uint4*>(&e);
+      uint4* dst = reinterpret_cast<uint4*>(ev.data + i);
+      dst[0] = src[0];
+      dst[1] = src[1];
+    }
+  }
+};
+
+__device__ __forceinline__ void load_state(const StateSoA& a, uint32_t p, bool noise, PixelRegs& s) {
+  s.t_ref = a.t_ref[p];
+  s.t_search = a.t_search[p];
+  s.blind_until = a.blind_until[p];
+  s.s3_ref = a.s3_ref[p];
+  s.n3_ref = a.n3_ref[p];
+  s.dr_ref = a.dr_ref[p];
+  s.i_scale = a.i_scale[p];
+  s.held = a.held[p];
+  s.flags = a.flags[p];
+  if (noise) {
+    s.t_shot = a.t_shot[p];
+    s.t_ba = a.t_ba[p];
+    s.n_shot = a.n_shot[p];
+    s.n_ba = a.n_ba[p];
+  } else {
+    s.t_shot = s.t_ba = kForever;
+    s.n_shot = s.n_ba = 0;
+  }
+}
+
+__device__ __forceinline__ void store_state(const StateSoA& a, uint32_t p, bool noise, const PixelRegs& s) {
+  a.t_ref[p] = s.t_ref;
+  a.t_search[p] = s.t_search;
+  a.blind_until[p] = s.blind_until;
+  a.s3_ref[p] = s.s3_ref;
+  a.n3_ref[p] = s.n3_ref;
+  a.dr_ref[p] = s.dr_ref;
+  a.i_scale[p] = s.i_scale;
+  a.held[p] = s.held;
+  a.flags[p] = s.flags;
+  if (noise) {
+    a.t_shot[p] = s.t_shot;
+    a.t_ba[p] = s.t_ba;
+    a.n_shot[p] = s.n_shot;
+    a.n_ba[p] = s.n_ba;
+  }
+}
+
+__device__ __forceinline__ void load_map(const MapSoA& m, uint32_t p, PixelMapRegs& r) {
+  r.theta_on = m.theta_on[p];
+  r.theta_off = m.theta_off[p];
+  r.leak = m.leak[p];
+  r.dark = m.dark[p];
+  r.scale = m.scale[p];
+  r.ba_rate_hz = m.ba_rate[p];
+  r.shot_max_hz = m.shot_max[p];
+}
+
+// Sums a value over the warp and adds it to a counter from lane 0 (all 32 lanes must call).
+__device__ __forceinline__ void warp_add(unsigned long long* dst, unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v != 0ull) atomicAdd(dst, v);
+}
+__device__ __forceinline__ void warp_or(unsigned long long* dst, unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v != 0ull) atomicOr(dst, v);
+}
+
+// ---------------------------------------------------------------------------------------------
+// init
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) init_kernel(SensorConsts k, MapSoA map, StateSoA st, uint32_t n_pixels,
+                                                   int64_t t0, const float* irr0, const uint32_t* pixel_ids,
+                                                   unsigned long long* counters) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long clamps = 0, err = 0;
+  if (p < n_pixels) {
+    const float raw = irr0[p];
+    if (!isfinite(raw)) err |= kErrNonFinite;
+    const float v = clamp_irr(raw, k.irr_max);
+    if (!(v == raw)) ++clamps;
+    PixelMapRegs m;
+    load_map(map, p, m);
+    PixelRegs s;
+    pixel_init(s, m, k, pixel_ids ? pixel_ids[p] : p, t0, v, map.phi0[p]);
+    store_state(st, p, true, s);
+  }
+  warp_add(&counters[kCntClamps], clamps);
+  warp_or(&counters[kCntErrors], err);
+}
+
+// ---------------------------------------------------------------------------------------------
+// CSR runs -> pixel model
+// ---------------------------------------------------------------------------------------------
+__global__ void scatter_rows_kernel(const uint32_t* pixel, uint32_t n, int32_t* row_of, uint32_t n_pixels,
+                                    unsigned long long* counters) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t p = pixel[i];
+  if (p >= n_pixels) {
+    atomicOr(&counters[kCntErrors], kErrPixelRange);
+    return;
+  }
+  if (atomicExch(&row_of[p], static_cast<int32_t>(i)) != -1) atomicOr(&counters[kCntErrors], kErrDuplicate);
+}
+
+struct RunArgs {
+  SensorConsts k;
+  MapSoA map;
+  StateSoA in, out;
+  uint32_t n_pixels;
+  const uint32_t* pixel_ids;
+  const int32_t* row_of;
+  const int64_t* row_start;
+  const int32_t* row_count;
+  const int64_t* t;
+  const float* irr;
+  uint64_t n_samples;
+  int64_t t_state, t_end;
+  EventBuf ev;
+  unsigned long long* counters;
+};
+
+__global__ void __launch_bounds__(128) advance_runs_kernel(RunArgs a) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  PixelCounters c;
+  unsigned long long clamps = 0, samples = 0, err = 0;
+  if (p < a.n_pixels) {
+    const bool noise = a.k.noise != 0;
+    PixelRegs s;
+    load_state(a.in, p, noise, s);
+    PixelMapRegs m;
+    load_map(a.map, p, m);
+    GlobalSink sink{a.ev, &a.counters[kCntEvents]};
+    PixelProc<GlobalSink> proc{s, m, a.k, a.pixel_ids ? a.pixel_ids[p] : p, sink, c};
+    int64_t prev_t = a.t_state;
+    float prev_v = s.held;
+    const int32_t row = a.row_of != nullptr ? a.row_of[p] : -1;
+    int32_t cnt = 0;
+    if (row >= 0) {
+      const int64_t s0 = a.row_start[row];
+      cnt = a.row_count[row];
+      if (cnt < 0 || s0 < 0 || static_cast<uint64_t>(s0) + static_cast<uint64_t>(cnt) > a.n_samples) {
+        err |= kErrRunRange;
+        cnt = 0;
+      } else {
+        const int64_t* tp = a.t + s0;
+        const float* vp = a.irr + s0;
+        for (int32_t i = 0; i < cnt; ++i) {
+          const int64_t ti = __ldg(tp + i);
+          const float raw = __ldg(vp + i);
+          if (!isfinite(raw)) err |= kErrNonFinite;
+          const float vi = clamp_irr(raw, a.k.irr_max);
+          if (!(vi == raw)) ++clamps;
+          if (i == 0 ? ti < a.t_state : ti <= prev_t) {
+            err |= kErrOrder;
+            break;
+          }
+          if (ti > a.t_end) {
+            err |= kErrAfterEnd;
+            break;
+          }
+          if (i == 0 && ti == a.t_state) {  // a sample at the model time replaces the held one (pixel.h:777)
+            prev_v = vi;
+            continue;
+          }
+          proc.segment(Segment{prev_t, ti, prev_v, vi}, prev_t, ti);
+          prev_t = ti;
+          prev_v = vi;
+        }
+        samples = static_cast<unsigned long long>(cnt);
+      }
+    }
+    proc.segment(Segment{prev_t, kForever, prev_v, prev_v}, prev_t, a.t_end);
+    if (row >= 0 && cnt > 0) s.held = prev_v;
+    store_state(a.out, p, noise, s);
+  }
+  __syncwarp();
+  warp_add(&a.counters[kCntClamps], clamps);
+  warp_add(&a.counters[kCntPieces], c.pieces);
+  warp_add(&a.counters[kCntLeaves], c.leaves);
+  warp_add(&a.counters[kCntSamples], samples);
+  warp_add(&a.counters[kCntNoise], c.noise_candidates);
+  warp_or(&a.counters[kCntErrors], err);
+}
+
+// ---------------------------------------------------------------------------------------------
+// sample_window
+// ---------------------------------------------------------------------------------------------
+struct WindowArgs {
+  FieldDev f;
+  SamplerRules r;
+  int64_t t_w;
+  const uint32_t* pixel;
+  const uint8_t* level;
+  uint32_t n;
+  const float* carried_in;
+  const uint64_t* sig_in;
+  uint32_t* counts;
+  const int64_t* offsets;
+  int64_t* t_out;
+  float* irr_out;
+  float* carried_out;
+  uint64_t* sig_out;
+};
+
+template <int kPass>
+__global__ void __launch_bounds__(128) sample_window_kernel(WindowArgs a) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool have = i < a.n;
+  const uint32_t px = have ? a.pixel[i] : 0u;
+  const uint32_t x = a.f.width > 0 ? px % a.f.width : 0u, y = a.f.width > 0 ? px / a.f.width : 0u;
+  const BlobMask mask = warp_blob_mask(a.f, 0xffffffffu, have, x, y, a.t_w);
+  if (!have) return;
+  const float carried = a.carried_in[i];
+  const bool flip = a.sig_in[i] != 0ull;
+  const FieldDev& f = a.f;
+  const int64_t t_w = a.t_w;
+  auto render = [&](uint32_t dt) { return field_eval(f, mask, x, y, t_w + dt); };
+  if (kPass == 0) {
+    const uint32_t n = sample_pixel_window(a.r, a.level[i], carried, flip, render, [](uint32_t, float) {});
+    a.counts[i] = n;
+  } else {
+    int64_t* t_out = a.t_out + a.offsets[i];
+    float* irr_out = a.irr_out + a.offsets[i];
+    uint32_t k = 0;
+    float last = carried;
+    sample_pixel_window(a.r, a.level[i], carried, flip, render, [&](uint32_t dt, float v) {
+      t_out[k] = t_w + dt;
+      irr_out[k] = v;
+      ++k;
+      last = v;
+    });
+    a.carried_out[i] = last;
+    a.sig_out[i] = 0ull;
+  }
+}
+
+__global__ void levels_kernel(FieldDev f, int64_t t_w, int32_t l_min, int32_t l_max, uint32_t n_pixels,
+                              uint8_t* level) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool have = p < n_pixels;
+  const uint32_t x = have ? p % f.width : 0u, y = have ? p / f.width : 0u;
+  const BlobMask mask = warp_blob_mask(f, 0xffffffffu, have, x, y, t_w);
+  if (have) level[p] = static_cast<uint8_t>(field_level(f, mask, x, y, t_w, l_min, l_max));
+}
+
+__global__ void field_frame_kernel(FieldDev f, int64_t t, uint32_t n_pixels, float* out) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n_pixels) out[p] = field_eval_all(f, p % f.width, p / f.width, t);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Exclusive scan (counts u32 -> offsets i64): per-block scan, a scan of the block sums, then the fix-up.
+// ---------------------------------------------------------------------------------------------
+constexpr int kScanBlock = 1024;
+
+__device__ __forceinline__ int64_t block_exclusive_scan(int64_t v, int64_t* total) {
+  __shared__ int64_t warp_sums[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int64_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sums[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    int64_t w = lane < nw ? warp_sums[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < nw) warp_sums[lane] = w;
+  }
+  __syncthreads();
+  const int64_t before = warp == 0 ? 0 : warp_sums[warp - 1];
+  *total = warp_sums[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return before + x - v;
+}
+
+__global__ void __launch_bounds__(kScanBlock) scan_blocks_kernel(const uint32_t* counts, uint32_t n, int64_t* out,
+                                                                 int64_t* block_sums) {
+  const uint32_t i = blockIdx.x * kScanBlock + threadIdx.x;
+  const int64_t v = i < n ? counts[i] : 0;
+  int64_t total;
+  const int64_t ex = block_exclusive_scan(v, &total);
+  if (i < n) out[i] = ex;
+  if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanBlock) scan_sums_kernel(int64_t* block_sums, uint32_t n_blocks,
+                                                               int64_t* out, uint32_t n) {
+  __shared__ int64_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (uint32_t b = 0; b < n_blocks; b += kScanBlock) {
+    const uint32_t i = b + threadIdx.x;
+    const int64_t v = i < n_blocks ? block_sums[i] : 0;
+    int64_t total;
+    const int64_t ex = block_exclusive_scan(v, &total);
+    if (i < n_blocks) block_sums[i] = ex + carry;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[n] = carry;
+}
+
+__global__ void scan_fix_kernel(int64_t* out, uint32_t n, const int64_t* block_sums) {
+  const uint32_t i = blockIdx.x * kScanBlock + threadIdx.x;
+  if (i < n) out[i] += block_sums[blockIdx.x];
+}
+
+// ---------------------------------------------------------------------------------------------
+// The fused engine
+// ---------------------------------------------------------------------------------------------
+struct EngineArgs {
+  const EngineSensor* sensors;
+  int n_sensors;
+  uint32_t total_tiles;
+  int64_t t0;
+  int32_t w0, w1;
+  SamplerRules r;
+  unsigned int* tile_counter;
+};
+
+struct WindowFeed {
+  PixelProc<GlobalSink>* proc;
+  int64_t t_w;
+  float irr_max;
+  int64_t prev_t;
+  float prev_v;
+  float last_raw;
+  __device__ __forceinline__ void operator()(uint32_t dt, float v) {
+    last_raw = v;
+    const float vc = clamp_irr(v, irr_max);
+    if (dt == 0u) {  // the carried sample sits at the model time: it replaces the held one
+      prev_v = vc;
+      return;
+    }
+    const int64_t t = t_w + dt;
+    proc->segment(Segment{prev_t, t, prev_v, vc}, prev_t, t);
+    prev_t = t;
+    prev_v = vc;
+  }
+};
+
+__global__ void __launch_bounds__(128) engine_kernel(EngineArgs a) {
+  const uint32_t lane = threadIdx.x & 31u;
+  for (;;) {
+    uint32_t tile = 0;
+    if (lane == 0) tile = atomicAdd(a.tile_counter, 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if (tile >= a.total_tiles) break;
+    int si = 0;
+    while (si + 1 < a.n_sensors && a.sensors[si + 1].tile0 <= tile) ++si;
+    const EngineSensor& S = a.sensors[si];
+    const uint32_t local = tile - S.tile0;
+    const uint32_t x = (local % S.tiles_x) * 8u + (lane & 7u), y = (local / S.tiles_x) * 4u + (lane >> 3);
+    const bool have = x < S.width && y < S.height;
+    const uint32_t p = have ? y * S.width + x : 0u;
+    const bool noise = S.consts.noise != 0;
+    PixelRegs s;
+    PixelMapRegs m;
+    float carried = 0.0f;
+    if (have) {
+      load_state(S.in, p, noise, s);
+      load_map(S.map, p, m);
+      carried = S.carried_in[p];
+    }
+    PixelCounters c;
+    unsigned long long samples = 0;
+    GlobalSink sink{S.ev, &S.counters[kCntEvents]};
+    PixelProc<GlobalSink> proc{s, m, S.consts, p, sink, c};
+    const FieldDev& f = S.field;
+    for (int32_t w = a.w0; w < a.w1; ++w) {
+      const int64_t t_w = a.t0 + static_cast<int64_t>(w) * kWindowNs;
+      const BlobMask mask = warp_blob_mask(f, 0xffffffffu, have, x, y, t_w);
+      if (have) {
+        const int level = field_level(f, mask, x, y, t_w, a.r.l_min, a.r.l_max);
+        WindowFeed feed{&proc, t_w, S.consts.irr_max, t_w, s.held, carried};
+        auto render = [&](uint32_t dt) { return field_eval(f, mask, x, y, t_w + dt); };
+        samples += sample_pixel_window(a.r, level, carried, false, render, feed);
+        s.held = feed.prev_v;
+        carried = feed.last_raw;
+      }
+      __syncwarp();
+    }
+    if (have) {
+      store_state(S.out, p, noise, s);
+      S.carried_out[p] = carried;
+    }
+    warp_add(&S.counters[kCntPieces], c.pieces);
+    warp_add(&S.counters[kCntLeaves], c.leaves);
+    warp_add(&S.counters[kCntSamples], samples);
+    warp_add(&S.counters[kCntNoise], c.noise_candidates);
+  }
+}
+
+// MidpointTest.eta (sampling.h:36-53): per group in order, dev = |(a + b) * -0.5 + m|, num += m_max dev,
+// den += m_min min(a, m, b), the mediant max(dev / low) when some group is modulated; eta = num / den.
+struct MidArgs {
+  float tol, dark;
+  int32_t g;
+  float m_min[8], m_max[8];
+  bool mediant;
+};
+
+__global__ void midpoint_eta_kernel(MidArgs p, const float* ea, const float* em, const float* eb, uint32_t n,
+                                    float* eta, uint8_t* exceeds) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float num = 0.0f, den = p.dark, mediant = 0.0f;
+  for (int32_t k = 0; k < p.g; ++k) {
+    const float a = ea[static_cast<size_t>(i) * p.g + k], m = em[static_cast<size_t>(i) * p.g + k];
+    const float b = eb[static_cast<size_t>(i) * p.g + k];
+    const float dev = fabs_f((a + b) * -0.5f + m);
+    const float low = np_min(np_min(a, m), b);
+    num = num + p.m_max[k] * dev;
+    den = den + p.m_min[k] * low;
+    if (p.mediant) {
+      const float q = dev == 0.0f ? 0.0f : dev / low;
+      mediant = (mediant >= q || mediant != mediant) ? mediant : q;  // NumPy maximum
+    }
+  }
+  float e = num / den;
+  if (p.mediant) e = np_min(e, mediant);
+  eta[i] = e;
+  exceeds[i] = e > p.tol ? 1 : 0;
+}
+
+}  // namespace
+
+void launch_midpoint_eta(float tol, float dark, int32_t g, const float* m_min, const float* m_max, const float* ea,
+                         const float* em, const float* eb, uint32_t n, float* eta, uint8_t* exceeds,
+                         cudaStream_t stream) {
+  MidArgs p{};
+  p.tol = tol;
+  p.dark = dark;
+  p.g = g;
+  p.mediant = false;
+  for (int32_t k = 0; k < g; ++k) {
+    p.m_min[k] = m_min[k];
+    p.m_max[k] = m_max[k];
+    p.mediant = p.mediant || m_min[k] != m_max[k];
+  }
+  if (n == 0) return;
+  midpoint_eta_kernel<<<(n + 255) / 256, 256, 0, stream>>>(p, ea, em, eb, n, eta, exceeds);
+}
+
+void launch_init_counted(const SensorConsts& k, const MapSoA& map, StateSoA st, uint32_t n_pixels, int64_t t0,
+                         const float* irr0, unsigned long long* counters, cudaStream_t stream) {
+  const int block = 256;
+  const unsigned grid = (n_pixels + block - 1) / block;
+  init_kernel<<<grid, block, 0, stream>>>(k, map, st, n_pixels, t0, irr0, nullptr, counters);
+}
+
+void launch_scatter_rows(const uint32_t* pixel, uint32_t n, int32_t* row_of, uint32_t n_pixels,
+                         unsigned long long* counters, cudaStream_t stream) {
+  if (n == 0) return;
+  scatter_rows_kernel<<<(n + 255) / 256, 256, 0, stream>>>(pixel, n, row_of, n_pixels, counters);
+}
+
+void launch_advance_runs(const SensorConsts& k, const MapSoA& map, StateSoA in, StateSoA out, uint32_t n_pixels,
+                         const uint32_t* pixel_ids, const int32_t* row_of, const int64_t* row_start,
+                         const int32_t* row_count, const int64_t* t, const float* irr, uint64_t n_samples,
+                         int64_t t_state, int64_t t_end, EventBuf ev, unsigned long long* counters, int block,
+                         cudaStream_t stream) {
+  RunArgs a{k, map, in, out, n_pixels, pixel_ids, row_of, row_start, row_count, t, irr, n_samples, t_state, t_end,
+            ev, counters};
+  if (block <= 0) block = 128;
+  const unsigned grid = (n_pixels + block - 1) / block;
+  advance_runs_kernel<<<grid, block, 0, stream>>>(a);
+}
+
+void launch_sample_window(const FieldDev& f, const SamplerRules& r, int64_t t_w, const uint32_t* pixel,
+                          const uint8_t* level, uint32_t n, const float* carried_in, const uint64_t* sig_in,
+                          uint32_t* counts, const int64_t* offsets, int64_t* t_out, float* irr_out,
+                          float* carried_out, uint64_t* sig_out, int pass, cudaStream_t stream) {
+  if (n == 0) return;
+  WindowArgs a{f, r, t_w, pixel, level, n, carried_in, sig_in, counts, offsets, t_out, irr_out, carried_out, sig_out};
+  const unsigned grid = (n + 127) / 128;
+  if (pass == 0) sample_window_kernel<0><<<grid, 128, 0, stream>>>(a);
+  else sample_window_kernel<1><<<grid, 128, 0, stream>>>(a);
+}
+
+size_t scan_scratch_words(uint32_t n) { return (n + kScanBlock - 1) / kScanBlock + 1; }
+
+void launch_scan(const uint32_t* counts, uint32_t n, int64_t* offsets, int64_t* scratch, cudaStream_t stream) {
+  const uint32_t blocks = n == 0 ? 1 : (n + kScanBlock - 1) / kScanBlock;
+  scan_blocks_kernel<<<blocks, kScanBlock, 0, stream>>>(counts, n, offsets, scratch);
+  scan_sums_kernel<<<1, kScanBlock, 0, stream>>>(scratch, blocks, offsets, n);
+  scan_fix_kernel<<<blocks, kScanBlock, 0, stream>>>(offsets, n, scratch);
+}
+
+void launch_levels(const FieldDev& f, int64_t t_w, int32_t l_min, int32_t l_max, uint32_t n_pixels, uint8_t* level,
+                   cudaStream_t stream) {
+  levels_kernel<<<(n_pixels + 127) / 128, 128, 0, stream>>>(f, t_w, l_min, l_max, n_pixels, level);
+}
+
+void launch_field_frame(const FieldDev& f, int64_t t, uint32_t n_pixels, float* out, cudaStream_t stream) {
+  field_frame_kernel<<<(n_pixels + 255) / 256, 256, 0, stream>>>(f, t, n_pixels, out);
+}
+
+void launch_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t total_tiles, int64_t t0, int32_t w0,
+                   int32_t w1, const SamplerRules& r, unsigned int* tile_counter, int blocks, int warps_per_block,
+                   cudaStream_t stream) {
+  EngineArgs a{sensors_dev, n_sensors, total_tiles, t0, w0, w1, r, tile_counter};
+  engine_kernel<<<blocks, warps_per_block * 32, 0, stream>>>(a);
+}
+
+int engine_max_blocks_per_sm(int warps_per_block) {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel, warps_per_block * 32, 0);
+  return n;
+}
+
+}  // namespace bs

@@ -1,0 +1,1223 @@
+// Host side of the C ABI (include/ballasim_b200.h): the sensor model, the window sampler and the fused engine as
+// C++ objects owning device memory, behind extern "C" entry points with status codes.
+//
+// SensorModel (src/sensor/sensor_model.h:98-320) on this path: parameter checks, the frozen maps drawn on the host
+// in fp64 (src/sensor/maps.cpp:26-156, with the deterministic log / sincos of bs_math.cuh so that they are the
+// reference's bits), the per-pixel state double-buffered on the device, and one synchronization per call to read
+// its counters. Events are sorted by (t_cross, pixel) and read out (src/sensor/readout.h:22-27) on download.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/ballasim_b200.h"
+#include "device.h"
+
+namespace bs {
+namespace {
+
+thread_local std::string g_error;
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct BudgetError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    if (e == cudaErrorMemoryAllocation) {
+      cudaGetLastError();
+      throw BudgetError(std::string(what) + ": out of device memory");
+    }
+    throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+#define CK(x) ck((x), #x)
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t cap = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  T* ensure(size_t n) {
+    if (n <= cap && p) return p;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    const size_t want = n == 0 ? 1 : n;
+    CK(cudaMalloc(&p, want * sizeof(T)));
+    cap = want;
+    return p;
+  }
+};
+
+template <class T>
+struct PinBuf {
+  T* p = nullptr;
+  size_t cap = 0;
+  PinBuf() = default;
+  PinBuf(const PinBuf&) = delete;
+  PinBuf& operator=(const PinBuf&) = delete;
+  ~PinBuf() {
+    if (p) cudaFreeHost(p);
+  }
+  T* ensure(size_t n) {
+    if (n <= cap && p) return p;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    const size_t want = n == 0 ? 1 : n;
+    CK(cudaMallocHost(&p, want * sizeof(T)));
+    cap = want;
+    return p;
+  }
+};
+
+bool device_ok() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return false;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, 0) != cudaSuccess) return false;
+  return prop.major == 10;
+}
+
+void require_device() {
+  if (!device_ok()) throw CudaError("no CUDA device of compute capability 10.x (B200) is visible");
+}
+
+// ---------------------------------------------------------------------------------------------
+// maps (src/sensor/maps.cpp:26-156), fp64
+// ---------------------------------------------------------------------------------------------
+struct HostMaps {
+  std::vector<double> theta_on, theta_off, leak, dark, phi0, ba_rate;
+};
+
+void normals4(uint64_t seed, uint32_t camera, uint32_t pixel, uint64_t block, double* out) {
+  const U4 r = draw(seed, kPurposeSensorMap, camera, pixel, block);
+  const double u0 = open_uniform_d(r.v[0]), u1 = open_uniform_d(r.v[1]);
+  const double u2 = open_uniform_d(r.v[2]), u3 = open_uniform_d(r.v[3]);
+  const double two_pi = 0x1.921fb54442d18p+2;
+  const double r0 = std::sqrt(-2.0 * log_d(u0)), r1 = std::sqrt(-2.0 * log_d(u2));
+  double s0, c0, s1, c1;
+  sincos_d(two_pi * u1, &s0, &c0);
+  sincos_d(two_pi * u3, &s1, &c1);
+  out[0] = r0 * c0;
+  out[1] = r0 * s0;
+  out[2] = r1 * c1;
+  out[3] = r1 * s1;
+}
+
+double arrhenius(double ea, double t, double t0) { return exp_d(-ea / 8.617333262e-5 * (1.0 / t - 1.0 / t0)); }
+double dmax(double a, double b) { return a < b ? b : a; }
+
+HostMaps draw_maps(const bs_params& p, uint64_t seed, uint32_t camera, uint32_t n) {
+  HostMaps m;
+  m.theta_on.resize(n);
+  m.theta_off.resize(n);
+  m.leak.resize(n);
+  m.dark.resize(n);
+  m.phi0.resize(n);
+  m.ba_rate.assign(n, 0.0);
+  const double leak_temp = arrhenius(p.leak_ea_eV, p.temperature_K, p.reference_temperature_K);
+  const double dark_temp = arrhenius(p.dark_ea_eV, p.temperature_K, p.reference_temperature_K);
+  const double rho = p.theta_onoff_corr, rho_c = std::sqrt(1.0 - rho * rho);
+  const double ln10 = log_d(10.0);
+  const bool ba = p.noise_ba_median_hz > 0.0;
+  for (uint32_t px = 0; px < n; ++px) {
+    double xi[4];
+    normals4(seed, camera, px, 0, xi);
+    const U4 u = draw(seed, kPurposeSensorMap, camera, px, 1);
+    const double u_phase = open_uniform_d(u.v[0]);
+    const double xi_off = rho == 0.0 ? xi[1] : rho * xi[0] + rho_c * xi[1];
+    const double on = dmax(p.theta_floor, p.theta_on + p.sigma_theta_on * xi[0]);
+    const double off = dmax(p.theta_floor, p.theta_off + p.sigma_theta_off * xi_off);
+    const double leak_rate = p.leak_rate_hz * exp_d(p.leak_sigma_log10 * xi[2] * ln10) * leak_temp;
+    m.dark[px] = p.dark_current_fA * exp_d(p.dark_sigma_ln * xi[3]) * dark_temp;
+    m.theta_on[px] = on;
+    m.theta_off[px] = off;
+    m.leak[px] = on * leak_rate;
+    m.phi0[px] = p.initial_phase == 0 ? u_phase * on : p.initial_phase == 1 ? -off + u_phase * (on + off) : 0.0;
+    if (ba) {
+      // The pixel's background-activity rate (this build's noise): log-normal, median noise_ba_median_hz, spread
+      // noise_ba_sigma_ln, from its own Box-Muller normal of stream 0x0082.
+      const U4 w = draw(seed, kPurposeBackgroundMap, camera, px, 0);
+      double s, c;
+      sincos_d(0x1.921fb54442d18p+2 * open_uniform_d(w.v[1]), &s, &c);
+      const double z = std::sqrt(-2.0 * log_d(open_uniform_d(w.v[0]))) * c;
+      m.ba_rate[px] = p.noise_ba_median_hz * exp_d(p.noise_ba_sigma_ln * z);
+    }
+  }
+  return m;
+}
+
+uint64_t fnv1a(const void* data, size_t n, uint64_t h = 0xcbf29ce484222325ull) {
+  const auto* b = static_cast<const unsigned char*>(data);
+  for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 0x100000001b3ull;
+  return h;
+}
+
+// ---------------------------------------------------------------------------------------------
+// device state
+// ---------------------------------------------------------------------------------------------
+struct StateBufs {
+  DevBuf<int64_t> i64;   // 5 x n: t_ref, t_search, blind_until, t_shot, t_ba
+  DevBuf<float> f32;     // 5 x n: s3_ref, n3_ref, dr_ref, i_scale, held
+  DevBuf<uint32_t> u32;  // 3 x n: flags, n_shot, n_ba
+  StateSoA soa(size_t n) {
+    i64.ensure(5 * n);
+    f32.ensure(5 * n);
+    u32.ensure(3 * n);
+    StateSoA s;
+    s.t_ref = i64.p;
+    s.t_search = i64.p + n;
+    s.blind_until = i64.p + 2 * n;
+    s.t_shot = i64.p + 3 * n;
+    s.t_ba = i64.p + 4 * n;
+    s.s3_ref = f32.p;
+    s.n3_ref = f32.p + n;
+    s.dr_ref = f32.p + 2 * n;
+    s.i_scale = f32.p + 3 * n;
+    s.held = f32.p + 4 * n;
+    s.flags = u32.p;
+    s.n_shot = u32.p + n;
+    s.n_ba = u32.p + 2 * n;
+    return s;
+  }
+};
+
+// The first member of every device object: refuses before any CUDA call when no B200 is visible.
+struct DeviceGate {
+  DeviceGate() { require_device(); }
+};
+
+struct Timer {
+  cudaEvent_t a = nullptr, b = nullptr;
+  Timer() {
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+  }
+  ~Timer() {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------
+// the sensor model
+// ---------------------------------------------------------------------------------------------
+struct Model {
+  DeviceGate gate;
+  bs_params p{};
+  uint32_t width = 0, height = 0, n = 0, camera = 0;
+  uint64_t seed = 0;
+  HostMaps maps;
+  SensorConsts k{};
+  cudaStream_t own = nullptr;
+  DevBuf<float> mapf;    // 6 x n
+  DevBuf<double> mapd;   // 2 x n
+  MapSoA map{};
+  StateBufs st[2];
+  StateSoA soa[2]{};
+  int cur = 0;
+  DevBuf<int32_t> row_of;
+  DevBuf<unsigned long long> counters;
+  PinBuf<unsigned long long> counters_h;
+  DevBuf<RawEvent> events;
+  size_t event_cap = 0;
+  size_t last_events = 0;      // events of the last device call (on the device)
+  std::vector<RawEvent> kept;  // host-kept events (advance_runs, engine runs)
+  // staging for host runs
+  DevBuf<uint32_t> s_pixel;
+  DevBuf<int64_t> s_start, s_t;
+  DevBuf<int32_t> s_count;
+  DevBuf<float> s_irr, s_frame;
+  int64_t t_state = 0;
+  bool initialized = false;
+  int block = 128;
+  uint64_t stat_pieces = 0, stat_leaves = 0, stat_clamps = 0, stat_samples = 0, stat_noise = 0, stat_launches = 0,
+           stat_reruns = 0;
+  double launch_ms_total = 0, launch_ms_max = 0;
+  int64_t readout_phase = 0;
+  Timer timer;
+
+  cudaStream_t stream_of(void* s) const { return s ? static_cast<cudaStream_t>(s) : own; }
+
+  Model(const bs_params& prm, uint32_t w, uint32_t h, uint64_t sd, uint32_t cam, int32_t groups)
+      : p(prm), width(w), height(h), camera(cam), seed(sd) {
+    validate(groups);
+    require_device();
+    n = w * h;
+    maps = draw_maps(p, seed, camera, n);
+    CK(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
+    // make_constants (src/sensor/sensor_model.cpp:394-433), fp32, gain 1.
+    k.irr_max = static_cast<float>(1e9 / (p.illuminance_scale * 1.0));
+    k.eps_ci = static_cast<float>(p.eps_ci);
+    k.label_cut = static_cast<float>(p.label_share_cut);
+    k.ideal_reset = p.reset_mode == 1;
+    k.refractory_ns = std::llround(p.refractory_s * 1e9);
+    k.noise = (p.noise_shot_rate_hz > 0.0 || p.noise_ba_median_hz > 0.0) ? 1 : 0;
+    k.shot_rate_hz = p.noise_shot_rate_hz;
+    k.seed = seed;
+    k.camera = camera;
+    upload_maps();
+    soa[0] = st[0].soa(n);
+    soa[1] = st[1].soa(n);
+    row_of.ensure(n);
+    counters.ensure(kCntWords);
+    counters_h.ensure(kCntWords);
+    ensure_events(1 << 16);
+    const int64_t q = std::llround(p.readout_quantum_s * 1e9);
+    readout_phase = q > 0 ? static_cast<int64_t>(draw(seed, kPurposeReadoutPhase, camera, 0, 0).v[0] %
+                                                 static_cast<uint64_t>(q))
+                          : 0;
+  }
+  ~Model() {
+    if (own) cudaStreamDestroy(own);
+  }
+
+  void validate(int32_t groups) const {
+    if (p.photoreceptor != 1) {
+      throw std::invalid_argument("SensorModel: this build runs photoreceptor 'instantaneous' only");
+    }
+    if (groups != 1) throw std::invalid_argument("SensorModel: this build runs one constant light group");
+    if (width == 0 || height == 0 || width > 65535 || height > 65535) {
+      throw std::invalid_argument("SensorModel: width and height must lie in [1, 65535]");
+    }
+    if (static_cast<uint64_t>(width) * height > 0xFFFFFFFFull) throw std::invalid_argument("SensorModel: too many pixels");
+    if (camera > 255) throw std::invalid_argument("SensorModel: camera index must be < 256 (purpose.h layout)");
+    if (p.hot_fraction != 0.0) throw std::invalid_argument("SensorModel: this build has no hot pixels (hot_fraction 0)");
+    if (!(p.illuminance_scale > 0.0)) throw std::invalid_argument("SensorParams: illuminance_scale must be > 0");
+    if (!(p.theta_on > p.theta_floor) || !(p.theta_off > p.theta_floor)) {
+      throw std::invalid_argument("SensorParams: theta_on and theta_off must exceed theta_floor");
+    }
+    if (!(std::fabs(p.eps_ci) < 0.5 * p.theta_floor)) {
+      throw std::invalid_argument("SensorParams: |eps_ci| must be < theta_floor / 2");
+    }
+    if (!(p.dark_current_fA > 0.0)) throw std::invalid_argument("SensorParams: dark_current_fA must be > 0");
+    if (!(p.refractory_s >= 0.0 && p.refractory_s < 10.0)) {
+      throw std::invalid_argument("SensorParams: refractory_s must lie in [0, 10)");
+    }
+  }
+
+  void upload_maps() {
+    std::vector<float> f(6 * static_cast<size_t>(n));
+    std::vector<double> d(2 * static_cast<size_t>(n));
+    for (uint32_t i = 0; i < n; ++i) {
+      f[i] = static_cast<float>(maps.theta_on[i]);
+      f[n + i] = static_cast<float>(maps.theta_off[i]);
+      f[2 * static_cast<size_t>(n) + i] = static_cast<float>(maps.leak[i]);
+      f[3 * static_cast<size_t>(n) + i] = static_cast<float>(maps.dark[i]);
+      f[4 * static_cast<size_t>(n) + i] = static_cast<float>(p.illuminance_scale) * 1.0f;
+      f[5 * static_cast<size_t>(n) + i] = static_cast<float>(maps.phi0[i]);
+      d[i] = maps.ba_rate[i];
+      // shot noise: lambda_max = r sqrt(100 fA / I_dk) over the pixel's fp32 dark current
+      d[n + i] = p.noise_shot_rate_hz > 0.0 ? p.noise_shot_rate_hz * std::sqrt(100.0 / static_cast<double>(f[3 * static_cast<size_t>(n) + i])) : 0.0;
+    }
+    mapf.ensure(f.size());
+    mapd.ensure(d.size());
+    CK(cudaMemcpy(mapf.p, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(mapd.p, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice));
+    map.theta_on = mapf.p;
+    map.theta_off = mapf.p + n;
+    map.leak = mapf.p + 2 * static_cast<size_t>(n);
+    map.dark = mapf.p + 3 * static_cast<size_t>(n);
+    map.scale = mapf.p + 4 * static_cast<size_t>(n);
+    map.phi0 = mapf.p + 5 * static_cast<size_t>(n);
+    map.ba_rate = mapd.p;
+    map.shot_max = mapd.p + n;
+  }
+
+  void ensure_events(size_t cap) {
+    if (cap <= event_cap) return;
+    events.ensure(cap);
+    event_cap = cap;
+  }
+
+  void read_counters(cudaStream_t s) {
+    CK(cudaMemcpyAsync(counters_h.p, counters.p, kCntWords * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+  }
+
+  void init_device(int64_t t0, const float* irr0_dev, cudaStream_t s, const float* host_copy) {
+    CK(cudaMemsetAsync(counters.p, 0, kCntWords * sizeof(unsigned long long), s));
+    launch_init_counted(k, map, soa[cur], n, t0, irr0_dev, counters.p, s);
+    CK(cudaGetLastError());
+    read_counters(s);
+    if (counters_h.p[kCntErrors] & kErrNonFinite) {
+      size_t at = 0;
+      if (host_copy) {
+        while (at < n && std::isfinite(host_copy[at])) ++at;
+      }
+      initialized = false;
+      throw std::invalid_argument("SensorModel.init: non-finite irradiance at pixel " + std::to_string(at));
+    }
+    stat_clamps += counters_h.p[kCntClamps];
+    t_state = t0;
+    initialized = true;
+    last_events = 0;
+    kept.clear();
+  }
+
+  void init_host(int64_t t0, const float* irr0) {
+    if (!irr0) throw std::invalid_argument("init: irradiance0 must have shape (height * width, groups)");
+    s_frame.ensure(n);
+    CK(cudaMemcpyAsync(s_frame.p, irr0, n * sizeof(float), cudaMemcpyHostToDevice, own));
+    init_device(t0, s_frame.p, own, irr0);
+  }
+
+  void check_ready(int64_t t_end) const {
+    if (!initialized) {
+      throw std::logic_error("SensorModel.advance: call init() or load_state() first (a call that failed part-way "
+                             "leaves the model uninitialized)");
+    }
+    if (t_end < t_state) throw std::invalid_argument("SensorModel.advance: t_end_ns is before the model time");
+  }
+
+  static const char* error_text(unsigned long long e) {
+    if (e & kErrPixelRange) return "SensorModel.advance: pixel id out of range";
+    if (e & kErrDuplicate) return "SensorModel.advance: duplicate pixel id";
+    if (e & kErrRunRange) return "SensorModel.advance: sample run out of range";
+    if (e & kErrOrder) {
+      return "SensorModel.advance: sample times must be strictly increasing and start at or after the model time";
+    }
+    if (e & kErrAfterEnd) return "SensorModel.advance: sample after t_end_ns";
+    if (e & kErrNonFinite) return "SensorModel.advance: non-finite irradiance";
+    return "SensorModel.advance: refused input";
+  }
+
+  // One device call over runs in device memory; the state is committed only when it succeeds.
+  void advance_device(const bs_device_runs& r, int64_t t_end, cudaStream_t s) {
+    check_ready(t_end);
+    if (r.n > n) throw std::invalid_argument("SensorModel.advance: more runs than pixels");
+    for (int attempt = 0;; ++attempt) {
+      CK(cudaMemsetAsync(counters.p, 0, kCntWords * sizeof(unsigned long long), s));
+      CK(cudaMemsetAsync(row_of.p, 0xFF, n * sizeof(int32_t), s));
+      launch_scatter_rows(r.pixel, static_cast<uint32_t>(r.n), row_of.p, n, counters.p, s);
+      CK(cudaEventRecord(timer.a, s));
+      launch_advance_runs(k, map, soa[cur], soa[1 - cur], n, nullptr, r.n ? row_of.p : nullptr, r.row_start,
+                          r.row_count, r.t, r.irr, r.n_samples, t_state, t_end,
+                          EventBuf{events.p, static_cast<unsigned long long>(event_cap)}, counters.p, block, s);
+      CK(cudaGetLastError());
+      CK(cudaEventRecord(timer.b, s));
+      read_counters(s);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, timer.a, timer.b);
+      ++stat_launches;
+      launch_ms_total += ms;
+      launch_ms_max = std::max(launch_ms_max, static_cast<double>(ms));
+      const unsigned long long* c = counters_h.p;
+      if (c[kCntErrors] != 0) throw std::invalid_argument(error_text(c[kCntErrors]));
+      if (c[kCntEvents] > event_cap) {
+        ++stat_reruns;
+        ensure_events(static_cast<size_t>(c[kCntEvents] + c[kCntEvents] / 4 + 1024));
+        continue;
+      }
+      stat_pieces += c[kCntPieces];
+      stat_leaves += c[kCntLeaves];
+      stat_clamps += c[kCntClamps];
+      stat_samples += c[kCntSamples];
+      stat_noise += c[kCntNoise];
+      last_events = static_cast<size_t>(c[kCntEvents]);
+      cur = 1 - cur;
+      t_state = t_end;
+      return;
+    }
+  }
+
+  void advance_host(const uint32_t* ids, size_t nr, const int64_t* t, const float* irr, size_t ns,
+                    const int64_t* row_start, const int32_t* row_count, int64_t t_end) {
+    check_ready(t_end);
+    if (nr > 0 && (!ids || !row_start || !row_count)) throw std::invalid_argument("advance: null run arrays");
+    if (ns > 0 && (!t || !irr)) throw std::invalid_argument("advance: null sample arrays");
+    s_pixel.ensure(nr);
+    s_start.ensure(nr);
+    s_count.ensure(nr);
+    s_t.ensure(ns);
+    s_irr.ensure(ns);
+    if (nr) {
+      CK(cudaMemcpyAsync(s_pixel.p, ids, nr * sizeof(uint32_t), cudaMemcpyHostToDevice, own));
+      CK(cudaMemcpyAsync(s_start.p, row_start, nr * sizeof(int64_t), cudaMemcpyHostToDevice, own));
+      CK(cudaMemcpyAsync(s_count.p, row_count, nr * sizeof(int32_t), cudaMemcpyHostToDevice, own));
+    }
+    if (ns) {
+      CK(cudaMemcpyAsync(s_t.p, t, ns * sizeof(int64_t), cudaMemcpyHostToDevice, own));
+      CK(cudaMemcpyAsync(s_irr.p, irr, ns * sizeof(float), cudaMemcpyHostToDevice, own));
+    }
+    bs_device_runs r{s_pixel.p, s_start.p, s_count.p, nr, s_t.p, s_irr.p, ns};
+    advance_device(r, t_end, own);
+    kept = download(events.p, last_events, own);
+  }
+
+  std::vector<RawEvent> download(const RawEvent* dev, size_t count, cudaStream_t s) const {
+    std::vector<RawEvent> out(count);
+    if (count) {
+      CK(cudaMemcpyAsync(out.data(), dev, count * sizeof(RawEvent), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+    }
+    std::sort(out.begin(), out.end(), [](const RawEvent& a, const RawEvent& b) {
+      return a.t_cross != b.t_cross ? a.t_cross < b.t_cross : a.pixel < b.pixel;
+    });
+    return out;
+  }
+
+  int64_t reported(int64_t t) const {
+    const int64_t q = std::llround(p.readout_quantum_s * 1e9);
+    int64_t r = t + std::llround(p.readout_delay_s * 1e9);
+    if (q > 0) {
+      const int64_t a = r - readout_phase;
+      const int64_t fd = a / q - ((a % q) < 0 ? 1 : 0);
+      r = readout_phase + q * fd;
+    }
+    return r + p.clock_offset_ns + std::llround(p.clock_drift_ppm * 1e-6 * static_cast<double>(r));
+  }
+
+  void columns(const std::vector<RawEvent>& ev, bs_event_columns* o) const {
+    for (size_t i = 0; i < ev.size(); ++i) {
+      const RawEvent& e = ev[i];
+      if (o->pixel) o->pixel[i] = e.pixel;
+      if (o->x) o->x[i] = static_cast<uint16_t>(e.pixel % width);
+      if (o->y) o->y[i] = static_cast<uint16_t>(e.pixel / width);
+      if (o->p) o->p[i] = e.polarity;
+      if (o->t_cross_ns) o->t_cross_ns[i] = e.t_cross;
+      if (o->t_reported_ns) o->t_reported_ns[i] = reported(e.t_cross);
+      if (o->label) o->label[i] = e.label;
+      if (o->flags) o->flags[i] = e.flags;
+      if (o->ds) o->ds[i] = e.ds;
+      if (o->dn) o->dn[i] = e.dn;
+      if (o->dl) o->dl[i] = e.dl;
+      if (o->l_first) o->l_first[i] = e.l_first;
+    }
+  }
+
+  // save / load: header + the current state arrays.
+  struct Header {
+    uint32_t magic, version, width, height, camera, pad;
+    uint64_t seed, fingerprint;
+    int64_t t_state;
+    uint32_t initialized, bytes_per_pixel;
+  };
+  static constexpr uint32_t kMagic = 0x32304253;  // "SB02"
+  static constexpr uint32_t kBytesPerPixel = 5 * 8 + 5 * 4 + 3 * 4;
+  size_t state_bytes() const { return sizeof(Header) + static_cast<size_t>(n) * kBytesPerPixel; }
+  uint64_t fingerprint() const { return fnv1a(&p, sizeof(p)); }
+
+  void save(uint8_t* out, size_t bytes) const {
+    if (bytes != state_bytes()) throw std::invalid_argument("SensorModel.save_state: buffer size does not match");
+    Header h{kMagic, 1, width, height, camera, 0, seed, fingerprint(), t_state, initialized ? 1u : 0u, kBytesPerPixel};
+    std::memcpy(out, &h, sizeof(h));
+    uint8_t* q = out + sizeof(h);
+    const StateBufs& b = st[cur];
+    CK(cudaMemcpy(q, b.i64.p, 5 * sizeof(int64_t) * n, cudaMemcpyDeviceToHost));
+    q += 5 * sizeof(int64_t) * n;
+    CK(cudaMemcpy(q, b.f32.p, 5 * sizeof(float) * n, cudaMemcpyDeviceToHost));
+    q += 5 * sizeof(float) * n;
+    CK(cudaMemcpy(q, b.u32.p, 3 * sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
+  }
+
+  void load(const uint8_t* data, size_t bytes) {
+    if (bytes != state_bytes()) throw std::invalid_argument("SensorModel.load_state: size does not match this model");
+    Header h;
+    std::memcpy(&h, data, sizeof(h));
+    if (h.magic != kMagic || h.version != 1 || h.bytes_per_pixel != kBytesPerPixel) {
+      throw std::invalid_argument("SensorModel.load_state: not a sensor state of this version");
+    }
+    if (h.width != width || h.height != height || h.camera != camera || h.seed != seed ||
+        h.fingerprint != fingerprint()) {
+      throw std::invalid_argument("SensorModel.load_state: state was saved by a model with other parameters");
+    }
+    initialized = false;
+    const uint8_t* q = data + sizeof(h);
+    StateBufs& b = st[cur];
+    CK(cudaMemcpy(b.i64.p, q, 5 * sizeof(int64_t) * n, cudaMemcpyHostToDevice));
+    q += 5 * sizeof(int64_t) * n;
+    CK(cudaMemcpy(b.f32.p, q, 5 * sizeof(float) * n, cudaMemcpyHostToDevice));
+    q += 5 * sizeof(float) * n;
+    CK(cudaMemcpy(b.u32.p, q, 3 * sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
+    t_state = h.t_state;
+    initialized = h.initialized != 0;
+    last_events = 0;
+    kept.clear();
+  }
+};
+
+// ---------------------------------------------------------------------------------------------
+// the sampler
+// ---------------------------------------------------------------------------------------------
+struct FieldHolder {
+  FieldDev f{};
+  DevBuf<float> blobs;
+  void set(const bs_field& h) {
+    if (h.kind != kFieldTanhEdge && h.kind != kFieldBlobs) throw std::invalid_argument("field: unknown kind");
+    if (h.width == 0 || h.height == 0) throw std::invalid_argument("field: empty frame");
+    if (h.kind == kFieldBlobs && h.n_blobs > 0 && !h.blobs) throw std::invalid_argument("field: null blob table");
+    f.kind = h.kind;
+    f.width = h.width;
+    f.height = h.height;
+    f.base = h.base;
+    f.amp = h.amp;
+    f.nx = h.nx;
+    f.ny = h.ny;
+    f.c = h.c;
+    f.speed = h.speed;
+    f.width_px = h.width_px;
+    f.n_blobs = h.kind == kFieldBlobs ? h.n_blobs : 0;
+    f.blobs = nullptr;
+    if (f.n_blobs > 0) {
+      blobs.ensure(static_cast<size_t>(f.n_blobs) * kBlobWords);
+      CK(cudaMemcpy(blobs.p, h.blobs, static_cast<size_t>(f.n_blobs) * kBlobWords * sizeof(float),
+                    cudaMemcpyHostToDevice));
+      f.blobs = blobs.p;
+    }
+  }
+};
+
+SamplerRules make_rules(const bs_sample_rules& r) {
+  if (r.min_dt_ns < 1 || r.min_dt_ns > kWindowNs || (r.min_dt_ns & (r.min_dt_ns - 1)) != 0) {
+    throw std::invalid_argument("min_dt_ns must be a power of two in [1, 2^23]");
+  }
+  if (r.max_refine_levels < 0) throw std::invalid_argument("max_refine_levels must be >= 0");
+  int shift = 0;
+  while ((int64_t{1} << shift) < r.min_dt_ns) ++shift;
+  SamplerRules s{};
+  s.tol = r.tol;
+  s.dark = r.dark;
+  s.midpoint = r.midpoint;
+  s.refine_signature = r.refine_signature;
+  // A depth-first walk stops where halves fall under min_split anyway; deeper caps change nothing.
+  s.max_refine_levels = std::min(r.max_refine_levels, 24);
+  s.min_split = static_cast<uint32_t>(2 * r.min_dt_ns);
+  s.l_min = r.l_min;
+  s.l_max = std::min(r.l_max, kWindowLog2 - shift);
+  return s;
+}
+
+struct Sampler {
+  DeviceGate gate;
+  FieldHolder field;
+  cudaStream_t own = nullptr;
+  DevBuf<uint32_t> pixel, counts;
+  DevBuf<uint8_t> level;
+  DevBuf<float> carried_in, carried_out, irr;
+  DevBuf<uint64_t> sig_in, sig_out;
+  DevBuf<int64_t> offsets, scratch, t;
+  size_t n = 0, samples = 0;
+  explicit Sampler(const bs_field& f) {
+    require_device();
+    field.set(f);
+    CK(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
+  }
+  ~Sampler() {
+    if (own) cudaStreamDestroy(own);
+  }
+
+  void window(int64_t t_w, const uint32_t* ids, const uint8_t* lv, size_t np, float* c_irr, uint64_t* c_sig,
+              const bs_sample_rules& rr) {
+    const SamplerRules r = make_rules(rr);
+    int shift = 0;
+    while ((int64_t{1} << shift) < rr.min_dt_ns) ++shift;
+    const int max_level = kWindowLog2 - shift;
+    for (size_t i = 0; i < np; ++i) {
+      if (lv[i] > max_level) throw std::invalid_argument("levels must lie in [0, 23 - log2(min_dt_ns)]");
+      if (ids[i] >= field.f.width * field.f.height) throw std::invalid_argument("pixel id outside the field");
+    }
+    if (np > 0xFFFFFFFFull) throw std::invalid_argument("too many pixels");
+    n = np;
+    pixel.ensure(np);
+    level.ensure(np);
+    carried_in.ensure(np);
+    carried_out.ensure(np);
+    sig_in.ensure(np);
+    sig_out.ensure(np);
+    counts.ensure(np);
+    offsets.ensure(np + 1);
+    scratch.ensure(scan_scratch_words(static_cast<uint32_t>(np)));
+    cudaStream_t s = own;
+    if (np) {
+      CK(cudaMemcpyAsync(pixel.p, ids, np * 4, cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(level.p, lv, np, cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(carried_in.p, c_irr, np * 4, cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(sig_in.p, c_sig, np * 8, cudaMemcpyHostToDevice, s));
+    }
+    launch_sample_window(field.f, r, t_w, pixel.p, level.p, static_cast<uint32_t>(np), carried_in.p, sig_in.p,
+                         counts.p, nullptr, nullptr, nullptr, nullptr, nullptr, 0, s);
+    launch_scan(counts.p, static_cast<uint32_t>(np), offsets.p, scratch.p, s);
+    CK(cudaGetLastError());
+    int64_t total = 0;
+    CK(cudaMemcpyAsync(&total, offsets.p + np, 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    samples = static_cast<size_t>(total);
+    t.ensure(samples);
+    irr.ensure(samples);
+    launch_sample_window(field.f, r, t_w, pixel.p, level.p, static_cast<uint32_t>(np), carried_in.p, sig_in.p,
+                         counts.p, offsets.p, t.p, irr.p, carried_out.p, sig_out.p, 1, s);
+    CK(cudaGetLastError());
+    if (np) {
+      CK(cudaMemcpyAsync(c_irr, carried_out.p, np * 4, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(c_sig, sig_out.p, np * 8, cudaMemcpyDeviceToHost, s));
+    }
+    CK(cudaStreamSynchronize(s));
+  }
+};
+
+// ---------------------------------------------------------------------------------------------
+// the fused engine
+// ---------------------------------------------------------------------------------------------
+struct Engine {
+  DeviceGate gate;
+  std::vector<Model*> models;
+  std::vector<std::unique_ptr<FieldHolder>> fields;
+  SamplerRules rules{};
+  std::vector<std::unique_ptr<DevBuf<float>>> carried;  // 2 per sensor
+  std::vector<int> carried_cur;
+  DevBuf<EngineSensor> sensors_dev;
+  DevBuf<unsigned int> tile_counter;
+  std::vector<EngineSensor> host;
+  uint32_t total_tiles = 0;
+  int warps_per_block = 4, blocks_per_sm = 0;
+  double last_ms = 0;
+  Timer timer;
+  cudaStream_t own = nullptr;
+
+  Engine(bs_model* const* ms, const bs_field* fs, int32_t cnt, const bs_sample_rules& r) {
+    require_device();
+    if (cnt < 1) throw std::invalid_argument("engine: at least one sensor");
+    rules = make_rules(r);
+    uint32_t tile0 = 0;
+    for (int32_t i = 0; i < cnt; ++i) {
+      Model* m = reinterpret_cast<Model*>(ms[i]);
+      if (!m) throw std::invalid_argument("engine: null model");
+      if (fs[i].width != m->width || fs[i].height != m->height) {
+        throw std::invalid_argument("engine: each field must have its model's frame size");
+      }
+      models.push_back(m);
+      auto f = std::make_unique<FieldHolder>();
+      f->set(fs[i]);
+      fields.push_back(std::move(f));
+      for (int b = 0; b < 2; ++b) {
+        carried.push_back(std::make_unique<DevBuf<float>>());
+        carried.back()->ensure(m->n);
+      }
+      carried_cur.push_back(0);
+      EngineSensor e{};
+      e.width = m->width;
+      e.height = m->height;
+      e.tiles_x = (m->width + 7) / 8;
+      e.tiles_y = (m->height + 3) / 4;
+      e.tile0 = tile0;
+      tile0 += e.tiles_x * e.tiles_y;
+      host.push_back(e);
+    }
+    total_tiles = tile0;
+    sensors_dev.ensure(host.size());
+    tile_counter.ensure(1);
+    CK(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
+  }
+  ~Engine() {
+    if (own) cudaStreamDestroy(own);
+  }
+
+  void start(int64_t t0, cudaStream_t s, const float* const* host_frames = nullptr) {
+    for (size_t i = 0; i < models.size(); ++i) {
+      Model* m = models[i];
+      float* frame = carried[2 * i + carried_cur[i]]->p;
+      if (host_frames != nullptr) {
+        if (!host_frames[i]) throw std::invalid_argument("engine: null frame");
+        CK(cudaMemcpyAsync(frame, host_frames[i], m->n * sizeof(float), cudaMemcpyHostToDevice, s));
+      } else {
+        launch_field_frame(fields[i]->f, t0, m->n, frame, s);
+        CK(cudaGetLastError());
+      }
+      m->init_device(t0, frame, s, host_frames ? host_frames[i] : nullptr);
+    }
+  }
+
+  void run(int32_t windows, cudaStream_t s, uint64_t* samples_out, uint64_t* events_out) {
+    if (windows < 0) throw std::invalid_argument("engine: windows must be >= 0");
+    const int64_t t0 = models[0]->t_state;
+    for (Model* m : models) {
+      if (!m->initialized) throw std::logic_error("engine: call start() first");
+      if (m->t_state != t0) throw std::logic_error("engine: the sensors' model times differ");
+      if ((t0 & (kWindowNs - 1)) != 0) throw std::invalid_argument("engine: the model time must be a window start");
+    }
+    int dev = 0, sms = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int per_sm = blocks_per_sm > 0 ? blocks_per_sm : std::max(1, engine_max_blocks_per_sm(warps_per_block));
+    const int blocks = static_cast<int>(std::min<uint64_t>(static_cast<uint64_t>(sms) * per_sm,
+                                                           (total_tiles + warps_per_block - 1) / warps_per_block));
+    for (;;) {
+      for (size_t i = 0; i < models.size(); ++i) {
+        Model* m = models[i];
+        EngineSensor& e = host[i];
+        e.field = fields[i]->f;
+        e.consts = m->k;
+        e.in = m->soa[m->cur];
+        e.out = m->soa[1 - m->cur];
+        e.map = m->map;
+        e.carried_in = carried[2 * i + carried_cur[i]]->p;
+        e.carried_out = carried[2 * i + 1 - carried_cur[i]]->p;
+        e.ev = EventBuf{m->events.p, static_cast<unsigned long long>(m->event_cap)};
+        e.counters = m->counters.p;
+        CK(cudaMemsetAsync(m->counters.p, 0, kCntWords * sizeof(unsigned long long), s));
+      }
+      CK(cudaMemcpyAsync(sensors_dev.p, host.data(), host.size() * sizeof(EngineSensor), cudaMemcpyHostToDevice, s));
+      CK(cudaMemsetAsync(tile_counter.p, 0, sizeof(unsigned int), s));
+      CK(cudaEventRecord(timer.a, s));
+      if (windows > 0 && total_tiles > 0) {
+        launch_engine(sensors_dev.p, static_cast<int>(host.size()), total_tiles, t0 - 0, 0, windows, rules,
+                      tile_counter.p, blocks, warps_per_block, s);
+      }
+      CK(cudaGetLastError());
+      CK(cudaEventRecord(timer.b, s));
+      bool rerun = false;
+      for (Model* m : models) {
+        CK(cudaMemcpyAsync(m->counters_h.p, m->counters.p, kCntWords * sizeof(unsigned long long),
+                           cudaMemcpyDeviceToHost, s));
+      }
+      CK(cudaStreamSynchronize(s));
+      float ms = 0;
+      cudaEventElapsedTime(&ms, timer.a, timer.b);
+      last_ms = ms;
+      for (Model* m : models) {
+        const unsigned long long ev = m->counters_h.p[kCntEvents];
+        if (ev > m->event_cap) {
+          m->ensure_events(static_cast<size_t>(ev + ev / 4 + 1024));
+          ++m->stat_reruns;
+          rerun = true;
+        }
+      }
+      if (rerun) continue;
+      uint64_t samples = 0, events = 0;
+      for (size_t i = 0; i < models.size(); ++i) {
+        Model* m = models[i];
+        const unsigned long long* c = m->counters_h.p;
+        m->stat_pieces += c[kCntPieces];
+        m->stat_leaves += c[kCntLeaves];
+        m->stat_samples += c[kCntSamples];
+        m->stat_noise += c[kCntNoise];
+        ++m->stat_launches;
+        m->launch_ms_total += ms;
+        m->launch_ms_max = std::max(m->launch_ms_max, static_cast<double>(ms));
+        m->last_events = static_cast<size_t>(c[kCntEvents]);
+        m->kept.clear();
+        m->cur = 1 - m->cur;
+        m->t_state = t0 + static_cast<int64_t>(windows) * kWindowNs;
+        carried_cur[i] = 1 - carried_cur[i];
+        samples += c[kCntSamples];
+        events += c[kCntEvents];
+      }
+      if (samples_out) *samples_out = samples;
+      if (events_out) *events_out = events;
+      return;
+    }
+  }
+};
+
+}  // namespace bs
+
+// ---------------------------------------------------------------------------------------------
+// extern "C"
+// ---------------------------------------------------------------------------------------------
+using bs::g_error;
+
+template <class F>
+static bs_status guarded(F&& f) {
+  try {
+    f();
+    return BS_OK;
+  } catch (const std::invalid_argument& e) {
+    g_error = e.what();
+    return BS_EINVAL;
+  } catch (const bs::BudgetError& e) {
+    g_error = e.what();
+    return BS_ENOMEM;
+  } catch (const bs::CudaError& e) {
+    g_error = e.what();
+    return BS_ECUDA;
+  } catch (const std::logic_error& e) {
+    g_error = e.what();
+    return BS_ELOGIC;
+  } catch (const std::bad_alloc&) {
+    g_error = "out of host memory";
+    return BS_ENOMEM;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return BS_ECUDA;
+  }
+}
+
+#define NEED(p)                                                      \
+  do {                                                               \
+    if (!(p)) throw std::invalid_argument("null argument: " #p);     \
+  } while (0)
+
+struct bs_model : bs::Model {
+  using bs::Model::Model;
+};
+struct bs_sampler : bs::Sampler {
+  using bs::Sampler::Sampler;
+};
+struct bs_engine : bs::Engine {
+  using bs::Engine::Engine;
+};
+
+extern "C" {
+
+const char* bs_last_error(void) { return g_error.c_str(); }
+const char* bs_version(void) { return "ballasim_b200 0.1 (sm_100a)"; }
+int32_t bs_cuda_available(void) { return bs::device_ok() ? 1 : 0; }
+
+bs_status bs_model_create(const bs_params* params, uint32_t width, uint32_t height, uint64_t seed, uint32_t camera,
+                          int32_t groups, bs_model** out) {
+  return guarded([&] {
+    NEED(params);
+    NEED(out);
+    *out = nullptr;
+    *out = new bs_model(*params, width, height, seed, camera, groups);
+  });
+}
+bs_status bs_model_destroy(bs_model* m) {
+  return guarded([&] { delete m; });
+}
+bs_status bs_model_init(bs_model* m, int64_t t0_ns, const float* irr0) {
+  return guarded([&] {
+    NEED(m);
+    m->init_host(t0_ns, irr0);
+  });
+}
+bs_status bs_model_init_device(bs_model* m, int64_t t0_ns, const float* irr0_dev, void* stream) {
+  return guarded([&] {
+    NEED(m);
+    NEED(irr0_dev);
+    m->init_device(t0_ns, irr0_dev, m->stream_of(stream), nullptr);
+  });
+}
+bs_status bs_model_advance_runs(bs_model* m, const uint32_t* pixel_ids, size_t n, const int64_t* t, const float* irr,
+                                size_t n_samples, const int64_t* row_start, const int32_t* row_count,
+                                int64_t t_end_ns, size_t* n_events) {
+  return guarded([&] {
+    NEED(m);
+    m->advance_host(pixel_ids, n, t, irr, n_samples, row_start, row_count, t_end_ns);
+    if (n_events) *n_events = m->kept.size();
+  });
+}
+bs_status bs_model_advance_device(bs_model* m, const bs_device_runs* runs, int64_t t_end_ns, void* stream,
+                                  bs_device_events* out) {
+  return guarded([&] {
+    NEED(m);
+    NEED(runs);
+    m->advance_device(*runs, t_end_ns, m->stream_of(stream));
+    m->kept.clear();
+    if (out) {
+      out->data = m->events.p;
+      out->count = m->last_events;
+    }
+  });
+}
+bs_status bs_model_download_events(bs_model* m, const bs_device_events* ev, bs_event_columns* out) {
+  return guarded([&] {
+    NEED(m);
+    NEED(ev);
+    NEED(out);
+    const std::vector<bs::RawEvent> v = m->download(static_cast<const bs::RawEvent*>(ev->data), ev->count, m->own);
+    m->columns(v, out);
+  });
+}
+bs_status bs_model_event_count(const bs_model* m, size_t* n) {
+  return guarded([&] {
+    NEED(m);
+    NEED(n);
+    *n = m->kept.empty() ? m->last_events : m->kept.size();
+  });
+}
+bs_status bs_model_take_events(bs_model* m, bs_event_columns* out) {
+  return guarded([&] {
+    NEED(m);
+    NEED(out);
+    if (m->kept.empty() && m->last_events > 0) m->kept = m->download(m->events.p, m->last_events, m->own);
+    m->columns(m->kept, out);
+    m->kept.clear();
+    m->last_events = 0;
+  });
+}
+bs_status bs_model_maps(const bs_model* m, double* on, double* off, double* leak, double* dark, double* phi0) {
+  return guarded([&] {
+    NEED(m);
+    const size_t n = m->n;
+    if (on) std::copy_n(m->maps.theta_on.data(), n, on);
+    if (off) std::copy_n(m->maps.theta_off.data(), n, off);
+    if (leak) std::copy_n(m->maps.leak.data(), n, leak);
+    if (dark) std::copy_n(m->maps.dark.data(), n, dark);
+    if (phi0) std::copy_n(m->maps.phi0.data(), n, phi0);
+  });
+}
+bs_status bs_model_stats(const bs_model* m, uint64_t out[9]) {
+  return guarded([&] {
+    NEED(m);
+    NEED(out);
+    out[0] = m->stat_pieces;
+    out[1] = m->stat_leaves;
+    out[2] = m->stat_clamps;
+    out[3] = m->stat_samples;
+    out[4] = m->stat_noise;
+    out[5] = m->stat_launches;
+    out[6] = m->stat_reruns;
+    out[7] = static_cast<uint64_t>(m->launch_ms_total * 1000.0);
+    out[8] = static_cast<uint64_t>(m->launch_ms_max * 1000.0);
+  });
+}
+bs_status bs_model_reset_stats(bs_model* m) {
+  return guarded([&] {
+    NEED(m);
+    m->stat_pieces = m->stat_leaves = m->stat_clamps = m->stat_samples = m->stat_noise = 0;
+    m->stat_launches = m->stat_reruns = 0;
+    m->launch_ms_total = m->launch_ms_max = 0;
+  });
+}
+bs_status bs_model_info(const bs_model* m, int64_t* time_ns, float* irr_max, int32_t* initialized) {
+  return guarded([&] {
+    NEED(m);
+    if (time_ns) *time_ns = m->t_state;
+    if (irr_max) *irr_max = m->k.irr_max;
+    if (initialized) *initialized = m->initialized ? 1 : 0;
+  });
+}
+bs_status bs_model_state_bytes(const bs_model* m, size_t* n) {
+  return guarded([&] {
+    NEED(m);
+    NEED(n);
+    *n = m->state_bytes();
+  });
+}
+bs_status bs_model_save_state(const bs_model* m, uint8_t* out, size_t n) {
+  return guarded([&] {
+    NEED(m);
+    NEED(out);
+    m->save(out, n);
+  });
+}
+bs_status bs_model_load_state(bs_model* m, const uint8_t* data, size_t n) {
+  return guarded([&] {
+    NEED(m);
+    NEED(data);
+    m->load(data, n);
+  });
+}
+bs_status bs_model_set_block(bs_model* m, int32_t threads) {
+  return guarded([&] {
+    NEED(m);
+    if (threads != 0 && (threads < 32 || threads > 128 || threads % 32 != 0)) {
+      throw std::invalid_argument("threads per block must be 32, 64, 96 or 128");
+    }
+    m->block = threads == 0 ? 128 : threads;
+  });
+}
+
+bs_status bs_sampler_create(const bs_field* field, bs_sampler** out) {
+  return guarded([&] {
+    NEED(field);
+    NEED(out);
+    *out = nullptr;
+    *out = new bs_sampler(*field);
+  });
+}
+bs_status bs_sampler_destroy(bs_sampler* s) {
+  return guarded([&] { delete s; });
+}
+bs_status bs_sample_window(bs_sampler* s, int64_t t_w, const uint32_t* pixel_ids, const uint8_t* levels, size_t n,
+                           float* carried_irr, uint64_t* carried_sig, const bs_sample_rules* rules,
+                           size_t* n_samples) {
+  return guarded([&] {
+    NEED(s);
+    NEED(rules);
+    if (n) {
+      NEED(pixel_ids);
+      NEED(levels);
+      NEED(carried_irr);
+      NEED(carried_sig);
+    }
+    s->window(t_w, pixel_ids, levels, n, carried_irr, carried_sig, *rules);
+    if (n_samples) *n_samples = s->samples;
+  });
+}
+bs_status bs_sampler_download(bs_sampler* s, int64_t* offsets, int64_t* t_ns, float* irr) {
+  return guarded([&] {
+    NEED(s);
+    if (offsets) bs::CK(cudaMemcpy(offsets, s->offsets.p, (s->n + 1) * 8, cudaMemcpyDeviceToHost));
+    if (t_ns && s->samples) bs::CK(cudaMemcpy(t_ns, s->t.p, s->samples * 8, cudaMemcpyDeviceToHost));
+    if (irr && s->samples) bs::CK(cudaMemcpy(irr, s->irr.p, s->samples * 4, cudaMemcpyDeviceToHost));
+  });
+}
+bs_status bs_sampler_device_runs(bs_sampler* s, bs_device_runs* out) {
+  return guarded([&] {
+    NEED(s);
+    NEED(out);
+    out->pixel = s->pixel.p;
+    out->row_start = s->offsets.p;
+    out->row_count = reinterpret_cast<const int32_t*>(s->counts.p);
+    out->n = s->n;
+    out->t = s->t.p;
+    out->irr = s->irr.p;
+    out->n_samples = s->samples;
+  });
+}
+bs_status bs_field_levels(bs_sampler* s, int64_t t_w, int32_t l_min, int32_t l_max, uint8_t* out) {
+  return guarded([&] {
+    NEED(s);
+    NEED(out);
+    const uint32_t n = s->field.f.width * s->field.f.height;
+    bs::DevBuf<uint8_t> lv;
+    lv.ensure(n);
+    bs::launch_levels(s->field.f, t_w, l_min, l_max, n, lv.p, s->own);
+    bs::CK(cudaGetLastError());
+    bs::CK(cudaMemcpyAsync(out, lv.p, n, cudaMemcpyDeviceToHost, s->own));
+    bs::CK(cudaStreamSynchronize(s->own));
+  });
+}
+bs_status bs_field_frame(bs_sampler* s, int64_t t_ns, float* out) {
+  return guarded([&] {
+    NEED(s);
+    NEED(out);
+    const uint32_t n = s->field.f.width * s->field.f.height;
+    bs::DevBuf<float> fr;
+    fr.ensure(n);
+    bs::launch_field_frame(s->field.f, t_ns, n, fr.p, s->own);
+    bs::CK(cudaGetLastError());
+    bs::CK(cudaMemcpyAsync(out, fr.p, n * 4, cudaMemcpyDeviceToHost, s->own));
+    bs::CK(cudaStreamSynchronize(s->own));
+  });
+}
+bs_status bs_midpoint_eta(float tol, float dark, int32_t groups, const float* m_min, const float* m_max,
+                          const float* ea, const float* em, const float* eb, size_t n, float* eta, uint8_t* exceeds) {
+  return guarded([&] {
+    if (groups < 1 || groups > 8) throw std::invalid_argument("midpoint test: need 1 to 8 light groups");
+    NEED(m_min);
+    NEED(m_max);
+    if (n == 0) return;
+    NEED(ea);
+    NEED(em);
+    NEED(eb);
+    NEED(eta);
+    NEED(exceeds);
+    bs::require_device();
+    const size_t w = n * static_cast<size_t>(groups);
+    bs::DevBuf<float> a, m, b, e;
+    bs::DevBuf<uint8_t> x;
+    a.ensure(w);
+    m.ensure(w);
+    b.ensure(w);
+    e.ensure(n);
+    x.ensure(n);
+    bs::CK(cudaMemcpy(a.p, ea, w * 4, cudaMemcpyHostToDevice));
+    bs::CK(cudaMemcpy(m.p, em, w * 4, cudaMemcpyHostToDevice));
+    bs::CK(cudaMemcpy(b.p, eb, w * 4, cudaMemcpyHostToDevice));
+    bs::launch_midpoint_eta(tol, dark, groups, m_min, m_max, a.p, m.p, b.p, static_cast<uint32_t>(n), e.p, x.p,
+                            nullptr);
+    bs::CK(cudaGetLastError());
+    bs::CK(cudaMemcpy(eta, e.p, n * 4, cudaMemcpyDeviceToHost));
+    bs::CK(cudaMemcpy(exceeds, x.p, n, cudaMemcpyDeviceToHost));
+  });
+}
+bs_status bs_level_cap(const int64_t* levels, size_t n, int64_t budget, int32_t l_min, int32_t* cap) {
+  return guarded([&] {
+    NEED(cap);
+    if (l_min < 0 || l_min > bs::kWindowLog2) throw std::invalid_argument("l_min must lie in [0, 23]");
+    std::vector<int64_t> counts;
+    for (size_t i = 0; i < n; ++i) {
+      if (levels[i] < 0 || levels[i] > bs::kWindowLog2) {
+        throw std::invalid_argument("level_cap: levels must lie in [0, 23]");
+      }
+      if (static_cast<size_t>(levels[i]) >= counts.size()) counts.resize(static_cast<size_t>(levels[i]) + 1, 0);
+      ++counts[static_cast<size_t>(levels[i])];
+    }
+    while (!counts.empty() && counts.back() == 0) counts.pop_back();
+    const auto total = [&](int64_t c) {
+      int64_t sum = 0;
+      for (size_t l = 0; l < counts.size(); ++l) sum += counts[l] * ((int64_t{1} << std::min<int64_t>(l, c)) + 1);
+      return sum;
+    };
+    const int64_t top = static_cast<int64_t>(counts.size()) - 1;
+    *cap = -1;
+    if (counts.empty() || total(top) <= budget) return;
+    for (int64_t c = top - 1; c >= l_min; --c) {
+      if (total(c) <= budget) {
+        *cap = static_cast<int32_t>(c);
+        return;
+      }
+    }
+    throw std::invalid_argument("accuracy.max_samples_per_window = " + std::to_string(budget) +
+                                " cannot hold one window of " + std::to_string(n) + " active pixels at level " +
+                                std::to_string(l_min) + " (" + std::to_string(total(l_min)) + " samples); raise it");
+  });
+}
+
+bs_status bs_engine_create(bs_model* const* models, const bs_field* fields, int32_t n, const bs_sample_rules* rules,
+                           bs_engine** out) {
+  return guarded([&] {
+    NEED(models);
+    NEED(fields);
+    NEED(rules);
+    NEED(out);
+    *out = nullptr;
+    *out = new bs_engine(models, fields, n, *rules);
+  });
+}
+bs_status bs_engine_destroy(bs_engine* e) {
+  return guarded([&] { delete e; });
+}
+bs_status bs_engine_start(bs_engine* e, int64_t t0_ns, void* stream) {
+  return guarded([&] {
+    NEED(e);
+    e->start(t0_ns, stream ? static_cast<cudaStream_t>(stream) : e->own);
+  });
+}
+bs_status bs_engine_start_frames(bs_engine* e, int64_t t0_ns, const float* const* frames, void* stream) {
+  return guarded([&] {
+    NEED(e);
+    NEED(frames);
+    e->start(t0_ns, stream ? static_cast<cudaStream_t>(stream) : e->own, frames);
+  });
+}
+bs_status bs_engine_run(bs_engine* e, int32_t windows, void* stream, uint64_t* pixel_samples, uint64_t* events) {
+  return guarded([&] {
+    NEED(e);
+    e->run(windows, stream ? static_cast<cudaStream_t>(stream) : e->own, pixel_samples, events);
+  });
+}
+bs_status bs_engine_set_launch(bs_engine* e, int32_t warps_per_block, int32_t blocks_per_sm) {
+  return guarded([&] {
+    NEED(e);
+    if (warps_per_block != 0 && (warps_per_block < 1 || warps_per_block > 4)) {
+      throw std::invalid_argument("warps per block must lie in [1, 4]");
+    }
+    if (blocks_per_sm < 0) throw std::invalid_argument("blocks per SM must be >= 0");
+    e->warps_per_block = warps_per_block == 0 ? 4 : warps_per_block;
+    e->blocks_per_sm = blocks_per_sm;
+  });
+}
+bs_status bs_engine_last_ms(const bs_engine* e, double* ms) {
+  return guarded([&] {
+    NEED(e);
+    NEED(ms);
+    *ms = e->last_ms;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,337 @@
+// The instantaneous pixel model of BallaSim (src/sensor/pixel.h: advance_instant :876-907, instant_search
+// :1886-1916, instant_may_fire :1853-1876, fire :1534-1588, init :792-818), restated for the device as a
+// streaming processor: the pixel's state lives in registers and is fed one linear sample segment at a time,
+// in time order, from wherever the samples come from (a CSR run in HBM, or the sampler on the same thread).
+//
+// Input model: one constant light group. Between consecutive samples (t0, v0), (t1, v1) the irradiance is
+// v0 + (v1 - v0) ((t - t0) / (t1 - t0)) (fp32, that operation order) and after the last sample it is held;
+// the photocurrent is I = I_dk + s v (s = illuminance_scale x gain); x(t) = ln(I / i_scale).
+// Comparator: Delta(t) = (x - s3_ref) + (0 - n3_ref) + (leak (t - t_ref) 1e-9 + dr_ref) fires at the first
+// integer ns of each piece where Delta >= theta_on or <= -theta_off, found by the time-ordered depth-first
+// bisection with the reference's exclusion test; pieces never cross a multiple of 2^23 ns.
+//
+// Noise (this project's, no reference counterpart): two Poisson chains of candidate times per pixel, keyed by
+// (pixel, candidate number) in Philox streams 0x0080 (shot) and 0x0081 (background activity). Candidate n's
+// gap from n - 1 is ceil(-ln(u0) / lambda_max 1e9) ns (>= 1), it is accepted when u1 < lambda(t) / lambda_max
+// and u2's low bit is its polarity (u_i = open uniform of word i of draw n). Shot noise: lambda = r sqrt(100 fA / I)
+// with lambda_max = r sqrt(100 fA / I_dk); background activity: lambda = lambda_max = the pixel's drawn rate. An
+// accepted candidate outside the refractory time fires as a comparator event of its polarity (label NOISE, the
+// pixel's reset applied); one inside it (or during an ideal reset's dead time) is dropped.
+#pragma once
+
+#include "bs_math.cuh"
+
+namespace bs {
+
+// Device copy of the reference's RawEvent (src/sensor/pixel.h:123-135), 32 bytes.
+struct RawEvent {
+  uint32_t pixel;
+  uint8_t polarity;
+  uint8_t label;
+  uint16_t flags;
+  int64_t t_cross;
+  float ds, dn, dl, l_first;
+};
+static_assert(sizeof(RawEvent) == 32, "RawEvent is 32 bytes");
+
+// Per-model constants of the kernel (KernelConstants<float>, src/sensor/pixel.h:215-252, on this path).
+struct SensorConsts {
+  float irr_max;
+  float eps_ci;
+  float label_cut;
+  int32_t ideal_reset;
+  int64_t refractory_ns;
+  int32_t noise;          // shot or background-activity noise on
+  double shot_rate_hz;    // r of lambda = r sqrt(100 fA / I); 0: no shot noise
+  uint64_t seed;
+  uint32_t camera;
+};
+
+// The state of one pixel between calls (SoA in HBM; see SensorDev).
+struct PixelRegs {
+  int64_t t_ref, t_search, blind_until;
+  float s3_ref, n3_ref, dr_ref, i_scale, held;
+  uint32_t flags;
+  int64_t t_shot, t_ba;
+  uint32_t n_shot, n_ba;
+};
+
+// The pixel's frozen map, fp32 as the kernel takes it (PixelMap's fp64 values cast once).
+struct PixelMapRegs {
+  float theta_on, theta_off, leak, dark, scale;
+  double ba_rate_hz;
+  double shot_max_hz;
+};
+
+struct PixelCounters {
+  uint32_t pieces = 0, leaves = 0, noise_candidates = 0;
+};
+
+BS_HD float clamp_irr(float v, float v_max) { return v >= 0.0f ? (v <= v_max ? v : v_max) : 0.0f; }
+BS_HD float since_ref(int64_t t, int64_t t_ref) { return static_cast<float>(static_cast<double>(t - t_ref) * 1e-9); }
+
+BS_HD uint8_t split_label(float ds, float dl, float D, float cut) {
+  const float a_s = ds / D, a_l = dl / D;
+  if (a_s >= cut && a_s >= a_l) return kLabelSignal;
+  if (a_l >= cut && a_l > a_s) return kLabelLeak;
+  return kLabelNoise;
+}
+BS_HD uint8_t first_label(bool on, float ds, float dn, float l, float cut) {
+  const float D = ds + dn + l;
+  return (on ? D > 0.0f : D < 0.0f) ? split_label(ds, l, D, cut) : kLabelNoise;
+}
+
+// The next candidate of a noise chain after t (kForever without a rate).
+BS_HD int64_t noise_next(uint64_t seed, uint32_t purpose, uint32_t camera, uint32_t pixel, uint32_t n, int64_t t,
+                         double rate_hz) {
+  if (!(rate_hz > 0.0)) return kForever;
+  const U4 w = draw(seed, purpose, camera, pixel, n);
+  const double dt = -log_d(open_uniform_d(w.v[0])) / rate_hz * 1e9;
+  const double step = ceil(dt);
+  if (!(step < 9.0e18)) return kForever;
+  return t + static_cast<int64_t>(step < 1.0 ? 1.0 : step);
+}
+
+// One linear sample segment: [t0, t1) between two samples, or held from t0 on (t1 = kForever).
+struct Segment {
+  int64_t t0, t1;
+  float v0, v1;
+};
+
+template <class Sink>
+struct PixelProc {
+  PixelRegs& s;
+  const PixelMapRegs& m;
+  const SensorConsts& k;
+  uint32_t pixel;  // the frame's pixel id (events, noise keys)
+  Sink& sink;
+  PixelCounters& c;
+
+  BS_HD float value(const Segment& g, int64_t t) const {
+    if (g.t1 == kForever) return g.v0;
+    const float f = static_cast<float>(t - g.t0) / static_cast<float>(g.t1 - g.t0);
+    return g.v0 + (g.v1 - g.v0) * f;
+  }
+  BS_HD float current(const Segment& g, int64_t t) const { return m.dark + m.scale * value(g, t); }
+  BS_HD float log_ratio(float I) const { return log_f(I / s.i_scale); }
+
+  BS_HD float delta(int64_t t, float x) const {
+    const float ds = x - s.s3_ref;
+    const float dn = 0.0f - s.n3_ref;
+    const float dl = m.leak * since_ref(t, s.t_ref) + s.dr_ref;
+    return ds + dn + dl;
+  }
+
+  BS_HD void set_reference(int64_t t, float s3, float offset) {
+    s.t_ref = t;
+    s.s3_ref = s3;
+    s.n3_ref = 0.0f;
+    s.dr_ref = offset;
+  }
+
+  // The event and the reset (pixel.h:1534-1588); label_override >= 0 labels a noise event.
+  BS_HD void fire(int64_t t, bool on, float x, int label_override) {
+    const float ds = x - s.s3_ref;
+    const float dn = 0.0f - s.n3_ref;
+    const float l = m.leak * since_ref(t, s.t_ref);
+    const float dl = l + s.dr_ref;
+    const float D = ds + dn + dl;
+    const bool first = (s.flags & kFlagFirstAfterInit) != 0u;
+    uint8_t label = first ? first_label(on, ds, dn, l, k.label_cut) : split_label(ds, dl, D, k.label_cut);
+    if (label_override >= 0) label = static_cast<uint8_t>(label_override);
+    RawEvent ev;
+    ev.pixel = pixel;
+    ev.polarity = on ? 1 : 0;
+    ev.label = label;
+    ev.flags = static_cast<uint16_t>(s.flags);
+    ev.t_cross = t;
+    ev.ds = ds;
+    ev.dn = dn;
+    ev.dl = dl;
+    ev.l_first = first ? l : 0.0f;
+    sink.push(ev);
+    s.flags = 0;
+    if (k.ideal_reset) {
+      set_reference(t, x, D - (on ? m.theta_on : -m.theta_off));
+      s.t_search = t + 1 + k.refractory_ns;
+    } else if (k.refractory_ns == 0) {
+      set_reference(t, x, -k.eps_ci);
+      s.t_search = t + 1;
+    } else {
+      s.blind_until = t + k.refractory_ns;
+      s.t_search = s.blind_until + 1;
+    }
+  }
+
+  // Can Delta reach a level at an integer of (a, c]? Constant light: curvature 0 and no range cap
+  // (instant_may_fire with instant_curvature's linear case).
+  BS_HD bool may_fire(int64_t a, int64_t cc, float Ia, float Ic) const {
+    const float eps = 0x1p-23f;
+    float hi = maxr(Ia, Ic), lo = minr(Ia, Ic);
+    const float margin = 64.0f * eps * (hi + 2.0f * 0.0f);
+    if (m.leak == 0.0f) {  // hi - lo >= 0.5 * (h^2 * 0): the extremes are at the endpoints
+      const float D = delta(cc, log_ratio(Ic));
+      return D >= m.theta_on || D <= -m.theta_off;
+    }
+    if (Ic >= Ia) return delta(cc, log_ratio(Ic)) >= m.theta_on;  // non-decreasing I, and leak >= 0
+    hi = minr(hi + 0.125f * 0.0f, kInfF) + margin;
+    lo = maxr(lo - 0.125f * 0.0f, m.dark) - margin;
+    const float dl_a = m.leak * since_ref(a, s.t_ref) + s.dr_ref;
+    const float dl_c = m.leak * since_ref(cc, s.t_ref) + s.dr_ref;
+    const float base = 0.0f - s.n3_ref - s.s3_ref;
+    const float x_hi = log_ratio(hi);
+    if (x_hi + base + dl_c + 16.0f * eps * (1.0f + fabs_f(x_hi) + fabs_f(s.s3_ref) + fabs_f(dl_c)) >= m.theta_on) {
+      return true;
+    }
+    if (!(lo > 0.0f)) return true;
+    const float x_lo = log_ratio(lo);
+    return x_lo + base + dl_a - 16.0f * eps * (1.0f + fabs_f(x_lo) + fabs_f(s.s3_ref) + fabs_f(dl_a)) <= -m.theta_off;
+  }
+
+  // The first integer t in [lo, hi) where Delta fires (instant_search): found, polarity, time and x(t).
+  BS_HD bool search(const Segment& g, int64_t lo, int64_t hi, int64_t& t_hit, bool& on, float& x_hit) {
+    const float I_lo = current(g, lo);
+    float x = log_ratio(I_lo);
+    float D = delta(lo, x);
+    if (D >= m.theta_on || D <= -m.theta_off) {
+      t_hit = lo;
+      on = D >= m.theta_on;
+      x_hit = x;
+      return true;
+    }
+    if (hi - lo == 1) return false;
+    int64_t sa[32], sc[32];
+    float sIa[32], sIc[32];
+    int sp = 0;
+    sa[0] = lo;
+    sc[0] = hi - 1;
+    sIa[0] = I_lo;
+    sIc[0] = current(g, hi - 1);
+    sp = 1;
+    while (sp > 0) {
+      --sp;
+      const int64_t a = sa[sp], cc = sc[sp];
+      const float Ia = sIa[sp], Ic = sIc[sp];
+      if (cc - a == 1) {
+        x = log_ratio(Ic);
+        D = delta(cc, x);
+        if (D >= m.theta_on || D <= -m.theta_off) {
+          t_hit = cc;
+          on = D >= m.theta_on;
+          x_hit = x;
+          return true;
+        }
+        continue;
+      }
+      ++c.leaves;
+      if (!may_fire(a, cc, Ia, Ic)) continue;
+      const int64_t mid = a + (cc - a) / 2;
+      const float Im = current(g, mid);
+      sa[sp] = mid;
+      sc[sp] = cc;
+      sIa[sp] = Im;
+      sIc[sp] = Ic;
+      ++sp;
+      sa[sp] = a;
+      sc[sp] = mid;
+      sIa[sp] = Ia;
+      sIc[sp] = Im;
+      ++sp;
+    }
+    return false;
+  }
+
+  // Drops the earliest noise candidate (refractory or dead time) or tests and fires it; advances its chain.
+  BS_HD void noise_candidate(const Segment& g, int64_t tn, bool blind) {
+    ++c.noise_candidates;
+    const bool shot = s.t_shot <= s.t_ba;
+    const uint32_t purpose = shot ? kPurposeShot : kPurposeBackground;
+    const uint32_t n = shot ? s.n_shot : s.n_ba;
+    const double rate = shot ? m.shot_max_hz : m.ba_rate_hz;
+    const int64_t next = noise_next(k.seed, purpose, k.camera, pixel, n + 1, tn, rate);
+    if (shot) {
+      s.n_shot = n + 1;
+      s.t_shot = next;
+    } else {
+      s.n_ba = n + 1;
+      s.t_ba = next;
+    }
+    if (blind) return;
+    const U4 w = draw(k.seed, purpose, k.camera, pixel, n);
+    const float I = current(g, tn);
+    const double accept = shot ? sqrt(static_cast<double>(m.dark) / static_cast<double>(I)) : 1.0;
+    if (open_uniform_d(w.v[1]) < accept) fire(tn, (w.v[2] & 1u) != 0u, log_ratio(I), kLabelNoise);
+  }
+
+  // One piece [t, e) inside segment g (advance_instant's inner loop), with the noise candidates it holds.
+  BS_HD void piece(const Segment& g, int64_t t, int64_t e) {
+    ++c.pieces;
+    for (;;) {
+      const int64_t tn = k.noise ? mini(s.t_shot, s.t_ba) : kForever;
+      if (s.blind_until != kNotBlind) {
+        if (s.blind_until >= e) {
+          if (tn < e) {
+            noise_candidate(g, tn, true);
+            continue;
+          }
+          break;
+        }
+        if (tn <= s.blind_until) {
+          noise_candidate(g, tn, true);
+          continue;
+        }
+        const int64_t tb = s.blind_until;  // the release (M3 A.16): a new reference at x(t_rel) - eps_ci
+        set_reference(tb, log_ratio(current(g, tb)), -k.eps_ci);
+        s.blind_until = kNotBlind;
+      }
+      const int64_t lo = maxi(s.t_search, t);
+      const int64_t stop = mini(e, tn);
+      if (lo < stop) {
+        int64_t th;
+        bool on;
+        float x;
+        if (search(g, lo, stop, th, on, x)) {
+          fire(th, on, x, -1);
+          continue;
+        }
+        s.t_search = maxi(s.t_search, stop);
+      }
+      if (tn >= e) break;
+      noise_candidate(g, tn, tn < s.t_search);
+    }
+  }
+
+  // [t_from, t_to) of segment g (t_from >= g.t0), cut into pieces at multiples of 2^23 ns.
+  BS_HD void segment(const Segment& g, int64_t t_from, int64_t t_to) {
+    const int64_t end = mini(g.t1, t_to);
+    int64_t t = t_from;
+    while (t < end) {
+      const int64_t e = mini(end, ((t >> kWindowLog2) + 1) * kWindowNs);
+      piece(g, t, e);
+      t = e;
+    }
+  }
+};
+
+// The init of the instantaneous response (pixel.h:792-818) for a pixel whose irradiance at t0 is v (clamped).
+BS_HD void pixel_init(PixelRegs& s, const PixelMapRegs& m, const SensorConsts& k, uint32_t pixel, int64_t t0,
+                      float v_clamped, float phi0) {
+  s.held = v_clamped;
+  s.i_scale = m.dark + m.scale * v_clamped;
+  const float I = m.dark + m.scale * v_clamped;
+  s.t_ref = t0;
+  s.s3_ref = log_f(I / s.i_scale);
+  s.n3_ref = 0.0f;
+  s.dr_ref = phi0;
+  s.blind_until = kNotBlind;
+  s.t_search = t0 + 1;
+  s.flags = kFlagFirstAfterInit;
+  s.n_shot = s.n_ba = 0;
+  s.t_shot = s.t_ba = kForever;
+  if (k.noise) {
+    s.t_shot = noise_next(k.seed, kPurposeShot, k.camera, pixel, 0, t0, m.shot_max_hz);
+    s.t_ba = noise_next(k.seed, kPurposeBackground, k.camera, pixel, 0, t0, m.ba_rate_hz);
+  }
+}
+
+}  // namespace bs

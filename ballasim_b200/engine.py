@@ -1,0 +1,79 @@
+"""The fused window engine: every window of one or more sensors sampled and sensed on the device, each pixel's
+sampler and pixel model on the same thread with the state in registers (the reference's per-window
+``Camera::sample_and_sense``, src/engine/engine_impl.h:1253-1357: WindowEngine runs, then
+SensorModel::advance_device, without the runs ever leaving the chip).
+
+    eng = Engine([(model, field), ...], tol=0.01, dark=0.01, min_dt_ns=8192, max_refine_levels=10)
+    eng.start(0)                       # renders every field at t0 and initializes each model from it
+    samples, events = eng.run(windows) # whole windows from the model time; events kept per model
+    cols = model.take_events()         # sorted (t_cross, pixel), as SensorModel.advance returns them
+
+The events are bit-identical to running, per window, ``sample_window`` (levels by the field's rule) and then
+``SensorModel.advance`` on its runs.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .fields import Field
+from .sampling import field_struct
+from .sensor import SensorModel
+
+
+class Engine:
+    def __init__(self, sensors, *, tol: float = 0.01, dark: float = 0.01, min_dt_ns: int = 8192,
+                 max_refine_levels: int = 10, l_min: int = 1, l_max: int = 10, refine_signature: bool = True):
+        self.sensors = [(m, f) for m, f in sensors]
+        if not self.sensors:
+            raise ValueError("engine: at least one sensor")
+        for m, f in self.sensors:
+            if not isinstance(m, SensorModel) or not isinstance(f, Field):
+                raise TypeError("engine: sensors are (SensorModel, Field) pairs")
+        n = len(self.sensors)
+        self._fields = (_lib.Field * n)(*[field_struct(f) for _, f in self.sensors])
+        self._keep = [field_struct(f) for _, f in self.sensors]  # blob tables alive during create
+        for i, s in enumerate(self._keep):
+            self._fields[i] = s
+        models = (C.c_void_p * n)(*[m.handle.value for m, _ in self.sensors])
+        self._rules = _lib.SampleRules(tol, dark, 1, 1 if refine_signature else 0, max_refine_levels, min_dt_ns,
+                                       l_min, l_max)
+        h = C.c_void_p()
+        _lib.check(_lib.lib().bs_engine_create(models, self._fields, n, C.byref(self._rules), C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.lib().bs_engine_destroy(h)
+            self._h = None
+
+    def start(self, t0_ns: int = 0, stream: int | None = None, frames=None) -> None:
+        """Initializes every model at t0: from its field rendered on the device, or from host frames (one float32
+        array of width * height per sensor; copied to the device)."""
+        if frames is None:
+            _lib.check(_lib.lib().bs_engine_start(self._h, int(t0_ns), stream))
+            return
+        arrs = [np.ascontiguousarray(f, np.float32).reshape(-1) for f in frames]
+        if len(arrs) != len(self.sensors) or any(a.size != m.width * m.height
+                                                 for a, (m, _) in zip(arrs, self.sensors)):
+            raise ValueError("engine: one frame of width * height per sensor")
+        ptrs = (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+        _lib.check(_lib.lib().bs_engine_start_frames(self._h, int(t0_ns), ptrs, stream))
+
+    def run(self, windows: int, stream: int | None = None) -> tuple[int, int]:
+        """Samples and senses `windows` whole windows; returns (pixel-samples, events) of the call."""
+        s, e = C.c_uint64(), C.c_uint64()
+        _lib.check(_lib.lib().bs_engine_run(self._h, int(windows), stream, C.byref(s), C.byref(e)))
+        return s.value, e.value
+
+    def set_launch(self, warps_per_block: int = 0, blocks_per_sm: int = 0) -> None:
+        _lib.check(_lib.lib().bs_engine_set_launch(self._h, int(warps_per_block), int(blocks_per_sm)))
+
+    @property
+    def last_ms(self) -> float:
+        ms = C.c_double()
+        _lib.check(_lib.lib().bs_engine_last_ms(self._h, C.byref(ms)))
+        return ms.value

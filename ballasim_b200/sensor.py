@@ -1,0 +1,263 @@
+"""The sensor model with the interface of ``ballasim._sensor`` (src/sensor/sensor_module.cpp:446-656).
+
+``SensorModel(params, width, height, seed, light_groups, camera, num_threads=0, precision=None, overrides=None,
+device='cuda', roi=None)`` runs BallaSim's instantaneous pixel model on the B200 through the C ABI; its events
+are the reference's CPU fp32 path's, bit for bit (the reference asserts the same of its own GPU path,
+src/sensor/sensor_cuda.h:1-3). This build runs device 'cuda', precision 'fp32', one constant light group and no
+region of interest; other values raise ValueError. Errors map as the reference's: ValueError for refused input
+(the model unchanged), RuntimeError for a call before init.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+
+import numpy as np
+
+from . import _lib
+from .params import SensorParams, preset_names, resolve  # noqa: F401  (re-exported: the reference's module API)
+
+cuda_available = _lib.cuda_available
+
+EVENT_COLUMNS = (("x", np.uint16), ("y", np.uint16), ("p", np.uint8), ("t_cross_ns", np.int64),
+                 ("t_reported_ns", np.int64), ("label", np.uint8), ("flags", np.uint16), ("ds", np.float32),
+                 ("dn", np.float32), ("dl", np.float32), ("l_first", np.float32))
+
+
+def params_struct(p: SensorParams) -> _lib.Params:
+    v = p.as_dict()
+    s = _lib.Params()
+    s.photoreceptor = 1 if v["photoreceptor"] == "instantaneous" else 0
+    for name in ("theta_on", "theta_off", "sigma_theta_on", "sigma_theta_off", "theta_onoff_corr", "theta_floor",
+                 "refractory_s", "eps_ci", "leak_rate_hz", "leak_sigma_log10", "leak_ea_eV", "dark_current_fA",
+                 "dark_sigma_ln", "dark_ea_eV", "temperature_K", "reference_temperature_K", "illuminance_scale",
+                 "label_share_cut", "readout_quantum_s", "readout_delay_s", "clock_drift_ppm", "hot_fraction",
+                 "noise_shot_rate_hz", "noise_ba_median_hz", "noise_ba_sigma_ln"):
+        setattr(s, name, float(v[name]))
+    s.reset_mode = 1 if v["reset_mode"] == "ideal" else 0
+    s.initial_phase = {"uniform": 0, "symmetric": 1, "zero": 2}[v["initial_phase"]]
+    s.clock_offset_ns = int(v["clock_offset_ns"])
+    return s
+
+
+def _check_light_groups(light_groups) -> int:
+    groups = list(light_groups)
+    if not groups:
+        raise ValueError("SensorModel: need 1 to 8 light groups")
+    for g in groups:
+        d = g.get("waveform", g) if isinstance(g, dict) else g
+        kind = d.get("type", "") if isinstance(d, dict) else ""
+        if kind not in ("constant", "fourier", "pulse"):
+            raise ValueError("light group: waveform type must be 'constant', 'fourier' or 'pulse'")
+        if kind != "constant":
+            raise ValueError("SensorModel: this build runs constant light groups only")
+    if len(groups) != 1:
+        raise ValueError("SensorModel: this build runs one light group")
+    return 1
+
+
+def new_columns(n: int) -> dict:
+    return {name: np.zeros(n, dt) for name, dt in EVENT_COLUMNS}
+
+
+def column_struct(cols: dict, with_pixel: np.ndarray | None = None) -> _lib.EventColumns:
+    s = _lib.EventColumns()
+    for name, _ in EVENT_COLUMNS:
+        setattr(s, name, cols[name].ctypes.data if len(cols[name]) else None)
+    s.pixel = with_pixel.ctypes.data if with_pixel is not None and len(with_pixel) else None
+    return s
+
+
+class SensorModel:
+    """One camera's sensor on the B200 (the reference's ballasim._sensor.SensorModel)."""
+
+    def __init__(self, params, width: int, height: int, seed: int, light_groups, camera: int, num_threads: int = 0,
+                 precision=None, overrides=None, device: str = "cuda", roi=None):
+        if device not in ("cpu", "cuda"):
+            raise ValueError("device must be 'cpu' or 'cuda'")
+        if device != "cuda":
+            raise ValueError("SensorModel: this build has no CPU path; use device='cuda'")
+        if precision not in (None, "fp32", "fp64"):
+            raise ValueError("precision must be 'fp64' or 'fp32'")
+        if precision == "fp64":
+            raise ValueError("SensorModel: the CUDA device runs fp32 only")
+        if roi is not None:
+            raise ValueError("SensorModel: this build has no region-of-interest models")
+        self._groups = _check_light_groups(light_groups)
+        self._params = resolve(params, overrides)
+        if self._params.photoreceptor != "instantaneous":
+            raise ValueError("SensorModel: this build runs photoreceptor 'instantaneous' only")
+        self._width, self._height, self._seed, self._camera = int(width), int(height), int(seed), int(camera)
+        self._num_threads = int(num_threads)
+        self._lock = threading.Lock()
+        L = _lib.lib()
+        h = C.c_void_p()
+        self._ps = params_struct(self._params)
+        _lib.check(L.bs_model_create(C.byref(self._ps), self._width, self._height, self._seed, self._camera,
+                                     self._groups, C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.lib().bs_model_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ---- properties ----
+    width = property(lambda self: self._width)
+    height = property(lambda self: self._height)
+    groups = property(lambda self: self._groups)
+    params = property(lambda self: self._params.copy())
+    num_threads = property(lambda self: self._num_threads)
+    precision = property(lambda self: "fp32")
+    device = property(lambda self: "cuda")
+    roi = property(lambda self: None)
+
+    def _info(self):
+        t, irr_max, init = C.c_int64(), C.c_float(), C.c_int32()
+        _lib.check(_lib.lib().bs_model_info(self._h, C.byref(t), C.byref(irr_max), C.byref(init)))
+        return t.value, irr_max.value, bool(init.value)
+
+    @property
+    def time_ns(self) -> int:
+        return self._info()[0]
+
+    @property
+    def irr_max(self) -> float:
+        return self._info()[1]
+
+    @property
+    def initialized(self) -> bool:
+        return self._info()[2]
+
+    # ---- calls ----
+    def init(self, t0_ns: int, irradiance0) -> None:
+        a = np.ascontiguousarray(irradiance0, np.float32)
+        n = self._width * self._height
+        if a.ndim != 2 or a.shape != (n, self._groups):
+            raise ValueError("init: irradiance0 must have shape (height * width, groups)")
+        with self._lock:
+            _lib.check(_lib.lib().bs_model_init(self._h, int(t0_ns), a.ctypes.data))
+
+    def advance(self, pixel_ids, t_ns, irradiance, t_end_ns: int, counts=None, offsets=None) -> dict:
+        """Advance to t_end_ns (sensor_module.cpp:302-351): rectangular runs t_ns (n, m), irradiance (n, m, groups)
+        with optional counts, or ragged runs t_ns (S,), irradiance (S, groups) and offsets (n + 1,). Returns the
+        event columns sorted by (t_cross_ns, pixel)."""
+        if not isinstance(pixel_ids, np.ndarray) or pixel_ids.dtype != np.uint32 or pixel_ids.ndim != 1:
+            raise TypeError("advance: pixel_ids must be a uint32 array (n,)")
+        ids = np.ascontiguousarray(pixel_ids)
+        n, G = len(ids), self._groups
+
+        def exact(a, dtype, ndim, what):
+            if not isinstance(a, np.ndarray) or a.dtype != dtype or a.ndim != ndim:
+                raise TypeError(f"advance: {what} has the wrong dtype or number of dimensions")
+            return np.ascontiguousarray(a)
+
+        if offsets is None:
+            t = exact(t_ns, np.int64, 2, "t_ns (int64, n x m)")
+            irr = np.ascontiguousarray(irradiance, np.float32)
+            if irr.ndim != 3:
+                raise TypeError("advance: irradiance (n x m x groups) has the wrong dtype or number of dimensions")
+            m = t.shape[1]
+            if t.shape[0] != n or irr.shape != (n, m, G):
+                raise ValueError("advance: t_ns must be (n, m) and irradiance (n, m, groups) for n pixel ids")
+            if counts is not None:
+                cnt = exact(counts, np.int32, 1, "counts (int32)")
+                if len(cnt) != n:
+                    raise ValueError("advance: counts must have one entry per pixel id")
+                if np.any(cnt < 0) or np.any(cnt > m):
+                    raise ValueError("SensorModel.advance: count out of range")
+            else:
+                cnt = np.full(n, m, np.int32)
+            start = np.arange(n, dtype=np.int64) * m
+            t_flat, irr_flat = t.reshape(-1), irr.reshape(-1)
+        else:
+            if counts is not None:
+                raise ValueError("advance: pass either counts or offsets, not both")
+            t_flat = exact(t_ns, np.int64, 1, "t_ns (int64, S)")
+            irr_flat = np.ascontiguousarray(irradiance, np.float32)
+            if irr_flat.ndim != 2:
+                raise TypeError("advance: irradiance (S x groups) has the wrong dtype or number of dimensions")
+            off = exact(offsets, np.int64, 1, "offsets (int64, n + 1)")
+            S = len(t_flat)
+            if irr_flat.shape != (S, G):
+                raise ValueError("advance: with offsets, t_ns must be (S,) and irradiance (S, groups)")
+            if len(off) != n + 1 or off[0] != 0 or off[n] != S:
+                raise ValueError("advance: offsets must be (n + 1,) from 0 to the number of samples")
+            d = np.diff(off)
+            if np.any(d < 0) or np.any(d > np.iinfo(np.int32).max):
+                raise ValueError("advance: offsets must be non-decreasing")
+            start, cnt = off[:-1].copy(), d.astype(np.int32)
+            irr_flat = irr_flat.reshape(-1)
+        return self.advance_runs(ids, t_flat, irr_flat, t_end_ns, start, cnt)
+
+    def advance_runs(self, pixel_ids, t_ns, irradiance, t_end_ns, row_start, row_count) -> dict:
+        """SensorModel::advance_runs: ragged runs in one sample array."""
+        ids = np.ascontiguousarray(pixel_ids, np.uint32)
+        t = np.ascontiguousarray(t_ns, np.int64).reshape(-1)
+        irr = np.ascontiguousarray(irradiance, np.float32).reshape(-1)
+        rs = np.ascontiguousarray(row_start, np.int64)
+        rc = np.ascontiguousarray(row_count, np.int32)
+        ne = C.c_size_t()
+        with self._lock:
+            _lib.check(_lib.lib().bs_model_advance_runs(self._h, _lib.ptr(ids), len(ids), _lib.ptr(t), _lib.ptr(irr),
+                                                        len(t), _lib.ptr(rs), _lib.ptr(rc), int(t_end_ns),
+                                                        C.byref(ne)))
+            return self._take(ne.value)
+
+    def _take(self, n: int, with_pixel: bool = False) -> dict:
+        cols = new_columns(n)
+        px = np.zeros(n, np.uint32) if with_pixel else None
+        s = column_struct(cols, px)
+        _lib.check(_lib.lib().bs_model_take_events(self._h, C.byref(s)))
+        if with_pixel:
+            cols["pixel"] = px
+        return cols
+
+    def take_events(self, with_pixel: bool = False) -> dict:
+        """The events the model keeps (an engine run's), sorted; the list is cleared."""
+        n = C.c_size_t()
+        with self._lock:
+            _lib.check(_lib.lib().bs_model_event_count(self._h, C.byref(n)))
+            return self._take(n.value, with_pixel)
+
+    def sensor_maps(self) -> dict:
+        n = self._width * self._height
+        a = {k: np.zeros(n) for k in ("theta_on", "theta_off", "leak", "dark_current_fA", "phi0")}
+        _lib.check(_lib.lib().bs_model_maps(self._h, *(a[k].ctypes.data for k in a)))
+        return {k: v.reshape(self._height, self._width) for k, v in a.items()}
+
+    def stats(self) -> dict:
+        out = np.zeros(9, np.uint64)
+        _lib.check(_lib.lib().bs_model_stats(self._h, out.ctypes.data))
+        return {"substeps": int(out[0]), "pieces": int(out[0]), "leaf_intervals": int(out[1]),
+                "input_clamps": int(out[2]), "pixel_samples": int(out[3]), "noise_candidates": int(out[4]),
+                "gpu_launches": int(out[5]), "gpu_reruns": int(out[6]), "gpu_launch_ms_total": out[7] / 1000.0,
+                "gpu_launch_ms_max": out[8] / 1000.0}
+
+    def reset_stats(self) -> None:
+        _lib.check(_lib.lib().bs_model_reset_stats(self._h))
+
+    def state_bytes(self) -> int:
+        n = C.c_size_t()
+        _lib.check(_lib.lib().bs_model_state_bytes(self._h, C.byref(n)))
+        return n.value
+
+    def save_state(self) -> bytes:
+        buf = np.zeros(self.state_bytes(), np.uint8)
+        with self._lock:
+            _lib.check(_lib.lib().bs_model_save_state(self._h, buf.ctypes.data, len(buf)))
+        return buf.tobytes()
+
+    def load_state(self, state: bytes) -> None:
+        b = np.frombuffer(state, np.uint8)
+        with self._lock:
+            _lib.check(_lib.lib().bs_model_load_state(self._h, b.ctypes.data, len(b)))
+
+    def set_block(self, threads: int) -> None:
+        """Threads per block of the pixel-model kernel (32..128)."""
+        _lib.check(_lib.lib().bs_model_set_block(self._h, int(threads)))

@@ -1,0 +1,330 @@
+"""Benchmark of the per-pixel event-generation path: pixel-samples/s and events/s on B200s.
+
+One step = one pass of the hot path over the workload: every sensor initialized at t0 from its seeded analytic
+field, then every window sampled (dyadic lattice + eta_L refinement) and sensed (the instantaneous pixel model),
+in the fused engine. At N = 1 the workload is the 346 x 260 sensor (16 blobs, 2.0 s = 239 windows, mismatch 0.03,
+refractory 100 us, noise off); --workload picks another. With N GPUs (torchrun, one rank per GPU) each rank runs
+its own replica of the workload (independent sensors, seeds offset by rank): weak scaling, no collective on the
+data path; value = all ranks' pixel-samples / the slowest rank's device time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+
+--impl reference times the reference's own CPU implementation (oracle/_ref: WindowEngine<kHost> and
+SensorModel fp32 on every host core) on a bounded sample of the same workload (its first windows), rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+from ballasim_b200 import workloads as W  # noqa: E402
+
+WORKLOADS = {
+    "blobs_346x260": W.blobs_346x260,
+    "edge_64x48": W.edge_64x48,
+    "blobs_1280x720": W.blobs_1280x720,
+    "six_sensors": W.six_sensors,
+}
+METRIC = "pixel-samples/s"
+L2_BYTES = 126 * 1024 * 1024
+FALLBACK_HBM_GBS = 6650.0
+
+
+def measured_hbm() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def replica(wl: W.Workload, rank: int) -> W.Workload:
+    """Rank r's replica: the same sizes and laws, fields and maps drawn from seeds offset by r."""
+    if rank == 0:
+        return wl
+    from ballasim_b200 import fields as F
+
+    sensors = []
+    for s in wl.sensors:
+        seed = s.seed + 1000 * rank
+        f = (F.blobs(s.width, s.height, seed, s.field.n_blobs) if s.field.kind == F.KIND_BLOBS
+             else F.tanh_edge(s.width, s.height, seed))
+        sensors.append(W.SensorSpec(s.width, s.height, seed, s.camera, dict(s.overrides), f))
+    return W.Workload(wl.name, sensors, wl.windows, wl.rules)
+
+
+class Clocks:
+    """nvidia-smi clock and throttle samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.file,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        self.file.flush()
+        rows = [r.split(",") for r in Path(self.file.name).read_text().splitlines() if r.strip()]
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for name, v in zip(names, r[5:9]):
+                    if v.strip().lower() in ("active", "1"):
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def b_sense(pixels: int, windows: int, samples: int, events: int) -> int:
+    """Algorithmic bytes of the pixel model over the run, per window call at the reference's DeviceRuns boundary:
+    12 B per pixel-sample (i64 t + f32 irr), 12 B per listed run, 2 x 48 B of state and 24 B of map per pixel, and
+    16 B per compact event."""
+    return samples * 12 + windows * pixels * (12 + 2 * 48 + 24) + events * 16
+
+
+def run_ours(args, rank: int, world: int) -> dict | None:
+    import torch
+    import torch.distributed as dist
+
+    from ballasim_b200 import _lib
+    from ballasim_b200.engine import Engine
+    from ballasim_b200.params import resolve
+    from ballasim_b200.sampling import field_frame
+    from ballasim_b200.sensor import SensorModel
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    if not _lib.cuda_available():
+        raise RuntimeError("bench: no B200 visible")
+    wl = replica(WORKLOADS[args.workload](), rank)
+    r = wl.rules
+    models = [SensorModel(resolve("ideal", s.overrides), s.width, s.height, s.seed, [{"type": "constant"}], s.camera)
+              for s in wl.sensors]
+    eng = Engine([(m, s.field) for m, s in zip(models, wl.sensors)], tol=r.tol, dark=r.dark, min_dt_ns=r.min_dt_ns,
+                 max_refine_levels=r.max_refine_levels, l_min=r.l_min, l_max=r.l_max)
+    if args.warps:
+        eng.set_launch(args.warps, args.blocks_per_sm)
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        eng.start(0, sptr)
+        return eng.run(wl.windows, sptr)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    kernel_ms, samples, events = [], 0, 0
+    with Clocks(torch.cuda.current_device()) as clk:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.zero_()  # L2 flush between steps (a write larger than L2), outside the step's events
+            starts[k].record(stream)
+            s, e = step()
+            ends[k].record(stream)
+            kernel_ms.append(eng.last_ms)
+            samples += s
+            events += e
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+    total_ms = float(sum(step_ms))
+    t = torch.tensor([total_ms, float(samples), float(events)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = t.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        total_ms_all, samples_all, events_all = float(mx[0]), float(sm[1]), float(sm[2])
+    else:
+        total_ms_all, samples_all, events_all = total_ms, float(samples), float(events)
+
+    # e2e through the public API with host buffers: the initial frames from pinned host memory in, every event out
+    frames = [torch.from_numpy(field_frame(s.field, 0)).pin_memory().numpy() for s in wl.sensors]
+    e2e_times, d2h = [], 0
+    for k in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng.start(0, sptr, frames=frames)
+        eng.run(wl.windows, sptr)
+        n_ev = 0
+        for m in models:
+            cols = m.take_events()
+            n_ev += len(cols["t_cross_ns"])
+        torch.cuda.synchronize()
+        if k >= args.warmup:
+            e2e_times.append(time.perf_counter() - t0)
+            d2h = n_ev * 32
+    e2e_s = torch.tensor([sum(e2e_times)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
+    h2d = sum(int(f.nbytes) for f in frames)
+
+    if rank != 0:
+        return None
+    pixels = wl.pixels
+    per_step_samples = samples / args.steps
+    per_step_events = events / args.steps
+    hbm, hbm_kind = measured_hbm()
+    kms = statistics.mean(kernel_ms)
+    alg = b_sense(pixels, wl.windows, int(per_step_samples), int(per_step_events))
+    achieved = alg / (kms * 1e-3) / 1e9
+    out = {
+        "metric": METRIC,
+        "value": samples_all / (total_ms_all * 1e-3),
+        "unit": "pixel-samples/s",
+        "events_per_s": events_all / (total_ms_all * 1e-3),
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms_all / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "fp32",
+        "data": "synthetic (seeded analytic irradiance fields evaluated on the device)",
+        "config": {**wl.describe(), "pixel_samples_per_step": int(per_step_samples),
+                   "events_per_step": int(per_step_events), "l2": "flushed between steps (256 MiB write)",
+                   "sampler": {"tol": r.tol, "min_dt_ns": r.min_dt_ns, "max_refine_levels": r.max_refine_levels,
+                               "levels": [r.l_min, r.l_max]},
+                   "parallelism": f"replicas x{world}"},
+        "gpu_launches": 3 * args.steps,
+        "clocks": {k: v for k, v in clk.summary().items() if k != "samples"},
+        "e2e": {"value": samples_all / float(e2e_s[0]), "unit": "pixel-samples/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "roofline": {"kernel": "engine_kernel (sampler + pixel model fused, runs kept on chip)", "bound": "hbm",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_kind": hbm_kind, "traffic": None, "algorithmic_bytes_per_launch": alg,
+                     "avg_launch_ms": kms, "runs_write_avoided_bytes": int(per_step_samples) * 12},
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(wl, args.cpu_windows)
+    return out
+
+
+def cpu_baseline(wl: W.Workload, windows: int) -> dict:
+    """The reference's own CPU path (oracle/_ref) on the first `windows` windows of the first sensor."""
+    from ballasim_b200.params import resolve
+    from oracle.oracle import Ref
+
+    spec = wl.sensors[0]
+    w = min(windows, wl.windows)
+    m = Ref.Model(resolve("ideal", spec.overrides), spec.width, spec.height, spec.seed, spec.camera)
+    t0 = time.perf_counter()
+    _, st = m.simulate(spec.field, wl.rules, w)
+    dt = time.perf_counter() - t0
+    return {"value": st["pixel_samples"] / dt, "unit": "pixel-samples/s", "cores": m.threads, "kind": "reference",
+            "sample": f"{spec.width}x{spec.height}, first {w} of {wl.windows} windows "
+                      f"({st['pixel_samples']} pixel-samples, {dt:.2f} s; sampler serial {st['sampler_s']:.2f} s, "
+                      f"pixel model on {m.threads} threads {st['sensor_s']:.2f} s)"}
+
+
+def run_reference(args, rank: int) -> dict | None:
+    if rank != 0:
+        return None
+    wl = WORKLOADS[args.workload]()
+    from ballasim_b200.params import resolve
+    from oracle.oracle import Ref
+
+    spec = wl.sensors[0]
+    w = min(args.cpu_windows, wl.windows)
+    vals, threads, samples = [], 0, 0
+    for k in range(args.warmup + args.steps):
+        m = Ref.Model(resolve("ideal", spec.overrides), spec.width, spec.height, spec.seed, spec.camera)
+        t0 = time.perf_counter()
+        _, st = m.simulate(spec.field, wl.rules, w)
+        dt = time.perf_counter() - t0
+        threads, samples = m.threads, st["pixel_samples"]
+        if k >= args.warmup:
+            vals.append(dt)
+    total = sum(vals)
+    value = samples * len(vals) / total
+    sample = f"{spec.width}x{spec.height}, first {w} of {wl.windows} windows per step ({samples} pixel-samples)"
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": "pixel-samples/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(vals),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+            "data": "synthetic (seeded analytic irradiance fields)", "config": {**wl.describe(), "bounded_windows": w},
+            "cpu_baseline": {"value": value, "unit": "pixel-samples/s", "cores": threads, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "pixel-samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="blobs_346x260")
+    ap.add_argument("--cpu-windows", type=int, default=40)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--warps", type=int, default=0)
+    ap.add_argument("--blocks-per-sm", type=int, default=0)
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        out = run_reference(args, rank)
+    else:
+        if world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        try:
+            out = run_ours(args, rank, world)
+        finally:
+            if world > 1:
+                import torch.distributed as dist
+
+                dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,202 @@
+/* ballasim_b200: the C ABI of a B200-native (sm_100a) implementation of BallaSim's per-pixel event-generation
+ * path: the window sampler (src/engine) and the instantaneous continuous-time pixel model (src/sensor).
+ *
+ * Plain C types only: opaque handles, plain pointers and sizes, an explicit CUDA stream as void* (NULL: the
+ * library's own stream). Every call returns a bs_status; bs_last_error() holds the message of the last failure
+ * on the calling thread. Status codes map to the reference's Python exceptions:
+ *   BS_EINVAL -> ValueError (std::invalid_argument), BS_ELOGIC -> RuntimeError (std::logic_error),
+ *   BS_ENOMEM -> MemoryError (MemoryBudgetError), BS_ECUDA -> RuntimeError (a CUDA failure or no device).
+ * There is no CPU fallback: without a CUDA device every compute call returns BS_ECUDA.
+ *
+ * Citations are to the reference project's files; each entry point names the interface it replaces. */
+#ifndef BALLASIM_B200_H
+#define BALLASIM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t bs_status;
+#define BS_OK 0
+#define BS_EINVAL 1
+#define BS_ELOGIC 2
+#define BS_ENOMEM 3
+#define BS_ECUDA 4
+
+typedef struct bs_model bs_model;
+typedef struct bs_sampler bs_sampler;
+typedef struct bs_engine bs_engine;
+
+/* The SensorParams rows this path reads (src/sensor/params.h:65-176), resolved from a preset and overrides by
+ * the caller. photoreceptor must be 1 (instantaneous); enums as in params.h (reset_mode 0 physical / 1 ideal,
+ * initial_phase 0 uniform / 1 symmetric / 2 zero). The noise_* rows are this project's shot and
+ * background-activity noise (0 = off; no reference counterpart). */
+typedef struct {
+  int32_t photoreceptor;
+  double theta_on, theta_off, sigma_theta_on, sigma_theta_off, theta_onoff_corr, theta_floor;
+  int32_t reset_mode;
+  double refractory_s, eps_ci;
+  int32_t initial_phase;
+  double leak_rate_hz, leak_sigma_log10, leak_ea_eV;
+  double dark_current_fA, dark_sigma_ln, dark_ea_eV, temperature_K, reference_temperature_K;
+  double illuminance_scale, label_share_cut;
+  double readout_quantum_s, readout_delay_s, clock_drift_ppm;
+  int64_t clock_offset_ns;
+  double hot_fraction;
+  double noise_shot_rate_hz, noise_ba_median_hz, noise_ba_sigma_ln;
+} bs_params;
+
+/* Event columns of the caller's arrays (count entries each; any pointer may be NULL to skip a column), sorted by
+ * (t_cross, pixel) as SensorModel::finish_events returns them (src/sensor/sensor_model.cpp:996-1029). */
+typedef struct {
+  uint32_t* pixel;
+  uint16_t *x, *y;
+  uint8_t* p;
+  int64_t *t_cross_ns, *t_reported_ns;
+  uint8_t* label;
+  uint16_t* flags;
+  float *ds, *dn, *dl, *l_first;
+} bs_event_columns;
+
+/* Sample runs in device memory (DeviceRuns, src/sensor/sensor_model.h:81-89): listed pixel pixel[i] takes
+ * row_count[i] samples starting at row_start[i] of t (int64 ns) and irr (n_samples x 1 group). */
+typedef struct {
+  const uint32_t* pixel;
+  const int64_t* row_start;
+  const int32_t* row_count;
+  size_t n;
+  const int64_t* t;
+  const float* irr;
+  size_t n_samples;
+} bs_device_runs;
+
+/* Events left in device memory (DeviceEvents, src/sensor/sensor_model.h:91-96): RawEvent records of 32 bytes
+ * (src/sensor/pixel.h:123-135), unordered; valid until the model advances again. */
+typedef struct {
+  const void* data;
+  size_t count;
+} bs_device_events;
+
+const char* bs_last_error(void);
+const char* bs_version(void);
+/* sensor_cuda_available (src/sensor/sensor_model.h:53): a CUDA device of compute capability 10.x is visible. */
+int32_t bs_cuda_available(void);
+
+/* ---- the sensor model: SensorModel (src/sensor/sensor_model.h:98-320) ---- */
+
+/* SensorModel(params, width, height, seed, light_groups, camera, precision='fp32', device='cuda')
+ * (sensor_model.h:114-117, sensor_module.cpp:236-253): validates, draws the frozen maps (maps.cpp:78-156) and
+ * allocates the device state. groups must be 1 (one constant light group). */
+bs_status bs_model_create(const bs_params* params, uint32_t width, uint32_t height, uint64_t seed, uint32_t camera,
+                          int32_t groups, bs_model** out);
+bs_status bs_model_destroy(bs_model* m);
+/* SensorModel::init (sensor_model.h:124-128): irr0 is a host array of width * height * groups floats. */
+bs_status bs_model_init(bs_model* m, int64_t t0_ns, const float* irr0);
+/* init from a device array (the engine's own frame). */
+bs_status bs_model_init_device(bs_model* m, int64_t t0_ns, const float* irr0_dev, void* stream);
+/* SensorModel::advance_runs (sensor_model.h:150-154) on host arrays: the runs are copied to the device, every
+ * pixel advances to t_end_ns, and the events are kept (sorted) for bs_model_take_events; *n_events receives their
+ * count. Refused input (ValueError) leaves the model unchanged. */
+bs_status bs_model_advance_runs(bs_model* m, const uint32_t* pixel_ids, size_t n, const int64_t* t, const float* irr,
+                                size_t n_samples, const int64_t* row_start, const int32_t* row_count,
+                                int64_t t_end_ns, size_t* n_events);
+/* SensorModel::advance_device (sensor_model.h:157-167): runs in device memory, queued on `stream`; the events stay
+ * on the device (out). One synchronization reads the call's counters. */
+bs_status bs_model_advance_device(bs_model* m, const bs_device_runs* runs, int64_t t_end_ns, void* stream,
+                                  bs_device_events* out);
+/* SensorModel::download_events (sensor_model.h:167): the device events of the last call, sorted, into host columns;
+ * and the kept events of bs_model_advance_runs / an engine run (then cleared). */
+bs_status bs_model_download_events(bs_model* m, const bs_device_events* ev, bs_event_columns* out);
+bs_status bs_model_event_count(const bs_model* m, size_t* n);
+bs_status bs_model_take_events(bs_model* m, bs_event_columns* out);
+/* SensorModel::maps (sensor_model.h:180; sensor_module.cpp sensor_maps): the fp64 maps, width * height each. */
+bs_status bs_model_maps(const bs_model* m, double* theta_on, double* theta_off, double* leak, double* dark_fA,
+                        double* phi0);
+/* Work counters since creation or bs_model_reset_stats (SensorModel::stats, sensor_module.cpp:112-136):
+ * [pieces, leaf_intervals, input_clamps, pixel_samples, noise_candidates, gpu_launches, gpu_reruns,
+ *  gpu_launch_ms_total x1000, gpu_launch_ms_max x1000]. */
+bs_status bs_model_stats(const bs_model* m, uint64_t out[9]);
+bs_status bs_model_reset_stats(bs_model* m);
+/* time_ns, irr_max, initialized (sensor_model.h:212-236). */
+bs_status bs_model_info(const bs_model* m, int64_t* time_ns, float* irr_max, int32_t* initialized);
+/* save_state / load_state / state_bytes (sensor_model.h:175-178): this build's own blob (magic, version, shape,
+ * seed, a parameter fingerprint, the model time, the per-pixel state). */
+bs_status bs_model_state_bytes(const bs_model* m, size_t* n);
+bs_status bs_model_save_state(const bs_model* m, uint8_t* out, size_t n);
+bs_status bs_model_load_state(bs_model* m, const uint8_t* data, size_t n);
+/* Launch policy: threads per block of the pixel-model kernel (0: the default). */
+bs_status bs_model_set_block(bs_model* m, int32_t threads);
+
+/* ---- the window sampler: sample_window (src/engine/bindings/engine_module.cpp:311-355), MidpointTest ---- */
+
+/* A seeded analytic field, evaluated on the device in place of the render hook (src/engine/window.h:69-84).
+ * kind 1: tanh edge (base, amp, nx, ny, c, speed, width_px); kind 2: blobs (base, n_blobs rows of 10 floats:
+ * a, cx0, cy0, vx, vy, 1/(2 r^2), (6 r)^2, (3 r)^2, |v|, pad), host memory, copied at create. */
+typedef struct {
+  int32_t kind;
+  uint32_t width, height;
+  float base, amp, nx, ny, c, speed, width_px;
+  int32_t n_blobs;
+  const float* blobs;
+} bs_field;
+
+/* SampleRules of sample_window: MidpointTest(tol, dark, [1], [1]) when midpoint != 0, refine_signature,
+ * max_refine_levels (>= 0), min_dt_ns (a power of two in [1, 2^23]); l_min / l_max clamp the field's level rule
+ * (the engine only). */
+typedef struct {
+  float tol, dark;
+  int32_t midpoint, refine_signature, max_refine_levels;
+  int64_t min_dt_ns;
+  int32_t l_min, l_max;
+} bs_sample_rules;
+
+bs_status bs_sampler_create(const bs_field* field, bs_sampler** out);
+bs_status bs_sampler_destroy(bs_sampler* s);
+/* sample_window on the device field: n active pixels (ids, lattice levels) with their carried samples (host, in
+ * and out: each pixel's last sample at t_w + W). The runs stay in the sampler's device memory; *n_samples gets
+ * their total. Levels must lie in [0, 23 - log2(min_dt_ns)] (engine_module.cpp:317-323). */
+bs_status bs_sample_window(bs_sampler* s, int64_t t_w, const uint32_t* pixel_ids, const uint8_t* levels, size_t n,
+                           float* carried_irr, uint64_t* carried_sig, const bs_sample_rules* rules,
+                           size_t* n_samples);
+/* The last window's runs to host arrays (WindowRuns: offsets n + 1, t_ns, irradiance), or as device runs for
+ * bs_model_advance_device (valid until the sampler runs again). */
+bs_status bs_sampler_download(bs_sampler* s, int64_t* offsets, int64_t* t_ns, float* irr);
+bs_status bs_sampler_device_runs(bs_sampler* s, bs_device_runs* out);
+/* The field's level rule per pixel at t_w, and the field itself at t (width * height, host outputs). */
+bs_status bs_field_levels(bs_sampler* s, int64_t t_w, int32_t l_min, int32_t l_max, uint8_t* out);
+bs_status bs_field_frame(bs_sampler* s, int64_t t_ns, float* out);
+/* MidpointTest.eta / .exceeds (engine_module.cpp:1363-1411): eta_L of n triples of `groups` light groups (host
+ * arrays n x groups; m_min / m_max per group, the mediant when they differ), evaluated on the device. */
+bs_status bs_midpoint_eta(float tol, float dark, int32_t groups, const float* m_min, const float* m_max,
+                          const float* ea, const float* em, const float* eb, size_t n, float* eta, uint8_t* exceeds);
+/* level_cap (src/engine/window.cpp:25-50): the finest level keeping a window within budget samples (-1: none). */
+bs_status bs_level_cap(const int64_t* levels, size_t n, int64_t budget, int32_t l_min, int32_t* cap);
+
+/* ---- the fused engine: every window of several sensors in one launch per call (Camera::sample_and_sense,
+ * src/engine/engine_impl.h:1253-1357, with the runs kept in registers) ---- */
+
+/* models[i] is sampled from fields[i]; the engine borrows the models (they must outlive it). */
+bs_status bs_engine_create(bs_model* const* models, const bs_field* fields, int32_t n, const bs_sample_rules* rules,
+                           bs_engine** out);
+bs_status bs_engine_destroy(bs_engine* e);
+/* Renders every field at t0 and initializes every model from it (CameraEngine::start without warm-up). */
+bs_status bs_engine_start(bs_engine* e, int64_t t0_ns, void* stream);
+/* The same from host frames: frames[i] holds sensor i's irradiance at t0 (width * height floats), copied to the
+ * device; each model starts from it and it is the window sampler's first carried sample. */
+bs_status bs_engine_start_frames(bs_engine* e, int64_t t0_ns, const float* const* frames, void* stream);
+/* Samples and senses `windows` whole windows of every sensor from the current model time; the events are kept in
+ * each model (bs_model_take_events). *pixel_samples and *events receive the totals of the call. */
+bs_status bs_engine_run(bs_engine* e, int32_t windows, void* stream, uint64_t* pixel_samples, uint64_t* events);
+/* Launch shape: warps per block and blocks per SM of the persistent grid (0: the defaults). */
+bs_status bs_engine_set_launch(bs_engine* e, int32_t warps_per_block, int32_t blocks_per_sm);
+/* Kernel time of the last bs_engine_run's launches (ms, CUDA events on its stream). */
+bs_status bs_engine_last_ms(const bs_engine* e, double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

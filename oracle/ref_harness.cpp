@@ -1,0 +1,281 @@
+// A C-ABI harness around the reference's own CPU implementation of the path, compiled from its
+// sources in place by oracle/build_ref.sh into oracle/_ref/libballa_ref.so. TEST INFRASTRUCTURE
+// ONLY: it pins the oracle port (oracle/port) and is the CPU baseline of bench.py's reference arm.
+//
+// It drives balla::sensor::SensorModel (src/sensor/sensor_model.h:98-320) on the fp32 precision
+// (the bitwise contract, src/sensor/sensor_cuda.h:1-3) and balla::engine::WindowEngine<kHost>
+// (src/engine/window.h:132-175) with a render hook that evaluates the project's analytic fields
+// through the oracle port's field evaluator (the same inputs for both sides).
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "engine/window.h"
+#include "sensor/params.h"
+#include "sensor/sensor_model.h"
+
+extern "C" {
+#include "port/oracle.h"
+}
+
+using namespace balla;
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(const std::exception& e) {
+  g_error = e.what();
+  return -1;
+}
+
+// Parameter overrides by field name (a subset of src/sensor/params.h's rows).
+void set_field(sensor::SensorParams& p, const std::string& key, double v) {
+  if (key == "theta_on") p.theta_on = v;
+  else if (key == "theta_off") p.theta_off = v;
+  else if (key == "sigma_theta_on") p.sigma_theta_on = v;
+  else if (key == "sigma_theta_off") p.sigma_theta_off = v;
+  else if (key == "theta_onoff_corr") p.theta_onoff_corr = v;
+  else if (key == "theta_floor") p.theta_floor = v;
+  else if (key == "reset_mode") p.reset_mode = static_cast<sensor::ResetMode>(static_cast<int32_t>(v));
+  else if (key == "refractory_s") p.refractory_s = v;
+  else if (key == "eps_ci") p.eps_ci = v;
+  else if (key == "initial_phase") p.initial_phase = static_cast<sensor::InitialPhase>(static_cast<int32_t>(v));
+  else if (key == "leak_rate_hz") p.leak_rate_hz = v;
+  else if (key == "leak_sigma_log10") p.leak_sigma_log10 = v;
+  else if (key == "dark_current_fA") p.dark_current_fA = v;
+  else if (key == "dark_sigma_ln") p.dark_sigma_ln = v;
+  else if (key == "illuminance_scale") p.illuminance_scale = v;
+  else if (key == "label_share_cut") p.label_share_cut = v;
+  else if (key == "readout_quantum_s") p.readout_quantum_s = v;
+  else if (key == "readout_delay_s") p.readout_delay_s = v;
+  else if (key == "temperature_K") p.temperature_K = v;
+  else throw std::invalid_argument("ref harness: unknown field " + key);
+}
+
+struct RefModel {
+  std::unique_ptr<sensor::SensorModel> model;
+  std::vector<sensor::RawEvent> events;
+};
+
+class FieldHook final : public engine::RenderHook {
+ public:
+  FieldHook(const orc_field* f, int64_t t_w) : f_(f), t_w_(t_w) {}
+  void render(render::SampleRequest* req, size_t n, const uint32_t* out_index, float* irr, uint64_t* sig, uint32_t*,
+              uint32_t) override {
+    for (size_t i = 0; i < n; ++i) {
+      const uint32_t px = req[i].pixel;
+      irr[out_index[i]] = orc_field_eval(f_, px % f_->width, px / f_->width, t_w_ + req[i].t_off_ns);
+      sig[out_index[i]] = 0;
+    }
+    calls_ += n;
+  }
+  size_t calls_ = 0;
+
+ private:
+  const orc_field* f_;
+  int64_t t_w_;
+};
+
+engine::SampleConfig make_config(float tol, float dark, int midpoint, int refine_signature, int max_refine_levels,
+                                 int64_t min_dt_ns) {
+  // sample_window's rules (src/engine/bindings/engine_module.cpp:311-355) with the default economy rules.
+  engine::SampleConfig cfg;
+  cfg.rules.refine_signature = refine_signature != 0;
+  cfg.rules.max_refine_levels = max_refine_levels;
+  cfg.rules.min_split = static_cast<uint32_t>(2 * min_dt_ns);
+  cfg.rules.shift = 0;
+  while ((int64_t{1} << cfg.rules.shift) < min_dt_ns) ++cfg.rules.shift;
+  cfg.rules.midpoint = midpoint != 0;
+  engine::economy_rules(cfg.rules, std::nullopt, std::nullopt, 0.0, 0.0, std::nullopt);
+  if (cfg.rules.midpoint) cfg.rules.mid = engine::midpoint_params(tol, dark, {{1.0, 1.0}});
+  cfg.groups = 1;
+  return cfg;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ref_last_error() { return g_error.c_str(); }
+
+// preset: a family name; keys/values: n_over overrides (SensorParams field names).
+void* ref_model_create(const char* preset, const char* const* keys, const double* values, int n_over, uint32_t width,
+                       uint32_t height, uint64_t seed, uint32_t camera, int num_threads) {
+  try {
+    sensor::SensorParams p = sensor::preset(preset);
+    for (int i = 0; i < n_over; ++i) set_field(p, keys[i], values[i]);
+    p.validate();
+    auto* m = new RefModel;
+    m->model = std::make_unique<sensor::SensorModel>(p, width, height, seed,
+                                                     std::vector<sensor::Waveform>{sensor::make_constant_waveform()},
+                                                     camera, num_threads, sensor::Precision::kFp32,
+                                                     sensor::Device::kCpu);
+    return m;
+  } catch (const std::exception& e) {
+    fail(e);
+    return nullptr;
+  }
+}
+
+void ref_model_destroy(void* h) { delete static_cast<RefModel*>(h); }
+
+int ref_model_init(void* h, int64_t t0, const float* irr0) {
+  try {
+    static_cast<RefModel*>(h)->model->init(t0, irr0);
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+// Appends the raw events (unsorted) of one advance; ref_model_take_events returns them sorted by (t_cross, pixel).
+int ref_model_advance_runs(void* h, const uint32_t* ids, size_t n, const int64_t* t, const float* irr, size_t ns,
+                           const int64_t* row_start, const int32_t* row_count, int64_t t_end) {
+  try {
+    auto* m = static_cast<RefModel*>(h);
+    std::vector<sensor::RawEvent> ev = m->model->advance_runs_raw(ids, n, t, irr, ns, row_start, row_count, t_end);
+    m->events.insert(m->events.end(), ev.begin(), ev.end());
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+size_t ref_model_event_count(void* h) { return static_cast<RefModel*>(h)->events.size(); }
+
+// Event columns sorted by (t_cross, pixel); clears the list.
+void ref_model_take_events(void* h, uint32_t* pixel, uint8_t* p, uint8_t* label, uint16_t* flags, int64_t* t,
+                           float* ds, float* dn, float* dl, float* l_first) {
+  auto* m = static_cast<RefModel*>(h);
+  std::sort(m->events.begin(), m->events.end(), [](const sensor::RawEvent& a, const sensor::RawEvent& b) {
+    return a.t_cross != b.t_cross ? a.t_cross < b.t_cross : a.pixel < b.pixel;
+  });
+  for (size_t i = 0; i < m->events.size(); ++i) {
+    const sensor::RawEvent& e = m->events[i];
+    pixel[i] = e.pixel;
+    p[i] = e.polarity;
+    label[i] = e.label;
+    flags[i] = e.flags;
+    t[i] = e.t_cross;
+    ds[i] = e.ds;
+    dn[i] = e.dn;
+    dl[i] = e.dl;
+    l_first[i] = e.l_first;
+  }
+  m->events.clear();
+}
+
+void ref_model_maps(void* h, double* on, double* off, double* leak, double* dark, double* phi0) {
+  const auto& px = static_cast<RefModel*>(h)->model->maps().pixels;
+  for (size_t i = 0; i < px.size(); ++i) {
+    on[i] = px[i].theta_on;
+    off[i] = px[i].theta_off;
+    leak[i] = px[i].leak;
+    dark[i] = px[i].dark_fA;
+    phi0[i] = px[i].phi0;
+  }
+}
+
+int64_t ref_model_time(void* h) { return static_cast<RefModel*>(h)->model->time_ns(); }
+int ref_model_threads(void* h) { return static_cast<RefModel*>(h)->model->num_threads(); }
+
+// The window's samples by WindowEngine<kHost>::run (src/engine/window_impl.h:715-867). Returns the sample count
+// (offsets n + 1, t and irr filled up to cap) or -(count) when cap is too small; carried_* updated in place.
+int64_t ref_sample_window(const orc_field* f, float tol, float dark, int midpoint, int refine_signature,
+                          int max_refine_levels, int64_t min_dt_ns, int64_t t_w, const uint32_t* pixel,
+                          const uint8_t* level, size_t n, float* carried_irr, uint64_t* carried_sig, int64_t* offsets,
+                          int64_t* t_out, float* irr_out, size_t cap) {
+  try {
+    const engine::SampleConfig cfg = make_config(tol, dark, midpoint, refine_signature, max_refine_levels, min_dt_ns);
+    engine::WindowEngine<engine::Space::kHost> eng;
+    FieldHook hook(f, t_w);
+    engine::WindowEngine<engine::Space::kHost>::Input in{};
+    in.t_w = t_w;
+    in.pixel = pixel;
+    in.level = level;
+    in.n = n;
+    in.carried_irr = carried_irr;
+    in.carried_sig = carried_sig;
+    eng.run(in, cfg, hook, std::numeric_limits<size_t>::max(), nullptr);
+    const size_t s = eng.samples();
+    std::memcpy(offsets, eng.offsets(), (n + 1) * sizeof(int64_t));
+    if (s > cap) return -static_cast<int64_t>(s);
+    std::memcpy(t_out, eng.t(), s * sizeof(int64_t));
+    std::memcpy(irr_out, eng.irr(), s * sizeof(float));
+    return static_cast<int64_t>(s);
+  } catch (const std::exception& e) {
+    fail(e);
+    return INT64_MIN;
+  }
+}
+
+// The whole chain of one sensor on an analytic field, the reference's own code end to end: init at t0 from the
+// field, then per window WindowEngine<kHost> (serial by design, src/engine/par.h:1-8) and SensorModel::advance_runs
+// on the model's thread pool. Levels: the field's rule per pixel and window. Returns the event count, or -1.
+// out_stats: [pixel-samples, sampler seconds, sensor seconds, windows].
+int64_t ref_simulate(void* h, const orc_field* f, float tol, float dark, int max_refine_levels, int64_t min_dt_ns,
+                     int32_t l_min, int32_t l_max, int64_t t0, int32_t windows, double* out_stats) {
+  try {
+    auto* m = static_cast<RefModel*>(h);
+    const uint32_t W = m->model->width(), H = m->model->height();
+    const size_t np = static_cast<size_t>(W) * H;
+    std::vector<float> frame(np);
+    for (size_t p = 0; p < np; ++p) frame[p] = orc_field_eval(f, p % W, p / W, t0);
+    m->model->init(t0, frame.data());
+    std::vector<uint32_t> ids(np);
+    for (size_t p = 0; p < np; ++p) ids[p] = static_cast<uint32_t>(p);
+    std::vector<uint8_t> lv(np);
+    std::vector<float> carried = frame;
+    std::vector<uint64_t> sig(np, 0);
+    std::vector<int32_t> counts(np);
+    const engine::SampleConfig cfg = make_config(tol, dark, 1, 1, max_refine_levels, min_dt_ns);
+    engine::WindowEngine<engine::Space::kHost> eng;
+    double samples = 0, t_sample = 0, t_sense = 0;
+    int64_t events = 0;
+    using clk = std::chrono::steady_clock;
+    for (int32_t w = 0; w < windows; ++w) {
+      const int64_t t_w = t0 + static_cast<int64_t>(w) * time::kWindowNs;
+      const auto a = clk::now();
+      for (size_t p = 0; p < np; ++p) {
+        lv[p] = static_cast<uint8_t>(orc_field_level(f, p % W, p / W, t_w, l_min, l_max));
+      }
+      FieldHook hook(f, t_w);
+      engine::WindowEngine<engine::Space::kHost>::Input in{};
+      in.t_w = t_w;
+      in.pixel = ids.data();
+      in.level = lv.data();
+      in.n = np;
+      in.carried_irr = carried.data();
+      in.carried_sig = sig.data();
+      eng.run(in, cfg, hook, std::numeric_limits<size_t>::max(), nullptr);
+      const auto b = clk::now();
+      const int64_t* off = eng.offsets();
+      for (size_t p = 0; p < np; ++p) counts[p] = static_cast<int32_t>(off[p + 1] - off[p]);
+      std::vector<sensor::RawEvent> ev = m->model->advance_runs_raw(ids.data(), np, eng.t(), eng.irr(), eng.samples(),
+                                                                    off, counts.data(), t_w + time::kWindowNs);
+      const auto c = clk::now();
+      samples += static_cast<double>(eng.samples());
+      events += static_cast<int64_t>(ev.size());
+      m->events.insert(m->events.end(), ev.begin(), ev.end());
+      t_sample += std::chrono::duration<double>(b - a).count();
+      t_sense += std::chrono::duration<double>(c - b).count();
+    }
+    if (out_stats != nullptr) {
+      out_stats[0] = samples;
+      out_stats[1] = t_sample;
+      out_stats[2] = t_sense;
+      out_stats[3] = windows;
+    }
+    return events;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,272 @@
+"""Parity of the CUDA path with the oracle, through the C ABI on a B200: the pixel model on ragged runs, the
+window sampler, the device fields, and the fused engine; bit-exact (integer times, polarities, labels, flags and
+the fp32 increments). Cases at sizes the CPU oracle finishes in seconds; full sizes are checked by properties
+(test_gpu_scale.py)."""
+import numpy as np
+import pytest
+
+from ballasim_b200 import workloads as W
+from ballasim_b200.params import resolve
+
+pytestmark = pytest.mark.gpu
+
+EVENT_KEYS = ("p", "label", "flags", "t_cross_ns", "ds", "dn", "dl", "l_first")
+
+
+def same_events(dev: dict, ora: dict, width: int) -> None:
+    assert len(dev["t_cross_ns"]) == len(ora["t_cross_ns"]), (len(dev["t_cross_ns"]), len(ora["t_cross_ns"]))
+    px = dev["y"].astype(np.int64) * width + dev["x"]
+    assert np.array_equal(px, ora["pixel"].astype(np.int64))
+    for k in EVENT_KEYS:
+        a, b = np.asarray(dev[k]), np.asarray(ora[k])
+        if a.dtype.kind == "f":
+            a, b = a.view(np.uint32), b.view(np.uint32)
+        assert np.array_equal(a, b), f"column {k} differs"
+
+
+def random_calls(rng, n, t0, calls):
+    out, t = [], t0
+    for _ in range(calls):
+        t_end = t + int(rng.integers(1, 3)) * (1 << 23) + int(rng.integers(0, 5000))
+        listed = rng.permutation(n)[: int(rng.integers(0, n + 1))].astype(np.uint32)
+        ts, vs, cnt = [], [], []
+        for _px in listed:
+            k = int(rng.integers(0, 14))
+            times = np.unique(rng.integers(t, t_end + 1, k))
+            if rng.random() < 0.3 and len(times):
+                times[0] = t
+                times = np.unique(times)
+            vals = (rng.uniform(5, 400, len(times)) * rng.choice([1, 1, 1, 3], len(times))).astype(np.float32)
+            ts.append(times.astype(np.int64))
+            vs.append(vals)
+            cnt.append(len(times))
+        tt = np.concatenate(ts) if ts else np.zeros(0, np.int64)
+        vv = np.concatenate(vs) if vs else np.zeros(0, np.float32)
+        starts = np.concatenate([[0], np.cumsum(cnt)[:-1]]).astype(np.int64) if cnt else np.zeros(0, np.int64)
+        out.append((listed, tt, vv, t_end, starts, np.array(cnt, np.int32)))
+        t = t_end
+    return out
+
+
+@pytest.mark.parametrize("overrides", [
+    {},
+    dict(W.MISMATCH),
+    {**W.MISMATCH, "leak_rate_hz": 2.0, "leak_sigma_log10": 0.1},
+    {"reset_mode": "physical", "refractory_s": 0.0, "eps_ci": 0.002, "initial_phase": "symmetric"},
+    {**W.MISMATCH, **W.NOISE, "noise_shot_rate_hz": 50.0, "noise_ba_median_hz": 20.0},
+])
+def test_pixel_model_on_random_runs(cuda_lib, oracle_port, overrides):
+    from ballasim_b200.sensor import SensorModel
+
+    rng = np.random.default_rng(17 + len(overrides))
+    Wd, Hd = 24, 20
+    n = Wd * Hd
+    p = resolve("ideal", overrides)
+    dev = SensorModel(p, Wd, Hd, 5, [{"type": "constant"}], 0)
+    ora = oracle_port.Model(p, Wd, Hd, 5, 0)
+    irr0 = rng.uniform(20, 200, n).astype(np.float32)
+    dev.init(0, irr0.reshape(n, 1))
+    ora.init(0, irr0)
+    got = []
+    for ids, tt, vv, t_end, starts, cnt in random_calls(rng, n, 0, 6):
+        got.append(dev.advance_runs(ids, tt, vv, t_end, starts, cnt))
+        ora.advance_runs(ids, tt, vv, starts, cnt, t_end)
+    merged = {k: np.concatenate([g[k] for g in got]) for k in got[0]}
+    same_events(merged, ora.take_events(), Wd)
+    assert len(merged["t_cross_ns"]) > 10
+    assert dev.time_ns == t_end
+
+
+def test_advance_rectangular_and_ragged_forms_agree(cuda_lib):
+    """Ragged runs give the padded rectangle's events bit for bit (tests/sensor/test_model.cpp:180)."""
+    from ballasim_b200.sensor import SensorModel
+
+    rng = np.random.default_rng(3)
+    n, m = 64, 6
+    t = np.sort(rng.integers(1, 1 << 23, (n, m)), axis=1).astype(np.int64)
+    t = np.maximum.accumulate(t + np.arange(m), axis=1)
+    irr = rng.uniform(10, 300, (n, m, 1)).astype(np.float32)
+    counts = rng.integers(0, m + 1, n).astype(np.int32)
+    ids = np.arange(n, dtype=np.uint32)
+    a = SensorModel("ideal", 8, 8, 2, [{"type": "constant"}], 0)
+    b = SensorModel("ideal", 8, 8, 2, [{"type": "constant"}], 0)
+    irr0 = np.full((n, 1), 100, np.float32)
+    a.init(0, irr0)
+    b.init(0, irr0)
+    ea = a.advance(ids, t, irr, 1 << 23, counts=counts)
+    off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    tt = np.concatenate([t[i, : counts[i]] for i in range(n)]).astype(np.int64)
+    vv = np.concatenate([irr[i, : counts[i]] for i in range(n)]).astype(np.float32)
+    eb = b.advance(ids, tt, vv, 1 << 23, offsets=off)
+    for k in ea:
+        assert np.array_equal(ea[k], eb[k]), k
+
+
+def test_refused_input_leaves_the_model_unchanged(cuda_lib):
+    from ballasim_b200.sensor import SensorModel
+
+    m = SensorModel("ideal", 4, 4, 1, [{"type": "constant"}], 0)
+    with pytest.raises(RuntimeError):
+        m.advance(np.zeros(0, np.uint32), np.zeros(0, np.int64), np.zeros((0, 1), np.float32), 10,
+                  offsets=np.zeros(1, np.int64))  # before init
+    m.init(100, np.full((16, 1), 50, np.float32))
+    one = lambda ids, t, v, t_end: m.advance(np.array(ids, np.uint32), np.array(t, np.int64),  # noqa: E731
+                                             np.array(v, np.float32).reshape(-1, 1), t_end,
+                                             offsets=np.arange(len(ids) + 1, dtype=np.int64))
+    before = m.save_state()
+    for bad in [([1], [900], [60], 800), ([1, 1], [200, 300], [60, 60], 2000), ([99], [300], [60], 2000),
+                ([2], [50], [60], 2000), ([3], [300], [np.nan], 2000)]:
+        with pytest.raises(ValueError):
+            one(*bad)
+        assert m.save_state() == before and m.time_ns == 100
+    with pytest.raises(ValueError):
+        one([1], [200], [60], 50)  # t_end before the model time
+    with pytest.raises(TypeError):
+        m.advance(np.array([1], np.int64), np.array([200], np.int64), np.array([[60]], np.float32), 300,
+                  offsets=np.array([0, 1], np.int64))
+
+
+def test_event_buffer_overflow_reruns(cuda_lib, oracle_port):
+    """More events than the initial device buffer: the call is re-run from its unchanged input state."""
+    from ballasim_b200.sensor import SensorModel
+
+    p = resolve("ideal", {"theta_on": 0.011, "theta_off": 0.011, "theta_floor": 0.01})
+    Wd, Hd = 128, 64
+    n = Wd * Hd
+    dev = SensorModel(p, Wd, Hd, 9, [{"type": "constant"}], 0)
+    ora = oracle_port.Model(p, Wd, Hd, 9, 0)
+    irr0 = np.full(n, 10, np.float32)
+    dev.init(0, irr0.reshape(n, 1))
+    ora.init(0, irr0)
+    ids = np.arange(n, dtype=np.uint32)
+    tt = np.tile(np.array([1 << 22, 1 << 23], np.int64), n)
+    vv = np.tile(np.array([400, 10], np.float32), n)
+    starts = np.arange(n, dtype=np.int64) * 2
+    cnt = np.full(n, 2, np.int32)
+    ev = dev.advance_runs(ids, tt, vv, 1 << 23, starts, cnt)
+    ora.advance_runs(ids, tt, vv, starts, cnt, 1 << 23)
+    assert len(ev["t_cross_ns"]) > (1 << 16)
+    same_events(ev, ora.take_events(), Wd)
+    assert dev.stats()["gpu_reruns"] >= 1
+
+
+def test_save_and_load_state_resume_bitwise(cuda_lib):
+    from ballasim_b200.sensor import SensorModel
+
+    rng = np.random.default_rng(8)
+    n = 10 * 10
+    calls = random_calls(rng, n, 0, 4)
+    full = SensorModel("ideal", 10, 10, 4, [{"type": "constant"}], 0, overrides=W.MISMATCH)
+    part = SensorModel("ideal", 10, 10, 4, [{"type": "constant"}], 0, overrides=W.MISMATCH)
+    irr0 = rng.uniform(20, 200, (n, 1)).astype(np.float32)
+    full.init(0, irr0)
+    part.init(0, irr0)
+    ev_full = [full.advance_runs(c[0], c[1], c[2], c[3], c[4], c[5]) for c in calls]
+    for c in calls[:2]:
+        part.advance_runs(c[0], c[1], c[2], c[3], c[4], c[5])
+    blob = part.save_state()
+    fresh = SensorModel("ideal", 10, 10, 4, [{"type": "constant"}], 0, overrides=W.MISMATCH)
+    fresh.load_state(blob)
+    rest = [fresh.advance_runs(c[0], c[1], c[2], c[3], c[4], c[5]) for c in calls[2:]]
+    for a, b in zip(ev_full[2:], rest):
+        for k in a:
+            assert np.array_equal(a[k], b[k]), k
+    other = SensorModel("ideal", 10, 10, 5, [{"type": "constant"}], 0)
+    with pytest.raises(ValueError):
+        other.load_state(blob)
+
+
+@pytest.mark.parametrize("case", ["edge", "blobs"])
+def test_fields_and_levels_equal_the_oracle(cuda_lib, oracle_port, case):
+    from ballasim_b200.sampling import field_frame, field_levels
+
+    wl = W.small("edge", 37, 23, 1) if case == "edge" else W.small("blobs", 70, 50, 1)
+    f = wl.sensors[0].field
+    for t in (0, 3 << 23, (5 << 23) + 12345):
+        assert np.array_equal(field_frame(f, t).view(np.uint32), oracle_port.field_frame(f, t).view(np.uint32))
+    for w in (0, 7):
+        assert np.array_equal(field_levels(f, w << 23), oracle_port.levels(f, w << 23, 1, 10))
+
+
+@pytest.mark.parametrize("case", ["edge", "blobs", "blobs_listed"])
+def test_sample_window_equals_the_oracle(cuda_lib, oracle_port, case):
+    from ballasim_b200.sampling import MidpointTest, sample_window
+
+    wl = W.small("edge", 20, 16, 1) if case == "edge" else W.small("blobs", 48, 40, 1)
+    spec, r = wl.sensors[0], wl.rules
+    f = spec.field
+    n = spec.width * spec.height
+    rng = np.random.default_rng(1)
+    ids = np.arange(n, dtype=np.uint32) if case != "blobs_listed" else rng.permutation(n)[: n // 3].astype(np.uint32)
+    mt = MidpointTest(r.tol, r.dark, [1.0], [1.0])
+    carried = oracle_port.field_frame(f, 0)[ids]
+    sig = np.zeros(len(ids), np.uint64)
+    if case == "blobs_listed":
+        sig[::7] = 5  # carried signatures that differ from the rendered ones flip the first interval
+    c_dev, s_dev = carried.copy(), sig.copy()
+    for w in range(3):
+        t_w = w << 23
+        lv_all = oracle_port.levels(f, t_w, 1, 10)
+        lv = lv_all[ids] if case != "edge" else np.minimum(lv_all[ids] + (ids % 3).astype(np.uint8), 10)
+        t, irr, off, carried, sig = oracle_port.sample_window(f, r, t_w, ids, lv, carried, sig)
+        runs = sample_window(t_w, ids, lv, np.arange(len(ids)), c_dev.reshape(-1, 1), s_dev, f,
+                             refine_signature=True, midpoint=mt, max_refine_levels=r.max_refine_levels,
+                             min_dt_ns=r.min_dt_ns)
+        assert np.array_equal(runs.offsets, off)
+        assert np.array_equal(runs.t_ns, t)
+        assert np.array_equal(runs.irradiance.reshape(-1).view(np.uint32), irr.view(np.uint32))
+        assert np.array_equal(runs.last_irradiance.reshape(-1).view(np.uint32), carried.view(np.uint32))
+        c_dev, s_dev = runs.last_irradiance.reshape(-1), runs.last_signature
+
+
+def test_midpoint_test_matches_numpy_fp32(cuda_lib):
+    """eta_L equals NumPy fp32 in sampling.py's operation order (tests/cpp/engine/test_window.cpp:19)."""
+    from ballasim_b200.sampling import MidpointTest
+
+    rng = np.random.default_rng(4)
+    a, m, b = (rng.uniform(0, 300, (500, 2)).astype(np.float32) for _ in range(3))
+    t = MidpointTest(0.01, 0.01, [0.5, 1.0], [1.5, 1.0])
+    got = t.eta(a, m, b)
+    dev = np.abs((a + b) * np.float32(-0.5) + m)
+    low = np.minimum(np.minimum(a, m), b)
+    num = np.float32(0) + np.float32(1.5) * dev[:, 0]
+    num = num + np.float32(1.0) * dev[:, 1]
+    den = np.float32(0.01) + np.float32(0.5) * low[:, 0]
+    den = den + np.float32(1.0) * low[:, 1]
+    med = np.maximum(np.maximum(np.float32(0), np.where(dev[:, 0] == 0, 0, dev[:, 0] / low[:, 0])),
+                     np.where(dev[:, 1] == 0, 0, dev[:, 1] / low[:, 1])).astype(np.float32)
+    want = np.minimum(num / den, med)
+    assert np.array_equal(got.view(np.uint32), want.astype(np.float32).view(np.uint32))
+    assert np.array_equal(t.exceeds(a, m, b), want > np.float32(0.01))
+
+
+@pytest.mark.parametrize("case", ["edge", "blobs", "noise"])
+def test_engine_equals_the_oracle_chain(cuda_lib, case):
+    """The fused engine (sampler and pixel model on one thread, all windows in one launch) gives the oracle
+    chain's events (sample_window, then advance, per window) bit for bit."""
+    from ballasim_b200.engine import Engine
+    from ballasim_b200.sensor import SensorModel
+    from oracle.oracle import simulate_port
+
+    wl = {"edge": lambda: W.small("edge", 30, 20, 24), "blobs": lambda: W.small("blobs", 60, 40, 24),
+          "noise": lambda: W.small("noise", 40, 30, 30)}[case]()
+    spec = wl.sensors[0]
+    p = resolve("ideal", spec.overrides)
+    if case == "noise":  # rates high enough for many noise events in a short run
+        p = resolve(p, {"noise_shot_rate_hz": 40.0, "noise_ba_median_hz": 30.0, "leak_rate_hz": 3.0})
+    ora, st = simulate_port(spec, wl.rules, wl.windows, params=p)
+    m = SensorModel(p, spec.width, spec.height, spec.seed, [{"type": "constant"}], spec.camera)
+    r = wl.rules
+    eng = Engine([(m, spec.field)], tol=r.tol, dark=r.dark, min_dt_ns=r.min_dt_ns,
+                 max_refine_levels=r.max_refine_levels, l_min=r.l_min, l_max=r.l_max)
+    eng.start(0)
+    samples = 0
+    for chunk in (5, wl.windows - 5):  # two calls: the state and carried samples cross the call boundary
+        s, _ = eng.run(chunk)
+        samples += s
+    ev = m.take_events()
+    assert samples == st["pixel_samples"]
+    same_events(ev, ora, spec.width)
+    assert len(ev["t_cross_ns"]) > 20
+    if case == "noise":
+        assert np.count_nonzero(ev["label"] == 1) > 5
