@@ -601,7 +601,7 @@ SamplerRules make_rules(const bs_sample_rules& r) {
   s.midpoint = r.midpoint;
   s.refine_signature = r.refine_signature;
   // A depth-first walk stops where halves fall under min_split anyway; deeper caps change nothing.
-  s.max_refine_levels = std::min(r.max_refine_levels, 24);
+  s.max_refine_levels = std::min(r.max_refine_levels, 23);
   s.min_split = static_cast<uint32_t>(2 * r.min_dt_ns);
   s.l_min = r.l_min;
   s.l_max = std::min(r.l_max, kWindowLog2 - shift);

@@ -52,7 +52,10 @@ BS_HD uint32_t sample_pixel_window(const SamplerRules& r, int level, float carri
     uint32_t phase;  // 0: mid not yet rendered; 1: left half done
     bool flip, bad;
   };
-  Frame st[16];
+  // A selected interval halves at most 22 times above min_split >= 2 (2^23 ns down to 2 ns), and the rules clamp
+  // max_refine_levels to kMaxDepth, so the walk never holds more than kMaxDepth frames.
+  constexpr int kMaxDepth = 24;
+  Frame st[kMaxDepth];
   const uint32_t count = (1u << level) + 1u, step = 1u << (kWindowLog2 - level);
   uint32_t n = 0;
   // Sliding lattice values v[j - 2], v[j - 1], v[j], v[j + 1].
@@ -75,7 +78,8 @@ BS_HD uint32_t sample_pixel_window(const SamplerRules& r, int level, float carri
           // HalfFlags (sampling.h:638-678): the triple (lo, mid, hi) flags both halves.
           f.bad = exceeds(r, f.vlo, f.vg, f.vhi);
           f.phase = 1u;
-          if ((f.flip || f.bad) && f.g - f.lo >= r.min_split && f.depth + 1 < r.max_refine_levels) {
+          if ((f.flip || f.bad) && f.g - f.lo >= r.min_split && f.depth + 1 < r.max_refine_levels &&
+              sp < kMaxDepth) {
             st[sp] = Frame{f.lo, f.g, 0u, f.vlo, f.vg, 0.0f, f.depth + 1, 0u, f.flip, false};
             ++sp;
           }

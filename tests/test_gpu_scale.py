@@ -20,11 +20,12 @@ def engine_events(wl, chunks):
     eng = Engine([(m, spec.field)], tol=r.tol, dark=r.dark, min_dt_ns=r.min_dt_ns,
                  max_refine_levels=r.max_refine_levels, l_min=r.l_min, l_max=r.l_max)
     eng.start(0)
-    total = 0
+    total, parts = 0, []
     for c in chunks:
         s, _ = eng.run(c)
         total += s
-    return m.take_events(with_pixel=True), total
+        parts.append(m.take_events(with_pixel=True))
+    return {k: np.concatenate([p[k] for p in parts]) for k in parts[0]}, total
 
 
 def test_engine_equals_sampler_then_sensor_at_full_frame(cuda_lib):
