@@ -91,6 +91,9 @@ _SIGS = {
     "bs_sample_window": (C.c_int32, [_P, C.c_int64, _P, _P, C.c_size_t, _P, _P, C.POINTER(SampleRules),
                                      C.POINTER(C.c_size_t)]),
     "bs_sampler_download": (C.c_int32, [_P, _P, _P, _P]),
+    "bs_sample_window_static": (C.c_int32, [C.POINTER(Field), C.c_int64, _P, _P, C.c_size_t, _P, _P,
+                                            C.POINTER(SampleRules), _P, _P, _P, C.c_size_t, _P, _P, _P,
+                                            C.POINTER(C.c_size_t)]),
     "bs_sampler_device_runs": (C.c_int32, [_P, C.POINTER(DeviceRuns)]),
     "bs_field_levels": (C.c_int32, [_P, C.c_int64, C.c_int32, C.c_int32, _P]),
     "bs_field_frame": (C.c_int32, [_P, C.c_int64, _P]),

@@ -863,6 +863,11 @@ static bs_status guarded(F&& f) {
   }
 }
 
+namespace bs {
+// For entry points in other translation units: the message bs_last_error() returns on this thread.
+void set_last_error(const char* msg) { g_error = msg; }
+}  // namespace bs
+
 #define NEED(p)                                                      \
   do {                                                               \
     if (!(p)) throw std::invalid_argument("null argument: " #p);     \

@@ -165,6 +165,22 @@ bs_status bs_sample_window(bs_sampler* s, int64_t t_w, const uint32_t* pixel_ids
  * bs_model_advance_device (valid until the sampler runs again). */
 bs_status bs_sampler_download(bs_sampler* s, int64_t* offsets, int64_t* t_ns, float* irr);
 bs_status bs_sampler_device_runs(bs_sampler* s, bs_device_runs* out);
+/* sample_window for callers that cannot allocate device memory: code running under an external memory manager with
+ * a fixed budget, or code that must not call cudaMalloc / cudaFree because they synchronize the device. No
+ * counterpart in the reference. Every array is the caller's, in device memory: the field's blob table, pixel ids,
+ * levels, carried samples in and out, offsets (n + 1), and t_ns / irr with room for `capacity` samples. The
+ * entry point allocates nothing: its scratch (the per-pixel sample counts and the scan's block sums) is one static
+ * device array sized for at most 1,048,576 pixels (about 4 MiB, held by every GPU that loads the library until the
+ * process exits); more pixels are refused (BS_EINVAL). It runs on the current device and on `stream` (NULL: the
+ * default stream); its first call on a device looks up the array's device address, so make that first call before
+ * any stream capture. *n_samples receives the window's sample count, also when it exceeds capacity (BS_EINVAL, the
+ * outputs then unwritten). All calls share the one array: calls that overlap on the GPU (other streams, other host
+ * threads) race and must be serialized by the caller. */
+bs_status bs_sample_window_static(const bs_field* field, int64_t t_w, const uint32_t* pixel_ids,
+                                  const uint8_t* levels, size_t n, const float* carried_irr,
+                                  const uint64_t* carried_sig, const bs_sample_rules* rules, int64_t* offsets,
+                                  int64_t* t_ns, float* irr, size_t capacity, float* carried_irr_out,
+                                  uint64_t* carried_sig_out, void* stream, size_t* n_samples);
 /* The field's level rule per pixel at t_w, and the field itself at t (width * height, host outputs). */
 bs_status bs_field_levels(bs_sampler* s, int64_t t_w, int32_t l_min, int32_t l_max, uint8_t* out);
 bs_status bs_field_frame(bs_sampler* s, int64_t t_ns, float* out);
