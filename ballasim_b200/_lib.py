@@ -80,6 +80,7 @@ _SIGS = {
     "bs_model_take_events": (C.c_int32, [_P, C.POINTER(EventColumns)]),
     "bs_model_maps": (C.c_int32, [_P, _P, _P, _P, _P, _P]),
     "bs_model_stats": (C.c_int32, [_P, _P]),
+    "bs_model_noise_maps": (C.c_int32, [_P, _P, _P]),
     "bs_model_reset_stats": (C.c_int32, [_P]),
     "bs_model_info": (C.c_int32, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_float), C.POINTER(C.c_int32)]),
     "bs_model_state_bytes": (C.c_int32, [_P, C.POINTER(C.c_size_t)]),
@@ -104,7 +105,7 @@ _SIGS = {
     "bs_engine_start": (C.c_int32, [_P, C.c_int64, _P]),
     "bs_engine_start_frames": (C.c_int32, [_P, C.c_int64, _P, _P]),
     "bs_engine_run": (C.c_int32, [_P, C.c_int32, _P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
-    "bs_engine_set_launch": (C.c_int32, [_P, C.c_int32, C.c_int32]),
+    "bs_engine_set_launch": (C.c_int32, [_P, C.c_int32, C.c_int32, C.c_int32]),
     "bs_engine_last_ms": (C.c_int32, [_P, C.POINTER(C.c_double)]),
 }
 

@@ -11,12 +11,16 @@
 
 #include <stdint.h>
 
+// BS_HD: shared host/device code, inlined where the compiler finds it worth it. BS_COLD: a rare path kept out of
+// line on the device, one copy per kernel, so that the hot loops' code stays small enough for the instruction cache.
 #if defined(__CUDACC__)
-#define BS_HD __host__ __device__ __forceinline__
+#define BS_HD __host__ __device__ inline
 #define BS_D __device__ __forceinline__
+#define BS_COLD __host__ __device__ __noinline__
 #else
 #define BS_HD inline
 #define BS_D inline
+#define BS_COLD
 #endif
 
 #if !defined(__CUDA_ARCH__)

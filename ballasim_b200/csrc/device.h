@@ -92,11 +92,12 @@ void launch_levels(const FieldDev& f, int64_t t_w, int32_t l_min, int32_t l_max,
                    cudaStream_t stream);
 void launch_field_frame(const FieldDev& f, int64_t t, uint32_t n_pixels, float* out, cudaStream_t stream);
 // The fused engine: windows [w0, w1) of every sensor, one warp per 8 x 4 pixel tile, tiles taken from a global
-// counter (work stealing) by a persistent grid.
+// counter (work stealing) by a persistent grid. stage 0: the sampler feeds the pixel model sample by sample;
+// 16 or 32: per window the samples are staged in shared memory (that many per lane) between the two phases.
 void launch_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t total_tiles, int64_t t0, int32_t w0,
                    int32_t w1, const SamplerRules& r, unsigned int* tile_counter, int blocks, int warps_per_block,
-                   cudaStream_t stream);
-int engine_max_blocks_per_sm(int warps_per_block);
+                   int stage, cudaStream_t stream);
+int engine_max_blocks_per_sm(int warps_per_block, int stage);
 // MidpointTest.eta over n triples of g groups (rows of g floats).
 void launch_midpoint_eta(float tol, float dark, int32_t g, const float* m_min, const float* m_max, const float* ea,
                          const float* em, const float* eb, uint32_t n, float* eta, uint8_t* exceeds,

@@ -175,6 +175,8 @@ __global__ void __launch_bounds__(128) advance_runs_kernel(RunArgs a) {
       } else {
         const int64_t* tp = a.t + s0;
         const float* vp = a.irr + s0;
+        float x_prev = 0.0f;
+        bool have_x = false;
         for (int32_t i = 0; i < cnt; ++i) {
           const int64_t ti = __ldg(tp + i);
           const float raw = __ldg(vp + i);
@@ -193,7 +195,17 @@ __global__ void __launch_bounds__(128) advance_runs_kernel(RunArgs a) {
             prev_v = vi;
             continue;
           }
-          proc.segment(Segment{prev_t, ti, prev_v, vi}, prev_t, ti);
+          // A segment inside one 2^23 ns piece takes the fast path with x at both ends (each computed once).
+          if (((ti - 1) >> kWindowLog2) == (prev_t >> kWindowLog2)) {
+            if (!have_x) x_prev = proc.x_at_sample(prev_v);
+            const float x1 = proc.x_at_sample(vi);
+            proc.segment_fast(Segment{prev_t, ti, prev_v, vi}, x_prev, x1);
+            x_prev = x1;
+            have_x = true;
+          } else {
+            proc.segment(Segment{prev_t, ti, prev_v, vi}, prev_t, ti);
+            have_x = false;
+          }
           prev_t = ti;
           prev_v = vi;
         }
@@ -239,20 +251,23 @@ __global__ void __launch_bounds__(128) sample_window_kernel(WindowArgs a) {
   const bool have = i < a.n;
   const uint32_t px = have ? a.pixel[i] : 0u;
   const uint32_t x = a.f.width > 0 ? px % a.f.width : 0u, y = a.f.width > 0 ? px / a.f.width : 0u;
-  const BlobMask mask = warp_blob_mask(a.f, 0xffffffffu, have, x, y, a.t_w);
+  __shared__ uint16_t lists[4][kMaxListed];
+  const BlobList list = warp_blob_list(a.f, have, x, y, a.t_w, a.t_w + kWindowNs, lists[threadIdx.x >> 5]);
   if (!have) return;
   const float carried = a.carried_in[i];
   const bool flip = a.sig_in[i] != 0ull;
   const FieldDev& f = a.f;
   const int64_t t_w = a.t_w;
-  auto render = [&](uint32_t dt) { return field_eval(f, mask, x, y, t_w + dt); };
+  auto render = [&](uint32_t dt) { return field_eval(f, list, x, y, t_w + dt); };
   if (kPass == 0) {
     const uint32_t n = sample_pixel_window(a.r, a.level[i], carried, flip, render, [](uint32_t, float) {});
     a.counts[i] = n;
   } else {
     int64_t* t_out = a.t_out + a.offsets[i];
     float* irr_out = a.irr_out + a.offsets[i];
-    uint32_t k = 0;
+    t_out[0] = t_w;  // slot 0: the carried sample
+    irr_out[0] = carried;
+    uint32_t k = 1;
     float last = carried;
     sample_pixel_window(a.r, a.level[i], carried, flip, render, [&](uint32_t dt, float v) {
       t_out[k] = t_w + dt;
@@ -270,8 +285,9 @@ __global__ void levels_kernel(FieldDev f, int64_t t_w, int32_t l_min, int32_t l_
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
   const bool have = p < n_pixels;
   const uint32_t x = have ? p % f.width : 0u, y = have ? p / f.width : 0u;
-  const BlobMask mask = warp_blob_mask(f, 0xffffffffu, have, x, y, t_w);
-  if (have) level[p] = static_cast<uint8_t>(field_level(f, mask, x, y, t_w, l_min, l_max));
+  __shared__ uint16_t lists[4][kMaxListed];
+  const BlobList list = warp_blob_list(f, have, x, y, t_w, t_w, lists[threadIdx.x >> 5]);
+  if (have) level[p] = static_cast<uint8_t>(field_level(f, list, x, y, t_w, l_min, l_max));
 }
 
 __global__ void field_frame_kernel(FieldDev f, int64_t t, uint32_t n_pixels, float* out) {
@@ -358,6 +374,8 @@ struct EngineArgs {
   unsigned int* tile_counter;
 };
 
+// Feeds a window's samples, in time order, to the pixel model: every segment lies inside the window, so each
+// takes the fast path with x at both ends, each x computed once.
 struct WindowFeed {
   PixelProc<GlobalSink>* proc;
   int64_t t_w;
@@ -365,17 +383,22 @@ struct WindowFeed {
   int64_t prev_t;
   float prev_v;
   float last_raw;
+  float x_prev;
+  // Slot 0, the carried sample, sits at the model time: it replaces the held one.
+  __device__ __forceinline__ void start(float carried) {
+    last_raw = carried;
+    prev_v = clamp_irr(carried, irr_max);
+    x_prev = proc->x_at_sample(prev_v);
+  }
   __device__ __forceinline__ void operator()(uint32_t dt, float v) {
     last_raw = v;
     const float vc = clamp_irr(v, irr_max);
-    if (dt == 0u) {  // the carried sample sits at the model time: it replaces the held one
-      prev_v = vc;
-      return;
-    }
     const int64_t t = t_w + dt;
-    proc->segment(Segment{prev_t, t, prev_v, vc}, prev_t, t);
+    const float x1 = proc->x_at_sample(vc);
+    proc->segment_fast(Segment{prev_t, t, prev_v, vc}, x_prev, x1);
     prev_t = t;
     prev_v = vc;
+    x_prev = x1;
   }
 };
 
@@ -407,14 +430,100 @@ __global__ void __launch_bounds__(128) engine_kernel(EngineArgs a) {
     GlobalSink sink{S.ev, &S.counters[kCntEvents]};
     PixelProc<GlobalSink> proc{s, m, S.consts, p, sink, c};
     const FieldDev& f = S.field;
+    __shared__ uint16_t lists[4][kMaxListed];
+    uint16_t* my_list = lists[threadIdx.x >> 5];
     for (int32_t w = a.w0; w < a.w1; ++w) {
       const int64_t t_w = a.t0 + static_cast<int64_t>(w) * kWindowNs;
-      const BlobMask mask = warp_blob_mask(f, 0xffffffffu, have, x, y, t_w);
+      const BlobList list = warp_blob_list(f, have, x, y, t_w, t_w + kWindowNs, my_list);
       if (have) {
-        const int level = field_level(f, mask, x, y, t_w, a.r.l_min, a.r.l_max);
-        WindowFeed feed{&proc, t_w, S.consts.irr_max, t_w, s.held, carried};
-        auto render = [&](uint32_t dt) { return field_eval(f, mask, x, y, t_w + dt); };
+        const int level = field_level(f, list, x, y, t_w, a.r.l_min, a.r.l_max);
+        WindowFeed feed{&proc, t_w, S.consts.irr_max, t_w, s.held, carried, 0.0f};
+        feed.start(carried);
+        auto render = [&](uint32_t dt) { return field_eval(f, list, x, y, t_w + dt); };
         samples += sample_pixel_window(a.r, level, carried, false, render, feed);
+        s.held = feed.prev_v;
+        carried = feed.last_raw;
+      }
+      __syncwarp();
+    }
+    if (have) {
+      store_state(S.out, p, noise, s);
+      S.carried_out[p] = carried;
+    }
+    warp_add(&S.counters[kCntPieces], c.pieces);
+    warp_add(&S.counters[kCntLeaves], c.leaves);
+    warp_add(&S.counters[kCntSamples], samples);
+    warp_add(&S.counters[kCntNoise], c.noise_candidates);
+  }
+}
+
+// The engine in two phases per window: phase A runs every lane's sampler walk and stages its samples (dt, v) in
+// shared memory, kStage per lane (lane-minor, so a warp's stores and loads hit 32 banks); phase B feeds every lane's
+// staged samples to its pixel model. Each phase is one compact loop that all lanes run together, instead of the
+// sampler and the pixel model alternating per sample across diverged lanes. A window with more samples than kStage
+// is redone by its lane in the streaming form (the same samples: the walk is deterministic).
+template <int kStage>
+__global__ void __launch_bounds__(128) engine_kernel_staged(EngineArgs a) {
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  __shared__ uint16_t lists[4][kMaxListed];
+  __shared__ uint32_t st_dt[4][kStage][32];
+  __shared__ float st_v[4][kStage][32];
+  uint16_t* my_list = lists[warp];
+  for (;;) {
+    uint32_t tile = 0;
+    if (lane == 0) tile = atomicAdd(a.tile_counter, 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if (tile >= a.total_tiles) break;
+    int si = 0;
+    while (si + 1 < a.n_sensors && a.sensors[si + 1].tile0 <= tile) ++si;
+    const EngineSensor& S = a.sensors[si];
+    const uint32_t local = tile - S.tile0;
+    const uint32_t x = (local % S.tiles_x) * 8u + (lane & 7u), y = (local / S.tiles_x) * 4u + (lane >> 3);
+    const bool have = x < S.width && y < S.height;
+    const uint32_t p = have ? y * S.width + x : 0u;
+    const bool noise = S.consts.noise != 0;
+    PixelRegs s;
+    PixelMapRegs m;
+    float carried = 0.0f;
+    if (have) {
+      load_state(S.in, p, noise, s);
+      load_map(S.map, p, m);
+      carried = S.carried_in[p];
+    }
+    PixelCounters c;
+    unsigned long long samples = 0;
+    GlobalSink sink{S.ev, &S.counters[kCntEvents]};
+    PixelProc<GlobalSink> proc{s, m, S.consts, p, sink, c};
+    const FieldDev& f = S.field;
+    for (int32_t w = a.w0; w < a.w1; ++w) {
+      const int64_t t_w = a.t0 + static_cast<int64_t>(w) * kWindowNs;
+      const BlobList list = warp_blob_list(f, have, x, y, t_w, t_w + kWindowNs, my_list);
+      auto render = [&](uint32_t dt) { return field_eval(f, list, x, y, t_w + dt); };
+      // Phase A: the walk, its first kStage samples after slot 0 staged.
+      uint32_t n = 0;
+      int level = 0;
+      if (have) {
+        level = field_level(f, list, x, y, t_w, a.r.l_min, a.r.l_max);
+        uint32_t k = 0;
+        n = sample_pixel_window(a.r, level, carried, false, render, [&](uint32_t dt, float v) {
+          if (k < static_cast<uint32_t>(kStage)) {
+            st_dt[warp][k][lane] = dt;
+            st_v[warp][k][lane] = v;
+          }
+          ++k;
+        });
+      }
+      __syncwarp();
+      // Phase B: the pixel model over the staged samples.
+      if (have) {
+        WindowFeed feed{&proc, t_w, S.consts.irr_max, t_w, s.held, carried, 0.0f};
+        feed.start(carried);
+        if (n - 1 <= static_cast<uint32_t>(kStage)) {
+          for (uint32_t k = 0; k + 1 < n; ++k) feed(st_dt[warp][k][lane], st_v[warp][k][lane]);
+        } else {
+          sample_pixel_window(a.r, level, carried, false, render, feed);
+        }
+        samples += n;
         s.held = feed.prev_v;
         carried = feed.last_raw;
       }
@@ -538,14 +647,22 @@ void launch_field_frame(const FieldDev& f, int64_t t, uint32_t n_pixels, float* 
 
 void launch_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t total_tiles, int64_t t0, int32_t w0,
                    int32_t w1, const SamplerRules& r, unsigned int* tile_counter, int blocks, int warps_per_block,
-                   cudaStream_t stream) {
+                   int stage, cudaStream_t stream) {
   EngineArgs a{sensors_dev, n_sensors, total_tiles, t0, w0, w1, r, tile_counter};
-  engine_kernel<<<blocks, warps_per_block * 32, 0, stream>>>(a);
+  if (stage == 16) engine_kernel_staged<16><<<blocks, warps_per_block * 32, 0, stream>>>(a);
+  else if (stage == 32) engine_kernel_staged<32><<<blocks, warps_per_block * 32, 0, stream>>>(a);
+  else engine_kernel<<<blocks, warps_per_block * 32, 0, stream>>>(a);
 }
 
-int engine_max_blocks_per_sm(int warps_per_block) {
+int engine_max_blocks_per_sm(int warps_per_block, int stage) {
   int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel, warps_per_block * 32, 0);
+  if (stage == 16) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel_staged<16>, warps_per_block * 32, 0);
+  } else if (stage == 32) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel_staged<32>, warps_per_block * 32, 0);
+  } else {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel, warps_per_block * 32, 0);
+  }
   return n;
 }
 

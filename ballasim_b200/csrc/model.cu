@@ -690,7 +690,7 @@ struct Engine {
   DevBuf<unsigned int> tile_counter;
   std::vector<EngineSensor> host;
   uint32_t total_tiles = 0;
-  int warps_per_block = 4, blocks_per_sm = 0;
+  int warps_per_block = 4, blocks_per_sm = 0, stage = 0;
   double last_ms = 0;
   Timer timer;
   cudaStream_t own = nullptr;
@@ -759,7 +759,8 @@ struct Engine {
     int dev = 0, sms = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const int per_sm = blocks_per_sm > 0 ? blocks_per_sm : std::max(1, engine_max_blocks_per_sm(warps_per_block));
+    const int per_sm =
+        blocks_per_sm > 0 ? blocks_per_sm : std::max(1, engine_max_blocks_per_sm(warps_per_block, stage));
     const int blocks = static_cast<int>(std::min<uint64_t>(static_cast<uint64_t>(sms) * per_sm,
                                                            (total_tiles + warps_per_block - 1) / warps_per_block));
     for (;;) {
@@ -781,8 +782,8 @@ struct Engine {
       CK(cudaMemsetAsync(tile_counter.p, 0, sizeof(unsigned int), s));
       CK(cudaEventRecord(timer.a, s));
       if (windows > 0 && total_tiles > 0) {
-        launch_engine(sensors_dev.p, static_cast<int>(host.size()), total_tiles, t0 - 0, 0, windows, rules,
-                      tile_counter.p, blocks, warps_per_block, s);
+        launch_engine(sensors_dev.p, static_cast<int>(host.size()), total_tiles, t0, 0, windows, rules,
+                      tile_counter.p, blocks, warps_per_block, stage, s);
       }
       CK(cudaGetLastError());
       CK(cudaEventRecord(timer.b, s));
@@ -971,6 +972,14 @@ bs_status bs_model_maps(const bs_model* m, double* on, double* off, double* leak
     if (leak) std::copy_n(m->maps.leak.data(), n, leak);
     if (dark) std::copy_n(m->maps.dark.data(), n, dark);
     if (phi0) std::copy_n(m->maps.phi0.data(), n, phi0);
+  });
+}
+bs_status bs_model_noise_maps(const bs_model* m, double* ba_rate_hz, double* shot_max_hz) {
+  return guarded([&] {
+    NEED(m);
+    const size_t n = m->n;
+    if (ba_rate_hz) std::copy_n(m->maps.ba_rate.data(), n, ba_rate_hz);
+    if (shot_max_hz) bs::CK(cudaMemcpy(shot_max_hz, m->map.shot_max, n * sizeof(double), cudaMemcpyDeviceToHost));
   });
 }
 bs_status bs_model_stats(const bs_model* m, uint64_t out[9]) {
@@ -1206,15 +1215,17 @@ bs_status bs_engine_run(bs_engine* e, int32_t windows, void* stream, uint64_t* p
     e->run(windows, stream ? static_cast<cudaStream_t>(stream) : e->own, pixel_samples, events);
   });
 }
-bs_status bs_engine_set_launch(bs_engine* e, int32_t warps_per_block, int32_t blocks_per_sm) {
+bs_status bs_engine_set_launch(bs_engine* e, int32_t warps_per_block, int32_t blocks_per_sm, int32_t stage) {
   return guarded([&] {
     NEED(e);
     if (warps_per_block != 0 && (warps_per_block < 1 || warps_per_block > 4)) {
       throw std::invalid_argument("warps per block must lie in [1, 4]");
     }
     if (blocks_per_sm < 0) throw std::invalid_argument("blocks per SM must be >= 0");
+    if (stage != 0 && stage != 16 && stage != 32) throw std::invalid_argument("staging depth must be 0, 16 or 32");
     e->warps_per_block = warps_per_block == 0 ? 4 : warps_per_block;
     e->blocks_per_sm = blocks_per_sm;
+    e->stage = stage;
   });
 }
 bs_status bs_engine_last_ms(const bs_engine* e, double* ms) {

@@ -82,8 +82,8 @@ BS_HD uint8_t first_label(bool on, float ds, float dn, float l, float cut) {
 }
 
 // The next candidate of a noise chain after t (kForever without a rate).
-BS_HD int64_t noise_next(uint64_t seed, uint32_t purpose, uint32_t camera, uint32_t pixel, uint32_t n, int64_t t,
-                         double rate_hz) {
+static BS_COLD int64_t noise_next(uint64_t seed, uint32_t purpose, uint32_t camera, uint32_t pixel, uint32_t n,
+                                  int64_t t, double rate_hz) {
   if (!(rate_hz > 0.0)) return kForever;
   const U4 w = draw(seed, purpose, camera, pixel, n);
   const double dt = -log_d(open_uniform_d(w.v[0])) / rate_hz * 1e9;
@@ -130,7 +130,7 @@ struct PixelProc {
   }
 
   // The event and the reset (pixel.h:1534-1588); label_override >= 0 labels a noise event.
-  BS_HD void fire(int64_t t, bool on, float x, int label_override) {
+  BS_COLD void fire(int64_t t, bool on, float x, int label_override) {
     const float ds = x - s.s3_ref;
     const float dn = 0.0f - s.n3_ref;
     const float l = m.leak * since_ref(t, s.t_ref);
@@ -165,7 +165,7 @@ struct PixelProc {
 
   // Can Delta reach a level at an integer of (a, c]? Constant light: curvature 0 and no range cap
   // (instant_may_fire with instant_curvature's linear case).
-  BS_HD bool may_fire(int64_t a, int64_t cc, float Ia, float Ic) const {
+  BS_COLD bool may_fire(int64_t a, int64_t cc, float Ia, float Ic) const {
     const float eps = 0x1p-23f;
     float hi = maxr(Ia, Ic), lo = minr(Ia, Ic);
     const float margin = 64.0f * eps * (hi + 2.0f * 0.0f);
@@ -189,7 +189,7 @@ struct PixelProc {
   }
 
   // The first integer t in [lo, hi) where Delta fires (instant_search): found, polarity, time and x(t).
-  BS_HD bool search(const Segment& g, int64_t lo, int64_t hi, int64_t& t_hit, bool& on, float& x_hit) {
+  BS_COLD bool search(const Segment& g, int64_t lo, int64_t hi, int64_t& t_hit, bool& on, float& x_hit) {
     const float I_lo = current(g, lo);
     float x = log_ratio(I_lo);
     float D = delta(lo, x);
@@ -242,7 +242,7 @@ struct PixelProc {
   }
 
   // Drops the earliest noise candidate (refractory or dead time) or tests and fires it; advances its chain.
-  BS_HD void noise_candidate(const Segment& g, int64_t tn, bool blind) {
+  BS_COLD void noise_candidate(const Segment& g, int64_t tn, bool blind) {
     ++c.noise_candidates;
     const bool shot = s.t_shot <= s.t_ba;
     const uint32_t purpose = shot ? kPurposeShot : kPurposeBackground;
@@ -264,7 +264,7 @@ struct PixelProc {
   }
 
   // One piece [t, e) inside segment g (advance_instant's inner loop), with the noise candidates it holds.
-  BS_HD void piece(const Segment& g, int64_t t, int64_t e) {
+  BS_COLD void piece(const Segment& g, int64_t t, int64_t e) {
     ++c.pieces;
     for (;;) {
       const int64_t tn = k.noise ? mini(s.t_shot, s.t_ba) : kForever;
@@ -310,6 +310,82 @@ struct PixelProc {
       piece(g, t, e);
       t = e;
     }
+  }
+
+  // x(t) = ln(I / i_scale) at a sample of value v (the start of the segment it opens).
+  BS_HD float x_at_sample(float v) const { return log_ratio(m.dark + m.scale * v); }
+
+  // A whole segment g = [t0, t1) that is one piece (no multiple of 2^23 ns inside), with x0 = x(t0) and
+  // x1 = x(t1) (the next segment's start, x_at_sample(g.v1)). Bitwise piece(g, t0, t1): where the pixel is not
+  // blind, nothing is pending before t0 and no noise candidate falls inside, Delta(t0) is tested exactly as the
+  // reference does; then the node (t0, t1 - 1] that the reference tests with instant_may_fire is excluded here
+  // when bounds from x0 and x1 prove that test false, and only otherwise is the reference's search run.
+  //
+  // The bounds: I(t1 - 1) interpolates between I(t0) and I(t1) (fp32 rounding keeps it within two ulp of that
+  // range, which is monotone in v), ln is monotone, the leak term leak (t - t_ref) 1e-9 + dr_ref is non-decreasing
+  // in t (leak >= 0), and fp32 sums round monotonically; kSlack covers the log's error, the ulps of I and the
+  // exclusion test's own 16-64 eps margins.
+  BS_HD void segment_fast(const Segment& g, float x0, float x1) {
+    const int64_t t0 = g.t0, e = g.t1;
+    const int64_t tn = k.noise ? mini(s.t_shot, s.t_ba) : kForever;
+    if (s.blind_until != kNotBlind || s.t_search > t0 || tn < e) {
+      piece(g, t0, e);
+      return;
+    }
+    ++c.pieces;
+    const float D0 = delta(t0, x0);
+    if (D0 >= m.theta_on || D0 <= -m.theta_off) {
+      fire(t0, D0 >= m.theta_on, x0, -1);
+      piece_rest(g, t0, e);
+      return;
+    }
+    if (e - t0 == 1) {
+      s.t_search = maxi(s.t_search, e);
+      return;
+    }
+    if (!excluded(g, t0, e, x0, x1)) {
+      piece_rest_from_search(g, t0, e);
+      return;
+    }
+    if (e - t0 > 2) ++c.leaves;
+    s.t_search = maxi(s.t_search, e);
+  }
+
+  // True when instant_may_fire(t0, t1 - 1, I(t0), I(t1 - 1)) and Delta(t1 - 1) are provably both false.
+  BS_HD bool excluded(const Segment& g, int64_t t0, int64_t e, float x0, float x1) const {
+    const float eps = 0x1p-23f;
+    const float xa = minr(x0, x1), xb = maxr(x0, x1);
+    const float dl0 = m.leak * since_ref(t0, s.t_ref) + s.dr_ref;
+    const float dl1 = m.leak * since_ref(e, s.t_ref) + s.dr_ref;
+    const float mag = 1.0f + fabs_f(xa) + fabs_f(xb) + fabs_f(s.s3_ref) + fabs_f(dl0) + fabs_f(dl1);
+    if (!(mag < 1.0e3f)) return false;
+    const float slack = 1.0e-5f + 64.0f * eps * mag;
+    const float hi = (((xb + slack) - s.s3_ref) + (0.0f - s.n3_ref)) + dl1;
+    if (!(hi < m.theta_on - slack)) return false;
+    const float lo_x = (((xa - slack) - s.s3_ref) + (0.0f - s.n3_ref)) + dl0;
+    if (m.leak == 0.0f || g.v1 >= g.v0) {
+      // leak 0: may_fire is Delta(t1 - 1) against both levels; v1 >= v0 (I non-decreasing): against theta_on only.
+      return lo_x > -m.theta_off + slack;
+    }
+    // leak > 0 and I decreasing: the exclusion test bounds I from below by min(I) - 64 eps max(I), whose log lies
+    // below xa by at most 64 eps I(t0) / I(t1) (relative) plus rounding.
+    const float I0 = m.dark + m.scale * g.v0, I1 = m.dark + m.scale * g.v1;
+    if (!(I1 > 1024.0f * eps * I0)) return false;  // keeps -ln(1 - u) <= 1.1 u for the correction below
+    const float corr = 1.1f * (8.0f * eps + 64.0f * eps * (I0 / I1));
+    const float lo = ((((xa - corr) - slack) - s.s3_ref) + (0.0f - s.n3_ref)) + dl0;
+    return lo > -m.theta_off + slack;
+  }
+
+  // The rest of piece(g, t, e) after an event inside it (the reference's loop with the new state).
+  BS_HD void piece_rest(const Segment& g, int64_t t, int64_t e) {
+    --c.pieces;  // piece() counts the piece again
+    piece(g, t, e);
+  }
+
+  // piece(g, t0, e) whose Delta(t0) is known not to fire: the reference's search from t0, then its loop.
+  BS_HD void piece_rest_from_search(const Segment& g, int64_t t0, int64_t e) {
+    --c.pieces;
+    piece(g, t0, e);
   }
 };
 

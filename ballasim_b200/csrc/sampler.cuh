@@ -40,8 +40,9 @@ BS_HD bool exceeds(const SamplerRules& r, float a, float m, float b) {
   return r.midpoint != 0 && midpoint_eta1(r.dark, a, m, b) > r.tol;
 }
 
-// Walks one pixel's window: render(dt) -> irradiance, emit(dt, v) in time order. carried: the slot-0 value;
-// carried_flip: its signature differs from the rendered ones (0). Returns the number of samples emitted.
+// Walks one pixel's window: render(dt) -> irradiance; emit(dt, v) for every sample after slot 0 in time order (one
+// call site). carried: the slot-0 value (the caller's to take); carried_flip: its signature differs from the
+// rendered ones (0). Returns the number of samples, slot 0 included.
 template <class Render, class Emit>
 BS_HD uint32_t sample_pixel_window(const SamplerRules& r, int level, float carried, bool carried_flip,
                                    Render&& render, Emit&& emit) {
@@ -53,53 +54,63 @@ BS_HD uint32_t sample_pixel_window(const SamplerRules& r, int level, float carri
     bool flip, bad;
   };
   // A selected interval halves at most 22 times above min_split >= 2 (2^23 ns down to 2 ns), and the rules clamp
-  // max_refine_levels to kMaxDepth, so the walk never holds more than kMaxDepth frames.
+  // max_refine_levels to 23, so the walk never holds more than kMaxDepth frames.
   constexpr int kMaxDepth = 24;
   Frame st[kMaxDepth];
   const uint32_t count = (1u << level) + 1u, step = 1u << (kWindowLog2 - level);
-  uint32_t n = 0;
+  uint32_t n = 1;
   // Sliding lattice values v[j - 2], v[j - 1], v[j], v[j + 1].
   float vm2 = 0.0f, vm1 = carried, v0 = render(step), vp1 = count > 2 ? render(2 * step) : 0.0f;
-  emit(0u, carried);
-  ++n;
-  for (uint32_t j = 1; j < count; ++j) {
-    // Round0Flags (sampling.h:490-523) of interval (j - 1, j): triples (j - 1, j, j + 1) and (j - 2, j - 1, j).
-    const bool flip = r.refine_signature != 0 && j == 1 && carried_flip;
-    const bool m = (j + 1 < count && exceeds(r, vm1, v0, vp1)) || (j >= 2 && exceeds(r, vm2, vm1, v0));
-    if ((flip || m) && step >= r.min_split && r.max_refine_levels > 0) {
-      int sp = 0;
-      st[0] = Frame{(j - 1) * step, j * step, 0u, vm1, v0, 0.0f, 0, 0u, flip, false};
-      sp = 1;
-      while (sp > 0) {
-        Frame& f = st[sp - 1];
-        if (f.phase == 0u) {
-          f.g = (f.lo + f.hi) >> 1;
-          f.vg = render(f.g);
-          // HalfFlags (sampling.h:638-678): the triple (lo, mid, hi) flags both halves.
-          f.bad = exceeds(r, f.vlo, f.vg, f.vhi);
-          f.phase = 1u;
-          if ((f.flip || f.bad) && f.g - f.lo >= r.min_split && f.depth + 1 < r.max_refine_levels &&
-              sp < kMaxDepth) {
-            st[sp] = Frame{f.lo, f.g, 0u, f.vlo, f.vg, 0.0f, f.depth + 1, 0u, f.flip, false};
-            ++sp;
-          }
-          continue;
+  uint32_t j = 1;
+  bool opened = false;  // interval (j - 1, j) flagged and its refinement started
+  int sp = 0;
+  while (j < count) {
+    uint32_t dt;
+    float v;
+    if (sp > 0) {
+      Frame& f = st[sp - 1];
+      if (f.phase == 0u) {
+        f.g = (f.lo + f.hi) >> 1;
+        f.vg = render(f.g);
+        // HalfFlags (sampling.h:638-678): the triple (lo, mid, hi) flags both halves.
+        f.bad = exceeds(r, f.vlo, f.vg, f.vhi);
+        f.phase = 1u;
+        if ((f.flip || f.bad) && f.g - f.lo >= r.min_split && f.depth + 1 < r.max_refine_levels &&
+            sp < kMaxDepth) {
+          st[sp] = Frame{f.lo, f.g, 0u, f.vlo, f.vg, 0.0f, f.depth + 1, 0u, f.flip, false};
+          ++sp;
         }
-        emit(f.g, f.vg);
-        ++n;
-        if (f.bad && f.hi - f.g >= r.min_split && f.depth + 1 < r.max_refine_levels) {
-          f = Frame{f.g, f.hi, 0u, f.vg, f.vhi, 0.0f, f.depth + 1, 0u, false, false};
-        } else {
-          --sp;
-        }
+        continue;
       }
+      dt = f.g;
+      v = f.vg;
+      if (f.bad && f.hi - f.g >= r.min_split && f.depth + 1 < r.max_refine_levels) {
+        f = Frame{f.g, f.hi, 0u, f.vg, f.vhi, 0.0f, f.depth + 1, 0u, false, false};
+      } else {
+        --sp;
+      }
+    } else if (!opened) {
+      // Round0Flags (sampling.h:490-523) of interval (j - 1, j): triples (j - 1, j, j + 1) and (j - 2, j - 1, j).
+      opened = true;
+      const bool flip = r.refine_signature != 0 && j == 1 && carried_flip;
+      const bool m = (j + 1 < count && exceeds(r, vm1, v0, vp1)) || (j >= 2 && exceeds(r, vm2, vm1, v0));
+      if ((flip || m) && step >= r.min_split && r.max_refine_levels > 0) {
+        st[0] = Frame{(j - 1) * step, j * step, 0u, vm1, v0, 0.0f, 0, 0u, flip, false};
+        sp = 1;
+      }
+      continue;
+    } else {
+      dt = j * step;
+      v = v0;
+      opened = false;
+      vm2 = vm1;
+      vm1 = v0;
+      v0 = vp1;
+      if (j + 2 < count) vp1 = render((j + 2) * step);
+      ++j;
     }
-    emit(j * step, v0);
+    emit(dt, v);
     ++n;
-    vm2 = vm1;
-    vm1 = v0;
-    v0 = vp1;
-    if (j + 2 < count) vp1 = render((j + 2) * step);
   }
   return n;
 }

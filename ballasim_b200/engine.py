@@ -69,8 +69,9 @@ class Engine:
         _lib.check(_lib.lib().bs_engine_run(self._h, int(windows), stream, C.byref(s), C.byref(e)))
         return s.value, e.value
 
-    def set_launch(self, warps_per_block: int = 0, blocks_per_sm: int = 0) -> None:
-        _lib.check(_lib.lib().bs_engine_set_launch(self._h, int(warps_per_block), int(blocks_per_sm)))
+    def set_launch(self, warps_per_block: int = 0, blocks_per_sm: int = 0, stage: int = 0) -> None:
+        """Launch shape of the persistent grid and the staging depth (0, 16 or 32)."""
+        _lib.check(_lib.lib().bs_engine_set_launch(self._h, int(warps_per_block), int(blocks_per_sm), int(stage)))
 
     @property
     def last_ms(self) -> float:

@@ -231,6 +231,15 @@ class SensorModel:
         _lib.check(_lib.lib().bs_model_maps(self._h, *(a[k].ctypes.data for k in a)))
         return {k: v.reshape(self._height, self._width) for k, v in a.items()}
 
+    def noise_maps(self) -> dict:
+        """This build's noise maps (height, width): the background-activity rate and the shot-noise dominating
+        rate r sqrt(100 fA / I_dk) of each pixel (Hz)."""
+        n = self._width * self._height
+        ba, shot = np.zeros(n), np.zeros(n)
+        _lib.check(_lib.lib().bs_model_noise_maps(self._h, ba.ctypes.data, shot.ctypes.data))
+        return {"ba_rate_hz": ba.reshape(self._height, self._width),
+                "shot_max_hz": shot.reshape(self._height, self._width)}
+
     def stats(self) -> dict:
         out = np.zeros(9, np.uint64)
         _lib.check(_lib.lib().bs_model_stats(self._h, out.ctypes.data))

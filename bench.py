@@ -134,13 +134,15 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     if not _lib.cuda_available():
         raise RuntimeError("bench: no B200 visible")
     wl = replica(WORKLOADS[args.workload](), rank)
+    if args.windows:
+        wl.windows = min(wl.windows, args.windows)
     r = wl.rules
     models = [SensorModel(resolve("ideal", s.overrides), s.width, s.height, s.seed, [{"type": "constant"}], s.camera)
               for s in wl.sensors]
     eng = Engine([(m, s.field) for m, s in zip(models, wl.sensors)], tol=r.tol, dark=r.dark, min_dt_ns=r.min_dt_ns,
                  max_refine_levels=r.max_refine_levels, l_min=r.l_min, l_max=r.l_max)
-    if args.warps:
-        eng.set_launch(args.warps, args.blocks_per_sm)
+    if args.warps or args.blocks_per_sm or args.stage:
+        eng.set_launch(args.warps, args.blocks_per_sm, args.stage)
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
@@ -185,7 +187,7 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     # e2e through the public API with host buffers: the initial frames from pinned host memory in, every event out
     frames = [torch.from_numpy(field_frame(s.field, 0)).pin_memory().numpy() for s in wl.sensors]
     e2e_times, d2h = [], 0
-    for k in range(args.warmup + args.steps):
+    for k in range(0 if args.profile else args.warmup + args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         eng.start(0, sptr, frames=frames)
@@ -233,14 +235,14 @@ def run_ours(args, rank: int, world: int) -> dict | None:
                    "parallelism": f"replicas x{world}"},
         "gpu_launches": 3 * args.steps,
         "clocks": {k: v for k, v in clk.summary().items() if k != "samples"},
-        "e2e": {"value": samples_all / float(e2e_s[0]), "unit": "pixel-samples/s", "h2d_bytes_per_step": h2d,
+        "e2e": {"value": samples_all / float(e2e_s[0]) if e2e_times else None, "unit": "pixel-samples/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "roofline": {"kernel": "engine_kernel (sampler + pixel model fused, runs kept on chip)", "bound": "hbm",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": hbm_kind, "traffic": None, "algorithmic_bytes_per_launch": alg,
                      "avg_launch_ms": kms, "runs_write_avoided_bytes": int(per_step_samples) * 12},
     }
-    if world == 1 and not args.no_cpu_baseline:
+    if world == 1 and not (args.no_cpu_baseline or args.profile):
         out["cpu_baseline"] = cpu_baseline(wl, args.cpu_windows)
     return out
 
@@ -303,6 +305,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--warps", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
+    ap.add_argument("--stage", type=int, default=0, help="engine staging depth: 0, 16 or 32")
+    ap.add_argument("--windows", type=int, default=0, help="run only the first windows (profiling a reduced case)")
+    ap.add_argument("--profile", action="store_true", help="no e2e or CPU legs (fewest launches, for ncu)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -115,6 +115,9 @@ bs_status bs_model_take_events(bs_model* m, bs_event_columns* out);
 /* SensorModel::maps (sensor_model.h:180; sensor_module.cpp sensor_maps): the fp64 maps, width * height each. */
 bs_status bs_model_maps(const bs_model* m, double* theta_on, double* theta_off, double* leak, double* dark_fA,
                         double* phi0);
+/* This build's noise maps (no reference counterpart), width * height each: the pixel's background-activity rate
+ * and its shot-noise dominating rate r sqrt(100 fA / I_dk) (Hz; 0 when that noise is off). */
+bs_status bs_model_noise_maps(const bs_model* m, double* ba_rate_hz, double* shot_max_hz);
 /* Work counters since creation or bs_model_reset_stats (SensorModel::stats, sensor_module.cpp:112-136):
  * [pieces, leaf_intervals, input_clamps, pixel_samples, noise_candidates, gpu_launches, gpu_reruns,
  *  gpu_launch_ms_total x1000, gpu_launch_ms_max x1000]. */
@@ -206,8 +209,10 @@ bs_status bs_engine_start_frames(bs_engine* e, int64_t t0_ns, const float* const
 /* Samples and senses `windows` whole windows of every sensor from the current model time; the events are kept in
  * each model (bs_model_take_events). *pixel_samples and *events receive the totals of the call. */
 bs_status bs_engine_run(bs_engine* e, int32_t windows, void* stream, uint64_t* pixel_samples, uint64_t* events);
-/* Launch shape: warps per block and blocks per SM of the persistent grid (0: the defaults). */
-bs_status bs_engine_set_launch(bs_engine* e, int32_t warps_per_block, int32_t blocks_per_sm);
+/* Launch shape: warps per block and blocks per SM of the persistent grid (0: the defaults), and the staging depth
+ * (0: the sampler feeds the pixel model sample by sample; 16 or 32: per window each lane's samples are staged in
+ * shared memory between a sampling phase and a sensing phase). */
+bs_status bs_engine_set_launch(bs_engine* e, int32_t warps_per_block, int32_t blocks_per_sm, int32_t stage);
 /* Kernel time of the last bs_engine_run's launches (ms, CUDA events on its stream). */
 bs_status bs_engine_last_ms(const bs_engine* e, double* ms);
 

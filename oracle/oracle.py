@@ -135,6 +135,7 @@ class Port:
             L.orc_model_take_events.argtypes = [C.c_void_p, C.c_void_p]
             L.orc_model_maps.argtypes = [C.c_void_p, _f64p, _f64p, _f64p, _f64p, _f64p]
             L.orc_model_state.argtypes = [C.c_void_p, _i64p, _i64p, _f32p, _f32p, _f32p]
+            L.orc_model_noise_maps.argtypes = [C.c_void_p, _f64p]
             L.orc_model_stat.restype = C.c_uint64
             L.orc_model_stat.argtypes = [C.c_void_p, C.c_int32]
             L.orc_last_error.restype = C.c_char_p
@@ -228,6 +229,11 @@ class Port:
             a = [np.zeros(n) for _ in range(5)]
             self.L.orc_model_maps(self.h, *a)
             return dict(zip(("theta_on", "theta_off", "leak", "dark_current_fA", "phi0"), a))
+
+        def ba_rates(self) -> np.ndarray:
+            out = np.zeros(self.width * self.height)
+            self.L.orc_model_noise_maps(self.h, out)
+            return out
 
         def state(self) -> dict:
             n = self.width * self.height

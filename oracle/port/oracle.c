@@ -938,6 +938,11 @@ void orc_model_state(const orc_model* m, int64_t* t_ref, int64_t* t_search, floa
   }
 }
 
+void orc_model_noise_maps(const orc_model* m, double* ba_rate_hz) {
+  const size_t n = (size_t)m->width * m->height;
+  for (size_t i = 0; i < n; ++i) ba_rate_hz[i] = m->maps[i].ba_rate_hz;
+}
+
 uint64_t orc_model_stat(const orc_model* m, int32_t which) {
   return which == 0 ? m->pieces : which == 1 ? m->leaves : m->clamps;
 }

@@ -97,6 +97,7 @@ void orc_model_maps(const orc_model* m, double* theta_on, double* theta_off, dou
 void orc_model_state(const orc_model* m, int64_t* t_ref, int64_t* t_search, float* s3_ref, float* dr_ref,
                      float* held);
 uint64_t orc_model_stat(const orc_model* m, int32_t which); /* 0 pieces, 1 leaf intervals, 2 clamps */
+void orc_model_noise_maps(const orc_model* m, double* ba_rate_hz); /* the background-activity rate map */
 const char* orc_last_error(void);
 
 /* ---- the window sampler (src/engine/sampling.h, window_impl.h:461-713) ---- */

@@ -240,10 +240,12 @@ def test_midpoint_test_matches_numpy_fp32(cuda_lib):
     assert np.array_equal(t.exceeds(a, m, b), want > np.float32(0.01))
 
 
+@pytest.mark.parametrize("stage", [0, 16, 32])
 @pytest.mark.parametrize("case", ["edge", "blobs", "noise"])
-def test_engine_equals_the_oracle_chain(cuda_lib, case):
-    """The fused engine (sampler and pixel model on one thread, all windows in one launch) gives the oracle
-    chain's events (sample_window, then advance, per window) bit for bit."""
+def test_engine_equals_the_oracle_chain(cuda_lib, case, stage):
+    """The fused engine (sampler and pixel model on one thread, all windows in one launch; streamed, or staged in
+    shared memory per window) gives the oracle chain's events (sample_window, then advance, per window) bit for
+    bit."""
     from ballasim_b200.engine import Engine
     from ballasim_b200.sensor import SensorModel
     from oracle.oracle import simulate_port
@@ -259,6 +261,7 @@ def test_engine_equals_the_oracle_chain(cuda_lib, case):
     r = wl.rules
     eng = Engine([(m, spec.field)], tol=r.tol, dark=r.dark, min_dt_ns=r.min_dt_ns,
                  max_refine_levels=r.max_refine_levels, l_min=r.l_min, l_max=r.l_max)
+    eng.set_launch(0, 0, stage)
     eng.start(0)
     samples, parts = 0, []
     for chunk in (5, wl.windows - 5):  # two calls: the state and carried samples cross the call boundary
