@@ -107,6 +107,20 @@ _SIGS = {
     "bs_engine_run": (C.c_int32, [_P, C.c_int32, _P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "bs_engine_set_launch": (C.c_int32, [_P, C.c_int32, C.c_int32, C.c_int32]),
     "bs_engine_last_ms": (C.c_int32, [_P, C.POINTER(C.c_double)]),
+    "bs_mlp_create": (C.c_int32, [C.c_uint64, C.POINTER(_P)]),
+    "bs_mlp_destroy": (C.c_int32, [_P]),
+    "bs_mlp_get_params": (C.c_int32, [_P, _P]),
+    "bs_mlp_set_params": (C.c_int32, [_P, _P]),
+    "bs_mlp_steps": (C.c_int32, [_P, C.POINTER(C.c_int64)]),
+    "bs_mlp_forward": (C.c_int32, [_P, _P, C.c_size_t, _P, _P]),
+    "bs_mlp_gradient": (C.c_int32, [_P, _P, _P, C.c_size_t, _P, C.POINTER(C.c_double), _P]),
+    "bs_mlp_train": (C.c_int32, [_P, _P, _P, C.c_size_t, C.c_int32, C.c_int32, C.c_float, C.c_uint64, _P, _P]),
+    "bs_trace_pairs": (C.c_int32, [C.POINTER(Field), C.POINTER(SampleRules), C.c_int64, C.c_int32, C.c_uint32,
+                                   C.c_float, C.c_uint64, _P, _P, _P, C.c_size_t, C.POINTER(C.c_size_t),
+                                   C.POINTER(C.c_size_t), _P]),
+    "bs_engine_set_proposal": (C.c_int32, [_P, _P, C.c_float]),
+    "bs_engine_set_record": (C.c_int32, [_P, C.c_size_t]),
+    "bs_engine_take_record": (C.c_int32, [_P, C.c_int32, C.c_size_t, _P, _P, _P, C.POINTER(C.c_size_t)]),
 }
 
 _lib = None

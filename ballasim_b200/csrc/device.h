@@ -14,6 +14,7 @@
 #include <stdint.h>
 
 #include "fields.cuh"
+#include "learned.cuh"
 #include "pixel.cuh"
 #include "sampler.cuh"
 
@@ -55,8 +56,31 @@ struct EventBuf {
   unsigned long long capacity;
 };
 
+// Walk state of the learned-proposal sampler, per pixel (double-buffered with the pixel state): hx, 8 planes of
+// n pixels (plane k = the k-th previous walk point's log irradiance); gaps (8 log2 gaps, byte 0 newest); pv
+// (irradiance at the previous walk point); valid (a real previous walk point exists). 45 B per pixel.
+struct LearnedSoA {
+  float* hx;
+  uint64_t* gaps;
+  float* pv;
+  uint8_t* valid;
+};
+
+// A device record of (time, pixel, value) rows, appended with warp-aggregated atomics (tests and diagnostics).
+struct RecRow {
+  int64_t t;
+  uint32_t pixel;  // sensor index << 24 | pixel
+  float v;         // the sample's irradiance, or the step's log2 for a proposal
+};
+struct RecBuf {
+  RecRow* data;
+  unsigned long long* count;
+  unsigned long long capacity;
+};
+
 // One sensor of a fused engine launch.
 struct EngineSensor {
+  LearnedSoA lin, lout;  // learned-proposal walk state (unused by the plain engine)
   FieldDev field;
   SensorConsts consts;
   StateSoA in, out;
@@ -98,6 +122,73 @@ void launch_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t tota
                    int32_t w1, const SamplerRules& r, unsigned int* tile_counter, int blocks, int warps_per_block,
                    int stage, cudaStream_t stream);
 int engine_max_blocks_per_sm(int warps_per_block, int stage);
+// The fused engine with the learned step proposal (BF16 MLP operands and FP32 parameters in device memory):
+// the same tiles and pixel model, each window sampled by proposed power-of-two steps judged by the plain rule.
+// rec_samples / rec_steps (capacity 0: off) record every sample and every proposed step.
+struct LearnedLaunch {
+  const uint16_t* ops;
+  const float* params;
+  float margin;
+  int32_t sh;  // log2 min_dt_ns
+  RecBuf rec_samples, rec_steps;
+};
+void launch_learned_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t total_tiles, int64_t t0,
+                           int32_t w0, int32_t w1, const SamplerRules& r, const LearnedLaunch& l,
+                           unsigned int* tile_counter, int blocks, int warps_per_block, cudaStream_t stream);
+int learned_engine_max_blocks_per_sm(int warps_per_block);
+// Resets the walk state of n pixels from their initial irradiance.
+void launch_learned_reset(LearnedSoA st, uint32_t n, const float* irr0, cudaStream_t stream);
+
+// ---- the MLP (learned.cu) ----
+// Training pairs from one window's plain runs (all n_pixels listed in order; t absolute): every stride-th pixel
+// walks its run; pairs are appended (x: 16 BF16 features, y: target, key: pixel << 32 | window << 11 | step).
+struct WalkArgs {
+  const int64_t* offsets;
+  const int64_t* t;
+  const float* irr;
+  const uint8_t* level;
+  uint32_t n_pixels, stride;
+  int64_t t_w;
+  int32_t window, reset;
+  int32_t sh;
+  float eps;
+  uint64_t seed;
+  LearnedSoA st;
+  uint16_t* x;
+  float* y;
+  uint64_t* key;
+  unsigned long long* count;
+  unsigned long long capacity;
+};
+void launch_walk_pairs(const WalkArgs& a, cudaStream_t stream);
+// One training step's gradient partials: grid = ceil(rows / 128) CTAs of 128 threads.
+struct TrainArgs {
+  const uint16_t* x;
+  const float* y;
+  uint64_t n;
+  uint32_t rows;     // rows of this step
+  int32_t sampled;   // 1: rows drawn with replacement from n (Philox, keyed by the step counter); 0: rows 0..n-1
+  uint64_t seed;
+  const int64_t* step;
+  const uint16_t* ops;
+  const float* params;
+  float* partial;         // [grid][kMlpParamsPad]
+  double* partial_loss;   // [grid]
+  float inv_rows;
+};
+int train_grid(uint32_t rows);
+void launch_train_partials(const TrainArgs& a, cudaStream_t stream);
+// Adam over the partials of `ctas` CTAs (lr, beta 0.9 / 0.999, eps 1e-8); advances the step counter; writes the
+// step's loss (sum / (2 rows)) at losses[step] when step < loss_cap.
+void launch_adam(float* params, float* m, float* v, uint16_t* ops, const float* partial, const double* partial_loss,
+                 int ctas, float lr, float inv_rows, int64_t* step, float* losses, int64_t loss_cap,
+                 unsigned int* done, cudaStream_t stream);
+// The summed gradient (FP64) and loss of the partials (the gradient check).
+void launch_reduce_partials(const float* partial, const double* partial_loss, int ctas, float inv_rows,
+                            double* grad, double* loss, cudaStream_t stream);
+void launch_operands(const float* params, uint16_t* ops, cudaStream_t stream);
+void launch_mlp_forward(const uint16_t* ops, const float* params, const uint16_t* x, uint64_t n, float* y,
+                        cudaStream_t stream);
 // MidpointTest.eta over n triples of g groups (rows of g floats).
 void launch_midpoint_eta(float tol, float dark, int32_t g, const float* m_min, const float* m_max, const float* ea,
                          const float* em, const float* eb, uint32_t n, float* eta, uint8_t* exceeds,

@@ -540,6 +540,150 @@ __global__ void __launch_bounds__(128) engine_kernel_staged(EngineArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// The fused engine with the learned step proposal
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ void load_learned(const LearnedSoA& a, uint32_t p, uint32_t n, LearnedPixel& L) {
+#pragma unroll
+  for (int k = 0; k < 8; ++k) L.hx[k] = a.hx[static_cast<size_t>(k) * n + p];
+  L.gaps = a.gaps[p];
+  L.pv = a.pv[p];
+  L.valid = a.valid[p];
+}
+__device__ __forceinline__ void store_learned(const LearnedSoA& a, uint32_t p, uint32_t n, const LearnedPixel& L) {
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a.hx[static_cast<size_t>(k) * n + p] = L.hx[k];
+  a.gaps[p] = L.gaps;
+  a.pv[p] = L.pv;
+  a.valid[p] = static_cast<uint8_t>(L.valid);
+}
+
+__device__ __forceinline__ void rec_push(const RecBuf& r, int64_t t, uint32_t pixel, float v) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  unsigned long long base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(r.count, static_cast<unsigned long long>(g.size()));
+  base = g.shfl(base, 0);
+  const unsigned long long i = base + g.thread_rank();
+  if (i < r.capacity) r.data[i] = RecRow{t, pixel, v};
+}
+
+__global__ void learned_reset_kernel(LearnedSoA st, uint32_t n, const float* irr0) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  LearnedPixel L;
+  learned_reset(L, irr0[p]);
+  store_learned(st, p, n, L);
+}
+
+// Per window and warp: every lane with its walk inside the window writes its 16 features, the warp runs the MLP on
+// the tensor cores (32 rows), and each lane takes its proposed step (judge, fallback and pixel model on its own);
+// the loop ends when every lane has reached the window's end.
+__global__ void __launch_bounds__(128) learned_engine_kernel(EngineArgs a, LearnedLaunch l) {
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  __shared__ MlpShared W;
+  __shared__ __align__(16) uint16_t rows[4][32 * kSF];
+  __shared__ float ys[4][32];
+  __shared__ uint16_t lists[4][kMaxListed];
+  mlp_load_shared(W, l.ops, l.params);
+  uint16_t* my_list = lists[warp];
+  uint16_t* my_rows = rows[warp];
+  float* my_y = ys[warp];
+  const bool rec_s = l.rec_samples.capacity > 0, rec_p = l.rec_steps.capacity > 0;
+  for (;;) {
+    uint32_t tile = 0;
+    if (lane == 0) tile = atomicAdd(a.tile_counter, 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if (tile >= a.total_tiles) break;
+    int si = 0;
+    while (si + 1 < a.n_sensors && a.sensors[si + 1].tile0 <= tile) ++si;
+    const EngineSensor& S = a.sensors[si];
+    const uint32_t local = tile - S.tile0;
+    const uint32_t x = (local % S.tiles_x) * 8u + (lane & 7u), y = (local / S.tiles_x) * 4u + (lane >> 3);
+    const bool have = x < S.width && y < S.height;
+    const uint32_t np = S.width * S.height;
+    const uint32_t p = have ? y * S.width + x : 0u;
+    const uint32_t tag = (static_cast<uint32_t>(si) << 24) | p;
+    const bool noise = S.consts.noise != 0;
+    PixelRegs s;
+    PixelMapRegs m;
+    LearnedPixel L;
+    float carried = 0.0f;
+    if (have) {
+      load_state(S.in, p, noise, s);
+      load_map(S.map, p, m);
+      load_learned(S.lin, p, np, L);
+      carried = S.carried_in[p];
+    }
+    PixelCounters c;
+    unsigned long long samples = 0;
+    GlobalSink sink{S.ev, &S.counters[kCntEvents]};
+    PixelProc<GlobalSink> proc{s, m, S.consts, p, sink, c};
+    const FieldDev& f = S.field;
+    for (int32_t w = a.w0; w < a.w1; ++w) {
+      const int64_t t_w = a.t0 + static_cast<int64_t>(w) * kWindowNs;
+      const BlobList list = warp_blob_list(f, have, x, y, t_w, t_w + kWindowNs, my_list);
+      auto render = [&](uint32_t dt) { return field_eval(f, list, x, y, t_w + dt); };
+      WindowFeed feed{&proc, t_w, S.consts.irr_max, t_w, s.held, carried, 0.0f};
+      int s_floor = kWindowLog2;
+      uint32_t cur = 0;
+      float v_cur = carried, x_cur = 0.0f;
+      if (have) {
+        s_floor = kWindowLog2 - field_level(f, list, x, y, t_w, a.r.l_min, a.r.l_max);
+        feed.start(carried);
+        x_cur = log_f(carried);
+      }
+      auto emit = [&](uint32_t dt, float v) {
+        feed(dt, v);
+        if (rec_s) rec_push(l.rec_samples, t_w + dt, tag, v);
+      };
+      for (;;) {
+        const bool act = have && cur < static_cast<uint32_t>(kWindowNs);
+        if (!__any_sync(0xffffffffu, act)) break;
+        float feat[16];
+        if (act) {
+          step_features(L.hx, L.gaps, x_cur, feat);
+        } else {
+#pragma unroll
+          for (int k = 0; k < 16; ++k) feat[k] = 0.0f;
+        }
+        uint32_t packed[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) packed[k] = pack2(feat[2 * k], feat[2 * k + 1]);
+        uint4* dst = reinterpret_cast<uint4*>(my_rows + lane * kSF);
+        dst[0] = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+        dst[1] = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+        __syncwarp();
+        mlp_forward_warp(W, my_rows, my_y);
+        if (act) {
+          const int sl = proposal_log2(my_y[lane], l.margin, l.sh, s_floor, cur);
+          if (rec_p) rec_push(l.rec_steps, t_w + cur, tag, static_cast<float>(sl));
+          float v_end = 0.0f;
+          samples += learned_step(a.r, cur, sl, v_cur, x_cur, L, v_end, render, emit);
+          cur += 1u << sl;
+          v_cur = v_end;
+          x_cur = log_f(v_end);
+        }
+        __syncwarp();
+      }
+      if (have) {
+        ++samples;  // the carried slot, as in the plain engine's count
+        s.held = feed.prev_v;
+        carried = feed.last_raw;
+      }
+      __syncwarp();
+    }
+    if (have) {
+      store_state(S.out, p, noise, s);
+      store_learned(S.lout, p, np, L);
+      S.carried_out[p] = carried;
+    }
+    warp_add(&S.counters[kCntPieces], c.pieces);
+    warp_add(&S.counters[kCntLeaves], c.leaves);
+    warp_add(&S.counters[kCntSamples], samples);
+    warp_add(&S.counters[kCntNoise], c.noise_candidates);
+  }
+}
+
 // MidpointTest.eta (sampling.h:36-53): per group in order, dev = |(a + b) * -0.5 + m|, num += m_max dev,
 // den += m_min min(a, m, b), the mediant max(dev / low) when some group is modulated; eta = num / den.
 struct MidArgs {
@@ -664,6 +808,30 @@ int engine_max_blocks_per_sm(int warps_per_block, int stage) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel, warps_per_block * 32, 0);
   }
   return n;
+}
+
+}  // namespace bs
+
+namespace bs {
+
+void launch_learned_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t total_tiles, int64_t t0,
+                           int32_t w0, int32_t w1, const SamplerRules& r, const LearnedLaunch& l,
+                           unsigned int* tile_counter, int blocks, int warps_per_block, cudaStream_t stream) {
+  EngineArgs a{sensors_dev, n_sensors, total_tiles, t0, w0, w1, r, tile_counter};
+  (void)warps_per_block;  // 4 warps: the shared tiles are sized for them
+  learned_engine_kernel<<<blocks, 128, 0, stream>>>(a, l);
+}
+
+int learned_engine_max_blocks_per_sm(int warps_per_block) {
+  (void)warps_per_block;
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, learned_engine_kernel, 128, 0);
+  return n;
+}
+
+void launch_learned_reset(LearnedSoA st, uint32_t n, const float* irr0, cudaStream_t stream) {
+  if (n == 0) return;
+  learned_reset_kernel<<<(n + 255) / 256, 256, 0, stream>>>(st, n, irr0);
 }
 
 }  // namespace bs

@@ -677,6 +677,255 @@ struct Sampler {
 };
 
 // ---------------------------------------------------------------------------------------------
+// the learned step proposal: the MLP and its training pairs
+// ---------------------------------------------------------------------------------------------
+struct LearnedBufs {
+  DevBuf<float> hx, pv;
+  DevBuf<uint64_t> gaps;
+  DevBuf<uint8_t> valid;
+  LearnedSoA soa(size_t n) {
+    return LearnedSoA{hx.ensure(8 * n), gaps.ensure(n), pv.ensure(n), valid.ensure(n)};
+  }
+};
+
+struct Mlp {
+  DeviceGate gate;
+  DevBuf<float> params, m, v, partial, losses;
+  DevBuf<uint16_t> ops;
+  DevBuf<double> partial_loss, grad, loss;
+  DevBuf<int64_t> step;
+  DevBuf<unsigned int> done;
+  cudaStream_t own = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t graph_key[8] = {};
+  static constexpr int64_t kLossCap = int64_t{1} << 22;  // steps whose loss is kept
+
+  // He-uniform weights (U(-a, a), a = sqrt(6 / fan_in)) from Philox, zero biases, Adam state zero.
+  explicit Mlp(uint64_t seed) {
+    CK(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
+    std::vector<float> h(kMlpParams, 0.0f);
+    for (int p = 0; p < kMlpParams; ++p) {
+      float a = 0.0f;
+      if (p < kOffB1) a = std::sqrt(6.0f / kMlpIn);
+      else if (p >= kOffW2 && p < kOffB2) a = std::sqrt(6.0f / kMlpHid);
+      else if (p >= kOffW3 && p < kOffB3) a = std::sqrt(6.0f / kMlpHid);
+      if (a == 0.0f) continue;
+      const U4 u = draw(seed, kPurposeInit, 0u, static_cast<uint32_t>(p), 0);
+      const float r = (static_cast<float>(u.v[0] >> 8) + 0.5f) * 0x1p-24f;
+      h[p] = (2.0f * r - 1.0f) * a;
+    }
+    params.ensure(kMlpParams);
+    m.ensure(kMlpParams);
+    v.ensure(kMlpParams);
+    ops.ensure(kOpWords);
+    step.ensure(1);
+    done.ensure(1);
+    grad.ensure(kMlpParams);
+    loss.ensure(1);
+    losses.ensure(kLossCap);
+    set(h.data());
+  }
+  ~Mlp() {
+    release_graph();
+    if (own) cudaStreamDestroy(own);
+  }
+  void release_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+  }
+
+  void set(const float* h) {
+    for (int p = 0; p < kMlpParams; ++p) {
+      if (!std::isfinite(h[p])) throw std::invalid_argument("mlp: non-finite parameter " + std::to_string(p));
+    }
+    CK(cudaMemcpyAsync(params.p, h, kMlpParams * sizeof(float), cudaMemcpyHostToDevice, own));
+    CK(cudaMemsetAsync(m.p, 0, kMlpParams * sizeof(float), own));
+    CK(cudaMemsetAsync(v.p, 0, kMlpParams * sizeof(float), own));
+    CK(cudaMemsetAsync(ops.p, 0, kOpWords * sizeof(uint16_t), own));
+    CK(cudaMemsetAsync(step.p, 0, sizeof(int64_t), own));
+    CK(cudaMemsetAsync(done.p, 0, sizeof(unsigned int), own));
+    launch_operands(params.p, ops.p, own);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(own));
+  }
+  void get(float* h) const {
+    CK(cudaMemcpy(h, params.p, kMlpParams * sizeof(float), cudaMemcpyDeviceToHost));
+  }
+  int64_t steps() const {
+    int64_t s = 0;
+    CK(cudaMemcpy(&s, step.p, sizeof(int64_t), cudaMemcpyDeviceToHost));
+    return s;
+  }
+
+  void forward(const uint16_t* x, size_t n, float* y, cudaStream_t s) {
+    if (n && (!x || !y)) throw std::invalid_argument("mlp.forward: null device array");
+    launch_mlp_forward(ops.p, params.p, x, n, y, s);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+  }
+
+  void gradient(const uint16_t* x, const float* y, size_t n, double* g_host, double* loss_host, cudaStream_t s) {
+    if (n == 0 || n > 0xFFFFFFFFull) throw std::invalid_argument("mlp.gradient: n must be in [1, 2^32)");
+    if (!x || !y) throw std::invalid_argument("mlp.gradient: null device array");
+    const int ctas = train_grid(static_cast<uint32_t>(n));
+    partial.ensure(static_cast<size_t>(ctas) * kMlpParamsPad);
+    partial_loss.ensure(ctas);
+    TrainArgs a{x, y, n, static_cast<uint32_t>(n), 0, 0, step.p, ops.p, params.p, partial.p, partial_loss.p,
+                1.0f / static_cast<float>(n)};
+    launch_train_partials(a, s);
+    launch_reduce_partials(partial.p, partial_loss.p, ctas, a.inv_rows, grad.p, loss.p, s);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(g_host, grad.p, kMlpParams * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(loss_host, loss.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+  }
+
+  // `steps` Adam steps on batches of `batch` rows drawn with replacement from the n pairs. The steps run from a
+  // CUDA graph of 32 steps (two launches each), replayed; the loss of every step is kept on the device.
+  void train(const uint16_t* x, const float* y, size_t n, int32_t steps, int32_t batch, float lr, uint64_t seed,
+             float* losses_host, cudaStream_t s) {
+    if (n == 0) throw std::invalid_argument("mlp.train: no pairs");
+    if (!x || !y) throw std::invalid_argument("mlp.train: null device array");
+    if (steps < 0 || batch < 1 || batch > (1 << 24)) throw std::invalid_argument("mlp.train: bad steps or batch");
+    if (!(lr > 0.0f) || !std::isfinite(lr)) throw std::invalid_argument("mlp.train: lr must be positive");
+    const int ctas = train_grid(static_cast<uint32_t>(batch));
+    partial.ensure(static_cast<size_t>(ctas) * kMlpParamsPad);
+    partial_loss.ensure(ctas);
+    const int64_t s0 = steps_from_device(s);
+    const TrainArgs a{x, y, n, static_cast<uint32_t>(batch), 1, seed, step.p, ops.p, params.p, partial.p,
+                      partial_loss.p, 1.0f / static_cast<float>(batch)};
+    auto one = [&](cudaStream_t st) {
+      launch_train_partials(a, st);
+      launch_adam(params.p, m.p, v.p, ops.p, partial.p, partial_loss.p, ctas, lr, a.inv_rows, step.p, losses.p,
+                  static_cast<int64_t>(losses.cap), done.p, st);
+    };
+    constexpr int kGraphSteps = 32;
+    int32_t left = steps;
+    if (left > 0) {  // the first step runs eagerly (it also configures the kernel's shared-memory size)
+      one(s);
+      CK(cudaGetLastError());
+      --left;
+    }
+    if (left >= kGraphSteps) {
+      // The graph holds its launches' arguments and buffer addresses: rebuild it when any of them changes.
+      const uint64_t key[8] = {reinterpret_cast<uint64_t>(x), reinterpret_cast<uint64_t>(y), n,
+                               (static_cast<uint64_t>(batch) << 32) ^ f2u(lr), seed,
+                               reinterpret_cast<uint64_t>(partial.p), reinterpret_cast<uint64_t>(partial_loss.p),
+                               static_cast<uint64_t>(ctas)};
+      if (!exec || std::memcmp(key, graph_key, sizeof(key)) != 0) {
+        release_graph();
+        CK(cudaStreamBeginCapture(own, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < kGraphSteps; ++k) one(own);
+        CK(cudaStreamEndCapture(own, &graph));
+        CK(cudaGraphInstantiate(&exec, graph, 0));
+        std::memcpy(graph_key, key, sizeof(key));
+      }
+      // The graph runs on the library's own stream, ordered after the caller's work.
+      cudaEvent_t ev;
+      CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      CK(cudaEventRecord(ev, s));
+      CK(cudaStreamWaitEvent(own, ev, 0));
+      while (left >= kGraphSteps) {
+        CK(cudaGraphLaunch(exec, own));
+        left -= kGraphSteps;
+      }
+      CK(cudaEventRecord(ev, own));
+      CK(cudaStreamWaitEvent(s, ev, 0));
+      CK(cudaEventDestroy(ev));
+    }
+    for (; left > 0; --left) one(s);
+    CK(cudaGetLastError());
+    if (losses_host && steps > 0) {
+      const int64_t kept = std::max<int64_t>(0, std::min<int64_t>(steps, kLossCap - s0));
+      for (int32_t i = static_cast<int32_t>(kept); i < steps; ++i) losses_host[i] = NAN;
+      if (kept > 0) {
+        CK(cudaMemcpyAsync(losses_host, losses.p + s0, static_cast<size_t>(kept) * sizeof(float),
+                           cudaMemcpyDeviceToHost, s));
+      }
+    }
+    CK(cudaStreamSynchronize(s));
+  }
+
+  int64_t steps_from_device(cudaStream_t s) {
+    int64_t v0 = 0;
+    CK(cudaMemcpyAsync(&v0, step.p, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return v0;
+  }
+};
+
+// Training pairs from the plain sampler over windows [0, windows) of a field (every pixel listed, levels by the
+// field's rule, runs on the device), walked by launch_walk_pairs.
+void trace_pairs(const bs_field& fh, const bs_sample_rules& rr, int64_t t0, int32_t windows, uint32_t stride,
+                 float eps, uint64_t seed, uint16_t* x, float* y, uint64_t* key, size_t cap, size_t* n_out,
+                 size_t* total, cudaStream_t s) {
+  if (windows < 0) throw std::invalid_argument("trace_pairs: windows must be >= 0");
+  if (stride < 1) throw std::invalid_argument("trace_pairs: stride must be >= 1");
+  if (!(eps > 0.0f)) throw std::invalid_argument("trace_pairs: eps must be positive");
+  if (cap > 0 && (!x || !y)) throw std::invalid_argument("trace_pairs: null device array");
+  if ((t0 & (kWindowNs - 1)) != 0) throw std::invalid_argument("trace_pairs: t0 must be a window start");
+  FieldHolder field;
+  field.set(fh);
+  const SamplerRules r = make_rules(rr);
+  int sh = 0;
+  while ((int64_t{1} << sh) < rr.min_dt_ns) ++sh;
+  const uint32_t np = field.f.width * field.f.height;
+  std::vector<uint32_t> iota(np);
+  for (uint32_t i = 0; i < np; ++i) iota[i] = i;
+  DevBuf<uint32_t> ids, counts;
+  DevBuf<uint8_t> level;
+  DevBuf<float> carried[2], irr;
+  DevBuf<uint64_t> sig[2];
+  DevBuf<int64_t> offsets, scratch, t;
+  DevBuf<unsigned long long> count;
+  LearnedBufs walk;
+  ids.ensure(np);
+  counts.ensure(np);
+  level.ensure(np);
+  carried[0].ensure(np);
+  carried[1].ensure(np);
+  sig[0].ensure(np);
+  sig[1].ensure(np);
+  offsets.ensure(np + 1);
+  scratch.ensure(scan_scratch_words(np));
+  count.ensure(1);
+  const LearnedSoA st = walk.soa(np);
+  CK(cudaMemcpyAsync(ids.p, iota.data(), np * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(sig[0].p, 0, np * sizeof(uint64_t), s));
+  CK(cudaMemsetAsync(count.p, 0, sizeof(unsigned long long), s));
+  launch_field_frame(field.f, t0, np, carried[0].p, s);
+  int cur = 0;
+  for (int32_t w = 0; w < windows; ++w) {
+    const int64_t t_w = t0 + static_cast<int64_t>(w) * kWindowNs;
+    launch_levels(field.f, t_w, r.l_min, r.l_max, np, level.p, s);
+    launch_sample_window(field.f, r, t_w, ids.p, level.p, np, carried[cur].p, sig[cur].p, counts.p, nullptr,
+                         nullptr, nullptr, nullptr, nullptr, 0, s);
+    launch_scan(counts.p, np, offsets.p, scratch.p, s);
+    CK(cudaGetLastError());
+    int64_t n_samples = 0;
+    CK(cudaMemcpyAsync(&n_samples, offsets.p + np, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    t.ensure(static_cast<size_t>(n_samples));
+    irr.ensure(static_cast<size_t>(n_samples));
+    launch_sample_window(field.f, r, t_w, ids.p, level.p, np, carried[cur].p, sig[cur].p, counts.p, offsets.p, t.p,
+                         irr.p, carried[1 - cur].p, sig[1 - cur].p, 1, s);
+    WalkArgs a{offsets.p, t.p, irr.p, level.p, np, stride, t_w, w, w == 0 ? 1 : 0, sh, eps, seed, st,
+               x, y, key, count.p, static_cast<unsigned long long>(cap)};
+    launch_walk_pairs(a, s);
+    CK(cudaGetLastError());
+    cur = 1 - cur;
+  }
+  unsigned long long produced = 0;
+  CK(cudaMemcpyAsync(&produced, count.p, sizeof(produced), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  *total = static_cast<size_t>(produced);
+  *n_out = std::min(static_cast<size_t>(produced), cap);
+}
+
+// ---------------------------------------------------------------------------------------------
 // the fused engine
 // ---------------------------------------------------------------------------------------------
 struct Engine {
@@ -694,6 +943,15 @@ struct Engine {
   double last_ms = 0;
   Timer timer;
   cudaStream_t own = nullptr;
+  // The learned step proposal (null: the plain sampler), its walk state (2 per sensor) and the record buffers.
+  const Mlp* mlp = nullptr;
+  float margin = 0.25f;
+  std::vector<std::unique_ptr<LearnedBufs>> lbufs;
+  std::vector<int> lcur;
+  DevBuf<RecRow> rec[2];
+  DevBuf<unsigned long long> rec_count;
+  size_t rec_cap = 0;
+  unsigned long long rec_n[2] = {0, 0};
 
   Engine(bs_model* const* ms, const bs_field* fs, int32_t cnt, const bs_sample_rules& r) {
     require_device();
@@ -746,6 +1004,55 @@ struct Engine {
       }
       m->init_device(t0, frame, s, host_frames ? host_frames[i] : nullptr);
     }
+    if (mlp) reset_walks(s);
+  }
+
+  // The learned walk state of every pixel restarts from the current carried frame (a flat virtual history).
+  void reset_walks(cudaStream_t s) {
+    while (lbufs.size() < 2 * models.size()) lbufs.push_back(std::make_unique<LearnedBufs>());
+    lcur.assign(models.size(), 0);
+    for (size_t i = 0; i < models.size(); ++i) {
+      const uint32_t n = models[i]->n;
+      launch_learned_reset(lbufs[2 * i]->soa(n), n, carried[2 * i + carried_cur[i]]->p, s);
+      lbufs[2 * i + 1]->soa(n);
+    }
+    CK(cudaGetLastError());
+  }
+
+  void set_proposal(const Mlp* p, float mg) {
+    if (p && !std::isfinite(mg)) throw std::invalid_argument("engine: margin must be finite");
+    mlp = p;
+    margin = mg;
+    if (p) {
+      reset_walks(own);
+      CK(cudaStreamSynchronize(own));
+    }
+  }
+
+  void set_record(size_t cap) {
+    rec_cap = cap;
+    rec_n[0] = rec_n[1] = 0;
+    if (cap) {
+      rec[0].ensure(cap);
+      rec[1].ensure(cap);
+    }
+    rec_count.ensure(2);
+  }
+
+  // Copies up to cap rows of record `which` (0 samples, 1 proposed steps) of the last run; n gets the rows recorded
+  // (more than the record's capacity means the record is incomplete).
+  void take_record(int which, size_t cap, int64_t* t, uint32_t* pixel, float* v, size_t* n) {
+    if (which != 0 && which != 1) throw std::invalid_argument("engine: record 0 (samples) or 1 (steps)");
+    const size_t have = static_cast<size_t>(std::min<unsigned long long>(rec_n[which], rec_cap));
+    const size_t k = std::min(have, cap);
+    std::vector<RecRow> rows(k);
+    if (k) CK(cudaMemcpy(rows.data(), rec[which].p, k * sizeof(RecRow), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < k; ++i) {
+      if (t) t[i] = rows[i].t;
+      if (pixel) pixel[i] = rows[i].pixel;
+      if (v) v[i] = rows[i].v;
+    }
+    *n = static_cast<size_t>(rec_n[which]);
   }
 
   void run(int32_t windows, cudaStream_t s, uint64_t* samples_out, uint64_t* events_out) {
@@ -759,10 +1066,13 @@ struct Engine {
     int dev = 0, sms = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const int per_sm =
-        blocks_per_sm > 0 ? blocks_per_sm : std::max(1, engine_max_blocks_per_sm(warps_per_block, stage));
-    const int blocks = static_cast<int>(std::min<uint64_t>(static_cast<uint64_t>(sms) * per_sm,
-                                                           (total_tiles + warps_per_block - 1) / warps_per_block));
+    const int wpb = mlp ? 4 : warps_per_block;
+    const int per_sm = blocks_per_sm > 0 ? blocks_per_sm
+                                         : std::max(1, mlp ? learned_engine_max_blocks_per_sm(wpb)
+                                                           : engine_max_blocks_per_sm(wpb, stage));
+    const int blocks = static_cast<int>(
+        std::min<uint64_t>(static_cast<uint64_t>(sms) * per_sm, (total_tiles + wpb - 1) / wpb));
+    if (mlp && lcur.size() != models.size()) throw std::logic_error("engine: call start() after set_proposal()");
     for (;;) {
       for (size_t i = 0; i < models.size(); ++i) {
         Model* m = models[i];
@@ -776,14 +1086,28 @@ struct Engine {
         e.carried_out = carried[2 * i + 1 - carried_cur[i]]->p;
         e.ev = EventBuf{m->events.p, static_cast<unsigned long long>(m->event_cap)};
         e.counters = m->counters.p;
+        if (mlp) {
+          e.lin = lbufs[2 * i + lcur[i]]->soa(m->n);
+          e.lout = lbufs[2 * i + 1 - lcur[i]]->soa(m->n);
+        }
         CK(cudaMemsetAsync(m->counters.p, 0, kCntWords * sizeof(unsigned long long), s));
       }
+      if (rec_cap) CK(cudaMemsetAsync(rec_count.p, 0, 2 * sizeof(unsigned long long), s));
       CK(cudaMemcpyAsync(sensors_dev.p, host.data(), host.size() * sizeof(EngineSensor), cudaMemcpyHostToDevice, s));
       CK(cudaMemsetAsync(tile_counter.p, 0, sizeof(unsigned int), s));
       CK(cudaEventRecord(timer.a, s));
       if (windows > 0 && total_tiles > 0) {
-        launch_engine(sensors_dev.p, static_cast<int>(host.size()), total_tiles, t0, 0, windows, rules,
-                      tile_counter.p, blocks, warps_per_block, stage, s);
+        if (mlp) {
+          int sh = 0;
+          while ((2u << sh) < rules.min_split) ++sh;
+          const LearnedLaunch l{mlp->ops.p, mlp->params.p, margin, sh,
+                                RecBuf{rec[0].p, rec_count.p, rec_cap}, RecBuf{rec[1].p, rec_count.p + 1, rec_cap}};
+          launch_learned_engine(sensors_dev.p, static_cast<int>(host.size()), total_tiles, t0, 0, windows, rules, l,
+                                tile_counter.p, blocks, wpb, s);
+        } else {
+          launch_engine(sensors_dev.p, static_cast<int>(host.size()), total_tiles, t0, 0, windows, rules,
+                        tile_counter.p, blocks, warps_per_block, stage, s);
+        }
       }
       CK(cudaGetLastError());
       CK(cudaEventRecord(timer.b, s));
@@ -792,6 +1116,7 @@ struct Engine {
         CK(cudaMemcpyAsync(m->counters_h.p, m->counters.p, kCntWords * sizeof(unsigned long long),
                            cudaMemcpyDeviceToHost, s));
       }
+      if (rec_cap) CK(cudaMemcpyAsync(rec_n, rec_count.p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
       float ms = 0;
       cudaEventElapsedTime(&ms, timer.a, timer.b);
@@ -821,6 +1146,7 @@ struct Engine {
         m->cur = 1 - m->cur;
         m->t_state = t0 + static_cast<int64_t>(windows) * kWindowNs;
         carried_cur[i] = 1 - carried_cur[i];
+        if (mlp) lcur[i] = 1 - lcur[i];
         samples += c[kCntSamples];
         events += c[kCntEvents];
       }
@@ -882,6 +1208,9 @@ struct bs_sampler : bs::Sampler {
 };
 struct bs_engine : bs::Engine {
   using bs::Engine::Engine;
+};
+struct bs_mlp : bs::Mlp {
+  using bs::Mlp::Mlp;
 };
 
 extern "C" {
@@ -1233,6 +1562,93 @@ bs_status bs_engine_last_ms(const bs_engine* e, double* ms) {
     NEED(e);
     NEED(ms);
     *ms = e->last_ms;
+  });
+}
+
+bs_status bs_mlp_create(uint64_t seed, bs_mlp** out) {
+  return guarded([&] {
+    NEED(out);
+    *out = nullptr;
+    *out = new bs_mlp(seed);
+  });
+}
+bs_status bs_mlp_destroy(bs_mlp* m) {
+  return guarded([&] { delete m; });
+}
+bs_status bs_mlp_get_params(const bs_mlp* m, float* params) {
+  return guarded([&] {
+    NEED(m);
+    NEED(params);
+    m->get(params);
+  });
+}
+bs_status bs_mlp_set_params(bs_mlp* m, const float* params) {
+  return guarded([&] {
+    NEED(m);
+    NEED(params);
+    m->set(params);
+  });
+}
+bs_status bs_mlp_steps(const bs_mlp* m, int64_t* steps) {
+  return guarded([&] {
+    NEED(m);
+    NEED(steps);
+    *steps = m->steps();
+  });
+}
+bs_status bs_mlp_forward(bs_mlp* m, const uint16_t* x, size_t n, float* y, void* stream) {
+  return guarded([&] {
+    NEED(m);
+    m->forward(x, n, y, stream ? static_cast<cudaStream_t>(stream) : m->own);
+  });
+}
+bs_status bs_mlp_gradient(bs_mlp* m, const uint16_t* x, const float* y, size_t n, double* grad, double* loss,
+                          void* stream) {
+  return guarded([&] {
+    NEED(m);
+    NEED(grad);
+    NEED(loss);
+    m->gradient(x, y, n, grad, loss, stream ? static_cast<cudaStream_t>(stream) : m->own);
+  });
+}
+bs_status bs_mlp_train(bs_mlp* m, const uint16_t* x, const float* y, size_t n, int32_t steps, int32_t batch, float lr,
+                       uint64_t seed, float* losses, void* stream) {
+  return guarded([&] {
+    NEED(m);
+    m->train(x, y, n, steps, batch, lr, seed, losses, stream ? static_cast<cudaStream_t>(stream) : m->own);
+  });
+}
+bs_status bs_trace_pairs(const bs_field* field, const bs_sample_rules* rules, int64_t t0_ns, int32_t windows,
+                         uint32_t stride, float eps, uint64_t seed, uint16_t* x, float* y, uint64_t* keys, size_t cap,
+                         size_t* n_out, size_t* total, void* stream) {
+  return guarded([&] {
+    NEED(field);
+    NEED(rules);
+    NEED(n_out);
+    NEED(total);
+    bs::require_device();
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    bs::trace_pairs(*field, *rules, t0_ns, windows, stride, eps, seed, x, y, keys, cap, n_out, total, s);
+  });
+}
+bs_status bs_engine_set_proposal(bs_engine* e, const bs_mlp* mlp, float margin) {
+  return guarded([&] {
+    NEED(e);
+    e->set_proposal(mlp, margin);
+  });
+}
+bs_status bs_engine_set_record(bs_engine* e, size_t capacity) {
+  return guarded([&] {
+    NEED(e);
+    e->set_record(capacity);
+  });
+}
+bs_status bs_engine_take_record(bs_engine* e, int32_t which, size_t cap, int64_t* t, uint32_t* pixel, float* v,
+                                size_t* n) {
+  return guarded([&] {
+    NEED(e);
+    NEED(n);
+    e->take_record(which, cap, t, pixel, v, n);
   });
 }
 

@@ -78,3 +78,34 @@ class Engine:
         ms = C.c_double()
         _lib.check(_lib.lib().bs_engine_last_ms(self._h, C.byref(ms)))
         return ms.value
+
+    def set_proposal(self, mlp=None, margin: float = 0.25) -> None:
+        """Samples with the learned step proposal of `mlp` (a learned.StepMLP; None: the plain sampler). Every
+        proposed step is judged by the plain midpoint rule, and a rejected one is refined by it. The walk state
+        restarts from the current frame, and again at every start()."""
+        self._mlp = mlp  # the engine borrows the network: keep it alive
+        _lib.check(_lib.lib().bs_engine_set_proposal(self._h, mlp.handle if mlp is not None else None,
+                                                     float(margin)))
+
+    def set_record(self, capacity: int) -> None:
+        """Records up to `capacity` rows of every sample and every proposed step of each following run (0: off)."""
+        _lib.check(_lib.lib().bs_engine_set_record(self._h, int(capacity)))
+
+    def take_record(self, which: str = "samples") -> dict:
+        """The last run's record: 'samples' (t_ns, sensor, pixel, irradiance) or 'steps' (t_ns, sensor, pixel,
+        log2 step), in recording order. Raises RuntimeError if the record's capacity was exceeded."""
+        w = {"samples": 0, "steps": 1}[which]
+        n = C.c_size_t()
+        _lib.check(_lib.lib().bs_engine_take_record(self._h, w, 0, None, None, None, C.byref(n)))
+        k = n.value
+        t = np.zeros(k, np.int64)
+        px = np.zeros(k, np.uint32)
+        v = np.zeros(k, np.float32)
+        got = C.c_size_t()
+        _lib.check(_lib.lib().bs_engine_take_record(self._h, w, k, t.ctypes.data, px.ctypes.data, v.ctypes.data,
+                                                    C.byref(got)))
+        if got.value != k:
+            raise RuntimeError(f"engine record: {got.value} rows recorded, more than its capacity")
+        out = {"t_ns": t, "sensor": (px >> 24).astype(np.int32), "pixel": px & 0xFFFFFF}
+        out["irradiance" if w == 0 else "log2_step"] = v if w == 0 else v.astype(np.int32)
+        return out

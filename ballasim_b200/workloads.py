@@ -112,3 +112,18 @@ def small(kind: str, width: int, height: int, windows: int, seed: int = 7) -> Wo
     ov = dict(MISMATCH) if kind == "blobs" else {**MISMATCH, **NOISE}
     return Workload(f"{kind}_{width}x{height}", [SensorSpec(width, height, seed, 0, ov,
                                                             F.blobs(width, height, seed, n))], windows)
+
+
+def blobs_noise(width: int, height: int, seed: int, seconds: float = 1.0) -> Workload:
+    """blobs_1280x720's laws (the mismatch sensor, leak, shot and background-activity noise) at another frame size,
+    with the same blob density (256 blobs per 1280 x 720 px). The learned step proposal trains on such fields with
+    training seeds and is evaluated on a held-out seed."""
+    n = max(1, round(256 * width * height / (1280 * 720)))
+    f = F.blobs(width, height, seed, n)
+    return Workload(f"blobs{n}_{width}x{height}_noise", [SensorSpec(width, height, seed, 0, {**MISMATCH, **NOISE}, f)],
+                    windows_for(seconds))
+
+
+# Seeds of the learned proposal's training fields and its held-out evaluation field.
+LEARN_TRAIN_SEEDS = (1001, 1002, 1003, 1004)
+LEARN_EVAL_SEED = 2077

@@ -244,7 +244,59 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     }
     if world == 1 and not (args.no_cpu_baseline or args.profile):
         out["cpu_baseline"] = cpu_baseline(wl, args.cpu_windows)
+    if rank == 0 and not (args.no_learned or args.profile):
+        out["learned_vs_plain"] = learned_comparison()
     return out
+
+
+def learned_comparison(train_stride: int = 4, steps: int = 9000) -> dict:
+    """The learned step proposal against the plain sampler (BASELINE's learned configuration): the network is
+    trained on the GPU on (history, step) pairs of the plain sampler over a training-seed 1280 x 720 field of
+    blobs_1280x720's laws (every train_stride-th pixel, 1.0 s), its margin calibrated on a validation seed at
+    640 x 360, and both samplers run the held-out-seed 1280 x 720, 1.0 s field with noise."""
+    import torch
+
+    from ballasim_b200.learned import StepMLP, calibrate_margin, compare_events, renders_and_events, trace_pairs
+
+    t0 = time.perf_counter()
+    tw = W.blobs_noise(1280, 720, W.LEARN_TRAIN_SEEDS[0])
+    x, y, _ = trace_pairs(tw.sensors[0].field, tw.rules, tw.windows, stride=train_stride, seed=1)
+    torch.cuda.synchronize()
+    t_pairs = time.perf_counter() - t0
+    net = StepMLP(seed=0)
+    t0 = time.perf_counter()
+    losses = net.train(x, y, steps=steps, batch=8192, lr=1e-3, seed=1)
+    t_train = time.perf_counter() - t0
+    n_pairs = int(len(y))
+    del x, y
+    margin, _ = calibrate_margin(net, W.blobs_noise(640, 360, W.LEARN_TRAIN_SEEDS[2]))
+    ev = W.blobs_noise(1280, 720, W.LEARN_EVAL_SEED)
+    px, sim_s = ev.pixels, ev.windows * W.WINDOW_NS * 1e-9
+    plain_r, plain_ev, plain_ms = renders_and_events(ev)
+    learned_r, learned_ev, learned_ms = renders_and_events(ev, net, margin)
+    sig = compare_events(plain_ev, learned_ev)
+    allc = compare_events(plain_ev, learned_ev, signal_only=False)
+    return {
+        "config": {"eval": f"{ev.name}, seed {W.LEARN_EVAL_SEED}, {ev.windows} windows ({sim_s:.4f} s)",
+                   "train": f"blobs256_1280x720_noise seed {W.LEARN_TRAIN_SEEDS[0]}, every {train_stride}th pixel",
+                   "pairs": n_pairs, "adam_steps": steps, "batch": 8192, "lr": 1e-3,
+                   "margin": margin, "margin_from": f"640x360 validation seed {W.LEARN_TRAIN_SEEDS[2]}"},
+        "train_s": round(t_train, 3), "pairs_s": round(t_pairs, 3),
+        "loss_first_last": [float(np.mean(losses[:10])), float(np.mean(losses[-200:]))],
+        "plain": {"renders_per_px": plain_r, "samples_per_px": plain_r + ev.windows,
+                  "events": len(plain_ev["t_cross_ns"]), "kernel_ms": plain_ms,
+                  "events_per_s": len(plain_ev["t_cross_ns"]) / (plain_ms * 1e-3)},
+        "learned": {"renders_per_px": learned_r, "samples_per_px": learned_r + ev.windows,
+                    "events": len(learned_ev["t_cross_ns"]), "kernel_ms": learned_ms,
+                    "events_per_s": len(learned_ev["t_cross_ns"]) / (learned_ms * 1e-3)},
+        "renders_ratio": plain_r / learned_r,
+        "samples_ratio": (plain_r + ev.windows) / (learned_r + ev.windows),
+        "count_diff": allc["count_diff"],
+        "signal_median_abs_dt_us": sig["median_abs_dt_ns"] / 1e3,
+        "signal_p90_abs_dt_us": sig["p90_abs_dt_ns"] / 1e3,
+        "signal_unmatched_share": sig["unmatched_share"],
+        "pixels": px,
+    }
 
 
 def cpu_baseline(wl: W.Workload, windows: int) -> dict:
@@ -307,7 +359,8 @@ def main():
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--stage", type=int, default=0, help="engine staging depth: 0, 16 or 32")
     ap.add_argument("--windows", type=int, default=0, help="run only the first windows (profiling a reduced case)")
-    ap.add_argument("--profile", action="store_true", help="no e2e or CPU legs (fewest launches, for ncu)")
+    ap.add_argument("--profile", action="store_true", help="no e2e, CPU or learned legs (fewest launches, for ncu)")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal comparison")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -216,6 +216,54 @@ bs_status bs_engine_set_launch(bs_engine* e, int32_t warps_per_block, int32_t bl
 /* Kernel time of the last bs_engine_run's launches (ms, CUDA events on its stream). */
 bs_status bs_engine_last_ms(const bs_engine* e, double* ms);
 
+/* ---- the learned step proposal (no reference counterpart: BallaSim samples with the plain lattice + midpoint rule
+ * only, src/engine/sampling.h; the plain rule stays the judge of every proposed step and its fallback) ----
+ *
+ * An MLP 16 -> 64 -> 64 -> 1 (ReLU), BF16 weights and activations with FP32 accumulation on the tensor cores,
+ * predicts log2(step / min_dt) of a pixel's next power-of-two sample step from its last 8 walk points. Parameters
+ * (FP32, BS_MLP_PARAMS floats): W1 [16 in][64 out], b1 [64], W2 [64 in][64 out], b2 [64], W3 [64], b3. Device
+ * arrays of pairs: x (n x 16 BF16 features, as uint16 bits), y (n FP32 targets). */
+#define BS_MLP_PARAMS 5313
+typedef struct bs_mlp bs_mlp;
+/* He-uniform weights drawn from Philox(seed), zero biases, Adam state zero. */
+bs_status bs_mlp_create(uint64_t seed, bs_mlp** out);
+bs_status bs_mlp_destroy(bs_mlp* m);
+bs_status bs_mlp_get_params(const bs_mlp* m, float* params);
+/* Sets the parameters (host, BS_MLP_PARAMS floats) and resets the Adam state and step counter. */
+bs_status bs_mlp_set_params(bs_mlp* m, const float* params);
+/* Adam steps taken so far. */
+bs_status bs_mlp_steps(const bs_mlp* m, int64_t* steps);
+/* y[i] = MLP(x[i]) for n rows (device arrays). */
+bs_status bs_mlp_forward(bs_mlp* m, const uint16_t* x, size_t n, float* y, void* stream);
+/* The gradient (host, BS_MLP_PARAMS doubles) and the loss of L = sum_i (MLP(x_i) - y_i)^2 / (2 n) over all n rows,
+ * from the training kernels' forward and backward passes. */
+bs_status bs_mlp_gradient(bs_mlp* m, const uint16_t* x, const float* y, size_t n, double* grad, double* loss,
+                          void* stream);
+/* `steps` Adam steps (lr, beta 0.9 / 0.999, eps 1e-8) on the same loss over batches of `batch` rows drawn with
+ * replacement from the n pairs (Philox(seed), keyed by the step count); losses (host, may be NULL) gets every
+ * step's batch loss. Runs from a CUDA graph of 32 steps. */
+bs_status bs_mlp_train(bs_mlp* m, const uint16_t* x, const float* y, size_t n, int32_t steps, int32_t batch, float lr,
+                       uint64_t seed, float* losses, void* stream);
+/* Training pairs from the plain sampler: windows [0, windows) of the field from t0 are sampled with the rules
+ * (every pixel, levels by the field's rule) and every stride-th pixel walks its runs. At each walk point the
+ * target is the longest aligned power-of-two step whose chord stays within eps of the run's log irradiance at every
+ * run sample it spans (never shorter than the plain lattice step); the walk then moves by the target lowered by
+ * 0-3 octaves (Philox(seed)). Pairs go to device arrays x (cap x 16 BF16), y (cap) and keys (cap, may be NULL:
+ * pixel << 32 | window << 11 | step); *n_out = pairs written, *total = pairs produced. */
+bs_status bs_trace_pairs(const bs_field* field, const bs_sample_rules* rules, int64_t t0_ns, int32_t windows,
+                         uint32_t stride, float eps, uint64_t seed, uint16_t* x, float* y, uint64_t* keys, size_t cap,
+                         size_t* n_out, size_t* total, void* stream);
+/* Samples the engine's windows with the learned proposal (mlp NULL: the plain sampler again). A proposal y becomes
+ * the step 2^s, s = log2 min_dt + floor(y + 0.5 - margin) clamped to [log2 min_dt, 23], raised to the plain level's
+ * lattice step and lowered until aligned. The walk state restarts from the current frame (and at every start). */
+bs_status bs_engine_set_proposal(bs_engine* e, const bs_mlp* mlp, float margin);
+/* Records up to `capacity` rows of every sample and every proposed step of each following run (0: off). */
+bs_status bs_engine_set_record(bs_engine* e, size_t capacity);
+/* Copies up to cap rows of the last run's record `which` (0: samples, v = irradiance; 1: steps, v = log2 step) to
+ * host columns t, pixel (sensor << 24 | pixel), v (any may be NULL); *n = rows recorded (> capacity: cut short). */
+bs_status bs_engine_take_record(bs_engine* e, int32_t which, size_t cap, int64_t* t, uint32_t* pixel, float* v,
+                                size_t* n);
+
 #ifdef __cplusplus
 }
 #endif

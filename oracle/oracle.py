@@ -99,6 +99,10 @@ def _events_from_records(rec: np.ndarray, width: int) -> dict:
             "dn": rec["dn"].copy(), "dl": rec["dl"].copy(), "l_first": rec["l_first"].copy()}
 
 
+class OrcWalk(C.Structure):
+    _fields_ = [("hx", C.c_float * 8), ("gaps", C.c_uint64), ("pv", C.c_float), ("valid", C.c_int32)]
+
+
 class Port:
     """The C restatement (oracle/port/oracle.c)."""
 
@@ -144,6 +148,18 @@ class Port:
                                             C.c_size_t, _f32p, _u64p, _i64p, _i64p, _f32p, C.c_size_t]
             L.orc_midpoint_eta.restype = C.c_float
             L.orc_midpoint_eta.argtypes = [C.c_float, C.c_float, C.c_float, C.c_float, C.c_float]
+            L.orc_bf16.restype = C.c_uint16
+            L.orc_bf16.argtypes = [C.c_float]
+            L.orc_step_features.argtypes = [_f32p, C.c_uint64, C.c_float, _f32p]
+            L.orc_walk_reset.argtypes = [C.POINTER(OrcWalk), C.c_float]
+            L.orc_walk_window.restype = C.c_int32
+            L.orc_walk_window.argtypes = [_i64p, _f32p, C.c_int32, C.c_int64, C.c_int32, C.c_int32, C.c_float,
+                                          C.c_uint64, C.c_uint32, C.c_int32, C.POINTER(OrcWalk), _u16p, _f32p,
+                                          _u64p, C.c_int32]
+            L.orc_learned_window.restype = C.c_int64
+            L.orc_learned_window.argtypes = [C.POINTER(OrcField), C.POINTER(OrcRules), C.c_int64, C.c_uint32,
+                                             C.c_uint32, C.c_int32, C.c_float, C.POINTER(OrcWalk), _i32p, C.c_int32,
+                                             _i64p, _f32p, C.c_size_t]
             cls._lib = L
         return cls._lib
 
@@ -189,6 +205,92 @@ class Port:
             if k >= 0:
                 return t[:k], irr[:k], off, ci, cs
             cap = -k
+
+    # ---- the learned step proposal ----
+    @classmethod
+    def step_features(cls, hx, gaps: int, x: float) -> np.ndarray:
+        out = np.zeros(16, np.float32)
+        cls.lib().orc_step_features(np.ascontiguousarray(hx, np.float32), int(gaps), float(x), out)
+        return out
+
+    @classmethod
+    def walk_pairs(cls, f, rules, windows: int, *, stride: int = 1, eps: float = 1e-4, seed: int = 0,
+                   t0: int = 0):
+        """The training walk over the oracle sampler's runs: (x uint16 (n, 16), y float32, keys uint64), in
+        (pixel, window, step) order."""
+        L = cls.lib()
+        sh = int(np.log2(rules.min_dt_ns))
+        np_ = f.width * f.height
+        ids = np.arange(np_, dtype=np.uint32)
+        carried = cls.field_frame(f, t0)
+        sig = np.zeros(np_, np.uint64)
+        walkers = ids[::stride]
+        walks = {int(p): OrcWalk() for p in walkers}
+        xs, ys, ks = [], [], []
+        for w in range(windows):
+            t_w = t0 + w * (1 << 23)
+            lv = cls.levels(f, t_w, rules.l_min, rules.l_max)
+            t, irr, off, carried, sig = cls.sample_window(f, rules, t_w, ids, lv, carried, sig)
+            for p in walkers:
+                a, b = int(off[p]), int(off[p + 1])
+                st = walks[int(p)]
+                if w == 0:
+                    L.orc_walk_reset(C.byref(st), float(irr[a]))
+                cap = 1 << 12
+                x = np.zeros((cap, 16), np.uint16)
+                y = np.zeros(cap, np.float32)
+                k = np.zeros(cap, np.uint64)
+                n = L.orc_walk_window(np.ascontiguousarray(t[a:b]), np.ascontiguousarray(irr[a:b]), b - a, t_w,
+                                      int(lv[p]), sh, float(eps), int(seed), int(p), w, C.byref(st), x, y, k, cap)
+                assert n <= cap
+                xs.append(x[:n])
+                ys.append(y[:n])
+                ks.append(k[:n])
+        x, y, k = np.concatenate(xs), np.concatenate(ys), np.concatenate(ks)
+        o = np.argsort(k, kind="stable")
+        return x[o], y[o], k[o]
+
+    @classmethod
+    def learned_replay(cls, f, rules, steps: dict, windows: int, pixels, t0: int = 0):
+        """The learned sampler's samples of the given pixels over `windows` windows for the recorded steps
+        (steps[pixel] = log2 of every proposed step in time order): {pixel: (t, v)}, slot 0 excluded."""
+        L = cls.lib()
+        s, r = field_struct(f), rules_struct(rules)
+        frame = cls.field_frame(f, t0)
+        out = {}
+        for p in pixels:
+            p = int(p)
+            x, y = p % f.width, p // f.width
+            w_st = OrcWalk()
+            L.orc_walk_reset(C.byref(w_st), float(frame[p]))
+            seq = np.ascontiguousarray(steps[p], np.int32)
+            k = 0
+            ts, vs = [], []
+            carried = float(frame[p])
+            for w in range(windows):
+                t_w = t0 + w * (1 << 23)
+                level = int(L.orc_field_level(C.byref(s), x, y, t_w, rules.l_min, rules.l_max))
+                # the steps of this window: those that start inside it
+                n_w = 0
+                cur = 0
+                while cur < (1 << 23):
+                    if k + n_w >= len(seq):
+                        raise AssertionError(f"pixel {p}: recorded steps end inside window {w}")
+                    cur += 1 << int(seq[k + n_w])
+                    n_w += 1
+                cap = 1 << 14
+                t = np.zeros(cap, np.int64)
+                v = np.zeros(cap, np.float32)
+                n = L.orc_learned_window(C.byref(s), C.byref(r), t_w, x, y, level, carried, C.byref(w_st),
+                                         np.ascontiguousarray(seq[k:k + n_w]), n_w, t, v, cap)
+                if n < 0:
+                    raise AssertionError(f"pixel {p} window {w}: invalid recorded steps (code {n})")
+                ts.append(t[:n])
+                vs.append(v[:n])
+                carried = float(v[n - 1])
+                k += n_w
+            out[p] = (np.concatenate(ts), np.concatenate(vs))
+        return out
 
     # ---- the sensor model ----
     class Model:

@@ -1029,3 +1029,122 @@ int64_t orc_sample_window(const orc_field* f, const orc_rules* r, int64_t t_w, c
   offsets[n] = (int64_t)c.n;
   return c.n <= cap ? (int64_t)c.n : -(int64_t)c.n;
 }
+
+/* ======================================================================================== */
+/* The learned step proposal: features, training walk and the sampler's judge / fallback.     */
+/* This project's own method (no reference counterpart); restated here from its definition:   */
+/* steps of 2^s ns aligned on their own lattice inside the window, judged by the plain        */
+/* midpoint rule and refined by it when rejected (sampling.h:26-69, 490-523, 638-678).        */
+/* ======================================================================================== */
+uint16_t orc_bf16(float f) {
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  if ((u & 0x7fffffffu) > 0x7f800000u) return (uint16_t)((u >> 16) | 0x40u);
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+
+static float quarter_asinh(float z) {
+  const float a = fabsf(z);
+  const float r = orc_logf(a + sqrtf(a * a + 1.0f)) * 0.25f;
+  return z < 0.0f ? -r : r;
+}
+
+void orc_step_features(const float hx[8], uint64_t gaps, float x, float out[16]) {
+  for (int k = 0; k < 8; ++k) out[k] = quarter_asinh((hx[k] - x) * 1e4f);
+  for (int k = 0; k < 8; ++k) out[8 + k] = (float)((int)((gaps >> (8 * k)) & 0xffu) - 13) * 0.1f;
+}
+
+void orc_walk_reset(orc_walk* w, float v0) {
+  const float x = orc_logf(v0);
+  for (int k = 0; k < 8; ++k) w->hx[k] = x;
+  w->gaps = 0x1717171717171717ull;
+  w->pv = v0;
+  w->valid = 0;
+}
+
+static void walk_push(orc_walk* w, float x, float v, int s) {
+  for (int k = 7; k > 0; --k) w->hx[k] = w->hx[k - 1];
+  w->hx[0] = x;
+  w->gaps = (w->gaps << 8) | (uint64_t)s;
+  w->pv = v;
+  w->valid = 1;
+}
+
+int orc_walk_window(const int64_t* t, const float* v, int n, int64_t t_w, int level, int sh, float eps, uint64_t seed,
+                    uint32_t pixel, int32_t window, orc_walk* w, uint16_t* x_out, float* y_out, uint64_t* key_out,
+                    int cap) {
+  const int s_floor = 23 - level;
+  uint32_t cur = 0;
+  int i = 0, np = 0;
+  uint32_t step_no = 0;
+  while (cur < (1u << 23) && i < n - 1) {
+    const float va = v[i], xa = orc_logf(va);
+    /* the target: the longest aligned step whose chord holds within eps at every run sample it spans */
+    int best = s_floor, j = i;
+    for (int s = s_floor + 1; s <= 23; ++s) {
+      if (cur & ((1u << s) - 1u)) break;
+      const uint32_t hi = cur + (1u << s);
+      while (j < n - 1 && (uint32_t)(t[j] - t_w) < hi) ++j;
+      if ((uint32_t)(t[j] - t_w) != hi) break;
+      const float vb = v[j], step = (float)(1u << s);
+      int ok = 1;
+      for (int k = i + 1; k < j && ok; ++k) {
+        const float lin = va + (vb - va) * ((float)((uint32_t)(t[k] - t_w) - cur) / step);
+        if (!(fabsf(orc_logf(v[k]) - orc_logf(lin)) <= eps)) ok = 0;
+      }
+      if (!ok) break;
+      best = s;
+    }
+    if (np < cap) {
+      float f[16];
+      orc_step_features(w->hx, w->gaps, xa, f);
+      for (int k = 0; k < 16; ++k) x_out[np * 16 + k] = orc_bf16(f[k]);
+      y_out[np] = (float)(best - sh);
+      key_out[np] = ((uint64_t)pixel << 32) | ((uint64_t)window << 11) | step_no;
+    }
+    ++np;
+    uint32_t d[4];
+    orc_draw(seed, 0x0090u, 0u, pixel, ((uint64_t)window << 11) | step_no, d);
+    const uint32_t u = d[0] & 7u;
+    int s_step = best - (u < 4u ? 0 : (u < 6u ? 1 : (int)u - 4));
+    if (s_step < s_floor) s_step = s_floor;
+    const uint32_t hi = cur + (1u << s_step);
+    while (i < n - 1 && (uint32_t)(t[i] - t_w) < hi) ++i;
+    walk_push(w, xa, va, s_step);
+    cur = hi;
+    ++step_no;
+  }
+  return np;
+}
+
+int64_t orc_learned_window(const orc_field* f, const orc_rules* r, int64_t t_w, uint32_t x, uint32_t y, int level,
+                           float carried, orc_walk* w, const int32_t* steps, int n_steps, int64_t* t_out,
+                           float* v_out, size_t cap) {
+  sampler_ctx c = {f, r, t_w, x, y, t_out, v_out, cap, 0};
+  const int s_floor = 23 - level;
+  const uint32_t min_split = (uint32_t)(2 * r->min_dt_ns);
+  uint32_t cur = 0;
+  float vc = carried;
+  int k = 0;
+  while (cur < (1u << 23)) {
+    if (k >= n_steps) return -1;
+    const int s = steps[k++];
+    if (s < s_floor || s > 23 || (cur & ((1u << s) - 1u)) != 0u) return -2;
+    const uint32_t dt = 1u << s, hi = cur + dt;
+    const float vb = orc_field_eval(f, x, y, t_w + hi);
+    if (dt >= min_split && !(w->valid && (int)(w->gaps & 0xffu) == s && !exceeds(r, w->pv, vc, vb))) {
+      const uint32_t g = cur + (dt >> 1);
+      const float vm = orc_field_eval(f, x, y, t_w + g);
+      const int bad = exceeds(r, vc, vm, vb);
+      if (bad && (int64_t)(g - cur) >= 2 * r->min_dt_ns) refine(&c, cur, g, vc, vm, 1, 0);
+      emit(&c, g, vm);
+      if (bad && (int64_t)(hi - g) >= 2 * r->min_dt_ns) refine(&c, g, hi, vm, vb, 1, 0);
+    }
+    emit(&c, hi, vb);
+    walk_push(w, orc_logf(vc), vc, s);
+    cur = hi;
+    vc = vb;
+  }
+  return k == n_steps ? (int64_t)c.n : -3;
+}

@@ -117,6 +117,30 @@ int64_t orc_sample_window(const orc_field* f, const orc_rules* r, int64_t t_w, c
 /* eta_L of triples (src/engine/sampling.h:36-53), G = 1. */
 float orc_midpoint_eta(float tol, float dark, float a, float m, float b);
 
+/* ---- the learned step proposal (this project's own method; no reference counterpart) ---- */
+typedef struct {
+  float hx[8];    /* log irradiance of the last 8 walk points, newest first */
+  uint64_t gaps;  /* byte k: log2 of the k-th previous gap (byte 0 newest) */
+  float pv;       /* irradiance at the previous walk point */
+  int32_t valid;  /* a real previous walk point exists */
+} orc_walk;
+
+uint16_t orc_bf16(float f); /* round to nearest even */
+void orc_step_features(const float hx[8], uint64_t gaps, float x, float out[16]);
+void orc_walk_reset(orc_walk* w, float v0);
+/* The training walk over one pixel's plain run of one window (t absolute, n samples, slot 0 at t_w and the last at
+ * t_w + 2^23): appends up to cap pairs (16 BF16 features, target log2(step) - sh, key pixel << 32 | window << 11 |
+ * step) and returns the number of walk points. */
+int orc_walk_window(const int64_t* t, const float* v, int n, int64_t t_w, int level, int sh, float eps, uint64_t seed,
+                    uint32_t pixel, int32_t window, orc_walk* w, uint16_t* x_out, float* y_out, uint64_t* key_out,
+                    int cap);
+/* The learned sampler's samples of one pixel and window for the given step sequence (log2 of each proposed step, as
+ * the device used them): the judge and the plain-rule refinement. Returns the samples written after slot 0, or a
+ * negative code: -1 too few steps, -2 a step below the plain lattice step, above 2^23 or unaligned, -3 steps left. */
+int64_t orc_learned_window(const orc_field* f, const orc_rules* r, int64_t t_w, uint32_t x, uint32_t y, int level,
+                           float carried, orc_walk* w, const int32_t* steps, int n_steps, int64_t* t_out,
+                           float* v_out, size_t cap);
+
 #ifdef __cplusplus
 }
 #endif
