@@ -105,7 +105,10 @@ _SIGS = {
     "bs_engine_start": (C.c_int32, [_P, C.c_int64, _P]),
     "bs_engine_start_frames": (C.c_int32, [_P, C.c_int64, _P, _P]),
     "bs_engine_run": (C.c_int32, [_P, C.c_int32, _P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
-    "bs_engine_set_launch": (C.c_int32, [_P, C.c_int32, C.c_int32, C.c_int32]),
+    "bs_engine_set_launch": (C.c_int32, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "bs_engine_get_launch": (C.c_int32, [_P, _P]),
+    "bs_engine_set_graph": (C.c_int32, [_P, C.c_int32]),
+    "bs_engine_autotune": (C.c_int32, [_P, C.c_int32, _P, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
     "bs_engine_last_ms": (C.c_int32, [_P, C.POINTER(C.c_double)]),
     "bs_mlp_create": (C.c_int32, [C.c_uint64, C.POINTER(_P)]),
     "bs_mlp_destroy": (C.c_int32, [_P]),
@@ -114,7 +117,8 @@ _SIGS = {
     "bs_mlp_steps": (C.c_int32, [_P, C.POINTER(C.c_int64)]),
     "bs_mlp_forward": (C.c_int32, [_P, _P, C.c_size_t, _P, _P]),
     "bs_mlp_gradient": (C.c_int32, [_P, _P, _P, C.c_size_t, _P, C.POINTER(C.c_double), _P]),
-    "bs_mlp_train": (C.c_int32, [_P, _P, _P, C.c_size_t, C.c_int32, C.c_int32, C.c_float, C.c_uint64, _P, _P]),
+    "bs_mlp_train": (C.c_int32, [_P, _P, _P, C.c_size_t, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_uint64, _P,
+                                 _P]),
     "bs_trace_pairs": (C.c_int32, [C.POINTER(Field), C.POINTER(SampleRules), C.c_int64, C.c_int32, C.c_uint32,
                                    C.c_float, C.c_uint64, _P, _P, _P, C.c_size_t, C.POINTER(C.c_size_t),
                                    C.POINTER(C.c_size_t), _P]),

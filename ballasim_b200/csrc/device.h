@@ -118,9 +118,10 @@ void launch_field_frame(const FieldDev& f, int64_t t, uint32_t n_pixels, float* 
 // The fused engine: windows [w0, w1) of every sensor, one warp per 8 x 4 pixel tile, tiles taken from a global
 // counter (work stealing) by a persistent grid. stage 0: the sampler feeds the pixel model sample by sample;
 // 16 or 32: per window the samples are staged in shared memory (that many per lane) between the two phases.
-void launch_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t total_tiles, int64_t t0, int32_t w0,
-                   int32_t w1, const SamplerRules& r, unsigned int* tile_counter, int blocks, int warps_per_block,
-                   int stage, cudaStream_t stream);
+// t0: the model time in device memory; tiles of 2^tile_lw x 2^(5 - tile_lw) pixels (tile_lw in [2, 5]).
+void launch_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t total_tiles, const int64_t* t0,
+                   int32_t w0, int32_t w1, const SamplerRules& r, unsigned int* tile_counter, int blocks,
+                   int warps_per_block, int stage, int tile_lw, cudaStream_t stream);
 int engine_max_blocks_per_sm(int warps_per_block, int stage);
 // The fused engine with the learned step proposal (BF16 MLP operands and FP32 parameters in device memory):
 // the same tiles and pixel model, each window sampled by proposed power-of-two steps judged by the plain rule.
@@ -132,9 +133,10 @@ struct LearnedLaunch {
   int32_t sh;  // log2 min_dt_ns
   RecBuf rec_samples, rec_steps;
 };
-void launch_learned_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t total_tiles, int64_t t0,
+void launch_learned_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t total_tiles, const int64_t* t0,
                            int32_t w0, int32_t w1, const SamplerRules& r, const LearnedLaunch& l,
-                           unsigned int* tile_counter, int blocks, int warps_per_block, cudaStream_t stream);
+                           unsigned int* tile_counter, int blocks, int warps_per_block, int tile_lw,
+                           cudaStream_t stream);
 int learned_engine_max_blocks_per_sm(int warps_per_block);
 // Resets the walk state of n pixels from their initial irradiance.
 void launch_learned_reset(LearnedSoA st, uint32_t n, const float* irr0, cudaStream_t stream);
@@ -175,6 +177,9 @@ struct TrainArgs {
   float* partial;         // [grid][kMlpParamsPad]
   double* partial_loss;   // [grid]
   float inv_rows;
+  // Expectile weight tau: a row's squared error counts 2 tau when the net predicts below its target and
+  // 2 (1 - tau) above it (0.5: the plain mean squared error).
+  float tau;
 };
 int train_grid(uint32_t rows);
 void launch_train_partials(const TrainArgs& a, cudaStream_t stream);

@@ -368,11 +368,19 @@ struct EngineArgs {
   const EngineSensor* sensors;
   int n_sensors;
   uint32_t total_tiles;
-  int64_t t0;
+  const int64_t* t0;  // the model time, in device memory (a captured launch replays at any time)
   int32_t w0, w1;
   SamplerRules r;
   unsigned int* tile_counter;
+  uint32_t tile_lw;   // log2 of the tile width: tiles of 2^lw x 2^(5 - lw) pixels, one warp each
 };
+
+// The pixel of `lane` in tile `local` of a sensor with tiles_x tiles per row.
+__device__ __forceinline__ void tile_xy(uint32_t local, uint32_t tiles_x, uint32_t lw, uint32_t lane, uint32_t& x,
+                                        uint32_t& y) {
+  x = (local % tiles_x) * (1u << lw) + (lane & ((1u << lw) - 1u));
+  y = (local / tiles_x) * (32u >> lw) + (lane >> lw);
+}
 
 // Feeds a window's samples, in time order, to the pixel model: every segment lies inside the window, so each
 // takes the fast path with x at both ends, each x computed once.
@@ -404,6 +412,7 @@ struct WindowFeed {
 
 __global__ void __launch_bounds__(128) engine_kernel(EngineArgs a) {
   const uint32_t lane = threadIdx.x & 31u;
+  const int64_t t0 = *a.t0;
   for (;;) {
     uint32_t tile = 0;
     if (lane == 0) tile = atomicAdd(a.tile_counter, 1u);
@@ -413,7 +422,8 @@ __global__ void __launch_bounds__(128) engine_kernel(EngineArgs a) {
     while (si + 1 < a.n_sensors && a.sensors[si + 1].tile0 <= tile) ++si;
     const EngineSensor& S = a.sensors[si];
     const uint32_t local = tile - S.tile0;
-    const uint32_t x = (local % S.tiles_x) * 8u + (lane & 7u), y = (local / S.tiles_x) * 4u + (lane >> 3);
+    uint32_t x, y;
+    tile_xy(local, S.tiles_x, a.tile_lw, lane, x, y);
     const bool have = x < S.width && y < S.height;
     const uint32_t p = have ? y * S.width + x : 0u;
     const bool noise = S.consts.noise != 0;
@@ -433,7 +443,7 @@ __global__ void __launch_bounds__(128) engine_kernel(EngineArgs a) {
     __shared__ uint16_t lists[4][kMaxListed];
     uint16_t* my_list = lists[threadIdx.x >> 5];
     for (int32_t w = a.w0; w < a.w1; ++w) {
-      const int64_t t_w = a.t0 + static_cast<int64_t>(w) * kWindowNs;
+      const int64_t t_w = t0 + static_cast<int64_t>(w) * kWindowNs;
       const BlobList list = warp_blob_list(f, have, x, y, t_w, t_w + kWindowNs, my_list);
       if (have) {
         const int level = field_level(f, list, x, y, t_w, a.r.l_min, a.r.l_max);
@@ -465,6 +475,7 @@ __global__ void __launch_bounds__(128) engine_kernel(EngineArgs a) {
 template <int kStage>
 __global__ void __launch_bounds__(128) engine_kernel_staged(EngineArgs a) {
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const int64_t t0 = *a.t0;
   __shared__ uint16_t lists[4][kMaxListed];
   __shared__ uint32_t st_dt[4][kStage][32];
   __shared__ float st_v[4][kStage][32];
@@ -478,7 +489,8 @@ __global__ void __launch_bounds__(128) engine_kernel_staged(EngineArgs a) {
     while (si + 1 < a.n_sensors && a.sensors[si + 1].tile0 <= tile) ++si;
     const EngineSensor& S = a.sensors[si];
     const uint32_t local = tile - S.tile0;
-    const uint32_t x = (local % S.tiles_x) * 8u + (lane & 7u), y = (local / S.tiles_x) * 4u + (lane >> 3);
+    uint32_t x, y;
+    tile_xy(local, S.tiles_x, a.tile_lw, lane, x, y);
     const bool have = x < S.width && y < S.height;
     const uint32_t p = have ? y * S.width + x : 0u;
     const bool noise = S.consts.noise != 0;
@@ -496,7 +508,7 @@ __global__ void __launch_bounds__(128) engine_kernel_staged(EngineArgs a) {
     PixelProc<GlobalSink> proc{s, m, S.consts, p, sink, c};
     const FieldDev& f = S.field;
     for (int32_t w = a.w0; w < a.w1; ++w) {
-      const int64_t t_w = a.t0 + static_cast<int64_t>(w) * kWindowNs;
+      const int64_t t_w = t0 + static_cast<int64_t>(w) * kWindowNs;
       const BlobList list = warp_blob_list(f, have, x, y, t_w, t_w + kWindowNs, my_list);
       auto render = [&](uint32_t dt) { return field_eval(f, list, x, y, t_w + dt); };
       // Phase A: the walk, its first kStage samples after slot 0 staged.
@@ -580,6 +592,7 @@ __global__ void learned_reset_kernel(LearnedSoA st, uint32_t n, const float* irr
 // the loop ends when every lane has reached the window's end.
 __global__ void __launch_bounds__(128) learned_engine_kernel(EngineArgs a, LearnedLaunch l) {
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const int64_t t0 = *a.t0;
   __shared__ MlpShared W;
   __shared__ __align__(16) uint16_t rows[4][32 * kSF];
   __shared__ float ys[4][32];
@@ -598,7 +611,8 @@ __global__ void __launch_bounds__(128) learned_engine_kernel(EngineArgs a, Learn
     while (si + 1 < a.n_sensors && a.sensors[si + 1].tile0 <= tile) ++si;
     const EngineSensor& S = a.sensors[si];
     const uint32_t local = tile - S.tile0;
-    const uint32_t x = (local % S.tiles_x) * 8u + (lane & 7u), y = (local / S.tiles_x) * 4u + (lane >> 3);
+    uint32_t x, y;
+    tile_xy(local, S.tiles_x, a.tile_lw, lane, x, y);
     const bool have = x < S.width && y < S.height;
     const uint32_t np = S.width * S.height;
     const uint32_t p = have ? y * S.width + x : 0u;
@@ -620,7 +634,7 @@ __global__ void __launch_bounds__(128) learned_engine_kernel(EngineArgs a, Learn
     PixelProc<GlobalSink> proc{s, m, S.consts, p, sink, c};
     const FieldDev& f = S.field;
     for (int32_t w = a.w0; w < a.w1; ++w) {
-      const int64_t t_w = a.t0 + static_cast<int64_t>(w) * kWindowNs;
+      const int64_t t_w = t0 + static_cast<int64_t>(w) * kWindowNs;
       const BlobList list = warp_blob_list(f, have, x, y, t_w, t_w + kWindowNs, my_list);
       auto render = [&](uint32_t dt) { return field_eval(f, list, x, y, t_w + dt); };
       WindowFeed feed{&proc, t_w, S.consts.irr_max, t_w, s.held, carried, 0.0f};
@@ -789,10 +803,10 @@ void launch_field_frame(const FieldDev& f, int64_t t, uint32_t n_pixels, float* 
   field_frame_kernel<<<(n_pixels + 255) / 256, 256, 0, stream>>>(f, t, n_pixels, out);
 }
 
-void launch_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t total_tiles, int64_t t0, int32_t w0,
-                   int32_t w1, const SamplerRules& r, unsigned int* tile_counter, int blocks, int warps_per_block,
-                   int stage, cudaStream_t stream) {
-  EngineArgs a{sensors_dev, n_sensors, total_tiles, t0, w0, w1, r, tile_counter};
+void launch_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t total_tiles, const int64_t* t0,
+                   int32_t w0, int32_t w1, const SamplerRules& r, unsigned int* tile_counter, int blocks,
+                   int warps_per_block, int stage, int tile_lw, cudaStream_t stream) {
+  EngineArgs a{sensors_dev, n_sensors, total_tiles, t0, w0, w1, r, tile_counter, static_cast<uint32_t>(tile_lw)};
   if (stage == 16) engine_kernel_staged<16><<<blocks, warps_per_block * 32, 0, stream>>>(a);
   else if (stage == 32) engine_kernel_staged<32><<<blocks, warps_per_block * 32, 0, stream>>>(a);
   else engine_kernel<<<blocks, warps_per_block * 32, 0, stream>>>(a);
@@ -814,10 +828,11 @@ int engine_max_blocks_per_sm(int warps_per_block, int stage) {
 
 namespace bs {
 
-void launch_learned_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t total_tiles, int64_t t0,
+void launch_learned_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t total_tiles, const int64_t* t0,
                            int32_t w0, int32_t w1, const SamplerRules& r, const LearnedLaunch& l,
-                           unsigned int* tile_counter, int blocks, int warps_per_block, cudaStream_t stream) {
-  EngineArgs a{sensors_dev, n_sensors, total_tiles, t0, w0, w1, r, tile_counter};
+                           unsigned int* tile_counter, int blocks, int warps_per_block, int tile_lw,
+                           cudaStream_t stream) {
+  EngineArgs a{sensors_dev, n_sensors, total_tiles, t0, w0, w1, r, tile_counter, static_cast<uint32_t>(tile_lw)};
   (void)warps_per_block;  // 4 warps: the shared tiles are sized for them
   learned_engine_kernel<<<blocks, 128, 0, stream>>>(a, l);
 }

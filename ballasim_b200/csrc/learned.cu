@@ -222,9 +222,10 @@ __global__ void __launch_bounds__(128) train_partials_kernel(TrainArgs a) {
     y0 += S.b3;
     y1 += S.b3;
     const float e0 = v0 ? y0 - a.y[i0] : 0.0f, e1 = v1 ? y1 - a.y[i1] : 0.0f;
-    const float dy0 = e0 * a.inv_rows, dy1 = e1 * a.inv_rows;
+    const float w0 = 2.0f * (e0 < 0.0f ? a.tau : 1.0f - a.tau), w1 = 2.0f * (e1 < 0.0f ? a.tau : 1.0f - a.tau);
+    const float dy0 = w0 * e0 * a.inv_rows, dy1 = w1 * e1 * a.inv_rows;
     if (q == 0) {
-      sloss += static_cast<double>(e0) * e0 + static_cast<double>(e1) * e1;
+      sloss += static_cast<double>(w0) * e0 * e0 + static_cast<double>(w1) * e1 * e1;
       sdy += dy0 + dy1;
     }
     // dH2 = dy W3^T masked by ReLU; the dW3 and db2 column sums

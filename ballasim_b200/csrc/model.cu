@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -774,7 +775,7 @@ struct Mlp {
     partial.ensure(static_cast<size_t>(ctas) * kMlpParamsPad);
     partial_loss.ensure(ctas);
     TrainArgs a{x, y, n, static_cast<uint32_t>(n), 0, 0, step.p, ops.p, params.p, partial.p, partial_loss.p,
-                1.0f / static_cast<float>(n)};
+                1.0f / static_cast<float>(n), 0.5f};
     launch_train_partials(a, s);
     launch_reduce_partials(partial.p, partial_loss.p, ctas, a.inv_rows, grad.p, loss.p, s);
     CK(cudaGetLastError());
@@ -785,8 +786,9 @@ struct Mlp {
 
   // `steps` Adam steps on batches of `batch` rows drawn with replacement from the n pairs. The steps run from a
   // CUDA graph of 32 steps (two launches each), replayed; the loss of every step is kept on the device.
-  void train(const uint16_t* x, const float* y, size_t n, int32_t steps, int32_t batch, float lr, uint64_t seed,
-             float* losses_host, cudaStream_t s) {
+  void train(const uint16_t* x, const float* y, size_t n, int32_t steps, int32_t batch, float lr, float tau,
+             uint64_t seed, float* losses_host, cudaStream_t s) {
+    if (!(tau > 0.0f && tau < 1.0f)) throw std::invalid_argument("mlp.train: tau must lie in (0, 1)");
     if (n == 0) throw std::invalid_argument("mlp.train: no pairs");
     if (!x || !y) throw std::invalid_argument("mlp.train: null device array");
     if (steps < 0 || batch < 1 || batch > (1 << 24)) throw std::invalid_argument("mlp.train: bad steps or batch");
@@ -796,7 +798,7 @@ struct Mlp {
     partial_loss.ensure(ctas);
     const int64_t s0 = steps_from_device(s);
     const TrainArgs a{x, y, n, static_cast<uint32_t>(batch), 1, seed, step.p, ops.p, params.p, partial.p,
-                      partial_loss.p, 1.0f / static_cast<float>(batch)};
+                      partial_loss.p, 1.0f / static_cast<float>(batch), tau};
     auto one = [&](cudaStream_t st) {
       launch_train_partials(a, st);
       launch_adam(params.p, m.p, v.p, ops.p, partial.p, partial_loss.p, ctas, lr, a.inv_rows, step.p, losses.p,
@@ -812,7 +814,7 @@ struct Mlp {
     if (left >= kGraphSteps) {
       // The graph holds its launches' arguments and buffer addresses: rebuild it when any of them changes.
       const uint64_t key[8] = {reinterpret_cast<uint64_t>(x), reinterpret_cast<uint64_t>(y), n,
-                               (static_cast<uint64_t>(batch) << 32) ^ f2u(lr), seed,
+                               (static_cast<uint64_t>(batch) << 32) ^ f2u(lr), seed ^ (uint64_t{f2u(tau)} << 32),
                                reinterpret_cast<uint64_t>(partial.p), reinterpret_cast<uint64_t>(partial_loss.p),
                                static_cast<uint64_t>(ctas)};
       if (!exec || std::memcmp(key, graph_key, sizeof(key)) != 0) {
@@ -939,10 +941,21 @@ struct Engine {
   DevBuf<unsigned int> tile_counter;
   std::vector<EngineSensor> host;
   uint32_t total_tiles = 0;
-  int warps_per_block = 4, blocks_per_sm = 0, stage = 0;
+  int warps_per_block = 4, blocks_per_sm = 0, stage = 0, tile_lw = 3;
   double last_ms = 0;
   Timer timer;
   cudaStream_t own = nullptr;
+  cudaEvent_t order = nullptr;
+  // The step as a CUDA graph (rebuilt when its launch shape, window count or proposal changes), fed from pinned
+  // descriptors and model time.
+  bool use_graph = true;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t graph_key[8] = {};
+  PinBuf<EngineSensor> host_pin;
+  PinBuf<int64_t> t0_pin;
+  DevBuf<int64_t> t0_dev;
+  PinBuf<unsigned long long> rec_n_pin;
   // The learned step proposal (null: the plain sampler), its walk state (2 per sensor) and the record buffers.
   const Mlp* mlp = nullptr;
   float margin = 0.25f;
@@ -983,11 +996,16 @@ struct Engine {
       host.push_back(e);
     }
     total_tiles = tile0;
+    retile();
     sensors_dev.ensure(host.size());
     tile_counter.ensure(1);
+    t0_dev.ensure(1);
     CK(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&order, cudaEventDisableTiming));
   }
   ~Engine() {
+    release_graph();
+    if (order) cudaEventDestroy(order);
     if (own) cudaStreamDestroy(own);
   }
 
@@ -1055,7 +1073,100 @@ struct Engine {
     *n = static_cast<size_t>(rec_n[which]);
   }
 
-  void run(int32_t windows, cudaStream_t s, uint64_t* samples_out, uint64_t* events_out) {
+  // The launch shape: tile width 2^tile_lw (tiles of 2^tile_lw x 2^(5 - tile_lw) px, one warp each), warps per
+  // block, blocks per SM (0: as many as fit) and the plain engine's staging depth.
+  void retile() {
+    uint32_t tile0 = 0;
+    const uint32_t tw = 1u << tile_lw, th = 32u >> tile_lw;
+    for (EngineSensor& e : host) {
+      e.tiles_x = (e.width + tw - 1) / tw;
+      e.tiles_y = (e.height + th - 1) / th;
+      e.tile0 = tile0;
+      tile0 += e.tiles_x * e.tiles_y;
+    }
+    total_tiles = tile0;
+  }
+
+  int block_warps() const { return mlp ? 4 : warps_per_block; }
+  int grid_blocks() const {
+    int dev = 0, sms = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int wpb = block_warps();
+    const int per_sm = blocks_per_sm > 0 ? blocks_per_sm
+                                         : std::max(1, mlp ? learned_engine_max_blocks_per_sm(wpb)
+                                                           : engine_max_blocks_per_sm(wpb, stage));
+    return static_cast<int>(
+        std::min<uint64_t>(static_cast<uint64_t>(sms) * per_sm, (total_tiles + wpb - 1) / wpb));
+  }
+
+  // Fills the pinned launch descriptors from the models' current buffers.
+  void describe(int64_t t0) {
+    host_pin.ensure(host.size());
+    for (size_t i = 0; i < models.size(); ++i) {
+      Model* m = models[i];
+      EngineSensor& e = host[i];
+      e.field = fields[i]->f;
+      e.consts = m->k;
+      e.in = m->soa[m->cur];
+      e.out = m->soa[1 - m->cur];
+      e.map = m->map;
+      e.carried_in = carried[2 * i + carried_cur[i]]->p;
+      e.carried_out = carried[2 * i + 1 - carried_cur[i]]->p;
+      e.ev = EventBuf{m->events.p, static_cast<unsigned long long>(m->event_cap)};
+      e.counters = m->counters.p;
+      if (mlp) {
+        e.lin = lbufs[2 * i + lcur[i]]->soa(m->n);
+        e.lout = lbufs[2 * i + 1 - lcur[i]]->soa(m->n);
+      }
+      host_pin.p[i] = e;
+    }
+    t0_pin.p[0] = t0;
+  }
+
+  // One step's device work, in stream order (what the CUDA graph holds): counters cleared, descriptors and the
+  // model time uploaded from pinned memory, the persistent kernel between two timing events, counters read back.
+  void enqueue(int32_t windows, int blocks, cudaStream_t st, bool capturing) {
+    const unsigned rec_flags = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+    for (Model* m : models) CK(cudaMemsetAsync(m->counters.p, 0, kCntWords * sizeof(unsigned long long), st));
+    if (rec_cap) CK(cudaMemsetAsync(rec_count.p, 0, 2 * sizeof(unsigned long long), st));
+    CK(cudaMemcpyAsync(sensors_dev.p, host_pin.p, host.size() * sizeof(EngineSensor), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(t0_dev.p, t0_pin.p, sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(tile_counter.p, 0, sizeof(unsigned int), st));
+    // Inside a captured graph, external records become event-record nodes (the timing of every replay).
+    CK(cudaEventRecordWithFlags(timer.a, st, rec_flags));
+    if (windows > 0 && total_tiles > 0) {
+      if (mlp) {
+        int sh = 0;
+        while ((2u << sh) < rules.min_split) ++sh;
+        const LearnedLaunch l{mlp->ops.p, mlp->params.p, margin, sh,
+                              RecBuf{rec[0].p, rec_count.p, rec_cap}, RecBuf{rec[1].p, rec_count.p + 1, rec_cap}};
+        launch_learned_engine(sensors_dev.p, static_cast<int>(host.size()), total_tiles, t0_dev.p, 0, windows,
+                              rules, l, tile_counter.p, blocks, block_warps(), tile_lw, st);
+      } else {
+        launch_engine(sensors_dev.p, static_cast<int>(host.size()), total_tiles, t0_dev.p, 0, windows, rules,
+                      tile_counter.p, blocks, warps_per_block, stage, tile_lw, st);
+      }
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecordWithFlags(timer.b, st, rec_flags));
+    for (Model* m : models) {
+      CK(cudaMemcpyAsync(m->counters_h.p, m->counters.p, kCntWords * sizeof(unsigned long long),
+                         cudaMemcpyDeviceToHost, st));
+    }
+    if (rec_cap) CK(cudaMemcpyAsync(rec_n_pin.p, rec_count.p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  }
+
+  void release_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+  }
+
+  // Runs the step once (re-running it with larger event buffers while they overflow); with commit the models move
+  // to the step's end, without it (a trial) they keep their state.
+  void step(int32_t windows, cudaStream_t s, bool commit, uint64_t* samples_out, uint64_t* events_out) {
     if (windows < 0) throw std::invalid_argument("engine: windows must be >= 0");
     const int64_t t0 = models[0]->t_state;
     for (Model* m : models) {
@@ -1063,64 +1174,46 @@ struct Engine {
       if (m->t_state != t0) throw std::logic_error("engine: the sensors' model times differ");
       if ((t0 & (kWindowNs - 1)) != 0) throw std::invalid_argument("engine: the model time must be a window start");
     }
-    int dev = 0, sms = 0;
-    CK(cudaGetDevice(&dev));
-    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const int wpb = mlp ? 4 : warps_per_block;
-    const int per_sm = blocks_per_sm > 0 ? blocks_per_sm
-                                         : std::max(1, mlp ? learned_engine_max_blocks_per_sm(wpb)
-                                                           : engine_max_blocks_per_sm(wpb, stage));
-    const int blocks = static_cast<int>(
-        std::min<uint64_t>(static_cast<uint64_t>(sms) * per_sm, (total_tiles + wpb - 1) / wpb));
     if (mlp && lcur.size() != models.size()) throw std::logic_error("engine: call start() after set_proposal()");
+    const int blocks = grid_blocks();
+    t0_pin.ensure(1);
+    rec_n_pin.ensure(2);
     for (;;) {
-      for (size_t i = 0; i < models.size(); ++i) {
-        Model* m = models[i];
-        EngineSensor& e = host[i];
-        e.field = fields[i]->f;
-        e.consts = m->k;
-        e.in = m->soa[m->cur];
-        e.out = m->soa[1 - m->cur];
-        e.map = m->map;
-        e.carried_in = carried[2 * i + carried_cur[i]]->p;
-        e.carried_out = carried[2 * i + 1 - carried_cur[i]]->p;
-        e.ev = EventBuf{m->events.p, static_cast<unsigned long long>(m->event_cap)};
-        e.counters = m->counters.p;
-        if (mlp) {
-          e.lin = lbufs[2 * i + lcur[i]]->soa(m->n);
-          e.lout = lbufs[2 * i + 1 - lcur[i]]->soa(m->n);
+      describe(t0);
+      if (use_graph && rec_cap == 0) {
+        const uint64_t key[8] = {static_cast<uint64_t>(windows), static_cast<uint64_t>(blocks),
+                                 static_cast<uint64_t>(block_warps()), static_cast<uint64_t>(stage),
+                                 static_cast<uint64_t>(tile_lw), reinterpret_cast<uint64_t>(mlp),
+                                 (static_cast<uint64_t>(f2u(margin)) << 32) | total_tiles, 1};
+        if (!exec || std::memcmp(key, graph_key, sizeof(key)) != 0) {
+          release_graph();
+          CK(cudaStreamBeginCapture(own, cudaStreamCaptureModeThreadLocal));
+          try {
+            enqueue(windows, blocks, own, true);
+          } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(own, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+          }
+          CK(cudaStreamEndCapture(own, &graph));
+          CK(cudaGraphInstantiate(&exec, graph, 0));
+          std::memcpy(graph_key, key, sizeof(key));
         }
-        CK(cudaMemsetAsync(m->counters.p, 0, kCntWords * sizeof(unsigned long long), s));
+        CK(cudaEventRecord(order, s));
+        CK(cudaStreamWaitEvent(own, order, 0));
+        CK(cudaGraphLaunch(exec, own));
+        CK(cudaEventRecord(order, own));
+        CK(cudaStreamWaitEvent(s, order, 0));
+        CK(cudaStreamSynchronize(own));
+      } else {
+        enqueue(windows, blocks, s, false);
+        CK(cudaStreamSynchronize(s));
       }
-      if (rec_cap) CK(cudaMemsetAsync(rec_count.p, 0, 2 * sizeof(unsigned long long), s));
-      CK(cudaMemcpyAsync(sensors_dev.p, host.data(), host.size() * sizeof(EngineSensor), cudaMemcpyHostToDevice, s));
-      CK(cudaMemsetAsync(tile_counter.p, 0, sizeof(unsigned int), s));
-      CK(cudaEventRecord(timer.a, s));
-      if (windows > 0 && total_tiles > 0) {
-        if (mlp) {
-          int sh = 0;
-          while ((2u << sh) < rules.min_split) ++sh;
-          const LearnedLaunch l{mlp->ops.p, mlp->params.p, margin, sh,
-                                RecBuf{rec[0].p, rec_count.p, rec_cap}, RecBuf{rec[1].p, rec_count.p + 1, rec_cap}};
-          launch_learned_engine(sensors_dev.p, static_cast<int>(host.size()), total_tiles, t0, 0, windows, rules, l,
-                                tile_counter.p, blocks, wpb, s);
-        } else {
-          launch_engine(sensors_dev.p, static_cast<int>(host.size()), total_tiles, t0, 0, windows, rules,
-                        tile_counter.p, blocks, warps_per_block, stage, s);
-        }
-      }
-      CK(cudaGetLastError());
-      CK(cudaEventRecord(timer.b, s));
-      bool rerun = false;
-      for (Model* m : models) {
-        CK(cudaMemcpyAsync(m->counters_h.p, m->counters.p, kCntWords * sizeof(unsigned long long),
-                           cudaMemcpyDeviceToHost, s));
-      }
-      if (rec_cap) CK(cudaMemcpyAsync(rec_n, rec_count.p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
       float ms = 0;
-      cudaEventElapsedTime(&ms, timer.a, timer.b);
+      CK(cudaEventElapsedTime(&ms, timer.a, timer.b));
       last_ms = ms;
+      bool rerun = false;
       for (Model* m : models) {
         const unsigned long long ev = m->counters_h.p[kCntEvents];
         if (ev > m->event_cap) {
@@ -1130,7 +1223,19 @@ struct Engine {
         }
       }
       if (rerun) continue;
+      if (rec_cap) {
+        rec_n[0] = rec_n_pin.p[0];
+        rec_n[1] = rec_n_pin.p[1];
+      }
       uint64_t samples = 0, events = 0;
+      for (size_t i = 0; i < models.size(); ++i) {
+        const unsigned long long* c = models[i]->counters_h.p;
+        samples += c[kCntSamples];
+        events += c[kCntEvents];
+      }
+      if (samples_out) *samples_out = samples;
+      if (events_out) *events_out = events;
+      if (!commit) return;
       for (size_t i = 0; i < models.size(); ++i) {
         Model* m = models[i];
         const unsigned long long* c = m->counters_h.p;
@@ -1147,13 +1252,56 @@ struct Engine {
         m->t_state = t0 + static_cast<int64_t>(windows) * kWindowNs;
         carried_cur[i] = 1 - carried_cur[i];
         if (mlp) lcur[i] = 1 - lcur[i];
-        samples += c[kCntSamples];
-        events += c[kCntEvents];
       }
-      if (samples_out) *samples_out = samples;
-      if (events_out) *events_out = events;
       return;
     }
+  }
+
+  void run(int32_t windows, cudaStream_t s, uint64_t* samples_out, uint64_t* events_out) {
+    step(windows, s, true, samples_out, events_out);
+  }
+
+  void set_launch(int32_t warps, int32_t per_sm, int32_t stg, int32_t lw) {
+    if (warps < 0 || warps > 4) throw std::invalid_argument("engine: warps per block must lie in [1, 4]");
+    if (per_sm < 0 || per_sm > 32) throw std::invalid_argument("engine: blocks_per_sm in [0, 32]");
+    if (stg != 0 && stg != 16 && stg != 32) throw std::invalid_argument("engine: stage 0, 16 or 32");
+    if (lw != 0 && (lw < 2 || lw > 5)) throw std::invalid_argument("engine: tile width 4, 8, 16 or 32");
+    warps_per_block = warps ? warps : 4;
+    blocks_per_sm = per_sm;
+    stage = stg;
+    tile_lw = lw ? lw : 3;
+    retile();
+  }
+
+  // Times each candidate launch shape on trial steps of `windows` windows from the current state (the models keep
+  // their state) and keeps the fastest. Candidates: tile width 4, 8, 16 px (height 8, 4, 2) x warps per block 2, 4 x
+  // staging depth 0, 16 (the learned engine: tile widths only). Returns the candidates tried (ms of the second of
+  // two trial steps each); rows are {tile_lw, warps, stage, ms}.
+  std::vector<std::array<double, 4>> autotune(int32_t windows, cudaStream_t s) {
+    if (windows < 1) throw std::invalid_argument("engine.autotune: windows >= 1");
+    std::vector<std::array<double, 4>> rows;
+    const int keep[4] = {tile_lw, warps_per_block, stage, blocks_per_sm};
+    double best = 1e300;
+    int bl = keep[0], bw = keep[1], bs = keep[2];
+    for (int lw : {2, 3, 4}) {
+      for (int w : {2, 4}) {
+        for (int st : {0, 16}) {
+          if (mlp && (w != 4 || st != 0)) continue;
+          set_launch(w, 0, st, lw);
+          step(windows, s, false, nullptr, nullptr);
+          step(windows, s, false, nullptr, nullptr);
+          rows.push_back({static_cast<double>(lw), static_cast<double>(w), static_cast<double>(st), last_ms});
+          if (last_ms < best) {
+            best = last_ms;
+            bl = lw;
+            bw = w;
+            bs = st;
+          }
+        }
+      }
+    }
+    set_launch(bw, keep[3], bs, bl);
+    return rows;
   }
 };
 
@@ -1544,17 +1692,47 @@ bs_status bs_engine_run(bs_engine* e, int32_t windows, void* stream, uint64_t* p
     e->run(windows, stream ? static_cast<cudaStream_t>(stream) : e->own, pixel_samples, events);
   });
 }
-bs_status bs_engine_set_launch(bs_engine* e, int32_t warps_per_block, int32_t blocks_per_sm, int32_t stage) {
+bs_status bs_engine_set_launch(bs_engine* e, int32_t warps_per_block, int32_t blocks_per_sm, int32_t stage,
+                               int32_t tile_width) {
   return guarded([&] {
     NEED(e);
-    if (warps_per_block != 0 && (warps_per_block < 1 || warps_per_block > 4)) {
-      throw std::invalid_argument("warps per block must lie in [1, 4]");
+    int lw = 0;
+    if (tile_width != 0) {
+      while ((1 << lw) < tile_width) ++lw;
+      if ((1 << lw) != tile_width) throw std::invalid_argument("tile width must be 4, 8, 16 or 32");
     }
-    if (blocks_per_sm < 0) throw std::invalid_argument("blocks per SM must be >= 0");
-    if (stage != 0 && stage != 16 && stage != 32) throw std::invalid_argument("staging depth must be 0, 16 or 32");
-    e->warps_per_block = warps_per_block == 0 ? 4 : warps_per_block;
-    e->blocks_per_sm = blocks_per_sm;
-    e->stage = stage;
+    e->set_launch(warps_per_block, blocks_per_sm, stage, lw);
+  });
+}
+bs_status bs_engine_get_launch(const bs_engine* e, int32_t out[4]) {
+  return guarded([&] {
+    NEED(e);
+    NEED(out);
+    out[0] = e->warps_per_block;
+    out[1] = e->blocks_per_sm;
+    out[2] = e->stage;
+    out[3] = 1 << e->tile_lw;
+  });
+}
+bs_status bs_engine_set_graph(bs_engine* e, int32_t on) {
+  return guarded([&] {
+    NEED(e);
+    e->use_graph = on != 0;
+    if (!e->use_graph) e->release_graph();
+  });
+}
+bs_status bs_engine_autotune(bs_engine* e, int32_t windows, void* stream, double* rows, size_t cap, size_t* n) {
+  return guarded([&] {
+    NEED(e);
+    NEED(n);
+    const auto r = e->autotune(windows, static_cast<cudaStream_t>(stream));
+    *n = r.size();
+    for (size_t i = 0; i < r.size() && i < cap && rows; ++i) {
+      rows[4 * i + 0] = static_cast<double>(1 << static_cast<int>(r[i][0]));
+      rows[4 * i + 1] = r[i][1];
+      rows[4 * i + 2] = r[i][2];
+      rows[4 * i + 3] = r[i][3];
+    }
   });
 }
 bs_status bs_engine_last_ms(const bs_engine* e, double* ms) {
@@ -1612,10 +1790,10 @@ bs_status bs_mlp_gradient(bs_mlp* m, const uint16_t* x, const float* y, size_t n
   });
 }
 bs_status bs_mlp_train(bs_mlp* m, const uint16_t* x, const float* y, size_t n, int32_t steps, int32_t batch, float lr,
-                       uint64_t seed, float* losses, void* stream) {
+                       float tau, uint64_t seed, float* losses, void* stream) {
   return guarded([&] {
     NEED(m);
-    m->train(x, y, n, steps, batch, lr, seed, losses, stream ? static_cast<cudaStream_t>(stream) : m->own);
+    m->train(x, y, n, steps, batch, lr, tau, seed, losses, stream ? static_cast<cudaStream_t>(stream) : m->own);
   });
 }
 bs_status bs_trace_pairs(const bs_field* field, const bs_sample_rules* rules, int64_t t0_ns, int32_t windows,

@@ -69,9 +69,32 @@ class Engine:
         _lib.check(_lib.lib().bs_engine_run(self._h, int(windows), stream, C.byref(s), C.byref(e)))
         return s.value, e.value
 
-    def set_launch(self, warps_per_block: int = 0, blocks_per_sm: int = 0, stage: int = 0) -> None:
-        """Launch shape of the persistent grid and the staging depth (0, 16 or 32)."""
-        _lib.check(_lib.lib().bs_engine_set_launch(self._h, int(warps_per_block), int(blocks_per_sm), int(stage)))
+    def set_launch(self, warps_per_block: int = 0, blocks_per_sm: int = 0, stage: int = 0,
+                   tile_width: int = 0) -> None:
+        """Launch shape of the persistent grid, the staging depth (0, 16 or 32) and the tile width (4, 8, 16 or 32
+        px; the tile is 32 / width px high)."""
+        _lib.check(_lib.lib().bs_engine_set_launch(self._h, int(warps_per_block), int(blocks_per_sm), int(stage),
+                                                   int(tile_width)))
+
+    @property
+    def launch(self) -> dict:
+        out = np.zeros(4, np.int32)
+        _lib.check(_lib.lib().bs_engine_get_launch(self._h, out.ctypes.data))
+        return {"warps_per_block": int(out[0]), "blocks_per_sm": int(out[1]), "stage": int(out[2]),
+                "tile_width": int(out[3])}
+
+    def set_graph(self, on: bool) -> None:
+        """Each run as one CUDA graph launch (default) or as separate stream operations."""
+        _lib.check(_lib.lib().bs_engine_set_graph(self._h, 1 if on else 0))
+
+    def autotune(self, windows: int = 8, stream: int | None = None) -> list[dict]:
+        """Times trial steps of `windows` windows for each candidate launch shape (the models keep their state) and
+        keeps the fastest; returns the candidates with their kernel ms."""
+        rows = np.zeros((64, 4))
+        n = C.c_size_t()
+        _lib.check(_lib.lib().bs_engine_autotune(self._h, int(windows), stream, rows.ctypes.data, 64, C.byref(n)))
+        return [{"tile_width": int(r[0]), "warps_per_block": int(r[1]), "stage": int(r[2]), "ms": float(r[3])}
+                for r in rows[:n.value]]
 
     @property
     def last_ms(self) -> float:

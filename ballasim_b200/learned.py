@@ -121,13 +121,16 @@ class StepMLP:
                                               torch.cuda.current_stream().cuda_stream))
         return g, loss.value
 
-    def train(self, x, y, steps: int, batch: int = 8192, lr: float = 1e-3, seed: int = 0) -> np.ndarray:
-        """`steps` Adam steps on batches drawn with replacement; returns every step's batch loss."""
+    def train(self, x, y, steps: int, batch: int = 8192, lr: float = 1e-3, seed: int = 0,
+              tau: float = 0.5) -> np.ndarray:
+        """`steps` Adam steps on batches drawn with replacement, on the expectile loss of weight tau (0.5: mean
+        squared error; below 0.5 an over-long prediction costs more than a short one); returns every step's batch
+        loss."""
         torch = _torch()
         _check_pairs(x, y)
         losses = np.zeros(int(steps), np.float32)
         _lib.check(_lib.lib().bs_mlp_train(self._h, _ptr(x), _ptr(y), x.shape[0], int(steps), int(batch),
-                                           float(lr), int(seed), losses.ctypes.data,
+                                           float(lr), float(tau), int(seed), losses.ctypes.data,
                                            torch.cuda.current_stream().cuda_stream))
         return losses
 
@@ -144,8 +147,9 @@ class StepMLP:
 def trace_pairs(field: Field, rules, windows: int, *, stride: int = 1, eps: float = 1e-4, seed: int = 0,
                 t0_ns: int = 0, capacity: int | None = None, keys: bool = False):
     """(x, y, keys) training pairs from the plain sampler over `windows` windows of `field` (rules: a
-    workloads.Rules); every stride-th pixel walks its runs. capacity defaults to 3 pairs per walked pixel and
-    window and is raised and the walk redone when it is not enough."""
+    workloads.Rules); every stride-th pixel walks its runs. The pairs come back in (pixel, window, step) order, so
+    that a dataset (and training on it) is reproducible. capacity defaults to 3 pairs per walked pixel and window
+    and is raised and the walk redone when it is not enough."""
     torch = _torch()
     fs = field_struct(field)
     rs = _lib.SampleRules(rules.tol, rules.dark, 1, 1, rules.max_refine_levels, rules.min_dt_ns, rules.l_min,
@@ -155,7 +159,7 @@ def trace_pairs(field: Field, rules, windows: int, *, stride: int = 1, eps: floa
     while True:
         x = torch.empty((cap, 16), dtype=torch.uint16, device="cuda")
         y = torch.empty(cap, dtype=torch.float32, device="cuda")
-        k = torch.empty(cap, dtype=torch.uint64, device="cuda") if keys else None
+        k = torch.empty(cap, dtype=torch.uint64, device="cuda")
         n_out, total = C.c_size_t(), C.c_size_t()
         _lib.check(_lib.lib().bs_trace_pairs(C.byref(fs), C.byref(rs), int(t0_ns), int(windows), int(stride),
                                              float(eps), int(seed), _ptr(x), _ptr(y), _ptr(k), cap,
@@ -163,7 +167,11 @@ def trace_pairs(field: Field, rules, windows: int, *, stride: int = 1, eps: floa
                                              torch.cuda.current_stream().cuda_stream))
         if total.value <= cap:
             n = n_out.value
-            return x[:n], y[:n], (k[:n] if keys else None)
+            order = torch.argsort(k[:n].view(torch.int64), stable=True)  # keys < 2^63
+            x = x[:n].view(torch.int16).index_select(0, order).view(torch.uint16)
+            y = y[:n].index_select(0, order)
+            k = k[:n].view(torch.int64).index_select(0, order).view(torch.uint64)
+            return x, y, (k if keys else None)
         if capacity is not None:
             raise MemoryError(f"trace_pairs: {total.value} pairs exceed the capacity {cap}")
         cap = total.value
@@ -218,7 +226,7 @@ def renders_and_events(workload, proposal=None, margin: float = 0.25):
     return (samples - workload.windows * px) / px, m.take_events(), eng.last_ms
 
 
-MARGINS = (0.0, 0.1, 0.2, 0.25, 0.3, 0.35, 0.45, 0.6, 0.8, 1.0)
+MARGINS = tuple(round(0.05 * i, 2) for i in range(21))  # 0.0 .. 1.0
 
 
 def calibrate_margin(net: StepMLP, validation, *, target_median_ns: float = 8000.0, max_count_diff: float = 0.005,

@@ -141,8 +141,13 @@ def run_ours(args, rank: int, world: int) -> dict | None:
               for s in wl.sensors]
     eng = Engine([(m, s.field) for m, s in zip(models, wl.sensors)], tol=r.tol, dark=r.dark, min_dt_ns=r.min_dt_ns,
                  max_refine_levels=r.max_refine_levels, l_min=r.l_min, l_max=r.l_max)
-    if args.warps or args.blocks_per_sm or args.stage:
-        eng.set_launch(args.warps, args.blocks_per_sm, args.stage)
+    if args.warps or args.blocks_per_sm or args.stage or args.tile_width:
+        eng.set_launch(args.warps, args.blocks_per_sm, args.stage, args.tile_width)
+    eng.set_graph(not args.no_graph)
+    tuned = None
+    if not (args.no_autotune or args.warps or args.stage or args.tile_width):
+        eng.start(0, torch.cuda.current_stream().cuda_stream)
+        tuned = eng.autotune(min(8, wl.windows), torch.cuda.current_stream().cuda_stream)
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
@@ -232,7 +237,9 @@ def run_ours(args, rank: int, world: int) -> dict | None:
                    "events_per_step": int(per_step_events), "l2": "flushed between steps (256 MiB write)",
                    "sampler": {"tol": r.tol, "min_dt_ns": r.min_dt_ns, "max_refine_levels": r.max_refine_levels,
                                "levels": [r.l_min, r.l_max]},
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": f"replicas x{world}",
+                   "launch": {**eng.launch, "autotuned": tuned is not None, "cuda_graph": not args.no_graph,
+                              "threads_per_pixel": 1}},
         "gpu_launches": 3 * args.steps,
         "clocks": {k: v for k, v in clk.summary().items() if k != "samples"},
         "e2e": {"value": samples_all / float(e2e_s[0]) if e2e_times else None, "unit": "pixel-samples/s", "h2d_bytes_per_step": h2d,
@@ -249,11 +256,12 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     return out
 
 
-def learned_comparison(train_stride: int = 4, steps: int = 9000) -> dict:
-    """The learned step proposal against the plain sampler (BASELINE's learned configuration): the network is
-    trained on the GPU on (history, step) pairs of the plain sampler over a training-seed 1280 x 720 field of
-    blobs_1280x720's laws (every train_stride-th pixel, 1.0 s), its margin calibrated on a validation seed at
-    640 x 360, and both samplers run the held-out-seed 1280 x 720, 1.0 s field with noise."""
+def learned_comparison(train_stride: int = 4, steps: int = 9000, tau: float = 0.25) -> dict:
+    """The learned step proposal against the plain sampler: the network is trained on the GPU (Adam, lr 1e-3,
+    batch 8192, expectile weight tau) on (history, step) pairs of the plain sampler over a training-seed
+    1280 x 720 field of blobs_1280x720's laws (every train_stride-th pixel, 1.0 s), its margin calibrated on a
+    validation seed at 640 x 360 (median |dt| <= 8 us), and both samplers run the held-out-seed 1280 x 720, 1.0 s
+    field with noise."""
     import torch
 
     from ballasim_b200.learned import StepMLP, calibrate_margin, compare_events, renders_and_events, trace_pairs
@@ -265,7 +273,7 @@ def learned_comparison(train_stride: int = 4, steps: int = 9000) -> dict:
     t_pairs = time.perf_counter() - t0
     net = StepMLP(seed=0)
     t0 = time.perf_counter()
-    losses = net.train(x, y, steps=steps, batch=8192, lr=1e-3, seed=1)
+    losses = net.train(x, y, steps=steps, batch=8192, lr=1e-3, seed=1, tau=tau)
     t_train = time.perf_counter() - t0
     n_pairs = int(len(y))
     del x, y
@@ -279,7 +287,7 @@ def learned_comparison(train_stride: int = 4, steps: int = 9000) -> dict:
     return {
         "config": {"eval": f"{ev.name}, seed {W.LEARN_EVAL_SEED}, {ev.windows} windows ({sim_s:.4f} s)",
                    "train": f"blobs256_1280x720_noise seed {W.LEARN_TRAIN_SEEDS[0]}, every {train_stride}th pixel",
-                   "pairs": n_pairs, "adam_steps": steps, "batch": 8192, "lr": 1e-3,
+                   "pairs": n_pairs, "adam_steps": steps, "batch": 8192, "lr": 1e-3, "expectile_tau": tau,
                    "margin": margin, "margin_from": f"640x360 validation seed {W.LEARN_TRAIN_SEEDS[2]}"},
         "train_s": round(t_train, 3), "pairs_s": round(t_pairs, 3),
         "loss_first_last": [float(np.mean(losses[:10])), float(np.mean(losses[-200:]))],
@@ -358,6 +366,9 @@ def main():
     ap.add_argument("--warps", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--stage", type=int, default=0, help="engine staging depth: 0, 16 or 32")
+    ap.add_argument("--tile-width", type=int, default=0, help="engine tile width: 4, 8, 16 or 32 px")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the given (or default) launch shape")
+    ap.add_argument("--no-graph", action="store_true", help="launch each step's operations without a CUDA graph")
     ap.add_argument("--windows", type=int, default=0, help="run only the first windows (profiling a reduced case)")
     ap.add_argument("--profile", action="store_true", help="no e2e, CPU or learned legs (fewest launches, for ncu)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal comparison")

@@ -209,10 +209,23 @@ bs_status bs_engine_start_frames(bs_engine* e, int64_t t0_ns, const float* const
 /* Samples and senses `windows` whole windows of every sensor from the current model time; the events are kept in
  * each model (bs_model_take_events). *pixel_samples and *events receive the totals of the call. */
 bs_status bs_engine_run(bs_engine* e, int32_t windows, void* stream, uint64_t* pixel_samples, uint64_t* events);
-/* Launch shape: warps per block and blocks per SM of the persistent grid (0: the defaults), and the staging depth
- * (0: the sampler feeds the pixel model sample by sample; 16 or 32: per window each lane's samples are staged in
- * shared memory between a sampling phase and a sensing phase). */
-bs_status bs_engine_set_launch(bs_engine* e, int32_t warps_per_block, int32_t blocks_per_sm, int32_t stage);
+/* Launch shape: warps per block and blocks per SM of the persistent grid (0: the defaults, 4 and as many as fit),
+ * the staging depth (0: the sampler feeds the pixel model sample by sample; 16 or 32: per window each lane's samples
+ * are staged in shared memory between a sampling phase and a sensing phase) and the tile width in pixels (4, 8, 16
+ * or 32; the tile is 32 / width pixels high, one warp per tile; 0: 8). The learned engine runs 4 warps per block. */
+bs_status bs_engine_set_launch(bs_engine* e, int32_t warps_per_block, int32_t blocks_per_sm, int32_t stage,
+                               int32_t tile_width);
+/* The current launch shape: warps per block, blocks per SM, staging depth, tile width. */
+bs_status bs_engine_get_launch(const bs_engine* e, int32_t out[4]);
+/* Runs each step as a CUDA graph (on, the default) or as separate stream operations (off). The graph holds the
+ * counter resets, the descriptor and model-time uploads, the persistent kernel and the counter read-back; it is
+ * rebuilt when the window count, launch shape or proposal changes. */
+bs_status bs_engine_set_graph(bs_engine* e, int32_t on);
+/* The autotuner: times trial steps of `windows` windows from the current state for each candidate launch shape
+ * (tile width 4, 8, 16 x warps per block 2, 4 x staging depth 0, 16; the learned engine: tile widths) without
+ * moving the models, and keeps the fastest. rows (cap x 4 doubles: tile width, warps, stage, ms) receives the
+ * candidates tried, *n their number. */
+bs_status bs_engine_autotune(bs_engine* e, int32_t windows, void* stream, double* rows, size_t cap, size_t* n);
 /* Kernel time of the last bs_engine_run's launches (ms, CUDA events on its stream). */
 bs_status bs_engine_last_ms(const bs_engine* e, double* ms);
 
@@ -239,11 +252,12 @@ bs_status bs_mlp_forward(bs_mlp* m, const uint16_t* x, size_t n, float* y, void*
  * from the training kernels' forward and backward passes. */
 bs_status bs_mlp_gradient(bs_mlp* m, const uint16_t* x, const float* y, size_t n, double* grad, double* loss,
                           void* stream);
-/* `steps` Adam steps (lr, beta 0.9 / 0.999, eps 1e-8) on the same loss over batches of `batch` rows drawn with
- * replacement from the n pairs (Philox(seed), keyed by the step count); losses (host, may be NULL) gets every
- * step's batch loss. Runs from a CUDA graph of 32 steps. */
+/* `steps` Adam steps (lr, beta 0.9 / 0.999, eps 1e-8) over batches of `batch` rows drawn with replacement from the
+ * n pairs (Philox(seed), keyed by the step count) on the expectile loss sum_i w_i (MLP(x_i) - y_i)^2 / (2 batch),
+ * w_i = 2 tau where the net predicts below y_i and 2 (1 - tau) above (tau = 0.5: the mean squared error above);
+ * losses (host, may be NULL) gets every step's batch loss. Runs from a CUDA graph of 32 steps. */
 bs_status bs_mlp_train(bs_mlp* m, const uint16_t* x, const float* y, size_t n, int32_t steps, int32_t batch, float lr,
-                       uint64_t seed, float* losses, void* stream);
+                       float tau, uint64_t seed, float* losses, void* stream);
 /* Training pairs from the plain sampler: windows [0, windows) of the field from t0 are sampled with the rules
  * (every pixel, levels by the field's rule) and every stride-th pixel walks its runs. At each walk point the
  * target is the longest aligned power-of-two step whose chord stays within eps of the run's log irradiance at every

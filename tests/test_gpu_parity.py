@@ -240,12 +240,13 @@ def test_midpoint_test_matches_numpy_fp32(cuda_lib):
     assert np.array_equal(t.exceeds(a, m, b), want > np.float32(0.01))
 
 
-@pytest.mark.parametrize("stage", [0, 16, 32])
+@pytest.mark.parametrize("stage,tile,graph", [(0, 8, True), (16, 8, True), (32, 8, True), (0, 4, True),
+                                              (16, 16, True), (0, 32, True), (0, 8, False)])
 @pytest.mark.parametrize("case", ["edge", "blobs", "noise"])
-def test_engine_equals_the_oracle_chain(cuda_lib, case, stage):
+def test_engine_equals_the_oracle_chain(cuda_lib, case, stage, tile, graph):
     """The fused engine (sampler and pixel model on one thread, all windows in one launch; streamed, or staged in
-    shared memory per window) gives the oracle chain's events (sample_window, then advance, per window) bit for
-    bit."""
+    shared memory per window; any tile shape; from a CUDA graph or not) gives the oracle chain's events
+    (sample_window, then advance, per window) bit for bit."""
     from ballasim_b200.engine import Engine
     from ballasim_b200.sensor import SensorModel
     from oracle.oracle import simulate_port
@@ -261,7 +262,8 @@ def test_engine_equals_the_oracle_chain(cuda_lib, case, stage):
     r = wl.rules
     eng = Engine([(m, spec.field)], tol=r.tol, dark=r.dark, min_dt_ns=r.min_dt_ns,
                  max_refine_levels=r.max_refine_levels, l_min=r.l_min, l_max=r.l_max)
-    eng.set_launch(0, 0, stage)
+    eng.set_launch(0, 0, stage, tile)
+    eng.set_graph(graph)
     eng.start(0)
     samples, parts = 0, []
     for chunk in (5, wl.windows - 5):  # two calls: the state and carried samples cross the call boundary
@@ -274,3 +276,31 @@ def test_engine_equals_the_oracle_chain(cuda_lib, case, stage):
     assert len(ev["t_cross_ns"]) > 20
     if case == "noise":
         assert np.count_nonzero(ev["label"] == 1) > 5
+
+
+@pytest.mark.gpu
+def test_autotune_keeps_the_state_and_the_events(cuda_lib):
+    """The autotuner's trial steps leave the models as they were: the run after it gives the events of a run
+    without it, at whatever launch shape it picked."""
+    from ballasim_b200.engine import Engine
+    from ballasim_b200.sensor import SensorModel
+
+    wl = W.small("noise", 64, 40, 12)
+    spec, r = wl.sensors[0], wl.rules
+    out = []
+    for tune in (False, True):
+        m = SensorModel(resolve("ideal", spec.overrides), spec.width, spec.height, spec.seed, [{"type": "constant"}],
+                        spec.camera)
+        eng = Engine([(m, spec.field)], tol=r.tol, dark=r.dark, min_dt_ns=r.min_dt_ns,
+                     max_refine_levels=r.max_refine_levels, l_min=r.l_min, l_max=r.l_max)
+        eng.start(0)
+        if tune:
+            rows = eng.autotune(4)
+            assert len(rows) == 12 and all(x["ms"] > 0 for x in rows)
+            best = min(rows, key=lambda x: x["ms"])
+            assert eng.launch["tile_width"] == best["tile_width"] and eng.launch["stage"] == best["stage"]
+        s, e = eng.run(wl.windows)
+        out.append((s, e, m.take_events(with_pixel=True)))
+    assert out[0][0] == out[1][0] and out[0][1] == out[1][1]
+    for k in ("pixel", "t_cross_ns", "p", "label"):
+        assert np.array_equal(out[0][2][k], out[1][2][k])

@@ -177,17 +177,18 @@ def test_training_lowers_loss_and_is_deterministic(cuda_lib):
 @pytest.mark.gpu
 @pytest.mark.parametrize("stride", [1, 5])
 def test_trace_pairs_match_the_oracle(cuda_lib, oracle_port, stride):
+    import torch
+
     from ballasim_b200.learned import trace_pairs
 
     wl = W.small("blobs", 64, 48, 6, seed=11)
     f, r = wl.sensors[0].field, wl.rules
     x, y, k = trace_pairs(f, r, 6, stride=stride, eps=1e-4, seed=21, keys=True)
     xo, yo, ko = oracle_port.walk_pairs(f, r, 6, stride=stride, eps=1e-4, seed=21)
-    k = k.cpu().numpy().view(np.uint64) if hasattr(k, "cpu") else k
-    o = np.argsort(k, kind="stable")
-    assert np.array_equal(k[o], ko)
-    assert np.array_equal(y.cpu().numpy()[o], yo)
-    assert np.array_equal(x.cpu().numpy().view(np.uint16)[o], xo)
+    k = k.view(torch.int64).cpu().numpy().view(np.uint64)
+    assert np.array_equal(k, ko)  # already in (pixel, window, step) order
+    assert np.array_equal(y.cpu().numpy(), yo)
+    assert np.array_equal(x.cpu().numpy().view(np.uint16), xo)
 
 
 def _learned_engine_case(margin, mlp_seed, windows=5, w=48, h=32, seed=13, train=False):
@@ -269,8 +270,8 @@ def test_learned_engine_matches_the_oracle(cuda_lib, oracle_port, margin, traine
 
 @pytest.mark.gpu
 def test_trained_proposal_halves_the_renders(cuda_lib):
-    """Train on fields of two training seeds, calibrate the margin on a third (validation), evaluate on a held-out
-    seed: C3's laws and blob density at 320 x 180, 1 s with noise. Renders per pixel at least 2x fewer than the
+    """Train on fields of three training seeds (expectile tau 0.25), calibrate the margin on a fourth (validation,
+    median |dt| <= 8 us), evaluate on a held-out seed: C3's laws and blob density at 320 x 180, 1 s with noise. Renders per pixel at least 2x fewer than the
     plain sampler's, event count within 1 %, median |dt| of matched signal events <= 10 us."""
     import torch
 
@@ -278,16 +279,16 @@ def test_trained_proposal_halves_the_renders(cuda_lib):
 
     w, h = 320, 180
     xs, ys = [], []
-    for s in W.LEARN_TRAIN_SEEDS[:2]:
+    for s in (W.LEARN_TRAIN_SEEDS[0], W.LEARN_TRAIN_SEEDS[1], W.LEARN_TRAIN_SEEDS[3]):
         tw = W.blobs_noise(w, h, s)
         x, y, _ = trace_pairs(tw.sensors[0].field, tw.rules, tw.windows, stride=1, seed=s)
         xs.append(x)
         ys.append(y)
     x, y = torch.cat(xs), torch.cat(ys)
     net = StepMLP(seed=0)
-    losses = net.train(x, y, steps=6000, batch=8192, lr=1e-3, seed=1)
+    losses = net.train(x, y, steps=9000, batch=8192, lr=1e-3, seed=1, tau=0.25)
     assert losses[-100:].mean() < 0.2 * losses[:10].mean()
-    margin, table = calibrate_margin(net, W.blobs_noise(w, h, W.LEARN_TRAIN_SEEDS[2]))
+    margin, table = calibrate_margin(net, W.blobs_noise(w, h, W.LEARN_TRAIN_SEEDS[2]), target_median_ns=8000.0)
     ev = W.blobs_noise(w, h, W.LEARN_EVAL_SEED)
     plain_r, plain_ev, _ = renders_and_events(ev)
     learned_r, learned_ev, _ = renders_and_events(ev, net, margin)
