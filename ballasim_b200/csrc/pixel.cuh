@@ -7,8 +7,10 @@
 // v0 + (v1 - v0) ((t - t0) / (t1 - t0)) (fp32, that operation order) and after the last sample it is held;
 // the photocurrent is I = I_dk + s v (s = illuminance_scale x gain); x(t) = ln(I / i_scale).
 // Comparator: Delta(t) = (x - s3_ref) + (0 - n3_ref) + (leak (t - t_ref) 1e-9 + dr_ref) fires at the first
-// integer ns of each piece where Delta >= theta_on or <= -theta_off, found by the time-ordered depth-first
-// bisection with the reference's exclusion test; pieces never cross a multiple of 2^23 ns.
+// integer ns of each piece where Delta >= theta_on or <= -theta_off, found by the reference's time-ordered
+// depth-first bisection, whose nodes are pruned here by an exact (margin-free) bound instead of the reference's
+// margins: the same first crossing, far fewer nodes where Delta lingers near a level; pieces never cross a
+// multiple of 2^23 ns.
 //
 // Noise (this project's, no reference counterpart): two Poisson chains of candidate times per pixel, keyed by
 // (pixel, candidate number) in Philox streams 0x0080 (shot) and 0x0081 (background activity). Candidate n's
@@ -163,35 +165,25 @@ struct PixelProc {
     }
   }
 
-  // Can Delta reach a level at an integer of (a, c]? Constant light: curvature 0 and no range cap
-  // (instant_may_fire with instant_curvature's linear case).
-  BS_COLD bool may_fire(int64_t a, int64_t cc, float Ia, float Ic) const {
-    const float eps = 0x1p-23f;
-    float hi = maxr(Ia, Ic), lo = minr(Ia, Ic);
-    const float margin = 64.0f * eps * (hi + 2.0f * 0.0f);
-    if (m.leak == 0.0f) {  // hi - lo >= 0.5 * (h^2 * 0): the extremes are at the endpoints
-      const float D = delta(cc, log_ratio(Ic));
-      return D >= m.theta_on || D <= -m.theta_off;
-    }
-    if (Ic >= Ia) return delta(cc, log_ratio(Ic)) >= m.theta_on;  // non-decreasing I, and leak >= 0
-    hi = minr(hi + 0.125f * 0.0f, kInfF) + margin;
-    lo = maxr(lo - 0.125f * 0.0f, m.dark) - margin;
+  // Can Delta reach a level at an integer of (a, c], given x at both ends? Exact for constant light: I(t) is a
+  // monotone fp32 interpolation between the samples, I / i_scale and this build's log_f are monotone (log_f is
+  // checked over every positive float), the leak term is non-decreasing in t (leak >= 0), and fp32 additions round
+  // monotonically; so Delta over (a, c] lies between its value formed from min(x) and dl(a) and its value formed
+  // from max(x) and dl(c), with no margin. It answers "no" only where no integer of (a, c] fires, and so prunes
+  // at least what instant_may_fire prunes; the time-ordered search then finds the same first crossing.
+  BS_HD bool may_fire_exact(int64_t a, int64_t cc, float xa, float xc) const {
+    const float dn = 0.0f - s.n3_ref;
     const float dl_a = m.leak * since_ref(a, s.t_ref) + s.dr_ref;
     const float dl_c = m.leak * since_ref(cc, s.t_ref) + s.dr_ref;
-    const float base = 0.0f - s.n3_ref - s.s3_ref;
-    const float x_hi = log_ratio(hi);
-    if (x_hi + base + dl_c + 16.0f * eps * (1.0f + fabs_f(x_hi) + fabs_f(s.s3_ref) + fabs_f(dl_c)) >= m.theta_on) {
-      return true;
-    }
-    if (!(lo > 0.0f)) return true;
-    const float x_lo = log_ratio(lo);
-    return x_lo + base + dl_a - 16.0f * eps * (1.0f + fabs_f(x_lo) + fabs_f(s.s3_ref) + fabs_f(dl_a)) <= -m.theta_off;
+    const float hi = ((maxr(xa, xc) - s.s3_ref) + dn) + dl_c;
+    const float lo = ((minr(xa, xc) - s.s3_ref) + dn) + dl_a;
+    return hi >= m.theta_on || lo <= -m.theta_off;
   }
 
-  // The first integer t in [lo, hi) where Delta fires (instant_search): found, polarity, time and x(t).
+  // The first integer t in [lo, hi) where Delta fires (instant_search's time-ordered depth-first bisection,
+  // pixel.h:1886-1916, with the exact node test above; each node carries x at its ends, one log per split).
   BS_COLD bool search(const Segment& g, int64_t lo, int64_t hi, int64_t& t_hit, bool& on, float& x_hit) {
-    const float I_lo = current(g, lo);
-    float x = log_ratio(I_lo);
+    float x = log_ratio(current(g, lo));
     float D = delta(lo, x);
     if (D >= m.theta_on || D <= -m.theta_off) {
       t_hit = lo;
@@ -201,41 +193,39 @@ struct PixelProc {
     }
     if (hi - lo == 1) return false;
     int64_t sa[32], sc[32];
-    float sIa[32], sIc[32];
-    int sp = 0;
+    float sxa[32], sxc[32];
+    int sp = 1;
     sa[0] = lo;
     sc[0] = hi - 1;
-    sIa[0] = I_lo;
-    sIc[0] = current(g, hi - 1);
-    sp = 1;
+    sxa[0] = x;
+    sxc[0] = log_ratio(current(g, hi - 1));
     while (sp > 0) {
       --sp;
       const int64_t a = sa[sp], cc = sc[sp];
-      const float Ia = sIa[sp], Ic = sIc[sp];
+      const float xa = sxa[sp], xc = sxc[sp];
       if (cc - a == 1) {
-        x = log_ratio(Ic);
-        D = delta(cc, x);
+        D = delta(cc, xc);
         if (D >= m.theta_on || D <= -m.theta_off) {
           t_hit = cc;
           on = D >= m.theta_on;
-          x_hit = x;
+          x_hit = xc;
           return true;
         }
         continue;
       }
       ++c.leaves;
-      if (!may_fire(a, cc, Ia, Ic)) continue;
+      if (!may_fire_exact(a, cc, xa, xc)) continue;
       const int64_t mid = a + (cc - a) / 2;
-      const float Im = current(g, mid);
+      const float xm = log_ratio(current(g, mid));
       sa[sp] = mid;
       sc[sp] = cc;
-      sIa[sp] = Im;
-      sIc[sp] = Ic;
+      sxa[sp] = xm;
+      sxc[sp] = xc;
       ++sp;
       sa[sp] = a;
       sc[sp] = mid;
-      sIa[sp] = Ia;
-      sIc[sp] = Im;
+      sxa[sp] = xa;
+      sxc[sp] = xm;
       ++sp;
     }
     return false;
