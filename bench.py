@@ -39,6 +39,9 @@ WORKLOADS = {
 }
 METRIC = "pixel-samples/s"
 L2_BYTES = 126 * 1024 * 1024
+# DRAM bytes (read + write) of one engine_kernel launch, from an ncu capture of this bench's own command
+# (profiles/engine_kernel_blobs16_346x260.md), per workload; other workloads report null.
+NCU_TRAFFIC_PER_LAUNCH = {"blobs16_346x260": 29.10e6 + 49.57e6}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -246,7 +249,7 @@ def run_ours(args, rank: int, world: int) -> dict | None:
                 "d2h_bytes_per_step": d2h},
         "roofline": {"kernel": "engine_kernel (sampler + pixel model fused, runs kept on chip)", "bound": "hbm",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "peak_kind": hbm_kind, "traffic": None, "algorithmic_bytes_per_launch": alg,
+                     "peak_kind": hbm_kind, "traffic": NCU_TRAFFIC_PER_LAUNCH.get(wl.name), "algorithmic_bytes_per_launch": alg,
                      "avg_launch_ms": kms, "runs_write_avoided_bytes": int(per_step_samples) * 12},
     }
     if world == 1 and not (args.no_cpu_baseline or args.profile):
