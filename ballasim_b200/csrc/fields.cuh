@@ -69,13 +69,23 @@ BS_HD float field_eval_all(const FieldDev& f, uint32_t x, uint32_t y, int64_t t_
   return e;
 }
 
-// E(x, y, t) over a warp's candidate list (bitwise field_eval_all when the list holds every blob in reach).
-BS_HD float field_eval(const FieldDev& f, const BlobList& l, uint32_t x, uint32_t y, int64_t t_ns) {
+// E(x, y, t) over a warp's candidate list (bitwise field_eval_all when the list holds every blob in reach). One
+// out-of-line copy serves the sampler's render sites (a smaller kernel for the instruction cache); blobs go in
+// pairs whose exp chains are independent, summed in list order.
+static __host__ __device__ __noinline__ float field_eval(const FieldDev& f, const BlobList& l, uint32_t x, uint32_t y,
+                                                         int64_t t_ns) {
   if (f.kind != kFieldBlobs || l.idx == nullptr) return field_eval_all(f, x, y, t_ns);
   const float ts = t_seconds(t_ns);
   const float xc = static_cast<float>(x) + 0.5f, yc = static_cast<float>(y) + 0.5f;
   float e = f.base;
-  for (int32_t i = 0; i < l.n; ++i) e = e + blob_term(f.blobs + static_cast<size_t>(l.idx[i]) * kBlobWords, xc, yc, ts);
+  int32_t i = 0;
+  for (; i + 1 < l.n; i += 2) {
+    const float t0 = blob_term(f.blobs + static_cast<size_t>(l.idx[i]) * kBlobWords, xc, yc, ts);
+    const float t1 = blob_term(f.blobs + static_cast<size_t>(l.idx[i + 1]) * kBlobWords, xc, yc, ts);
+    e = e + t0;
+    e = e + t1;
+  }
+  if (i < l.n) e = e + blob_term(f.blobs + static_cast<size_t>(l.idx[i]) * kBlobWords, xc, yc, ts);
   return e;
 }
 
