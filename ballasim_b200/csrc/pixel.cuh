@@ -231,8 +231,19 @@ struct PixelProc {
     return false;
   }
 
-  // Drops the earliest noise candidate (refractory or dead time) or tests and fires it; advances its chain.
-  BS_COLD void noise_candidate(const Segment& g, int64_t tn, bool blind) {
+  // Is the earliest noise candidate (at tn) accepted by thinning (u1 < lambda(t) / lambda_max)? on: its polarity,
+  // I: the photocurrent at tn. No side effects.
+  BS_COLD bool candidate_accepted(const Segment& g, int64_t tn, bool& on, float& I) const {
+    const bool shot = s.t_shot <= s.t_ba;
+    const U4 w = draw(k.seed, shot ? kPurposeShot : kPurposeBackground, k.camera, pixel, shot ? s.n_shot : s.n_ba);
+    I = current(g, tn);
+    const double accept = shot ? sqrt(static_cast<double>(m.dark) / static_cast<double>(I)) : 1.0;
+    on = (w.v[2] & 1u) != 0u;
+    return open_uniform_d(w.v[1]) < accept;
+  }
+
+  // Moves the earliest candidate's chain (the one at tn) on to its next candidate.
+  BS_COLD void advance_chain(int64_t tn) {
     ++c.noise_candidates;
     const bool shot = s.t_shot <= s.t_ba;
     const uint32_t purpose = shot ? kPurposeShot : kPurposeBackground;
@@ -246,11 +257,15 @@ struct PixelProc {
       s.n_ba = n + 1;
       s.t_ba = next;
     }
-    if (blind) return;
-    const U4 w = draw(k.seed, purpose, k.camera, pixel, n);
-    const float I = current(g, tn);
-    const double accept = shot ? sqrt(static_cast<double>(m.dark) / static_cast<double>(I)) : 1.0;
-    if (open_uniform_d(w.v[1]) < accept) fire(tn, (w.v[2] & 1u) != 0u, log_ratio(I), kLabelNoise);
+  }
+
+  // Drops the earliest noise candidate (refractory or dead time) or tests and fires it; advances its chain.
+  BS_COLD void noise_candidate(const Segment& g, int64_t tn, bool blind) {
+    bool on = false;
+    float I = 0.0f;
+    const bool fires = !blind && candidate_accepted(g, tn, on, I);
+    advance_chain(tn);
+    if (fires) fire(tn, on, log_ratio(I), kLabelNoise);
   }
 
   // One piece [t, e) inside segment g (advance_instant's inner loop), with the noise candidates it holds.
@@ -307,19 +322,44 @@ struct PixelProc {
 
   // A whole segment g = [t0, t1) that is one piece (no multiple of 2^23 ns inside), with x0 = x(t0) and
   // x1 = x(t1) (the next segment's start, x_at_sample(g.v1)). Bitwise piece(g, t0, t1): where the pixel is not
-  // blind, nothing is pending before t0 and no noise candidate falls inside, Delta(t0) is tested exactly as the
-  // reference does; then the node (t0, t1 - 1] that the reference tests with instant_may_fire is excluded here
-  // when bounds from x0 and x1 prove that test false, and only otherwise is the reference's search run.
+  // blind and nothing is pending before t0, Delta(t0) is tested exactly as the reference does; then the node
+  // (t0, t1 - 1] is excluded here when bounds from x0 and x1 prove that no integer of it fires, and only otherwise
+  // is the reference's search run.
   //
-  // The bounds: I(t1 - 1) interpolates between I(t0) and I(t1) (fp32 rounding keeps it within two ulp of that
-  // range, which is monotone in v), ln is monotone, the leak term leak (t - t_ref) 1e-9 + dr_ref is non-decreasing
-  // in t (leak >= 0), and fp32 sums round monotonically; kSlack covers the log's error, the ulps of I and the
-  // exclusion test's own 16-64 eps margins.
+  // Noise candidates inside the segment: when Delta(t0) and the whole node are excluded, no crossing can occur in
+  // [t0, t1) while the reference stays put, so the candidates are the only events possible. A rejected candidate
+  // changes nothing but its chain; the first accepted one hands over to the reference's loop at its time (which
+  // handles a candidate before the comparator at the same ns), with the search known clear up to it.
   BS_HD void segment_fast(const Segment& g, float x0, float x1) {
     const int64_t t0 = g.t0, e = g.t1;
-    const int64_t tn = k.noise ? mini(s.t_shot, s.t_ba) : kForever;
-    if (s.blind_until != kNotBlind || s.t_search > t0 || tn < e) {
+    if (s.blind_until != kNotBlind || s.t_search > t0) {
       piece(g, t0, e);
+      return;
+    }
+    int64_t tn = k.noise ? mini(s.t_shot, s.t_ba) : kForever;
+    if (tn < e) {
+      if (tn < t0) {  // a candidate left before the segment (none is, by construction): the reference's loop
+        piece(g, t0, e);
+        return;
+      }
+      const float D0 = delta(t0, x0);
+      if (D0 >= m.theta_on || D0 <= -m.theta_off || (e - t0 > 1 && !excluded(g, t0, e, x0, x1))) {
+        piece(g, t0, e);
+        return;
+      }
+      ++c.pieces;
+      do {
+        bool on;
+        float I;
+        if (candidate_accepted(g, tn, on, I)) {
+          s.t_search = maxi(s.t_search, tn);
+          piece_rest(g, tn, e);
+          return;
+        }
+        advance_chain(tn);
+        tn = mini(s.t_shot, s.t_ba);
+      } while (tn < e);
+      s.t_search = maxi(s.t_search, e);
       return;
     }
     ++c.pieces;
@@ -343,6 +383,16 @@ struct PixelProc {
 
   // True when instant_may_fire(t0, t1 - 1, I(t0), I(t1 - 1)) and Delta(t1 - 1) are provably both false.
   BS_HD bool excluded(const Segment& g, int64_t t0, int64_t e, float x0, float x1) const {
+    // The interpolation reaches v1 exactly (v0 + (v1 - v0) == v1 in fp32): I over [t0, t1] then lies between its
+    // end values, and the exact bounds of may_fire_exact hold with x0, x1 (dl(t1) >= dl(t1 - 1)).
+    if (g.v0 + (g.v1 - g.v0) == g.v1) {
+      const float dn = 0.0f - s.n3_ref;
+      const float dl0 = m.leak * since_ref(t0, s.t_ref) + s.dr_ref;
+      const float dl1 = m.leak * since_ref(e, s.t_ref) + s.dr_ref;
+      const float hi = ((maxr(x0, x1) - s.s3_ref) + dn) + dl1;
+      const float lo = ((minr(x0, x1) - s.s3_ref) + dn) + dl0;
+      return hi < m.theta_on && lo > -m.theta_off;
+    }
     const float eps = 0x1p-23f;
     const float xa = minr(x0, x1), xb = maxr(x0, x1);
     const float dl0 = m.leak * since_ref(t0, s.t_ref) + s.dr_ref;

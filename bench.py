@@ -30,6 +30,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 from ballasim_b200 import workloads as W  # noqa: E402
+from ballasim_b200.replicas import reduce_max, reduce_step, replica  # noqa: E402
 
 WORKLOADS = {
     "blobs_346x260": W.blobs_346x260,
@@ -51,21 +52,6 @@ def measured_hbm() -> tuple[float, str]:
         return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
     except Exception:
         return FALLBACK_HBM_GBS, "fallback"
-
-
-def replica(wl: W.Workload, rank: int) -> W.Workload:
-    """Rank r's replica: the same sizes and laws, fields and maps drawn from seeds offset by r."""
-    if rank == 0:
-        return wl
-    from ballasim_b200 import fields as F
-
-    sensors = []
-    for s in wl.sensors:
-        seed = s.seed + 1000 * rank
-        f = (F.blobs(s.width, s.height, seed, s.field.n_blobs) if s.field.kind == F.KIND_BLOBS
-             else F.tanh_edge(s.width, s.height, seed))
-        sensors.append(W.SensorSpec(s.width, s.height, seed, s.camera, dict(s.overrides), f))
-    return W.Workload(wl.name, sensors, wl.windows, wl.rules)
 
 
 class Clocks:
@@ -182,15 +168,7 @@ def run_ours(args, rank: int, world: int) -> dict | None:
             dist.barrier()
     step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
     total_ms = float(sum(step_ms))
-    t = torch.tensor([total_ms, float(samples), float(events)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = t.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        total_ms_all, samples_all, events_all = float(mx[0]), float(sm[1]), float(sm[2])
-    else:
-        total_ms_all, samples_all, events_all = total_ms, float(samples), float(events)
+    total_ms_all, samples_all, events_all = reduce_step(total_ms, float(samples), float(events), world)
 
     # e2e through the public API with host buffers: the initial frames from pinned host memory in, every event out
     frames = [torch.from_numpy(field_frame(s.field, 0)).pin_memory().numpy() for s in wl.sensors]
@@ -208,9 +186,7 @@ def run_ours(args, rank: int, world: int) -> dict | None:
         if k >= args.warmup:
             e2e_times.append(time.perf_counter() - t0)
             d2h = n_ev * 32
-    e2e_s = torch.tensor([sum(e2e_times)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
+    e2e_s = reduce_max(sum(e2e_times), world)
     h2d = sum(int(f.nbytes) for f in frames)
 
     if rank != 0:
@@ -245,7 +221,7 @@ def run_ours(args, rank: int, world: int) -> dict | None:
                               "threads_per_pixel": 1}},
         "gpu_launches": 3 * args.steps,
         "clocks": {k: v for k, v in clk.summary().items() if k != "samples"},
-        "e2e": {"value": samples_all / float(e2e_s[0]) if e2e_times else None, "unit": "pixel-samples/s", "h2d_bytes_per_step": h2d,
+        "e2e": {"value": samples_all / e2e_s if e2e_times else None, "unit": "pixel-samples/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "roofline": {"kernel": "engine_kernel (sampler + pixel model fused, runs kept on chip)", "bound": "hbm",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
