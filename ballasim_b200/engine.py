@@ -46,9 +46,12 @@ class Engine:
 
     def __del__(self):
         h = getattr(self, "_h", None)
+        self._h = None
         if h:
-            _lib.lib().bs_engine_destroy(h)
-            self._h = None
+            try:
+                _lib.lib().bs_engine_destroy(h)
+            except Exception:  # interpreter shutdown
+                pass
 
     def start(self, t0_ns: int = 0, stream: int | None = None, frames=None) -> None:
         """Initializes every model at t0: from its field rendered on the device, or from host frames (one float32

@@ -75,9 +75,12 @@ class StepMLP:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h and _lib is not None and getattr(_lib, "_lib", None) is not None:
-            _lib.lib().bs_mlp_destroy(h)
         self._h = None
+        if h:
+            try:
+                _lib.lib().bs_mlp_destroy(h)
+            except Exception:  # interpreter shutdown
+                pass
 
     @property
     def handle(self) -> C.c_void_p:

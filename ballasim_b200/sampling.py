@@ -137,9 +137,13 @@ class _Sampler:
         self.h = h
 
     def __del__(self):
-        if getattr(self, "h", None):
-            _lib.lib().bs_sampler_destroy(self.h)
-            self.h = None
+        h = getattr(self, "h", None)
+        self.h = None
+        if h:
+            try:
+                _lib.lib().bs_sampler_destroy(h)
+            except Exception:  # interpreter shutdown
+                pass
 
 
 _samplers = _SamplerCache()

@@ -99,9 +99,12 @@ class SensorModel:
 
     def __del__(self):
         h = getattr(self, "_h", None)
+        self._h = None
         if h:
-            _lib.lib().bs_model_destroy(h)
-            self._h = None
+            try:
+                _lib.lib().bs_model_destroy(h)
+            except Exception:  # interpreter shutdown: the library (and the process) is going away
+                pass
 
     @property
     def handle(self):

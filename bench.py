@@ -42,7 +42,7 @@ METRIC = "pixel-samples/s"
 L2_BYTES = 126 * 1024 * 1024
 # DRAM bytes (read + write) of one engine_kernel launch, from an ncu capture of this bench's own command
 # (profiles/engine_kernel_blobs16_346x260.md), per workload; other workloads report null.
-NCU_TRAFFIC_PER_LAUNCH = {"blobs16_346x260": 29.10e6 + 49.57e6}
+NCU_TRAFFIC_PER_LAUNCH = {"blobs16_346x260": 29.39e6 + 49.19e6}
 FALLBACK_HBM_GBS = 6650.0
 
 
