@@ -141,6 +141,11 @@ int learned_engine_max_blocks_per_sm(int warps_per_block);
 // Resets the walk state of n pixels from their initial irradiance.
 void launch_learned_reset(LearnedSoA st, uint32_t n, const float* irr0, cudaStream_t stream);
 
+// ---- event output order (events.cu) ----
+// Sorts n device events by (t_cross, pixel) into out (device), using sort_events_scratch_bytes(n) bytes of scratch.
+size_t sort_events_scratch_bytes(uint32_t n);
+cudaError_t sort_events(const RawEvent* ev, uint32_t n, RawEvent* out, void* scratch, cudaStream_t stream);
+
 // ---- the MLP (learned.cu) ----
 // Training pairs from one window's plain runs (all n_pixels listed in order; t absolute): every stride-th pixel
 // walks its run; pairs are appended (x: 16 BF16 features, y: target, key: pixel << 32 | window << 11 | step).

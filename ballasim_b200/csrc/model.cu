@@ -466,17 +466,28 @@ struct Model {
     kept = download(events.p, last_events, own);
   }
 
-  std::vector<RawEvent> download(const RawEvent* dev, size_t count, cudaStream_t s) const {
-    std::vector<RawEvent> out(count);
+  // The events of a call, sorted by (t_cross, pixel) on the device (finish_events' order) and copied into pinned
+  // host memory; the pointer stays valid until the next download.
+  const RawEvent* download_pinned(const RawEvent* dev, size_t count, cudaStream_t s) const {
+    staged.ensure(count);
     if (count) {
-      CK(cudaMemcpyAsync(out.data(), dev, count * sizeof(RawEvent), cudaMemcpyDeviceToHost, s));
+      if (count > 0x7fffffffull) throw std::invalid_argument("too many events in one call");
+      const uint32_t n = static_cast<uint32_t>(count);
+      sorted.ensure(count);
+      sort_scratch.ensure(sort_events_scratch_bytes(n));
+      CK(sort_events(dev, n, sorted.p, sort_scratch.p, s));
+      CK(cudaMemcpyAsync(staged.p, sorted.p, count * sizeof(RawEvent), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
     }
-    std::sort(out.begin(), out.end(), [](const RawEvent& a, const RawEvent& b) {
-      return a.t_cross != b.t_cross ? a.t_cross < b.t_cross : a.pixel < b.pixel;
-    });
-    return out;
+    return staged.p;
   }
+  std::vector<RawEvent> download(const RawEvent* dev, size_t count, cudaStream_t s) const {
+    const RawEvent* p = download_pinned(dev, count, s);
+    return std::vector<RawEvent>(p, p + count);
+  }
+  mutable DevBuf<RawEvent> sorted;
+  mutable DevBuf<unsigned char> sort_scratch;
+  mutable PinBuf<RawEvent> staged;
 
   int64_t reported(int64_t t) const {
     const int64_t q = std::llround(p.readout_quantum_s * 1e9);
@@ -489,8 +500,9 @@ struct Model {
     return r + p.clock_offset_ns + std::llround(p.clock_drift_ppm * 1e-6 * static_cast<double>(r));
   }
 
-  void columns(const std::vector<RawEvent>& ev, bs_event_columns* o) const {
-    for (size_t i = 0; i < ev.size(); ++i) {
+  void columns(const std::vector<RawEvent>& ev, bs_event_columns* o) const { columns(ev.data(), ev.size(), o); }
+  void columns(const RawEvent* ev, size_t n, bs_event_columns* o) const {
+    for (size_t i = 0; i < n; ++i) {
       const RawEvent& e = ev[i];
       if (o->pixel) o->pixel[i] = e.pixel;
       if (o->x) o->x[i] = static_cast<uint16_t>(e.pixel % width);
@@ -1419,8 +1431,7 @@ bs_status bs_model_download_events(bs_model* m, const bs_device_events* ev, bs_e
     NEED(m);
     NEED(ev);
     NEED(out);
-    const std::vector<bs::RawEvent> v = m->download(static_cast<const bs::RawEvent*>(ev->data), ev->count, m->own);
-    m->columns(v, out);
+    m->columns(m->download_pinned(static_cast<const bs::RawEvent*>(ev->data), ev->count, m->own), ev->count, out);
   });
 }
 bs_status bs_model_event_count(const bs_model* m, size_t* n) {
@@ -1434,8 +1445,11 @@ bs_status bs_model_take_events(bs_model* m, bs_event_columns* out) {
   return guarded([&] {
     NEED(m);
     NEED(out);
-    if (m->kept.empty() && m->last_events > 0) m->kept = m->download(m->events.p, m->last_events, m->own);
-    m->columns(m->kept, out);
+    if (m->kept.empty() && m->last_events > 0) {
+      m->columns(m->download_pinned(m->events.p, m->last_events, m->own), m->last_events, out);
+    } else {
+      m->columns(m->kept, out);
+    }
     m->kept.clear();
     m->last_events = 0;
   });

@@ -136,7 +136,7 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     tuned = None
     if not (args.no_autotune or args.warps or args.stage or args.tile_width):
         eng.start(0, torch.cuda.current_stream().cuda_stream)
-        tuned = eng.autotune(min(8, wl.windows), torch.cuda.current_stream().cuda_stream)
+        tuned = eng.autotune(wl.windows, torch.cuda.current_stream().cuda_stream)  # trial steps of the full run
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
