@@ -40,6 +40,11 @@ class EventColumns(C.Structure):
                 ("l_first", C.c_void_p)]
 
 
+class OutputColumns(C.Structure):
+    _fields_ = [("t_reported_ns", C.c_void_p), ("t_cross_ns", C.c_void_p), ("x", C.c_void_p), ("y", C.c_void_p),
+                ("flags", C.c_void_p), ("p", C.c_void_p), ("label", C.c_void_p)]
+
+
 class DeviceRuns(C.Structure):
     _fields_ = [("pixel", C.c_void_p), ("row_start", C.c_void_p), ("row_count", C.c_void_p), ("n", C.c_size_t),
                 ("t", C.c_void_p), ("irr", C.c_void_p), ("n_samples", C.c_size_t)]
@@ -81,6 +86,9 @@ _SIGS = {
     "bs_model_maps": (C.c_int32, [_P, _P, _P, _P, _P, _P]),
     "bs_model_stats": (C.c_int32, [_P, _P]),
     "bs_model_noise_maps": (C.c_int32, [_P, _P, _P]),
+    "bs_model_output_prepare": (C.c_int32, [_P, C.POINTER(C.c_size_t)]),
+    "bs_model_output_take": (C.c_int32, [_P, C.POINTER(OutputColumns)]),
+    "bs_model_output_held": (C.c_int32, [_P, C.POINTER(C.c_size_t)]),
     "bs_model_reset_stats": (C.c_int32, [_P]),
     "bs_model_info": (C.c_int32, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_float), C.POINTER(C.c_int32)]),
     "bs_model_state_bytes": (C.c_int32, [_P, C.POINTER(C.c_size_t)]),

@@ -146,6 +146,46 @@ void launch_learned_reset(LearnedSoA st, uint32_t n, const float* irr0, cudaStre
 size_t sort_events_scratch_bytes(uint32_t n);
 cudaError_t sort_events(const RawEvent* ev, uint32_t n, RawEvent* out, void* scratch, cudaStream_t stream);
 
+// The readout of a crossing (Readout, src/sensor/readout.h:14-27): delayed, floored to the counter quantum from its
+// phase, then on the sensor clock (offset, drift).
+struct ReadoutDev {
+  int64_t quantum_ns, delay_ns, phase_ns, offset_ns;
+  double drift_ppm;
+};
+BS_HD int64_t reported_time(const ReadoutDev& r, int64_t t_cross) {
+  int64_t t = t_cross + r.delay_ns;
+  if (r.quantum_ns > 0) {
+    const int64_t a = t - r.phase_ns;
+    const int64_t fd = a / r.quantum_ns - ((a % r.quantum_ns) < 0 ? 1 : 0);
+    t = r.phase_ns + r.quantum_ns * fd;
+  }
+  return t + r.offset_ns + llround(r.drift_ppm * 1e-6 * static_cast<double>(t));
+}
+// The output cut after model time t_end (output_cut, src/sensor/output_order.h:48-53): the window end on the sensor
+// clock (no delay, no quantum).
+BS_HD int64_t output_cut(const ReadoutDev& r, int64_t t_end) {
+  ReadoutDev clock = r;
+  clock.delay_ns = 0;
+  clock.quantum_ns = 0;
+  return reported_time(clock, t_end);
+}
+
+// One output event (OutEvent, src/engine/output.h:25-32, without the ground-truth fields): 24 bytes.
+struct OutRecord {
+  int64_t t_reported, t_cross;
+  uint16_t x, y, flags;
+  uint8_t p, label;  // label: the S1 code (label_s1, src/sensor/output_order.h:23-26)
+};
+
+// The output stage (Camera::output, src/engine/engine_impl.h:1761-1847, without crop and ground truth): the held
+// records (device, n_held) and the call's raw events become records, all sorted by (t_reported, x, y, t_cross) by
+// three stable radix passes (t_cross, (x, y), t_reported: order_key, src/sensor/output_order.h:28-36) into out
+// (device, n_held + n_raw); *n_ready gets how many lead with t_reported < limit (the released ones).
+size_t output_scratch_bytes(uint32_t n);
+cudaError_t output_stage(const OutRecord* held, uint32_t n_held, const RawEvent* raw, uint32_t n_raw, uint32_t width,
+                         int y_bits, const ReadoutDev& rd, int64_t limit, OutRecord* all, OutRecord* out,
+                         void* scratch, unsigned long long* ready_dev, cudaStream_t stream);
+
 // ---- the MLP (learned.cu) ----
 // Training pairs from one window's plain runs (all n_pixels listed in order; t absolute): every stride-th pixel
 // walks its run; pairs are appended (x: 16 BF16 features, y: target, key: pixel << 32 | window << 11 | step).

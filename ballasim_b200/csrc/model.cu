@@ -374,6 +374,7 @@ struct Model {
     initialized = true;
     last_events = 0;
     kept.clear();
+    n_held = n_ready = 0;  // a new run: nothing held by the output stage
   }
 
   void init_host(int64_t t0, const float* irr0) {
@@ -489,16 +490,74 @@ struct Model {
   mutable DevBuf<unsigned char> sort_scratch;
   mutable PinBuf<RawEvent> staged;
 
-  int64_t reported(int64_t t) const {
-    const int64_t q = std::llround(p.readout_quantum_s * 1e9);
-    int64_t r = t + std::llround(p.readout_delay_s * 1e9);
-    if (q > 0) {
-      const int64_t a = r - readout_phase;
-      const int64_t fd = a / q - ((a % q) < 0 ? 1 : 0);
-      r = readout_phase + q * fd;
-    }
-    return r + p.clock_offset_ns + std::llround(p.clock_drift_ppm * 1e-6 * static_cast<double>(r));
+  // ---- the output stage: events in output order, released at the model time's cut, the rest held ----
+  DevBuf<OutRecord> out_held, out_all, out_sorted;
+  DevBuf<unsigned char> out_scratch;
+  DevBuf<unsigned long long> out_ready;
+  PinBuf<OutRecord> out_pin;
+  PinBuf<unsigned long long> out_ready_h;
+  size_t n_held = 0, n_ready = 0;
+
+  ReadoutDev readout() const {
+    return ReadoutDev{std::llround(p.readout_quantum_s * 1e9), std::llround(p.readout_delay_s * 1e9), readout_phase,
+                      p.clock_offset_ns, p.clock_drift_ppm};
   }
+  int y_bits() const {
+    int b = 1;
+    while ((uint64_t{1} << b) < height) ++b;
+    return b;
+  }
+
+  // Moves the last call's events (not yet taken) and the held ones through the output stage; returns how many are
+  // released (output_take copies them out).
+  size_t output_prepare() {
+    const size_t n_raw = last_events;
+    const size_t total = n_held + n_raw;
+    if (total > 0x7fffffffull) throw std::invalid_argument("too many events for the output stage");
+    const uint32_t n = static_cast<uint32_t>(total);
+    out_all.ensure(total);
+    out_sorted.ensure(total);
+    out_scratch.ensure(output_scratch_bytes(n));
+    out_ready.ensure(1);
+    out_ready_h.ensure(1);
+    const int64_t limit = output_cut(readout(), t_state);
+    CK(output_stage(out_held.p, static_cast<uint32_t>(n_held), events.p, static_cast<uint32_t>(n_raw), width,
+                    y_bits(), readout(), limit, out_all.p, out_sorted.p, out_scratch.p, out_ready.p, own));
+    CK(cudaMemcpyAsync(out_ready_h.p, out_ready.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, own));
+    CK(cudaStreamSynchronize(own));
+    n_ready = static_cast<size_t>(out_ready_h.p[0]);
+    out_pin.ensure(n_ready);
+    if (n_ready) {
+      CK(cudaMemcpyAsync(out_pin.p, out_sorted.p, n_ready * sizeof(OutRecord), cudaMemcpyDeviceToHost, own));
+    }
+    const size_t keep = total - n_ready;
+    out_held.ensure(keep);
+    if (keep) {
+      CK(cudaMemcpyAsync(out_held.p, out_sorted.p + n_ready, keep * sizeof(OutRecord), cudaMemcpyDeviceToDevice,
+                         own));
+    }
+    CK(cudaStreamSynchronize(own));
+    n_held = keep;
+    last_events = 0;  // the call's events now belong to the output stage
+    kept.clear();
+    return n_ready;
+  }
+
+  void output_take(bs_output_columns* o) {
+    for (size_t i = 0; i < n_ready; ++i) {
+      const OutRecord& r = out_pin.p[i];
+      if (o->t_reported_ns) o->t_reported_ns[i] = r.t_reported;
+      if (o->t_cross_ns) o->t_cross_ns[i] = r.t_cross;
+      if (o->x) o->x[i] = r.x;
+      if (o->y) o->y[i] = r.y;
+      if (o->flags) o->flags[i] = r.flags;
+      if (o->p) o->p[i] = r.p;
+      if (o->label) o->label[i] = r.label;
+    }
+    n_ready = 0;
+  }
+
+  int64_t reported(int64_t t) const { return reported_time(readout(), t); }
 
   void columns(const std::vector<RawEvent>& ev, bs_event_columns* o) const { columns(ev.data(), ev.size(), o); }
   void columns(const RawEvent* ev, size_t n, bs_event_columns* o) const {
@@ -1452,6 +1511,28 @@ bs_status bs_model_take_events(bs_model* m, bs_event_columns* out) {
     }
     m->kept.clear();
     m->last_events = 0;
+  });
+}
+bs_status bs_model_output_prepare(bs_model* m, size_t* n_ready) {
+  return guarded([&] {
+    NEED(m);
+    NEED(n_ready);
+    if (!m->initialized) throw std::logic_error("output: call init() first");
+    *n_ready = m->output_prepare();
+  });
+}
+bs_status bs_model_output_take(bs_model* m, bs_output_columns* out) {
+  return guarded([&] {
+    NEED(m);
+    NEED(out);
+    m->output_take(out);
+  });
+}
+bs_status bs_model_output_held(const bs_model* m, size_t* n_held) {
+  return guarded([&] {
+    NEED(m);
+    NEED(n_held);
+    *n_held = m->n_held;
   });
 }
 bs_status bs_model_maps(const bs_model* m, double* on, double* off, double* leak, double* dark, double* phi0) {

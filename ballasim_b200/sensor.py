@@ -228,6 +228,30 @@ class SensorModel:
             _lib.check(_lib.lib().bs_model_event_count(self._h, C.byref(n)))
             return self._take(n.value, with_pixel)
 
+    def take_output(self) -> dict:
+        """The engine's output stage (Camera::output, src/engine/engine_impl.h:1761-1847, without crop and ground
+        truth): the events not taken with take_events, with those held from earlier calls, in output order
+        (t_reported, x, y, t_cross); the ones reported before the model time on the sensor clock are returned
+        (columns t_reported_ns, t_cross_ns, x, y, p, label (S1 codes: 0 signal, 2 noise, 3 leak, 4 hot), flags),
+        the rest stay held for the next call."""
+        n = C.c_size_t()
+        with self._lock:
+            _lib.check(_lib.lib().bs_model_output_prepare(self._h, C.byref(n)))
+            k = n.value
+            cols = {"t_reported_ns": np.zeros(k, np.int64), "t_cross_ns": np.zeros(k, np.int64),
+                    "x": np.zeros(k, np.uint16), "y": np.zeros(k, np.uint16), "flags": np.zeros(k, np.uint16),
+                    "p": np.zeros(k, np.uint8), "label": np.zeros(k, np.uint8)}
+            s = _lib.OutputColumns(*(cols[f].ctypes.data for f, _ in _lib.OutputColumns._fields_))
+            _lib.check(_lib.lib().bs_model_output_take(self._h, C.byref(s)))
+            return cols
+
+    @property
+    def output_held(self) -> int:
+        """Events the output stage holds for a later call."""
+        n = C.c_size_t()
+        _lib.check(_lib.lib().bs_model_output_held(self._h, C.byref(n)))
+        return n.value
+
     def sensor_maps(self) -> dict:
         n = self._width * self._height
         a = {k: np.zeros(n) for k in ("theta_on", "theta_off", "leak", "dark_current_fA", "phi0")}

@@ -115,6 +115,21 @@ bs_status bs_model_take_events(bs_model* m, bs_event_columns* out);
 /* SensorModel::maps (sensor_model.h:180; sensor_module.cpp sensor_maps): the fp64 maps, width * height each. */
 bs_status bs_model_maps(const bs_model* m, double* theta_on, double* theta_off, double* leak, double* dark_fA,
                         double* phi0);
+/* The engine's output stage (Camera::output, src/engine/engine_impl.h:1761-1847, without crop and ground truth):
+ * records with the reported time (src/sensor/readout.h:22-27) and the S1 label (label_s1,
+ * src/sensor/output_order.h:23-26), in output order (t_reported, x, y, t_cross) (output_order,
+ * src/sensor/output_order.h:88-107). bs_model_output_prepare moves the last call's events (those not taken with
+ * bs_model_take_events) and the held ones through the stage on the device and releases those reported before the
+ * model time on the sensor clock (output_cut, :48-53); the rest stay held for the next call. *n_ready receives the
+ * released count; bs_model_output_take copies them to host columns (any may be NULL). init() clears what is held. */
+typedef struct {
+  int64_t *t_reported_ns, *t_cross_ns;
+  uint16_t *x, *y, *flags;
+  uint8_t *p, *label;
+} bs_output_columns;
+bs_status bs_model_output_prepare(bs_model* m, size_t* n_ready);
+bs_status bs_model_output_take(bs_model* m, bs_output_columns* out);
+bs_status bs_model_output_held(const bs_model* m, size_t* n_held);
 /* This build's noise maps (no reference counterpart), width * height each: the pixel's background-activity rate
  * and its shot-noise dominating rate r sqrt(100 fA / I_dk) (Hz; 0 when that noise is off). */
 bs_status bs_model_noise_maps(const bs_model* m, double* ba_rate_hz, double* shot_max_hz);

@@ -384,11 +384,30 @@ class Ref:
             L.ref_sample_window.argtypes = [C.POINTER(OrcField), C.c_float, C.c_float, C.c_int, C.c_int, C.c_int,
                                             C.c_int64, C.c_int64, _u32p, _u8p, C.c_size_t, _f32p, _u64p, _i64p,
                                             _i64p, _f32p, C.c_size_t]
+            L.ref_output_order.argtypes = [_i64p, _u16p, _u16p, _i64p, C.c_size_t, C.c_uint32, _u32p]
+            L.ref_reported_time.restype = C.c_int64
+            L.ref_reported_time.argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_int64]
+            L.ref_output_cut.restype = C.c_int64
+            L.ref_output_cut.argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_int64]
+            L.ref_label_s1.restype = C.c_uint8
+            L.ref_label_s1.argtypes = [C.c_uint8]
+            L.ref_readout_phase.restype = C.c_int64
+            L.ref_readout_phase.argtypes = [C.c_uint64, C.c_uint32, C.c_int64]
             L.ref_simulate.restype = C.c_int64
             L.ref_simulate.argtypes = [C.c_void_p, C.POINTER(OrcField), C.c_float, C.c_float, C.c_int, C.c_int64,
                                        C.c_int32, C.c_int32, C.c_int64, C.c_int32, _f64p]
             cls._lib = L
         return cls._lib
+
+    @classmethod
+    def output_order(cls, t_cross, x, y, t_reported, height) -> np.ndarray:
+        """The reference's output permutation of the event columns (output_order)."""
+        n = len(t_cross)
+        perm = np.zeros(n, np.uint32)
+        cls.lib().ref_output_order(np.ascontiguousarray(t_cross, np.int64), np.ascontiguousarray(x, np.uint16),
+                                   np.ascontiguousarray(y, np.uint16), np.ascontiguousarray(t_reported, np.int64), n,
+                                   height, perm)
+        return perm
 
     @classmethod
     def sample_window(cls, f, rules, t_w, pixel, level, carried_irr, carried_sig):

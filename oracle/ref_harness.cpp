@@ -16,7 +16,9 @@
 #include <vector>
 
 #include "engine/window.h"
+#include "sensor/output_order.h"
 #include "sensor/params.h"
+#include "sensor/readout.h"
 #include "sensor/sensor_model.h"
 
 extern "C" {
@@ -276,6 +278,25 @@ int64_t ref_simulate(void* h, const orc_field* f, float tol, float dark, int max
   } catch (const std::exception& e) {
     return fail(e);
   }
+}
+
+// The reference's output order (sensor/output_order.h output_order) of n event columns, and its readout
+// (sensor/readout.h reported_time) and output cut, for the output stage's parity.
+void ref_output_order(const int64_t* t_cross, const uint16_t* x, const uint16_t* y, const int64_t* t_reported,
+                      size_t n, uint32_t height, uint32_t* perm) {
+  std::vector<uint32_t> p;
+  balla::sensor::output_order({t_cross, n}, {x, n}, {y, n}, {t_reported, n}, balla::sensor::order_y_bits(height), p);
+  std::memcpy(perm, p.data(), n * sizeof(uint32_t));
+}
+int64_t ref_reported_time(int64_t quantum, int64_t delay, int64_t phase, int64_t offset, double drift, int64_t t) {
+  return balla::sensor::reported_time(balla::sensor::Readout{quantum, delay, phase, offset, drift}, t);
+}
+int64_t ref_output_cut(int64_t quantum, int64_t delay, int64_t phase, int64_t offset, double drift, int64_t t_end) {
+  return balla::sensor::output_cut(balla::sensor::Readout{quantum, delay, phase, offset, drift}, t_end);
+}
+uint8_t ref_label_s1(uint8_t c3) { return balla::sensor::label_s1(c3); }
+int64_t ref_readout_phase(uint64_t seed, uint32_t camera, int64_t quantum) {
+  return balla::sensor::readout_phase_ns(seed, camera, quantum);
 }
 
 }  // extern "C"

@@ -304,3 +304,46 @@ def test_autotune_keeps_the_state_and_the_events(cuda_lib):
     assert out[0][0] == out[1][0] and out[0][1] == out[1][1]
     for k in ("pixel", "t_cross_ns", "p", "label"):
         assert np.array_equal(out[0][2][k], out[1][2][k])
+
+
+@pytest.mark.gpu
+def test_output_stage_follows_the_reference_order(cuda_lib, ref):
+    """The output stage (records released in (t_reported, x, y, t_cross) order at each call's cut on the sensor clock,
+    the rest held) equals the reference's output_order and output_cut applied to the same events."""
+    from ballasim_b200.engine import Engine
+    from ballasim_b200.sensor import SensorModel
+
+    wl = W.small("noise", 48, 32, 12)
+    spec, r = wl.sensors[0], wl.rules
+    ov = {**spec.overrides, "noise_shot_rate_hz": 40.0, "noise_ba_median_hz": 30.0, "readout_quantum_s": 1e-6,
+          "readout_delay_s": 3e-6, "clock_drift_ppm": 40.0, "clock_offset_ns": 12345}
+    p = resolve("ideal", ov)
+    outs, evs, held = [], [], 0
+    for mode in ("output", "events"):
+        m = SensorModel(p, spec.width, spec.height, spec.seed, [{"type": "constant"}], spec.camera)
+        eng = Engine([(m, spec.field)], tol=r.tol, dark=r.dark, min_dt_ns=r.min_dt_ns,
+                     max_refine_levels=r.max_refine_levels, l_min=r.l_min, l_max=r.l_max)
+        eng.start(0)
+        for chunk in (3, 4, 5):
+            eng.run(chunk)
+            if mode == "output":
+                outs.append(m.take_output())
+            else:
+                evs.append(m.take_events())
+        if mode == "output":
+            held = m.output_held
+    got = {k: np.concatenate([o[k] for o in outs]) for k in outs[0]}
+    ev = {k: np.concatenate([e[k] for e in evs]) for k in evs[0]}
+    L = ref.lib()
+    phase = L.ref_readout_phase(spec.seed, spec.camera, 1000)
+    want_rep = [L.ref_reported_time(1000, 3000, phase, 12345, 40.0, int(t)) for t in ev["t_cross_ns"]]
+    assert np.array_equal(ev["t_reported_ns"], np.array(want_rep, np.int64))
+    perm = ref.output_order(ev["t_cross_ns"], ev["x"], ev["y"], ev["t_reported_ns"], spec.height)
+    cut = L.ref_output_cut(0, 0, 0, 12345, 40.0, wl.windows << 23)
+    order = perm[ev["t_reported_ns"][perm] < cut]
+    assert len(got["t_cross_ns"]) == len(order) > 100 and held == len(perm) - len(order)
+    for k in ("t_reported_ns", "t_cross_ns", "x", "y", "p", "flags"):
+        assert np.array_equal(got[k], ev[k][order]), k
+    s1 = np.array([L.ref_label_s1(int(c)) for c in ev["label"][order]], np.uint8)
+    assert np.array_equal(got["label"], s1)
+    assert len(np.unique(ev["label"])) > 1
