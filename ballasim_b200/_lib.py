@@ -30,7 +30,8 @@ class Params(C.Structure):
                                           "illuminance_scale", "label_share_cut", "readout_quantum_s",
                                           "readout_delay_s", "clock_drift_ppm")] + \
                [("clock_offset_ns", C.c_int64), ("hot_fraction", C.c_double), ("noise_shot_rate_hz", C.c_double),
-                ("noise_ba_median_hz", C.c_double), ("noise_ba_sigma_ln", C.c_double)]
+                ("noise_ba_median_hz", C.c_double), ("noise_ba_sigma_ln", C.c_double)] + \
+               [(n, C.c_double) for n in ("k", "tau_o", "tau_sf", "eps_L")] + [("noise", C.c_int32)]
 
 
 class EventColumns(C.Structure):

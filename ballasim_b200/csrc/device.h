@@ -4,7 +4,8 @@
 // contiguous segment per field:
 //   state (double-buffered: a call reads one copy and writes the other, so a failed or overflowing call
 //   leaves the model as it was): t_ref, t_search, blind_until, t_shot, t_ba (i64); s3_ref, n3_ref, dr_ref,
-//   i_scale, held (f32); flags, n_shot, n_ba (u32): 72 B per pixel (the noise words are read only with noise on).
+//   i_scale, held (f32); flags, n_shot, n_ba (u32): 72 B per pixel (the noise words are read only with noise on);
+//   with the cascade photoreceptor also z, x1, s2, s3, tv (f32): 20 B more.
 //   map: theta_on, theta_off, leak, dark, scale, phi0 (f32), ba_rate, shot_max (f64): 40 B per pixel.
 // Sample runs follow the reference's DeviceRuns (src/sensor/sensor_model.h:81-89): pixel[i], row_start[i],
 // row_count[i], t (i64), irr (f32): 12 B per sample.
@@ -13,6 +14,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "cascade.cuh"
 #include "fields.cuh"
 #include "learned.cuh"
 #include "pixel.cuh"
@@ -24,6 +26,7 @@ struct StateSoA {
   int64_t *t_ref, *t_search, *blind_until, *t_shot, *t_ba;
   float *s3_ref, *n3_ref, *dr_ref, *i_scale, *held;
   uint32_t *flags, *n_shot, *n_ba;
+  float *z, *x1, *s2, *s3, *tv;  // the cascade's (null without it)
 };
 
 struct MapSoA {
@@ -40,6 +43,7 @@ enum CounterWord : int {
   kCntLeaves = 4,     // bisection nodes tested
   kCntSamples = 5,    // pixel-samples consumed
   kCntNoise = 6,      // noise candidates
+  kCntSubsteps = 7,   // accepted cascade sub-steps
   kCntWords = 8
 };
 enum ErrorBit : unsigned long long {
@@ -83,6 +87,7 @@ struct EngineSensor {
   LearnedSoA lin, lout;  // learned-proposal walk state (unused by the plain engine)
   FieldDev field;
   SensorConsts consts;
+  CascadeConsts cc;      // the cascade's constants (consts.cascade)
   StateSoA in, out;
   MapSoA map;
   float* carried_in;   // the sampler's carried sample (irradiance at the window start), per pixel
@@ -99,7 +104,9 @@ void launch_init_counted(const SensorConsts& k, const MapSoA& map, StateSoA st, 
                          const float* irr0, unsigned long long* counters, cudaStream_t stream);
 void launch_scatter_rows(const uint32_t* pixel, uint32_t n, int32_t* row_of, uint32_t n_pixels,
                          unsigned long long* counters, cudaStream_t stream);
-void launch_advance_runs(const SensorConsts& k, const MapSoA& map, StateSoA in, StateSoA out, uint32_t n_pixels,
+// The CSR-runs kernel of the instantaneous response, or of the cascade when k.cascade (cc its constants).
+void launch_advance_runs(const SensorConsts& k, const CascadeConsts& cc, const MapSoA& map, StateSoA in, StateSoA out,
+                         uint32_t n_pixels,
                          const uint32_t* pixel_ids, const int32_t* row_of, const int64_t* row_start,
                          const int32_t* row_count, const int64_t* t, const float* irr, uint64_t n_samples,
                          int64_t t_state, int64_t t_end, EventBuf ev, unsigned long long* counters, int block,
@@ -119,10 +126,11 @@ void launch_field_frame(const FieldDev& f, int64_t t, uint32_t n_pixels, float* 
 // counter (work stealing) by a persistent grid. stage 0: the sampler feeds the pixel model sample by sample;
 // 16 or 32: per window the samples are staged in shared memory (that many per lane) between the two phases.
 // t0: the model time in device memory; tiles of 2^tile_lw x 2^(5 - tile_lw) pixels (tile_lw in [2, 5]).
+// cascade: every sensor runs the cascade photoreceptor (streaming form; stage is ignored).
 void launch_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t total_tiles, const int64_t* t0,
                    int32_t w0, int32_t w1, const SamplerRules& r, unsigned int* tile_counter, int blocks,
-                   int warps_per_block, int stage, int tile_lw, cudaStream_t stream);
-int engine_max_blocks_per_sm(int warps_per_block, int stage);
+                   int warps_per_block, int stage, int tile_lw, bool cascade, cudaStream_t stream);
+int engine_max_blocks_per_sm(int warps_per_block, int stage, bool cascade);
 // The fused engine with the learned step proposal (BF16 MLP operands and FP32 parameters in device memory):
 // the same tiles and pixel model, each window sampled by proposed power-of-two steps judged by the plain rule.
 // rec_samples / rec_steps (capacity 0: off) record every sample and every proposed step.

@@ -73,6 +73,22 @@ __device__ __forceinline__ void store_state(const StateSoA& a, uint32_t p, bool 
   }
 }
 
+__device__ __forceinline__ void load_cascade(const StateSoA& a, uint32_t p, CascadeRegs& q) {
+  q.z = a.z[p];
+  q.x1 = a.x1[p];
+  q.s2 = a.s2[p];
+  q.s3 = a.s3[p];
+  q.tv = a.tv[p];
+}
+
+__device__ __forceinline__ void store_cascade(const StateSoA& a, uint32_t p, const CascadeRegs& q) {
+  a.z[p] = q.z;
+  a.x1[p] = q.x1;
+  a.s2[p] = q.s2;
+  a.s3[p] = q.s3;
+  a.tv[p] = q.tv;
+}
+
 __device__ __forceinline__ void load_map(const MapSoA& m, uint32_t p, PixelMapRegs& r) {
   r.theta_on = m.theta_on[p];
   r.theta_off = m.theta_off[p];
@@ -113,6 +129,11 @@ __global__ void __launch_bounds__(256) init_kernel(SensorConsts k, MapSoA map, S
     PixelRegs s;
     pixel_init(s, m, k, pixel_ids ? pixel_ids[p] : p, t0, v, map.phi0[p]);
     store_state(st, p, true, s);
+    if (k.cascade) {
+      CascadeRegs q;
+      cascade_init(q, s);
+      store_cascade(st, p, q);
+    }
   }
   warp_add(&counters[kCntClamps], clamps);
   warp_or(&counters[kCntErrors], err);
@@ -135,6 +156,7 @@ __global__ void scatter_rows_kernel(const uint32_t* pixel, uint32_t n, int32_t* 
 
 struct RunArgs {
   SensorConsts k;
+  CascadeConsts cc;
   MapSoA map;
   StateSoA in, out;
   uint32_t n_pixels;
@@ -222,6 +244,73 @@ __global__ void __launch_bounds__(128) advance_runs_kernel(RunArgs a) {
   warp_add(&a.counters[kCntLeaves], c.leaves);
   warp_add(&a.counters[kCntSamples], samples);
   warp_add(&a.counters[kCntNoise], c.noise_candidates);
+  warp_or(&a.counters[kCntErrors], err);
+}
+
+// The cascade on CSR runs: the same run checks as advance_runs_kernel, every segment through CascadeProc.
+__global__ void __launch_bounds__(128) advance_runs_cascade_kernel(RunArgs a) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  PixelCounters c;
+  CascadeCounters cn;
+  unsigned long long clamps = 0, samples = 0, err = 0;
+  if (p < a.n_pixels) {
+    PixelRegs s;
+    load_state(a.in, p, false, s);
+    CascadeRegs q;
+    load_cascade(a.in, p, q);
+    PixelMapRegs m;
+    load_map(a.map, p, m);
+    GlobalSink sink{a.ev, &a.counters[kCntEvents]};
+    CascadeProc<GlobalSink> proc{s, q, m, a.k, a.cc, a.pixel_ids ? a.pixel_ids[p] : p, sink, c, cn};
+    int64_t prev_t = a.t_state;
+    float prev_v = s.held;
+    const int32_t row = a.row_of != nullptr ? a.row_of[p] : -1;
+    int32_t cnt = 0;
+    if (row >= 0) {
+      const int64_t s0 = a.row_start[row];
+      cnt = a.row_count[row];
+      if (cnt < 0 || s0 < 0 || static_cast<uint64_t>(s0) + static_cast<uint64_t>(cnt) > a.n_samples) {
+        err |= kErrRunRange;
+        cnt = 0;
+      } else {
+        const int64_t* tp = a.t + s0;
+        const float* vp = a.irr + s0;
+        for (int32_t i = 0; i < cnt; ++i) {
+          const int64_t ti = __ldg(tp + i);
+          const float raw = __ldg(vp + i);
+          if (!isfinite(raw)) err |= kErrNonFinite;
+          const float vi = clamp_irr(raw, a.k.irr_max);
+          if (!(vi == raw)) ++clamps;
+          if (i == 0 ? ti < a.t_state : ti <= prev_t) {
+            err |= kErrOrder;
+            break;
+          }
+          if (ti > a.t_end) {
+            err |= kErrAfterEnd;
+            break;
+          }
+          if (i == 0 && ti == a.t_state) {  // a sample at the model time replaces the held one (pixel.h:777)
+            prev_v = vi;
+            continue;
+          }
+          proc.segment(Segment{prev_t, ti, prev_v, vi}, prev_t, ti);
+          prev_t = ti;
+          prev_v = vi;
+        }
+        samples = static_cast<unsigned long long>(cnt);
+      }
+    }
+    proc.segment(Segment{prev_t, kForever, prev_v, prev_v}, prev_t, a.t_end);
+    if (row >= 0 && cnt > 0) s.held = prev_v;
+    store_state(a.out, p, false, s);
+    store_cascade(a.out, p, q);
+  }
+  __syncwarp();
+  warp_add(&a.counters[kCntClamps], clamps);
+  warp_add(&a.counters[kCntPieces], c.pieces);
+  warp_add(&a.counters[kCntLeaves], c.leaves);
+  warp_add(&a.counters[kCntSamples], samples);
+  warp_add(&a.counters[kCntSubsteps], cn.substeps);
   warp_or(&a.counters[kCntErrors], err);
 }
 
@@ -464,6 +553,89 @@ __global__ void __launch_bounds__(128) engine_kernel(EngineArgs a) {
     warp_add(&S.counters[kCntLeaves], c.leaves);
     warp_add(&S.counters[kCntSamples], samples);
     warp_add(&S.counters[kCntNoise], c.noise_candidates);
+  }
+}
+
+// The fused engine with the cascade photoreceptor (noise lattice off): the tile loop of engine_kernel, each window's
+// samples fed as segments to CascadeProc (a segment never crosses the window, so each is one piece).
+struct CascadeFeed {
+  CascadeProc<GlobalSink>* proc;
+  int64_t t_w;
+  float irr_max;
+  int64_t prev_t;
+  float prev_v;
+  float last_raw;
+  __device__ __forceinline__ void start(float carried) {
+    last_raw = carried;
+    prev_v = clamp_irr(carried, irr_max);
+  }
+  __device__ __forceinline__ void operator()(uint32_t dt, float v) {
+    last_raw = v;
+    const float vc = clamp_irr(v, irr_max);
+    const int64_t t = t_w + dt;
+    proc->segment(Segment{prev_t, t, prev_v, vc}, prev_t, t);
+    prev_t = t;
+    prev_v = vc;
+  }
+};
+
+__global__ void __launch_bounds__(128) engine_cascade_kernel(EngineArgs a) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const int64_t t0 = *a.t0;
+  for (;;) {
+    uint32_t tile = 0;
+    if (lane == 0) tile = atomicAdd(a.tile_counter, 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if (tile >= a.total_tiles) break;
+    int si = 0;
+    while (si + 1 < a.n_sensors && a.sensors[si + 1].tile0 <= tile) ++si;
+    const EngineSensor& S = a.sensors[si];
+    const uint32_t local = tile - S.tile0;
+    uint32_t x, y;
+    tile_xy(local, S.tiles_x, a.tile_lw, lane, x, y);
+    const bool have = x < S.width && y < S.height;
+    const uint32_t p = have ? y * S.width + x : 0u;
+    PixelRegs s;
+    CascadeRegs q;
+    PixelMapRegs m;
+    float carried = 0.0f;
+    if (have) {
+      load_state(S.in, p, false, s);
+      load_cascade(S.in, p, q);
+      load_map(S.map, p, m);
+      carried = S.carried_in[p];
+    }
+    PixelCounters c;
+    CascadeCounters cn;
+    unsigned long long samples = 0;
+    GlobalSink sink{S.ev, &S.counters[kCntEvents]};
+    CascadeProc<GlobalSink> proc{s, q, m, S.consts, S.cc, p, sink, c, cn};
+    const FieldDev& f = S.field;
+    __shared__ uint16_t lists[4][kMaxListed];
+    uint16_t* my_list = lists[threadIdx.x >> 5];
+    for (int32_t w = a.w0; w < a.w1; ++w) {
+      const int64_t t_w = t0 + static_cast<int64_t>(w) * kWindowNs;
+      const BlobList list = warp_blob_list(f, have, x, y, t_w, t_w + kWindowNs, my_list);
+      if (have) {
+        const int level = field_level(f, list, x, y, t_w, a.r.l_min, a.r.l_max);
+        CascadeFeed feed{&proc, t_w, S.consts.irr_max, t_w, s.held, carried};
+        feed.start(carried);
+        auto render = [&](uint32_t dt) { return field_eval(f, list, x, y, t_w + dt); };
+        samples += sample_pixel_window(a.r, level, carried, false, render, feed);
+        s.held = feed.prev_v;
+        carried = feed.last_raw;
+      }
+      __syncwarp();
+    }
+    if (have) {
+      store_state(S.out, p, false, s);
+      store_cascade(S.out, p, q);
+      S.carried_out[p] = carried;
+    }
+    warp_add(&S.counters[kCntPieces], c.pieces);
+    warp_add(&S.counters[kCntLeaves], c.leaves);
+    warp_add(&S.counters[kCntSamples], samples);
+    warp_add(&S.counters[kCntSubsteps], cn.substeps);
   }
 }
 
@@ -762,16 +934,17 @@ void launch_scatter_rows(const uint32_t* pixel, uint32_t n, int32_t* row_of, uin
   scatter_rows_kernel<<<(n + 255) / 256, 256, 0, stream>>>(pixel, n, row_of, n_pixels, counters);
 }
 
-void launch_advance_runs(const SensorConsts& k, const MapSoA& map, StateSoA in, StateSoA out, uint32_t n_pixels,
-                         const uint32_t* pixel_ids, const int32_t* row_of, const int64_t* row_start,
+void launch_advance_runs(const SensorConsts& k, const CascadeConsts& cc, const MapSoA& map, StateSoA in, StateSoA out,
+                         uint32_t n_pixels, const uint32_t* pixel_ids, const int32_t* row_of, const int64_t* row_start,
                          const int32_t* row_count, const int64_t* t, const float* irr, uint64_t n_samples,
                          int64_t t_state, int64_t t_end, EventBuf ev, unsigned long long* counters, int block,
                          cudaStream_t stream) {
-  RunArgs a{k, map, in, out, n_pixels, pixel_ids, row_of, row_start, row_count, t, irr, n_samples, t_state, t_end,
+  RunArgs a{k, cc, map, in, out, n_pixels, pixel_ids, row_of, row_start, row_count, t, irr, n_samples, t_state, t_end,
             ev, counters};
   if (block <= 0) block = 128;
   const unsigned grid = (n_pixels + block - 1) / block;
-  advance_runs_kernel<<<grid, block, 0, stream>>>(a);
+  if (k.cascade) advance_runs_cascade_kernel<<<grid, block, 0, stream>>>(a);
+  else advance_runs_kernel<<<grid, block, 0, stream>>>(a);
 }
 
 void launch_sample_window(const FieldDev& f, const SamplerRules& r, int64_t t_w, const uint32_t* pixel,
@@ -805,16 +978,19 @@ void launch_field_frame(const FieldDev& f, int64_t t, uint32_t n_pixels, float* 
 
 void launch_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t total_tiles, const int64_t* t0,
                    int32_t w0, int32_t w1, const SamplerRules& r, unsigned int* tile_counter, int blocks,
-                   int warps_per_block, int stage, int tile_lw, cudaStream_t stream) {
+                   int warps_per_block, int stage, int tile_lw, bool cascade, cudaStream_t stream) {
   EngineArgs a{sensors_dev, n_sensors, total_tiles, t0, w0, w1, r, tile_counter, static_cast<uint32_t>(tile_lw)};
-  if (stage == 16) engine_kernel_staged<16><<<blocks, warps_per_block * 32, 0, stream>>>(a);
+  if (cascade) engine_cascade_kernel<<<blocks, warps_per_block * 32, 0, stream>>>(a);
+  else if (stage == 16) engine_kernel_staged<16><<<blocks, warps_per_block * 32, 0, stream>>>(a);
   else if (stage == 32) engine_kernel_staged<32><<<blocks, warps_per_block * 32, 0, stream>>>(a);
   else engine_kernel<<<blocks, warps_per_block * 32, 0, stream>>>(a);
 }
 
-int engine_max_blocks_per_sm(int warps_per_block, int stage) {
+int engine_max_blocks_per_sm(int warps_per_block, int stage, bool cascade) {
   int n = 0;
-  if (stage == 16) {
+  if (cascade) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_cascade_kernel, warps_per_block * 32, 0);
+  } else if (stage == 16) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel_staged<16>, warps_per_block * 32, 0);
   } else if (stage == 32) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel_staged<32>, warps_per_block * 32, 0);

@@ -177,11 +177,11 @@ uint64_t fnv1a(const void* data, size_t n, uint64_t h = 0xcbf29ce484222325ull) {
 // ---------------------------------------------------------------------------------------------
 struct StateBufs {
   DevBuf<int64_t> i64;   // 5 x n: t_ref, t_search, blind_until, t_shot, t_ba
-  DevBuf<float> f32;     // 5 x n: s3_ref, n3_ref, dr_ref, i_scale, held
+  DevBuf<float> f32;     // 5 x n: s3_ref, n3_ref, dr_ref, i_scale, held; with the cascade 5 x n more: z, x1, s2, s3, tv
   DevBuf<uint32_t> u32;  // 3 x n: flags, n_shot, n_ba
-  StateSoA soa(size_t n) {
+  StateSoA soa(size_t n, bool cascade) {
     i64.ensure(5 * n);
-    f32.ensure(5 * n);
+    f32.ensure((cascade ? 10 : 5) * n);
     u32.ensure(3 * n);
     StateSoA s;
     s.t_ref = i64.p;
@@ -197,6 +197,12 @@ struct StateBufs {
     s.flags = u32.p;
     s.n_shot = u32.p + n;
     s.n_ba = u32.p + 2 * n;
+    float* c = cascade ? f32.p + 5 * n : nullptr;
+    s.z = c;
+    s.x1 = c ? c + n : nullptr;
+    s.s2 = c ? c + 2 * n : nullptr;
+    s.s3 = c ? c + 3 * n : nullptr;
+    s.tv = c ? c + 4 * n : nullptr;
     return s;
   }
 };
@@ -230,6 +236,7 @@ struct Model {
   uint64_t seed = 0;
   HostMaps maps;
   SensorConsts k{};
+  CascadeConsts cc{};
   cudaStream_t own = nullptr;
   DevBuf<float> mapf;    // 6 x n
   DevBuf<double> mapd;   // 2 x n
@@ -277,9 +284,22 @@ struct Model {
     k.shot_rate_hz = p.noise_shot_rate_hz;
     k.seed = seed;
     k.camera = camera;
+    k.cascade = p.photoreceptor == 0 ? 1 : 0;
+    if (k.cascade) {
+      // cascade_constants<float> (src/sensor/sensor_model.cpp:376-389) and eps_pl_base (:397).
+      const double eps_h = p.eps_L / 8.0;
+      cc.k = static_cast<float>(p.k * 1e-15);
+      cc.a2 = static_cast<float>(1.0 / p.tau_o);
+      cc.a3 = static_cast<float>(1.0 / p.tau_sf);
+      cc.tau_o = static_cast<float>(p.tau_o);
+      cc.tau_sf = static_cast<float>(p.tau_sf);
+      cc.eps_accept = static_cast<float>(eps_h / 1.5);
+      cc.eps_drop = static_cast<float>(std::max(eps_h / 1024.0, 32.0 * 0x1p-23));
+      cc.eps_pl_base = static_cast<float>(p.eps_L / 8.0);
+    }
     upload_maps();
-    soa[0] = st[0].soa(n);
-    soa[1] = st[1].soa(n);
+    soa[0] = st[0].soa(n, k.cascade != 0);
+    soa[1] = st[1].soa(n, k.cascade != 0);
     row_of.ensure(n);
     counters.ensure(kCntWords);
     counters_h.ensure(kCntWords);
@@ -294,8 +314,25 @@ struct Model {
   }
 
   void validate(int32_t groups) const {
-    if (p.photoreceptor != 1) {
-      throw std::invalid_argument("SensorModel: this build runs photoreceptor 'instantaneous' only");
+    if (p.photoreceptor != 0 && p.photoreceptor != 1) {
+      throw std::invalid_argument("SensorParams: photoreceptor must be 'cascade' or 'instantaneous'");
+    }
+    if (p.photoreceptor == 0) {
+      if (p.noise != 0) {
+        throw std::invalid_argument(
+            "SensorModel: this build runs the cascade photoreceptor without its noise lattice (noise = false)");
+      }
+      if (p.noise_shot_rate_hz > 0.0 || p.noise_ba_median_hz > 0.0) {
+        throw std::invalid_argument("SensorModel: shot and background-activity noise run with the instantaneous "
+                                    "response only");
+      }
+      if (!(p.k > 0.0) || !(p.tau_o > 0.0) || !(p.tau_sf > 0.0) || !(p.eps_L > 0.0)) {
+        throw std::invalid_argument("SensorParams: k, tau_o, tau_sf and eps_L must be > 0");
+      }
+      if (!(std::max(p.tau_o, p.tau_sf) >= 1.1 * std::min(p.tau_o, p.tau_sf))) {
+        throw std::invalid_argument(
+            "SensorParams: tau_sf and tau_o must differ by at least 10 % (the larger >= 1.1 x the smaller)");
+      }
     }
     if (groups != 1) throw std::invalid_argument("SensorModel: this build runs one constant light group");
     if (width == 0 || height == 0 || width > 65535 || height > 65535) {
@@ -413,7 +450,7 @@ struct Model {
       CK(cudaMemsetAsync(row_of.p, 0xFF, n * sizeof(int32_t), s));
       launch_scatter_rows(r.pixel, static_cast<uint32_t>(r.n), row_of.p, n, counters.p, s);
       CK(cudaEventRecord(timer.a, s));
-      launch_advance_runs(k, map, soa[cur], soa[1 - cur], n, nullptr, r.n ? row_of.p : nullptr, r.row_start,
+      launch_advance_runs(k, cc, map, soa[cur], soa[1 - cur], n, nullptr, r.n ? row_of.p : nullptr, r.row_start,
                           r.row_count, r.t, r.irr, r.n_samples, t_state, t_end,
                           EventBuf{events.p, static_cast<unsigned long long>(event_cap)}, counters.p, block, s);
       CK(cudaGetLastError());
@@ -586,20 +623,21 @@ struct Model {
     uint32_t initialized, bytes_per_pixel;
   };
   static constexpr uint32_t kMagic = 0x32304253;  // "SB02"
-  static constexpr uint32_t kBytesPerPixel = 5 * 8 + 5 * 4 + 3 * 4;
-  size_t state_bytes() const { return sizeof(Header) + static_cast<size_t>(n) * kBytesPerPixel; }
+  size_t f32_words() const { return k.cascade ? 10 : 5; }
+  uint32_t bytes_per_pixel() const { return static_cast<uint32_t>(5 * 8 + f32_words() * 4 + 3 * 4); }
+  size_t state_bytes() const { return sizeof(Header) + static_cast<size_t>(n) * bytes_per_pixel(); }
   uint64_t fingerprint() const { return fnv1a(&p, sizeof(p)); }
 
   void save(uint8_t* out, size_t bytes) const {
     if (bytes != state_bytes()) throw std::invalid_argument("SensorModel.save_state: buffer size does not match");
-    Header h{kMagic, 1, width, height, camera, 0, seed, fingerprint(), t_state, initialized ? 1u : 0u, kBytesPerPixel};
+    Header h{kMagic, 1, width, height, camera, 0, seed, fingerprint(), t_state, initialized ? 1u : 0u, bytes_per_pixel()};
     std::memcpy(out, &h, sizeof(h));
     uint8_t* q = out + sizeof(h);
     const StateBufs& b = st[cur];
     CK(cudaMemcpy(q, b.i64.p, 5 * sizeof(int64_t) * n, cudaMemcpyDeviceToHost));
     q += 5 * sizeof(int64_t) * n;
-    CK(cudaMemcpy(q, b.f32.p, 5 * sizeof(float) * n, cudaMemcpyDeviceToHost));
-    q += 5 * sizeof(float) * n;
+    CK(cudaMemcpy(q, b.f32.p, f32_words() * sizeof(float) * n, cudaMemcpyDeviceToHost));
+    q += f32_words() * sizeof(float) * n;
     CK(cudaMemcpy(q, b.u32.p, 3 * sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
   }
 
@@ -607,7 +645,7 @@ struct Model {
     if (bytes != state_bytes()) throw std::invalid_argument("SensorModel.load_state: size does not match this model");
     Header h;
     std::memcpy(&h, data, sizeof(h));
-    if (h.magic != kMagic || h.version != 1 || h.bytes_per_pixel != kBytesPerPixel) {
+    if (h.magic != kMagic || h.version != 1 || h.bytes_per_pixel != bytes_per_pixel()) {
       throw std::invalid_argument("SensorModel.load_state: not a sensor state of this version");
     }
     if (h.width != width || h.height != height || h.camera != camera || h.seed != seed ||
@@ -619,8 +657,8 @@ struct Model {
     StateBufs& b = st[cur];
     CK(cudaMemcpy(b.i64.p, q, 5 * sizeof(int64_t) * n, cudaMemcpyHostToDevice));
     q += 5 * sizeof(int64_t) * n;
-    CK(cudaMemcpy(b.f32.p, q, 5 * sizeof(float) * n, cudaMemcpyHostToDevice));
-    q += 5 * sizeof(float) * n;
+    CK(cudaMemcpy(b.f32.p, q, f32_words() * sizeof(float) * n, cudaMemcpyHostToDevice));
+    q += f32_words() * sizeof(float) * n;
     CK(cudaMemcpy(b.u32.p, q, 3 * sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
     t_state = h.t_state;
     initialized = h.initialized != 0;
@@ -1037,6 +1075,9 @@ struct Engine {
   size_t rec_cap = 0;
   unsigned long long rec_n[2] = {0, 0};
 
+  static int32_t models_cascade(bs_model* m) { return m ? reinterpret_cast<Model*>(m)->k.cascade : 0; }
+  bool cascade() const { return !models.empty() && models[0]->k.cascade != 0; }
+
   Engine(bs_model* const* ms, const bs_field* fs, int32_t cnt, const bs_sample_rules& r) {
     require_device();
     if (cnt < 1) throw std::invalid_argument("engine: at least one sensor");
@@ -1047,6 +1088,9 @@ struct Engine {
       if (!m) throw std::invalid_argument("engine: null model");
       if (fs[i].width != m->width || fs[i].height != m->height) {
         throw std::invalid_argument("engine: each field must have its model's frame size");
+      }
+      if (m->k.cascade != models_cascade(ms[0])) {
+        throw std::invalid_argument("engine: the sensors of one engine run the same photoreceptor");
       }
       models.push_back(m);
       auto f = std::make_unique<FieldHolder>();
@@ -1110,6 +1154,7 @@ struct Engine {
 
   void set_proposal(const Mlp* p, float mg) {
     if (p && !std::isfinite(mg)) throw std::invalid_argument("engine: margin must be finite");
+    if (p && cascade()) throw std::invalid_argument("engine: the learned proposal runs with the instantaneous response");
     mlp = p;
     margin = mg;
     if (p) {
@@ -1166,7 +1211,7 @@ struct Engine {
     const int wpb = block_warps();
     const int per_sm = blocks_per_sm > 0 ? blocks_per_sm
                                          : std::max(1, mlp ? learned_engine_max_blocks_per_sm(wpb)
-                                                           : engine_max_blocks_per_sm(wpb, stage));
+                                                           : engine_max_blocks_per_sm(wpb, stage, cascade()));
     return static_cast<int>(
         std::min<uint64_t>(static_cast<uint64_t>(sms) * per_sm, (total_tiles + wpb - 1) / wpb));
   }
@@ -1179,6 +1224,7 @@ struct Engine {
       EngineSensor& e = host[i];
       e.field = fields[i]->f;
       e.consts = m->k;
+      e.cc = m->cc;
       e.in = m->soa[m->cur];
       e.out = m->soa[1 - m->cur];
       e.map = m->map;
@@ -1216,7 +1262,7 @@ struct Engine {
                               rules, l, tile_counter.p, blocks, block_warps(), tile_lw, st);
       } else {
         launch_engine(sensors_dev.p, static_cast<int>(host.size()), total_tiles, t0_dev.p, 0, windows, rules,
-                      tile_counter.p, blocks, warps_per_block, stage, tile_lw, st);
+                      tile_counter.p, blocks, warps_per_block, stage, tile_lw, cascade(), st);
       }
     }
     CK(cudaGetLastError());
@@ -1336,6 +1382,7 @@ struct Engine {
     if (warps < 0 || warps > 4) throw std::invalid_argument("engine: warps per block must lie in [1, 4]");
     if (per_sm < 0 || per_sm > 32) throw std::invalid_argument("engine: blocks_per_sm in [0, 32]");
     if (stg != 0 && stg != 16 && stg != 32) throw std::invalid_argument("engine: stage 0, 16 or 32");
+    if (stg != 0 && cascade()) throw std::invalid_argument("engine: the cascade runs unstaged (stage 0)");
     if (lw != 0 && (lw < 2 || lw > 5)) throw std::invalid_argument("engine: tile width 4, 8, 16 or 32");
     warps_per_block = warps ? warps : 4;
     blocks_per_sm = per_sm;
@@ -1346,7 +1393,7 @@ struct Engine {
 
   // Times each candidate launch shape on trial steps of `windows` windows from the current state (the models keep
   // their state) and keeps the fastest. Candidates: tile width 4, 8, 16 px (height 8, 4, 2) x warps per block 2, 4 x
-  // staging depth 0, 16 (the learned engine: tile widths only). Returns the candidates tried (ms of the second of
+  // staging depth 0, 16 (the learned engine: tile widths only; the cascade: stage 0). Returns the candidates tried (ms of the second of
   // two trial steps each); rows are {tile_lw, warps, stage, ms}.
   std::vector<std::array<double, 4>> autotune(int32_t windows, cudaStream_t s) {
     if (windows < 1) throw std::invalid_argument("engine.autotune: windows >= 1");
@@ -1357,7 +1404,7 @@ struct Engine {
     for (int lw : {2, 3, 4}) {
       for (int w : {2, 4}) {
         for (int st : {0, 16}) {
-          if (mlp && (w != 4 || st != 0)) continue;
+          if ((mlp && (w != 4 || st != 0)) || (cascade() && st != 0)) continue;
           set_launch(w, 0, st, lw);
           step(windows, s, false, nullptr, nullptr);
           step(windows, s, false, nullptr, nullptr);

@@ -44,6 +44,7 @@ struct SensorConsts {
   int32_t ideal_reset;
   int64_t refractory_ns;
   int32_t noise;          // shot or background-activity noise on
+  int32_t cascade;        // the cascade photoreceptor (cascade.cuh) instead of the instantaneous response
   double shot_rate_hz;    // r of lambda = r sqrt(100 fA / I); 0: no shot noise
   uint64_t seed;
   uint32_t camera;

@@ -31,9 +31,11 @@ typedef struct bs_sampler bs_sampler;
 typedef struct bs_engine bs_engine;
 
 /* The SensorParams rows this path reads (src/sensor/params.h:65-176), resolved from a preset and overrides by
- * the caller. photoreceptor must be 1 (instantaneous); enums as in params.h (reset_mode 0 physical / 1 ideal,
- * initial_phase 0 uniform / 1 symmetric / 2 zero). The noise_* rows are this project's shot and
- * background-activity noise (0 = off; no reference counterpart). */
+ * the caller. photoreceptor: 1 instantaneous, or 0 cascade with noise 0 (the cascade's noise lattice is not part of
+ * this build); enums as in params.h (reset_mode 0 physical / 1 ideal, initial_phase 0 uniform / 1 symmetric /
+ * 2 zero). k, tau_o, tau_sf and eps_L are the cascade's rows (read only with photoreceptor 0). The noise_* rows are
+ * this project's shot and background-activity noise (0 = off; instantaneous response only; no reference
+ * counterpart). */
 typedef struct {
   int32_t photoreceptor;
   double theta_on, theta_off, sigma_theta_on, sigma_theta_off, theta_onoff_corr, theta_floor;
@@ -47,6 +49,8 @@ typedef struct {
   int64_t clock_offset_ns;
   double hot_fraction;
   double noise_shot_rate_hz, noise_ba_median_hz, noise_ba_sigma_ln;
+  double k, tau_o, tau_sf, eps_L;
+  int32_t noise;
 } bs_params;
 
 /* Event columns of the caller's arrays (count entries each; any pointer may be NULL to skip a column), sorted by

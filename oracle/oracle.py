@@ -391,6 +391,8 @@ class Ref:
             L.ref_output_cut.argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_int64]
             L.ref_label_s1.restype = C.c_uint8
             L.ref_label_s1.argtypes = [C.c_uint8]
+            L.ref_special.restype = None
+            L.ref_special.argtypes = [C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]
             L.ref_readout_phase.restype = C.c_int64
             L.ref_readout_phase.argtypes = [C.c_uint64, C.c_uint32, C.c_int64]
             L.ref_simulate.restype = C.c_int64
@@ -432,16 +434,19 @@ class Ref:
         # Overrides the harness understands (the SensorParams rows this path reads), from a resolved SensorParams.
         KEYS = ("theta_on", "theta_off", "sigma_theta_on", "sigma_theta_off", "theta_onoff_corr", "theta_floor",
                 "refractory_s", "eps_ci", "leak_rate_hz", "leak_sigma_log10", "dark_current_fA", "dark_sigma_ln",
-                "illuminance_scale", "label_share_cut", "readout_quantum_s", "readout_delay_s")
+                "illuminance_scale", "label_share_cut", "readout_quantum_s", "readout_delay_s", "k", "tau_o", "tau_sf",
+                "eps_L")
 
         def __init__(self, params, width, height, seed, camera=0, num_threads=0):
             self.L = Ref.lib()
             self.width, self.height = width, height
             v = params.as_dict()
-            keys = list(self.KEYS) + ["reset_mode", "initial_phase"]
+            keys = list(self.KEYS) + ["reset_mode", "initial_phase", "photoreceptor", "noise"]
             vals = [float(v[k]) for k in self.KEYS] + [1.0 if v["reset_mode"] == "ideal" else 0.0,
                                                         {"uniform": 0.0, "symmetric": 1.0, "zero": 2.0}[
-                                                            v["initial_phase"]]]
+                                                            v["initial_phase"]],
+                                                        0.0 if v["photoreceptor"] == "cascade" else 1.0,
+                                                        1.0 if v["noise"] else 0.0]
             ck = (C.c_char_p * len(keys))(*[k.encode() for k in keys])
             cv = (C.c_double * len(vals))(*vals)
             self.h = self.L.ref_model_create(v["family"].encode(), ck, cv, len(keys), width, height, seed, camera,

@@ -20,6 +20,8 @@
 #include "sensor/params.h"
 #include "sensor/readout.h"
 #include "sensor/sensor_model.h"
+#include "sensor/stage1.h"
+#include "core/pmath/special.h"
 
 extern "C" {
 #include "port/oracle.h"
@@ -57,6 +59,13 @@ void set_field(sensor::SensorParams& p, const std::string& key, double v) {
   else if (key == "readout_quantum_s") p.readout_quantum_s = v;
   else if (key == "readout_delay_s") p.readout_delay_s = v;
   else if (key == "temperature_K") p.temperature_K = v;
+  else if (key == "photoreceptor") {
+    p.photoreceptor = v == 0.0 ? sensor::Photoreceptor::kCascade : sensor::Photoreceptor::kInstantaneous;
+  } else if (key == "noise") p.noise = v != 0.0;
+  else if (key == "k") p.k = v;
+  else if (key == "tau_o") p.tau_o = v;
+  else if (key == "tau_sf") p.tau_sf = v;
+  else if (key == "eps_L") p.eps_L = v;
   else throw std::invalid_argument("ref harness: unknown field " + key);
 }
 
@@ -295,6 +304,17 @@ int64_t ref_output_cut(int64_t quantum, int64_t delay, int64_t phase, int64_t of
   return balla::sensor::output_cut(balla::sensor::Readout{quantum, delay, phase, offset, drift}, t_end);
 }
 uint8_t ref_label_s1(uint8_t c3) { return balla::sensor::label_s1(c3); }
+// The reference's fp32 special functions (core/pmath) and stage-1 solve (sensor/stage1.h z_step): which 0 expm1,
+// 1..5 resid_exp(j = which - 1), 6 erfcx, 7 dawson, 8 z_step (x: z0, I0, I1, h, k per entry).
+void ref_special(int which, const float* x, size_t n, float* out) {
+  for (size_t i = 0; i < n; ++i) {
+    if (which == 0) out[i] = balla::pmath::expm1(x[i]);
+    else if (which <= 5) out[i] = balla::pmath::resid_exp(which - 1, x[i]);
+    else if (which == 6) out[i] = balla::pmath::erfcx(x[i]);
+    else if (which == 7) out[i] = balla::pmath::dawson(x[i]);
+    else out[i] = balla::sensor::z_step(x[5 * i], x[5 * i + 1], x[5 * i + 2], x[5 * i + 3], x[5 * i + 4]);
+  }
+}
 int64_t ref_readout_phase(uint64_t seed, uint32_t camera, int64_t quantum) {
   return balla::sensor::readout_phase_ns(seed, camera, quantum);
 }

@@ -1,0 +1,147 @@
+// Host build of the device's cascade processor (ballasim_b200/csrc/cascade.cuh), for CPU parity tests against
+// the reference's fp32 kernel: the same per-pixel loop over CSR runs as advance_runs_kernel, with g++ and
+// -ffp-contract=off in place of nvcc and --fmad=false.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "cascade.cuh"
+
+using namespace bs;
+
+namespace {
+
+struct VecSink {
+  std::vector<RawEvent>* out;
+  void push(const RawEvent& e) { out->push_back(e); }
+};
+
+struct Host {
+  uint32_t n;
+  std::vector<PixelMapRegs> maps;
+  std::vector<float> phi0;
+  std::vector<PixelRegs> st;
+  std::vector<CascadeRegs> cq;
+  SensorConsts k{};
+  CascadeConsts cc{};
+  int64_t t_state = 0;
+  std::vector<RawEvent> events;
+  uint64_t substeps = 0, attempts = 0, leaves = 0;
+};
+
+}  // namespace
+
+extern "C" {
+
+// consts: k, a2, a3, tau_o, tau_sf, eps_accept, eps_drop, eps_pl_base, eps_ci, label_cut, irr_max.
+void* hc_create(uint32_t n, const float* on, const float* off, const float* leak, const float* dark,
+                const float* phi0, float scale, const float* consts, int ideal_reset, int64_t refractory_ns) {
+  auto* h = new Host;
+  h->n = n;
+  h->maps.resize(n);
+  h->phi0.assign(phi0, phi0 + n);
+  for (uint32_t p = 0; p < n; ++p) {
+    h->maps[p] = PixelMapRegs{on[p], off[p], leak[p], dark[p], scale, 0.0, 0.0};
+  }
+  h->cc = CascadeConsts{consts[0], consts[1], consts[2], consts[3], consts[4], consts[5], consts[6], consts[7]};
+  h->k.eps_ci = consts[8];
+  h->k.label_cut = consts[9];
+  h->k.irr_max = consts[10];
+  h->k.ideal_reset = ideal_reset;
+  h->k.refractory_ns = refractory_ns;
+  h->k.noise = 0;
+  h->st.resize(n);
+  h->cq.resize(n);
+  return h;
+}
+
+void hc_destroy(void* hp) { delete static_cast<Host*>(hp); }
+
+void hc_init(void* hp, int64_t t0, const float* irr0) {
+  Host& h = *static_cast<Host*>(hp);
+  for (uint32_t p = 0; p < h.n; ++p) {
+    const float v = clamp_irr(irr0[p], h.k.irr_max);
+    pixel_init(h.st[p], h.maps[p], h.k, p, t0, v, h.phi0[p]);
+    cascade_init(h.cq[p], h.st[p]);
+  }
+  h.t_state = t0;
+}
+
+// One call: rows (ids[i], row_start[i], row_count[i]) of (t, irr) samples, then every pixel to t_end.
+void hc_advance(void* hp, const uint32_t* ids, size_t n_ids, const int64_t* t, const float* irr,
+                const int64_t* row_start, const int32_t* row_count, int64_t t_end) {
+  Host& h = *static_cast<Host*>(hp);
+  std::vector<int32_t> row_of(h.n, -1);
+  for (size_t i = 0; i < n_ids; ++i) row_of[ids[i]] = static_cast<int32_t>(i);
+  VecSink sink{&h.events};
+  for (uint32_t p = 0; p < h.n; ++p) {
+    PixelRegs& s = h.st[p];
+    PixelCounters c;
+    CascadeCounters cn;
+    CascadeProc<VecSink> proc{s, h.cq[p], h.maps[p], h.k, h.cc, p, sink, c, cn};
+    int64_t prev_t = h.t_state;
+    float prev_v = s.held;
+    const int32_t row = row_of[p];
+    int32_t cnt = 0;
+    if (row >= 0) {
+      cnt = row_count[row];
+      for (int32_t i = 0; i < cnt; ++i) {
+        const int64_t ti = t[row_start[row] + i];
+        const float vi = clamp_irr(irr[row_start[row] + i], h.k.irr_max);
+        if (i == 0 && ti == h.t_state) {
+          prev_v = vi;
+          continue;
+        }
+        proc.segment(Segment{prev_t, ti, prev_v, vi}, prev_t, ti);
+        prev_t = ti;
+        prev_v = vi;
+      }
+    }
+    proc.segment(Segment{prev_t, kForever, prev_v, prev_v}, prev_t, t_end);
+    if (row >= 0 && cnt > 0) s.held = prev_v;
+    h.substeps += cn.substeps;
+    h.attempts += cn.attempts;
+    h.leaves += c.leaves;
+  }
+  h.t_state = t_end;
+}
+
+size_t hc_event_count(void* hp) { return static_cast<Host*>(hp)->events.size(); }
+
+void hc_take(void* hp, RawEvent* out) {
+  Host& h = *static_cast<Host*>(hp);
+  if (!h.events.empty()) std::memcpy(out, h.events.data(), h.events.size() * sizeof(RawEvent));
+  h.events.clear();
+}
+
+// The cascade state of every pixel: z, x1, s2, s3, tv (5 floats per pixel).
+void hc_state(void* hp, float* out) {
+  Host& h = *static_cast<Host*>(hp);
+  for (uint32_t p = 0; p < h.n; ++p) {
+    const CascadeRegs& q = h.cq[p];
+    const float v[5] = {q.z, q.x1, q.s2, q.s3, q.tv};
+    std::memcpy(out + 5 * p, v, sizeof v);
+  }
+}
+
+void hc_stats(void* hp, uint64_t* out) {
+  Host& h = *static_cast<Host*>(hp);
+  out[0] = h.substeps;
+  out[1] = h.attempts;
+  out[2] = h.leaves;
+}
+
+// The special functions alone, for bitwise checks against the reference's: which 0 expm1, 1..5 resid_exp(j = which
+// - 1), 6 erfcx, 7 dawson, 8 z_step (x: z0, I0, I1, h, k per entry, 5 floats).
+void hc_special(int which, const float* x, size_t n, float* out) {
+  for (size_t i = 0; i < n; ++i) {
+    if (which == 0) out[i] = expm1_f(x[i]);
+    else if (which <= 5) out[i] = resid_exp_f(which - 1, x[i]);
+    else if (which == 6) out[i] = erfcx_f(x[i]);
+    else if (which == 7) out[i] = dawson_f(x[i]);
+    else out[i] = z_step(x[5 * i], x[5 * i + 1], x[5 * i + 2], x[5 * i + 3], x[5 * i + 4]);
+  }
+}
+
+}  // extern "C"

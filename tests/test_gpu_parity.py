@@ -7,6 +7,7 @@ import pytest
 
 from ballasim_b200 import workloads as W
 from ballasim_b200.params import resolve
+from runs import random_calls, wide_calls
 
 pytestmark = pytest.mark.gpu
 
@@ -22,30 +23,6 @@ def same_events(dev: dict, ora: dict, width: int) -> None:
         if a.dtype.kind == "f":
             a, b = a.view(np.uint32), b.view(np.uint32)
         assert np.array_equal(a, b), f"column {k} differs"
-
-
-def random_calls(rng, n, t0, calls):
-    out, t = [], t0
-    for _ in range(calls):
-        t_end = t + int(rng.integers(1, 3)) * (1 << 23) + int(rng.integers(0, 5000))
-        listed = rng.permutation(n)[: int(rng.integers(0, n + 1))].astype(np.uint32)
-        ts, vs, cnt = [], [], []
-        for _px in listed:
-            k = int(rng.integers(0, 14))
-            times = np.unique(rng.integers(t, t_end + 1, k))
-            if rng.random() < 0.3 and len(times):
-                times[0] = t
-                times = np.unique(times)
-            vals = (rng.uniform(5, 400, len(times)) * rng.choice([1, 1, 1, 3], len(times))).astype(np.float32)
-            ts.append(times.astype(np.int64))
-            vs.append(vals)
-            cnt.append(len(times))
-        tt = np.concatenate(ts) if ts else np.zeros(0, np.int64)
-        vv = np.concatenate(vs) if vs else np.zeros(0, np.float32)
-        starts = np.concatenate([[0], np.cumsum(cnt)[:-1]]).astype(np.int64) if cnt else np.zeros(0, np.int64)
-        out.append((listed, tt, vv, t_end, starts, np.array(cnt, np.int32)))
-        t = t_end
-    return out
 
 
 @pytest.mark.parametrize("overrides", [
@@ -150,14 +127,15 @@ def test_event_buffer_overflow_reruns(cuda_lib, oracle_port):
     assert dev.stats()["gpu_reruns"] >= 1
 
 
-def test_save_and_load_state_resume_bitwise(cuda_lib):
+@pytest.mark.parametrize("family,overrides", [("ideal", W.MISMATCH), ("prophesee_gen3", {"noise": False})])
+def test_save_and_load_state_resume_bitwise(cuda_lib, family, overrides):
     from ballasim_b200.sensor import SensorModel
 
     rng = np.random.default_rng(8)
     n = 10 * 10
     calls = random_calls(rng, n, 0, 4)
-    full = SensorModel("ideal", 10, 10, 4, [{"type": "constant"}], 0, overrides=W.MISMATCH)
-    part = SensorModel("ideal", 10, 10, 4, [{"type": "constant"}], 0, overrides=W.MISMATCH)
+    full = SensorModel(family, 10, 10, 4, [{"type": "constant"}], 0, overrides=overrides)
+    part = SensorModel(family, 10, 10, 4, [{"type": "constant"}], 0, overrides=overrides)
     irr0 = rng.uniform(20, 200, (n, 1)).astype(np.float32)
     full.init(0, irr0)
     part.init(0, irr0)
@@ -165,15 +143,49 @@ def test_save_and_load_state_resume_bitwise(cuda_lib):
     for c in calls[:2]:
         part.advance_runs(c[0], c[1], c[2], c[3], c[4], c[5])
     blob = part.save_state()
-    fresh = SensorModel("ideal", 10, 10, 4, [{"type": "constant"}], 0, overrides=W.MISMATCH)
+    fresh = SensorModel(family, 10, 10, 4, [{"type": "constant"}], 0, overrides=overrides)
     fresh.load_state(blob)
     rest = [fresh.advance_runs(c[0], c[1], c[2], c[3], c[4], c[5]) for c in calls[2:]]
     for a, b in zip(ev_full[2:], rest):
         for k in a:
             assert np.array_equal(a[k], b[k]), k
-    other = SensorModel("ideal", 10, 10, 5, [{"type": "constant"}], 0)
+    assert sum(len(a["t_cross_ns"]) for a in ev_full[2:]) > 10
+    other = SensorModel(family, 10, 10, 5, [{"type": "constant"}], 0, overrides=overrides)
     with pytest.raises(ValueError):
         other.load_state(blob)
+
+
+@pytest.mark.parametrize("family,overrides,calls,t0", [
+    ("prophesee_gen3", {}, random_calls, 0),
+    ("prophesee_gen3", {"leak_rate_hz": 2.0, "leak_sigma_log10": 0.1}, random_calls, 0),
+    ("prophesee_gen3", {"reset_mode": "ideal", "refractory_s": 0.0}, random_calls, 0),
+    ("prophesee_gen3", {"sigma_theta_on": 0.03, "sigma_theta_off": 0.03, "dark_sigma_ln": 0.5}, wide_calls, 0),
+    ("prophesee_gen3", {"leak_rate_hz": 1.0, "refractory_s": 0.0}, wide_calls, -123456789),
+    ("prophesee_gen3", {"refractory_s": 1e-3, "eps_L": 0.001}, wide_calls, 0),
+    ("samsung_gen3", {}, wide_calls, 0),
+])
+def test_cascade_model_equals_the_reference(cuda_lib, ref, family, overrides, calls, t0):
+    """The cascade photoreceptor (noise off) on the device, through the C ABI, gives the reference's fp32 SensorModel
+    events bit for bit on random ragged runs (host runs and device runs alike)."""
+    from ballasim_b200.sensor import SensorModel
+
+    p = resolve(family, {"noise": False, **overrides})
+    Wd, Hd, seed = 24, 20, 9 + len(overrides)
+    n = Wd * Hd
+    rng = np.random.default_rng(seed)
+    dev = SensorModel(p, Wd, Hd, seed, [{"type": "constant"}], 0)
+    ora = ref.Model(p, Wd, Hd, seed, 0)
+    irr0 = rng.uniform(5, 400, n).astype(np.float32)
+    dev.init(t0, irr0.reshape(n, 1))
+    ora.init(t0, irr0)
+    got = []
+    for ids, tt, vv, t_end, starts, cnt in calls(rng, n, t0, 6):
+        got.append(dev.advance_runs(ids, tt, vv, t_end, starts, cnt))
+        ora.advance_runs(ids, tt, vv, starts, cnt, t_end)
+    merged = {k: np.concatenate([g[k] for g in got]) for k in got[0]}
+    same_events(merged, ora.take_events(), Wd)
+    assert len(merged["t_cross_ns"]) > 500
+    assert dev.time_ns == t_end
 
 
 @pytest.mark.parametrize("case", ["edge", "blobs"])
