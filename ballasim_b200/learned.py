@@ -217,7 +217,7 @@ def renders_and_events(workload, proposal=None, margin: float = 0.25):
     from .sensor import SensorModel
 
     spec, r = workload.sensors[0], workload.rules
-    m = SensorModel(resolve("ideal", spec.overrides), spec.width, spec.height, spec.seed, [{"type": "constant"}],
+    m = SensorModel(resolve(spec.preset, spec.overrides), spec.width, spec.height, spec.seed, [{"type": "constant"}],
                     spec.camera)
     eng = Engine([(m, spec.field)], tol=r.tol, dark=r.dark, min_dt_ns=r.min_dt_ns,
                  max_refine_levels=r.max_refine_levels, l_min=r.l_min, l_max=r.l_max)

@@ -21,7 +21,7 @@ def replica(wl: W.Workload, rank: int) -> W.Workload:
         seed = s.seed + 1000 * rank
         f = (F.blobs(s.width, s.height, seed, s.field.n_blobs) if s.field.kind == F.KIND_BLOBS
              else F.tanh_edge(s.width, s.height, seed))
-        sensors.append(W.SensorSpec(s.width, s.height, seed, s.camera, dict(s.overrides), f))
+        sensors.append(W.SensorSpec(s.width, s.height, seed, s.camera, dict(s.overrides), f, s.preset))
     return W.Workload(wl.name, sensors, wl.windows, wl.rules)
 
 

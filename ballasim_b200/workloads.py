@@ -26,8 +26,9 @@ class SensorSpec:
     height: int
     seed: int
     camera: int
-    overrides: dict
+    overrides: dict  # of the preset below
     field: F.Field
+    preset: str = "ideal"
 
 
 @dataclass
@@ -80,6 +81,16 @@ def blobs_346x260(seconds: float = 2.0, seed: int = 2) -> Workload:
     """346x260 px, 16 blobs, theta 0.25/0.2 with mismatch 0.03, physical reset, refractory 100 us, noise off."""
     f = F.blobs(346, 260, seed, 16)
     return Workload("blobs16_346x260", [SensorSpec(346, 260, seed, 0, dict(MISMATCH), f)], windows_for(seconds))
+
+
+def blobs_346x260_cascade(seconds: float = 2.0, seed: int = 2) -> Workload:
+    """blobs_346x260's field and comparator laws (theta 0.25/0.2 with mismatch 0.03, physical reset, refractory
+    100 us) with the cascade photoreceptor of preset prophesee_gen3 (k 1e16 A^-1 s^-1, tau_o 25 us, tau_sf 100 us,
+    eps_L 0.002, dark current 0.21 fA), its noise lattice off."""
+    f = F.blobs(346, 260, seed, 16)
+    return Workload("blobs16_346x260_cascade",
+                    [SensorSpec(346, 260, seed, 0, {**MISMATCH, "noise": False}, f, "prophesee_gen3")],
+                    windows_for(seconds))
 
 
 def blobs_1280x720(seconds: float = 1.0, seed: int = 3) -> Workload:

@@ -509,7 +509,7 @@ def simulate_port(spec, rules, windows, t0=0, params=None):
     field's rule) and the pixel model. Returns (events, stats)."""
     from ballasim_b200.params import resolve
 
-    p = params if params is not None else resolve("ideal", spec.overrides)
+    p = params if params is not None else resolve(spec.preset, spec.overrides)
     f = spec.field
     np_ = spec.width * spec.height
     m = Port.Model(p, spec.width, spec.height, spec.seed, spec.camera)

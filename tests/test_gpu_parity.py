@@ -359,3 +359,51 @@ def test_output_stage_follows_the_reference_order(cuda_lib, ref):
     s1 = np.array([L.ref_label_s1(int(c)) for c in ev["label"][order]], np.uint8)
     assert np.array_equal(got["label"], s1)
     assert len(np.unique(ev["label"])) > 1
+
+
+@pytest.mark.parametrize("tile", [8, 4, 16])
+@pytest.mark.parametrize("case", ["blobs", "leak"])
+def test_cascade_engine_equals_the_reference_chain(cuda_lib, ref, case, tile):
+    """The fused engine with the cascade photoreceptor (noise lattice off) gives the reference's own chain
+    (WindowEngine<kHost> sampling, then the fp32 SensorModel's cascade on the runs, per window) bit for bit, over two
+    calls and any tile shape."""
+    from ballasim_b200.engine import Engine
+    from ballasim_b200.sensor import SensorModel
+
+    wl = W.small("blobs", 60, 40, 24)
+    spec, r = wl.sensors[0], wl.rules
+    over = {**W.MISMATCH, "noise": False}
+    if case == "leak":
+        over.update(leak_rate_hz=2.0, leak_sigma_log10=0.1, refractory_s=0.0)
+    p = resolve("prophesee_gen3", over)
+    want, st = ref.Model(p, spec.width, spec.height, spec.seed, spec.camera).simulate(spec.field, r, wl.windows)
+    m = SensorModel(p, spec.width, spec.height, spec.seed, [{"type": "constant"}], spec.camera)
+    eng = Engine([(m, spec.field)], tol=r.tol, dark=r.dark, min_dt_ns=r.min_dt_ns,
+                 max_refine_levels=r.max_refine_levels, l_min=r.l_min, l_max=r.l_max)
+    eng.set_launch(0, 0, 0, tile)
+    eng.start(0)
+    samples, parts = 0, []
+    for chunk in (5, wl.windows - 5):
+        s, _ = eng.run(chunk)
+        samples += s
+        parts.append(m.take_events())
+    ev = {k: np.concatenate([x[k] for x in parts]) for k in parts[0]}
+    assert samples == st["pixel_samples"]
+    same_events(ev, want, spec.width)
+    assert len(ev["t_cross_ns"]) > 100
+
+
+@pytest.mark.gpu
+def test_engine_refuses_mixed_photoreceptors_and_cascade_options(cuda_lib):
+    from ballasim_b200.engine import Engine
+    from ballasim_b200.sensor import SensorModel
+
+    wl = W.small("blobs", 32, 16, 2)
+    spec, r = wl.sensors[0], wl.rules
+    inst = SensorModel(resolve("ideal", spec.overrides), 32, 16, 1, [{"type": "constant"}], 0)
+    casc = SensorModel(resolve("prophesee_gen3", {"noise": False}), 32, 16, 2, [{"type": "constant"}], 1)
+    with pytest.raises(ValueError):
+        Engine([(inst, spec.field), (casc, spec.field)], tol=r.tol, dark=r.dark, min_dt_ns=r.min_dt_ns)
+    eng = Engine([(casc, spec.field)], tol=r.tol, dark=r.dark, min_dt_ns=r.min_dt_ns)
+    with pytest.raises(ValueError):
+        eng.set_launch(0, 0, 16, 8)
