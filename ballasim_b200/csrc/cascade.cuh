@@ -449,12 +449,67 @@ BS_HD bool cascade_settled(const CascadeConsts& cc, const CascadeState3& st, flo
          fabs_f(st.s3 - x1) <= cc.eps_drop;
 }
 
-// ---------------------------------------------------------------------------------------------
-// The processor
-// ---------------------------------------------------------------------------------------------
 struct CascadeCounters {
   uint32_t substeps = 0, attempts = 0, fallbacks = 0, quarantines = 0;
 };
+
+// The next accepted sub-step from ta inside piece pc (substep.h next_substep with pixel.h make_substep :1477-1502 and
+// quarantine :1506-1515): the rest of the piece when the cascade is settled under constant input, else the longest
+// dyadic halving that try_substep accepts; the state advances to its end (a non-finite one restarts at the steady
+// state of the current input, flagged QUARANTINED).
+BS_HD int64_t cascade_substep(const CascadeConsts& cc, CascadeRegs& q, uint32_t& flags, float i_scale,
+                              const LinearPiece& pc, int64_t ta, int64_t& h_hint, SubStep& sub, CascadeCounters& cn) {
+  const CascadeState3 st{q.z, q.s2, q.s3};
+  const float I_a = pc.at(ta);
+  ++cn.substeps;
+  sub.t_a = ta;
+  if (pc.I_a == pc.I_b && cascade_settled(cc, st, q.x1, I_a)) {
+    sub.t_b = pc.t_b;
+    const float h = static_cast<float>(pc.t_b - ta) * kNsF;
+    sub.s3 = constant_expcubic(st.s3, cc.a2, cc.a3);
+    sub.x1_a = sub.x1_b = q.x1;
+    sub.int_ku = cc.k * h / st.z;
+    sub.fallback = false;
+    if (q.tv != 0.0f) q.tv = q.tv * exp_f(-sub.int_ku);
+    return pc.t_b;
+  }
+  CascadeState3 next{};
+  int64_t tb = h_hint > 0 ? mini(pc.t_b, ta + 2 * h_hint) : pc.t_b;
+  while (true) {
+    const int64_t h_ns = tb - ta;
+    ++cn.attempts;
+    if (try_substep(cc, st, i_scale, I_a, pc.at(tb), static_cast<float>(h_ns) * kNsF, h_ns <= 1, sub, next)) break;
+    tb = ta + h_ns / 2;
+  }
+  if (tb < pc.t_b || h_hint > 0) h_hint = tb - ta;
+  sub.t_b = tb;
+  if (sub.fallback) {
+    flags |= kFlagSolverFallback;
+    ++cn.fallbacks;
+  }
+  if (!(finite_f(next.z) && next.z > 0.0f && finite_f(next.s2) && finite_f(next.s3))) {
+    const float I = pc.at(tb);
+    q.z = 1.0f / I;
+    q.x1 = -log_f(q.z * i_scale);
+    q.s2 = q.s3 = q.x1;
+    q.tv = 0.0f;
+    sub.s3 = constant_expcubic(q.s3, cc.a2, cc.a3);
+    sub.x1_a = sub.x1_b = q.x1;
+    flags |= kFlagQuarantined;
+    ++cn.quarantines;
+  } else {
+    q.z = next.z;
+    q.s2 = next.s2;
+    q.s3 = next.s3;
+    q.x1 = sub.x1_b;
+    q.tv = q.tv * exp_f(-sub.int_ku) + fabs_f(sub.x1_b - sub.x1_a);
+  }
+  return tb;
+}
+
+// ---------------------------------------------------------------------------------------------
+// The processor
+// ---------------------------------------------------------------------------------------------
 
 template <class Sink>
 struct CascadeProc {
@@ -496,58 +551,8 @@ struct CascadeProc {
     }
   }
 
-  // The next accepted sub-step from ta (substep.h next_substep with pixel.h make_substep :1477-1502).
   BS_HD int64_t make_substep(const LinearPiece& pc, int64_t ta, int64_t& h_hint, SubStep& sub) {
-    const CascadeState3 st{q.z, q.s2, q.s3};
-    const float I_a = pc.at(ta);
-    ++cn.substeps;
-    sub.t_a = ta;
-    if (pc.I_a == pc.I_b && cascade_settled(cc, st, q.x1, I_a)) {
-      sub.t_b = pc.t_b;
-      const float h = static_cast<float>(pc.t_b - ta) * kNsF;
-      sub.s3 = constant_expcubic(st.s3, cc.a2, cc.a3);
-      sub.x1_a = sub.x1_b = q.x1;
-      sub.int_ku = cc.k * h / st.z;
-      sub.fallback = false;
-      if (q.tv != 0.0f) q.tv = q.tv * exp_f(-sub.int_ku);
-      return pc.t_b;
-    }
-    CascadeState3 next{};
-    int64_t tb = h_hint > 0 ? mini(pc.t_b, ta + 2 * h_hint) : pc.t_b;
-    while (true) {
-      const int64_t h_ns = tb - ta;
-      ++cn.attempts;
-      if (try_substep(cc, st, s.i_scale, I_a, pc.at(tb), static_cast<float>(h_ns) * kNsF, h_ns <= 1, sub, next)) break;
-      tb = ta + h_ns / 2;
-    }
-    if (tb < pc.t_b || h_hint > 0) h_hint = tb - ta;
-    sub.t_b = tb;
-    if (sub.fallback) {
-      s.flags |= kFlagSolverFallback;
-      ++cn.fallbacks;
-    }
-    if (!(finite_f(next.z) && next.z > 0.0f && finite_f(next.s2) && finite_f(next.s3))) {
-      quarantine(pc.at(tb), sub);
-    } else {
-      q.z = next.z;
-      q.s2 = next.s2;
-      q.s3 = next.s3;
-      q.x1 = sub.x1_b;
-      q.tv = q.tv * exp_f(-sub.int_ku) + fabs_f(sub.x1_b - sub.x1_a);
-    }
-    return tb;
-  }
-
-  // A non-finite cascade restarts at the steady state of the current input (pixel.h:1506-1515).
-  BS_COLD void quarantine(float I, SubStep& sub) {
-    q.z = 1.0f / I;
-    q.x1 = -log_f(q.z * s.i_scale);
-    q.s2 = q.s3 = q.x1;
-    q.tv = 0.0f;
-    sub.s3 = constant_expcubic(q.s3, cc.a2, cc.a3);
-    sub.x1_a = sub.x1_b = q.x1;
-    s.flags |= kFlagQuarantined;
-    ++cn.quarantines;
+    return cascade_substep(cc, q, s.flags, s.i_scale, pc, ta, h_hint, sub, cn);
   }
 
   BS_HD float s3_at(const SubStep& sub, int64_t t) const { return sub.s3(static_cast<float>(t - sub.t_a) * kNsF); }

@@ -391,6 +391,8 @@ class Ref:
             L.ref_output_cut.argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_int64]
             L.ref_label_s1.restype = C.c_uint8
             L.ref_label_s1.argtypes = [C.c_uint8]
+            L.ref_noise_table.restype = C.c_int64
+            L.ref_noise_table.argtypes = [C.c_double] * 4 + [C.c_int, C.c_void_p, C.c_size_t]
             L.ref_special.restype = None
             L.ref_special.argtypes = [C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]
             L.ref_readout_phase.restype = C.c_int64
@@ -435,7 +437,7 @@ class Ref:
         KEYS = ("theta_on", "theta_off", "sigma_theta_on", "sigma_theta_off", "theta_onoff_corr", "theta_floor",
                 "refractory_s", "eps_ci", "leak_rate_hz", "leak_sigma_log10", "dark_current_fA", "dark_sigma_ln",
                 "illuminance_scale", "label_share_cut", "readout_quantum_s", "readout_delay_s", "k", "tau_o", "tau_sf",
-                "eps_L")
+                "eps_L", "sigma_o", "noise_leaf_level", "noise_margin_z")
 
         def __init__(self, params, width, height, seed, camera=0, num_threads=0):
             self.L = Ref.lib()

@@ -21,6 +21,7 @@
 #include "sensor/readout.h"
 #include "sensor/sensor_model.h"
 #include "sensor/stage1.h"
+#include "sensor/noise_tables.h"
 #include "core/pmath/special.h"
 
 extern "C" {
@@ -66,6 +67,9 @@ void set_field(sensor::SensorParams& p, const std::string& key, double v) {
   else if (key == "tau_o") p.tau_o = v;
   else if (key == "tau_sf") p.tau_sf = v;
   else if (key == "eps_L") p.eps_L = v;
+  else if (key == "sigma_o") p.sigma_o = v;
+  else if (key == "noise_leaf_level") p.noise_leaf_level = static_cast<int32_t>(v);
+  else if (key == "noise_margin_z") p.noise_margin_z = v;
   else throw std::invalid_argument("ref harness: unknown field " + key);
 }
 
@@ -313,6 +317,25 @@ void ref_special(int which, const float* x, size_t n, float* out) {
     else if (which == 6) out[i] = balla::pmath::erfcx(x[i]);
     else if (which == 7) out[i] = balla::pmath::dawson(x[i]);
     else out[i] = balla::sensor::z_step(x[5 * i], x[5 * i + 1], x[5 * i + 2], x[5 * i + 3], x[5 * i + 4]);
+  }
+}
+// The reference's fp32 noise-lattice tables (sensor/noise_tables.h NoiseTables, frozen diffusion): copies up to cap
+// floats; returns n_nodes * stride (stride = 18 + 47 levels).
+int64_t ref_noise_table(double kq, double a2, double a3, double sigma_o, int levels, float* out, size_t cap) {
+  try {
+    balla::sensor::NoiseModel nm{};
+    nm.kq = kq;
+    nm.a2 = a2;
+    nm.a3 = a3;
+    nm.sigma_o = sigma_o;
+    nm.levels = levels;
+    nm.margin_z = 6.0;
+    balla::sensor::NoiseTables t(nm);
+    const std::vector<float>& d = t.data32();
+    std::memcpy(out, d.data(), std::min(cap, d.size()) * sizeof(float));
+    return static_cast<int64_t>(d.size());
+  } catch (const std::exception& e) {
+    return fail(e);
   }
 }
 int64_t ref_readout_phase(uint64_t seed, uint32_t camera, int64_t quantum) {

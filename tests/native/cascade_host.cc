@@ -1,12 +1,15 @@
-// Host build of the device's cascade processor (ballasim_b200/csrc/cascade.cuh), for CPU parity tests against
-// the reference's fp32 kernel: the same per-pixel loop over CSR runs as advance_runs_kernel, with g++ and
-// -ffp-contract=off in place of nvcc and --fmad=false.
+// Host build of the device's cascade processors (ballasim_b200/csrc/cascade.cuh, lattice.cuh) and noise tables
+// (noise_build.h), for CPU parity tests against the reference's fp32 kernel: the same per-pixel loops over CSR runs
+// as advance_runs_cascade_kernel and advance_runs_lattice_kernel, with g++ and -ffp-contract=off in place of nvcc
+// and --fmad=false.
 #include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <vector>
 
 #include "cascade.cuh"
+#include "lattice.cuh"
+#include "noise_build.h"
 
 using namespace bs;
 
@@ -143,5 +146,87 @@ void hc_special(int which, const float* x, size_t n, float* out) {
     else out[i] = z_step(x[5 * i], x[5 * i + 1], x[5 * i + 2], x[5 * i + 3], x[5 * i + 4]);
   }
 }
+
+// This build's noise tables (noise_build.h): copies up to cap floats; returns n_nodes * stride.
+int64_t hc_noise_table(double kq, double a2, double a3, double sigma_o, int levels, float* out, size_t cap) {
+  const NoiseTablesH t = build_noise_tables(NoiseModelH{kq, a2, a3, sigma_o, levels});
+  std::memcpy(out, t.data.data(), std::min(cap, t.data.size()) * sizeof(float));
+  return static_cast<int64_t>(t.data.size());
+}
+
+// ---- the cascade with its noise lattice (lattice.cuh) ----
+namespace {
+struct HostLattice {
+  Host base;
+  NoiseTablesH tables;
+  NoiseTableDev view{};
+  std::vector<LatticeRegs> lat;
+};
+}  // namespace
+
+// lat: kq, sigma_o, margin_z, a2 = 1 / tau_o, a3 = 1 / tau_sf (fp64); levels; seed; camera.
+void* hl_create(uint32_t n, const float* on, const float* off, const float* leak, const float* dark, const float* phi0,
+                float scale, const float* consts, int ideal_reset, int64_t refractory_ns, const double* lat, int levels,
+                uint64_t seed, uint32_t camera) {
+  auto* h = new HostLattice;
+  Host* b = static_cast<Host*>(hc_create(n, on, off, leak, dark, phi0, scale, consts, ideal_reset, refractory_ns));
+  h->base = std::move(*b);
+  delete b;
+  h->base.k.seed = seed;
+  h->base.k.camera = camera;
+  h->tables = build_noise_tables(NoiseModelH{lat[0], lat[3], lat[4], lat[1], levels});
+  h->view = NoiseTableDev{h->tables.data.data(), h->tables.n_nodes, h->tables.stride, levels,
+                          static_cast<float>(kNoiseLnA1Min), static_cast<float>(h->tables.inv_dln),
+                          static_cast<float>(lat[2])};
+  h->lat.resize(n);
+  return h;
+}
+
+void hl_destroy(void* hp) { delete static_cast<HostLattice*>(hp); }
+
+void hl_init(void* hp, int64_t t0, const float* irr0) {
+  HostLattice& h = *static_cast<HostLattice*>(hp);
+  Host& b = h.base;
+  VecSink sink{&b.events};
+  for (uint32_t p = 0; p < b.n; ++p) {
+    const float v = clamp_irr(irr0[p], b.k.irr_max);
+    pixel_init(b.st[p], b.maps[p], b.k, p, t0, v, b.phi0[p]);
+    cascade_init(b.cq[p], b.st[p]);
+    PixelCounters c;
+    CascadeCounters cn;
+    const RunInput in{t0, v, nullptr, nullptr, 0, 0, b.k.irr_max};
+    LatticeProc<VecSink> proc{b.st[p], b.cq[p], h.lat[p], b.maps[p], b.k, b.cc, h.view, p, sink, c, cn, in};
+    proc.init(t0, b.phi0[p]);
+  }
+  b.t_state = t0;
+}
+
+void hl_advance(void* hp, const uint32_t* ids, size_t n_ids, const int64_t* t, const float* irr,
+                const int64_t* row_start, const int32_t* row_count, int64_t t_end) {
+  HostLattice& h = *static_cast<HostLattice*>(hp);
+  Host& b = h.base;
+  std::vector<int32_t> row_of(b.n, -1);
+  for (size_t i = 0; i < n_ids; ++i) row_of[ids[i]] = static_cast<int32_t>(i);
+  VecSink sink{&b.events};
+  for (uint32_t p = 0; p < b.n; ++p) {
+    const int32_t row = row_of[p];
+    const int32_t cnt = row >= 0 ? row_count[row] : 0;
+    const int64_t* tp = row >= 0 ? t + row_start[row] : nullptr;
+    const float* vp = row >= 0 ? irr + row_start[row] : nullptr;
+    const int32_t skip = cnt > 0 && tp[0] == b.t_state ? 1 : 0;
+    const RunInput in{b.t_state, b.st[p].held, tp, vp, cnt, skip, b.k.irr_max};
+    PixelCounters c;
+    CascadeCounters cn;
+    LatticeProc<VecSink> proc{b.st[p], b.cq[p], h.lat[p], b.maps[p], b.k, b.cc, h.view, p, sink, c, cn, in};
+    proc.resume();
+    proc.advance(t_end);
+    b.substeps += cn.substeps;
+    b.leaves += c.leaves;
+  }
+  b.t_state = t_end;
+}
+
+size_t hl_event_count(void* hp) { return static_cast<HostLattice*>(hp)->base.events.size(); }
+void hl_take(void* hp, RawEvent* out) { hc_take(&static_cast<HostLattice*>(hp)->base, out); }
 
 }  // extern "C"

@@ -1,7 +1,8 @@
-"""The cascade photoreceptor's device code (ballasim_b200/csrc/cascade.cuh, special.cuh) built for the host with g++
-and checked bitwise against the reference's fp32 kernel on the CPU: the special functions and z_step over wide
-sweeps, and the processor on random ragged runs against the reference's SensorModel (photoreceptor cascade, noise
-off). The same code runs on the device under nvcc --fmad=false; the gpu tests repeat the model check there."""
+"""The cascade photoreceptor's device code (ballasim_b200/csrc/cascade.cuh, special.cuh, lattice.cuh, noise_build.h)
+built for the host with g++ and checked bitwise against the reference's fp32 kernel on the CPU: the special functions
+and z_step over wide sweeps, the noise-lattice tables, and the processors on random ragged runs against the
+reference's SensorModel (photoreceptor cascade, noise lattice off and on). The same code runs on the device under
+nvcc --fmad=false; the gpu tests repeat the model checks there."""
 import ctypes as C
 import re
 import subprocess
@@ -39,6 +40,19 @@ def host(tmp_path_factory):
     H.hc_state.argtypes = [C.c_void_p, C.c_void_p]
     H.hc_destroy.argtypes = [C.c_void_p]
     H.hc_special.argtypes = [C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]
+    H.hc_noise_table.restype = C.c_int64
+    H.hc_noise_table.argtypes = [C.c_double] * 4 + [C.c_int, C.c_void_p, C.c_size_t]
+    H.hl_create.restype = C.c_void_p
+    H.hl_create.argtypes = [C.c_uint32] + [C.c_void_p] * 5 + [C.c_float, C.c_void_p, C.c_int, C.c_int64, C.c_void_p,
+                                                              C.c_int, C.c_uint64, C.c_uint32]
+    for f in ("hl_init", "hl_advance", "hl_take", "hl_destroy"):
+        getattr(H, f).restype = None
+    H.hl_init.argtypes = [C.c_void_p, C.c_int64, C.c_void_p]
+    H.hl_advance.argtypes = H.hc_advance.argtypes
+    H.hl_event_count.restype = C.c_size_t
+    H.hl_event_count.argtypes = [C.c_void_p]
+    H.hl_take.argtypes = [C.c_void_p, C.c_void_p]
+    H.hl_destroy.argtypes = [C.c_void_p]
     return H
 
 
@@ -115,10 +129,8 @@ CASES = [
 ]
 
 
-@pytest.mark.parametrize("family,overrides,calls,t0", CASES)
-def test_cascade_host_equals_the_reference(host, ref, family, overrides, calls, t0):
-    p = resolve(family, {"noise": False, **overrides})
-    W, Hh, seed = 12, 9, 5 + len(overrides)
+def _host_vs_reference(host, ref, p, calls, t0, seed, n_calls=6):
+    W, Hh = 12, 9
     n = W * Hh
     rng = np.random.default_rng(seed)
     model = ref.Model(p, W, Hh, seed)
@@ -128,22 +140,42 @@ def test_cascade_host_equals_the_reference(host, ref, family, overrides, calls, 
     arrs = [np.ascontiguousarray(mp[k], np.float32) for k in ("theta_on", "theta_off", "leak", "dark_current_fA",
                                                                "phi0")]
     cs = cascade_consts(p)
-    h = host.hc_create(n, *[a.ctypes.data for a in arrs], float(np.float32(p.illuminance_scale)), cs.ctypes.data,
-                       1 if p.reset_mode == "ideal" else 0, int(round(p.refractory_s * 1e9)))
+    lattice = bool(p.noise)
+    pre = "hl" if lattice else "hc"
+    if lattice:
+        lat = np.array([p.k * 1.602176634e-19, p.sigma_o, p.noise_margin_z, 1.0 / p.tau_o, 1.0 / p.tau_sf])
+        h = host.hl_create(n, *[a.ctypes.data for a in arrs], float(np.float32(p.illuminance_scale)), cs.ctypes.data,
+                           1 if p.reset_mode == "ideal" else 0, int(round(p.refractory_s * 1e9)), lat.ctypes.data,
+                           int(p.noise_leaf_level), seed, 0)
+    else:
+        h = host.hc_create(n, *[a.ctypes.data for a in arrs], float(np.float32(p.illuminance_scale)), cs.ctypes.data,
+                           1 if p.reset_mode == "ideal" else 0, int(round(p.refractory_s * 1e9)))
+    fn = lambda name: getattr(host, f"{pre}_{name}")  # noqa: E731
     try:
-        host.hc_init(h, t0, irr0.ctypes.data)
+        fn("init")(h, t0, irr0.ctypes.data)
         want, got = [], []
-        for ids, tt, vv, t_end, starts, cnt in calls(rng, n, t0, 6):
+        for ids, tt, vv, t_end, starts, cnt in calls(rng, n, t0, n_calls):
             model.advance_runs(ids, tt, vv, starts, cnt, t_end)
-            host.hc_advance(h, ids.ctypes.data, len(ids), np.ascontiguousarray(tt).ctypes.data,
-                            np.ascontiguousarray(vv).ctypes.data, np.ascontiguousarray(starts).ctypes.data,
-                            np.ascontiguousarray(cnt).ctypes.data, t_end)
+            fn("advance")(h, ids.ctypes.data, len(ids), np.ascontiguousarray(tt).ctypes.data,
+                          np.ascontiguousarray(vv).ctypes.data, np.ascontiguousarray(starts).ctypes.data,
+                          np.ascontiguousarray(cnt).ctypes.data, t_end)
             want.append(model.take_events())
-            m = np.zeros(host.hc_event_count(h), EV)
-            host.hc_take(h, m.ctypes.data)
+            m = np.zeros(fn("event_count")(h), EV)
+            fn("take")(h, m.ctypes.data)
             got.append(m[np.lexsort((m["pixel"], m["t"]))])
     finally:
-        host.hc_destroy(h)
+        fn("destroy")(h)
+    return W, want, got
+
+
+@pytest.mark.parametrize("family,overrides,calls,t0", CASES)
+def test_cascade_host_equals_the_reference(host, ref, family, overrides, calls, t0):
+    p = resolve(family, {"noise": False, **overrides})
+    W, want, got = _host_vs_reference(host, ref, p, calls, t0, 5 + len(overrides))
+    _same(W, want, got)
+
+
+def _same(W, want, got):
     e = {k: np.concatenate([x[k] for x in want]) for k in want[0]}
     m = np.concatenate(got)
     assert len(m) == len(e["t_cross_ns"]) > 200
@@ -153,3 +185,38 @@ def test_cascade_host_equals_the_reference(host, ref, family, overrides, calls, 
         assert np.array_equal(m[k], e[k]), k
     for k in ("ds", "dn", "dl", "l_first"):
         assert np.array_equal(m[k].view(np.uint32), np.asarray(e[k], np.float32).view(np.uint32)), k
+
+
+def test_noise_tables_equal_the_reference(host, ref):
+    """The lattice tables (noise_build.h, long double on the host) are the reference's NoiseTables, bit for bit."""
+    L = ref.lib()
+    for k, tau_o, tau_sf, sigma_o, levels in [(1e16, 25e-6, 100e-6, 0.06, 5), (1e16, 100e-6, 25e-6, 0.06, 3),
+                                              (3e15, 40e-6, 200e-6, 0.02, 7), (1e16, 25e-6, 100e-6, 0.06, 0)]:
+        kq = k * 1.602176634e-19
+        cap = 800 * (18 + 47 * levels)
+        a, b = np.zeros(cap, np.float32), np.zeros(cap, np.float32)
+        na = L.ref_noise_table(kq, 1 / tau_o, 1 / tau_sf, sigma_o, levels, a.ctypes.data, cap)
+        nb = host.hc_noise_table(kq, 1 / tau_o, 1 / tau_sf, sigma_o, levels, b.ctypes.data, cap)
+        assert na == nb > 0
+        assert np.array_equal(a[:na].view(np.uint32), b[:nb].view(np.uint32)), levels
+
+
+LATTICE_CASES = [
+    ("prophesee_gen3", {}, random_calls, 0),
+    ("prophesee_gen3", {}, random_calls, 12345),
+    ("prophesee_gen3", {"noise_leaf_level": 0}, random_calls, 777),
+    ("prophesee_gen3", {"noise_leaf_level": 3, "leak_rate_hz": 2.0, "leak_sigma_log10": 0.1}, wide_calls, 0),
+    ("prophesee_gen3", {"noise_leaf_level": 7, "reset_mode": "ideal", "refractory_s": 0.0}, random_calls, -123456789),
+    ("prophesee_gen3", {"refractory_s": 0.0, "noise_margin_z": 3.0}, wide_calls, 0),
+    ("samsung_gen3", {}, wide_calls, 65536 * 3 + 5),
+    ("prophesee_gen3", {"sigma_o": 0.2, "sigma_theta_on": 0.03}, random_calls, 0),
+]
+
+
+@pytest.mark.parametrize("family,overrides,calls,t0", LATTICE_CASES)
+def test_lattice_host_equals_the_reference(host, ref, family, overrides, calls, t0):
+    """The cascade with its noise lattice (frozen diffusion): init mid-cell and on a node, leaf levels 0 to 7, both
+    resets, the refractory time, leak, another margin z and sigma_o, negative times."""
+    p = resolve(family, {"noise": True, **overrides})
+    W, want, got = _host_vs_reference(host, ref, p, calls, t0, 5 + len(overrides) + (t0 & 7))
+    _same(W, want, got)
