@@ -31,7 +31,9 @@ class Params(C.Structure):
                                           "readout_delay_s", "clock_drift_ppm")] + \
                [("clock_offset_ns", C.c_int64), ("hot_fraction", C.c_double), ("noise_shot_rate_hz", C.c_double),
                 ("noise_ba_median_hz", C.c_double), ("noise_ba_sigma_ln", C.c_double)] + \
-               [(n, C.c_double) for n in ("k", "tau_o", "tau_sf", "eps_L")] + [("noise", C.c_int32)]
+               [(n, C.c_double) for n in ("k", "tau_o", "tau_sf", "eps_L")] + [("noise", C.c_int32)] + \
+               [("sigma_o", C.c_double), ("noise_margin_z", C.c_double), ("noise_leaf_level", C.c_int32),
+                ("noise_diffusion", C.c_int32)]
 
 
 class EventColumns(C.Structure):

@@ -16,6 +16,7 @@
 
 #include "cascade.cuh"
 #include "fields.cuh"
+#include "lattice.cuh"
 #include "learned.cuh"
 #include "pixel.cuh"
 #include "sampler.cuh"
@@ -27,6 +28,9 @@ struct StateSoA {
   float *s3_ref, *n3_ref, *dr_ref, *i_scale, *held;
   uint32_t *flags, *n_shot, *n_ba;
   float *z, *x1, *s2, *s3, *tv;  // the cascade's (null without it)
+  float* lat;                    // the noise lattice's: 7 planes of n (nk 0..2, nk1 0..2, ln_a1); null without it
+  int64_t* cell;
+  uint32_t* have_k1;
 };
 
 struct MapSoA {
@@ -88,6 +92,7 @@ struct EngineSensor {
   FieldDev field;
   SensorConsts consts;
   CascadeConsts cc;      // the cascade's constants (consts.cascade)
+  NoiseTableDev tab;     // the noise lattice's tables (data null without the lattice)
   StateSoA in, out;
   MapSoA map;
   float* carried_in;   // the sampler's carried sample (irradiance at the window start), per pixel
@@ -99,14 +104,15 @@ struct EngineSensor {
   unsigned long long* counters;
 };
 
-// Launchers (stream-ordered; no synchronization inside).
-void launch_init_counted(const SensorConsts& k, const MapSoA& map, StateSoA st, uint32_t n_pixels, int64_t t0,
-                         const float* irr0, unsigned long long* counters, cudaStream_t stream);
+// Launchers (stream-ordered; no synchronization inside). tab.data non-null: the cascade's noise lattice is on.
+void launch_init_counted(const SensorConsts& k, const CascadeConsts& cc, const NoiseTableDev& tab, const MapSoA& map,
+                         StateSoA st, uint32_t n_pixels, int64_t t0, const float* irr0, unsigned long long* counters,
+                         cudaStream_t stream);
 void launch_scatter_rows(const uint32_t* pixel, uint32_t n, int32_t* row_of, uint32_t n_pixels,
                          unsigned long long* counters, cudaStream_t stream);
 // The CSR-runs kernel of the instantaneous response, or of the cascade when k.cascade (cc its constants).
-void launch_advance_runs(const SensorConsts& k, const CascadeConsts& cc, const MapSoA& map, StateSoA in, StateSoA out,
-                         uint32_t n_pixels,
+void launch_advance_runs(const SensorConsts& k, const CascadeConsts& cc, const NoiseTableDev& tab, const MapSoA& map,
+                         StateSoA in, StateSoA out, uint32_t n_pixels,
                          const uint32_t* pixel_ids, const int32_t* row_of, const int64_t* row_start,
                          const int32_t* row_count, const int64_t* t, const float* irr, uint64_t n_samples,
                          int64_t t_state, int64_t t_end, EventBuf ev, unsigned long long* counters, int block,
@@ -126,11 +132,12 @@ void launch_field_frame(const FieldDev& f, int64_t t, uint32_t n_pixels, float* 
 // counter (work stealing) by a persistent grid. stage 0: the sampler feeds the pixel model sample by sample;
 // 16 or 32: per window the samples are staged in shared memory (that many per lane) between the two phases.
 // t0: the model time in device memory; tiles of 2^tile_lw x 2^(5 - tile_lw) pixels (tile_lw in [2, 5]).
-// cascade: every sensor runs the cascade photoreceptor (streaming form; stage is ignored).
+// cascade: 0 the instantaneous response; 1 every sensor runs the cascade photoreceptor, 2 with its noise lattice
+// (streaming form; stage is ignored).
 void launch_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t total_tiles, const int64_t* t0,
                    int32_t w0, int32_t w1, const SamplerRules& r, unsigned int* tile_counter, int blocks,
-                   int warps_per_block, int stage, int tile_lw, bool cascade, cudaStream_t stream);
-int engine_max_blocks_per_sm(int warps_per_block, int stage, bool cascade);
+                   int warps_per_block, int stage, int tile_lw, int cascade, cudaStream_t stream);
+int engine_max_blocks_per_sm(int warps_per_block, int stage, int cascade);
 // The fused engine with the learned step proposal (BF16 MLP operands and FP32 parameters in device memory):
 // the same tiles and pixel model, each window sampled by proposed power-of-two steps judged by the plain rule.
 // rec_samples / rec_steps (capacity 0: off) record every sample and every proposed step.

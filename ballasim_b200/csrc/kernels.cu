@@ -89,6 +89,31 @@ __device__ __forceinline__ void store_cascade(const StateSoA& a, uint32_t p, con
   a.tv[p] = q.tv;
 }
 
+__device__ __forceinline__ void load_lattice(const StateSoA& a, uint32_t p, uint32_t n, LatticeRegs& L) {
+  for (int i = 0; i < 3; ++i) {
+    L.nk[i] = a.lat[static_cast<size_t>(i) * n + p];
+    L.nk1[i] = a.lat[static_cast<size_t>(3 + i) * n + p];
+  }
+  L.ln_a1 = a.lat[static_cast<size_t>(6) * n + p];
+  L.cell = a.cell[p];
+  L.have_k1 = a.have_k1[p];
+}
+
+__device__ __forceinline__ void store_lattice(const StateSoA& a, uint32_t p, uint32_t n, const LatticeRegs& L) {
+  for (int i = 0; i < 3; ++i) {
+    a.lat[static_cast<size_t>(i) * n + p] = L.nk[i];
+    a.lat[static_cast<size_t>(3 + i) * n + p] = L.nk1[i];
+  }
+  a.lat[static_cast<size_t>(6) * n + p] = L.ln_a1;
+  a.cell[p] = L.cell;
+  a.have_k1[p] = L.have_k1;
+}
+
+// Drops events (the init of the noise lattice fires nothing).
+struct NullSink {
+  __device__ void push(const RawEvent&) {}
+};
+
 __device__ __forceinline__ void load_map(const MapSoA& m, uint32_t p, PixelMapRegs& r) {
   r.theta_on = m.theta_on[p];
   r.theta_off = m.theta_off[p];
@@ -114,9 +139,9 @@ __device__ __forceinline__ void warp_or(unsigned long long* dst, unsigned long l
 // ---------------------------------------------------------------------------------------------
 // init
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) init_kernel(SensorConsts k, MapSoA map, StateSoA st, uint32_t n_pixels,
-                                                   int64_t t0, const float* irr0, const uint32_t* pixel_ids,
-                                                   unsigned long long* counters) {
+__global__ void __launch_bounds__(128) init_kernel(SensorConsts k, CascadeConsts cc, NoiseTableDev tab, MapSoA map,
+                                                   StateSoA st, uint32_t n_pixels, int64_t t0, const float* irr0,
+                                                   const uint32_t* pixel_ids, unsigned long long* counters) {
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long clamps = 0, err = 0;
   if (p < n_pixels) {
@@ -132,6 +157,19 @@ __global__ void __launch_bounds__(256) init_kernel(SensorConsts k, MapSoA map, S
     if (k.cascade) {
       CascadeRegs q;
       cascade_init(q, s);
+      if (tab.data != nullptr) {
+        // The noise lattice's init (the noise at the cell's first node, the part of the cell before t0): its
+        // look-ahead sees the held input.
+        LatticeRegs L;
+        NullSink none;
+        PixelCounters c;
+        CascadeCounters cn;
+        const RunInput in{t0, v, nullptr, nullptr, 0, 0, k.irr_max};
+        LatticeProc<NullSink> proc{s, q, L, m, k, cc, tab, pixel_ids ? pixel_ids[p] : p, none, c, cn, in};
+        proc.init(t0, map.phi0[p]);
+        store_state(st, p, true, s);
+        store_lattice(st, p, n_pixels, L);
+      }
       store_cascade(st, p, q);
     }
   }
@@ -157,6 +195,7 @@ __global__ void scatter_rows_kernel(const uint32_t* pixel, uint32_t n, int32_t* 
 struct RunArgs {
   SensorConsts k;
   CascadeConsts cc;
+  NoiseTableDev tab;
   MapSoA map;
   StateSoA in, out;
   uint32_t n_pixels;
@@ -244,6 +283,69 @@ __global__ void __launch_bounds__(128) advance_runs_kernel(RunArgs a) {
   warp_add(&a.counters[kCntLeaves], c.leaves);
   warp_add(&a.counters[kCntSamples], samples);
   warp_add(&a.counters[kCntNoise], c.noise_candidates);
+  warp_or(&a.counters[kCntErrors], err);
+}
+
+// The cascade with its noise lattice on CSR runs: the row is checked first (the same errors as advance_runs_kernel),
+// then the processor reads it with random access (the lattice's look-ahead).
+__global__ void __launch_bounds__(128) advance_runs_lattice_kernel(RunArgs a) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  PixelCounters c;
+  CascadeCounters cn;
+  unsigned long long clamps = 0, samples = 0, err = 0;
+  if (p < a.n_pixels) {
+    PixelRegs s;
+    load_state(a.in, p, false, s);
+    CascadeRegs q;
+    load_cascade(a.in, p, q);
+    LatticeRegs L;
+    load_lattice(a.in, p, a.n_pixels, L);
+    PixelMapRegs m;
+    load_map(a.map, p, m);
+    const int32_t row = a.row_of != nullptr ? a.row_of[p] : -1;
+    int32_t cnt = 0;
+    const int64_t* tp = nullptr;
+    const float* vp = nullptr;
+    if (row >= 0) {
+      const int64_t s0 = a.row_start[row];
+      cnt = a.row_count[row];
+      if (cnt < 0 || s0 < 0 || static_cast<uint64_t>(s0) + static_cast<uint64_t>(cnt) > a.n_samples) {
+        err |= kErrRunRange;
+        cnt = 0;
+      } else {
+        tp = a.t + s0;
+        vp = a.irr + s0;
+        int64_t prev_t = a.t_state;
+        for (int32_t i = 0; i < cnt; ++i) {
+          const int64_t ti = __ldg(tp + i);
+          const float raw = __ldg(vp + i);
+          if (!isfinite(raw)) err |= kErrNonFinite;
+          if (!(clamp_irr(raw, a.k.irr_max) == raw)) ++clamps;
+          if (i == 0 ? ti < a.t_state : ti <= prev_t) err |= kErrOrder;
+          if (ti > a.t_end) err |= kErrAfterEnd;
+          prev_t = ti;
+        }
+        samples = static_cast<unsigned long long>(cnt);
+      }
+    }
+    if (err == 0) {
+      GlobalSink sink{a.ev, &a.counters[kCntEvents]};
+      const int32_t skip = cnt > 0 && tp[0] == a.t_state ? 1 : 0;
+      const RunInput in{a.t_state, s.held, tp, vp, cnt, skip, a.k.irr_max};
+      LatticeProc<GlobalSink> proc{s, q, L, m, a.k, a.cc, a.tab, a.pixel_ids ? a.pixel_ids[p] : p, sink, c, cn, in};
+      proc.resume();
+      proc.advance(a.t_end);
+    }
+    store_state(a.out, p, false, s);
+    store_cascade(a.out, p, q);
+    store_lattice(a.out, p, a.n_pixels, L);
+  }
+  __syncwarp();
+  warp_add(&a.counters[kCntClamps], clamps);
+  warp_add(&a.counters[kCntPieces], c.pieces);
+  warp_add(&a.counters[kCntLeaves], c.leaves);
+  warp_add(&a.counters[kCntSamples], samples);
+  warp_add(&a.counters[kCntSubsteps], cn.substeps);
   warp_or(&a.counters[kCntErrors], err);
 }
 
@@ -639,6 +741,170 @@ __global__ void __launch_bounds__(128) engine_cascade_kernel(EngineArgs a) {
   }
 }
 
+// The fused engine with the cascade's noise lattice. A cell's look-ahead needs the cell's input up to its end, so
+// the window's samples are buffered from the last one at or before the current time to the first one at or after
+// the cell's end, and the cell then runs on that buffer. A window's last sample is at its end, so each window is
+// one call, as in the reference's engine (a cell that crosses the window end sees the held input beyond it).
+// kCellBuf bounds the buffer: the engine refuses min_dt_ns < 4096 with the lattice (a cell then holds at most 16
+// sample intervals).
+constexpr int kCellBuf = 20;
+
+struct CellInput {
+  int64_t t_w;
+  const uint32_t* dt;  // offsets from t_w, the first at or before the processed range
+  const float* v;      // clamped values
+  int32_t count;
+  BS_HD int n_aug() const { return count; }
+  BS_HD int64_t time(int i) const { return t_w + dt[i]; }
+  BS_HD float value(int i) const { return v[i]; }
+  BS_HD int segment_at(int64_t tt) const {
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) / 2;
+      if (time(mid) <= tt) lo = mid;
+      else hi = mid - 1;
+    }
+    return lo;
+  }
+  BS_HD int segment_of(int seg, int64_t tt) const {
+    while (seg < count - 1 && time(seg + 1) <= tt) ++seg;
+    return seg;
+  }
+  BS_HD int64_t segment_end(int seg) const { return seg + 1 < count ? time(seg + 1) : kForever; }
+  BS_HD float group_value(int seg, int64_t tt) const {
+    if (seg + 1 >= count) return v[seg];
+    const int64_t t0 = time(seg), t1 = time(seg + 1);
+    const float f = static_cast<float>(tt - t0) / static_cast<float>(t1 - t0);
+    return v[seg] + (v[seg + 1] - v[seg]) * f;
+  }
+};
+
+struct LatticeFeed {
+  LatticeProc<GlobalSink, CellInput>* proc;
+  CellInput* in;
+  uint32_t* dt;
+  float* v;
+  int64_t t_w, t_cur, t_end;
+  float irr_max;
+  float last_raw;
+  bool overflow;
+  __device__ __forceinline__ void start(float carried) {
+    last_raw = carried;
+    dt[0] = 0;
+    v[0] = clamp_irr(carried, irr_max);
+    in->count = 1;
+    t_cur = t_w;
+  }
+  // Runs [t_cur, t_to) on the buffer, then drops the samples before the last one at or before t_to.
+  __device__ __forceinline__ void run_to(int64_t t_to) {
+    proc->advance_range(t_cur, t_to);
+    t_cur = t_to;
+    int keep = 0;
+    while (keep + 1 < in->count && t_w + dt[keep + 1] <= t_to) ++keep;
+    if (keep > 0) {
+      for (int i = keep; i < in->count; ++i) {
+        dt[i - keep] = dt[i];
+        v[i - keep] = v[i];
+      }
+      in->count -= keep;
+    }
+  }
+  __device__ __forceinline__ void operator()(uint32_t d, float val) {
+    last_raw = val;
+    if (in->count == kCellBuf) {
+      overflow = true;
+      return;
+    }
+    dt[in->count] = d;
+    v[in->count] = clamp_irr(val, irr_max);
+    ++in->count;
+    const int64_t t = t_w + d;
+    while (t_cur < t_end) {
+      const int64_t tc1 = ((t_cur >> kNoiseCellLog2) + 1) * kNoiseCellNs;
+      if (t < tc1) break;
+      run_to(mini(tc1, t_end));
+    }
+  }
+  __device__ __forceinline__ void finish() {
+    if (t_cur < t_end) run_to(t_end);
+  }
+};
+
+__global__ void __launch_bounds__(128) engine_lattice_kernel(EngineArgs a) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const int64_t t0 = *a.t0;
+  for (;;) {
+    uint32_t tile = 0;
+    if (lane == 0) tile = atomicAdd(a.tile_counter, 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if (tile >= a.total_tiles) break;
+    int si = 0;
+    while (si + 1 < a.n_sensors && a.sensors[si + 1].tile0 <= tile) ++si;
+    const EngineSensor& S = a.sensors[si];
+    const uint32_t local = tile - S.tile0;
+    uint32_t x, y;
+    tile_xy(local, S.tiles_x, a.tile_lw, lane, x, y);
+    const bool have = x < S.width && y < S.height;
+    const uint32_t n_px = S.width * S.height;
+    const uint32_t p = have ? y * S.width + x : 0u;
+    PixelRegs s;
+    CascadeRegs q;
+    LatticeRegs L;
+    PixelMapRegs m;
+    float carried = 0.0f;
+    if (have) {
+      load_state(S.in, p, false, s);
+      load_cascade(S.in, p, q);
+      load_lattice(S.in, p, n_px, L);
+      load_map(S.map, p, m);
+      carried = S.carried_in[p];
+    }
+    PixelCounters c;
+    CascadeCounters cn;
+    unsigned long long samples = 0, err = 0;
+    GlobalSink sink{S.ev, &S.counters[kCntEvents]};
+    uint32_t buf_dt[kCellBuf];
+    float buf_v[kCellBuf];
+    CellInput in{0, buf_dt, buf_v, 0};
+    LatticeProc<GlobalSink, CellInput> proc{s, q, L, m, S.consts, S.cc, S.tab, p, sink, c, cn, in};
+    if (have) proc.resume();
+    const FieldDev& f = S.field;
+    __shared__ uint16_t lists[4][kMaxListed];
+    uint16_t* my_list = lists[threadIdx.x >> 5];
+    for (int32_t w = a.w0; w < a.w1; ++w) {
+      const int64_t t_w = t0 + static_cast<int64_t>(w) * kWindowNs;
+      const BlobList list = warp_blob_list(f, have, x, y, t_w, t_w + kWindowNs, my_list);
+      if (have && err == 0) {
+        const int level = field_level(f, list, x, y, t_w, a.r.l_min, a.r.l_max);
+        in.t_w = t_w;
+        LatticeFeed feed{&proc, &in, buf_dt, buf_v, t_w, t_w, t_w + kWindowNs, S.consts.irr_max, carried, false};
+        feed.start(carried);
+        auto render = [&](uint32_t dt) { return field_eval(f, list, x, y, t_w + dt); };
+        samples += sample_pixel_window(a.r, level, carried, false, render, feed);
+        if (feed.overflow) {
+          err |= kErrRunRange;
+        } else {
+          feed.finish();
+          s.held = buf_v[in.count - 1];
+        }
+        carried = feed.last_raw;
+      }
+      __syncwarp();
+    }
+    if (have) {
+      store_state(S.out, p, false, s);
+      store_cascade(S.out, p, q);
+      store_lattice(S.out, p, n_px, L);
+      S.carried_out[p] = carried;
+    }
+    warp_add(&S.counters[kCntPieces], c.pieces);
+    warp_add(&S.counters[kCntLeaves], c.leaves);
+    warp_add(&S.counters[kCntSamples], samples);
+    warp_add(&S.counters[kCntSubsteps], cn.substeps);
+    warp_or(&S.counters[kCntErrors], err);
+  }
+}
+
 // The engine in two phases per window: phase A runs every lane's sampler walk and stages its samples (dt, v) in
 // shared memory, kStage per lane (lane-minor, so a warp's stores and loads hit 32 banks); phase B feeds every lane's
 // staged samples to its pixel model. Each phase is one compact loop that all lanes run together, instead of the
@@ -921,11 +1187,12 @@ void launch_midpoint_eta(float tol, float dark, int32_t g, const float* m_min, c
   midpoint_eta_kernel<<<(n + 255) / 256, 256, 0, stream>>>(p, ea, em, eb, n, eta, exceeds);
 }
 
-void launch_init_counted(const SensorConsts& k, const MapSoA& map, StateSoA st, uint32_t n_pixels, int64_t t0,
-                         const float* irr0, unsigned long long* counters, cudaStream_t stream) {
-  const int block = 256;
+void launch_init_counted(const SensorConsts& k, const CascadeConsts& cc, const NoiseTableDev& tab, const MapSoA& map,
+                         StateSoA st, uint32_t n_pixels, int64_t t0, const float* irr0, unsigned long long* counters,
+                         cudaStream_t stream) {
+  const int block = 128;
   const unsigned grid = (n_pixels + block - 1) / block;
-  init_kernel<<<grid, block, 0, stream>>>(k, map, st, n_pixels, t0, irr0, nullptr, counters);
+  init_kernel<<<grid, block, 0, stream>>>(k, cc, tab, map, st, n_pixels, t0, irr0, nullptr, counters);
 }
 
 void launch_scatter_rows(const uint32_t* pixel, uint32_t n, int32_t* row_of, uint32_t n_pixels,
@@ -934,16 +1201,17 @@ void launch_scatter_rows(const uint32_t* pixel, uint32_t n, int32_t* row_of, uin
   scatter_rows_kernel<<<(n + 255) / 256, 256, 0, stream>>>(pixel, n, row_of, n_pixels, counters);
 }
 
-void launch_advance_runs(const SensorConsts& k, const CascadeConsts& cc, const MapSoA& map, StateSoA in, StateSoA out,
-                         uint32_t n_pixels, const uint32_t* pixel_ids, const int32_t* row_of, const int64_t* row_start,
-                         const int32_t* row_count, const int64_t* t, const float* irr, uint64_t n_samples,
-                         int64_t t_state, int64_t t_end, EventBuf ev, unsigned long long* counters, int block,
-                         cudaStream_t stream) {
-  RunArgs a{k, cc, map, in, out, n_pixels, pixel_ids, row_of, row_start, row_count, t, irr, n_samples, t_state, t_end,
-            ev, counters};
+void launch_advance_runs(const SensorConsts& k, const CascadeConsts& cc, const NoiseTableDev& tab, const MapSoA& map,
+                         StateSoA in, StateSoA out, uint32_t n_pixels, const uint32_t* pixel_ids, const int32_t* row_of,
+                         const int64_t* row_start, const int32_t* row_count, const int64_t* t, const float* irr,
+                         uint64_t n_samples, int64_t t_state, int64_t t_end, EventBuf ev, unsigned long long* counters,
+                         int block, cudaStream_t stream) {
+  RunArgs a{k, cc, tab, map, in, out, n_pixels, pixel_ids, row_of, row_start, row_count, t, irr, n_samples, t_state,
+            t_end, ev, counters};
   if (block <= 0) block = 128;
   const unsigned grid = (n_pixels + block - 1) / block;
-  if (k.cascade) advance_runs_cascade_kernel<<<grid, block, 0, stream>>>(a);
+  if (k.cascade && tab.data != nullptr) advance_runs_lattice_kernel<<<grid, block, 0, stream>>>(a);
+  else if (k.cascade) advance_runs_cascade_kernel<<<grid, block, 0, stream>>>(a);
   else advance_runs_kernel<<<grid, block, 0, stream>>>(a);
 }
 
@@ -978,17 +1246,20 @@ void launch_field_frame(const FieldDev& f, int64_t t, uint32_t n_pixels, float* 
 
 void launch_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t total_tiles, const int64_t* t0,
                    int32_t w0, int32_t w1, const SamplerRules& r, unsigned int* tile_counter, int blocks,
-                   int warps_per_block, int stage, int tile_lw, bool cascade, cudaStream_t stream) {
+                   int warps_per_block, int stage, int tile_lw, int cascade, cudaStream_t stream) {
   EngineArgs a{sensors_dev, n_sensors, total_tiles, t0, w0, w1, r, tile_counter, static_cast<uint32_t>(tile_lw)};
-  if (cascade) engine_cascade_kernel<<<blocks, warps_per_block * 32, 0, stream>>>(a);
+  if (cascade == 2) engine_lattice_kernel<<<blocks, warps_per_block * 32, 0, stream>>>(a);
+  else if (cascade == 1) engine_cascade_kernel<<<blocks, warps_per_block * 32, 0, stream>>>(a);
   else if (stage == 16) engine_kernel_staged<16><<<blocks, warps_per_block * 32, 0, stream>>>(a);
   else if (stage == 32) engine_kernel_staged<32><<<blocks, warps_per_block * 32, 0, stream>>>(a);
   else engine_kernel<<<blocks, warps_per_block * 32, 0, stream>>>(a);
 }
 
-int engine_max_blocks_per_sm(int warps_per_block, int stage, bool cascade) {
+int engine_max_blocks_per_sm(int warps_per_block, int stage, int cascade) {
   int n = 0;
-  if (cascade) {
+  if (cascade == 2) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_lattice_kernel, warps_per_block * 32, 0);
+  } else if (cascade == 1) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_cascade_kernel, warps_per_block * 32, 0);
   } else if (stage == 16) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel_staged<16>, warps_per_block * 32, 0);

@@ -176,13 +176,19 @@ uint64_t fnv1a(const void* data, size_t n, uint64_t h = 0xcbf29ce484222325ull) {
 // device state
 // ---------------------------------------------------------------------------------------------
 struct StateBufs {
-  DevBuf<int64_t> i64;   // 5 x n: t_ref, t_search, blind_until, t_shot, t_ba
-  DevBuf<float> f32;     // 5 x n: s3_ref, n3_ref, dr_ref, i_scale, held; with the cascade 5 x n more: z, x1, s2, s3, tv
-  DevBuf<uint32_t> u32;  // 3 x n: flags, n_shot, n_ba
-  StateSoA soa(size_t n, bool cascade) {
-    i64.ensure(5 * n);
-    f32.ensure((cascade ? 10 : 5) * n);
-    u32.ensure(3 * n);
+  DevBuf<int64_t> i64;   // 5 x n: t_ref, t_search, blind_until, t_shot, t_ba; with the lattice 1 x n more: cell
+  DevBuf<float> f32;     // 5 x n: s3_ref, n3_ref, dr_ref, i_scale, held; with the cascade 5 x n more: z, x1, s2, s3,
+                         // tv; with the lattice 7 x n more: nk 0..2, nk1 0..2, ln_a1
+  DevBuf<uint32_t> u32;  // 3 x n: flags, n_shot, n_ba; with the lattice 1 x n more: have_k1
+  static size_t i64_words(int mode) { return mode == 2 ? 6 : 5; }
+  static size_t f32_words(int mode) { return mode == 2 ? 17 : mode == 1 ? 10 : 5; }
+  static size_t u32_words(int mode) { return mode == 2 ? 4 : 3; }
+  // mode 0: the instantaneous response, 1: the cascade, 2: the cascade with its noise lattice.
+  StateSoA soa(size_t n, int mode) {
+    const bool cascade = mode != 0;
+    i64.ensure(i64_words(mode) * n);
+    f32.ensure(f32_words(mode) * n);
+    u32.ensure(u32_words(mode) * n);
     StateSoA s;
     s.t_ref = i64.p;
     s.t_search = i64.p + n;
@@ -203,6 +209,9 @@ struct StateBufs {
     s.s2 = c ? c + 2 * n : nullptr;
     s.s3 = c ? c + 3 * n : nullptr;
     s.tv = c ? c + 4 * n : nullptr;
+    s.lat = mode == 2 ? f32.p + 10 * n : nullptr;
+    s.cell = mode == 2 ? i64.p + 5 * n : nullptr;
+    s.have_k1 = mode == 2 ? u32.p + 3 * n : nullptr;
     return s;
   }
 };
@@ -237,6 +246,8 @@ struct Model {
   HostMaps maps;
   SensorConsts k{};
   CascadeConsts cc{};
+  DevBuf<float> tables;   // the noise lattice's (noise_build.h), on the device
+  NoiseTableDev tab{};    // data null without the lattice
   cudaStream_t own = nullptr;
   DevBuf<float> mapf;    // 6 x n
   DevBuf<double> mapd;   // 2 x n
@@ -296,10 +307,19 @@ struct Model {
       cc.eps_accept = static_cast<float>(eps_h / 1.5);
       cc.eps_drop = static_cast<float>(std::max(eps_h / 1024.0, 32.0 * 0x1p-23));
       cc.eps_pl_base = static_cast<float>(p.eps_L / 8.0);
+      if (p.noise != 0) {
+        // The noise model of the lattice (src/sensor/sensor_model.cpp:260-268): k q with q the elementary charge.
+        const NoiseTablesH t = build_noise_tables(
+            NoiseModelH{p.k * 1.602176634e-19, 1.0 / p.tau_o, 1.0 / p.tau_sf, p.sigma_o, p.noise_leaf_level});
+        tables.ensure(t.data.size());
+        CK(cudaMemcpy(tables.p, t.data.data(), t.data.size() * sizeof(float), cudaMemcpyHostToDevice));
+        tab = NoiseTableDev{tables.p, t.n_nodes, t.stride, t.levels, static_cast<float>(kNoiseLnA1Min),
+                            static_cast<float>(t.inv_dln), static_cast<float>(p.noise_margin_z)};
+      }
     }
     upload_maps();
-    soa[0] = st[0].soa(n, k.cascade != 0);
-    soa[1] = st[1].soa(n, k.cascade != 0);
+    soa[0] = st[0].soa(n, mode());
+    soa[1] = st[1].soa(n, mode());
     row_of.ensure(n);
     counters.ensure(kCntWords);
     counters_h.ensure(kCntWords);
@@ -318,10 +338,14 @@ struct Model {
       throw std::invalid_argument("SensorParams: photoreceptor must be 'cascade' or 'instantaneous'");
     }
     if (p.photoreceptor == 0) {
-      if (p.noise != 0) {
+      if (p.noise != 0 && p.noise_diffusion != 0) {
         throw std::invalid_argument(
-            "SensorModel: this build runs the cascade photoreceptor without its noise lattice (noise = false)");
+            "SensorModel: this build runs the noise lattice with frozen diffusion (accuracy.noise_diffusion frozen)");
       }
+      if (p.noise != 0 && (p.noise_leaf_level < 0 || p.noise_leaf_level > 10)) {
+        throw std::invalid_argument("SensorParams: noise_leaf_level must lie in [0, 10]");
+      }
+      if (p.noise != 0 && !(p.sigma_o >= 0.0)) throw std::invalid_argument("SensorParams: sigma_o must be >= 0");
       if (p.noise_shot_rate_hz > 0.0 || p.noise_ba_median_hz > 0.0) {
         throw std::invalid_argument("SensorModel: shot and background-activity noise run with the instantaneous "
                                     "response only");
@@ -395,7 +419,7 @@ struct Model {
 
   void init_device(int64_t t0, const float* irr0_dev, cudaStream_t s, const float* host_copy) {
     CK(cudaMemsetAsync(counters.p, 0, kCntWords * sizeof(unsigned long long), s));
-    launch_init_counted(k, map, soa[cur], n, t0, irr0_dev, counters.p, s);
+    launch_init_counted(k, cc, tab, map, soa[cur], n, t0, irr0_dev, counters.p, s);
     CK(cudaGetLastError());
     read_counters(s);
     if (counters_h.p[kCntErrors] & kErrNonFinite) {
@@ -450,7 +474,7 @@ struct Model {
       CK(cudaMemsetAsync(row_of.p, 0xFF, n * sizeof(int32_t), s));
       launch_scatter_rows(r.pixel, static_cast<uint32_t>(r.n), row_of.p, n, counters.p, s);
       CK(cudaEventRecord(timer.a, s));
-      launch_advance_runs(k, cc, map, soa[cur], soa[1 - cur], n, nullptr, r.n ? row_of.p : nullptr, r.row_start,
+      launch_advance_runs(k, cc, tab, map, soa[cur], soa[1 - cur], n, nullptr, r.n ? row_of.p : nullptr, r.row_start,
                           r.row_count, r.t, r.irr, r.n_samples, t_state, t_end,
                           EventBuf{events.p, static_cast<unsigned long long>(event_cap)}, counters.p, block, s);
       CK(cudaGetLastError());
@@ -623,8 +647,13 @@ struct Model {
     uint32_t initialized, bytes_per_pixel;
   };
   static constexpr uint32_t kMagic = 0x32304253;  // "SB02"
-  size_t f32_words() const { return k.cascade ? 10 : 5; }
-  uint32_t bytes_per_pixel() const { return static_cast<uint32_t>(5 * 8 + f32_words() * 4 + 3 * 4); }
+  int mode() const { return k.cascade == 0 ? 0 : (p.noise != 0 ? 2 : 1); }
+  size_t i64_words() const { return StateBufs::i64_words(mode()); }
+  size_t f32_words() const { return StateBufs::f32_words(mode()); }
+  size_t u32_words() const { return StateBufs::u32_words(mode()); }
+  uint32_t bytes_per_pixel() const {
+    return static_cast<uint32_t>(i64_words() * 8 + f32_words() * 4 + u32_words() * 4);
+  }
   size_t state_bytes() const { return sizeof(Header) + static_cast<size_t>(n) * bytes_per_pixel(); }
   uint64_t fingerprint() const { return fnv1a(&p, sizeof(p)); }
 
@@ -634,11 +663,11 @@ struct Model {
     std::memcpy(out, &h, sizeof(h));
     uint8_t* q = out + sizeof(h);
     const StateBufs& b = st[cur];
-    CK(cudaMemcpy(q, b.i64.p, 5 * sizeof(int64_t) * n, cudaMemcpyDeviceToHost));
-    q += 5 * sizeof(int64_t) * n;
+    CK(cudaMemcpy(q, b.i64.p, i64_words() * sizeof(int64_t) * n, cudaMemcpyDeviceToHost));
+    q += i64_words() * sizeof(int64_t) * n;
     CK(cudaMemcpy(q, b.f32.p, f32_words() * sizeof(float) * n, cudaMemcpyDeviceToHost));
     q += f32_words() * sizeof(float) * n;
-    CK(cudaMemcpy(q, b.u32.p, 3 * sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(q, b.u32.p, u32_words() * sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
   }
 
   void load(const uint8_t* data, size_t bytes) {
@@ -655,11 +684,11 @@ struct Model {
     initialized = false;
     const uint8_t* q = data + sizeof(h);
     StateBufs& b = st[cur];
-    CK(cudaMemcpy(b.i64.p, q, 5 * sizeof(int64_t) * n, cudaMemcpyHostToDevice));
-    q += 5 * sizeof(int64_t) * n;
+    CK(cudaMemcpy(b.i64.p, q, i64_words() * sizeof(int64_t) * n, cudaMemcpyHostToDevice));
+    q += i64_words() * sizeof(int64_t) * n;
     CK(cudaMemcpy(b.f32.p, q, f32_words() * sizeof(float) * n, cudaMemcpyHostToDevice));
     q += f32_words() * sizeof(float) * n;
-    CK(cudaMemcpy(b.u32.p, q, 3 * sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b.u32.p, q, u32_words() * sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
     t_state = h.t_state;
     initialized = h.initialized != 0;
     last_events = 0;
@@ -1075,8 +1104,9 @@ struct Engine {
   size_t rec_cap = 0;
   unsigned long long rec_n[2] = {0, 0};
 
-  static int32_t models_cascade(bs_model* m) { return m ? reinterpret_cast<Model*>(m)->k.cascade : 0; }
-  bool cascade() const { return !models.empty() && models[0]->k.cascade != 0; }
+  static int32_t models_cascade(bs_model* m) { return m ? reinterpret_cast<Model*>(m)->mode() : 0; }
+  // 0 the instantaneous response, 1 the cascade, 2 the cascade with its noise lattice (every sensor alike).
+  int cascade() const { return models.empty() ? 0 : models[0]->mode(); }
 
   Engine(bs_model* const* ms, const bs_field* fs, int32_t cnt, const bs_sample_rules& r) {
     require_device();
@@ -1089,8 +1119,11 @@ struct Engine {
       if (fs[i].width != m->width || fs[i].height != m->height) {
         throw std::invalid_argument("engine: each field must have its model's frame size");
       }
-      if (m->k.cascade != models_cascade(ms[0])) {
-        throw std::invalid_argument("engine: the sensors of one engine run the same photoreceptor");
+      if (m->mode() != models_cascade(ms[0])) {
+        throw std::invalid_argument("engine: the sensors of one engine run the same photoreceptor and noise model");
+      }
+      if (m->mode() == 2 && r.min_dt_ns < 4096) {
+        throw std::invalid_argument("engine: the noise lattice needs min_dt_ns >= 4096 (at most 16 samples a cell)");
       }
       models.push_back(m);
       auto f = std::make_unique<FieldHolder>();
@@ -1225,6 +1258,7 @@ struct Engine {
       e.field = fields[i]->f;
       e.consts = m->k;
       e.cc = m->cc;
+      e.tab = m->tab;
       e.in = m->soa[m->cur];
       e.out = m->soa[1 - m->cur];
       e.map = m->map;

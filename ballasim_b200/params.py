@@ -3,8 +3,8 @@
 
 The family priors are configuration data that a drop-in must reproduce value for value (the same preset must
 mean the same sensor); they are listed here as data. This path runs the instantaneous log response
-(``photoreceptor = "instantaneous"``) with constant light groups, and the cascade photoreceptor without its noise
-lattice (``photoreceptor = "cascade"``, ``noise = False``); SensorModel refuses the lattice.
+(``photoreceptor = "instantaneous"``) with constant light groups, and the cascade photoreceptor with or without its
+noise lattice (``photoreceptor = "cascade"``; the lattice with frozen diffusion).
 
 Three rows are this project's own (no reference counterpart, off unless set): ``noise_shot_rate_hz`` (shot-noise
 event rate at a photocurrent of 100 fA; the rate scales as 1/sqrt(I)), ``noise_ba_median_hz`` and

@@ -2,7 +2,7 @@
 
 ``SensorModel(params, width, height, seed, light_groups, camera, num_threads=0, precision=None, overrides=None,
 device='cuda', roi=None)`` runs BallaSim's pixel model (the instantaneous response, or the cascade photoreceptor
-without its noise lattice) on the B200 through the C ABI; its events
+with or without its noise lattice) on the B200 through the C ABI; its events
 are the reference's CPU fp32 path's, bit for bit (the reference asserts the same of its own GPU path,
 src/sensor/sensor_cuda.h:1-3). This build runs device 'cuda', precision 'fp32', one constant light group and no
 region of interest; other values raise ValueError. Errors map as the reference's: ValueError for refused input
@@ -33,9 +33,12 @@ def params_struct(p: SensorParams) -> _lib.Params:
                  "refractory_s", "eps_ci", "leak_rate_hz", "leak_sigma_log10", "leak_ea_eV", "dark_current_fA",
                  "dark_sigma_ln", "dark_ea_eV", "temperature_K", "reference_temperature_K", "illuminance_scale",
                  "label_share_cut", "readout_quantum_s", "readout_delay_s", "clock_drift_ppm", "hot_fraction",
-                 "noise_shot_rate_hz", "noise_ba_median_hz", "noise_ba_sigma_ln", "k", "tau_o", "tau_sf", "eps_L"):
+                 "noise_shot_rate_hz", "noise_ba_median_hz", "noise_ba_sigma_ln", "k", "tau_o", "tau_sf", "eps_L",
+                 "sigma_o", "noise_margin_z"):
         setattr(s, name, float(v[name]))
     s.noise = 1 if v["noise"] else 0
+    s.noise_leaf_level = int(v["noise_leaf_level"])
+    s.noise_diffusion = 1 if v["noise_diffusion"] == "transient" else 0
     s.reset_mode = 1 if v["reset_mode"] == "ideal" else 0
     s.initial_phase = {"uniform": 0, "symmetric": 1, "zero": 2}[v["initial_phase"]]
     s.clock_offset_ns = int(v["clock_offset_ns"])
@@ -87,9 +90,10 @@ class SensorModel:
             raise ValueError("SensorModel: this build has no region-of-interest models")
         self._groups = _check_light_groups(light_groups)
         self._params = resolve(params, overrides)
-        if self._params.photoreceptor == "cascade" and self._params.noise:
-            raise ValueError("SensorModel: this build runs the cascade photoreceptor without its noise lattice "
-                             "(noise = false)")
+        if self._params.photoreceptor == "cascade" and self._params.noise and \
+                self._params.noise_diffusion != "frozen":
+            raise ValueError("SensorModel: this build runs the noise lattice with frozen diffusion "
+                             "(accuracy.noise_diffusion = 'frozen')")
         if self._params.photoreceptor == "cascade" and self._params.noise_on():
             raise ValueError("SensorModel: shot and background-activity noise run with the instantaneous response only")
         self._width, self._height, self._seed, self._camera = int(width), int(height), int(seed), int(camera)

@@ -93,6 +93,15 @@ def blobs_346x260_cascade(seconds: float = 2.0, seed: int = 2) -> Workload:
                     windows_for(seconds))
 
 
+def blobs_346x260_lattice(seconds: float = 2.0, seed: int = 2) -> Workload:
+    """blobs_346x260_cascade with the cascade's in-path noise lattice on (preset prophesee_gen3's full model: sigma_o
+    0.06, leaf level 5, margin z 6, frozen diffusion)."""
+    f = F.blobs(346, 260, seed, 16)
+    return Workload("blobs16_346x260_lattice",
+                    [SensorSpec(346, 260, seed, 0, {**MISMATCH, "noise": True}, f, "prophesee_gen3")],
+                    windows_for(seconds))
+
+
 def blobs_1280x720(seconds: float = 1.0, seed: int = 3) -> Workload:
     """1280x720 px, 256 blobs, the mismatch sensor with leak 0.1 Hz, shot and background-activity noise."""
     f = F.blobs(1280, 720, seed, 256)

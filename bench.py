@@ -2,7 +2,8 @@
 
 One step = one pass of the hot path over the workload: every sensor initialized at t0 from its seeded analytic
 field, then every window sampled (dyadic lattice + eta_L refinement) and sensed (the instantaneous pixel model, or
-the cascade photoreceptor in workload blobs_346x260_cascade), in the fused engine. At N = 1 the workload is the 346 x 260 sensor (16 blobs, 2.0 s = 239 windows, mismatch 0.03,
+the cascade photoreceptor in workloads blobs_346x260_cascade and, with its noise lattice, blobs_346x260_lattice), in
+the fused engine. At N = 1 the workload is the 346 x 260 sensor (16 blobs, 2.0 s = 239 windows, mismatch 0.03,
 refractory 100 us, noise off); --workload picks another. With N GPUs (torchrun, one rank per GPU) each rank runs
 its own replica of the workload (independent sensors, seeds offset by rank): weak scaling, no collective on the
 data path; value = all ranks' pixel-samples / the slowest rank's device time.
@@ -38,6 +39,7 @@ WORKLOADS = {
     "blobs_1280x720": W.blobs_1280x720,
     "six_sensors": W.six_sensors,
     "blobs_346x260_cascade": W.blobs_346x260_cascade,
+    "blobs_346x260_lattice": W.blobs_346x260_lattice,
 }
 METRIC = "pixel-samples/s"
 L2_BYTES = 126 * 1024 * 1024
@@ -129,7 +131,8 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     r = wl.rules
     models = [SensorModel(resolve(s.preset, s.overrides), s.width, s.height, s.seed, [{"type": "constant"}], s.camera)
               for s in wl.sensors]
-    cascade = resolve(wl.sensors[0].preset, wl.sensors[0].overrides).photoreceptor == "cascade"
+    p0 = resolve(wl.sensors[0].preset, wl.sensors[0].overrides)
+    cascade, lattice = p0.photoreceptor == "cascade", p0.photoreceptor == "cascade" and bool(p0.noise)
     eng = Engine([(m, s.field) for m, s in zip(models, wl.sensors)], tol=r.tol, dark=r.dark, min_dt_ns=r.min_dt_ns,
                  max_refine_levels=r.max_refine_levels, l_min=r.l_min, l_max=r.l_max)
     if args.warps or args.blocks_per_sm or args.stage or args.tile_width:
@@ -225,7 +228,8 @@ def run_ours(args, rank: int, world: int) -> dict | None:
         "clocks": {k: v for k, v in clk.summary().items() if k != "samples"},
         "e2e": {"value": samples_all / e2e_s if e2e_times else None, "unit": "pixel-samples/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
-        "roofline": {"kernel": ("engine_cascade_kernel" if cascade else "engine_kernel") +
+        "roofline": {"kernel": (("engine_lattice_kernel" if lattice else "engine_cascade_kernel") if cascade
+                                else "engine_kernel") +
                                " (sampler + pixel model fused, runs kept on chip)", "bound": "hbm",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": hbm_kind, "traffic": NCU_TRAFFIC_PER_LAUNCH.get(wl.name), "algorithmic_bytes_per_launch": alg,

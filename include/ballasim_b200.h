@@ -31,11 +31,12 @@ typedef struct bs_sampler bs_sampler;
 typedef struct bs_engine bs_engine;
 
 /* The SensorParams rows this path reads (src/sensor/params.h:65-176), resolved from a preset and overrides by
- * the caller. photoreceptor: 1 instantaneous, or 0 cascade with noise 0 (the cascade's noise lattice is not part of
- * this build); enums as in params.h (reset_mode 0 physical / 1 ideal, initial_phase 0 uniform / 1 symmetric /
- * 2 zero). k, tau_o, tau_sf and eps_L are the cascade's rows (read only with photoreceptor 0). The noise_* rows are
- * this project's shot and background-activity noise (0 = off; instantaneous response only; no reference
- * counterpart). */
+ * the caller. photoreceptor: 1 instantaneous or 0 cascade; enums as in params.h (reset_mode 0 physical / 1 ideal,
+ * initial_phase 0 uniform / 1 symmetric / 2 zero, noise_diffusion 0 frozen / 1 transient). k, tau_o, tau_sf, eps_L
+ * and noise (the cascade's in-path noise lattice) with sigma_o, noise_margin_z, noise_leaf_level and
+ * noise_diffusion are the cascade's rows (read only with photoreceptor 0; the lattice runs frozen diffusion). The
+ * noise_shot_rate_hz / noise_ba_* rows are this project's shot and background-activity noise (0 = off;
+ * instantaneous response only; no reference counterpart). */
 typedef struct {
   int32_t photoreceptor;
   double theta_on, theta_off, sigma_theta_on, sigma_theta_off, theta_onoff_corr, theta_floor;
@@ -51,6 +52,8 @@ typedef struct {
   double noise_shot_rate_hz, noise_ba_median_hz, noise_ba_sigma_ln;
   double k, tau_o, tau_sf, eps_L;
   int32_t noise;
+  double sigma_o, noise_margin_z;
+  int32_t noise_leaf_level, noise_diffusion;
 } bs_params;
 
 /* Event columns of the caller's arrays (count entries each; any pointer may be NULL to skip a column), sorted by

@@ -127,7 +127,8 @@ def test_event_buffer_overflow_reruns(cuda_lib, oracle_port):
     assert dev.stats()["gpu_reruns"] >= 1
 
 
-@pytest.mark.parametrize("family,overrides", [("ideal", W.MISMATCH), ("prophesee_gen3", {"noise": False})])
+@pytest.mark.parametrize("family,overrides", [("ideal", W.MISMATCH), ("prophesee_gen3", {"noise": False}),
+                                              ("prophesee_gen3", {})])
 def test_save_and_load_state_resume_bitwise(cuda_lib, family, overrides):
     from ballasim_b200.sensor import SensorModel
 
@@ -163,10 +164,16 @@ def test_save_and_load_state_resume_bitwise(cuda_lib, family, overrides):
     ("prophesee_gen3", {"leak_rate_hz": 1.0, "refractory_s": 0.0}, wide_calls, -123456789),
     ("prophesee_gen3", {"refractory_s": 1e-3, "eps_L": 0.001}, wide_calls, 0),
     ("samsung_gen3", {}, wide_calls, 0),
+    ("prophesee_gen3", {"noise": True}, random_calls, 12345),
+    ("prophesee_gen3", {"noise": True, "noise_leaf_level": 3, "leak_rate_hz": 2.0, "leak_sigma_log10": 0.1},
+     wide_calls, 0),
+    ("prophesee_gen3", {"noise": True, "noise_leaf_level": 7, "reset_mode": "ideal", "refractory_s": 0.0},
+     random_calls, -123456789),
+    ("samsung_gen3", {"noise": True, "sigma_o": 0.2}, wide_calls, 65536 * 3 + 5),
 ])
 def test_cascade_model_equals_the_reference(cuda_lib, ref, family, overrides, calls, t0):
-    """The cascade photoreceptor (noise off) on the device, through the C ABI, gives the reference's fp32 SensorModel
-    events bit for bit on random ragged runs (host runs and device runs alike)."""
+    """The cascade photoreceptor on the device (with its noise lattice where noise is on), through the C ABI, gives
+    the reference's fp32 SensorModel events bit for bit on random ragged runs."""
     from ballasim_b200.sensor import SensorModel
 
     p = resolve(family, {"noise": False, **overrides})
@@ -362,7 +369,7 @@ def test_output_stage_follows_the_reference_order(cuda_lib, ref):
 
 
 @pytest.mark.parametrize("tile", [8, 4, 16])
-@pytest.mark.parametrize("case", ["blobs", "leak"])
+@pytest.mark.parametrize("case", ["blobs", "leak", "lattice", "lattice_leak"])
 def test_cascade_engine_equals_the_reference_chain(cuda_lib, ref, case, tile):
     """The fused engine with the cascade photoreceptor (noise lattice off) gives the reference's own chain
     (WindowEngine<kHost> sampling, then the fp32 SensorModel's cascade on the runs, per window) bit for bit, over two
@@ -372,8 +379,8 @@ def test_cascade_engine_equals_the_reference_chain(cuda_lib, ref, case, tile):
 
     wl = W.small("blobs", 60, 40, 24)
     spec, r = wl.sensors[0], wl.rules
-    over = {**W.MISMATCH, "noise": False}
-    if case == "leak":
+    over = {**W.MISMATCH, "noise": case.startswith("lattice")}
+    if case.endswith("leak"):
         over.update(leak_rate_hz=2.0, leak_sigma_log10=0.1, refractory_s=0.0)
     p = resolve("prophesee_gen3", over)
     want, st = ref.Model(p, spec.width, spec.height, spec.seed, spec.camera).simulate(spec.field, r, wl.windows)

@@ -89,4 +89,5 @@ def test_sensor_model_argument_checks():
     with pytest.raises(ValueError):
         SensorModel("ideal", 8, 8, 1, [{"type": "fourier", "f0_hz": 100, "a": [0.1], "phi": [0]}], 0)
     with pytest.raises(ValueError):
-        SensorModel("prophesee_gen3", 8, 8, 1, [{"type": "constant"}], 0)  # the cascade's noise lattice is not built
+        SensorModel("prophesee_gen3", 8, 8, 1, [{"type": "constant"}], 0,
+                    overrides={"noise_diffusion": "transient"})  # the lattice runs frozen diffusion only
