@@ -12,8 +12,10 @@
 // Philox(seed, purpose, camera, pixel, node time): noise and events do not depend on the sample schedule.
 //
 // The processor reads its input as the reference's kernel does (a run with the held sample at the model time,
-// random access for the look-ahead) and runs the general path only; the reference's quiet-cell shortcut performs
-// the same operations (pixel.h:1399-1406), so the results are the same bits.
+// random access for the look-ahead) and runs the general path for every cell: the reference's quiet-cell shortcut
+// performs the same operations (pixel.h:1399-1406, the same bits), but on the device it splits a warp between two
+// code paths, which measured slower. The interpolated table blocks of the last rate and the settled rate of the last
+// z are kept (pixel.h:1320-1376 kCacheBlocks and settled_rate's memo): a settled pixel reuses them cell after cell.
 #pragma once
 
 #include "cascade.cuh"
@@ -374,6 +376,12 @@ struct LatticeProc {
   int seg = 0;
   float hc0[4] = {0.0f, 0.0f, 0.0f, 0.0f};
   float margin0 = 0.0f;
+  // The blocks of the last rate looked up (step Phi and chol, the level-0 margin) and the settled rate of the last z.
+  bool cache_valid = false;
+  float cache_ln = 0.0f;
+  float cache_step[12];
+  float cache_m0[23];
+  float settled_z = -1.0f, settled_ln = 0.0f;
 
   BS_HD Tri nk() const { return Tri{{L.nk[0], L.nk[1], L.nk[2]}}; }
   BS_HD Tri nk1() const { return Tri{{L.nk1[0], L.nk1[1], L.nk1[2]}}; }
@@ -404,15 +412,33 @@ struct LatticeProc {
 
   // The lattice draw of n at the cell's end at the cell's rate, and the level-0 hull (pixel.h:1336-1376).
   BS_HD void draw_lattice(int64_t tc1) {
-    float xi[3], step[12];
+    float xi[3];
     normals3_f(k.seed, kPurposeNoise, k.camera, pixel, static_cast<uint64_t>(tc1), xi);
-    const NoisePosF pos = noise_pos(tab, L.ln_a1);
-    noise_lookup(tab, pos, NoiseLayoutF::kStepPhi, 12, step);
-    lattice_step(step, step + 6, L.nk, xi, L.nk1);
-    float m0[23];
-    if (tab.levels > 0) noise_lookup(tab, pos, NoiseLayoutF{tab.levels}.margin(0), 23, m0);
-    level0(m0);
+    if (!cache_valid || cache_ln != L.ln_a1) {
+      const NoisePosF pos = noise_pos(tab, L.ln_a1);
+      cache_ln = L.ln_a1;
+      noise_lookup(tab, pos, NoiseLayoutF::kStepPhi, 12, cache_step);
+      if (tab.levels > 0) noise_lookup(tab, pos, NoiseLayoutF{tab.levels}.margin(0), 23, cache_m0);
+      cache_valid = true;
+    }
+    lattice_step(cache_step, cache_step + 6, L.nk, xi, L.nk1);
+    level0(cache_m0);
     L.have_k1 = 1;
+  }
+
+  // A settled pixel under constant input for the whole cell: a1 = k u = k / z (pixel.h:1320-1333).
+  BS_HD void settled_rate(int64_t t, float pre, int64_t tc1) {
+    if (pre == 0.0f && q.z == settled_z) {
+      L.ln_a1 = settled_ln;
+      return;
+    }
+    const float h_cell = static_cast<float>(kNoiseCellNs) * kNsF;
+    const float int_ku = pre + cc.k * static_cast<float>(tc1 - t) * kNsF / q.z;
+    L.ln_a1 = log_f(int_ku / h_cell);
+    if (pre == 0.0f) {
+      settled_z = q.z;
+      settled_ln = L.ln_a1;
+    }
   }
 
   // The cell's frozen rate from a z-only look-ahead to its end (pixel.h:1272-1316 and settled_rate :1320-1333);
@@ -425,8 +451,7 @@ struct LatticeProc {
     const CascadeState3 st{q.z, q.s2, q.s3};
     const float h_cell = static_cast<float>(kNoiseCellNs) * kNsF;
     if (pc.t_b == tc1 && pc.I_a == pc.I_b && cascade_settled(cc, st, q.x1, pc.I_a)) {
-      const float int_ku = pre + cc.k * static_cast<float>(tc1 - t) * kNsF / q.z;
-      L.ln_a1 = log_f(int_ku / h_cell);
+      settled_rate(t, pre, tc1);
     } else {
       float z = q.z, int_kI = 0.0f;
       while (true) {
