@@ -14,8 +14,9 @@
 // The processor reads its input as the reference's kernel does (a run with the held sample at the model time,
 // random access for the look-ahead) and runs the general path for every cell: the reference's quiet-cell shortcut
 // performs the same operations (pixel.h:1399-1406, the same bits), but on the device it splits a warp between two
-// code paths, which measured slower. The interpolated table blocks of the last rate and the settled rate of the last
-// z are kept (pixel.h:1320-1376 kCacheBlocks and settled_rate's memo): a settled pixel reuses them cell after cell.
+// code paths, which measured slower. Like the reference's device kernels, the table blocks are interpolated at every
+// draw rather than kept per rate (keeping them raised the kernel to 255 registers and measured slower); the settled
+// rate of the last z is kept (settled_rate's memo, pixel.h:1320-1333).
 #pragma once
 
 #include "cascade.cuh"
@@ -376,11 +377,7 @@ struct LatticeProc {
   int seg = 0;
   float hc0[4] = {0.0f, 0.0f, 0.0f, 0.0f};
   float margin0 = 0.0f;
-  // The blocks of the last rate looked up (step Phi and chol, the level-0 margin) and the settled rate of the last z.
-  bool cache_valid = false;
-  float cache_ln = 0.0f;
-  float cache_step[12];
-  float cache_m0[23];
+  // The settled rate of the last z.
   float settled_z = -1.0f, settled_ln = 0.0f;
 
   BS_HD Tri nk() const { return Tri{{L.nk[0], L.nk[1], L.nk[2]}}; }
@@ -412,17 +409,14 @@ struct LatticeProc {
 
   // The lattice draw of n at the cell's end at the cell's rate, and the level-0 hull (pixel.h:1336-1376).
   BS_HD void draw_lattice(int64_t tc1) {
-    float xi[3];
+    float xi[3], step[12];
     normals3_f(k.seed, kPurposeNoise, k.camera, pixel, static_cast<uint64_t>(tc1), xi);
-    if (!cache_valid || cache_ln != L.ln_a1) {
-      const NoisePosF pos = noise_pos(tab, L.ln_a1);
-      cache_ln = L.ln_a1;
-      noise_lookup(tab, pos, NoiseLayoutF::kStepPhi, 12, cache_step);
-      if (tab.levels > 0) noise_lookup(tab, pos, NoiseLayoutF{tab.levels}.margin(0), 23, cache_m0);
-      cache_valid = true;
-    }
-    lattice_step(cache_step, cache_step + 6, L.nk, xi, L.nk1);
-    level0(cache_m0);
+    const NoisePosF pos = noise_pos(tab, L.ln_a1);
+    noise_lookup(tab, pos, NoiseLayoutF::kStepPhi, 12, step);
+    lattice_step(step, step + 6, L.nk, xi, L.nk1);
+    float m0[23];
+    if (tab.levels > 0) noise_lookup(tab, pos, NoiseLayoutF{tab.levels}.margin(0), 23, m0);
+    level0(m0);
     L.have_k1 = 1;
   }
 

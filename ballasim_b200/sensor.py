@@ -94,6 +94,10 @@ class SensorModel:
                 self._params.noise_diffusion != "frozen":
             raise ValueError("SensorModel: this build runs the noise lattice with frozen diffusion "
                              "(accuracy.noise_diffusion = 'frozen')")
+        if self._params.photoreceptor == "cascade" and self._params.noise and \
+                self._params.initial_state == "stationary":
+            raise ValueError("SensorModel: this build starts the noise lattice from the phase law "
+                             "(accuracy.initial_state = 'phase'); the stationary probe is not built")
         if self._params.photoreceptor == "cascade" and self._params.noise_on():
             raise ValueError("SensorModel: shot and background-activity noise run with the instantaneous response only")
         self._width, self._height, self._seed, self._camera = int(width), int(height), int(seed), int(camera)
