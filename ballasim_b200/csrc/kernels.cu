@@ -905,6 +905,161 @@ __global__ void __launch_bounds__(128) engine_lattice_kernel(EngineArgs a) {
   }
 }
 
+// The lattice engine in two phases per window, so that a warp's lanes run the lattice's code together: phase A runs
+// every lane's sampler walk and stages its window's samples in shared memory (kLatStage per lane, lane-minor, slot 0
+// the carried sample); phase B runs every lane's 128 cells from its staged samples. A window with more samples than
+// kLatStage is redone by its lane in the streaming form (the same samples: the walk is deterministic).
+constexpr int kLatStage = 32;
+
+struct StagedInput {
+  int64_t t_w;
+  const uint32_t* dt;  // entry i at dt[i * 32]
+  const float* v;      // clamped values, entry i at v[i * 32]
+  int32_t count;
+  BS_HD int n_aug() const { return count; }
+  BS_HD int64_t time(int i) const { return t_w + dt[i * 32]; }
+  BS_HD float value(int i) const { return v[i * 32]; }
+  BS_HD int segment_at(int64_t tt) const {
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) / 2;
+      if (time(mid) <= tt) lo = mid;
+      else hi = mid - 1;
+    }
+    return lo;
+  }
+  BS_HD int segment_of(int seg, int64_t tt) const {
+    while (seg < count - 1 && time(seg + 1) <= tt) ++seg;
+    return seg;
+  }
+  BS_HD int64_t segment_end(int seg) const { return seg + 1 < count ? time(seg + 1) : kForever; }
+  BS_HD float group_value(int seg, int64_t tt) const {
+    if (seg + 1 >= count) return value(seg);
+    const int64_t t0 = time(seg), t1 = time(seg + 1);
+    const float f = static_cast<float>(tt - t0) / static_cast<float>(t1 - t0);
+    const float v0 = value(seg), v1 = value(seg + 1);
+    return v0 + (v1 - v0) * f;
+  }
+};
+
+struct LatticeStageFeed {
+  uint32_t* dt;
+  float* v;
+  float irr_max;
+  int32_t n;
+  bool overflow;
+  float last_raw;
+  __device__ __forceinline__ void start(float carried) {
+    last_raw = carried;
+    dt[0] = 0;
+    v[0] = clamp_irr(carried, irr_max);
+    n = 1;
+  }
+  __device__ __forceinline__ void operator()(uint32_t d, float val) {
+    last_raw = val;
+    if (n == kLatStage) {
+      overflow = true;
+      return;
+    }
+    dt[n * 32] = d;
+    v[n * 32] = clamp_irr(val, irr_max);
+    ++n;
+  }
+};
+
+__global__ void __launch_bounds__(128) engine_lattice_kernel_staged(EngineArgs a) {
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const int64_t t0 = *a.t0;
+  __shared__ uint16_t lists[4][kMaxListed];
+  __shared__ uint32_t st_dt[4][kLatStage][32];
+  __shared__ float st_v[4][kLatStage][32];
+  uint16_t* my_list = lists[warp];
+  for (;;) {
+    uint32_t tile = 0;
+    if (lane == 0) tile = atomicAdd(a.tile_counter, 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if (tile >= a.total_tiles) break;
+    int si = 0;
+    while (si + 1 < a.n_sensors && a.sensors[si + 1].tile0 <= tile) ++si;
+    const EngineSensor& S = a.sensors[si];
+    const uint32_t local = tile - S.tile0;
+    uint32_t x, y;
+    tile_xy(local, S.tiles_x, a.tile_lw, lane, x, y);
+    const bool have = x < S.width && y < S.height;
+    const uint32_t n_px = S.width * S.height;
+    const uint32_t p = have ? y * S.width + x : 0u;
+    PixelRegs s;
+    CascadeRegs q;
+    LatticeRegs L;
+    PixelMapRegs m;
+    float carried = 0.0f;
+    if (have) {
+      load_state(S.in, p, false, s);
+      load_cascade(S.in, p, q);
+      load_lattice(S.in, p, n_px, L);
+      load_map(S.map, p, m);
+      carried = S.carried_in[p];
+    }
+    PixelCounters c;
+    CascadeCounters cn;
+    unsigned long long samples = 0, err = 0;
+    GlobalSink sink{S.ev, &S.counters[kCntEvents]};
+    const FieldDev& f = S.field;
+    uint32_t* my_dt = &st_dt[warp][0][lane];
+    float* my_v = &st_v[warp][0][lane];
+    for (int32_t w = a.w0; w < a.w1; ++w) {
+      const int64_t t_w = t0 + static_cast<int64_t>(w) * kWindowNs;
+      const BlobList list = warp_blob_list(f, have, x, y, t_w, t_w + kWindowNs, my_list);
+      auto render = [&](uint32_t dt) { return field_eval(f, list, x, y, t_w + dt); };
+      int level = 0;
+      LatticeStageFeed stage{my_dt, my_v, S.consts.irr_max, 0, false, carried};
+      if (have && err == 0) {
+        level = field_level(f, list, x, y, t_w, a.r.l_min, a.r.l_max);
+        stage.start(carried);
+        samples += sample_pixel_window(a.r, level, carried, false, render, stage);
+      }
+      __syncwarp();
+      if (have && err == 0) {
+        if (!stage.overflow) {
+          const StagedInput in{t_w, my_dt, my_v, stage.n};
+          LatticeProc<GlobalSink, StagedInput> proc{s, q, L, m, S.consts, S.cc, S.tab, p, sink, c, cn, in};
+          proc.resume();
+          proc.advance_range(t_w, t_w + kWindowNs);
+          s.held = my_v[(stage.n - 1) * 32];
+        } else {
+          uint32_t buf_dt[kCellBuf];
+          float buf_v[kCellBuf];
+          CellInput in{t_w, buf_dt, buf_v, 0};
+          LatticeProc<GlobalSink, CellInput> proc{s, q, L, m, S.consts, S.cc, S.tab, p, sink, c, cn, in};
+          proc.resume();
+          LatticeFeed feed{&proc, &in, buf_dt, buf_v, t_w, t_w, t_w + kWindowNs, S.consts.irr_max, carried, false};
+          feed.start(carried);
+          sample_pixel_window(a.r, level, carried, false, render, feed);
+          if (feed.overflow) {
+            err |= kErrRunRange;
+          } else {
+            feed.finish();
+            s.held = buf_v[in.count - 1];
+          }
+        }
+        carried = stage.last_raw;
+      }
+      __syncwarp();
+    }
+    if (have) {
+      store_state(S.out, p, false, s);
+      store_cascade(S.out, p, q);
+      store_lattice(S.out, p, n_px, L);
+      S.carried_out[p] = carried;
+    }
+    warp_add(&S.counters[kCntPieces], c.pieces);
+    warp_add(&S.counters[kCntLeaves], c.leaves);
+    warp_add(&S.counters[kCntSamples], samples);
+    warp_add(&S.counters[kCntSubsteps], cn.substeps);
+    warp_or(&S.counters[kCntErrors], err);
+  }
+}
+
 // The engine in two phases per window: phase A runs every lane's sampler walk and stages its samples (dt, v) in
 // shared memory, kStage per lane (lane-minor, so a warp's stores and loads hit 32 banks); phase B feeds every lane's
 // staged samples to its pixel model. Each phase is one compact loop that all lanes run together, instead of the
@@ -1248,7 +1403,8 @@ void launch_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t tota
                    int32_t w0, int32_t w1, const SamplerRules& r, unsigned int* tile_counter, int blocks,
                    int warps_per_block, int stage, int tile_lw, int cascade, cudaStream_t stream) {
   EngineArgs a{sensors_dev, n_sensors, total_tiles, t0, w0, w1, r, tile_counter, static_cast<uint32_t>(tile_lw)};
-  if (cascade == 2) engine_lattice_kernel<<<blocks, warps_per_block * 32, 0, stream>>>(a);
+  if (cascade == 2 && stage != 0) engine_lattice_kernel_staged<<<blocks, warps_per_block * 32, 0, stream>>>(a);
+  else if (cascade == 2) engine_lattice_kernel<<<blocks, warps_per_block * 32, 0, stream>>>(a);
   else if (cascade == 1) engine_cascade_kernel<<<blocks, warps_per_block * 32, 0, stream>>>(a);
   else if (stage == 16) engine_kernel_staged<16><<<blocks, warps_per_block * 32, 0, stream>>>(a);
   else if (stage == 32) engine_kernel_staged<32><<<blocks, warps_per_block * 32, 0, stream>>>(a);
@@ -1257,7 +1413,9 @@ void launch_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t tota
 
 int engine_max_blocks_per_sm(int warps_per_block, int stage, int cascade) {
   int n = 0;
-  if (cascade == 2) {
+  if (cascade == 2 && stage != 0) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_lattice_kernel_staged, warps_per_block * 32, 0);
+  } else if (cascade == 2) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_lattice_kernel, warps_per_block * 32, 0);
   } else if (cascade == 1) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_cascade_kernel, warps_per_block * 32, 0);

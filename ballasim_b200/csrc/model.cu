@@ -1416,7 +1416,10 @@ struct Engine {
     if (warps < 0 || warps > 4) throw std::invalid_argument("engine: warps per block must lie in [1, 4]");
     if (per_sm < 0 || per_sm > 32) throw std::invalid_argument("engine: blocks_per_sm in [0, 32]");
     if (stg != 0 && stg != 16 && stg != 32) throw std::invalid_argument("engine: stage 0, 16 or 32");
-    if (stg != 0 && cascade()) throw std::invalid_argument("engine: the cascade runs unstaged (stage 0)");
+    if (stg != 0 && cascade() == 1) throw std::invalid_argument("engine: the cascade runs unstaged (stage 0)");
+    if (stg != 0 && stg != 32 && cascade() == 2) {
+      throw std::invalid_argument("engine: the noise lattice runs unstaged (stage 0) or staged 32 deep (stage 32)");
+    }
     if (lw != 0 && (lw < 2 || lw > 5)) throw std::invalid_argument("engine: tile width 4, 8, 16 or 32");
     warps_per_block = warps ? warps : 4;
     blocks_per_sm = per_sm;
@@ -1438,7 +1441,8 @@ struct Engine {
     for (int lw : {2, 3, 4}) {
       for (int w : {2, 4}) {
         for (int st : {0, 16}) {
-          if ((mlp && (w != 4 || st != 0)) || (cascade() && st != 0)) continue;
+          if ((mlp && (w != 4 || st != 0)) || (cascade() == 1 && st != 0)) continue;
+          if (cascade() == 2 && st != 0) st = 32;
           set_launch(w, 0, st, lw);
           step(windows, s, false, nullptr, nullptr);
           step(windows, s, false, nullptr, nullptr);

@@ -369,25 +369,31 @@ def test_output_stage_follows_the_reference_order(cuda_lib, ref):
 
 
 @pytest.mark.parametrize("tile", [8, 4, 16])
-@pytest.mark.parametrize("case", ["blobs", "leak", "lattice", "lattice_leak"])
+@pytest.mark.parametrize("case", ["blobs", "leak", "lattice", "lattice_leak", "lattice_staged", "lattice_leak_staged",
+                                  "lattice_dense_staged"])
 def test_cascade_engine_equals_the_reference_chain(cuda_lib, ref, case, tile):
-    """The fused engine with the cascade photoreceptor (noise lattice off) gives the reference's own chain
-    (WindowEngine<kHost> sampling, then the fp32 SensorModel's cascade on the runs, per window) bit for bit, over two
-    calls and any tile shape."""
+    """The fused engine with the cascade photoreceptor, with and without its noise lattice, gives the reference's own
+    chain (WindowEngine<kHost> sampling, then the fp32 SensorModel on the runs, per window) bit for bit, over two
+    calls and any tile shape; the staged lattice engine too, also where every window overflows its stage (lattice
+    levels from 6: at least 65 samples a window) and is redone streaming."""
+    import dataclasses
+
     from ballasim_b200.engine import Engine
     from ballasim_b200.sensor import SensorModel
 
     wl = W.small("blobs", 60, 40, 24)
     spec, r = wl.sensors[0], wl.rules
+    if "dense" in case:
+        r = dataclasses.replace(r, l_min=6)
     over = {**W.MISMATCH, "noise": case.startswith("lattice")}
-    if case.endswith("leak"):
+    if "leak" in case:
         over.update(leak_rate_hz=2.0, leak_sigma_log10=0.1, refractory_s=0.0)
     p = resolve("prophesee_gen3", over)
     want, st = ref.Model(p, spec.width, spec.height, spec.seed, spec.camera).simulate(spec.field, r, wl.windows)
     m = SensorModel(p, spec.width, spec.height, spec.seed, [{"type": "constant"}], spec.camera)
     eng = Engine([(m, spec.field)], tol=r.tol, dark=r.dark, min_dt_ns=r.min_dt_ns,
                  max_refine_levels=r.max_refine_levels, l_min=r.l_min, l_max=r.l_max)
-    eng.set_launch(0, 0, 0, tile)
+    eng.set_launch(0, 0, 32 if case.endswith("staged") else 0, tile)
     eng.start(0)
     samples, parts = 0, []
     for chunk in (5, wl.windows - 5):
