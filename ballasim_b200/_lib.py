@@ -33,7 +33,8 @@ class Params(C.Structure):
                 ("noise_ba_median_hz", C.c_double), ("noise_ba_sigma_ln", C.c_double)] + \
                [(n, C.c_double) for n in ("k", "tau_o", "tau_sf", "eps_L")] + [("noise", C.c_int32)] + \
                [("sigma_o", C.c_double), ("noise_margin_z", C.c_double), ("noise_leaf_level", C.c_int32),
-                ("noise_diffusion", C.c_int32)]
+                ("noise_diffusion", C.c_int32), ("initial_state", C.c_int32), ("stationary_probe_pixels", C.c_int32),
+                ("stationary_burnin_ns", C.c_int64)]
 
 
 class EventColumns(C.Structure):

@@ -18,6 +18,7 @@
 
 #include "../../include/ballasim_b200.h"
 #include "device.h"
+#include "stationary.h"
 
 namespace bs {
 namespace {
@@ -248,6 +249,7 @@ struct Model {
   CascadeConsts cc{};
   DevBuf<float> tables;   // the noise lattice's (noise_build.h), on the device
   NoiseTableDev tab{};    // data null without the lattice
+  std::vector<float> tables_host;  // and on the host (the stationary start's histories)
   cudaStream_t own = nullptr;
   DevBuf<float> mapf;    // 6 x n
   DevBuf<double> mapd;   // 2 x n
@@ -313,6 +315,7 @@ struct Model {
             NoiseModelH{p.k * 1.602176634e-19, 1.0 / p.tau_o, 1.0 / p.tau_sf, p.sigma_o, p.noise_leaf_level});
         tables.ensure(t.data.size());
         CK(cudaMemcpy(tables.p, t.data.data(), t.data.size() * sizeof(float), cudaMemcpyHostToDevice));
+        tables_host = t.data;
         tab = NoiseTableDev{tables.p, t.n_nodes, t.stride, t.levels, static_cast<float>(kNoiseLnA1Min),
                             static_cast<float>(t.inv_dln), static_cast<float>(p.noise_margin_z)};
       }
@@ -346,6 +349,10 @@ struct Model {
         throw std::invalid_argument("SensorParams: noise_leaf_level must lie in [0, 10]");
       }
       if (p.noise != 0 && !(p.sigma_o >= 0.0)) throw std::invalid_argument("SensorParams: sigma_o must be >= 0");
+      if (p.initial_state == 1 && (p.stationary_probe_pixels < 1 || p.stationary_burnin_ns < 0)) {
+        throw std::invalid_argument(
+            "SensorParams: stationary_probe_pixels must be >= 1 and stationary_burnin_ns >= 0");
+      }
       if (p.noise_shot_rate_hz > 0.0 || p.noise_ba_median_hz > 0.0) {
         throw std::invalid_argument("SensorModel: shot and background-activity noise run with the instantaneous "
                                     "response only");
@@ -431,11 +438,96 @@ struct Model {
       throw std::invalid_argument("SensorModel.init: non-finite irradiance at pixel " + std::to_string(at));
     }
     stat_clamps += counters_h.p[kCntClamps];
+    if (mode() == 2 && p.initial_state == 1) stationary(t0, irr0_dev, host_copy, s);
     t_state = t0;
     initialized = true;
     last_events = 0;
     kept.clear();
     n_held = n_ready = 0;  // a new run: nothing held by the output stage
+  }
+
+  // The stationary start of the lattice (stationary.h) on the host, from the phase-law states init just wrote.
+  void stationary(int64_t t0, const float* irr0_dev, const float* host_copy, cudaStream_t s) {
+    CK(cudaStreamSynchronize(s));
+    std::vector<float> frame(n);
+    if (host_copy) {
+      std::copy(host_copy, host_copy + n, frame.begin());
+    } else {
+      CK(cudaMemcpy(frame.data(), irr0_dev, n * sizeof(float), cudaMemcpyDeviceToHost));
+    }
+    StateBufs& b = st[cur];
+    const size_t ni = i64_words() * n, nf = f32_words() * n, nu = u32_words() * n;
+    std::vector<int64_t> i64(ni);
+    std::vector<float> f32(nf);
+    std::vector<uint32_t> u32(nu);
+    CK(cudaMemcpy(i64.data(), b.i64.p, ni * sizeof(int64_t), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(f32.data(), b.f32.p, nf * sizeof(float), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(u32.data(), b.u32.p, nu * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    // The planes of StateBufs::soa (mode 2).
+    std::vector<HostPixel> px(n);
+    std::vector<PixelMapRegs> regs(n);
+    std::vector<float> phi0(n);
+    for (size_t i = 0; i < n; ++i) {
+      HostPixel& x = px[i];
+      x.s.t_ref = i64[i];
+      x.s.t_search = i64[n + i];
+      x.s.blind_until = i64[2 * n + i];
+      x.s.t_shot = i64[3 * n + i];
+      x.s.t_ba = i64[4 * n + i];
+      x.L.cell = i64[5 * n + i];
+      x.s.s3_ref = f32[i];
+      x.s.n3_ref = f32[n + i];
+      x.s.dr_ref = f32[2 * n + i];
+      x.s.i_scale = f32[3 * n + i];
+      x.s.held = f32[4 * n + i];
+      x.q = CascadeRegs{f32[5 * n + i], f32[6 * n + i], f32[7 * n + i], f32[8 * n + i], f32[9 * n + i]};
+      for (int j = 0; j < 3; ++j) {
+        x.L.nk[j] = f32[(10 + j) * n + i];
+        x.L.nk1[j] = f32[(13 + j) * n + i];
+      }
+      x.L.ln_a1 = f32[16 * n + i];
+      x.s.flags = u32[i];
+      x.s.n_shot = u32[n + i];
+      x.s.n_ba = u32[2 * n + i];
+      x.L.have_k1 = u32[3 * n + i];
+      regs[i] = PixelMapRegs{static_cast<float>(maps.theta_on[i]), static_cast<float>(maps.theta_off[i]),
+                             static_cast<float>(maps.leak[i]), static_cast<float>(maps.dark[i]),
+                             static_cast<float>(p.illuminance_scale) * 1.0f, 0.0, 0.0};
+      phi0[i] = static_cast<float>(maps.phi0[i]);
+    }
+    NoiseTableDev host_tab = tab;
+    host_tab.data = tables_host.data();
+    const double leak_at_t = p.leak_rate_hz * arrhenius(p.leak_ea_eV, p.temperature_K, p.reference_temperature_K);
+    const StationaryInputs in{regs.data(), maps.theta_on.data(), maps.theta_off.data(), maps.leak.data(),
+                              phi0.data(), frame.data(), k, cc, host_tab,
+                              NoiseModelH{p.k * 1.602176634e-19, 1.0 / p.tau_o, 1.0 / p.tau_sf, p.sigma_o,
+                                          p.noise_leaf_level},
+                              p.k, leak_at_t, p.stationary_burnin_ns, p.stationary_probe_pixels};
+    stationary_start(px, in, t0);
+    for (size_t i = 0; i < n; ++i) {
+      const HostPixel& x = px[i];
+      i64[i] = x.s.t_ref;
+      i64[n + i] = x.s.t_search;
+      i64[2 * n + i] = x.s.blind_until;
+      i64[5 * n + i] = x.L.cell;
+      f32[i] = x.s.s3_ref;
+      f32[n + i] = x.s.n3_ref;
+      f32[2 * n + i] = x.s.dr_ref;
+      f32[3 * n + i] = x.s.i_scale;
+      f32[4 * n + i] = x.s.held;
+      const float qv[5] = {x.q.z, x.q.x1, x.q.s2, x.q.s3, x.q.tv};
+      for (int j = 0; j < 5; ++j) f32[(5 + j) * n + i] = qv[j];
+      for (int j = 0; j < 3; ++j) {
+        f32[(10 + j) * n + i] = x.L.nk[j];
+        f32[(13 + j) * n + i] = x.L.nk1[j];
+      }
+      f32[16 * n + i] = x.L.ln_a1;
+      u32[i] = x.s.flags;
+      u32[3 * n + i] = x.L.have_k1;
+    }
+    CK(cudaMemcpy(b.i64.p, i64.data(), ni * sizeof(int64_t), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b.f32.p, f32.data(), nf * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b.u32.p, u32.data(), nu * sizeof(uint32_t), cudaMemcpyHostToDevice));
   }
 
   void init_host(int64_t t0, const float* irr0) {

@@ -39,6 +39,9 @@ def params_struct(p: SensorParams) -> _lib.Params:
     s.noise = 1 if v["noise"] else 0
     s.noise_leaf_level = int(v["noise_leaf_level"])
     s.noise_diffusion = 1 if v["noise_diffusion"] == "transient" else 0
+    s.initial_state = 1 if v["initial_state"] == "stationary" else 0
+    s.stationary_probe_pixels = int(v["stationary_probe_pixels"])
+    s.stationary_burnin_ns = int(v["stationary_burnin_ns"])
     s.reset_mode = 1 if v["reset_mode"] == "ideal" else 0
     s.initial_phase = {"uniform": 0, "symmetric": 1, "zero": 2}[v["initial_phase"]]
     s.clock_offset_ns = int(v["clock_offset_ns"])
@@ -94,10 +97,6 @@ class SensorModel:
                 self._params.noise_diffusion != "frozen":
             raise ValueError("SensorModel: this build runs the noise lattice with frozen diffusion "
                              "(accuracy.noise_diffusion = 'frozen')")
-        if self._params.photoreceptor == "cascade" and self._params.noise and \
-                self._params.initial_state == "stationary":
-            raise ValueError("SensorModel: this build starts the noise lattice from the phase law "
-                             "(accuracy.initial_state = 'phase'); the stationary probe is not built")
         if self._params.photoreceptor == "cascade" and self._params.noise_on():
             raise ValueError("SensorModel: shot and background-activity noise run with the instantaneous response only")
         self._width, self._height, self._seed, self._camera = int(width), int(height), int(seed), int(camera)

@@ -34,7 +34,8 @@ typedef struct bs_engine bs_engine;
  * the caller. photoreceptor: 1 instantaneous or 0 cascade; enums as in params.h (reset_mode 0 physical / 1 ideal,
  * initial_phase 0 uniform / 1 symmetric / 2 zero, noise_diffusion 0 frozen / 1 transient). k, tau_o, tau_sf, eps_L
  * and noise (the cascade's in-path noise lattice) with sigma_o, noise_margin_z, noise_leaf_level and
- * noise_diffusion are the cascade's rows (read only with photoreceptor 0; the lattice runs frozen diffusion). The
+ * noise_diffusion are the cascade's rows (read only with photoreceptor 0; the lattice runs frozen diffusion), and
+ * initial_state (0 phase / 1 stationary), stationary_probe_pixels and stationary_burnin_ns its initial state. The
  * noise_shot_rate_hz / noise_ba_* rows are this project's shot and background-activity noise (0 = off;
  * instantaneous response only; no reference counterpart). */
 typedef struct {
@@ -54,6 +55,8 @@ typedef struct {
   int32_t noise;
   double sigma_o, noise_margin_z;
   int32_t noise_leaf_level, noise_diffusion;
+  int32_t initial_state, stationary_probe_pixels;
+  int64_t stationary_burnin_ns;
 } bs_params;
 
 /* Event columns of the caller's arrays (count entries each; any pointer may be NULL to skip a column), sorted by

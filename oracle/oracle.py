@@ -437,18 +437,20 @@ class Ref:
         KEYS = ("theta_on", "theta_off", "sigma_theta_on", "sigma_theta_off", "theta_onoff_corr", "theta_floor",
                 "refractory_s", "eps_ci", "leak_rate_hz", "leak_sigma_log10", "dark_current_fA", "dark_sigma_ln",
                 "illuminance_scale", "label_share_cut", "readout_quantum_s", "readout_delay_s", "k", "tau_o", "tau_sf",
-                "eps_L", "sigma_o", "noise_leaf_level", "noise_margin_z")
+                "eps_L", "sigma_o", "noise_leaf_level", "noise_margin_z", "stationary_burnin_ns",
+                "stationary_probe_pixels")
 
         def __init__(self, params, width, height, seed, camera=0, num_threads=0):
             self.L = Ref.lib()
             self.width, self.height = width, height
             v = params.as_dict()
-            keys = list(self.KEYS) + ["reset_mode", "initial_phase", "photoreceptor", "noise"]
+            keys = list(self.KEYS) + ["reset_mode", "initial_phase", "photoreceptor", "noise", "initial_state"]
             vals = [float(v[k]) for k in self.KEYS] + [1.0 if v["reset_mode"] == "ideal" else 0.0,
                                                         {"uniform": 0.0, "symmetric": 1.0, "zero": 2.0}[
                                                             v["initial_phase"]],
                                                         0.0 if v["photoreceptor"] == "cascade" else 1.0,
-                                                        1.0 if v["noise"] else 0.0]
+                                                        1.0 if v["noise"] else 0.0,
+                                                        1.0 if v["initial_state"] == "stationary" else 0.0]
             ck = (C.c_char_p * len(keys))(*[k.encode() for k in keys])
             cv = (C.c_double * len(vals))(*vals)
             self.h = self.L.ref_model_create(v["family"].encode(), ck, cv, len(keys), width, height, seed, camera,

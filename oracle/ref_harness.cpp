@@ -70,6 +70,10 @@ void set_field(sensor::SensorParams& p, const std::string& key, double v) {
   else if (key == "sigma_o") p.sigma_o = v;
   else if (key == "noise_leaf_level") p.noise_leaf_level = static_cast<int32_t>(v);
   else if (key == "noise_margin_z") p.noise_margin_z = v;
+  else if (key == "initial_state") {
+    p.initial_state = v == 0.0 ? sensor::InitialState::kPhase : sensor::InitialState::kStationary;
+  } else if (key == "stationary_burnin_ns") p.stationary_burnin_ns = static_cast<int64_t>(v);
+  else if (key == "stationary_probe_pixels") p.stationary_probe_pixels = static_cast<int32_t>(v);
   else throw std::invalid_argument("ref harness: unknown field " + key);
 }
 

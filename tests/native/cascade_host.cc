@@ -10,6 +10,7 @@
 #include "cascade.cuh"
 #include "lattice.cuh"
 #include "noise_build.h"
+#include "stationary.h"
 
 using namespace bs;
 
@@ -199,6 +200,24 @@ void hl_init(void* hp, int64_t t0, const float* irr0) {
     proc.init(t0, b.phi0[p]);
   }
   b.t_state = t0;
+}
+
+// The stationary start after hl_init (stationary.h): maps64 = theta_on, theta_off, leak (fp64, n each); st = kq, a2,
+// a3, sigma_o, k (A^-1 s^-1), the leak rate at the temperature; burnin_ns; probe_pixels.
+void hl_stationary(void* hp, int64_t t0, const float* frame, const double* maps64, const double* st, int64_t burnin_ns,
+                   int32_t probe_pixels) {
+  HostLattice& h = *static_cast<HostLattice*>(hp);
+  Host& b = h.base;
+  std::vector<HostPixel> px(b.n);
+  for (uint32_t p = 0; p < b.n; ++p) px[p] = HostPixel{b.st[p], b.cq[p], h.lat[p]};
+  StationaryInputs in{b.maps.data(), maps64, maps64 + b.n, maps64 + 2 * b.n, b.phi0.data(), frame, b.k, b.cc, h.view,
+                      NoiseModelH{st[0], st[1], st[2], st[3], h.view.levels}, st[4], st[5], burnin_ns, probe_pixels};
+  stationary_start(px, in, t0);
+  for (uint32_t p = 0; p < b.n; ++p) {
+    b.st[p] = px[p].s;
+    b.cq[p] = px[p].q;
+    h.lat[p] = px[p].L;
+  }
 }
 
 void hl_advance(void* hp, const uint32_t* ids, size_t n_ids, const int64_t* t, const float* irr,

@@ -24,7 +24,7 @@ EV = np.dtype([("pixel", "u4"), ("p", "u1"), ("label", "u1"), ("flags", "u2"), (
 @pytest.fixture(scope="session")
 def host(tmp_path_factory):
     so = tmp_path_factory.mktemp("cascade") / "libcascade_host.so"
-    subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared",
+    subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared", "-pthread",
                     f"-I{CSRC}", str(ROOT / "tests" / "native" / "cascade_host.cc"), "-o", str(so)], check=True)
     H = C.CDLL(str(so))
     H.hc_create.restype = C.c_void_p
@@ -53,6 +53,8 @@ def host(tmp_path_factory):
     H.hl_event_count.argtypes = [C.c_void_p]
     H.hl_take.argtypes = [C.c_void_p, C.c_void_p]
     H.hl_destroy.argtypes = [C.c_void_p]
+    H.hl_stationary.restype = None
+    H.hl_stationary.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32]
     return H
 
 
@@ -129,8 +131,8 @@ CASES = [
 ]
 
 
-def _host_vs_reference(host, ref, p, calls, t0, seed, n_calls=6):
-    W, Hh = 12, 9
+def _host_vs_reference(host, ref, p, calls, t0, seed, n_calls=6, size=(12, 9)):
+    W, Hh = size
     n = W * Hh
     rng = np.random.default_rng(seed)
     model = ref.Model(p, W, Hh, seed)
@@ -153,6 +155,11 @@ def _host_vs_reference(host, ref, p, calls, t0, seed, n_calls=6):
     fn = lambda name: getattr(host, f"{pre}_{name}")  # noqa: E731
     try:
         fn("init")(h, t0, irr0.ctypes.data)
+        if lattice and p.initial_state == "stationary":
+            maps64 = np.concatenate([mp["theta_on"], mp["theta_off"], mp["leak"]]).astype(np.float64)
+            st = np.array([p.k * 1.602176634e-19, 1.0 / p.tau_o, 1.0 / p.tau_sf, p.sigma_o, p.k, p.leak_rate_hz])
+            host.hl_stationary(h, t0, irr0.ctypes.data, maps64.ctypes.data, st.ctypes.data,
+                               int(p.stationary_burnin_ns), int(p.stationary_probe_pixels))
         want, got = [], []
         for ids, tt, vv, t_end, starts, cnt in calls(rng, n, t0, n_calls):
             model.advance_runs(ids, tt, vv, starts, cnt, t_end)
@@ -220,3 +227,23 @@ def test_lattice_host_equals_the_reference(host, ref, family, overrides, calls, 
     p = resolve(family, {"noise": True, **overrides})
     W, want, got = _host_vs_reference(host, ref, p, calls, t0, 5 + len(overrides) + (t0 & 7))
     _same(W, want, got)
+
+
+@pytest.mark.parametrize("overrides,t0", [
+    ({"stationary_burnin_ns": 500_000_000}, 0),
+    ({"stationary_burnin_ns": 300_000_000, "leak_rate_hz": 2.0, "refractory_s": 0.0}, 12345),
+    ({"stationary_burnin_ns": 200_000_000, "stationary_probe_pixels": 7, "reset_mode": "ideal"}, -65536 * 9),
+])
+def test_stationary_start_equals_the_reference(host, ref, overrides, t0):
+    """The lattice's stationary initial state (stationary.h: probes, their histories, the transfer) equals the
+    reference's (sensor_model.cpp:492-700): the events of the calls after it, bit for bit. The default 60 s history
+    is checked on the B200 (test_gpu_parity.py)."""
+    p = resolve("prophesee_gen3", {"noise": True, "initial_state": "stationary", **overrides})
+    W, want, got = _host_vs_reference(host, ref, p, random_calls, t0, 5 + len(overrides), size=(16, 12))
+    _same(W, want, got)
+    phase = resolve("prophesee_gen3", {"noise": True, **overrides})
+    _, want_phase, _ = _host_vs_reference(host, ref, phase, random_calls, t0, 5 + len(overrides), size=(16, 12))
+    n_st, n_ph = (sum(len(x["t_cross_ns"]) for x in w) for w in (want, want_phase))
+    first_st = np.concatenate([x["t_cross_ns"] for x in want])[:50]
+    first_ph = np.concatenate([x["t_cross_ns"] for x in want_phase])[:50]
+    assert n_st != n_ph or not np.array_equal(first_st, first_ph)  # the start does change the events

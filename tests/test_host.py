@@ -91,6 +91,4 @@ def test_sensor_model_argument_checks():
     with pytest.raises(ValueError):
         SensorModel("prophesee_gen3", 8, 8, 1, [{"type": "constant"}], 0,
                     overrides={"noise_diffusion": "transient"})  # the lattice runs frozen diffusion only
-    with pytest.raises(ValueError):
-        SensorModel("prophesee_gen3", 8, 8, 1, [{"type": "constant"}], 0,
-                    overrides={"initial_state": "stationary"})  # the lattice's stationary probe is not built
+
