@@ -28,7 +28,7 @@ struct StateSoA {
   float *s3_ref, *n3_ref, *dr_ref, *i_scale, *held;
   uint32_t *flags, *n_shot, *n_ba;
   float *z, *x1, *s2, *s3, *tv;  // the cascade's (null without it)
-  float* lat;                    // the noise lattice's: 7 planes of n (nk 0..2, nk1 0..2, ln_a1); null without it
+  float* lat;                    // the noise lattice's: 8 planes of n (nk 0..2, nk1 0..2, ln_a1, rho); null without it
   int64_t* cell;
   uint32_t* have_k1;
 };

@@ -95,6 +95,7 @@ __device__ __forceinline__ void load_lattice(const StateSoA& a, uint32_t p, uint
     L.nk1[i] = a.lat[static_cast<size_t>(3 + i) * n + p];
   }
   L.ln_a1 = a.lat[static_cast<size_t>(6) * n + p];
+  L.rho = a.lat[static_cast<size_t>(7) * n + p];
   L.cell = a.cell[p];
   L.have_k1 = a.have_k1[p];
 }
@@ -105,6 +106,7 @@ __device__ __forceinline__ void store_lattice(const StateSoA& a, uint32_t p, uin
     a.lat[static_cast<size_t>(3 + i) * n + p] = L.nk1[i];
   }
   a.lat[static_cast<size_t>(6) * n + p] = L.ln_a1;
+  a.lat[static_cast<size_t>(7) * n + p] = L.rho;
   a.cell[p] = L.cell;
   a.have_k1[p] = L.have_k1;
 }

@@ -1,4 +1,5 @@
-// The cascade photoreceptor with its in-path noise lattice (photoreceptor = cascade, noise = true, frozen diffusion):
+// The cascade photoreceptor with its in-path noise lattice (photoreceptor = cascade, noise = true; frozen or transient
+// diffusion):
 // BallaSim's default sensor model, restated for the device.
 //
 // The linearized noise n = (n1, n2, n3) lives on a lattice of cells of 2^16 ns (src/sensor/noise.h,
@@ -31,14 +32,16 @@ struct NoiseTableDev {
   const float* data;
   int32_t n_nodes, stride, levels;
   float ln_a1_min, inv_dln, margin_z;
+  int32_t transient;  // accuracy.noise_diffusion transient: the tables hold the split blocks
 };
 
-// The lattice's part of a pixel's state (PixelState nk, nk1, ln_a1, cell, have_k1; fp32 values).
+// The lattice's part of a pixel's state (PixelState nk, nk1, ln_a1, cell, have_k1 and rho = 1 + rho_m1; fp32 values).
 struct LatticeRegs {
   float nk[3], nk1[3];
   float ln_a1;
   int64_t cell;
   uint32_t have_k1;
+  float rho;  // the cell's diffusion ratio (1 under frozen diffusion; rho - 1 is exact in fp32)
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -167,6 +170,168 @@ BS_HD float noise_margin(const float* m, float z, const float* xl, const float* 
 
 BS_HD int64_t level_length(int level) { return kNoiseCellNs >> level; }
 
+// ---------------------------------------------------------------------------------------------
+// Transient diffusion (noise.h:70-160, pixel.h:420-560): a cell whose input-node diffusion is rho D1 has
+// Q = rho Q1 + Q2; the kernel factors it and forms its bridges in information form.
+// ---------------------------------------------------------------------------------------------
+BS_HD void lower3_tmul(const float* L, const float* x, float* y) {
+  y[0] = L[0] * x[0] + L[1] * x[1] + L[3] * x[2];
+  y[1] = L[2] * x[1] + L[4] * x[2];
+  y[2] = L[5] * x[2];
+}
+
+// Lower Cholesky factor of a packed symmetric PSD 3x3; a pivot at or below a tiny fraction of the trace is 0 with its
+// column.
+BS_HD void chol3_f(const float* q, float* c) {
+  const float tiny = (fabs_f(q[0]) + fabs_f(q[2]) + fabs_f(q[5])) * static_cast<float>(1e-20);
+  float d = q[0];
+  c[0] = d > tiny ? sqrt_f(d) : 0.0f;
+  c[1] = c[0] > 0.0f ? q[1] / c[0] : 0.0f;
+  c[3] = c[0] > 0.0f ? q[3] / c[0] : 0.0f;
+  d = q[2] - c[1] * c[1];
+  c[2] = d > tiny ? sqrt_f(d) : 0.0f;
+  c[4] = c[2] > 0.0f ? (q[4] - c[3] * c[1]) / c[2] : 0.0f;
+  d = q[5] - c[3] * c[3] - c[4] * c[4];
+  c[5] = d > tiny ? sqrt_f(d) : 0.0f;
+}
+
+BS_HD void split_chol(const float* q12, float rho, float* c) {
+  float q[6];
+  for (int i = 0; i < 6; ++i) q[i] = rho * q12[i] + q12[6 + i];
+  chol3_f(q, c);
+}
+
+// The midpoint of a node with ratio rho from the half-node's block (Phi_l, Q1_l, Q2_l): precision J = Q^-1 +
+// Phi^T Q^-1 Phi, mean J^-1 (Q^-1 Phi x_L + Phi^T Q^-1 x_R), drawn as U^-T (U^-1 b + xi) with U = chol J.
+static BS_COLD void bridge_midpoint_split(const float* blk, float rho, const float* xl, const float* xr,
+                                          const float* xi, float* xm) {
+  const float* phi = blk;
+  float c[6];
+  split_chol(blk + 6, rho, c);
+  float n[6];
+  n[0] = 1.0f / c[0];
+  n[2] = 1.0f / c[2];
+  n[5] = 1.0f / c[5];
+  n[1] = -c[1] * n[0] * n[2];
+  n[4] = -c[4] * n[2] * n[5];
+  n[3] = -(c[3] * n[0] + c[4] * n[1]) * n[5];
+  float m[6];
+  m[0] = n[0] * phi[0];
+  m[1] = n[1] * phi[0] + n[2] * phi[1];
+  m[2] = n[2] * phi[2];
+  m[3] = n[3] * phi[0] + n[4] * phi[1] + n[5] * phi[3];
+  m[4] = n[4] * phi[2] + n[5] * phi[4];
+  m[5] = n[5] * phi[5];
+  float j[6];
+  j[0] = (n[0] * n[0] + n[1] * n[1] + n[3] * n[3]) + (m[0] * m[0] + m[1] * m[1] + m[3] * m[3]);
+  j[1] = (n[2] * n[1] + n[4] * n[3]) + (m[2] * m[1] + m[4] * m[3]);
+  j[2] = (n[2] * n[2] + n[4] * n[4]) + (m[2] * m[2] + m[4] * m[4]);
+  j[3] = n[5] * n[3] + m[5] * m[3];
+  j[4] = n[5] * n[4] + m[5] * m[4];
+  j[5] = n[5] * n[5] + m[5] * m[5];
+  float u[6];
+  chol3_f(j, u);
+  float a[3], b1[3], b2[3];
+  lower3_mul(m, xl, a);
+  lower3_tmul(n, a, b1);
+  lower3_mul(n, xr, a);
+  lower3_tmul(m, a, b2);
+  float y[3];
+  y[0] = (b1[0] + b2[0]) / u[0];
+  y[1] = ((b1[1] + b2[1]) - u[1] * y[0]) / u[2];
+  y[2] = ((b1[2] + b2[2]) - u[3] * y[0] - u[4] * y[1]) / u[5];
+  for (int i = 0; i < 3; ++i) y[i] = y[i] + xi[i];
+  xm[2] = y[2] / u[5];
+  xm[1] = (y[1] - u[4] * xm[2]) / u[2];
+  xm[0] = (y[0] - u[1] * xm[1] - u[3] * xm[2]) / u[0];
+}
+
+// The margin of a node with ratio rho: sigma_br(rho) <= sigma_br(1) sqrt(1 + (rho - 1) f_l) for rho > 1, and the
+// mean-mismatch term scaled by sqrt(max(1, rho)).
+BS_HD float noise_margin_rho(const float* m, float z, const float* xl, const float* xr, float rho, float f_l) {
+  const float e[6] = {xl[0], xl[1], xl[2], xr[0], xr[1], xr[2]};
+  const float* W = m + 2;
+  float norm2 = 0.0f;
+  int idx = 0;
+  for (int i = 0; i < 6; ++i) {
+    float s = 0.0f;
+    for (int jj = 0; jj <= i; ++jj) s = s + W[idx++] * e[jj];
+    norm2 = norm2 + s * s;
+  }
+  const float big = rho > 1.0f ? rho : 1.0f;
+  const float s_br = rho > 1.0f ? sqrt_f(1.0f + (rho - 1.0f) * f_l) : 1.0f;
+  return z * m[0] * s_br + m[1] * sqrt_f(norm2) * sqrt_f(big);
+}
+
+// One input piece's step of J = int over the cell of e^{-2 int_s^te k u} k (I + u) ds (pixel.h:467-489).
+BS_HD float diffusion_ramp(float jw, float ikI, float dl, float dkI) {
+  const float a = 2.0f * dl;
+  const float em = expm1_f(-a);
+  float g0, c;
+  if (a > static_cast<float>(0.05)) {
+    g0 = -em / a;
+    c = 1.0f / a - g0 * (1.0f / a + 0.5f);
+  } else {
+    g0 = 1.0f - a * (0.5f - a * (1.0f / 6.0f));
+    c = a * (1.0f / 12.0f - a * (1.0f / 24.0f - a * (1.0f / 80.0f)));
+  }
+  return jw * (1.0f + em) + (ikI + dl) * g0 + dkI * c;
+}
+
+// J over one input piece (pixel.h:494-537): a constant piece in closed form; a ramp in at most 32 sub-pieces, only
+// its last 12 units of int k u where longer.
+static BS_COLD float diffusion_weight(float jw, float z_a, float z_b, float I_a, float I_b, float ikI, float h,
+                                      float k) {
+  if (I_a == I_b) {
+    const float em = expm1_f(-ikI);
+    const float e1 = 1.0f + em, e2 = e1 * e1;
+    const float r = z_a * I_a - 1.0f;
+    const float d = 1.0f + r * e1;
+    const float zr = z_b / z_a;
+    const float jp = ((-em) * (2.0f + em) + 3.0f * r * (-em) * e1 + ikI * (r * r) * e2) / (d * d);
+    return jw * (e2 / (zr * zr)) + jp;
+  }
+  float z = z_a, I0 = I_a, hr = h, ik = ikI;
+  float dl = log_f(z_b / z_a) + ikI;
+  if (dl > 12.0f) {
+    const float tail = 12.0f * z_b / k;
+    if (tail < h) {
+      const float hh = h - tail;
+      const float Im = I_a + (I_b - I_a) * (hh / h);
+      const float zm = z_step(z_a, I_a, Im, hh, k);
+      const float ih = integrated_pole(I_a, Im, hh, k);
+      jw = diffusion_ramp(jw, ih, log_f(zm / z_a) + ih, hh * k * (Im - I_a));
+      z = zm;
+      I0 = Im;
+      hr = tail;
+      ik = integrated_pole(I0, I_b, hr, k);
+      dl = log_f(z_b / z) + ik;
+    }
+  }
+  const float total = ik + dl;
+  int n = static_cast<int>(total * 4.0f) + 1;
+  n = n < 32 ? n : 32;
+  if (n == 1) return diffusion_ramp(jw, ik, dl, hr * k * (I_b - I0));
+  const float hs = hr / static_cast<float>(n), dI = (I_b - I0) / static_cast<float>(n), Is = I0;
+  for (int i = 0; i < n; ++i) {
+    const float I1 = i + 1 == n ? I_b : Is + dI * static_cast<float>(i + 1);
+    const float z1 = i + 1 == n ? z_b : z_step(z, I0, I1, hs, k);
+    const float ik1 = integrated_pole(I0, I1, hs, k);
+    jw = diffusion_ramp(jw, ik1, log_f(z1 / z) + ik1, hs * k * (I1 - I0));
+    z = z1;
+    I0 = I1;
+  }
+  return jw;
+}
+
+// rho = J / (1 - e^{-2 int k u}) clamped to [1/2, 1e6] and rounded to fp32 (pixel.h:541-547).
+BS_HD float diffusion_ratio(float jw, float int_ku) {
+  const float den = -expm1_f(-2.0f * int_ku);
+  if (!(den > 0.0f) || !finite_f(jw)) return 1.0f;
+  const float rho = jw / den;
+  return rho < 1e6f ? (rho > 0.5f ? rho : 0.5f) : 1e6f;
+}
+
 // The comparand of the reference kernel (pixel.h:312-320).
 struct Comparand {
   int64_t t_ref;
@@ -200,18 +365,39 @@ struct Tri {
   float v[3];
 };
 
-// The midpoint of a tree node at `level` (time t_mid) from its endpoints (pixel.h:450-464, rho = 1).
+// The midpoint of a tree node at `level` (time t_mid) from its endpoints (pixel.h:450-464); a cell with rho != 1
+// forms it from the split blocks.
 BS_HD void bridge_child(const NoiseTableDev& tab, uint64_t seed, uint32_t camera, uint32_t pixel, NoisePosF pos,
-                        int level, int64_t t_mid, const float* xl, const float* xr, float* xm) {
-  float xi[3], blk[24];
+                        float rho, int level, int64_t t_mid, const float* xl, const float* xr, float* xm) {
+  float xi[3];
   normals3_f(seed, kPurposeNoise, camera, pixel, static_cast<uint64_t>(t_mid), xi);
+  if (rho != 1.0f) {
+    float blk[18];
+    noise_lookup(tab, pos, NoiseLayoutF{tab.levels, true}.split_level(level), 18, blk);
+    bridge_midpoint_split(blk, rho, xl, xr, xi, xm);
+    return;
+  }
+  float blk[24];
   noise_lookup(tab, pos, NoiseLayoutF{tab.levels}.bridge(level), 24, blk);
   bridge_midpoint(blk, xl, xr, xi, xm);
 }
 
+// The margin of a level-l node: the table's, or with rho != 1 its bound from the split tables (pixel.h:551-561).
+BS_HD float node_margin(const NoiseTableDev& tab, NoisePosF pos, int level, float rho, const float* xl,
+                        const float* xr) {
+  float m[23];
+  noise_lookup(tab, pos, NoiseLayoutF{tab.levels}.margin(level), 23, m);
+  if (rho != 1.0f) {
+    float f_l;
+    noise_lookup(tab, pos, NoiseLayoutF{tab.levels, true}.split_margin(level), 1, &f_l);
+    return noise_margin_rho(m, tab.margin_z, xl, xr, rho, f_l);
+  }
+  return noise_margin(m, tab.margin_z, xl, xr);
+}
+
 // n3(t) in the cell from tc0 (nodes nk, nk1, rate ln_a1) by descending the keyed tree (pixel.h:565-594).
 static BS_COLD float n3_at(const NoiseTableDev& tab, float a3, uint64_t seed, uint32_t camera, uint32_t pixel,
-                           float ln_a1, Tri nk, Tri nk1, int64_t tc0, int64_t t) {
+                           float ln_a1, float rho, Tri nk, Tri nk1, int64_t tc0, int64_t t) {
   if (t == tc0) return nk.v[2];
   if (t == tc0 + kNoiseCellNs) return nk1.v[2];
   const NoisePosF pos = noise_pos(tab, ln_a1);
@@ -223,7 +409,7 @@ static BS_COLD float n3_at(const NoiseTableDev& tab, float a3, uint64_t seed, ui
   int64_t node_t = tc0;
   for (int l = 1; l <= tab.levels; ++l) {
     const int64_t mid = node_t + level_length(l);
-    bridge_child(tab, seed, camera, pixel, pos, l, mid, xl, xr, xm);
+    bridge_child(tab, seed, camera, pixel, pos, rho, l, mid, xl, xr, xm);
     if (t == mid) return xm[2];
     if (t < mid) {
       for (int i = 0; i < 3; ++i) xr[i] = xm[i];
@@ -249,7 +435,8 @@ struct Found {
 // that may fire (pixel.h:634-725 without the high-pass filter, rho = 1): a non-leaf node is split only where its
 // margin-widened hull may reach a level; leaves are searched exactly; the first crossing wins.
 static BS_COLD Found walk(const NoiseTableDev& tab, float a3, uint64_t seed, uint32_t camera, uint32_t pixel,
-                          float ln_a1, Tri nk, Tri nk1, int64_t tc0, const SubStep sub, int64_t lo, Comparand c) {
+                          float ln_a1, float rho, Tri nk, Tri nk1, int64_t tc0, const SubStep sub, int64_t lo,
+                          Comparand c) {
   struct Node {
     int level;
     int64_t t;
@@ -257,7 +444,6 @@ static BS_COLD Found walk(const NoiseTableDev& tab, float a3, uint64_t seed, uin
   };
   Found out{false, false, 0, 0.0f, 0.0f, 0};
   const NoisePosF pos = noise_pos(tab, ln_a1);
-  const NoiseLayoutF lay{tab.levels};
   Node stack[12];
   int sp = 0;
   Node& root = stack[sp++];
@@ -275,17 +461,16 @@ static BS_COLD Found walk(const NoiseTableDev& tab, float a3, uint64_t seed, uin
     if (span_lo >= span_hi) continue;
     if (node.level < tab.levels) {
       if (!top) {
-        float hc[4], mblk[23];
+        float hc[4];
         noise_hermite(node.xl, node.xr, a3, static_cast<float>(length) * kNsF, hc);
-        noise_lookup(tab, pos, lay.margin(node.level), 23, mblk);
-        const float margin = noise_margin(mblk, tab.margin_z, node.xl, node.xr);
+        const float margin = node_margin(tab, pos, node.level, rho, node.xl, node.xr);
         const int64_t e0 = maxi(sub.t_a, span_lo), e1 = mini(sub.t_b, span_hi);
         if (e0 >= e1 || !may_cross(delta_noise(sub, e0, hc, node.t, c), e0, e1, lo, margin, c)) continue;
       }
       top = false;
       const int64_t mid = node.t + level_length(node.level + 1);
       float xm[3];
-      bridge_child(tab, seed, camera, pixel, pos, node.level + 1, mid, node.xl, node.xr, xm);
+      bridge_child(tab, seed, camera, pixel, pos, rho, node.level + 1, mid, node.xl, node.xr, xm);
       Node& right = stack[sp++];
       right.level = node.level + 1;
       right.t = mid;
@@ -388,11 +573,7 @@ struct LatticeProc {
 
   // A resumed call inside a cell: its level-0 hull as the lattice draw left it (pixel.h:1003-1012).
   BS_HD void resume() {
-    if (L.have_k1) {
-      float m0[23];
-      if (tab.levels > 0) noise_lookup(tab, noise_pos(tab, L.ln_a1), NoiseLayoutF{tab.levels}.margin(0), 23, m0);
-      level0(m0);
-    }
+    if (L.have_k1) level0(noise_pos(tab, L.ln_a1));
   }
 
   // The piece from t within one segment, up to limit (pixel.h:1189-1232, constant groups).
@@ -402,26 +583,34 @@ struct LatticeProc {
     return LinearPiece{t, tb, m.dark + m.scale * in.group_value(sg, t), m.dark + m.scale * in.group_value(sg, tb)};
   }
 
-  BS_HD void level0(const float* m0) {
+  BS_HD void level0(NoisePosF pos) {
     noise_hermite(L.nk, L.nk1, cc.a3, static_cast<float>(kNoiseCellNs) * kNsF, hc0);
-    if (tab.levels > 0) margin0 = noise_margin(m0, tab.margin_z, L.nk, L.nk1);
+    if (tab.levels > 0) margin0 = node_margin(tab, pos, 0, L.rho, L.nk, L.nk1);
   }
 
-  // The lattice draw of n at the cell's end at the cell's rate, and the level-0 hull (pixel.h:1336-1376).
+  // The lattice draw of n at the cell's end at the cell's rate, and the level-0 hull (pixel.h:1336-1376); a cell with
+  // rho != 1 factors rho Q1 + Q2 (split_lattice_step, pixel.h:420-431).
   BS_HD void draw_lattice(int64_t tc1) {
     float xi[3], step[12];
     normals3_f(k.seed, kPurposeNoise, k.camera, pixel, static_cast<uint64_t>(tc1), xi);
     const NoisePosF pos = noise_pos(tab, L.ln_a1);
-    noise_lookup(tab, pos, NoiseLayoutF::kStepPhi, 12, step);
-    lattice_step(step, step + 6, L.nk, xi, L.nk1);
-    float m0[23];
-    if (tab.levels > 0) noise_lookup(tab, pos, NoiseLayoutF{tab.levels}.margin(0), 23, m0);
-    level0(m0);
+    if (L.rho != 1.0f) {
+      float q12[12], chol[6];
+      noise_lookup(tab, pos, NoiseLayoutF::kStepPhi, 6, step);
+      noise_lookup(tab, pos, NoiseLayoutF{tab.levels, true}.split_step(), 12, q12);
+      split_chol(q12, L.rho, chol);
+      lattice_step(step, chol, L.nk, xi, L.nk1);
+    } else {
+      noise_lookup(tab, pos, NoiseLayoutF::kStepPhi, 12, step);
+      lattice_step(step, step + 6, L.nk, xi, L.nk1);
+    }
+    level0(pos);
     L.have_k1 = 1;
   }
 
   // A settled pixel under constant input for the whole cell: a1 = k u = k / z (pixel.h:1320-1333).
   BS_HD void settled_rate(int64_t t, float pre, int64_t tc1) {
+    L.rho = 1.0f;  // settled: u = I, the transient diffusion is the frozen one
     if (pre == 0.0f && q.z == settled_z) {
       L.ln_a1 = settled_ln;
       return;
@@ -448,15 +637,22 @@ struct LatticeProc {
       settled_rate(t, pre, tc1);
     } else {
       float z = q.z, int_kI = 0.0f;
+      // Transient diffusion: J over the cell; before t0 (init) the pixel is settled, which contributes 1 - e^{-2 pre}.
+      float jw = 0.0f;
+      if (tab.transient && pre > 0.0f) jw = diffusion_weight(jw, 1.0f, 1.0f, 1.0f, 1.0f, pre, 0.0f, 0.0f);
       while (true) {
         const float h = static_cast<float>(pc.t_b - pc.t_a) * kNsF;
+        const float z_a = z;
         if (!(pc.I_a == pc.I_b && fabs_f(z * pc.I_a - 1.0f) <= cc.eps_drop)) z = z_step(z, pc.I_a, pc.I_b, h, cc.k);
-        int_kI = int_kI + integrated_pole(pc.I_a, pc.I_b, h, cc.k);
+        const float ikI = integrated_pole(pc.I_a, pc.I_b, h, cc.k);
+        int_kI = int_kI + ikI;
+        if (tab.transient) jw = diffusion_weight(jw, z_a, z, pc.I_a, pc.I_b, ikI, h, cc.k);
         if (pc.t_b >= tc1) break;
         pc = next_piece(sg, pc.t_b, tc1);
       }
       const float int_ku = pre + log_f(z / q.z) + int_kI;
       L.ln_a1 = log_f(maxr(int_ku / h_cell, static_cast<float>(1e-30)));
+      L.rho = tab.transient ? diffusion_ratio(jw, int_ku) : 1.0f;
     }
     draw_lattice(tc1);
   }
@@ -468,7 +664,7 @@ struct LatticeProc {
   }
 
   BS_HD float n3_here(int64_t t) const {
-    return n3_at(tab, cc.a3, k.seed, k.camera, pixel, L.ln_a1, nk(), nk1(), L.cell * kNoiseCellNs, t);
+    return n3_at(tab, cc.a3, k.seed, k.camera, pixel, L.ln_a1, L.rho, nk(), nk1(), L.cell * kNoiseCellNs, t);
   }
 
   BS_HD void set_reference(int64_t t, float s3, float n3, float offset) {
@@ -529,7 +725,7 @@ struct LatticeProc {
         s.t_search = maxi(s.t_search, sub.t_b);
         return;
       }
-      const Found f = walk(tab, cc.a3, k.seed, k.camera, pixel, L.ln_a1, nk(), nk1(), tc0, sub, lo, cm);
+      const Found f = walk(tab, cc.a3, k.seed, k.camera, pixel, L.ln_a1, L.rho, nk(), nk1(), tc0, sub, lo, cm);
       c.leaves += f.leaves;
       if (!f.found) {
         s.t_search = maxi(s.t_search, sub.t_b);
@@ -586,6 +782,7 @@ struct LatticeProc {
     noise_lookup(tab, noise_pos(tab, log_f(cc.k * s.i_scale)), NoiseLayoutF::kPinfChol, 6, chol);
     lower3_mul(chol, xi, L.nk);
     L.have_k1 = 0;
+    L.rho = 1.0f;
     float n3_0;
     if (t0 != tk) {
       seg = in.segment_at(t0);

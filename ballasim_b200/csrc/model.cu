@@ -179,10 +179,10 @@ uint64_t fnv1a(const void* data, size_t n, uint64_t h = 0xcbf29ce484222325ull) {
 struct StateBufs {
   DevBuf<int64_t> i64;   // 5 x n: t_ref, t_search, blind_until, t_shot, t_ba; with the lattice 1 x n more: cell
   DevBuf<float> f32;     // 5 x n: s3_ref, n3_ref, dr_ref, i_scale, held; with the cascade 5 x n more: z, x1, s2, s3,
-                         // tv; with the lattice 7 x n more: nk 0..2, nk1 0..2, ln_a1
+                         // tv; with the lattice 8 x n more: nk 0..2, nk1 0..2, ln_a1, rho
   DevBuf<uint32_t> u32;  // 3 x n: flags, n_shot, n_ba; with the lattice 1 x n more: have_k1
   static size_t i64_words(int mode) { return mode == 2 ? 6 : 5; }
-  static size_t f32_words(int mode) { return mode == 2 ? 17 : mode == 1 ? 10 : 5; }
+  static size_t f32_words(int mode) { return mode == 2 ? 18 : mode == 1 ? 10 : 5; }
   static size_t u32_words(int mode) { return mode == 2 ? 4 : 3; }
   // mode 0: the instantaneous response, 1: the cascade, 2: the cascade with its noise lattice.
   StateSoA soa(size_t n, int mode) {
@@ -311,13 +311,14 @@ struct Model {
       cc.eps_pl_base = static_cast<float>(p.eps_L / 8.0);
       if (p.noise != 0) {
         // The noise model of the lattice (src/sensor/sensor_model.cpp:260-268): k q with q the elementary charge.
-        const NoiseTablesH t = build_noise_tables(
-            NoiseModelH{p.k * 1.602176634e-19, 1.0 / p.tau_o, 1.0 / p.tau_sf, p.sigma_o, p.noise_leaf_level});
+        const NoiseTablesH t = build_noise_tables(NoiseModelH{p.k * 1.602176634e-19, 1.0 / p.tau_o, 1.0 / p.tau_sf,
+                                                              p.sigma_o, p.noise_leaf_level, p.noise_diffusion == 1});
         tables.ensure(t.data.size());
         CK(cudaMemcpy(tables.p, t.data.data(), t.data.size() * sizeof(float), cudaMemcpyHostToDevice));
         tables_host = t.data;
         tab = NoiseTableDev{tables.p, t.n_nodes, t.stride, t.levels, static_cast<float>(kNoiseLnA1Min),
-                            static_cast<float>(t.inv_dln), static_cast<float>(p.noise_margin_z)};
+                            static_cast<float>(t.inv_dln), static_cast<float>(p.noise_margin_z),
+                            p.noise_diffusion == 1 ? 1 : 0};
       }
     }
     upload_maps();
@@ -341,9 +342,8 @@ struct Model {
       throw std::invalid_argument("SensorParams: photoreceptor must be 'cascade' or 'instantaneous'");
     }
     if (p.photoreceptor == 0) {
-      if (p.noise != 0 && p.noise_diffusion != 0) {
-        throw std::invalid_argument(
-            "SensorModel: this build runs the noise lattice with frozen diffusion (accuracy.noise_diffusion frozen)");
+      if (p.noise != 0 && p.noise_diffusion != 0 && p.noise_diffusion != 1) {
+        throw std::invalid_argument("SensorParams: noise_diffusion must be 'frozen' or 'transient'");
       }
       if (p.noise != 0 && (p.noise_leaf_level < 0 || p.noise_leaf_level > 10)) {
         throw std::invalid_argument("SensorParams: noise_leaf_level must lie in [0, 10]");
@@ -486,6 +486,7 @@ struct Model {
         x.L.nk1[j] = f32[(13 + j) * n + i];
       }
       x.L.ln_a1 = f32[16 * n + i];
+      x.L.rho = f32[17 * n + i];
       x.s.flags = u32[i];
       x.s.n_shot = u32[n + i];
       x.s.n_ba = u32[2 * n + i];
@@ -501,7 +502,7 @@ struct Model {
     const StationaryInputs in{regs.data(), maps.theta_on.data(), maps.theta_off.data(), maps.leak.data(),
                               phi0.data(), frame.data(), k, cc, host_tab,
                               NoiseModelH{p.k * 1.602176634e-19, 1.0 / p.tau_o, 1.0 / p.tau_sf, p.sigma_o,
-                                          p.noise_leaf_level},
+                                          p.noise_leaf_level, p.noise_diffusion == 1},
                               p.k, leak_at_t, p.stationary_burnin_ns, p.stationary_probe_pixels};
     stationary_start(px, in, t0);
     for (size_t i = 0; i < n; ++i) {
@@ -522,6 +523,7 @@ struct Model {
         f32[(13 + j) * n + i] = x.L.nk1[j];
       }
       f32[16 * n + i] = x.L.ln_a1;
+      f32[17 * n + i] = x.L.rho;
       u32[i] = x.s.flags;
       u32[3 * n + i] = x.L.have_k1;
     }

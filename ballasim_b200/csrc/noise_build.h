@@ -1,4 +1,4 @@
-// Host construction of the cascade's noise-lattice tables (src/sensor/noise_tables.cpp:10-411, frozen diffusion):
+// Host construction of the cascade's noise-lattice tables (src/sensor/noise_tables.cpp:10-411):
 // per node of ln a1 on [ln 1e-2, ln 1e9] at 64 nodes per decade, the lattice step Phi(h0) and chol Q(h0), chol of
 // the stationary covariance, per tree level l = 1..L the midpoint bridge (A_m, K, chol Sigma_m) of a node of
 // h0 / 2^(l-1), and per level l = 0..L-1 the exclusion margin (sigma_br, g, W = chol(C_ee)^-1 packed).
@@ -28,18 +28,25 @@ constexpr int kNoiseNodesPerDecade = 64;
 
 // Per-node layout (floats): step Phi 6 (packed lower: 00, 10, 11, 20, 21, 22), step chol 6, P_inf chol 6; then per
 // level l = 1..L the bridge A (9, row-major), K (9), chol Sigma (6); then per level l = 0..L-1 the margin sigma_br,
-// g and W (21, packed lower row-major).
+// g and W (21, packed lower row-major). With the split blocks (transient diffusion): Q1_0 and Q2_0 of the lattice
+// step (12, symmetric packed as the lower triangle); per level l = 1..L Phi_l (6), Q1_l (6), Q2_l (6); per level
+// l = 0..L-1 the input node's largest share f_l of the bridge residual (1).
 struct NoiseLayoutF {
   int levels;
+  bool split = false;
   static constexpr int kStepPhi = 0, kStepChol = 6, kPinfChol = 12;
-  BS_HD int stride() const { return 18 + 47 * levels; }
+  BS_HD int stride() const { return 18 + 47 * levels + (split ? 12 + 19 * levels : 0); }
   BS_HD int bridge(int l) const { return 18 + 24 * (l - 1); }
   BS_HD int margin(int l) const { return 18 + 24 * levels + 23 * l; }
+  BS_HD int split_step() const { return 18 + 47 * levels; }
+  BS_HD int split_level(int l) const { return 18 + 47 * levels + 12 + 18 * (l - 1); }
+  BS_HD int split_margin(int l) const { return 18 + 47 * levels + 12 + 18 * levels + l; }
 };
 
 struct NoiseModelH {
   double kq, a2, a3, sigma_o;
   int levels;
+  bool split = false;  // also the blocks of transient diffusion
 };
 
 namespace noise_host {
@@ -89,15 +96,18 @@ struct Sys {
   M3 A, GG;
 };
 
-inline Sys system_of(const NoiseModelH& m, LD a1) {
+// The noise sources of a system: both, the input node's only (D1) or the output node's only (D2); Q1 + Q2 = Q.
+enum class Sources { kBoth, kInput, kOutput };
+
+inline Sys system_of(const NoiseModelH& m, LD a1, Sources src = Sources::kBoth) {
   Sys s;
   s.A.m[0][0] = -a1;
   s.A.m[1][0] = m.a2;
   s.A.m[1][1] = -m.a2;
   s.A.m[2][1] = m.a3;
   s.A.m[2][2] = -m.a3;
-  s.GG.m[0][0] = 2 * static_cast<LD>(m.kq) * a1;
-  s.GG.m[1][1] = 2 * static_cast<LD>(m.sigma_o) * m.sigma_o * m.a2;
+  if (src != Sources::kOutput) s.GG.m[0][0] = 2 * static_cast<LD>(m.kq) * a1;
+  if (src != Sources::kInput) s.GG.m[1][1] = 2 * static_cast<LD>(m.sigma_o) * m.sigma_o * m.a2;
   return s;
 }
 
@@ -287,6 +297,64 @@ inline void margin_block(const NoiseModelH& m, const Sys& sys, LD a1, LD h, doub
     for (int j = 0; j <= i; ++j) out[idx++] = static_cast<double>(W[i][j]);
 }
 
+// The input node's largest share f = max_t V1 / (V1 + V2) of the bridge residual of n3 on a node of length h, with the
+// predictor of margin_block held fixed (noise_tables.cpp:271-325).
+inline LD margin_share(const NoiseModelH& m, const Sys& sys, LD a1, LD h) {
+  NoiseModelH m1 = m, m2 = m;
+  m1.sigma_o = 0;
+  m2.kq = 0;
+  const M3 P = stationary(m, a1), P1 = stationary(m1, a1), P2 = stationary(m2, a1);
+  constexpr int kPoints = 20;
+  M3 step, unused;
+  transition(sys, h / kPoints, step, unused);
+  M3 pw[kPoints + 1];
+  pw[0] = identity();
+  for (int i = 1; i <= kPoints; ++i) pw[i] = mul(pw[i - 1], step);
+  const M3& phi_h = pw[kPoints];
+  const auto cee = [&](const M3& Pk, LD (&C)[6][6]) {
+    const M3 PphiT = mul(Pk, tr(phi_h)), phiP = mul(phi_h, Pk);
+    for (int i = 0; i < 3; ++i) {
+      for (int j = 0; j < 3; ++j) {
+        C[i][j] = Pk.m[i][j];
+        C[i][j + 3] = PphiT.m[i][j];
+        C[i + 3][j] = phiP.m[i][j];
+        C[i + 3][j + 3] = Pk.m[i][j];
+      }
+    }
+  };
+  LD C[6][6], C1[6][6], C2[6][6], L6[6][6];
+  cee(P, C);
+  cee(P1, C1);
+  cee(P2, C2);
+  cholesky<6>(C, L6);
+  LD f = 0;
+  for (int iu = 1; iu < kPoints; ++iu) {
+    const auto c_of = [&](const M3& Pk, LD (&c)[6]) {
+      const M3 cL = mul(pw[iu], Pk), cR = mul(Pk, tr(pw[kPoints - iu]));
+      for (int j = 0; j < 3; ++j) {
+        c[j] = cL.m[2][j];
+        c[j + 3] = cR.m[2][j];
+      }
+    };
+    LD c[6], c1[6], c2[6], w[6];
+    c_of(P, c);
+    c_of(P1, c1);
+    c_of(P2, c2);
+    chol_solve<6>(L6, c, w);
+    const auto resid = [&](const M3& Pk, const LD (&ck)[6], const LD (&Ck)[6][6]) {
+      LD v = Pk.m[2][2];
+      for (int i = 0; i < 6; ++i) {
+        v -= 2 * w[i] * ck[i];
+        for (int j = 0; j < 6; ++j) v += w[i] * Ck[i][j] * w[j];
+      }
+      return std::max(v, LD(0));
+    };
+    const LD v1 = resid(P1, c1, C1), v2 = resid(P2, c2, C2);
+    if (v1 + v2 > 0) f = std::max(f, v1 / (v1 + v2));
+  }
+  return f;
+}
+
 }  // namespace noise_host
 
 struct NoiseTablesH {
@@ -295,7 +363,7 @@ struct NoiseTablesH {
   std::vector<float> data;  // n_nodes x stride
 };
 
-// The tables of one model (noise_tables.cpp:347-408 without the split blocks).
+// The tables of one model (noise_tables.cpp:347-408).
 inline NoiseTablesH build_noise_tables(const NoiseModelH& model) {
   using namespace noise_host;
   if (model.levels < 0 || model.levels > 10) throw std::invalid_argument("noise tables: levels must lie in [0, 10]");
@@ -304,7 +372,7 @@ inline NoiseTablesH build_noise_tables(const NoiseModelH& model) {
   const double dln = log_d(10.0) / kNoiseNodesPerDecade;
   t.inv_dln = 1.0 / dln;
   t.n_nodes = static_cast<int>(std::lround((kNoiseLnA1Max - kNoiseLnA1Min) * t.inv_dln)) + 1;
-  const NoiseLayoutF lay{model.levels};
+  const NoiseLayoutF lay{model.levels, model.split};
   t.stride = lay.stride();
   std::vector<double> d64(static_cast<size_t>(t.n_nodes) * t.stride, 0.0);
   const LD h0 = static_cast<LD>(kNoiseCellNs) * 1e-9L;
@@ -336,6 +404,26 @@ inline NoiseTablesH build_noise_tables(const NoiseModelH& model) {
     }
     for (int l = 0; l < model.levels; ++l) {
       margin_block(model, sys, a1, h0 / static_cast<LD>(int64_t{1} << l), row + lay.margin(l));
+    }
+    if (model.split) {
+      const Sys s_in = system_of(model, a1, Sources::kInput), s_out = system_of(model, a1, Sources::kOutput);
+      for (int l = 0; l <= model.levels; ++l) {
+        M3 phi, q1, q2;
+        const LD h = h0 / static_cast<LD>(int64_t{1} << l);
+        transition(s_in, h, phi, q1);
+        transition(s_out, h, phi, q2);
+        double* b = row + (l == 0 ? lay.split_step() : lay.split_level(l));
+        if (l > 0) {
+          pack_lower3(phis[l], b);
+          b += 6;
+        }
+        pack_lower3(q1, b);
+        pack_lower3(q2, b + 6);
+      }
+      for (int l = 0; l < model.levels; ++l) {
+        row[lay.split_margin(l)] =
+            static_cast<double>(margin_share(model, sys, a1, h0 / static_cast<LD>(int64_t{1} << l)));
+      }
     }
   }
   t.data.resize(d64.size());

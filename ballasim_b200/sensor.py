@@ -93,10 +93,6 @@ class SensorModel:
             raise ValueError("SensorModel: this build has no region-of-interest models")
         self._groups = _check_light_groups(light_groups)
         self._params = resolve(params, overrides)
-        if self._params.photoreceptor == "cascade" and self._params.noise and \
-                self._params.noise_diffusion != "frozen":
-            raise ValueError("SensorModel: this build runs the noise lattice with frozen diffusion "
-                             "(accuracy.noise_diffusion = 'frozen')")
         if self._params.photoreceptor == "cascade" and self._params.noise_on():
             raise ValueError("SensorModel: shot and background-activity noise run with the instantaneous response only")
         self._width, self._height, self._seed, self._camera = int(width), int(height), int(seed), int(camera)

@@ -392,7 +392,7 @@ class Ref:
             L.ref_label_s1.restype = C.c_uint8
             L.ref_label_s1.argtypes = [C.c_uint8]
             L.ref_noise_table.restype = C.c_int64
-            L.ref_noise_table.argtypes = [C.c_double] * 4 + [C.c_int, C.c_void_p, C.c_size_t]
+            L.ref_noise_table.argtypes = [C.c_double] * 4 + [C.c_int, C.c_int, C.c_void_p, C.c_size_t]
             L.ref_special.restype = None
             L.ref_special.argtypes = [C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]
             L.ref_readout_phase.restype = C.c_int64
@@ -444,13 +444,15 @@ class Ref:
             self.L = Ref.lib()
             self.width, self.height = width, height
             v = params.as_dict()
-            keys = list(self.KEYS) + ["reset_mode", "initial_phase", "photoreceptor", "noise", "initial_state"]
+            keys = list(self.KEYS) + ["reset_mode", "initial_phase", "photoreceptor", "noise", "initial_state",
+                                      "noise_diffusion"]
             vals = [float(v[k]) for k in self.KEYS] + [1.0 if v["reset_mode"] == "ideal" else 0.0,
                                                         {"uniform": 0.0, "symmetric": 1.0, "zero": 2.0}[
                                                             v["initial_phase"]],
                                                         0.0 if v["photoreceptor"] == "cascade" else 1.0,
                                                         1.0 if v["noise"] else 0.0,
-                                                        1.0 if v["initial_state"] == "stationary" else 0.0]
+                                                        1.0 if v["initial_state"] == "stationary" else 0.0,
+                                                        1.0 if v["noise_diffusion"] == "transient" else 0.0]
             ck = (C.c_char_p * len(keys))(*[k.encode() for k in keys])
             cv = (C.c_double * len(vals))(*vals)
             self.h = self.L.ref_model_create(v["family"].encode(), ck, cv, len(keys), width, height, seed, camera,

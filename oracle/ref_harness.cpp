@@ -70,7 +70,9 @@ void set_field(sensor::SensorParams& p, const std::string& key, double v) {
   else if (key == "sigma_o") p.sigma_o = v;
   else if (key == "noise_leaf_level") p.noise_leaf_level = static_cast<int32_t>(v);
   else if (key == "noise_margin_z") p.noise_margin_z = v;
-  else if (key == "initial_state") {
+  else if (key == "noise_diffusion") {
+    p.noise_diffusion = v == 0.0 ? sensor::NoiseDiffusion::kFrozen : sensor::NoiseDiffusion::kTransient;
+  } else if (key == "initial_state") {
     p.initial_state = v == 0.0 ? sensor::InitialState::kPhase : sensor::InitialState::kStationary;
   } else if (key == "stationary_burnin_ns") p.stationary_burnin_ns = static_cast<int64_t>(v);
   else if (key == "stationary_probe_pixels") p.stationary_probe_pixels = static_cast<int32_t>(v);
@@ -324,10 +326,12 @@ void ref_special(int which, const float* x, size_t n, float* out) {
   }
 }
 // The reference's fp32 noise-lattice tables (sensor/noise_tables.h NoiseTables, frozen diffusion): copies up to cap
-// floats; returns n_nodes * stride (stride = 18 + 47 levels).
-int64_t ref_noise_table(double kq, double a2, double a3, double sigma_o, int levels, float* out, size_t cap) {
+// floats; returns n_nodes * stride (stride = 18 + 47 levels, + 12 + 19 levels with the split blocks).
+int64_t ref_noise_table(double kq, double a2, double a3, double sigma_o, int levels, int split, float* out,
+                        size_t cap) {
   try {
     balla::sensor::NoiseModel nm{};
+    nm.split = split != 0;
     nm.kq = kq;
     nm.a2 = a2;
     nm.a3 = a3;

@@ -149,8 +149,9 @@ void hc_special(int which, const float* x, size_t n, float* out) {
 }
 
 // This build's noise tables (noise_build.h): copies up to cap floats; returns n_nodes * stride.
-int64_t hc_noise_table(double kq, double a2, double a3, double sigma_o, int levels, float* out, size_t cap) {
-  const NoiseTablesH t = build_noise_tables(NoiseModelH{kq, a2, a3, sigma_o, levels});
+int64_t hc_noise_table(double kq, double a2, double a3, double sigma_o, int levels, int split, float* out,
+                       size_t cap) {
+  const NoiseTablesH t = build_noise_tables(NoiseModelH{kq, a2, a3, sigma_o, levels, split != 0});
   std::memcpy(out, t.data.data(), std::min(cap, t.data.size()) * sizeof(float));
   return static_cast<int64_t>(t.data.size());
 }
@@ -165,7 +166,7 @@ struct HostLattice {
 };
 }  // namespace
 
-// lat: kq, sigma_o, margin_z, a2 = 1 / tau_o, a3 = 1 / tau_sf (fp64); levels; seed; camera.
+// lat: kq, sigma_o, margin_z, a2 = 1 / tau_o, a3 = 1 / tau_sf, transient (0 or 1) (fp64); levels; seed; camera.
 void* hl_create(uint32_t n, const float* on, const float* off, const float* leak, const float* dark, const float* phi0,
                 float scale, const float* consts, int ideal_reset, int64_t refractory_ns, const double* lat, int levels,
                 uint64_t seed, uint32_t camera) {
@@ -175,10 +176,10 @@ void* hl_create(uint32_t n, const float* on, const float* off, const float* leak
   delete b;
   h->base.k.seed = seed;
   h->base.k.camera = camera;
-  h->tables = build_noise_tables(NoiseModelH{lat[0], lat[3], lat[4], lat[1], levels});
+  h->tables = build_noise_tables(NoiseModelH{lat[0], lat[3], lat[4], lat[1], levels, lat[5] != 0.0});
   h->view = NoiseTableDev{h->tables.data.data(), h->tables.n_nodes, h->tables.stride, levels,
                           static_cast<float>(kNoiseLnA1Min), static_cast<float>(h->tables.inv_dln),
-                          static_cast<float>(lat[2])};
+                          static_cast<float>(lat[2]), lat[5] != 0.0 ? 1 : 0};
   h->lat.resize(n);
   return h;
 }
@@ -211,7 +212,8 @@ void hl_stationary(void* hp, int64_t t0, const float* frame, const double* maps6
   std::vector<HostPixel> px(b.n);
   for (uint32_t p = 0; p < b.n; ++p) px[p] = HostPixel{b.st[p], b.cq[p], h.lat[p]};
   StationaryInputs in{b.maps.data(), maps64, maps64 + b.n, maps64 + 2 * b.n, b.phi0.data(), frame, b.k, b.cc, h.view,
-                      NoiseModelH{st[0], st[1], st[2], st[3], h.view.levels}, st[4], st[5], burnin_ns, probe_pixels};
+                      NoiseModelH{st[0], st[1], st[2], st[3], h.view.levels, h.view.transient != 0}, st[4], st[5],
+                      burnin_ns, probe_pixels};
   stationary_start(px, in, t0);
   for (uint32_t p = 0; p < b.n; ++p) {
     b.st[p] = px[p].s;

@@ -41,7 +41,7 @@ def host(tmp_path_factory):
     H.hc_destroy.argtypes = [C.c_void_p]
     H.hc_special.argtypes = [C.c_int, C.c_void_p, C.c_size_t, C.c_void_p]
     H.hc_noise_table.restype = C.c_int64
-    H.hc_noise_table.argtypes = [C.c_double] * 4 + [C.c_int, C.c_void_p, C.c_size_t]
+    H.hc_noise_table.argtypes = [C.c_double] * 4 + [C.c_int, C.c_int, C.c_void_p, C.c_size_t]
     H.hl_create.restype = C.c_void_p
     H.hl_create.argtypes = [C.c_uint32] + [C.c_void_p] * 5 + [C.c_float, C.c_void_p, C.c_int, C.c_int64, C.c_void_p,
                                                               C.c_int, C.c_uint64, C.c_uint32]
@@ -145,7 +145,8 @@ def _host_vs_reference(host, ref, p, calls, t0, seed, n_calls=6, size=(12, 9)):
     lattice = bool(p.noise)
     pre = "hl" if lattice else "hc"
     if lattice:
-        lat = np.array([p.k * 1.602176634e-19, p.sigma_o, p.noise_margin_z, 1.0 / p.tau_o, 1.0 / p.tau_sf])
+        lat = np.array([p.k * 1.602176634e-19, p.sigma_o, p.noise_margin_z, 1.0 / p.tau_o, 1.0 / p.tau_sf,
+                        1.0 if p.noise_diffusion == "transient" else 0.0])
         h = host.hl_create(n, *[a.ctypes.data for a in arrs], float(np.float32(p.illuminance_scale)), cs.ctypes.data,
                            1 if p.reset_mode == "ideal" else 0, int(round(p.refractory_s * 1e9)), lat.ctypes.data,
                            int(p.noise_leaf_level), seed, 0)
@@ -197,13 +198,14 @@ def _same(W, want, got):
 def test_noise_tables_equal_the_reference(host, ref):
     """The lattice tables (noise_build.h, long double on the host) are the reference's NoiseTables, bit for bit."""
     L = ref.lib()
-    for k, tau_o, tau_sf, sigma_o, levels in [(1e16, 25e-6, 100e-6, 0.06, 5), (1e16, 100e-6, 25e-6, 0.06, 3),
-                                              (3e15, 40e-6, 200e-6, 0.02, 7), (1e16, 25e-6, 100e-6, 0.06, 0)]:
+    for k, tau_o, tau_sf, sigma_o, levels, split in [(1e16, 25e-6, 100e-6, 0.06, 5, 0), (1e16, 100e-6, 25e-6, 0.06, 3, 0),
+                                                     (3e15, 40e-6, 200e-6, 0.02, 7, 0), (1e16, 25e-6, 100e-6, 0.06, 0, 0),
+                                                     (1e16, 25e-6, 100e-6, 0.06, 5, 1), (3e15, 40e-6, 200e-6, 0.02, 2, 1)]:
         kq = k * 1.602176634e-19
-        cap = 800 * (18 + 47 * levels)
+        cap = 800 * (18 + 47 * levels + 12 + 19 * levels)
         a, b = np.zeros(cap, np.float32), np.zeros(cap, np.float32)
-        na = L.ref_noise_table(kq, 1 / tau_o, 1 / tau_sf, sigma_o, levels, a.ctypes.data, cap)
-        nb = host.hc_noise_table(kq, 1 / tau_o, 1 / tau_sf, sigma_o, levels, b.ctypes.data, cap)
+        na = L.ref_noise_table(kq, 1 / tau_o, 1 / tau_sf, sigma_o, levels, split, a.ctypes.data, cap)
+        nb = host.hc_noise_table(kq, 1 / tau_o, 1 / tau_sf, sigma_o, levels, split, b.ctypes.data, cap)
         assert na == nb > 0
         assert np.array_equal(a[:na].view(np.uint32), b[:nb].view(np.uint32)), levels
 
@@ -217,6 +219,11 @@ LATTICE_CASES = [
     ("prophesee_gen3", {"refractory_s": 0.0, "noise_margin_z": 3.0}, wide_calls, 0),
     ("samsung_gen3", {}, wide_calls, 65536 * 3 + 5),
     ("prophesee_gen3", {"sigma_o": 0.2, "sigma_theta_on": 0.03}, random_calls, 0),
+    ("prophesee_gen3", {"noise_diffusion": "transient"}, wide_calls, 0),
+    ("prophesee_gen3", {"noise_diffusion": "transient", "noise_leaf_level": 3, "leak_rate_hz": 2.0,
+                        "refractory_s": 0.0}, wide_calls, 12345),
+    ("samsung_gen3", {"noise_diffusion": "transient", "reset_mode": "ideal", "refractory_s": 0.0}, random_calls,
+     -65536 * 5),
 ]
 
 

@@ -170,6 +170,9 @@ def test_save_and_load_state_resume_bitwise(cuda_lib, family, overrides):
     ("prophesee_gen3", {"noise": True, "noise_leaf_level": 7, "reset_mode": "ideal", "refractory_s": 0.0},
      random_calls, -123456789),
     ("samsung_gen3", {"noise": True, "sigma_o": 0.2}, wide_calls, 65536 * 3 + 5),
+    ("prophesee_gen3", {"noise": True, "noise_diffusion": "transient"}, wide_calls, 0),
+    ("prophesee_gen3", {"noise": True, "noise_diffusion": "transient", "noise_leaf_level": 3, "leak_rate_hz": 2.0,
+                        "refractory_s": 0.0}, wide_calls, 12345),
     ("prophesee_gen3", {"noise": True, "initial_state": "stationary"}, random_calls, 0),
     ("prophesee_gen3", {"noise": True, "initial_state": "stationary", "stationary_burnin_ns": 300_000_000,
                         "leak_rate_hz": 2.0, "refractory_s": 0.0}, wide_calls, 12345),
@@ -373,7 +376,8 @@ def test_output_stage_follows_the_reference_order(cuda_lib, ref):
 
 @pytest.mark.parametrize("tile", [8, 4, 16])
 @pytest.mark.parametrize("case", ["blobs", "leak", "lattice", "lattice_leak", "lattice_staged", "lattice_leak_staged",
-                                  "lattice_dense_staged", "lattice_stationary_staged"])
+                                  "lattice_dense_staged", "lattice_stationary_staged", "lattice_transient_staged",
+                                  "lattice_transient"])
 def test_cascade_engine_equals_the_reference_chain(cuda_lib, ref, case, tile):
     """The fused engine with the cascade photoreceptor, with and without its noise lattice, gives the reference's own
     chain (WindowEngine<kHost> sampling, then the fp32 SensorModel on the runs, per window) bit for bit, over two
@@ -391,6 +395,8 @@ def test_cascade_engine_equals_the_reference_chain(cuda_lib, ref, case, tile):
     over = {**W.MISMATCH, "noise": case.startswith("lattice")}
     if "stationary" in case:
         over.update(initial_state="stationary", stationary_burnin_ns=400_000_000)
+    if "transient" in case:
+        over.update(noise_diffusion="transient")
     if "leak" in case:
         over.update(leak_rate_hz=2.0, leak_sigma_log10=0.1, refractory_s=0.0)
     p = resolve("prophesee_gen3", over)

@@ -88,7 +88,4 @@ def test_sensor_model_argument_checks():
         SensorModel("ideal", 8, 8, 1, [{"type": "constant"}], 0, device="cpu")
     with pytest.raises(ValueError):
         SensorModel("ideal", 8, 8, 1, [{"type": "fourier", "f0_hz": 100, "a": [0.1], "phi": [0]}], 0)
-    with pytest.raises(ValueError):
-        SensorModel("prophesee_gen3", 8, 8, 1, [{"type": "constant"}], 0,
-                    overrides={"noise_diffusion": "transient"})  # the lattice runs frozen diffusion only
 
