@@ -186,6 +186,19 @@ BS_HD int64_t output_cut(const ReadoutDev& r, int64_t t_end) {
 }
 
 // One output event (OutEvent, src/engine/output.h:25-32, without the ground-truth fields): 24 bytes.
+// Device event columns (any pointer null: that column is skipped).
+struct EventColumnsDev {
+  uint32_t* pixel;
+  uint16_t *x, *y;
+  uint8_t* p;
+  int64_t *t_cross, *t_reported;
+  uint8_t* label;
+  uint16_t* flags;
+  float *ds, *dn, *dl, *l_first;
+};
+cudaError_t event_columns(const RawEvent* ev, uint32_t n, uint32_t width, const ReadoutDev& rd,
+                          const EventColumnsDev& cols, cudaStream_t stream);
+
 struct OutRecord {
   int64_t t_reported, t_cross;
   uint16_t x, y, flags;

@@ -6,6 +6,9 @@
 // them out. (t_cross, pixel) is unique per event (a pixel fires at most once per ns), so the order is the host
 // sort's exactly.
 //
+// event_columns: the sorted records split into event columns (x, y from the pixel index, the readout's reported time)
+// on the device, so that the host copies each column out whole.
+//
 // output_stage: the engine's output stage (Camera::output, src/engine/engine_impl.h:1761-1847): records with the
 // readout's reported time, three stable radix passes (t_cross, (x, y), t_reported) that order them by
 // (t_reported, x, y, t_cross) as src/sensor/output_order.h:88-107 does, and the cut of the released prefix.
@@ -184,6 +187,34 @@ cudaError_t output_stage(const OutRecord* held, uint32_t n_held, const RawEvent*
     idx_alt = t;
   }
   gather_out_kernel<<<grid, 256, 0, stream>>>(all, idx, n, limit, out, ready_dev);
+  return cudaGetLastError();
+}
+
+// ---- event columns: the sorted records split into the caller's columns on the device ----
+namespace {
+__global__ void columns_kernel(const RawEvent* ev, uint32_t n, uint32_t width, ReadoutDev rd, EventColumnsDev c) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const RawEvent e = ev[i];
+  if (c.pixel) c.pixel[i] = e.pixel;
+  if (c.x) c.x[i] = static_cast<uint16_t>(e.pixel % width);
+  if (c.y) c.y[i] = static_cast<uint16_t>(e.pixel / width);
+  if (c.p) c.p[i] = e.polarity;
+  if (c.t_cross) c.t_cross[i] = e.t_cross;
+  if (c.t_reported) c.t_reported[i] = reported_time(rd, e.t_cross);
+  if (c.label) c.label[i] = e.label;
+  if (c.flags) c.flags[i] = e.flags;
+  if (c.ds) c.ds[i] = e.ds;
+  if (c.dn) c.dn[i] = e.dn;
+  if (c.dl) c.dl[i] = e.dl;
+  if (c.l_first) c.l_first[i] = e.l_first;
+}
+}  // namespace
+
+cudaError_t event_columns(const RawEvent* ev, uint32_t n, uint32_t width, const ReadoutDev& rd,
+                          const EventColumnsDev& cols, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  columns_kernel<<<(n + 255) / 256, 256, 0, stream>>>(ev, n, width, rd, cols);
   return cudaGetLastError();
 }
 

@@ -14,6 +14,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/ballasim_b200.h"
@@ -644,6 +645,60 @@ struct Model {
   mutable DevBuf<RawEvent> sorted;
   mutable DevBuf<unsigned char> sort_scratch;
   mutable PinBuf<RawEvent> staged;
+  mutable DevBuf<unsigned char> col_dev;
+  mutable PinBuf<unsigned char> col_pin;
+
+  // The events of a device buffer, sorted on the device, split there into the requested columns (256-byte aligned,
+  // side by side), copied out in one transfer through pinned memory, then each column into the caller's array.
+  void download_columns(const RawEvent* dev, size_t count, bs_event_columns* o, cudaStream_t s) const {
+    if (count == 0) return;
+    if (count > 0x7fffffffull) throw std::invalid_argument("too many events in one call");
+    const uint32_t n = static_cast<uint32_t>(count);
+    sorted.ensure(count);
+    sort_scratch.ensure(sort_events_scratch_bytes(n));
+    CK(sort_events(dev, n, sorted.p, sort_scratch.p, s));
+    struct Col {
+      void* dst;
+      size_t elem;
+      size_t at;
+    };
+    Col cols[12] = {{o->pixel, 4, 0},      {o->x, 2, 0},     {o->y, 2, 0},  {o->p, 1, 0},
+                    {o->t_cross_ns, 8, 0}, {o->t_reported_ns, 8, 0},        {o->label, 1, 0},
+                    {o->flags, 2, 0},      {o->ds, 4, 0},    {o->dn, 4, 0}, {o->dl, 4, 0},
+                    {o->l_first, 4, 0}};
+    size_t total = 0;
+    for (Col& c : cols) {
+      if (!c.dst) continue;
+      c.at = total;
+      total += (c.elem * count + 255) & ~size_t{255};
+    }
+    if (total == 0) return;
+    col_dev.ensure(total);
+    col_pin.ensure(total);
+    unsigned char* base = col_dev.p;
+    const auto at = [&](int i) { return cols[i].dst ? static_cast<void*>(base + cols[i].at) : nullptr; };
+    const EventColumnsDev d{static_cast<uint32_t*>(at(0)), static_cast<uint16_t*>(at(1)),
+                            static_cast<uint16_t*>(at(2)), static_cast<uint8_t*>(at(3)),
+                            static_cast<int64_t*>(at(4)), static_cast<int64_t*>(at(5)),
+                            static_cast<uint8_t*>(at(6)), static_cast<uint16_t*>(at(7)),
+                            static_cast<float*>(at(8)),   static_cast<float*>(at(9)),
+                            static_cast<float*>(at(10)),  static_cast<float*>(at(11))};
+    CK(event_columns(sorted.p, n, width, readout(), d, s));
+    CK(cudaMemcpyAsync(col_pin.p, col_dev.p, total, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const auto copy = [&](const Col& c) { std::memcpy(c.dst, col_pin.p + c.at, c.elem * count); };
+    if (count < 65536) {
+      for (const Col& c : cols) {
+        if (c.dst) copy(c);
+      }
+    } else {
+      std::vector<std::thread> th;
+      for (const Col& c : cols) {
+        if (c.dst) th.emplace_back(copy, c);
+      }
+      for (std::thread& t : th) t.join();
+    }
+  }
 
   // ---- the output stage: events in output order, released at the model time's cut, the rest held ----
   DevBuf<OutRecord> out_held, out_all, out_sorted;
@@ -1669,7 +1724,7 @@ bs_status bs_model_download_events(bs_model* m, const bs_device_events* ev, bs_e
     NEED(m);
     NEED(ev);
     NEED(out);
-    m->columns(m->download_pinned(static_cast<const bs::RawEvent*>(ev->data), ev->count, m->own), ev->count, out);
+    m->download_columns(static_cast<const bs::RawEvent*>(ev->data), ev->count, out, m->own);
   });
 }
 bs_status bs_model_event_count(const bs_model* m, size_t* n) {
@@ -1684,7 +1739,7 @@ bs_status bs_model_take_events(bs_model* m, bs_event_columns* out) {
     NEED(m);
     NEED(out);
     if (m->kept.empty() && m->last_events > 0) {
-      m->columns(m->download_pinned(m->events.p, m->last_events, m->own), m->last_events, out);
+      m->download_columns(m->events.p, m->last_events, out, m->own);
     } else {
       m->columns(m->kept, out);
     }
