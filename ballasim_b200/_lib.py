@@ -95,6 +95,8 @@ _SIGS = {
     "bs_model_output_held": (C.c_int32, [_P, C.POINTER(C.c_size_t)]),
     "bs_model_reset_stats": (C.c_int32, [_P]),
     "bs_model_info": (C.c_int32, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_float), C.POINTER(C.c_int32)]),
+    "bs_model_set_photometry": (C.c_int32, [_P, C.c_double, _P, C.c_size_t]),
+    "bs_model_gain_map": (C.c_int32, [_P, _P]),
     "bs_model_state_bytes": (C.c_int32, [_P, C.POINTER(C.c_size_t)]),
     "bs_model_save_state": (C.c_int32, [_P, _P, C.c_size_t]),
     "bs_model_load_state": (C.c_int32, [_P, _P, C.c_size_t]),

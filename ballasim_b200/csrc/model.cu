@@ -255,6 +255,8 @@ struct Model {
   DevBuf<float> mapf;    // 6 x n
   DevBuf<double> mapd;   // 2 x n
   MapSoA map{};
+  std::vector<float> gain;  // set_photometry's per-pixel gains (empty: 1 everywhere)
+  double gain_max = 1.0;    // the largest of them (1 without a gain map)
   StateBufs st[2];
   StateSoA soa[2]{};
   int cur = 0;
@@ -288,8 +290,8 @@ struct Model {
     n = w * h;
     maps = draw_maps(p, seed, camera, n);
     CK(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
-    // make_constants (src/sensor/sensor_model.cpp:394-433), fp32, gain 1.
-    k.irr_max = static_cast<float>(1e9 / (p.illuminance_scale * 1.0));
+    // make_constants (src/sensor/sensor_model.cpp:394-433), fp32; the clamp at the largest gain.
+    k.irr_max = static_cast<float>(1e9 / (p.illuminance_scale * gain_max));
     k.eps_ci = static_cast<float>(p.eps_ci);
     k.label_cut = static_cast<float>(p.label_share_cut);
     k.ideal_reset = p.reset_mode == 1;
@@ -386,6 +388,34 @@ struct Model {
     }
   }
 
+  // A pixel's photocurrent per renderer unit, fp32 scale x gain (src/sensor/pixel.h:775).
+  float pixel_scale(uint32_t i) const {
+    return static_cast<float>(p.illuminance_scale) * (gain.empty() ? 1.0f : gain[i]);
+  }
+
+  // SensorModel::set_photometry (src/sensor/sensor_model.cpp:350-373): the scale and the gain map (g null: 1
+  // everywhere); the clamp follows the largest gain, and the states take it at the next init.
+  void set_photometry(double scale, const float* g, size_t n_gain) {
+    if (g && n_gain != n) {
+      throw std::invalid_argument("SensorModel.set_photometry: one gain per pixel of the frame (or none)");
+    }
+    if (!(scale > 0.0) || !std::isfinite(scale)) {
+      throw std::invalid_argument("SensorParams: illuminance_scale must be > 0");
+    }
+    double g_max = g ? 0.0 : 1.0;
+    for (size_t i = 0; g && i < n_gain; ++i) {
+      if (!(g[i] > 0.0f) || !std::isfinite(g[i])) {
+        throw std::invalid_argument("SensorModel.set_photometry: gains must be finite and > 0");
+      }
+      g_max = std::max(g_max, static_cast<double>(g[i]));
+    }
+    p.illuminance_scale = scale;
+    gain.assign(g, g ? g + n_gain : g);
+    gain_max = g_max;
+    k.irr_max = static_cast<float>(1e9 / (p.illuminance_scale * gain_max));
+    upload_maps();
+  }
+
   void upload_maps() {
     std::vector<float> f(6 * static_cast<size_t>(n));
     std::vector<double> d(2 * static_cast<size_t>(n));
@@ -394,7 +424,7 @@ struct Model {
       f[n + i] = static_cast<float>(maps.theta_off[i]);
       f[2 * static_cast<size_t>(n) + i] = static_cast<float>(maps.leak[i]);
       f[3 * static_cast<size_t>(n) + i] = static_cast<float>(maps.dark[i]);
-      f[4 * static_cast<size_t>(n) + i] = static_cast<float>(p.illuminance_scale) * 1.0f;
+      f[4 * static_cast<size_t>(n) + i] = pixel_scale(i);
       f[5 * static_cast<size_t>(n) + i] = static_cast<float>(maps.phi0[i]);
       d[i] = maps.ba_rate[i];
       // shot noise: lambda_max = r sqrt(100 fA / I_dk) over the pixel's fp32 dark current
@@ -494,7 +524,7 @@ struct Model {
       x.L.have_k1 = u32[3 * n + i];
       regs[i] = PixelMapRegs{static_cast<float>(maps.theta_on[i]), static_cast<float>(maps.theta_off[i]),
                              static_cast<float>(maps.leak[i]), static_cast<float>(maps.dark[i]),
-                             static_cast<float>(p.illuminance_scale) * 1.0f, 0.0, 0.0};
+                             pixel_scale(static_cast<uint32_t>(i)), 0.0, 0.0};
       phi0[i] = static_cast<float>(maps.phi0[i]);
     }
     NoiseTableDev host_tab = tab;
@@ -804,7 +834,12 @@ struct Model {
     return static_cast<uint32_t>(i64_words() * 8 + f32_words() * 4 + u32_words() * 4);
   }
   size_t state_bytes() const { return sizeof(Header) + static_cast<size_t>(n) * bytes_per_pixel(); }
-  uint64_t fingerprint() const { return fnv1a(&p, sizeof(p)); }
+  // The parameters, and the gains when some gain is not 1 (src/sensor/sensor_model.cpp:53-66).
+  uint64_t fingerprint() const {
+    const uint64_t h = fnv1a(&p, sizeof(p));
+    if (std::all_of(gain.begin(), gain.end(), [](float v) { return v == 1.0f; })) return h;
+    return fnv1a(gain.data(), gain.size() * sizeof(float), h);
+  }
 
   void save(uint8_t* out, size_t bytes) const {
     if (bytes != state_bytes()) throw std::invalid_argument("SensorModel.save_state: buffer size does not match");
@@ -1778,6 +1813,24 @@ bs_status bs_model_maps(const bs_model* m, double* on, double* off, double* leak
     if (leak) std::copy_n(m->maps.leak.data(), n, leak);
     if (dark) std::copy_n(m->maps.dark.data(), n, dark);
     if (phi0) std::copy_n(m->maps.phi0.data(), n, phi0);
+  });
+}
+bs_status bs_model_set_photometry(bs_model* m, double illuminance_scale, const float* gain, size_t n_gain) {
+  return guarded([&] {
+    NEED(m);
+    if (!gain && n_gain != 0) throw std::invalid_argument("SensorModel.set_photometry: gain is NULL");
+    m->set_photometry(illuminance_scale, gain, n_gain);
+  });
+}
+bs_status bs_model_gain_map(const bs_model* m, float* out) {
+  return guarded([&] {
+    NEED(m);
+    NEED(out);
+    if (m->gain.empty()) {
+      std::fill_n(out, m->n, 1.0f);
+    } else {
+      std::copy_n(m->gain.data(), m->n, out);
+    }
   });
 }
 bs_status bs_model_noise_maps(const bs_model* m, double* ba_rate_hz, double* shot_max_hz) {

@@ -153,13 +153,124 @@ def sampler_for(f: Field):
     return _samplers.get(f)
 
 
+def _render_batch(render, pixel: np.ndarray, t: np.ndarray, groups: int):
+    """One render call: the callable gets (pixel_ids uint32 (n,), t_ns int64 (n,)) and returns (irradiance (n,
+    groups), signature (n,)) (engine_module.cpp:227-262)."""
+    res = render(pixel, t)
+    e = np.ascontiguousarray(res[0], np.float32)
+    s = np.ascontiguousarray(res[1], np.uint64)
+    n = len(pixel)
+    if e.ndim != 2 or e.shape != (n, groups) or s.shape != (n,):
+        raise ValueError("render: the callable must return (irradiance (n, groups), signature (n,))")
+    return e, s
+
+
+def _host_window(t_w: int, ids: np.ndarray, lv: np.ndarray, ci: np.ndarray, cs: np.ndarray, render, midpoint,
+                 refine_signature: bool, max_refine_levels: int, min_split: int, cancel) -> tuple:
+    """The window with a Python callable as the renderer, breadth-first as the host WindowEngine runs it
+    (src/engine/window_impl.h:462-714): the lattice of every pixel rendered in one call (slot 0 is the carried
+    sample), round 0's flags (sampling.h:471-520), then up to max_refine_levels rounds, each rendering the listed
+    intervals' midpoints in one call and flagging their halves (sampling.h:612-660); the runs sorted by time per
+    pixel; ci / cs take each pixel's sample at t_w + 2^23. The midpoint triples of a round go to the device in one
+    launch (MidpointTest)."""
+    n, G = len(ids), ci.shape[1]
+    stats = {"pixels": n, "samples_by_round": [0], "flagged_signature": 0, "flagged_midpoint": 0,
+             "refine_cap_hits": 0, "band_samples_by_round": [0]}
+    if n == 0:
+        return np.zeros(0, np.int64), np.zeros((0, G), np.float32), np.zeros(1, np.int64), stats
+    if cancel is not None and cancel.is_set():
+        raise RuntimeError("window: batch: cancelled")
+    count = (np.int64(1) << lv.astype(np.int64)) + 1
+    off0 = np.zeros(n + 1, np.int64)
+    np.cumsum(count, out=off0[1:])
+    s0 = int(off0[-1])
+    owner = np.repeat(np.arange(n, dtype=np.int64), count)
+    j = np.arange(s0, dtype=np.int64) - off0[owner]
+    dt = j << (23 - lv.astype(np.int64)[owner])
+    irr = np.zeros((s0, G), np.float32)
+    sig = np.zeros(s0, np.uint64)
+    irr[off0[:-1]] = ci
+    sig[off0[:-1]] = cs
+    req = np.nonzero(j != 0)[0]
+    irr[req], sig[req] = _render_batch(render, ids[owner[req]], t_w + dt[req], G)
+    rounds = [len(req)]
+
+    def exceeds(a, m, b):
+        if midpoint is None or len(a) == 0:
+            return np.zeros(len(a), bool)
+        return midpoint.exceeds(irr[a], irr[m], irr[b])
+
+    # Round 0: interval (i - 1, i) of every slot i past a pixel's first; node k tests the triple (k - 1, k, k + 1).
+    i = req
+    cnt_i = count[owner[i]]
+    flip = (sig[i] != sig[i - 1]) if refine_signature else np.zeros(len(i), bool)
+    node = np.zeros(s0, bool)
+    inner = i[j[i] + 1 < cnt_i]
+    node[inner] = exceeds(inner - 1, inner, inner + 1)
+    mid = ((j[i] + 1 < cnt_i) & node[i]) | ((j[i] >= 2) & node[i - 1])
+    want = flip | mid
+    split = want & (dt[i] - dt[i - 1] >= min_split)
+    words = [int(flip.sum()), int((mid & ~flip).sum()), int((want & ~split).sum())]
+    lo, hi = i[split] - 1, i[split]
+    parts_dt, parts_owner, parts_irr, parts_sig = [dt], [owner], [irr], [sig]
+    samples = s0
+    k = 0
+    while True:
+        stats["flagged_signature"] += words[0]
+        stats["flagged_midpoint"] += words[1]
+        if k == max_refine_levels:
+            stats["refine_cap_hits"] += words[2] + len(lo)
+            break
+        stats["refine_cap_hits"] += words[2]
+        if len(lo) == 0:
+            break
+        if cancel is not None and cancel.is_set():
+            raise RuntimeError("window: refinement round: cancelled")
+        m = len(lo)
+        g = np.arange(samples, samples + m, dtype=np.int64)
+        d_g = (dt[lo] + dt[hi]) >> 1
+        o_g = owner[hi]
+        e_g, s_g = _render_batch(render, ids[o_g], t_w + d_g, G)
+        dt, owner = np.concatenate([dt, d_g]), np.concatenate([owner, o_g])
+        irr, sig = np.concatenate([irr, e_g]), np.concatenate([sig, s_g])
+        samples += m
+        s1 = (sig[lo] != sig[g]) if refine_signature else np.zeros(m, bool)
+        s2 = (sig[g] != sig[hi]) if refine_signature else np.zeros(m, bool)
+        bad = exceeds(lo, g, hi)
+        f1, f2 = s1 | bad, s2 | bad
+        p1 = f1 & (dt[g] - dt[lo] >= min_split)
+        p2 = f2 & (dt[hi] - dt[g] >= min_split)
+        words = [int(s1.sum() + s2.sum()), int((bad & ~s1).sum() + (bad & ~s2).sum()),
+                 int((f1 & ~p1).sum() + (f2 & ~p2).sum())]
+        # Candidates (lo, g), (g, hi) per listed interval, kept in order.
+        c_lo = np.stack([lo, g], 1).reshape(-1)
+        c_hi = np.stack([g, hi], 1).reshape(-1)
+        keep = np.stack([p1, p2], 1).reshape(-1)
+        lo, hi = c_lo[keep], c_hi[keep]
+        rounds.append(m)
+        k += 1
+    stats["samples_by_round"] = rounds
+    stats["band_samples_by_round"] = [0] * len(rounds)
+    order = np.lexsort((dt, owner))
+    last = off0[1:] - 1
+    ci[:] = irr[last]
+    cs[:] = sig[last]
+    off = np.zeros(n + 1, np.int64)
+    off[1:] = np.cumsum(np.bincount(owner, minlength=n))
+    return t_w + dt[order], irr[order], off, stats
+
+
 def sample_window(t_w: int, pixel_ids, levels, rank, carried_irr, carried_sig, render, *, refine_signature: bool,
                   midpoint, max_refine_levels: int, min_dt_ns: int, mid_levels=None, tau_jump_ns=None,
                   delta_ref: float = 0.0, half_ratio: float = 0.0, eps_jump=None, jump=None, counters: bool = False,
                   carried_class=None, cancel=None) -> WindowRuns:
-    """sample_window (engine_module.cpp:311-355) on the device field ``render``."""
-    if not isinstance(render, Field):
-        raise TypeError("sample_window: render must be a device field (ballasim_b200.fields.Field) on this build")
+    """sample_window (engine_module.cpp:311-355). ``render`` is a device field (ballasim_b200.fields.Field), sampled
+    inside the sampler kernel, or a Python callable render(pixel_ids, t_ns) -> (irradiance (n, groups), signature
+    (n,)) as the reference's host path takes (engine_module.cpp:227-305): that window runs breadth-first on the
+    host with the midpoint tests on the device."""
+    host = not isinstance(render, Field)
+    if host and not callable(render):
+        raise TypeError("sample_window: render must be a device field or a callable render(pixel_ids, t_ns)")
     if any(v is not None for v in (mid_levels, tau_jump_ns, eps_jump, jump, carried_class)) or delta_ref != 0.0 \
             or half_ratio != 0.0 or counters:
         raise ValueError("sample_window: the economy-schedule switches are not on this path (Phase 1 rules only)")
@@ -183,6 +294,15 @@ def sample_window(t_w: int, pixel_ids, levels, rank, carried_irr, carried_sig, r
     cs = np.array(carried_sig, np.uint64, copy=True).reshape(-1)
     if len(rk) != n or ci.shape[0] != n or len(cs) != n or len(lv) != n:
         raise ValueError("pixel_ids, levels, rank, carried_irr and carried_sig need one entry per pixel")
+    if host:
+        G = ci.shape[1]
+        if G < 1 or G > 8:
+            raise ValueError("need 1 to 8 light groups")
+        if midpoint is not None and (len(midpoint.m_min) != G or len(midpoint.m_max) != G):
+            raise ValueError("MidpointTest: one waveform range per light group is needed")
+        t, irr, off, stats = _host_window(int(t_w), ids, lv, ci, cs, render, midpoint, bool(refine_signature),
+                                          int(max_refine_levels), 2 * int(min_dt_ns), cancel)
+        return WindowRuns(ids.copy(), t, irr, off, ci, cs, stats)
     if ci.shape[1] != 1:
         raise ValueError("sample_window: this build samples one light group")
     rules = rules_struct(midpoint, refine_signature, max_refine_levels, min_dt_ns)

@@ -266,6 +266,33 @@ class SensorModel:
         _lib.check(_lib.lib().bs_model_maps(self._h, *(a[k].ctypes.data for k in a)))
         return {k: v.reshape(self._height, self._width) for k, v in a.items()}
 
+    def set_photometry(self, illuminance_scale: float, gain=None) -> None:
+        """Photometry (sensor_module.cpp:477-486): the photocurrent scale (fA per renderer unit on axis) and the
+        per-pixel gain map (height * width gains in pixel order, any shape; None: 1 everywhere). irr_max follows the
+        largest gain at once; the states take the photometry at the next init: call it before init."""
+        g = None
+        if gain is not None:
+            try:
+                g = np.ascontiguousarray(gain, np.float32).reshape(-1)
+            except (TypeError, ValueError):
+                raise TypeError("set_photometry: gain must be a float array") from None
+            if not np.all(np.isfinite(g) & (g > 0)):
+                raise ValueError("set_photometry: gains must be finite and > 0")
+        p = self._params.copy()
+        p.illuminance_scale = float(illuminance_scale)
+        p.validate()
+        with self._lock:
+            _lib.check(_lib.lib().bs_model_set_photometry(self._h, float(illuminance_scale),
+                                                          g.ctypes.data if g is not None else None,
+                                                          g.size if g is not None else 0))
+            self._params = p
+
+    def gain_map(self) -> np.ndarray:
+        """The static pixel gains (height, width), float32 (set_photometry; 1 everywhere by default)."""
+        g = np.zeros(self._width * self._height, np.float32)
+        _lib.check(_lib.lib().bs_model_gain_map(self._h, g.ctypes.data))
+        return g.reshape(self._height, self._width)
+
     def noise_maps(self) -> dict:
         """This build's noise maps (height, width): the background-activity rate and the shot-noise dominating
         rate r sqrt(100 fA / I_dk) of each pixel (Hz)."""

@@ -148,6 +148,13 @@ bs_status bs_model_noise_maps(const bs_model* m, double* ba_rate_hz, double* sho
  *  gpu_launch_ms_total x1000, gpu_launch_ms_max x1000]. */
 bs_status bs_model_stats(const bs_model* m, uint64_t out[9]);
 bs_status bs_model_reset_stats(bs_model* m);
+/* SensorModel.set_photometry (sensor_module.cpp:477-486, sensor_model.cpp:350-373): the photocurrent scale (fA
+ * per renderer unit) and the per-pixel gain map, width * height floats in pixel order (gain NULL, n_gain 0: 1
+ * everywhere). Each gain finite and > 0; irr_max becomes 1e9 fA / (scale x the largest gain). The states take the
+ * new photometry at the next init. */
+bs_status bs_model_set_photometry(bs_model* m, double illuminance_scale, const float* gain, size_t n_gain);
+/* SensorModel.gain_map (sensor_module.cpp:487-502): width * height gains (1 without a gain map). */
+bs_status bs_model_gain_map(const bs_model* m, float* out);
 /* time_ns, irr_max, initialized (sensor_model.h:212-236). */
 bs_status bs_model_info(const bs_model* m, int64_t* time_ns, float* irr_max, int32_t* initialized);
 /* save_state / load_state / state_bytes (sensor_model.h:175-178): this build's own blob (magic, version, shape,

@@ -126,6 +126,7 @@ class Port:
             L.orc_field_level.argtypes = [C.POINTER(OrcField), C.c_uint32, C.c_uint32, C.c_int64, C.c_int32,
                                           C.c_int32]
             L.orc_field_frame.argtypes = [C.POINTER(OrcField), C.c_int64, _f32p]
+            L.orc_field_samples.argtypes = [C.POINTER(OrcField), _u32p, _i64p, C.c_size_t, _f32p]
             L.orc_field_levels.argtypes = [C.POINTER(OrcField), C.c_int64, C.c_int32, C.c_int32, _u8p]
             L.orc_model_create.restype = C.c_void_p
             L.orc_model_create.argtypes = [C.POINTER(OrcParams), C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32,
@@ -181,6 +182,14 @@ class Port:
         s = field_struct(f)
         out = np.zeros(f.width * f.height, np.float32)
         cls.lib().orc_field_frame(C.byref(s), t_ns, out)
+        return out
+
+    @classmethod
+    def field_samples(cls, f, pixel, t_ns) -> np.ndarray:
+        s = field_struct(f)
+        px = np.ascontiguousarray(pixel, np.uint32)
+        out = np.zeros(len(px), np.float32)
+        cls.lib().orc_field_samples(C.byref(s), px, np.ascontiguousarray(t_ns, np.int64), len(px), out)
         return out
 
     @classmethod
@@ -380,10 +389,17 @@ class Ref:
             L.ref_model_maps.argtypes = [C.c_void_p, _f64p, _f64p, _f64p, _f64p, _f64p]
             L.ref_model_threads.restype = C.c_int
             L.ref_model_threads.argtypes = [C.c_void_p]
+            L.ref_model_irr_max.restype = C.c_float
+            L.ref_model_irr_max.argtypes = [C.c_void_p]
+            L.ref_model_set_photometry.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_size_t]
             L.ref_sample_window.restype = C.c_int64
             L.ref_sample_window.argtypes = [C.POINTER(OrcField), C.c_float, C.c_float, C.c_int, C.c_int, C.c_int,
                                             C.c_int64, C.c_int64, _u32p, _u8p, C.c_size_t, _f32p, _u64p, _i64p,
                                             _i64p, _f32p, C.c_size_t]
+            L.ref_sample_window_cb.restype = C.c_int64
+            L.ref_sample_window_cb.argtypes = [C.c_int, C.c_float, C.c_float, _f64p, _f64p, C.c_int, C.c_int, C.c_int,
+                                               C.c_int64, C.c_int64, _u32p, _u8p, C.c_size_t, _f32p, _u64p,
+                                               C.c_void_p, C.c_void_p, _i64p, _i64p, _f32p, C.c_size_t, _u64p]
             L.ref_output_order.argtypes = [_i64p, _u16p, _u16p, _i64p, C.c_size_t, C.c_uint32, _u32p]
             L.ref_reported_time.restype = C.c_int64
             L.ref_reported_time.argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_int64]
@@ -432,6 +448,50 @@ class Ref:
                 return t[:k], irr[:k], off, ci, cs
             cap = -k
 
+    RENDER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_int64), C.c_size_t,
+                            C.POINTER(C.c_float), C.POINTER(C.c_uint64))
+
+    @classmethod
+    def sample_window_cb(cls, render, groups, midpoint, refine_signature, max_refine_levels, min_dt_ns, t_w, pixel,
+                         level, carried_irr, carried_sig):
+        """WindowEngine<kHost> with the Python callable render(pixel_ids, t_ns) -> (irradiance (n, groups),
+        signature (n,)) as its renderer; midpoint: None or an object with tol, dark, m_min and m_max. Returns
+        (t, irr (S, groups), offsets, last_irradiance, last_signature, stats)."""
+        def fn(_user, px, tt, n, irr, sig):
+            if n == 0:
+                return 0
+            e, s = render(np.ctypeslib.as_array(px, (n,)).copy(), np.ctypeslib.as_array(tt, (n,)).copy())
+            np.ctypeslib.as_array(irr, (n * groups,))[:] = np.asarray(e, np.float32).reshape(-1)
+            np.ctypeslib.as_array(sig, (n,))[:] = np.asarray(s, np.uint64).reshape(-1)
+            return 0
+
+        cb = cls.RENDER_FN(fn)
+        n = len(pixel)
+        mn = np.asarray(midpoint.m_min if midpoint else [1.0] * groups, np.float64)
+        mx = np.asarray(midpoint.m_max if midpoint else [1.0] * groups, np.float64)
+        cap = max(16, int(np.sum((1 << np.asarray(level, np.int64)) + 1)) * 4)
+        while True:
+            off = np.zeros(n + 1, np.int64)
+            t = np.zeros(cap, np.int64)
+            irr = np.zeros(cap * groups, np.float32)
+            ci = np.array(carried_irr, np.float32).reshape(n, groups).copy()
+            cs = np.array(carried_sig, np.uint64).copy()
+            st = np.zeros(37, np.uint64)
+            k = cls.lib().ref_sample_window_cb(groups, midpoint.tol if midpoint else 0.0,
+                                               midpoint.dark if midpoint else 0.0, mn, mx, 1 if midpoint else 0,
+                                               1 if refine_signature else 0, max_refine_levels, min_dt_ns, t_w,
+                                               np.ascontiguousarray(pixel, np.uint32),
+                                               np.ascontiguousarray(level, np.uint8), n, ci.reshape(-1), cs,
+                                               C.cast(cb, C.c_void_p), None, off, t, irr, cap, st)
+            if k == np.iinfo(np.int64).min:
+                raise ValueError(cls.lib().ref_last_error().decode())
+            if k >= 0:
+                stats = {"flagged_signature": int(st[0]), "flagged_midpoint": int(st[1]),
+                         "refine_cap_hits": int(st[2]), "render_calls": int(st[3]),
+                         "samples_by_round": [int(v) for v in st[5:5 + int(st[4])]]}
+                return t[:k], irr[:k * groups].reshape(k, groups), off, ci, cs, stats
+            cap = -k
+
     class Model:
         # Overrides the harness understands (the SensorParams rows this path reads), from a resolved SensorParams.
         KEYS = ("theta_on", "theta_off", "sigma_theta_on", "sigma_theta_off", "theta_onoff_corr", "theta_floor",
@@ -468,6 +528,16 @@ class Ref:
         @property
         def threads(self) -> int:
             return self.L.ref_model_threads(self.h)
+
+        @property
+        def irr_max(self) -> float:
+            return self.L.ref_model_irr_max(self.h)
+
+        def set_photometry(self, scale, gain=None):
+            g = None if gain is None else np.ascontiguousarray(gain, np.float32).reshape(-1)
+            if self.L.ref_model_set_photometry(self.h, float(scale), None if g is None else g.ctypes.data,
+                                               0 if g is None else g.size) != 0:
+                raise ValueError(self.L.ref_last_error().decode())
 
         def init(self, t0, irr0):
             if self.L.ref_model_init(self.h, t0, np.ascontiguousarray(irr0, np.float32)) != 0:

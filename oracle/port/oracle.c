@@ -309,6 +309,10 @@ void orc_field_frame(const orc_field* f, int64_t t_ns, float* out) {
     for (uint32_t x = 0; x < f->width; ++x) out[(size_t)y * f->width + x] = orc_field_eval(f, x, y, t_ns);
 }
 
+void orc_field_samples(const orc_field* f, const uint32_t* pixel, const int64_t* t_ns, size_t n, float* out) {
+  for (size_t i = 0; i < n; ++i) out[i] = orc_field_eval(f, pixel[i] % f->width, pixel[i] / f->width, t_ns[i]);
+}
+
 void orc_field_levels(const orc_field* f, int64_t t_w, int32_t l_min, int32_t l_max, uint8_t* out) {
   for (uint32_t y = 0; y < f->height; ++y)
     for (uint32_t x = 0; x < f->width; ++x)

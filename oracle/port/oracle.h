@@ -52,6 +52,8 @@ int32_t orc_field_level(const orc_field* f, uint32_t x, uint32_t y, int64_t t_w,
 
 void orc_field_frame(const orc_field* f, int64_t t_ns, float* out);              /* width x height */
 void orc_field_levels(const orc_field* f, int64_t t_w, int32_t l_min, int32_t l_max, uint8_t* out);
+/* The field at (pixel id, t) pairs, as a renderer callback would sample it. */
+void orc_field_samples(const orc_field* f, const uint32_t* pixel, const int64_t* t_ns, size_t n, float* out);
 
 /* ---- sensor parameters (src/sensor/params.h:65-176) ---- */
 typedef struct {

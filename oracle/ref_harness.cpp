@@ -204,6 +204,18 @@ void ref_model_maps(void* h, double* on, double* off, double* leak, double* dark
 }
 
 int64_t ref_model_time(void* h) { return static_cast<RefModel*>(h)->model->time_ns(); }
+float ref_model_irr_max(void* h) { return static_cast<RefModel*>(h)->model->irr_max(); }
+
+// SensorModel::set_photometry; gain NULL (n 0): 1 everywhere.
+int ref_model_set_photometry(void* h, double scale, const float* gain, size_t n) {
+  try {
+    static_cast<RefModel*>(h)->model->set_photometry(scale, gain ? std::vector<float>(gain, gain + n)
+                                                                 : std::vector<float>{});
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
 int ref_model_threads(void* h) { return static_cast<RefModel*>(h)->model->num_threads(); }
 
 // The window's samples by WindowEngine<kHost>::run (src/engine/window_impl.h:715-867). Returns the sample count
@@ -229,6 +241,85 @@ int64_t ref_sample_window(const orc_field* f, float tol, float dark, int midpoin
     if (s > cap) return -static_cast<int64_t>(s);
     std::memcpy(t_out, eng.t(), s * sizeof(int64_t));
     std::memcpy(irr_out, eng.irr(), s * sizeof(float));
+    return static_cast<int64_t>(s);
+  } catch (const std::exception& e) {
+    fail(e);
+    return INT64_MIN;
+  }
+}
+
+// A C callback as the renderer (the role engine_module.cpp:227-262 gives a Python callable): pixel ids and absolute
+// times in request order, irradiance (n, groups) and signatures (n,) back; a non-zero return fails the window.
+typedef int (*ref_render_fn)(void* user, const uint32_t* pixel, const int64_t* t, size_t n, float* irr, uint64_t* sig);
+
+class CallbackHook final : public engine::RenderHook {
+ public:
+  CallbackHook(ref_render_fn fn, void* user, int64_t t_w, int groups) : fn_(fn), user_(user), t_w_(t_w), g_(groups) {}
+  void render(render::SampleRequest* req, size_t n, const uint32_t* out_index, float* irr, uint64_t* sig, uint32_t*,
+              uint32_t) override {
+    std::vector<uint32_t> px(n);
+    std::vector<int64_t> t(n);
+    std::vector<float> e(n * static_cast<size_t>(g_));
+    std::vector<uint64_t> s(n);
+    for (size_t i = 0; i < n; ++i) {
+      px[i] = req[i].pixel;
+      t[i] = t_w_ + req[i].t_off_ns;
+    }
+    if (fn_(user_, px.data(), t.data(), n, e.data(), s.data()) != 0) throw std::runtime_error("render callback failed");
+    for (size_t i = 0; i < n; ++i) {
+      std::memcpy(irr + static_cast<size_t>(out_index[i]) * g_, e.data() + i * g_, g_ * sizeof(float));
+      sig[out_index[i]] = s[i];
+    }
+    ++calls_;
+  }
+  size_t calls_ = 0;
+
+ private:
+  ref_render_fn fn_;
+  void* user_;
+  int64_t t_w_;
+  int g_;
+};
+
+// sample_window with a renderer callback (engine_module.cpp:265-355 on WindowEngine<kHost>), groups light groups and
+// the midpoint test's waveform ranges m_min / m_max (midpoint 0: none). As ref_sample_window (irr_out (S, groups));
+// stats: flagged_signature, flagged_midpoint, refine_cap_hits, render calls, rounds, then samples_by_round (at most
+// 32 rounds written).
+int64_t ref_sample_window_cb(int groups, float tol, float dark, const double* m_min, const double* m_max, int midpoint,
+                             int refine_signature, int max_refine_levels, int64_t min_dt_ns, int64_t t_w,
+                             const uint32_t* pixel, const uint8_t* level, size_t n, float* carried_irr,
+                             uint64_t* carried_sig, ref_render_fn fn, void* user, int64_t* offsets, int64_t* t_out,
+                             float* irr_out, size_t cap, uint64_t* stats) {
+  try {
+    engine::SampleConfig cfg = make_config(tol, dark, 0, refine_signature, max_refine_levels, min_dt_ns);
+    cfg.groups = groups;
+    if (midpoint != 0) {
+      std::vector<std::pair<double, double>> ranges;
+      for (int g = 0; g < groups; ++g) ranges.emplace_back(m_min[g], m_max[g]);
+      cfg.rules.midpoint = true;
+      cfg.rules.mid = engine::midpoint_params(tol, dark, ranges);
+    }
+    engine::WindowEngine<engine::Space::kHost> eng;
+    CallbackHook hook(fn, user, t_w, groups);
+    engine::WindowEngine<engine::Space::kHost>::Input in{};
+    in.t_w = t_w;
+    in.pixel = pixel;
+    in.level = level;
+    in.n = n;
+    in.carried_irr = carried_irr;
+    in.carried_sig = carried_sig;
+    const engine::WindowStats st = eng.run(in, cfg, hook, std::numeric_limits<size_t>::max(), nullptr);
+    stats[0] = st.flagged_signature;
+    stats[1] = st.flagged_midpoint;
+    stats[2] = st.refine_cap_hits;
+    stats[3] = hook.calls_;
+    stats[4] = st.samples_by_round.size();
+    for (size_t k = 0; k < st.samples_by_round.size() && k < 32; ++k) stats[5 + k] = st.samples_by_round[k];
+    const size_t s = eng.samples();
+    std::memcpy(offsets, eng.offsets(), (n + 1) * sizeof(int64_t));
+    if (s > cap) return -static_cast<int64_t>(s);
+    std::memcpy(t_out, eng.t(), s * sizeof(int64_t));
+    std::memcpy(irr_out, eng.irr(), s * static_cast<size_t>(groups) * sizeof(float));
     return static_cast<int64_t>(s);
   } catch (const std::exception& e) {
     fail(e);

@@ -431,3 +431,84 @@ def test_engine_refuses_mixed_photoreceptors_and_cascade_options(cuda_lib):
     eng = Engine([(casc, spec.field)], tol=r.tol, dark=r.dark, min_dt_ns=r.min_dt_ns)
     with pytest.raises(ValueError):
         eng.set_launch(0, 0, 16, 8)
+
+
+@pytest.mark.parametrize("family,overrides", [
+    ("ideal", W.MISMATCH),
+    ("prophesee_gen3", {"noise": False}),
+    ("prophesee_gen3", {"noise": True, "initial_state": "stationary", "stationary_burnin_ns": 300_000_000}),
+])
+def test_photometry_gain_map_equals_the_reference(cuda_lib, ref, family, overrides):
+    """set_photometry (sensor_module.cpp:477-502): a scale and a per-pixel gain map move irr_max to the largest gain
+    and each pixel's photocurrent to scale x gain; the model's events equal the reference's own after the same call,
+    bit for bit, and a state saved under one gain map does not load under another."""
+    from ballasim_b200.sensor import SensorModel
+
+    p = resolve(family, overrides)
+    Wd, Hd, seed = 24, 20, 31
+    n = Wd * Hd
+    rng = np.random.default_rng(seed)
+    gain = rng.uniform(0.4, 1.6, (Hd, Wd)).astype(np.float32)
+    dev = SensorModel(p, Wd, Hd, seed, [{"type": "constant"}], 0)
+    ora = ref.Model(p, Wd, Hd, seed, 0)
+    assert np.array_equal(dev.gain_map(), np.ones((Hd, Wd), np.float32))
+    dev.set_photometry(2.5, gain)
+    ora.set_photometry(2.5, gain)
+    assert np.array_equal(dev.gain_map(), gain)
+    assert dev.params.illuminance_scale == 2.5
+    assert np.float32(dev.irr_max) == np.float32(ora.irr_max)
+    assert dev.irr_max == np.float32(1e9 / (2.5 * float(gain.max())))
+    irr0 = rng.uniform(5, 400, n).astype(np.float32)
+    dev.init(0, irr0.reshape(n, 1))
+    ora.init(0, irr0)
+    got = []
+    for ids, tt, vv, t_end, starts, cnt in random_calls(rng, n, 0, 4):
+        got.append(dev.advance_runs(ids, tt, vv, t_end, starts, cnt))
+        ora.advance_runs(ids, tt, vv, starts, cnt, t_end)
+    merged = {k: np.concatenate([g[k] for g in got]) for k in got[0]}
+    same_events(merged, ora.take_events(), Wd)
+    assert len(merged["t_cross_ns"]) > 100
+    blob = dev.save_state()
+    other = SensorModel(p, Wd, Hd, seed, [{"type": "constant"}], 0)
+    other.set_photometry(2.5, np.where(gain > 1, gain, 1).astype(np.float32))
+    with pytest.raises(ValueError):
+        other.load_state(blob)
+    other.set_photometry(2.5, gain)
+    other.load_state(blob)
+    for bad in (np.ones(n - 1, np.float32), np.full(n, -1.0, np.float32), np.full(n, np.inf, np.float32)):
+        with pytest.raises(ValueError):
+            other.set_photometry(1.0, bad)
+    with pytest.raises(ValueError):
+        other.set_photometry(0.0)
+    other.set_photometry(1.0)
+    assert np.array_equal(other.gain_map(), np.ones((Hd, Wd), np.float32))
+    assert other.irr_max == np.float32(1e9)
+
+
+@pytest.mark.parametrize("family,overrides", [("ideal", W.MISMATCH), ("prophesee_gen3", W.MISMATCH),
+                                              ("prophesee_gen3", {**W.MISMATCH, "noise": True})])
+def test_engine_with_a_gain_map_equals_the_reference_chain(cuda_lib, ref, family, overrides):
+    """The fused engine reads each pixel's scale x gain and the camera's clamp: with a vignetting-like gain map its
+    events equal the reference's chain under the same set_photometry."""
+    from ballasim_b200.engine import Engine
+    from ballasim_b200.sensor import SensorModel
+
+    wl = W.small("blobs", 60, 40, 12)
+    spec, r = wl.sensors[0], wl.rules
+    p = resolve(family, overrides)
+    yy, xx = np.mgrid[0:spec.height, 0:spec.width]
+    rr = ((xx - spec.width / 2) ** 2 + (yy - spec.height / 2) ** 2) / (spec.width / 2) ** 2
+    gain = (1.0 / (1.0 + 0.5 * rr) ** 2).astype(np.float32)
+    o = ref.Model(p, spec.width, spec.height, spec.seed, spec.camera)
+    o.set_photometry(0.8, gain)
+    want, st = o.simulate(spec.field, r, wl.windows)
+    m = SensorModel(p, spec.width, spec.height, spec.seed, [{"type": "constant"}], spec.camera)
+    m.set_photometry(0.8, gain)
+    eng = Engine([(m, spec.field)], tol=r.tol, dark=r.dark, min_dt_ns=r.min_dt_ns,
+                 max_refine_levels=r.max_refine_levels, l_min=r.l_min, l_max=r.l_max)
+    eng.start(0)
+    s, _ = eng.run(wl.windows)
+    ev = m.take_events()
+    assert s == st["pixel_samples"]
+    same_events(ev, want, spec.width)
+    assert len(ev["t_cross_ns"]) > 100

@@ -1,0 +1,157 @@
+"""sample_window with a Python callable as the renderer (engine_module.cpp:227-355): the window runs breadth-first on
+the host as the reference's WindowEngine<kHost> does, and its runs, carried samples and round statistics equal the
+reference's own engine driven by the same callable through the harness. Signature-only rules need no device (the
+CPU cases); the midpoint test's triples go to the device (the gpu cases), which also check that a host callable
+evaluating the field gives the device-field sampler's runs bit for bit."""
+import numpy as np
+import pytest
+
+from ballasim_b200 import fields as F
+from ballasim_b200 import workloads as W
+
+
+def _fast_blobs():
+    """Small blobs crossing pixels within a window: midpoint flags at coarse lattice levels."""
+    return F.blobs(24, 18, 5, 6, r_lo=1.5, r_hi=4.0, v_sigma=3000.0)
+
+
+def _field_render(port, f, groups=1, step=None):
+    """A renderer callable on the oracle's field: group g is the field at t + g x 1 ms scaled by 1 / (g + 1); the
+    signature counts the steps of `step` below group 0 (0 everywhere without a step)."""
+
+    def render(pixel, t):
+        cols = [port.field_samples(f, pixel, t + g * 1_000_000) / np.float32(g + 1) for g in range(groups)]
+        e = np.stack(cols, 1).astype(np.float32)
+        s = np.zeros(len(pixel), np.uint64) if step is None else np.floor(e[:, 0] / step).astype(np.uint64)
+        return e, s
+
+    return render
+
+
+def _same_runs(runs, want):
+    t, irr, off, ci, cs, st = want
+    assert np.array_equal(runs.offsets, off)
+    assert np.array_equal(runs.t_ns, t)
+    assert np.array_equal(runs.irradiance.view(np.uint32), irr.view(np.uint32))
+    assert np.array_equal(runs.last_irradiance.view(np.uint32), ci.view(np.uint32))
+    assert np.array_equal(runs.last_signature, cs)
+    for k in ("flagged_signature", "flagged_midpoint", "refine_cap_hits", "samples_by_round"):
+        assert runs.stats[k] == st[k], k
+    assert runs.stats["band_samples_by_round"] == [0] * len(st["samples_by_round"])
+
+
+def _window_case(port, ref, f, n_px, groups, step, midpoint, refine_signature, max_refine_levels, min_dt_ns,
+                 windows=2, listed=False, seed=3, level_cap=8):
+    from ballasim_b200.sampling import sample_window
+
+    rng = np.random.default_rng(seed)
+    ids = np.arange(n_px, dtype=np.uint32) if not listed else rng.permutation(n_px)[: n_px // 2].astype(np.uint32)
+    render = _field_render(port, f, groups, step)
+    carried, sig = render(ids, np.zeros(len(ids), np.int64))
+    c_ref, s_ref = carried.copy(), sig.copy()
+    max_level = 23 - (min_dt_ns.bit_length() - 1)
+    rounds = 0
+    for w in range(windows):
+        t_w = w << 23
+        lv = np.minimum(port.levels(f, t_w, 0, level_cap)[ids] + (ids % 3).astype(np.uint8), max_level)
+        lv = lv.astype(np.uint8)
+        want = ref.sample_window_cb(render, groups, midpoint, refine_signature, max_refine_levels, min_dt_ns, t_w, ids,
+                                    lv, c_ref, s_ref)
+        runs = sample_window(t_w, ids, lv, np.arange(len(ids)), carried, sig, render,
+                             refine_signature=refine_signature, midpoint=midpoint,
+                             max_refine_levels=max_refine_levels, min_dt_ns=min_dt_ns)
+        _same_runs(runs, want)
+        carried, sig = runs.last_irradiance, runs.last_signature
+        c_ref, s_ref = want[3], want[4]
+        rounds = max(rounds, len(want[5]["samples_by_round"]))
+    return rounds
+
+
+@pytest.mark.parametrize("groups,max_refine_levels,min_dt_ns,listed,fast", [
+    (1, 4, 8192, False, False),
+    (1, 0, 8192, False, False),
+    (3, 6, 1024, True, False),
+    (2, 2, 1 << 16, False, False),
+    (1, 10, 2048, False, True),
+])
+def test_signature_refinement_equals_the_reference_engine(oracle_port, ref, groups, max_refine_levels, min_dt_ns,
+                                                          listed, fast):
+    f = _fast_blobs() if fast else W.small("blobs", 24, 18, 1).sensors[0].field
+    rounds = _window_case(oracle_port, ref, f, 24 * 18, groups, 9.0, None, True, max_refine_levels, min_dt_ns,
+                          listed=listed, level_cap=2 if fast else 8)
+    assert rounds >= min(max_refine_levels, 1) + 1
+
+
+def test_no_refinement_and_edge_inputs(oracle_port, ref):
+    from ballasim_b200.sampling import sample_window
+
+    f = W.small("edge", 16, 8, 1).sensors[0].field
+    # Signatures off: the lattice alone, whatever the callable's signatures.
+    _window_case(oracle_port, ref, f, 16 * 8, 1, 5.0, None, False, 5, 8192)
+    render = _field_render(oracle_port, f)
+    empty = sample_window(0, np.zeros(0, np.uint32), np.zeros(0, np.uint8), np.zeros(0, np.uint32),
+                          np.zeros((0, 1), np.float32), np.zeros(0, np.uint64), render, refine_signature=True,
+                          midpoint=None, max_refine_levels=3, min_dt_ns=8192)
+    assert empty.offsets.tolist() == [0] and len(empty.t_ns) == 0 and empty.stats["samples_by_round"] == [0]
+    ids = np.arange(4, dtype=np.uint32)
+    one = np.ones((4, 1), np.float32)
+    with pytest.raises(ValueError):  # a callable that returns the wrong shape
+        sample_window(0, ids, np.zeros(4, np.uint8), ids, one, np.zeros(4, np.uint64),
+                      lambda p, t: (np.zeros(len(p), np.float32), np.zeros(len(p), np.uint64)),
+                      refine_signature=True, midpoint=None, max_refine_levels=1, min_dt_ns=8192)
+    with pytest.raises(ValueError):  # a level finer than min_dt_ns allows
+        sample_window(0, ids, np.full(4, 11, np.uint8), ids, one, np.zeros(4, np.uint64), render,
+                      refine_signature=True, midpoint=None, max_refine_levels=1, min_dt_ns=8192)
+    with pytest.raises(TypeError):
+        sample_window(0, ids, np.zeros(4, np.uint8), ids, one, np.zeros(4, np.uint64), object(),
+                      refine_signature=True, midpoint=None, max_refine_levels=1, min_dt_ns=8192)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("groups,refine_signature,max_refine_levels,min_dt_ns", [
+    (1, True, 8, 2048),
+    (1, False, 3, 8192),
+    (2, True, 5, 4096),
+])
+def test_midpoint_refinement_equals_the_reference_engine(cuda_lib, oracle_port, ref, groups, refine_signature,
+                                                         max_refine_levels, min_dt_ns):
+    from ballasim_b200.sampling import MidpointTest
+
+    r = W.small("blobs", 24, 18, 1).rules
+    ranges = [(1.0, 1.0), (0.4, 1.0)][:groups]
+    mt = MidpointTest(r.tol, r.dark, [a for a, _ in ranges], [b for _, b in ranges])
+    rounds = _window_case(oracle_port, ref, _fast_blobs(), 24 * 18, groups, 12.0 if refine_signature else None, mt,
+                          refine_signature, max_refine_levels, min_dt_ns, windows=3, listed=groups == 2, level_cap=2)
+    assert rounds >= 3
+
+
+@pytest.mark.gpu
+def test_host_callable_equals_the_device_field_sampler(cuda_lib, oracle_port):
+    """The same field sampled by the device kernel and by a host callable that evaluates it: the same runs."""
+    from ballasim_b200.sampling import MidpointTest, sample_window
+
+    r = W.small("blobs", 24, 18, 1).rules
+    f = _fast_blobs()
+    n = f.width * f.height
+    ids = np.arange(n, dtype=np.uint32)
+    mt = MidpointTest(r.tol, r.dark, [1.0], [1.0])
+    render = _field_render(oracle_port, f)
+    c0 = oracle_port.field_frame(f, 0).reshape(-1, 1)
+    s0 = np.zeros(n, np.uint64)
+    c_dev, s_dev, c_host, s_host = c0.copy(), s0.copy(), c0.copy(), s0.copy()
+    flagged = 0
+    for w in range(3):
+        t_w = w << 23
+        lv = np.minimum(oracle_port.levels(f, t_w, r.l_min, r.l_max), 3)
+        kw = dict(refine_signature=True, midpoint=mt, max_refine_levels=r.max_refine_levels, min_dt_ns=r.min_dt_ns)
+        dev = sample_window(t_w, ids, lv, ids, c_dev, s_dev, f, **kw)
+        host = sample_window(t_w, ids, lv, ids, c_host, s_host, render, **kw)
+        assert np.array_equal(dev.offsets, host.offsets)
+        assert np.array_equal(dev.t_ns, host.t_ns)
+        assert np.array_equal(dev.irradiance.view(np.uint32), host.irradiance.view(np.uint32))
+        assert np.array_equal(dev.last_irradiance.view(np.uint32), host.last_irradiance.view(np.uint32))
+        assert host.stats["samples_by_round"][0] + n == int(np.sum((1 << lv.astype(np.int64)) + 1))
+        c_dev, s_dev = dev.last_irradiance, dev.last_signature
+        c_host, s_host = host.last_irradiance, host.last_signature
+        flagged += host.stats["flagged_midpoint"]
+    assert flagged > 1000
