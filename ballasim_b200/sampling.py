@@ -10,6 +10,7 @@ jump, counters, carried_class) must keep their Phase 1 defaults on this path.
 from __future__ import annotations
 
 import ctypes as C
+import threading
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -18,6 +19,30 @@ from . import _lib
 from .fields import Field
 
 WINDOW_NS = 1 << 23
+
+
+class Cancelled(Exception):
+    """A window stopped by its CancelToken (the reference's _engine.Cancelled, src/engine/cancel.h:28-30)."""
+
+
+class CancelToken:
+    """A cooperative cancel (the reference's _engine.CancelToken, engine_module.cpp:1351-1357): set() from any
+    thread; sample_window checks it at each pixel batch and refinement round."""
+
+    def __init__(self):
+        self._ev = threading.Event()
+
+    def set(self) -> None:
+        """Requests the cancel (never cleared)."""
+        self._ev.set()
+
+    def is_set(self) -> bool:
+        return self._ev.is_set()
+
+
+def _check_cancel(cancel, where: str) -> None:
+    if cancel is not None and cancel.is_set():
+        raise Cancelled(where + ": cancelled")
 
 
 def waveform_range(waveform) -> tuple[float, float]:
@@ -178,8 +203,7 @@ def _host_window(t_w: int, ids: np.ndarray, lv: np.ndarray, ci: np.ndarray, cs: 
              "refine_cap_hits": 0, "band_samples_by_round": [0]}
     if n == 0:
         return np.zeros(0, np.int64), np.zeros((0, G), np.float32), np.zeros(1, np.int64), stats
-    if cancel is not None and cancel.is_set():
-        raise RuntimeError("window: batch: cancelled")
+    _check_cancel(cancel, "window: batch")
     count = (np.int64(1) << lv.astype(np.int64)) + 1
     off0 = np.zeros(n + 1, np.int64)
     np.cumsum(count, out=off0[1:])
@@ -224,8 +248,7 @@ def _host_window(t_w: int, ids: np.ndarray, lv: np.ndarray, ci: np.ndarray, cs: 
         stats["refine_cap_hits"] += words[2]
         if len(lo) == 0:
             break
-        if cancel is not None and cancel.is_set():
-            raise RuntimeError("window: refinement round: cancelled")
+        _check_cancel(cancel, "window: refinement round")
         m = len(lo)
         g = np.arange(samples, samples + m, dtype=np.int64)
         d_g = (dt[lo] + dt[hi]) >> 1
@@ -278,8 +301,8 @@ def sample_window(t_w: int, pixel_ids, levels, rank, carried_irr, carried_sig, r
         raise ValueError("min_dt_ns must be a power of two in [1, 2^23]")
     if max_refine_levels < 0:
         raise ValueError("max_refine_levels must be >= 0")
-    if cancel is not None and getattr(cancel, "is_set", lambda: False)():
-        raise RuntimeError("window: batch: cancelled")
+    if not host:
+        _check_cancel(cancel, "window: batch")
     ids = np.ascontiguousarray(pixel_ids, np.uint32).reshape(-1)
     n = len(ids)
     lv64 = np.ascontiguousarray(levels, np.int64).reshape(-1)

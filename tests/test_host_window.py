@@ -155,3 +155,31 @@ def test_host_callable_equals_the_device_field_sampler(cuda_lib, oracle_port):
         c_host, s_host = host.last_irradiance, host.last_signature
         flagged += host.stats["flagged_midpoint"]
     assert flagged > 1000
+
+
+def test_cancel_token_stops_the_window(oracle_port):
+    """A CancelToken (engine_module.cpp:1351-1357) set before the window stops it at its batch, with no render call;
+    set by the renderer during round 0 it stops the window at the first refinement round."""
+    from ballasim_b200.sampling import CancelToken, Cancelled, sample_window
+
+    f = _fast_blobs()
+    n = f.width * f.height
+    ids = np.arange(n, dtype=np.uint32)
+    lv = np.full(n, 2, np.uint8)
+    base = _field_render(oracle_port, f, 1, 9.0)
+    calls = []
+    tok = CancelToken()
+
+    def render(p, t):
+        calls.append(len(p))
+        tok.set()
+        return base(p, t)
+
+    c, s = base(ids, np.zeros(n, np.int64))
+    kw = dict(refine_signature=True, midpoint=None, max_refine_levels=4, min_dt_ns=8192)
+    with pytest.raises(Cancelled, match="refinement round: cancelled"):
+        sample_window(0, ids, lv, ids, c, s, render, cancel=tok, **kw)
+    assert calls == [4 * n]
+    with pytest.raises(Cancelled, match="batch: cancelled"):
+        sample_window(0, ids, lv, ids, c, s, render, cancel=tok, **kw)
+    assert calls == [4 * n]
