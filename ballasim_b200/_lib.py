@@ -12,7 +12,18 @@ import numpy as np
 
 LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libballasim_b200.so"
 
-BS_OK, BS_EINVAL, BS_ELOGIC, BS_ENOMEM, BS_ECUDA = 0, 1, 2, 3, 4
+BS_OK, BS_EINVAL, BS_ELOGIC, BS_ENOMEM, BS_ECUDA, BS_EREFUSED, BS_EIO = 0, 1, 2, 3, 4, 5, 6
+
+
+class FileInfo(C.Structure):
+    """bs_file_info: an event file's size, SHA-256 and its events stream."""
+    _fields_ = [("bytes", C.c_uint64), ("sha256", C.c_char * 65), ("count", C.c_int64), ("t_first", C.c_int64),
+                ("t_last", C.c_int64)]
+
+
+class ExportError(ValueError):
+    """An export refused its input or options; the message names the reason (the reference's
+    ballasim.export.errors.ExportError, raised for the writers' Refused)."""
 
 
 class MemoryBudgetError(MemoryError):
@@ -96,6 +107,16 @@ _SIGS = {
     "bs_model_reset_stats": (C.c_int32, [_P]),
     "bs_model_info": (C.c_int32, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_float), C.POINTER(C.c_int32)]),
     "bs_model_set_photometry": (C.c_int32, [_P, C.c_double, _P, C.c_size_t]),
+    "bs_raw_writer_create": (C.c_int32, [C.c_char_p, C.c_char_p, C.c_int32, C.c_int32, C.c_int64, C.c_int64,
+                                         C.c_char_p, C.c_int32, C.c_int32, C.c_char_p, C.POINTER(C.c_void_p)]),
+    "bs_dat_writer_create": (C.c_int32, [C.c_char_p, C.c_int32, C.c_int32, C.c_int64, C.c_int64, C.c_int32,
+                                         C.c_int32, C.c_char_p, C.POINTER(C.c_void_p)]),
+    "bs_event_writer_append": (C.c_int32, [_P, _P, _P, _P, _P, C.c_size_t]),
+    "bs_event_writer_append_device": (C.c_int32, [_P, _P, _P, _P, _P, C.c_size_t, _P]),
+    "bs_event_writer_close": (C.c_int32, [_P, _P]),
+    "bs_event_writer_launches": (C.c_int32, [_P, C.POINTER(C.c_uint64)]),
+    "bs_event_writer_destroy": (C.c_int32, [_P]),
+    "bs_sha256_hex": (C.c_int32, [_P, C.c_size_t, C.c_char_p]),
     "bs_model_gain_map": (C.c_int32, [_P, _P]),
     "bs_model_state_bytes": (C.c_int32, [_P, C.POINTER(C.c_size_t)]),
     "bs_model_save_state": (C.c_int32, [_P, _P, C.c_size_t]),
@@ -173,6 +194,10 @@ def check(status: int) -> None:
         raise ValueError(msg)
     if status == BS_ENOMEM:
         raise MemoryBudgetError(msg)
+    if status == BS_EREFUSED:
+        raise ExportError(msg)
+    if status == BS_EIO:
+        raise OSError(msg)
     raise RuntimeError(msg)
 
 

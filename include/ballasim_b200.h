@@ -5,7 +5,9 @@
  * library's own stream). Every call returns a bs_status; bs_last_error() holds the message of the last failure
  * on the calling thread. Status codes map to the reference's Python exceptions:
  *   BS_EINVAL -> ValueError (std::invalid_argument), BS_ELOGIC -> RuntimeError (std::logic_error),
- *   BS_ENOMEM -> MemoryError (MemoryBudgetError), BS_ECUDA -> RuntimeError (a CUDA failure or no device).
+ *   BS_ENOMEM -> MemoryError (MemoryBudgetError), BS_ECUDA -> RuntimeError (a CUDA failure or no device),
+ *   BS_EREFUSED -> ExportError, a ValueError (the exporters' Refused), BS_EIO -> OSError (a file that cannot be
+ *   created, written or read).
  * There is no CPU fallback: without a CUDA device every compute call returns BS_ECUDA.
  *
  * Citations are to the reference project's files; each entry point names the interface it replaces. */
@@ -25,6 +27,8 @@ typedef int32_t bs_status;
 #define BS_ELOGIC 2
 #define BS_ENOMEM 3
 #define BS_ECUDA 4
+#define BS_EREFUSED 5
+#define BS_EIO 6
 
 typedef struct bs_model bs_model;
 typedef struct bs_sampler bs_sampler;
@@ -309,6 +313,49 @@ bs_status bs_engine_set_record(bs_engine* e, size_t capacity);
  * host columns t, pixel (sensor << 24 | pixel), v (any may be NULL); *n = rows recorded (> capacity: cut short). */
 bs_status bs_engine_take_record(bs_engine* e, int32_t which, size_t cap, int64_t* t, uint32_t* pixel, float* v,
                                 size_t* n);
+
+/* ---- the event file sink: Prophesee RAW and DAT files of one camera's events ---- */
+
+typedef struct bs_event_writer bs_event_writer;
+
+/* What close returns (FileInfo and its one events stream, src/export/sink.h:24-36): the file's size and SHA-256
+ * (lower-case hex), the events written and the first and last T1a time u (us after the origin; 0 without events). */
+typedef struct {
+  uint64_t bytes;
+  char sha256[65];
+  int64_t count, t_first, t_last;
+} bs_file_info;
+
+/* RawWriter (src/export/raw_writer.h:33-49; ballasim._export.RawWriter, export_module.cpp:331-361): format "evt2",
+ * "evt21" or "evt3"; width and height in [1, 2048]; origin_us and epoch_ns of the T1a rule u = floor(t_ns / 1000) -
+ * origin_us (epoch_ns a multiple of 1000, recorded in the header); evt2_time_high "openeb" or "change" (EVT 2.0
+ * only); [t_ns_rem_min, t_ns_rem_max] the window's sub-us parts (-1, -1: no events); version (may be NULL) goes to
+ * the header's plugin_version. The file is created and its header written here (no device needed). */
+bs_status bs_raw_writer_create(const char* path, const char* format, int32_t width, int32_t height, int64_t origin_us,
+                               int64_t epoch_ns, const char* evt2_time_high, int32_t t_ns_rem_min,
+                               int32_t t_ns_rem_max, const char* version, bs_event_writer** out);
+/* DatWriter (raw_writer.h:51-66; export_module.cpp:363-387): as RawWriter with width and height in [1, 16384]; the
+ * version is not written. */
+bs_status bs_dat_writer_create(const char* path, int32_t width, int32_t height, int64_t origin_us, int64_t epoch_ns,
+                               int32_t t_ns_rem_min, int32_t t_ns_rem_max, const char* version,
+                               bs_event_writer** out);
+/* RawWriter::append / DatWriter::append (raw_writer.h:41-46): n events in output order from host columns x, y
+ * (uint16), p (uint8, 0/1) and t_ns (int64, t_reported). The words are built on the device. A batch that breaks a
+ * rule (order within and across calls, x < width, y < height, p <= 1, t_ns mod 1000 in the declared range, u >= 0,
+ * EVT 2.0/2.1's first u < 2^34, DAT's u < 2^32) is refused whole: BS_EREFUSED, nothing written. */
+bs_status bs_event_writer_append(bs_event_writer* w, const uint16_t* x, const uint16_t* y, const uint8_t* p,
+                                 const int64_t* t_ns, size_t n);
+/* As bs_event_writer_append with device columns (for example an output stage's), on stream (NULL: the legacy
+ * default stream); returns after the batch's words are in the file. */
+bs_status bs_event_writer_append_device(bs_event_writer* w, const uint16_t* x, const uint16_t* y, const uint8_t* p,
+                                        const int64_t* t_ns, size_t n, void* stream);
+/* RawWriter::close / DatWriter::close (raw_writer.h:47, 65): EVT 2.1's open word, then the file closed and hashed. */
+bs_status bs_event_writer_close(bs_event_writer* w, bs_file_info* info);
+/* Kernel launches of the writer's appends so far (no reference counterpart). */
+bs_status bs_event_writer_launches(const bs_event_writer* w, uint64_t* launches);
+bs_status bs_event_writer_destroy(bs_event_writer* w);
+/* SHA-256 (FIPS 180-4) of n bytes as 64 lower-case hex digits and a NUL (config::Sha256, src/config/sha256.h). */
+bs_status bs_sha256_hex(const void* data, size_t n, char out[65]);
 
 #ifdef __cplusplus
 }

@@ -31,6 +31,7 @@ REF_SOURCES = [
     "src/sensor/resim.cpp",
     "src/engine/window.cpp",
     "src/engine/par_host.cpp",
+    "src/export/raw_writer.cpp",
 ]
 REF_FLAGS = ["-std=c++20", "-O3", "-DNDEBUG", "-ffp-contract=off", "-fno-fast-math", "-march=x86-64-v3", "-fPIC"]
 PORT_FLAGS = ["-std=c11", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-Wall"]

@@ -396,6 +396,10 @@ class Ref:
             L.ref_sample_window.argtypes = [C.POINTER(OrcField), C.c_float, C.c_float, C.c_int, C.c_int, C.c_int,
                                             C.c_int64, C.c_int64, _u32p, _u8p, C.c_size_t, _f32p, _u64p, _i64p,
                                             _i64p, _f32p, C.c_size_t]
+            L.ref_event_file.restype = C.c_int
+            L.ref_event_file.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_int64, C.c_int64,
+                                         C.c_int32, C.c_int32, C.c_char_p, _u16p, _u16p, _u8p, _i64p, _i64p, C.c_int,
+                                         _i32p, C.c_char_p, C.c_size_t, _i64p, C.c_char_p]
             L.ref_sample_window_cb.restype = C.c_int64
             L.ref_sample_window_cb.argtypes = [C.c_int, C.c_float, C.c_float, _f64p, _f64p, C.c_int, C.c_int, C.c_int,
                                                C.c_int64, C.c_int64, _u32p, _u8p, C.c_size_t, _f32p, _u64p,
@@ -447,6 +451,30 @@ class Ref:
             if k >= 0:
                 return t[:k], irr[:k], off, ci, cs
             cap = -k
+
+    FILE_FORMATS = {"evt2": 0, "evt21": 1, "evt3": 2, "dat": 3}
+
+    @classmethod
+    def event_file(cls, path, format, width, height, origin_us, epoch_ns, x, y, p, t_ns, bounds=None,
+                   evt2_time_high="openeb", t_ns_rem_min=0, t_ns_rem_max=0, version=""):
+        """The reference's RawWriter / DatWriter (format "dat") fed the batches [bounds[k], bounds[k + 1]) (None: one
+        batch). Returns (info {bytes, sha256, count, t_first, t_last}, per-batch refused flags, last refusal)."""
+        n = len(t_ns)
+        b = np.asarray([0, n] if bounds is None else bounds, np.int64)
+        status = np.zeros(len(b) - 1, np.int32)
+        msg = C.create_string_buffer(1024)
+        info = np.zeros(4, np.int64)
+        sha = C.create_string_buffer(65)
+        rc = cls.lib().ref_event_file(str(path).encode(), cls.FILE_FORMATS[format],
+                                      1 if evt2_time_high == "change" else 0, width, height, origin_us, epoch_ns,
+                                      t_ns_rem_min, t_ns_rem_max, version.encode(),
+                                      np.ascontiguousarray(x, np.uint16), np.ascontiguousarray(y, np.uint16),
+                                      np.ascontiguousarray(p, np.uint8), np.ascontiguousarray(t_ns, np.int64), b,
+                                      len(b) - 1, status, msg, 1024, info, sha)
+        if rc != 0:
+            raise ValueError(cls.lib().ref_last_error().decode())
+        return ({"bytes": int(info[0]), "sha256": sha.value.decode(), "count": int(info[1]),
+                 "t_first": int(info[2]), "t_last": int(info[3])}, status.astype(bool), msg.value.decode())
 
     RENDER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_int64), C.c_size_t,
                             C.POINTER(C.c_float), C.POINTER(C.c_uint64))

@@ -16,6 +16,8 @@
 #include <vector>
 
 #include "engine/window.h"
+#include "export/errors.h"
+#include "export/raw_writer.h"
 #include "sensor/output_order.h"
 #include "sensor/params.h"
 #include "sensor/readout.h"
@@ -324,6 +326,58 @@ int64_t ref_sample_window_cb(int groups, float tol, float dark, const double* m_
   } catch (const std::exception& e) {
     fail(e);
     return INT64_MIN;
+  }
+}
+
+// The reference's event files: RawWriter (format 0 evt2, 1 evt21, 2 evt3; th_change: EVT 2.0's on-change TIME_HIGH)
+// or DatWriter (format 3), fed batches [bounds[k], bounds[k + 1]) of the columns; status[k] = 1 for a refused batch
+// (message: the last refusal). info: bytes, count, t_first, t_last; sha: 65 chars. Returns 0, or -1 when the
+// writer could not be made or closed (ref_last_error).
+int ref_event_file(const char* path, int format, int th_change, int32_t width, int32_t height, int64_t origin_us,
+                   int64_t epoch_ns, int32_t rem_min, int32_t rem_max, const char* version, const uint16_t* x,
+                   const uint16_t* y, const uint8_t* p, const int64_t* t, const int64_t* bounds, int n_batches,
+                   int32_t* status, char* message, size_t message_cap, int64_t* info, char* sha) {
+  try {
+    exporter::RawOptions o;
+    o.evt2_time_high = th_change ? exporter::Evt2TimeHigh::kOnChange : exporter::Evt2TimeHigh::kOpenEb;
+    o.t_ns_rem_min = rem_min;
+    o.t_ns_rem_max = rem_max;
+    o.version = version;
+    const exporter::TimeMap m{origin_us, epoch_ns};
+    std::unique_ptr<exporter::RawWriter> raw;
+    std::unique_ptr<exporter::DatWriter> dat;
+    if (format == 3) {
+      dat = std::make_unique<exporter::DatWriter>(path, width, height, m, o);
+    } else {
+      const exporter::RawFormat f = format == 0   ? exporter::RawFormat::kEvt2
+                                    : format == 1 ? exporter::RawFormat::kEvt21
+                                                  : exporter::RawFormat::kEvt3;
+      raw = std::make_unique<exporter::RawWriter>(path, f, width, height, m, o);
+    }
+    for (int k = 0; k < n_batches; ++k) {
+      const size_t a = static_cast<size_t>(bounds[k]), b = static_cast<size_t>(bounds[k + 1]);
+      const exporter::Events e{x + a, y + a, p + a, t + a, b - a};
+      status[k] = 0;
+      try {
+        if (dat) {
+          dat->append(e);
+        } else {
+          raw->append(e);
+        }
+      } catch (const exporter::Refused& r) {
+        status[k] = 1;
+        std::snprintf(message, message_cap, "%s", r.what());
+      }
+    }
+    const exporter::FileInfo fi = dat ? dat->close() : raw->close();
+    info[0] = static_cast<int64_t>(fi.bytes);
+    info[1] = fi.streams.at(0).count;
+    info[2] = fi.streams.at(0).t_first;
+    info[3] = fi.streams.at(0).t_last;
+    std::snprintf(sha, 65, "%s", fi.sha256.c_str());
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
   }
 }
 
