@@ -114,7 +114,8 @@ _SIGS = {
     "bs_event_writer_append": (C.c_int32, [_P, _P, _P, _P, _P, C.c_size_t]),
     "bs_event_writer_append_device": (C.c_int32, [_P, _P, _P, _P, _P, C.c_size_t, _P]),
     "bs_event_writer_close": (C.c_int32, [_P, _P]),
-    "bs_event_writer_launches": (C.c_int32, [_P, C.POINTER(C.c_uint64)]),
+    "bs_event_writer_stats": (C.c_int32, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_double),
+                                          C.POINTER(C.c_uint64), _P]),
     "bs_event_writer_destroy": (C.c_int32, [_P]),
     "bs_sha256_hex": (C.c_int32, [_P, C.c_size_t, C.c_char_p]),
     "bs_model_gain_map": (C.c_int32, [_P, _P]),

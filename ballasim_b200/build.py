@@ -1,9 +1,10 @@
 """Builds the CUDA library of the package in place: ballasim_b200/_lib/libballasim_b200.so.
 
-nvcc compiles every source in csrc/ for sm_100a only (-gencode arch=compute_100a,code=sm_100a) with the
+nvcc compiles every .cu source in csrc/ for sm_100a only (-gencode arch=compute_100a,code=sm_100a) with the
 floating-point policy the bitwise contract needs: no fused multiply-add on the device (--fmad=false) or the
 host (-ffp-contract=off), IEEE division and square root, no flush to zero. The CUDA runtime is linked
-statically, so the library needs only the driver at run time. Run ``python -m ballasim_b200.build``.
+statically, so the library needs only the driver at run time. The host-only .cpp sources (the SHA-256 of the event files, which
+uses the x86 SHA extensions) go through g++ with the same host policy. Run ``python -m ballasim_b200.build``.
 """
 from __future__ import annotations
 
@@ -31,13 +32,15 @@ def nvcc() -> str:
     return cand if Path(cand).exists() else "nvcc"
 
 
+CXX_FLAGS = ["-std=c++17", "-O3", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-I", str(INCLUDE)]
+
+
 def sources() -> list[Path]:
-    return sorted(CSRC.glob("*.cu"))
+    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
 
 
 def _deps() -> list[Path]:
-    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + \
-        sorted(INCLUDE.glob("*.h"))
+    return sources() + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + sorted(INCLUDE.glob("*.h"))
 
 
 def up_to_date() -> bool:
@@ -51,9 +54,12 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     obj_dir.mkdir(parents=True, exist_ok=True)
 
     def compile_one(src: Path) -> Path:
-        out = obj_dir / (src.stem + ".o")
-        cmd = [nvcc(), *NVCC_FLAGS, "-c", str(src), "-o", str(out)]
-        if verbose:
+        out = obj_dir / (src.stem + src.suffix.replace(".", "_") + ".o")
+        if src.suffix == ".cpp":
+            cmd = [os.environ.get("CXX", "g++"), *CXX_FLAGS, "-c", str(src), "-o", str(out)]
+        else:
+            cmd = [nvcc(), *NVCC_FLAGS, "-c", str(src), "-o", str(out)]
+        if verbose and src.suffix == ".cu":
             cmd.insert(1, "-Xptxas=-v")
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:

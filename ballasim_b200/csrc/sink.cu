@@ -18,18 +18,21 @@
 #include <unistd.h>
 
 #include <cerrno>
+#include <chrono>
 #include <climits>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <cub/device/device_scan.cuh>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <system_error>
 #include <vector>
 
 #include "../../include/ballasim_b200.h"
+#include "sha256.h"
 
 namespace bs {
 
@@ -306,120 +309,6 @@ __global__ void write_kernel(Args a, const unsigned long long* first, unsigned l
   encode(a, i, o);
 }
 
-// ---------------------------------------------------------------------------------------------------------------
-// SHA-256 (FIPS 180-4). The round constants are the first 32 bits of the fractional parts of the cube roots of the
-// first 64 primes, the initial hash those of the square roots of the first 8, computed here in integer arithmetic.
-// ---------------------------------------------------------------------------------------------------------------
-
-class Sha256 {
- public:
-  Sha256() {
-    static const Tables t;
-    k_ = t.k;
-    for (int i = 0; i < 8; ++i) h_[i] = t.h0[i];
-  }
-
-  void update(const void* data, size_t n) {
-    const auto* p = static_cast<const uint8_t*>(data);
-    bytes_ += n;
-    while (n > 0) {
-      const size_t take = n < 64 - fill_ ? n : 64 - fill_;
-      std::memcpy(buf_ + fill_, p, take);
-      fill_ += take;
-      p += take;
-      n -= take;
-      if (fill_ == 64) {
-        block(buf_);
-        fill_ = 0;
-      }
-    }
-  }
-
-  std::string hex() {
-    const uint64_t bits = bytes_ * 8;
-    const uint8_t one = 0x80;
-    update(&one, 1);
-    const uint8_t zero = 0;
-    while (fill_ != 56) update(&zero, 1);
-    uint8_t len[8];
-    for (int i = 0; i < 8; ++i) len[i] = static_cast<uint8_t>(bits >> (56 - 8 * i));
-    update(len, 8);
-    static const char* digits = "0123456789abcdef";
-    std::string out;
-    for (int i = 0; i < 8; ++i) {
-      for (int s = 28; s >= 0; s -= 4) out.push_back(digits[(h_[i] >> s) & 15]);
-    }
-    return out;
-  }
-
- private:
-  struct Tables {
-    uint32_t k[64], h0[8];
-    Tables() {
-      int primes[64], n = 0;
-      for (int c = 2; n < 64; ++c) {
-        bool prime = true;
-        for (int d = 2; d * d <= c; ++d) prime = prime && c % d != 0;
-        if (prime) primes[n++] = c;
-      }
-      // floor(root(p) 2^32) mod 2^32 from the integer root of p 2^96 (cube) or p 2^64 (square).
-      for (int i = 0; i < 64; ++i) k[i] = static_cast<uint32_t>(iroot(static_cast<unsigned __int128>(primes[i]) << 96, 3));
-      for (int i = 0; i < 8; ++i) h0[i] = static_cast<uint32_t>(iroot(static_cast<unsigned __int128>(primes[i]) << 64, 2));
-    }
-    static uint64_t iroot(unsigned __int128 v, int e) {
-      uint64_t lo = 0, hi = uint64_t{1} << 40;
-      while (hi - lo > 1) {
-        const uint64_t m = lo + (hi - lo) / 2;
-        unsigned __int128 p = m;
-        for (int j = 1; j < e; ++j) p *= m;
-        (p <= v ? lo : hi) = m;
-      }
-      return lo;
-    }
-  };
-
-  static uint32_t rotr(uint32_t x, int n) { return (x >> n) | (x << (32 - n)); }
-
-  void block(const uint8_t* b) {
-    uint32_t w[64];
-    for (int i = 0; i < 16; ++i) {
-      w[i] = (uint32_t{b[4 * i]} << 24) | (uint32_t{b[4 * i + 1]} << 16) | (uint32_t{b[4 * i + 2]} << 8) | b[4 * i + 3];
-    }
-    for (int i = 16; i < 64; ++i) {
-      const uint32_t s0 = rotr(w[i - 15], 7) ^ rotr(w[i - 15], 18) ^ (w[i - 15] >> 3);
-      const uint32_t s1 = rotr(w[i - 2], 17) ^ rotr(w[i - 2], 19) ^ (w[i - 2] >> 10);
-      w[i] = w[i - 16] + s0 + w[i - 7] + s1;
-    }
-    uint32_t a = h_[0], bb = h_[1], c = h_[2], d = h_[3], e = h_[4], f = h_[5], g = h_[6], h = h_[7];
-    for (int i = 0; i < 64; ++i) {
-      const uint32_t t1 = h + (rotr(e, 6) ^ rotr(e, 11) ^ rotr(e, 25)) + ((e & f) ^ (~e & g)) + k_[i] + w[i];
-      const uint32_t t2 = (rotr(a, 2) ^ rotr(a, 13) ^ rotr(a, 22)) + ((a & bb) ^ (a & c) ^ (bb & c));
-      h = g;
-      g = f;
-      f = e;
-      e = d + t1;
-      d = c;
-      c = bb;
-      bb = a;
-      a = t1 + t2;
-    }
-    h_[0] += a;
-    h_[1] += bb;
-    h_[2] += c;
-    h_[3] += d;
-    h_[4] += e;
-    h_[5] += f;
-    h_[6] += g;
-    h_[7] += h;
-  }
-
-  const uint32_t* k_;
-  uint32_t h_[8];
-  uint8_t buf_[64];
-  size_t fill_ = 0;
-  uint64_t bytes_ = 0;
-};
-
 [[noreturn]] void io_error(const std::string& what, const std::string& path) {
   throw std::system_error(errno, std::generic_category(), what + " " + path);
 }
@@ -427,7 +316,7 @@ class Sha256 {
 std::string sha256_file(const std::string& path, uint64_t* bytes) {
   const int fd = ::open(path.c_str(), O_RDONLY | O_CLOEXEC);
   if (fd < 0) io_error("cannot open", path);
-  Sha256 sha;
+  bs::Sha256 sha;
   std::vector<char> buf(size_t{1} << 20);
   uint64_t total = 0;
   for (;;) {
@@ -500,6 +389,55 @@ struct DBuf {
   }
 };
 
+// A writer's device and pinned buffers, its stream and timing events. A closed writer leaves its set for the next
+// one of the process (one spare, per device), so that a file per camera and run does not pay the allocations again.
+struct Scratch {
+  int device = -1;
+  DBuf<unsigned long long> scalars, counts, offsets;
+  DBuf<Info> info;
+  DBuf<uint8_t> temp, words, stage;
+  uint8_t* pin = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  ~Scratch() {
+    for (cudaEvent_t e : ev) {
+      if (e) cudaEventDestroy(e);
+    }
+    if (pin) cudaFreeHost(pin);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+std::mutex g_spare_mutex;
+Scratch* g_spare = nullptr;  // released by the process's exit
+
+Scratch* take_scratch() {
+  int dev = 0;
+  ck(cudaGetDevice(&dev), "event sink: device");
+  {
+    std::lock_guard<std::mutex> lock(g_spare_mutex);
+    if (g_spare && g_spare->device == dev) {
+      Scratch* s = g_spare;
+      g_spare = nullptr;
+      return s;
+    }
+  }
+  auto* s = new Scratch;
+  s->device = dev;
+  for (cudaEvent_t& e : s->ev) ck(cudaEventCreate(&e), "event sink: event");
+  return s;
+}
+
+void give_scratch(Scratch* s) {
+  if (!s) return;
+  std::lock_guard<std::mutex> lock(g_spare_mutex);
+  if (!g_spare) {
+    g_spare = s;
+  } else {
+    delete s;
+  }
+}
+
 class Writer {
  public:
   Writer(const char* what, const std::string& path, int32_t format, int32_t width, int32_t height, int64_t origin_us,
@@ -557,13 +495,13 @@ class Writer {
 
   ~Writer() {
     if (fd_ >= 0) ::close(fd_);
-    if (pin_) cudaFreeHost(pin_);
-    if (stream_) cudaStreamDestroy(stream_);
+    give_scratch(sc_);
   }
 
   // A batch of device columns in output order; refused whole (nothing written) when any event breaks a rule.
   void append_device(const uint16_t* x, const uint16_t* y, const uint8_t* p, const int64_t* t, size_t n,
                      cudaStream_t s) {
+    const auto t_begin = std::chrono::steady_clock::now();
     if (closed_) throw Refused(what_ + ": append after close");
     if (n == 0) return;
     if (!x || !y || !p || !t) throw std::invalid_argument(what_ + ": null event columns");
@@ -572,40 +510,60 @@ class Writer {
     Args a{format_, width_, height_, rem_min_, rem_max_, origin_, prev_, Cols{x, y, p, t, static_cast<uint32_t>(n)}};
     const int block = 256;
     const unsigned grid = static_cast<unsigned>((n + block) / block);
-    unsigned long long* bad = scalars_.ensure(1);
-    Info* info = info_.ensure(1);
+    if (!sc_) sc_ = take_scratch();
+    Scratch& sc = *sc_;
+    unsigned long long* bad = sc.scalars.ensure(1);
+    Info* info = sc.info.ensure(1);
     ck(cudaMemsetAsync(bad, 0xFF, sizeof(unsigned long long), s), "event sink: memset");
+    ck(cudaEventRecord(sc.ev[0], s), "event sink: event");
     check_kernel<<<grid, block, 0, s>>>(a, bad);
     info_kernel<<<1, 1, 0, s>>>(a, bad, info);
     ck(cudaGetLastError(), "event sink: check launch");
+    ck(cudaEventRecord(sc.ev[1], s), "event sink: event");
     Info r{};
     ck(cudaMemcpyAsync(&r, info, sizeof r, cudaMemcpyDeviceToHost, s), "event sink: copy");
     ck(cudaStreamSynchronize(s), "event sink: check");
     refuse_bad(r, n);
+    float ms = 0, part = 0;
+    ck(cudaEventElapsedTime(&part, sc.ev[0], sc.ev[1]), "event sink: timing");
+    ms += part;
     // Counts, scan, then the words chunk by chunk.
-    unsigned long long* cnt = counts_.ensure(n + 1);
-    unsigned long long* first = offsets_.ensure(n + 1);
+    unsigned long long* cnt = sc.counts.ensure(n + 1);
+    unsigned long long* first = sc.offsets.ensure(n + 1);
+    ck(cudaEventRecord(sc.ev[0], s), "event sink: event");
     count_kernel<<<grid, block, 0, s>>>(a, cnt);
     ck(cudaGetLastError(), "event sink: count launch");
     size_t temp_bytes = 0;
     ck(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, cnt, first, static_cast<int64_t>(n + 1), s), "scan");
-    uint8_t* temp = temp_.ensure(temp_bytes + 1);
+    uint8_t* temp = sc.temp.ensure(temp_bytes + 1);
     ck(cub::DeviceScan::ExclusiveSum(temp, temp_bytes, cnt, first, static_cast<int64_t>(n + 1), s), "scan");
     unsigned long long total = 0;
+    ck(cudaEventRecord(sc.ev[1], s), "event sink: event");
     ck(cudaMemcpyAsync(&total, first + n, sizeof total, cudaMemcpyDeviceToHost, s), "event sink: copy");
     ck(cudaStreamSynchronize(s), "event sink: scan");
+    ck(cudaEventElapsedTime(&part, sc.ev[0], sc.ev[1]), "event sink: timing");
+    ms += part;
     const unsigned long long chunk_words = kChunkBytes / static_cast<size_t>(word_bytes_);
-    uint8_t* dbuf = words_.ensure(kChunkBytes);
-    if (!pin_) ck(cudaMallocHost(&pin_, kChunkBytes), "event sink: pinned allocation");
+    uint8_t* dbuf = sc.words.ensure(kChunkBytes);
+    double write_ms = 0;
+    if (!sc.pin) ck(cudaMallocHost(&sc.pin, kChunkBytes), "event sink: pinned allocation");
     for (unsigned long long w0 = 0; w0 < total; w0 += chunk_words) {
       const unsigned long long w1 = total - w0 < chunk_words ? total : w0 + chunk_words;
+      ck(cudaEventRecord(sc.ev[0], s), "event sink: event");
       write_kernel<<<grid, block, 0, s>>>(a, first, w0, w1, word_bytes_, dbuf);
       ck(cudaGetLastError(), "event sink: write launch");
+      ck(cudaEventRecord(sc.ev[1], s), "event sink: event");
       const size_t bytes = static_cast<size_t>(w1 - w0) * static_cast<size_t>(word_bytes_);
-      ck(cudaMemcpyAsync(pin_, dbuf, bytes, cudaMemcpyDeviceToHost, s), "event sink: copy");
+      ck(cudaMemcpyAsync(sc.pin, dbuf, bytes, cudaMemcpyDeviceToHost, s), "event sink: copy");
       ck(cudaStreamSynchronize(s), "event sink: write");
-      write_bytes(pin_, bytes);
+      ck(cudaEventElapsedTime(&part, sc.ev[0], sc.ev[1]), "event sink: timing");
+      ms += part;
+      const auto t_w = std::chrono::steady_clock::now();
+      write_bytes(sc.pin, bytes);
+      write_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_w).count();
     }
+    kernel_ms_ = ms;
+    words_out_ = total;
     launches_ += 4 + (total + chunk_words - 1) / chunk_words;
     // The new state and the stream's counters.
     if (count_ == 0) t_first_u_ = t1a_us(r.t_first, origin_);
@@ -618,6 +576,8 @@ class Writer {
     ck(cudaMemcpyAsync(&lp, p + n - 1, sizeof lp, cudaMemcpyDeviceToHost, s), "event sink: copy");
     ck(cudaStreamSynchronize(s), "event sink: state");
     prev_ = Prev{1, lx, ly, lp, t_last_u_, r.t_last, r.tail_mask};
+    host_ms_[0] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_begin).count();
+    host_ms_[1] = write_ms;
   }
 
   // A batch of host columns: staged to the device, then as append_device.
@@ -626,17 +586,19 @@ class Writer {
     if (n == 0) return;
     if (!x || !y || !p || !t) throw std::invalid_argument(what_ + ": null event columns");
     need_device();
-    if (!stream_) ck(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "event sink: stream");
-    uint8_t* d = stage_.ensure(n * 13 + 64);
+    if (!sc_) sc_ = take_scratch();
+    Scratch& sc = *sc_;
+    if (!sc.stream) ck(cudaStreamCreateWithFlags(&sc.stream, cudaStreamNonBlocking), "event sink: stream");
+    uint8_t* d = sc.stage.ensure(n * 13 + 64);
     int64_t* dt = reinterpret_cast<int64_t*>(d);
     uint16_t* dx = reinterpret_cast<uint16_t*>(d + n * 8);
     uint16_t* dy = dx + n;
     uint8_t* dp = reinterpret_cast<uint8_t*>(dy + n);
-    ck(cudaMemcpyAsync(dt, t, n * 8, cudaMemcpyHostToDevice, stream_), "event sink: copy in");
-    ck(cudaMemcpyAsync(dx, x, n * 2, cudaMemcpyHostToDevice, stream_), "event sink: copy in");
-    ck(cudaMemcpyAsync(dy, y, n * 2, cudaMemcpyHostToDevice, stream_), "event sink: copy in");
-    ck(cudaMemcpyAsync(dp, p, n, cudaMemcpyHostToDevice, stream_), "event sink: copy in");
-    append_device(dx, dy, dp, dt, n, stream_);
+    ck(cudaMemcpyAsync(dt, t, n * 8, cudaMemcpyHostToDevice, sc.stream), "event sink: copy in");
+    ck(cudaMemcpyAsync(dx, x, n * 2, cudaMemcpyHostToDevice, sc.stream), "event sink: copy in");
+    ck(cudaMemcpyAsync(dy, y, n * 2, cudaMemcpyHostToDevice, sc.stream), "event sink: copy in");
+    ck(cudaMemcpyAsync(dp, p, n, cudaMemcpyHostToDevice, sc.stream), "event sink: copy in");
+    append_device(dx, dy, dp, dt, n, sc.stream);
   }
 
   // Writes EVT 2.1's open word, closes and hashes the file.
@@ -651,7 +613,9 @@ class Writer {
     fd_ = -1;
     if (::close(fd) != 0) io_error("cannot close", path_);
     uint64_t bytes = 0;
+    const auto t_h = std::chrono::steady_clock::now();
     const std::string sha = sha256_file(path_, &bytes);
+    host_ms_[2] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_h).count();
     if (bytes != written_) {
       throw std::runtime_error(what_ + ": " + path_ + " holds " + std::to_string(bytes) + " bytes after close, " +
                                std::to_string(written_) + " were written");
@@ -664,6 +628,10 @@ class Writer {
   }
 
   uint64_t launches() const { return launches_; }
+  double kernel_ms() const { return kernel_ms_; }
+  const double* host_ms() const { return host_ms_; }
+  uint64_t words_out() const { return words_out_; }
+  int32_t word_bytes() const { return word_bytes_; }
 
  private:
   // The reference's message for the first event that breaks a rule, then the first and last times' rules
@@ -723,11 +691,10 @@ class Writer {
   uint64_t written_ = 0, launches_ = 0;
   Prev prev_{};
   int64_t count_ = 0, t_first_u_ = 0, t_last_u_ = 0;
-  DBuf<unsigned long long> scalars_, counts_, offsets_;
-  DBuf<Info> info_;
-  DBuf<uint8_t> temp_, words_, stage_;
-  uint8_t* pin_ = nullptr;
-  cudaStream_t stream_ = nullptr;
+  Scratch* sc_ = nullptr;
+  double kernel_ms_ = 0;       // device time of the last append's kernels (check, count + scan, writes)
+  uint64_t words_out_ = 0;     // words of the last append
+  double host_ms_[3] = {0, 0, 0};  // wall time of the last append, of its file writes, and of close's hash
 };
 
 template <class F>
@@ -842,11 +809,15 @@ bs_status bs_event_writer_close(bs_event_writer* w, bs_file_info* info) {
   });
 }
 
-bs_status bs_event_writer_launches(const bs_event_writer* w, uint64_t* launches) {
+bs_status bs_event_writer_stats(const bs_event_writer* w, uint64_t* launches, double* kernel_ms,
+                                uint64_t* bytes_out, double host_ms[3]) {
   using namespace bs::sink;
   return sink_guarded([&] {
-    if (!w || !launches) throw std::invalid_argument("null argument");
-    *launches = w->w->launches();
+    if (!w) throw std::invalid_argument("null argument");
+    if (launches) *launches = w->w->launches();
+    if (kernel_ms) *kernel_ms = w->w->kernel_ms();
+    if (bytes_out) *bytes_out = w->w->words_out() * static_cast<uint64_t>(w->w->word_bytes());
+    if (host_ms) std::memcpy(host_ms, w->w->host_ms(), 3 * sizeof(double));
   });
 }
 
@@ -859,7 +830,7 @@ bs_status bs_sha256_hex(const void* data, size_t n, char out[65]) {
   using namespace bs::sink;
   return sink_guarded([&] {
     if ((!data && n > 0) || !out) throw std::invalid_argument("null argument");
-    Sha256 s;
+    bs::Sha256 s;
     s.update(data, n);
     std::snprintf(out, 65, "%s", s.hex().c_str());
   });

@@ -24,8 +24,6 @@ def _column(a, dtype, name: str) -> np.ndarray:
 
 
 class _EventWriter:
-    _what = "writer"
-
     def __init__(self, h: C.c_void_p, path: str):
         self._h = h
         self._path = path
@@ -71,11 +69,14 @@ class _EventWriter:
                 "streams": [{"camera": "", "kind": "events", "id": "", "count": int(info.count),
                              "t_first": int(info.t_first), "t_last": int(info.t_last)}]}
 
-    @property
-    def gpu_launches(self) -> int:
-        n = C.c_uint64()
-        _lib.check(_lib.lib().bs_event_writer_launches(self._h, C.byref(n)))
-        return n.value
+    def stats(self) -> dict:
+        """This build's counters: kernel launches of the appends so far; the last append's kernel device time (ms),
+        the bytes of its words, its wall time and its file writes' (ms); close's hash of the file (ms)."""
+        n, ms, b = C.c_uint64(), C.c_double(), C.c_uint64()
+        host = (C.c_double * 3)()
+        _lib.check(_lib.lib().bs_event_writer_stats(self._h, C.byref(n), C.byref(ms), C.byref(b), host))
+        return {"gpu_launches": n.value, "last_kernel_ms": ms.value, "last_words_bytes": b.value,
+                "last_append_ms": host[0], "last_file_write_ms": host[1], "close_hash_ms": host[2]}
 
 
 class RawWriter(_EventWriter):

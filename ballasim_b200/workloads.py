@@ -147,3 +147,53 @@ def blobs_noise(width: int, height: int, seed: int, seconds: float = 1.0) -> Wor
 # Seeds of the learned proposal's training fields and its held-out evaluation field.
 LEARN_TRAIN_SEEDS = (1001, 1002, 1003, 1004)
 LEARN_EVAL_SEED = 2077
+
+
+@dataclass
+class EventStream:
+    """A camera's events in output order for the event file sink: x, y (uint16), p (uint8) and t_ns (int64, the
+    sub-microsecond part 0), with their sizes."""
+    name: str
+    width: int
+    height: int
+    x: object
+    y: object
+    p: object
+    t_ns: object
+
+    def describe(self) -> dict:
+        n = len(self.t_ns)
+        span_us = int(self.t_ns[-1] - self.t_ns[0]) // 1000 if n else 0
+        return {"workload": self.name, "sensor": f"{self.width}x{self.height}", "events": n,
+                "span_us": span_us, "column_bytes": 13 * n}
+
+
+def event_stream(n: int = 32 << 20, width: int = 1280, height: int = 720, rate_hz: float = 50e6,
+                 seed: int = 5) -> EventStream:
+    """n events of a 1280 x 720 camera at about rate_hz, as edges make them: runs of 1 + Geometric(1/4) neighbouring
+    pixels of one row at one microsecond (the runs' times uniform over n / rate_hz), in the output order (t, then
+    y, then x); polarities by run."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    runs = []
+    total = 0
+    span_us = max(1, int(n / rate_hz * 1e6))
+    while total < n:
+        m = (n - total) // 4 + 16
+        length = rng.geometric(0.25, m)
+        u = rng.integers(0, span_us, m)
+        y = rng.integers(0, height, m)
+        x0 = rng.integers(0, width, m)
+        p = rng.integers(0, 2, m)
+        runs.append((length, u, y, x0, p))
+        total += int(length.sum())
+    length, u, y, x0, p = (np.concatenate(c) for c in zip(*runs))
+    rep = np.repeat(np.arange(len(length)), length)
+    off = np.arange(len(rep)) - np.repeat(np.cumsum(length) - length, length)
+    xs = np.minimum(x0[rep] + off, width - 1)
+    # One sort of the packed key (t, y, x, p) gives the output order; the first n are kept.
+    key = np.sort((u[rep] << 23) | (y[rep] << 12) | (xs << 1) | p[rep])[:n]
+    return EventStream(f"events{n >> 20}M_{width}x{height}", width, height, ((key >> 1) & 2047).astype(np.uint16),
+                       ((key >> 12) & 2047).astype(np.uint16), (key & 1).astype(np.uint8),
+                       1000 * (key >> 23))

@@ -12,6 +12,11 @@ data path; value = all ranks' pixel-samples / the slowest rank's device time.
 
 --impl reference times the reference's own CPU implementation (oracle/_ref: WindowEngine<kHost> and
 SensorModel fp32 on every host core) on a bounded sample of the same workload (its first windows), rank 0 only.
+
+The sink_* workloads measure the event file sink instead: one step writes a whole RAW (EVT 2.0, 2.1, 3.0) or DAT
+file of a seeded 1280 x 720 stream of 32 Mi events (about 50 Mev/s, runs along rows; workloads.event_stream): the
+writer made, the columns appended (device-resident for `value`, pinned host columns for `e2e`), the file closed
+and hashed. Metric events/s; the reference arm runs the reference's own RawWriter / DatWriter on one host core.
 """
 from __future__ import annotations
 
@@ -42,6 +47,8 @@ WORKLOADS = {
     "blobs_346x260_lattice": W.blobs_346x260_lattice,
 }
 METRIC = "pixel-samples/s"
+SINKS = {"sink_evt3_1280x720": "evt3", "sink_evt21_1280x720": "evt21", "sink_evt2_1280x720": "evt2",
+         "sink_dat_1280x720": "dat"}
 L2_BYTES = 126 * 1024 * 1024
 # DRAM bytes (read + write) of one engine_kernel launch, from an ncu capture of this bench's own command
 # (profiles/engine_kernel_blobs16_346x260.md), per workload; other workloads report null.
@@ -242,6 +249,122 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     return out
 
 
+def _sink_writer(fmt: str, path: str, es):
+    from ballasim_b200.export import DatWriter, RawWriter
+
+    if fmt == "dat":
+        return DatWriter(path, es.width, es.height, 0, 0, 0, 0)
+    return RawWriter(path, fmt, es.width, es.height, 0, 0, "openeb", 0, 0)
+
+
+def run_sink(args, rank: int, world: int) -> dict | None:
+    """The event file sink: whole files of the workload's event stream, device columns (value) and pinned host
+    columns (e2e), each step timed between CUDA events on the writer's stream (the step includes its host part: the
+    chunk copies, the file writes and close's SHA-256 of the file read back)."""
+    import shutil
+
+    import torch
+
+    from ballasim_b200 import _lib
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    if not _lib.cuda_available():
+        raise RuntimeError("bench: no B200 visible")
+    fmt = SINKS[args.workload]
+    es = W.event_stream(seed=5 + 1000 * rank)
+    n = len(es.t_ns)
+    cols = (es.x, es.y, es.p, es.t_ns)
+    dev = [torch.from_numpy(c.view(np.int16) if c.dtype == np.uint16 else c).cuda() for c in cols]
+    host = [torch.from_numpy(c.view(np.int16) if c.dtype == np.uint16 else c).pin_memory().numpy() for c in cols]
+    host = [h.view(c.dtype) for h, c in zip(host, cols)]
+    stream = torch.cuda.current_stream()
+    tmp = tempfile.mkdtemp(prefix="bs_sink_")
+    last = {}
+
+    def step(k: int, device: bool) -> None:
+        path = os.path.join(tmp, f"r{rank}_{k}.{fmt}")
+        w = _sink_writer(fmt, path, es)
+        if device:
+            w.append_device(*(d.data_ptr() for d in dev), n, stream.cuda_stream)
+        else:
+            w.append(*host)
+        last["info"], last["stats"] = w.close(), w.stats()
+        os.remove(path)
+
+    try:
+        for k in range(args.warmup):
+            step(k, True)
+        torch.cuda.synchronize()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        kernel_ms = []
+        with Clocks(torch.cuda.current_device()) as clk:
+            if world > 1:
+                import torch.distributed as dist
+
+                dist.barrier()
+            torch.cuda.synchronize()
+            for k in range(args.steps):
+                starts[k].record(stream)
+                step(k, True)
+                ends[k].record(stream)
+                kernel_ms.append(last["stats"]["last_kernel_ms"])
+            torch.cuda.synchronize()
+        launches = last["stats"]["gpu_launches"] * args.steps  # each writer's own count, one file per step
+        step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+        total_ms, ev_all, _ = reduce_step(float(sum(step_ms)), float(n * args.steps), 0.0, world)
+        e2e = []
+        for k in range(args.warmup + args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            step(k, False)
+            if k >= args.warmup:
+                e2e.append(time.perf_counter() - t0)
+        e2e_s = reduce_max(sum(e2e), world)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    if rank != 0:
+        return None
+    words = last["stats"]["last_words_bytes"]
+    hbm, hbm_kind = measured_hbm()
+    kms = statistics.mean(kernel_ms)
+    alg = 13 * n + words
+    achieved = alg / (kms * 1e-3) / 1e9
+    out = {
+        "metric": "events/s", "value": ev_all / (total_ms * 1e-3), "unit": "events/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64/uint16", "data": "synthetic (seeded event stream)",
+        "config": {**es.describe(), "format": fmt, "file_bytes": last["info"]["bytes"],
+                   "l2": "inputs larger than L2 (436 MiB of columns)", "parallelism": f"replicas x{world}",
+                   "step": "writer made, one append of every event, close (file written and hashed)"},
+        "gpu_launches": launches,
+        "clocks": {k: v for k, v in clk.summary().items() if k != "samples"},
+        "e2e": {"value": ev_all / e2e_s, "unit": "events/s", "h2d_bytes_per_step": 13 * n,
+                "d2h_bytes_per_step": words},
+        "roofline": {"kernel": "sink check_kernel + count_kernel + scan + write_kernel (per append)", "bound": "hbm",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": hbm_kind,
+                     "traffic": None, "algorithmic_bytes_per_launch": alg, "avg_launch_ms": kms},
+    }
+    if world == 1 and not (args.no_cpu_baseline or args.profile):
+        out["cpu_baseline"] = sink_reference(fmt, es, 8 << 20)
+    return out
+
+
+def sink_reference(fmt: str, es, n: int) -> dict:
+    """The reference's own writer (oracle/_ref) on the first n events of the stream, one host core."""
+    from oracle.oracle import Ref
+
+    n = min(n, len(es.t_ns))
+    with tempfile.TemporaryDirectory(prefix="bs_sink_ref_") as d:
+        path = Path(d) / f"ref.{fmt}"
+        t0 = time.perf_counter()
+        Ref.event_file(path, fmt, es.width, es.height, 0, 0, es.x[:n], es.y[:n], es.p[:n], es.t_ns[:n],
+                       t_ns_rem_min=0, t_ns_rem_max=0)
+        dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "events/s", "cores": 1, "kind": "reference",
+            "sample": f"first {n} of {len(es.t_ns)} events, one file ({dt:.2f} s with close's SHA-256)"}
+
+
 def learned_comparison(train_stride: int = 4, steps: int = 9000, tau: float = 0.25) -> dict:
     """The learned step proposal against the plain sampler: the network is trained on the GPU (Adam, lr 1e-3,
     batch 8192, expectile weight tau) on (history, step) pairs of the plain sampler over a training-seed
@@ -313,6 +436,20 @@ def cpu_baseline(wl: W.Workload, windows: int) -> dict:
 def run_reference(args, rank: int) -> dict | None:
     if rank != 0:
         return None
+    if args.workload in SINKS:
+        es = W.event_stream()
+        vals, cb = [], None
+        for k in range(args.warmup + args.steps):
+            cb = sink_reference(SINKS[args.workload], es, len(es.t_ns))
+            if k >= args.warmup:
+                vals.append(cb["value"])
+        value = statistics.mean(vals)
+        return {"impl": "reference", "metric": "events/s", "value": value, "unit": "events/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * len(es.t_ns) / value,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64/uint16",
+                "data": "synthetic (seeded event stream)", "config": {**es.describe(), "format": SINKS[args.workload]},
+                "cpu_baseline": {**cb, "value": value},
+                "e2e": {"value": value, "unit": "events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     wl = WORKLOADS[args.workload]()
     from ballasim_b200.params import resolve
     from oracle.oracle import Ref
@@ -346,7 +483,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="blobs_346x260")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(SINKS), default="blobs_346x260")
     ap.add_argument("--cpu-windows", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--warps", type=int, default=0)
@@ -371,7 +508,7 @@ def main():
 
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         try:
-            out = run_ours(args, rank, world)
+            out = run_sink(args, rank, world) if args.workload in SINKS else run_ours(args, rank, world)
         finally:
             if world > 1:
                 import torch.distributed as dist

@@ -351,8 +351,11 @@ bs_status bs_event_writer_append_device(bs_event_writer* w, const uint16_t* x, c
                                         const int64_t* t_ns, size_t n, void* stream);
 /* RawWriter::close / DatWriter::close (raw_writer.h:47, 65): EVT 2.1's open word, then the file closed and hashed. */
 bs_status bs_event_writer_close(bs_event_writer* w, bs_file_info* info);
-/* Kernel launches of the writer's appends so far (no reference counterpart). */
-bs_status bs_event_writer_launches(const bs_event_writer* w, uint64_t* launches);
+/* This build's counters (no reference counterpart; any may be NULL): kernel launches of the appends so far; of the
+ * last append the device time of its kernels (ms, CUDA events around them) and the bytes of its words; host_ms the
+ * wall time (ms) of the last append, of its file writes, and of close's hash of the file. */
+bs_status bs_event_writer_stats(const bs_event_writer* w, uint64_t* launches, double* kernel_ms, uint64_t* bytes_out,
+                                double host_ms[3]);
 bs_status bs_event_writer_destroy(bs_event_writer* w);
 /* SHA-256 (FIPS 180-4) of n bytes as 64 lower-case hex digits and a NUL (config::Sha256, src/config/sha256.h). */
 bs_status bs_sha256_hex(const void* data, size_t n, char out[65]);

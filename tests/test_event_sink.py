@@ -269,4 +269,6 @@ def test_device_columns_give_the_same_file(cuda_lib, tmp_path):
     w.append_device(d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), d[3].data_ptr(), len(cols[3]))
     w.close()
     assert (tmp_path / "dev").read_bytes() == a
-    assert w.gpu_launches >= 5
+    st = w.stats()
+    assert st["gpu_launches"] >= 5 and st["last_kernel_ms"] > 0
+    assert st["last_words_bytes"] == len(a) - a.index(b"% end\n") - 6 - 8  # all but the header and the open word
