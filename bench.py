@@ -314,13 +314,13 @@ def run_sink(args, rank: int, world: int) -> dict | None:
         step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
         total_ms, ev_all, _ = reduce_step(float(sum(step_ms)), float(n * args.steps), 0.0, world)
         e2e = []
-        for k in range(args.warmup + args.steps):
+        for k in range(0 if args.profile else args.warmup + args.steps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             step(k, False)
             if k >= args.warmup:
                 e2e.append(time.perf_counter() - t0)
-        e2e_s = reduce_max(sum(e2e), world)
+        e2e_s = reduce_max(sum(e2e), world) if e2e else None
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
     if rank != 0:
@@ -339,7 +339,7 @@ def run_sink(args, rank: int, world: int) -> dict | None:
                    "step": "writer made, one append of every event, close (file written and hashed)"},
         "gpu_launches": launches,
         "clocks": {k: v for k, v in clk.summary().items() if k != "samples"},
-        "e2e": {"value": ev_all / e2e_s, "unit": "events/s", "h2d_bytes_per_step": 13 * n,
+        "e2e": {"value": ev_all / e2e_s if e2e_s else None, "unit": "events/s", "h2d_bytes_per_step": 13 * n,
                 "d2h_bytes_per_step": words},
         "roofline": {"kernel": "sink check_kernel + count_kernel + scan + write_kernel (per append)", "bound": "hbm",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": hbm_kind,
