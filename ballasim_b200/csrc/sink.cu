@@ -11,8 +11,9 @@
 //   3. write: each event writes its words at its offset, in output chunks of at most kChunkBytes, each copied out
 //      once into pinned memory and appended to the file.
 // The encoder state between batches (the last event, EVT 2.1's open word mask) stays on the host, so one append
-// and many give the same bytes. close() writes EVT 2.1's open word, then hashes the closed file (SHA-256, FIPS
-// 180-4) read back, as the reference does.
+// and many give the same bytes. Each chunk is hashed (SHA-256, FIPS 180-4) on a second host thread while it is
+// written; close() writes EVT 2.1's open word and returns the digest, which is the closed file's: RAW and DAT files
+// are written once, never patched (the reference reads the closed file back for the same digest).
 #include <cuda_runtime.h>
 #include <fcntl.h>
 #include <unistd.h>
@@ -28,7 +29,10 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <sys/stat.h>
+
 #include <system_error>
+#include <thread>
 #include <vector>
 
 #include "../../include/ballasim_b200.h"
@@ -60,7 +64,7 @@ constexpr int64_t kEvt2MaxFirstU = (int64_t{1} << 34) - 1;          // EVT 2.0/2
 constexpr int64_t kDatMaxU = (int64_t{1} << 32) - 1;                // DAT's u32 microseconds
 constexpr int64_t kKeepaliveSteps = 128;                            // on-change TIME_HIGH keepalive (8.192 ms)
 constexpr int64_t kWrapSteps = int64_t{1} << 28;                    // the 28-bit TIME_HIGH value's wrap
-constexpr size_t kChunkBytes = size_t{32} << 20;                    // one output chunk (device and pinned)
+constexpr size_t kChunkBytes = size_t{64} << 20;                    // one output chunk (device and pinned)
 
 __host__ __device__ inline int64_t floor_div(int64_t a, int64_t b) {
   const int64_t q = a / b;
@@ -94,12 +98,13 @@ struct Args {
   Cols c;
 };
 
-// What the host reads back after the check: the first bad event with its predecessor's time, the first and last
-// times, and EVT 2.1's open word mask after the batch.
+// What the host reads back after the counts: the first bad event with its predecessor's time, the first and last
+// times, the last event's address and polarity, and EVT 2.1's open word mask after the batch.
 struct Info {
   unsigned long long first_bad;
   int64_t t_first, t_last, bad_t, bad_t_prev;
   uint32_t bad_x, bad_y, bad_p, tail_mask;
+  uint32_t last_x, last_y, last_p;
 };
 
 struct Ev {
@@ -198,20 +203,39 @@ __device__ void steps(Out& o, int64_t from, int64_t to, Word word) {
 
 // The on-change TIME_HIGH steps before an event in 64 us step k (evt.h:31-66): the keepalive multiples of 128 after
 // the last emitted step L and below k, then k; with the wrap guard (EVT 2.1) a step that starts a 2^28-step block
-// is preceded by the block's last step unless that was the last one emitted.
+// is preceded by the block's last step unless that was the last one emitted. The keepalives between two block
+// starts are one word each, taken as one run (steps() skips what lies before the output range), so a gap of any
+// length costs one iteration per 2^28-step block.
 template <class Out, class Word>
 __device__ void on_change(Out& o, bool started, int64_t L, int64_t k, bool wrap, Word word) {
   if (started && k <= L) return;
-  int64_t last = L;
-  const auto put = [&](int64_t step) {
-    if (wrap && started && step % kWrapSteps == 0 && step - 1 > last) o.put(word(step - 1));
-    o.put(word(step));
-    last = step;
-  };
-  if (started) {
-    for (int64_t m = (L / kKeepaliveSteps + 1) * kKeepaliveSteps; m < k && !o.done(); m += kKeepaliveSteps) put(m);
+  if (!started) {  // the stream's first TIME_HIGH
+    o.put(word(k));
+    return;
   }
-  if (!o.done()) put(k);
+  const int64_t base = (L / kKeepaliveSteps + 1) * kKeepaliveSteps;  // the first keepalive
+  const int64_t K = k > base ? (k - 1 - base) / kKeepaliveSteps + 1 : 0;  // keepalives base + 128 s, s < K
+  int64_t s = 0;
+  while (s < K && !o.done()) {
+    const int64_t m = base + kKeepaliveSteps * s;
+    if (wrap && m % kWrapSteps == 0) {  // a block's first step: its guard unless the last one emitted is m - 1
+      if (!(s == 0 && m - 1 == L)) o.put(word(m - 1));
+      o.put(word(m));
+      ++s;
+      continue;
+    }
+    int64_t end = K;  // the run of plain keepalives up to the next block start
+    if (wrap) {
+      const int64_t g = (m / kWrapSteps + 1) * kWrapSteps;
+      end = (g - base) / kKeepaliveSteps < K ? (g - base) / kKeepaliveSteps : K;
+    }
+    steps(o, s, end - 1, [&](int64_t j) { return word(base + kKeepaliveSteps * j); });
+    s = end;
+  }
+  if (o.done()) return;
+  const int64_t last = K > 0 ? base + kKeepaliveSteps * (K - 1) : L;
+  if (wrap && k % kWrapSteps == 0 && k - 1 > last) o.put(word(k - 1));
+  o.put(word(k));
 }
 
 // The words of event i (evt.h:68-171, dat.h:18-22), in stream order.
@@ -257,15 +281,13 @@ __device__ void encode(const Args& a, uint32_t i, Out& o) {
   }
 }
 
-__global__ void check_kernel(Args a, unsigned long long* first_bad) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.c.n) return;
+// The rules of one event (raw_writer.cpp:91-117): order, range, polarity and the declared sub-us part.
+__device__ inline bool bad_event(const Args& a, uint32_t i) {
   const int64_t t = a.c.t[i];
   const int64_t tp = i > 0 ? a.c.t[i - 1] : (a.prev.started ? a.prev.t : INT64_MIN);
   const int64_t rem = t - 1000 * floor_div(t, 1000);
-  const bool bad = t < tp || a.c.x[i] >= a.width || a.c.y[i] >= a.height || a.c.p[i] > 1 || rem < a.rem_min ||
-                   rem > a.rem_max;
-  if (bad) atomicMin(first_bad, static_cast<unsigned long long>(i));
+  return t < tp || a.c.x[i] >= a.width || a.c.y[i] >= a.height || a.c.p[i] > 1 || rem < a.rem_min ||
+         rem > a.rem_max;
 }
 
 // One thread: the batch's ends, the first bad event's columns and EVT 2.1's open word mask after the batch.
@@ -274,6 +296,9 @@ __global__ void info_kernel(Args a, const unsigned long long* first_bad, Info* i
   r.first_bad = *first_bad;
   r.t_first = a.c.t[0];
   r.t_last = a.c.t[a.c.n - 1];
+  r.last_x = a.c.x[a.c.n - 1];
+  r.last_y = a.c.y[a.c.n - 1];
+  r.last_p = a.c.p[a.c.n - 1];
   if (r.first_bad < a.c.n) {
     const uint32_t i = static_cast<uint32_t>(r.first_bad);
     r.bad_t = a.c.t[i];
@@ -287,22 +312,48 @@ __global__ void info_kernel(Args a, const unsigned long long* first_bad, Info* i
   *info = r;
 }
 
-__global__ void count_kernel(Args a, unsigned long long* words) {
+// Pass 1: the rules (the first bad event) and the words each event adds (counted whether or not the batch is
+// refused: the counts are O(1) per event, or one step per 2^28-step block of an on-change gap).
+__global__ void count_kernel(Args a, unsigned long long* words, unsigned long long* first_bad) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i > a.c.n) return;
   if (i == a.c.n) {  // the scan's total
     words[i] = 0;
     return;
   }
+  if (bad_event(a, i)) atomicMin(first_bad, static_cast<unsigned long long>(i));
   CountOut o;
   encode(a, i, o);
   words[i] = o.n;
 }
 
-__global__ void write_kernel(Args a, const unsigned long long* first, unsigned long long w0, unsigned long long w1,
-                             int32_t ws, uint8_t* buf) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.c.n) return;
+// The events whose words meet the output range [w0, w1): [range[0], range[1]) by two binary searches over the
+// scanned offsets (first, n + 1 entries, non-decreasing).
+__global__ void range_kernel(const unsigned long long* first, uint32_t n, unsigned long long w0,
+                             unsigned long long w1, uint32_t* range) {
+  uint32_t lo = 0, hi = n;  // the last event starting at or before w0
+  while (hi - lo > 1) {
+    const uint32_t m = lo + (hi - lo) / 2;
+    (first[m] <= w0 ? lo : hi) = m;
+  }
+  uint32_t a = lo, b = n;  // the first event starting at or after w1
+  while (a < b) {
+    const uint32_t m = a + (b - a) / 2;
+    if (first[m] < w1) {
+      a = m + 1;
+    } else {
+      b = m;
+    }
+  }
+  range[0] = lo;
+  range[1] = a;
+}
+
+// Pass 2: the words of the events in range (range_kernel) that fall in [w0, w1).
+__global__ void write_kernel(Args a, const unsigned long long* first, const uint32_t* range, unsigned long long w0,
+                             unsigned long long w1, int32_t ws, uint8_t* buf) {
+  const uint32_t i = range[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= range[1]) return;
   const unsigned long long b = first[i], e = first[i + 1];
   if (e <= w0 || b >= w1 || b == e) return;
   WriteOut o{b, w0, w1, buf, ws};
@@ -313,29 +364,6 @@ __global__ void write_kernel(Args a, const unsigned long long* first, unsigned l
   throw std::system_error(errno, std::generic_category(), what + " " + path);
 }
 
-std::string sha256_file(const std::string& path, uint64_t* bytes) {
-  const int fd = ::open(path.c_str(), O_RDONLY | O_CLOEXEC);
-  if (fd < 0) io_error("cannot open", path);
-  bs::Sha256 sha;
-  std::vector<char> buf(size_t{1} << 20);
-  uint64_t total = 0;
-  for (;;) {
-    const ssize_t r = ::read(fd, buf.data(), buf.size());
-    if (r < 0 && errno == EINTR) continue;
-    if (r < 0) {
-      const int e = errno;
-      ::close(fd);
-      errno = e;
-      io_error("cannot read", path);
-    }
-    if (r == 0) break;
-    sha.update(buf.data(), static_cast<size_t>(r));
-    total += static_cast<uint64_t>(r);
-  }
-  ::close(fd);
-  *bytes = total;
-  return sha.hex();
-}
 
 // "YYYY-MM-DD HH:MM:SS" (UTC, proleptic Gregorian) of the second that holds ns since the Unix epoch, by the
 // days-to-civil conversion of H. Hinnant's "chrono-Compatible Low-Level Date Algorithms".
@@ -512,45 +540,42 @@ class Writer {
     const unsigned grid = static_cast<unsigned>((n + block) / block);
     if (!sc_) sc_ = take_scratch();
     Scratch& sc = *sc_;
-    unsigned long long* bad = sc.scalars.ensure(1);
+    unsigned long long* bad = sc.scalars.ensure(2);
+    uint32_t* range = reinterpret_cast<uint32_t*>(bad + 1);
     Info* info = sc.info.ensure(1);
-    ck(cudaMemsetAsync(bad, 0xFF, sizeof(unsigned long long), s), "event sink: memset");
-    ck(cudaEventRecord(sc.ev[0], s), "event sink: event");
-    check_kernel<<<grid, block, 0, s>>>(a, bad);
-    info_kernel<<<1, 1, 0, s>>>(a, bad, info);
-    ck(cudaGetLastError(), "event sink: check launch");
-    ck(cudaEventRecord(sc.ev[1], s), "event sink: event");
-    Info r{};
-    ck(cudaMemcpyAsync(&r, info, sizeof r, cudaMemcpyDeviceToHost, s), "event sink: copy");
-    ck(cudaStreamSynchronize(s), "event sink: check");
-    refuse_bad(r, n);
-    float ms = 0, part = 0;
-    ck(cudaEventElapsedTime(&part, sc.ev[0], sc.ev[1]), "event sink: timing");
-    ms += part;
-    // Counts, scan, then the words chunk by chunk.
     unsigned long long* cnt = sc.counts.ensure(n + 1);
     unsigned long long* first = sc.offsets.ensure(n + 1);
+    // Pass 1 (the rules and the word counts), the batch's info, the scan; one read-back.
+    ck(cudaMemsetAsync(bad, 0xFF, sizeof(unsigned long long), s), "event sink: memset");
     ck(cudaEventRecord(sc.ev[0], s), "event sink: event");
-    count_kernel<<<grid, block, 0, s>>>(a, cnt);
+    count_kernel<<<grid, block, 0, s>>>(a, cnt, bad);
+    info_kernel<<<1, 1, 0, s>>>(a, bad, info);
     ck(cudaGetLastError(), "event sink: count launch");
     size_t temp_bytes = 0;
     ck(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, cnt, first, static_cast<int64_t>(n + 1), s), "scan");
     uint8_t* temp = sc.temp.ensure(temp_bytes + 1);
     ck(cub::DeviceScan::ExclusiveSum(temp, temp_bytes, cnt, first, static_cast<int64_t>(n + 1), s), "scan");
-    unsigned long long total = 0;
     ck(cudaEventRecord(sc.ev[1], s), "event sink: event");
+    Info r{};
+    unsigned long long total = 0;
+    ck(cudaMemcpyAsync(&r, info, sizeof r, cudaMemcpyDeviceToHost, s), "event sink: copy");
     ck(cudaMemcpyAsync(&total, first + n, sizeof total, cudaMemcpyDeviceToHost, s), "event sink: copy");
-    ck(cudaStreamSynchronize(s), "event sink: scan");
+    ck(cudaStreamSynchronize(s), "event sink: count");
+    refuse_bad(r, n);  // before any byte of the batch is written
+    float ms = 0, part = 0;
     ck(cudaEventElapsedTime(&part, sc.ev[0], sc.ev[1]), "event sink: timing");
     ms += part;
+    // Pass 2: the words, chunk by chunk, each copied out once through pinned memory and written.
     const unsigned long long chunk_words = kChunkBytes / static_cast<size_t>(word_bytes_);
     uint8_t* dbuf = sc.words.ensure(kChunkBytes);
     double write_ms = 0;
     if (!sc.pin) ck(cudaMallocHost(&sc.pin, kChunkBytes), "event sink: pinned allocation");
-    for (unsigned long long w0 = 0; w0 < total; w0 += chunk_words) {
+    uint64_t chunks = 0;
+    for (unsigned long long w0 = 0; w0 < total; w0 += chunk_words, ++chunks) {
       const unsigned long long w1 = total - w0 < chunk_words ? total : w0 + chunk_words;
       ck(cudaEventRecord(sc.ev[0], s), "event sink: event");
-      write_kernel<<<grid, block, 0, s>>>(a, first, w0, w1, word_bytes_, dbuf);
+      range_kernel<<<1, 1, 0, s>>>(first, static_cast<uint32_t>(n), w0, w1, range);
+      write_kernel<<<grid, block, 0, s>>>(a, first, range, w0, w1, word_bytes_, dbuf);
       ck(cudaGetLastError(), "event sink: write launch");
       ck(cudaEventRecord(sc.ev[1], s), "event sink: event");
       const size_t bytes = static_cast<size_t>(w1 - w0) * static_cast<size_t>(word_bytes_);
@@ -559,23 +584,17 @@ class Writer {
       ck(cudaEventElapsedTime(&part, sc.ev[0], sc.ev[1]), "event sink: timing");
       ms += part;
       const auto t_w = std::chrono::steady_clock::now();
-      write_bytes(sc.pin, bytes);
+      write_hashed(sc.pin, bytes);
       write_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_w).count();
     }
     kernel_ms_ = ms;
     words_out_ = total;
-    launches_ += 4 + (total + chunk_words - 1) / chunk_words;
+    launches_ += 4 + 2 * chunks;  // count, info, the scan's two kernels; range + write per chunk
     // The new state and the stream's counters.
     if (count_ == 0) t_first_u_ = t1a_us(r.t_first, origin_);
     t_last_u_ = t1a_us(r.t_last, origin_);
     count_ += static_cast<int64_t>(n);
-    uint16_t lx = 0, ly = 0;
-    uint8_t lp = 0;
-    ck(cudaMemcpyAsync(&lx, x + n - 1, sizeof lx, cudaMemcpyDeviceToHost, s), "event sink: copy");
-    ck(cudaMemcpyAsync(&ly, y + n - 1, sizeof ly, cudaMemcpyDeviceToHost, s), "event sink: copy");
-    ck(cudaMemcpyAsync(&lp, p + n - 1, sizeof lp, cudaMemcpyDeviceToHost, s), "event sink: copy");
-    ck(cudaStreamSynchronize(s), "event sink: state");
-    prev_ = Prev{1, lx, ly, lp, t_last_u_, r.t_last, r.tail_mask};
+    prev_ = Prev{1, r.last_x, r.last_y, r.last_p, t_last_u_, r.t_last, r.tail_mask};
     host_ms_[0] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_begin).count();
     host_ms_[1] = write_ms;
   }
@@ -609,12 +628,14 @@ class Writer {
       write_bytes(&w, sizeof w);
     }
     closed_ = true;
+    const auto t_h = std::chrono::steady_clock::now();
+    struct stat st{};
+    if (::fstat(fd_, &st) != 0) io_error("cannot stat", path_);
     const int fd = fd_;
     fd_ = -1;
     if (::close(fd) != 0) io_error("cannot close", path_);
-    uint64_t bytes = 0;
-    const auto t_h = std::chrono::steady_clock::now();
-    const std::string sha = sha256_file(path_, &bytes);
+    const uint64_t bytes = static_cast<uint64_t>(st.st_size);
+    const std::string sha = sha_.hex();
     host_ms_[2] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_h).count();
     if (bytes != written_) {
       throw std::runtime_error(what_ + ": " + path_ + " holds " + std::to_string(bytes) + " bytes after close, " +
@@ -667,7 +688,25 @@ class Writer {
     }
   }
 
+  // A chunk of words: written on this thread while another hashes the same bytes.
+  void write_hashed(const void* data, size_t n) {
+    std::thread hasher([&] { sha_.update(data, n); });
+    try {
+      write_raw(data, n);
+    } catch (...) {
+      hasher.join();
+      throw;
+    }
+    hasher.join();
+  }
+
+  // The header and the last word: written and hashed in turn.
   void write_bytes(const void* data, size_t n) {
+    write_raw(data, n);
+    sha_.update(data, n);
+  }
+
+  void write_raw(const void* data, size_t n) {
     const auto* q = static_cast<const char*>(data);
     while (n > 0) {
       const ssize_t r = ::write(fd_, q, n);
@@ -692,6 +731,7 @@ class Writer {
   Prev prev_{};
   int64_t count_ = 0, t_first_u_ = 0, t_last_u_ = 0;
   Scratch* sc_ = nullptr;
+  bs::Sha256 sha_;  // of every byte written: RAW and DAT files are never patched, so it is the closed file's hash
   double kernel_ms_ = 0;       // device time of the last append's kernels (check, count + scan, writes)
   uint64_t words_out_ = 0;     // words of the last append
   double host_ms_[3] = {0, 0, 0};  // wall time of the last append, of its file writes, and of close's hash

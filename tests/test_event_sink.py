@@ -233,6 +233,27 @@ def test_files_equal_the_reference_byte_for_byte(cuda_lib, ref, tmp_path, name, 
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name", ["evt2_change", "evt21", "evt3"])
+def test_hours_long_gaps_across_the_time_high_wrap(cuda_lib, ref, tmp_path, name):
+    """Idle gaps of hours: on-change keepalives by the million, the 2^28-step block start (u = 2^34 us) crossed
+    inside a gap (EVT 2.1's guard word before a keepalive) and right at an event; EVT 3.0's dense TIME_HIGH."""
+    rng = np.random.default_rng(29)
+    origin = 1_000
+    a = _stream(rng, 3_000, t0_us=origin + (1 << 34) - 5_000_000)
+    b = _stream(rng, 3_000, t0_us=origin + (1 << 34) + 3 * 3600 * 1_000_000)  # 3 hours later, past the block start
+    c = _stream(rng, 50, t0_us=origin + (1 << 35) - 64 * 128 * 3)  # keepalives, then an event on a block start
+    u_single = np.array([(1 << 35), (1 << 35) + (1 << 34) - 64 * 100, (1 << 35) + (1 << 34)], np.int64)
+    d = (np.array([5, 6, 7], np.uint16), np.array([7, 7, 7], np.uint16), np.array([1, 0, 1], np.uint8),
+         1000 * (origin + u_single) + 419)  # the last: a block start with no keepalive before it
+    cols = tuple(np.concatenate(z) for z in zip(a, b, c, d))
+    assert np.all(np.diff(cols[3]) >= 0)
+    bounds = [0, 3_000, 3_001, 6_000, len(cols[3])]
+    kw = dict(origin_us=origin, epoch_ns=0)
+    _same(_our_file(tmp_path / "ours", name, cols, bounds, **kw), _ref_file(ref, tmp_path / "ref", name, cols, bounds,
+                                                                          **kw))
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("name", FORMATS)
 def test_refused_batches_write_nothing_and_name_the_reference_reason(cuda_lib, ref, tmp_path, name):
     rng = np.random.default_rng(11)
