@@ -341,7 +341,7 @@ def run_sink(args, rank: int, world: int) -> dict | None:
         "clocks": {k: v for k, v in clk.summary().items() if k != "samples"},
         "e2e": {"value": ev_all / e2e_s if e2e_s else None, "unit": "events/s", "h2d_bytes_per_step": 13 * n,
                 "d2h_bytes_per_step": words},
-        "roofline": {"kernel": "sink check_kernel + count_kernel + scan + write_kernel (per append)", "bound": "hbm",
+        "roofline": {"kernel": "sink count_kernel + scan + range_kernel + write_kernel (per append)", "bound": "hbm",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": hbm_kind,
                      "traffic": None, "algorithmic_bytes_per_launch": alg, "avg_launch_ms": kms},
     }
