@@ -344,6 +344,55 @@ def sample_window(t_w: int, pixel_ids, levels, rank, carried_irr, carried_sig, r
     return WindowRuns(ids.copy(), t, irr.reshape(S, 1), off, cflat.reshape(n, 1), cs, stats)
 
 
+def fixed_rate_samples(t_w: int, period_ns: int) -> int:
+    """Samples of the fixed-rate grid in the window at t_w besides its carried one (src/engine/window.cpp:52-56):
+    the multiples of period_ns strictly inside (t_w, t_w + W), plus t_w + W itself."""
+    q = t_w // period_ns
+    inner = -((-(t_w + WINDOW_NS)) // period_ns) - q - 1
+    return max(inner, 0) + 1
+
+
+def fixed_rate_window(t_w: int, pixel_ids, rank, period_ns: int, carried_irr, carried_sig, render) -> WindowRuns:
+    """fixed_rate_window (engine_module.cpp:356-365) with a Python callable render(pixel_ids, t_ns) ->
+    (irradiance (n, groups), signature (n,)): every pixel's samples at the absolute multiples of period_ns inside
+    (t_w, t_w + W) and at t_w + W (sampling.h:344-350), after its carried one; no refinement. One render call, in
+    pixel-major slot order."""
+    if period_ns < 1:
+        raise ValueError("period_ns must be >= 1")
+    ids = np.ascontiguousarray(pixel_ids, np.uint32).reshape(-1)
+    n = len(ids)
+    rk = np.ascontiguousarray(rank, np.uint32).reshape(-1)
+    ci = np.array(carried_irr, np.float32, copy=True)
+    if ci.ndim == 1:
+        ci = ci.reshape(-1, 1)
+    cs = np.array(carried_sig, np.uint64, copy=True).reshape(-1)
+    if len(rk) != n or ci.shape[0] != n or len(cs) != n:
+        raise ValueError("pixel_ids, levels, rank, carried_irr and carried_sig need one entry per pixel")
+    G = ci.shape[1]
+    if G < 1 or G > 8:
+        raise ValueError("need 1 to 8 light groups")
+    m = fixed_rate_samples(int(t_w), int(period_ns))
+    stats = {"pixels": n, "samples_by_round": [0], "flagged_signature": 0, "flagged_midpoint": 0,
+             "refine_cap_hits": 0, "band_samples_by_round": [0]}
+    if n == 0:
+        return WindowRuns(ids.copy(), np.zeros(0, np.int64), np.zeros((0, G), np.float32), np.zeros(1, np.int64), ci,
+                          cs, stats)
+    j = np.arange(m + 1, dtype=np.int64)
+    dt = np.where(j == 0, 0, np.where(j >= m, WINDOW_NS, (int(t_w) // int(period_ns) + j) * int(period_ns) - int(t_w)))
+    t = np.tile(int(t_w) + dt, n)
+    irr = np.zeros((n * (m + 1), G), np.float32)
+    first = np.arange(n, dtype=np.int64) * (m + 1)
+    irr[first] = ci
+    req = np.nonzero(np.tile(j != 0, n))[0]
+    e, sig = _render_batch(render, np.repeat(ids, m), t[req], G)
+    irr[req] = e
+    last = first + m
+    ci[:] = irr[last]
+    cs[:] = sig.reshape(n, m)[:, -1]
+    stats["samples_by_round"] = [len(req)]
+    return WindowRuns(ids.copy(), t, irr, np.arange(n + 1, dtype=np.int64) * (m + 1), ci, cs, stats)
+
+
 def field_levels(f: Field, t_w: int, l_min: int = 1, l_max: int = 10) -> np.ndarray:
     """The field's level rule per pixel at the window start t_w (uint8, pixel order), on the device."""
     s = sampler_for(f)

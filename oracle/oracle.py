@@ -396,6 +396,9 @@ class Ref:
             L.ref_sample_window.argtypes = [C.POINTER(OrcField), C.c_float, C.c_float, C.c_int, C.c_int, C.c_int,
                                             C.c_int64, C.c_int64, _u32p, _u8p, C.c_size_t, _f32p, _u64p, _i64p,
                                             _i64p, _f32p, C.c_size_t]
+            L.ref_fixed_rate_window_cb.restype = C.c_int64
+            L.ref_fixed_rate_window_cb.argtypes = [C.c_int, C.c_int64, C.c_int64, _u32p, C.c_size_t, _f32p, _u64p,
+                                                   C.c_void_p, C.c_void_p, _i64p, _i64p, _f32p, C.c_size_t, _u64p]
             L.ref_event_file.restype = C.c_int
             L.ref_event_file.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_int64, C.c_int64,
                                          C.c_int32, C.c_int32, C.c_char_p, _u16p, _u16p, _u8p, _i64p, _i64p, C.c_int,
@@ -452,6 +455,32 @@ class Ref:
                 return t[:k], irr[:k], off, ci, cs
             cap = -k
 
+    @classmethod
+    def fixed_rate_window_cb(cls, render, groups, period_ns, t_w, pixel, carried_irr, carried_sig):
+        """WindowEngine<kHost> on the fixed-rate grid with the Python callable as its renderer. Returns (t, irr (S,
+        groups), offsets, last_irradiance, last_signature, stats)."""
+        cb = cls.RENDER_FN(cls._callback(render, groups))
+        n = len(pixel)
+        cap = max(16, n * (int((1 << 23) // max(1, period_ns)) + 3))
+        while True:
+            off = np.zeros(n + 1, np.int64)
+            t = np.zeros(cap, np.int64)
+            irr = np.zeros(cap * groups, np.float32)
+            ci = np.array(carried_irr, np.float32).reshape(n, groups).copy()
+            cs = np.array(carried_sig, np.uint64).copy()
+            st = np.zeros(37, np.uint64)
+            k = cls.lib().ref_fixed_rate_window_cb(groups, period_ns, t_w, np.ascontiguousarray(pixel, np.uint32), n,
+                                                   ci.reshape(-1), cs, C.cast(cb, C.c_void_p), None, off, t, irr, cap,
+                                                   st)
+            if k == np.iinfo(np.int64).min:
+                raise ValueError(cls.lib().ref_last_error().decode())
+            if k >= 0:
+                stats = {"flagged_signature": int(st[0]), "flagged_midpoint": int(st[1]),
+                         "refine_cap_hits": int(st[2]), "render_calls": int(st[3]),
+                         "samples_by_round": [int(v) for v in st[5:5 + int(st[4])]]}
+                return t[:k], irr[:k * groups].reshape(k, groups), off, ci, cs, stats
+            cap = -k
+
     FILE_FORMATS = {"evt2": 0, "evt21": 1, "evt3": 2, "dat": 3}
 
     @classmethod
@@ -479,12 +508,8 @@ class Ref:
     RENDER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_int64), C.c_size_t,
                             C.POINTER(C.c_float), C.POINTER(C.c_uint64))
 
-    @classmethod
-    def sample_window_cb(cls, render, groups, midpoint, refine_signature, max_refine_levels, min_dt_ns, t_w, pixel,
-                         level, carried_irr, carried_sig):
-        """WindowEngine<kHost> with the Python callable render(pixel_ids, t_ns) -> (irradiance (n, groups),
-        signature (n,)) as its renderer; midpoint: None or an object with tol, dark, m_min and m_max. Returns
-        (t, irr (S, groups), offsets, last_irradiance, last_signature, stats)."""
+    @staticmethod
+    def _callback(render, groups):
         def fn(_user, px, tt, n, irr, sig):
             if n == 0:
                 return 0
@@ -493,7 +518,15 @@ class Ref:
             np.ctypeslib.as_array(sig, (n,))[:] = np.asarray(s, np.uint64).reshape(-1)
             return 0
 
-        cb = cls.RENDER_FN(fn)
+        return fn
+
+    @classmethod
+    def sample_window_cb(cls, render, groups, midpoint, refine_signature, max_refine_levels, min_dt_ns, t_w, pixel,
+                         level, carried_irr, carried_sig):
+        """WindowEngine<kHost> with the Python callable render(pixel_ids, t_ns) -> (irradiance (n, groups),
+        signature (n,)) as its renderer; midpoint: None or an object with tol, dark, m_min and m_max. Returns
+        (t, irr (S, groups), offsets, last_irradiance, last_signature, stats)."""
+        cb = cls.RENDER_FN(cls._callback(render, groups))
         n = len(pixel)
         mn = np.asarray(midpoint.m_min if midpoint else [1.0] * groups, np.float64)
         mx = np.asarray(midpoint.m_max if midpoint else [1.0] * groups, np.float64)

@@ -381,6 +381,45 @@ int ref_event_file(const char* path, int format, int th_change, int32_t width, i
   }
 }
 
+// fixed_rate_window with a renderer callback (engine_module.cpp:356-365): the fixed-rate grid of period_ns, no
+// refinement. As ref_sample_window_cb otherwise (stats: samples_by_round at stats[5]).
+int64_t ref_fixed_rate_window_cb(int groups, int64_t period_ns, int64_t t_w, const uint32_t* pixel, size_t n,
+                                 float* carried_irr, uint64_t* carried_sig, ref_render_fn fn, void* user,
+                                 int64_t* offsets, int64_t* t_out, float* irr_out, size_t cap, uint64_t* stats) {
+  try {
+    engine::SampleConfig cfg;
+    cfg.rules.fixed = true;
+    cfg.rules.period_ns = period_ns;
+    cfg.rules.m = engine::fixed_rate_samples(t_w, period_ns);
+    cfg.groups = groups;
+    engine::WindowEngine<engine::Space::kHost> eng;
+    CallbackHook hook(fn, user, t_w, groups);
+    engine::WindowEngine<engine::Space::kHost>::Input in{};
+    in.t_w = t_w;
+    in.pixel = pixel;
+    in.level = nullptr;
+    in.n = n;
+    in.carried_irr = carried_irr;
+    in.carried_sig = carried_sig;
+    const engine::WindowStats st = eng.run(in, cfg, hook, std::numeric_limits<size_t>::max(), nullptr);
+    stats[0] = st.flagged_signature;
+    stats[1] = st.flagged_midpoint;
+    stats[2] = st.refine_cap_hits;
+    stats[3] = hook.calls_;
+    stats[4] = st.samples_by_round.size();
+    for (size_t k = 0; k < st.samples_by_round.size() && k < 32; ++k) stats[5 + k] = st.samples_by_round[k];
+    const size_t s = eng.samples();
+    std::memcpy(offsets, eng.offsets(), (n + 1) * sizeof(int64_t));
+    if (s > cap) return -static_cast<int64_t>(s);
+    std::memcpy(t_out, eng.t(), s * sizeof(int64_t));
+    std::memcpy(irr_out, eng.irr(), s * static_cast<size_t>(groups) * sizeof(float));
+    return static_cast<int64_t>(s);
+  } catch (const std::exception& e) {
+    fail(e);
+    return INT64_MIN;
+  }
+}
+
 // The whole chain of one sensor on an analytic field, the reference's own code end to end: init at t0 from the
 // field, then per window WindowEngine<kHost> (serial by design, src/engine/par.h:1-8) and SensorModel::advance_runs
 // on the model's thread pool. Levels: the field's rule per pixel and window. Returns the event count, or -1.

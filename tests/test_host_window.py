@@ -183,3 +183,23 @@ def test_cancel_token_stops_the_window(oracle_port):
     with pytest.raises(Cancelled, match="batch: cancelled"):
         sample_window(0, ids, lv, ids, c, s, render, cancel=tok, **kw)
     assert calls == [4 * n]
+
+
+@pytest.mark.parametrize("period_ns,t_w", [(1_000_000, 0), (333_333, 5 << 23), (1 << 23, 3 << 23), (7, -(1 << 23)),
+                                           (10 << 23, 2 << 23), (3_000_001, -12345)])
+def test_fixed_rate_window_equals_the_reference_engine(oracle_port, ref, period_ns, t_w):
+    """fixed_rate_window (engine_module.cpp:356-365): the grid of absolute multiples of the period inside the window,
+    then t_w + W, every pixel after its carried sample; runs, carried samples and statistics as the reference's
+    WindowEngine<kHost> gives them for the same callable."""
+    from ballasim_b200.sampling import fixed_rate_samples, fixed_rate_window
+
+    f = _fast_blobs()
+    ids = np.random.default_rng(4).permutation(f.width * f.height)[:100].astype(np.uint32)
+    render = _field_render(oracle_port, f, 2, 9.0)
+    carried, sig = render(ids, np.full(len(ids), t_w, np.int64))
+    if period_ns == 7:  # about 1.2 M samples per pixel: a few pixels only
+        ids, carried, sig = ids[:2], carried[:2], sig[:2]
+    want = ref.fixed_rate_window_cb(render, 2, period_ns, t_w, ids, carried, sig)
+    runs = fixed_rate_window(t_w, ids, np.arange(len(ids)), period_ns, carried, sig, render)
+    _same_runs(runs, want)
+    assert runs.stats["samples_by_round"] == [len(ids) * fixed_rate_samples(t_w, period_ns)]
