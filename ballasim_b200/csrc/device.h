@@ -57,6 +57,7 @@ enum ErrorBit : unsigned long long {
   kErrOrder = 8ull,
   kErrAfterEnd = 16ull,
   kErrNonFinite = 32ull,
+  kErrSearchBound = 64ull,  // a warp-cooperative crossing search or its warp loop ran past its bound
 };
 
 struct EventBuf {

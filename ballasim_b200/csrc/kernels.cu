@@ -1148,6 +1148,277 @@ __global__ void __launch_bounds__(128) engine_kernel_staged(EngineArgs a) {
 }
 
 // ---------------------------------------------------------------------------------------------
+// The fused engine with the warp-cooperative crossing search
+// ---------------------------------------------------------------------------------------------
+
+// One pixel's crossing search as every lane of the warp needs it: the piece and the comparator's state.
+struct SearchReq {
+  int64_t g_t0, g_t1, lo, hi, t_ref;
+  float g_v0, g_v1, i_scale, s3_ref, n3_ref, dr_ref, leak, theta_on, theta_off, dark, scale;
+};
+
+__device__ __forceinline__ SearchReq request_of(const PixelProc<GlobalSink>& p) {
+  return SearchReq{p.pg.t0, p.pg.t1, p.p_lo, p.p_stop, p.s.t_ref, p.pg.v0, p.pg.v1, p.s.i_scale, p.s.s3_ref,
+                   p.s.n3_ref, p.s.dr_ref, p.m.leak, p.m.theta_on, p.m.theta_off, p.m.dark, p.m.scale};
+}
+
+__device__ __forceinline__ SearchReq shfl_req(const SearchReq& r, int src) {
+  const unsigned full = 0xffffffffu;
+  SearchReq o;
+  o.g_t0 = __shfl_sync(full, r.g_t0, src);
+  o.g_t1 = __shfl_sync(full, r.g_t1, src);
+  o.lo = __shfl_sync(full, r.lo, src);
+  o.hi = __shfl_sync(full, r.hi, src);
+  o.t_ref = __shfl_sync(full, r.t_ref, src);
+  o.g_v0 = __shfl_sync(full, r.g_v0, src);
+  o.g_v1 = __shfl_sync(full, r.g_v1, src);
+  o.i_scale = __shfl_sync(full, r.i_scale, src);
+  o.s3_ref = __shfl_sync(full, r.s3_ref, src);
+  o.n3_ref = __shfl_sync(full, r.n3_ref, src);
+  o.dr_ref = __shfl_sync(full, r.dr_ref, src);
+  o.leak = __shfl_sync(full, r.leak, src);
+  o.theta_on = __shfl_sync(full, r.theta_on, src);
+  o.theta_off = __shfl_sync(full, r.theta_off, src);
+  o.dark = __shfl_sync(full, r.dark, src);
+  o.scale = __shfl_sync(full, r.scale, src);
+  return o;
+}
+
+// The first integer t in [lo, hi) where Delta fires, searched by the whole warp (all 32 lanes, uniform control
+// flow): the time-ordered search of PixelProc::search with 32-way splits. A node (a, c] with x at its ends splits
+// at a + len j / 32; lane j takes sub-interval j (the exact node test, or Delta itself at a single integer), a ballot
+// picks the earliest candidate, and the rest of the node after it (when a later sub-interval is a candidate too)
+// waits on a stack; a node of at most 32 integers is tested integer by integer, one per lane. Every evaluation is
+// PixelProc's own, and any time-ordered exhaustive search with a sound node test finds the same first integer.
+// Returns false when no integer fires; *err set if the search ran past its bound (it cannot: each round either
+// shrinks the node 32-fold or pops the stack).
+__device__ bool coop_search(const SearchReq& r, const SensorConsts& k, uint32_t lane, int64_t& t_hit, bool& on,
+                            float& x_hit, unsigned long long* err) {
+  const unsigned full = 0xffffffffu;
+  PixelRegs rs{};
+  rs.t_ref = r.t_ref;
+  rs.s3_ref = r.s3_ref;
+  rs.n3_ref = r.n3_ref;
+  rs.dr_ref = r.dr_ref;
+  rs.i_scale = r.i_scale;
+  PixelMapRegs rm{r.theta_on, r.theta_off, r.leak, r.dark, r.scale, 0.0, 0.0};
+  NullSink ns;
+  PixelCounters pc;
+  const PixelProc<NullSink> ev{rs, rm, k, 0u, ns, pc};
+  const Segment g{r.g_t0, r.g_t1, r.g_v0, r.g_v1};
+  const auto fires = [&](float D) { return D >= r.theta_on || D <= -r.theta_off; };
+  const float x_lo = ev.log_ratio(ev.current(g, r.lo));
+  const float D_lo = ev.delta(r.lo, x_lo);
+  if (fires(D_lo)) {
+    t_hit = r.lo;
+    on = D_lo >= r.theta_on;
+    x_hit = x_lo;
+    return true;
+  }
+  if (r.hi - r.lo == 1) return false;
+  constexpr int kStack = 16;  // one entry per nesting level: 2^23 integers need 5
+  int64_t sa[kStack], sc[kStack];
+  float sxa[kStack], sxc[kStack];
+  int sp = 0;
+  int64_t a = r.lo, c = r.hi - 1;
+  float xa = x_lo, xc = ev.log_ratio(ev.current(g, c));
+  for (int round = 0; round < 4096; ++round) {
+    const int64_t len = c - a;
+    if (len <= 32) {
+      const int64_t t = a + 1 + lane;
+      bool f = false, ont = false;
+      float xt = 0.0f;
+      if (t <= c) {
+        xt = t == c ? xc : ev.log_ratio(ev.current(g, t));
+        const float Dt = ev.delta(t, xt);
+        f = fires(Dt);
+        ont = Dt >= r.theta_on;
+      }
+      const unsigned b = __ballot_sync(full, f);
+      if (b != 0u) {
+        const int j = __ffs(b) - 1;
+        t_hit = a + 1 + j;
+        on = __shfl_sync(full, ont, j);
+        x_hit = __shfl_sync(full, xt, j);
+        return true;
+      }
+    } else {
+      const int64_t bl = a + (len * lane) / 32, br = a + (len * (lane + 1)) / 32;
+      const float xr = lane == 31 ? xc : ev.log_ratio(ev.current(g, br));
+      float xl = __shfl_up_sync(full, xr, 1);
+      if (lane == 0) xl = xa;
+      bool may;
+      if (br - bl == 1) {
+        may = fires(ev.delta(br, xr));
+      } else {
+        may = ev.may_fire_exact(bl, br, xl, xr);
+      }
+      const unsigned b = __ballot_sync(full, may);
+      if (b != 0u) {
+        const int j = __ffs(b) - 1;
+        const int64_t nl = a + (len * j) / 32, nr = a + (len * (j + 1)) / 32;
+        const float nxl = __shfl_sync(full, xl, j), nxr = __shfl_sync(full, xr, j);
+        if ((b >> j) > 1u) {  // a later sub-interval is a candidate too: the rest of the node waits
+          if (sp == kStack) {
+            *err |= kErrSearchBound;
+            return false;
+          }
+          sa[sp] = nr;
+          sc[sp] = c;
+          sxa[sp] = nxr;
+          sxc[sp] = xc;
+          ++sp;
+        }
+        a = nl;
+        c = nr;
+        xa = nxl;
+        xc = nxr;
+        continue;
+      }
+    }
+    if (sp == 0) return false;
+    --sp;
+    a = sa[sp];
+    c = sc[sp];
+    xa = sxa[sp];
+    xc = sxc[sp];
+  }
+  *err |= kErrSearchBound;
+  return false;
+}
+
+// The staged engine (engine_kernel_staged<32>) with the crossing search taken by the whole warp. Phase B is one
+// warp-uniform loop: every lane feeds its staged samples with the search deferred, up to its first search or the
+// window's end; the warp then runs the posted searches one by one, 32 lanes each; the lanes apply the outcomes
+// (the event, or the search cleared to its stop) and resume their pieces. Where many lanes search at once (dense
+// events with noise and leak: C3, C4) the searches queue behind one another and the autotuner keeps another stage. Lanes whose window overflowed the stage
+// run it alone afterwards, searching as the other engines do.
+__global__ void __launch_bounds__(128) engine_kernel_coop(EngineArgs a) {
+  constexpr int kStage = 32;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const unsigned full = 0xffffffffu;
+  const int64_t t0 = *a.t0;
+  __shared__ uint16_t lists[4][kMaxListed];
+  __shared__ uint32_t st_dt[4][kStage][32];
+  __shared__ float st_v[4][kStage][32];
+  uint16_t* my_list = lists[warp];
+  for (;;) {
+    uint32_t tile = 0;
+    if (lane == 0) tile = atomicAdd(a.tile_counter, 1u);
+    tile = __shfl_sync(full, tile, 0);
+    if (tile >= a.total_tiles) break;
+    int si = 0;
+    while (si + 1 < a.n_sensors && a.sensors[si + 1].tile0 <= tile) ++si;
+    const EngineSensor& S = a.sensors[si];
+    const uint32_t local = tile - S.tile0;
+    uint32_t x, y;
+    tile_xy(local, S.tiles_x, a.tile_lw, lane, x, y);
+    const bool have = x < S.width && y < S.height;
+    const uint32_t p = have ? y * S.width + x : 0u;
+    const bool noise = S.consts.noise != 0;
+    PixelRegs s;
+    PixelMapRegs m;
+    float carried = 0.0f;
+    if (have) {
+      load_state(S.in, p, noise, s);
+      load_map(S.map, p, m);
+      carried = S.carried_in[p];
+    }
+    PixelCounters c;
+    unsigned long long samples = 0, err = 0;
+    GlobalSink sink{S.ev, &S.counters[kCntEvents]};
+    PixelProc<GlobalSink> proc{s, m, S.consts, p, sink, c};
+    const FieldDev& f = S.field;
+    for (int32_t w = a.w0; w < a.w1; ++w) {
+      const int64_t t_w = t0 + static_cast<int64_t>(w) * kWindowNs;
+      const BlobList list = warp_blob_list(f, have, x, y, t_w, t_w + kWindowNs, my_list);
+      auto render = [&](uint32_t dt) { return field_eval(f, list, x, y, t_w + dt); };
+      // Phase A: the walk, its first kStage samples after slot 0 staged.
+      uint32_t n = 0;
+      int level = 0;
+      if (have) {
+        level = field_level(f, list, x, y, t_w, a.r.l_min, a.r.l_max);
+        uint32_t kk = 0;
+        n = sample_pixel_window(a.r, level, carried, false, render, [&](uint32_t dt, float v) {
+          if (kk < static_cast<uint32_t>(kStage)) {
+            st_dt[warp][kk][lane] = dt;
+            st_v[warp][kk][lane] = v;
+          }
+          ++kk;
+        });
+      }
+      __syncwarp();
+      // Phase B, the warp together.
+      WindowFeed feed{&proc, t_w, S.consts.irr_max, t_w, s.held, carried, 0.0f};
+      const bool staged = have && n - 1 <= static_cast<uint32_t>(kStage);
+      if (staged) feed.start(carried);
+      proc.defer = true;
+      uint32_t next = 0;
+      for (int iter = 0;; ++iter) {
+        if (staged && !proc.pending) {
+          while (next + 1 < n) {
+            feed(st_dt[warp][next][lane], st_v[warp][next][lane]);
+            ++next;
+            if (proc.pending) break;
+          }
+        }
+        unsigned mask = __ballot_sync(full, staged && proc.pending);
+        if (mask == 0u) break;
+        if (iter >= (1 << 16)) {  // a bound on the window's searches per lane: every outcome moves its search on
+          err |= kErrSearchBound;
+          break;
+        }
+        bool found = false, on = false;
+        int64_t th = 0;
+        float xh = 0.0f;
+        const SearchReq mine = request_of(proc);
+        while (mask != 0u) {
+          const int src = __ffs(mask) - 1;
+          mask &= mask - 1u;
+          const SearchReq r = shfl_req(mine, src);
+          int64_t t_hit = 0;
+          bool o = false;
+          float xv = 0.0f;
+          const bool fnd = coop_search(r, S.consts, lane, t_hit, o, xv, &err);
+          if (static_cast<int>(lane) == src) {
+            found = fnd;
+            th = t_hit;
+            on = o;
+            xh = xv;
+          }
+        }
+        if (staged && proc.pending) proc.resume_search(found, th, on, xh);
+      }
+      proc.defer = false;
+      if (have) {
+        if (staged) {
+          samples += n;
+          s.held = feed.prev_v;
+          carried = feed.last_raw;
+        } else {  // the window overflowed the stage: this lane alone, the walk again with the model fed inline
+          WindowFeed alone{&proc, t_w, S.consts.irr_max, t_w, s.held, carried, 0.0f};
+          alone.start(carried);
+          sample_pixel_window(a.r, level, carried, false, render, alone);
+          samples += n;
+          s.held = alone.prev_v;
+          carried = alone.last_raw;
+        }
+      }
+      __syncwarp();
+    }
+    if (have) {
+      store_state(S.out, p, noise, s);
+      S.carried_out[p] = carried;
+    }
+    warp_add(&S.counters[kCntPieces], c.pieces);
+    warp_add(&S.counters[kCntLeaves], c.leaves);
+    warp_add(&S.counters[kCntSamples], samples);
+    warp_add(&S.counters[kCntNoise], c.noise_candidates);
+    warp_or(&S.counters[kCntErrors], err);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
 // The fused engine with the learned step proposal
 // ---------------------------------------------------------------------------------------------
 __device__ __forceinline__ void load_learned(const LearnedSoA& a, uint32_t p, uint32_t n, LearnedPixel& L) {
@@ -1408,6 +1679,7 @@ void launch_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t tota
   if (cascade == 2 && stage != 0) engine_lattice_kernel_staged<<<blocks, warps_per_block * 32, 0, stream>>>(a);
   else if (cascade == 2) engine_lattice_kernel<<<blocks, warps_per_block * 32, 0, stream>>>(a);
   else if (cascade == 1) engine_cascade_kernel<<<blocks, warps_per_block * 32, 0, stream>>>(a);
+  else if (stage == 64) engine_kernel_coop<<<blocks, warps_per_block * 32, 0, stream>>>(a);
   else if (stage == 16) engine_kernel_staged<16><<<blocks, warps_per_block * 32, 0, stream>>>(a);
   else if (stage == 32) engine_kernel_staged<32><<<blocks, warps_per_block * 32, 0, stream>>>(a);
   else engine_kernel<<<blocks, warps_per_block * 32, 0, stream>>>(a);
@@ -1421,6 +1693,8 @@ int engine_max_blocks_per_sm(int warps_per_block, int stage, int cascade) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_lattice_kernel, warps_per_block * 32, 0);
   } else if (cascade == 1) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_cascade_kernel, warps_per_block * 32, 0);
+  } else if (stage == 64) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel_coop, warps_per_block * 32, 0);
   } else if (stage == 16) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel_staged<16>, warps_per_block * 32, 0);
   } else if (stage == 32) {

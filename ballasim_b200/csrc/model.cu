@@ -587,6 +587,7 @@ struct Model {
     }
     if (e & kErrAfterEnd) return "SensorModel.advance: sample after t_end_ns";
     if (e & kErrNonFinite) return "SensorModel.advance: non-finite irradiance";
+    if (e & kErrSearchBound) return "engine: a crossing search ran past its bound";
     return "SensorModel.advance: refused input";
   }
 
@@ -1599,7 +1600,12 @@ struct Engine {
   void set_launch(int32_t warps, int32_t per_sm, int32_t stg, int32_t lw) {
     if (warps < 0 || warps > 4) throw std::invalid_argument("engine: warps per block must lie in [1, 4]");
     if (per_sm < 0 || per_sm > 32) throw std::invalid_argument("engine: blocks_per_sm in [0, 32]");
-    if (stg != 0 && stg != 16 && stg != 32) throw std::invalid_argument("engine: stage 0, 16 or 32");
+    if (stg != 0 && stg != 16 && stg != 32 && stg != 64) {
+      throw std::invalid_argument("engine: stage 0, 16, 32 or 64 (32 deep with the warp-cooperative search)");
+    }
+    if (stg == 64 && (cascade() != 0 || mlp)) {
+      throw std::invalid_argument("engine: the warp-cooperative search (stage 64) is the instantaneous response's");
+    }
     if (stg != 0 && cascade() == 1) throw std::invalid_argument("engine: the cascade runs unstaged (stage 0)");
     if (stg != 0 && stg != 32 && cascade() == 2) {
       throw std::invalid_argument("engine: the noise lattice runs unstaged (stage 0) or staged 32 deep (stage 32)");
@@ -1614,7 +1620,8 @@ struct Engine {
 
   // Times each candidate launch shape on trial steps of `windows` windows from the current state (the models keep
   // their state) and keeps the fastest. Candidates: tile width 4, 8, 16 px (height 8, 4, 2) x warps per block 2, 4 x
-  // staging depth 0, 16 (the learned engine: tile widths only; the cascade: stage 0). Returns the candidates tried (ms of the second of
+  // staging depth 0, 16, 64 (32 deep with the warp-cooperative search; the learned engine: tile widths only; the
+  // cascade: stage 0; the lattice: 0 or 32). Returns the candidates tried (ms of the second of
   // two trial steps each); rows are {tile_lw, warps, stage, ms}.
   std::vector<std::array<double, 4>> autotune(int32_t windows, cudaStream_t s) {
     if (windows < 1) throw std::invalid_argument("engine.autotune: windows >= 1");
@@ -1624,8 +1631,9 @@ struct Engine {
     int bl = keep[0], bw = keep[1], bs = keep[2];
     for (int lw : {2, 3, 4}) {
       for (int w : {2, 4}) {
-        for (int st : {0, 16}) {
+        for (int st : {0, 16, 64}) {
           if ((mlp && (w != 4 || st != 0)) || (cascade() == 1 && st != 0)) continue;
+          if (cascade() == 2 && st == 64) continue;
           if (cascade() == 2 && st != 0) st = 32;
           set_launch(w, 0, st, lw);
           step(windows, s, false, nullptr, nullptr);

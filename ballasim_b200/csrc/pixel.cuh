@@ -109,6 +109,13 @@ struct PixelProc {
   uint32_t pixel;  // the frame's pixel id (events, noise keys)
   Sink& sink;
   PixelCounters& c;
+  // The deferred search (the warp-cooperative engine): with defer set, piece() records the search it needs
+  // (pending; the piece g, [p_t, p_e) and the search's [p_lo, p_stop)) and returns; resume_search applies the
+  // outcome as piece() would have and resumes the piece.
+  bool defer = false;
+  bool pending = false;
+  Segment pg{};
+  int64_t p_t = 0, p_e = 0, p_lo = 0, p_stop = 0;
 
   BS_HD float value(const Segment& g, int64_t t) const {
     if (g.t1 == kForever) return g.v0;
@@ -293,6 +300,15 @@ struct PixelProc {
       const int64_t lo = maxi(s.t_search, t);
       const int64_t stop = mini(e, tn);
       if (lo < stop) {
+        if (defer) {
+          pending = true;
+          pg = g;
+          p_t = t;
+          p_e = e;
+          p_lo = lo;
+          p_stop = stop;
+          return;
+        }
         int64_t th;
         bool on;
         float x;
@@ -415,6 +431,19 @@ struct PixelProc {
     const float corr = 1.1f * (8.0f * eps + 64.0f * eps * (I0 / I1));
     const float lo = ((((xa - corr) - slack) - s.s3_ref) + (0.0f - s.n3_ref)) + dl0;
     return lo > -m.theta_off + slack;
+  }
+
+  // The outcome of the deferred search (found: the first firing integer th, its polarity and x), applied as piece()
+  // applies its search's, then the piece resumed from its start (its loop holds no state but the pixel's).
+  BS_HD void resume_search(bool found, int64_t th, bool on, float x) {
+    pending = false;
+    if (found) {
+      fire(th, on, x, -1);
+    } else {
+      s.t_search = maxi(s.t_search, p_stop);
+    }
+    --c.pieces;  // piece() counts the piece again
+    piece(pg, p_t, p_e);
   }
 
   // The rest of piece(g, t, e) after an event inside it (the reference's loop with the new state).

@@ -266,12 +266,13 @@ def test_midpoint_test_matches_numpy_fp32(cuda_lib):
 
 
 @pytest.mark.parametrize("stage,tile,graph", [(0, 8, True), (16, 8, True), (32, 8, True), (0, 4, True),
-                                              (16, 16, True), (0, 32, True), (0, 8, False)])
+                                              (16, 16, True), (0, 32, True), (0, 8, False), (64, 8, True),
+                                              (64, 4, True), (64, 16, False)])
 @pytest.mark.parametrize("case", ["edge", "blobs", "noise"])
 def test_engine_equals_the_oracle_chain(cuda_lib, case, stage, tile, graph):
     """The fused engine (sampler and pixel model on one thread, all windows in one launch; streamed, or staged in
-    shared memory per window; any tile shape; from a CUDA graph or not) gives the oracle chain's events
-    (sample_window, then advance, per window) bit for bit."""
+    shared memory per window, stage 64 with the warp-cooperative crossing search; any tile shape; from a CUDA graph
+    or not) gives the oracle chain's events (sample_window, then advance, per window) bit for bit."""
     from ballasim_b200.engine import Engine
     from ballasim_b200.sensor import SensorModel
     from oracle.oracle import simulate_port
@@ -321,7 +322,7 @@ def test_autotune_keeps_the_state_and_the_events(cuda_lib):
         eng.start(0)
         if tune:
             rows = eng.autotune(4)
-            assert len(rows) == 12 and all(x["ms"] > 0 for x in rows)
+            assert len(rows) == 18 and all(x["ms"] > 0 for x in rows)  # 3 tile widths x 2 warps x stage 0, 16, 64
             best = min(rows, key=lambda x: x["ms"])
             assert eng.launch["tile_width"] == best["tile_width"] and eng.launch["stage"] == best["stage"]
         s, e = eng.run(wl.windows)
