@@ -50,9 +50,9 @@ METRIC = "pixel-samples/s"
 SINKS = {"sink_evt3_1280x720": "evt3", "sink_evt21_1280x720": "evt21", "sink_evt2_1280x720": "evt2",
          "sink_dat_1280x720": "dat"}
 L2_BYTES = 126 * 1024 * 1024
-# DRAM bytes (read + write) of one engine_kernel launch, from an ncu capture of this bench's own command
-# (profiles/engine_kernel_blobs16_346x260.md), per workload; other workloads report null.
-NCU_TRAFFIC_PER_LAUNCH = {"blobs16_346x260": 29.39e6 + 49.19e6}
+# DRAM bytes (read + write) of one launch of the engine kernel the autotuner picks, from an ncu capture of this
+# bench's own command (profiles/engine_kernel_coop_blobs16_346x260.md), per workload; other workloads report null.
+NCU_TRAFFIC_PER_LAUNCH = {"blobs16_346x260": 8.74e6 + 4.56e6}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -236,7 +236,8 @@ def run_ours(args, rank: int, world: int) -> dict | None:
         "e2e": {"value": samples_all / e2e_s if e2e_times else None, "unit": "pixel-samples/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "roofline": {"kernel": (("engine_lattice_kernel" if lattice else "engine_cascade_kernel") if cascade
-                                else "engine_kernel") +
+                                else {64: "engine_kernel_coop", 16: "engine_kernel_staged<16>",
+                                      32: "engine_kernel_staged<32>"}.get(eng.launch["stage"], "engine_kernel")) +
                                " (sampler + pixel model fused, runs kept on chip)", "bound": "hbm",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": hbm_kind, "traffic": NCU_TRAFFIC_PER_LAUNCH.get(wl.name), "algorithmic_bytes_per_launch": alg,
