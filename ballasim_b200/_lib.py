@@ -132,6 +132,10 @@ _SIGS = {
                                             C.POINTER(SampleRules), _P, _P, _P, C.c_size_t, _P, _P, _P,
                                             C.POINTER(C.c_size_t)]),
     "bs_sampler_device_runs": (C.c_int32, [_P, C.POINTER(DeviceRuns)]),
+    "bs_sample_window_device": (C.c_int32, [_P, C.c_int64, _P, _P, C.c_size_t, _P, _P, _P, _P,
+                                            C.POINTER(SampleRules), _P, C.POINTER(C.c_size_t)]),
+    "bs_field_levels_device": (C.c_int32, [_P, C.c_int64, C.c_int32, C.c_int32, _P, _P]),
+    "bs_field_frame_device": (C.c_int32, [_P, C.c_int64, _P, _P]),
     "bs_field_levels": (C.c_int32, [_P, C.c_int64, C.c_int32, C.c_int32, _P]),
     "bs_field_frame": (C.c_int32, [_P, C.c_int64, _P]),
     "bs_midpoint_eta": (C.c_int32, [C.c_float, C.c_float, C.c_int32, _P, _P, _P, _P, _P, C.c_size_t, _P, _P]),

@@ -129,6 +129,9 @@ void launch_scan(const uint32_t* counts, uint32_t n, int64_t* offsets, int64_t* 
 void launch_levels(const FieldDev& f, int64_t t_w, int32_t l_min, int32_t l_max, uint32_t n_pixels, uint8_t* level,
                    cudaStream_t stream);
 void launch_field_frame(const FieldDev& f, int64_t t, uint32_t n_pixels, float* out, cudaStream_t stream);
+// ORs into *err: bit 0 where a level exceeds max_level, bit 1 where a pixel id is outside the field.
+void launch_check_window(const uint32_t* pixel, const uint8_t* level, uint32_t n, uint32_t n_field, int max_level,
+                         unsigned long long* err, cudaStream_t stream);
 // The fused engine: windows [w0, w1) of every sensor, one warp per 8 x 4 pixel tile, tiles taken from a global
 // counter (work stealing) by a persistent grid. stage 0: the sampler feeds the pixel model sample by sample;
 // 16 or 32: per window the samples are staged in shared memory (that many per lane) between the two phases.

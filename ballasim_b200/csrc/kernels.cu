@@ -1190,10 +1190,16 @@ __device__ __forceinline__ SearchReq shfl_req(const SearchReq& r, int src) {
 // picks the earliest candidate, and the rest of the node after it (when a later sub-interval is a candidate too)
 // waits on a stack; a node of at most 32 integers is tested integer by integer, one per lane. Every evaluation is
 // PixelProc's own, and any time-ordered exhaustive search with a sound node test finds the same first integer.
-// Returns false when no integer fires; *err set if the search ran past its bound (it cannot: each round either
-// shrinks the node 32-fold or pops the stack).
+// Returns false when no integer fires. *leaves counts the nodes tested with the node test (32 per split round, one
+// per sub-interval longer than one integer): they are this search's nodes, not the serial search's.
+//
+// The round bound is derived from the piece: every round that removes no integer from the unexplored set (the node
+// and the stack) descends one 32-fold level, at most 5 levels below the node it started from, so a search of
+// hi - lo integers ends within 6 (hi - lo) + 6 rounds. (Where Delta stays just under a level over a long piece, most
+// sub-intervals stay candidates and the search really visits about (hi - lo) / 32 leaves, like the serial one.) The
+// stack holds one entry per level. *err is set only if either bound is passed, which the argument above excludes.
 __device__ bool coop_search(const SearchReq& r, const SensorConsts& k, uint32_t lane, int64_t& t_hit, bool& on,
-                            float& x_hit, unsigned long long* err) {
+                            float& x_hit, uint32_t* leaves, unsigned long long* err) {
   const unsigned full = 0xffffffffu;
   PixelRegs rs{};
   rs.t_ref = r.t_ref;
@@ -1222,7 +1228,8 @@ __device__ bool coop_search(const SearchReq& r, const SensorConsts& k, uint32_t 
   int sp = 0;
   int64_t a = r.lo, c = r.hi - 1;
   float xa = x_lo, xc = ev.log_ratio(ev.current(g, c));
-  for (int round = 0; round < 4096; ++round) {
+  const int64_t max_rounds = 6 * (r.hi - r.lo) + 64;
+  for (int64_t round = 0; round < max_rounds; ++round) {
     const int64_t len = c - a;
     if (len <= 32) {
       const int64_t t = a + 1 + lane;
@@ -1253,6 +1260,7 @@ __device__ bool coop_search(const SearchReq& r, const SensorConsts& k, uint32_t 
       } else {
         may = ev.may_fire_exact(bl, br, xl, xr);
       }
+      *leaves += __popc(__ballot_sync(full, br - bl > 1));
       const unsigned b = __ballot_sync(full, may);
       if (b != 0u) {
         const int j = __ffs(b) - 1;
@@ -1354,7 +1362,7 @@ __global__ void __launch_bounds__(128) engine_kernel_coop(EngineArgs a) {
       if (staged) feed.start(carried);
       proc.defer = true;
       uint32_t next = 0;
-      for (int iter = 0;; ++iter) {
+      for (int64_t iter = 0;; ++iter) {
         if (staged && !proc.pending) {
           while (next + 1 < n) {
             feed(st_dt[warp][next][lane], st_v[warp][next][lane]);
@@ -1364,7 +1372,9 @@ __global__ void __launch_bounds__(128) engine_kernel_coop(EngineArgs a) {
         }
         unsigned mask = __ballot_sync(full, staged && proc.pending);
         if (mask == 0u) break;
-        if (iter >= (1 << 16)) {  // a bound on the window's searches per lane: every outcome moves its search on
+        // Every outcome moves the lane's search at least 1 ns on (an event re-arms it after the event's ns), so a
+        // lane posts at most one search per ns of the window and per piece: 2^25 rounds cannot be reached.
+        if (iter >= (int64_t{1} << 25)) {
           err |= kErrSearchBound;
           break;
         }
@@ -1379,8 +1389,10 @@ __global__ void __launch_bounds__(128) engine_kernel_coop(EngineArgs a) {
           int64_t t_hit = 0;
           bool o = false;
           float xv = 0.0f;
-          const bool fnd = coop_search(r, S.consts, lane, t_hit, o, xv, &err);
+          uint32_t lv = 0;
+          const bool fnd = coop_search(r, S.consts, lane, t_hit, o, xv, &lv, &err);
           if (static_cast<int>(lane) == src) {
+            c.leaves += lv;
             found = fnd;
             th = t_hit;
             on = o;
@@ -1670,6 +1682,25 @@ void launch_levels(const FieldDev& f, int64_t t_w, int32_t l_min, int32_t l_max,
 
 void launch_field_frame(const FieldDev& f, int64_t t, uint32_t n_pixels, float* out, cudaStream_t stream) {
   field_frame_kernel<<<(n_pixels + 255) / 256, 256, 0, stream>>>(f, t, n_pixels, out);
+}
+
+namespace {
+// The window inputs' checks on the device (bit 0: a level above max_level, bit 1: an id outside the field).
+__global__ void check_window_kernel(const uint32_t* pixel, const uint8_t* level, uint32_t n, uint32_t n_field,
+                                    int max_level, unsigned long long* err) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long bits = 0;
+  if (i < n) {
+    if (level[i] > max_level) bits |= 1ull;
+    if (pixel[i] >= n_field) bits |= 2ull;
+  }
+  warp_or(err, bits);
+}
+}  // namespace
+
+void launch_check_window(const uint32_t* pixel, const uint8_t* level, uint32_t n, uint32_t n_field, int max_level,
+                         unsigned long long* err, cudaStream_t stream) {
+  if (n > 0) check_window_kernel<<<(n + 255) / 256, 256, 0, stream>>>(pixel, level, n, n_field, max_level, err);
 }
 
 void launch_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t total_tiles, const int64_t* t0,

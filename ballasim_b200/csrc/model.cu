@@ -963,6 +963,7 @@ struct Sampler {
     }
     if (np > 0xFFFFFFFFull) throw std::invalid_argument("too many pixels");
     n = np;
+    dev_ids = nullptr;
     pixel.ensure(np);
     level.ensure(np);
     carried_in.ensure(np);
@@ -998,6 +999,50 @@ struct Sampler {
     }
     CK(cudaStreamSynchronize(s));
   }
+
+  // The same window with every input and the carried samples in device memory (WindowEngine<Space::kDevice>::run,
+  // src/engine/window.h:133-174): the ids and levels are read in place and checked on the device, the carried
+  // samples are read from c_in / s_in and the window's last samples written to c_out / s_out (the caller's device
+  // arrays; they may not alias). The runs stay in this sampler's memory (bs_sampler_device_runs). Two
+  // synchronizations of `s` read the check and the sample count; the write pass is left queued on `s`.
+  void window_device(int64_t t_w, const uint32_t* ids, const uint8_t* lv, size_t np, const float* c_in,
+                     const uint64_t* s_in, float* c_out, uint64_t* s_out, const bs_sample_rules& rr, cudaStream_t s) {
+    const SamplerRules r = make_rules(rr);
+    int shift = 0;
+    while ((int64_t{1} << shift) < rr.min_dt_ns) ++shift;
+    if (np > 0xFFFFFFFFull) throw std::invalid_argument("too many pixels");
+    const uint32_t nn = static_cast<uint32_t>(np);
+    counts.ensure(np);
+    offsets.ensure(np + 1);
+    scratch.ensure(scan_scratch_words(nn));
+    err.ensure(1);
+    info.ensure(2);
+    // The inputs are checked before the walk runs on them (a lattice level sets the walk's length).
+    CK(cudaMemsetAsync(err.p, 0, sizeof(unsigned long long), s));
+    launch_check_window(ids, lv, nn, field.f.width * field.f.height, kWindowLog2 - shift, err.p, s);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(info.p, err.p, 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (info.p[0] & 1ull) throw std::invalid_argument("levels must lie in [0, 23 - log2(min_dt_ns)]");
+    if (info.p[0] & 2ull) throw std::invalid_argument("pixel id outside the field");
+    launch_sample_window(field.f, r, t_w, ids, lv, nn, c_in, s_in, counts.p, nullptr, nullptr, nullptr, nullptr,
+                         nullptr, 0, s);
+    launch_scan(counts.p, nn, offsets.p, scratch.p, s);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(info.p + 1, offsets.p + np, 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    n = np;
+    dev_ids = ids;
+    samples = static_cast<size_t>(info.p[1]);
+    t.ensure(samples);
+    irr.ensure(samples);
+    launch_sample_window(field.f, r, t_w, ids, lv, nn, c_in, s_in, counts.p, offsets.p, t.p, irr.p, c_out, s_out, 1,
+                         s);
+    CK(cudaGetLastError());
+  }
+  DevBuf<unsigned long long> err;
+  PinBuf<unsigned long long> info;
+  const uint32_t* dev_ids = nullptr;  // the last device window's ids (the caller's array), null after a host window
 };
 
 // ---------------------------------------------------------------------------------------------
@@ -1938,6 +1983,46 @@ bs_status bs_sample_window(bs_sampler* s, int64_t t_w, const uint32_t* pixel_ids
     if (n_samples) *n_samples = s->samples;
   });
 }
+bs_status bs_sample_window_device(bs_sampler* s, int64_t t_w, const uint32_t* pixel_ids, const uint8_t* levels,
+                                  size_t n, const float* carried_irr, const uint64_t* carried_sig,
+                                  float* carried_irr_out, uint64_t* carried_sig_out, const bs_sample_rules* rules,
+                                  void* stream, size_t* n_samples) {
+  return guarded([&] {
+    NEED(s);
+    NEED(rules);
+    if (n) {
+      NEED(pixel_ids);
+      NEED(levels);
+      NEED(carried_irr);
+      NEED(carried_sig);
+      NEED(carried_irr_out);
+      NEED(carried_sig_out);
+    }
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->own;
+    s->window_device(t_w, pixel_ids, levels, n, carried_irr, carried_sig, carried_irr_out, carried_sig_out, *rules,
+                     st);
+    if (n_samples) *n_samples = s->samples;
+  });
+}
+bs_status bs_field_levels_device(bs_sampler* s, int64_t t_w, int32_t l_min, int32_t l_max, uint8_t* out,
+                                 void* stream) {
+  return guarded([&] {
+    NEED(s);
+    NEED(out);
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->own;
+    bs::launch_levels(s->field.f, t_w, l_min, l_max, s->field.f.width * s->field.f.height, out, st);
+    bs::CK(cudaGetLastError());
+  });
+}
+bs_status bs_field_frame_device(bs_sampler* s, int64_t t_ns, float* out, void* stream) {
+  return guarded([&] {
+    NEED(s);
+    NEED(out);
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->own;
+    bs::launch_field_frame(s->field.f, t_ns, s->field.f.width * s->field.f.height, out, st);
+    bs::CK(cudaGetLastError());
+  });
+}
 bs_status bs_sampler_download(bs_sampler* s, int64_t* offsets, int64_t* t_ns, float* irr) {
   return guarded([&] {
     NEED(s);
@@ -1950,7 +2035,7 @@ bs_status bs_sampler_device_runs(bs_sampler* s, bs_device_runs* out) {
   return guarded([&] {
     NEED(s);
     NEED(out);
-    out->pixel = s->pixel.p;
+    out->pixel = s->dev_ids ? s->dev_ids : s->pixel.p;
     out->row_start = s->offsets.p;
     out->row_count = reinterpret_cast<const int32_t*>(s->counts.p);
     out->n = s->n;

@@ -220,6 +220,33 @@ class SensorModel:
                                                         C.byref(ne)))
             return self._take(ne.value)
 
+    def init_device(self, t0_ns: int, irradiance0_ptr: int, stream: int | None = None) -> None:
+        """init from a device array of height * width floats (the frame a device renderer wrote), on stream."""
+        with self._lock:
+            _lib.check(_lib.lib().bs_model_init_device(self._h, int(t0_ns), irradiance0_ptr, stream))
+
+    def advance_device(self, runs: _lib.DeviceRuns, t_end_ns: int, stream: int | None = None) -> _lib.DeviceEvents:
+        """SensorModel::advance_device (src/sensor/sensor_model.h:157-167): runs in device memory (DeviceRuns), queued
+        on stream; one synchronization reads the call's counters. The events stay on the device (RawEvent records,
+        unordered), valid until the model advances again."""
+        ev = _lib.DeviceEvents()
+        with self._lock:
+            _lib.check(_lib.lib().bs_model_advance_device(self._h, C.byref(runs), int(t_end_ns), stream, C.byref(ev)))
+        return ev
+
+    def download_events(self, events: _lib.DeviceEvents, with_pixel: bool = False) -> dict:
+        """SensorModel::download_events (sensor_model.h:167): a call's device events as host columns sorted by
+        (t_cross_ns, pixel)."""
+        n = int(events.count)
+        cols = new_columns(n)
+        px = np.zeros(n, np.uint32) if with_pixel else None
+        s = column_struct(cols, px)
+        with self._lock:
+            _lib.check(_lib.lib().bs_model_download_events(self._h, C.byref(events), C.byref(s)))
+        if with_pixel:
+            cols["pixel"] = px
+        return cols
+
     def _take(self, n: int, with_pixel: bool = False) -> dict:
         cols = new_columns(n)
         px = np.zeros(n, np.uint32) if with_pixel else None

@@ -3,15 +3,22 @@
 One step = one pass of the hot path over the workload: every sensor initialized at t0 from its seeded analytic
 field, then every window sampled (dyadic lattice + eta_L refinement) and sensed (the instantaneous pixel model, or
 the cascade photoreceptor in workloads blobs_346x260_cascade and, with its noise lattice, blobs_346x260_lattice), in
-the fused engine. At N = 1 the workload is the 346 x 260 sensor (16 blobs, 2.0 s = 239 windows, mismatch 0.03,
-refractory 100 us, noise off); --workload picks another. With N GPUs (torchrun, one rank per GPU) each rank runs
-its own replica of the workload (independent sensors, seeds offset by rank): weak scaling, no collective on the
-data path; value = all ranks' pixel-samples / the slowest rank's device time.
+the fused engine. At N = 1 the workload is the largest one-GPU configuration: six sensors (346x260, 640x480 x2,
+1280x720 x2, 1920x1080; 4,621,160 px), 128 blobs each, thresholds per sensor, mismatch, leak, shot and
+background-activity noise, 0.5 s (60 windows), in one persistent launch; --workload picks another. With N GPUs
+(torchrun, one rank per GPU) each rank runs its own replica of the workload (independent sensors, seeds offset by
+rank): weak scaling, no collective on the data path; value = all ranks' pixel-samples / the slowest rank's device
+time.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
 
+The runs_* workloads take the reference engine's own two-kernel route instead (Camera::sample_and_sense): per
+sensor and window, sample_window on the device writes CSR runs to HBM and SensorModel::advance_device reads them
+(ballasim_b200.windows); the roofline line is then the pixel model on the runs (advance_runs_kernel).
+
 --impl reference times the reference's own CPU implementation (oracle/_ref: WindowEngine<kHost> and
-SensorModel fp32 on every host core) on a bounded sample of the same workload (its first windows), rank 0 only.
+SensorModel fp32 on every host core) on a bounded sample of the same workload (the first windows of every
+sensor), rank 0 only, with its fp64 kernel timed once on the same sample beside it.
 
 The sink_* workloads measure the event file sink instead: one step writes a whole RAW (EVT 2.0, 2.1, 3.0) or DAT
 file of a seeded 1280 x 720 stream of 32 Mi events (about 50 Mev/s, runs along rows; workloads.event_stream): the
@@ -46,13 +53,26 @@ WORKLOADS = {
     "blobs_346x260_cascade": W.blobs_346x260_cascade,
     "blobs_346x260_lattice": W.blobs_346x260_lattice,
 }
+# The same workloads through the reference engine's two-kernel route (runs in HBM).
+RUNS = {"runs_six_sensors": W.six_sensors, "runs_blobs_346x260": W.blobs_346x260,
+        "runs_blobs_1280x720": W.blobs_1280x720}
+DEFAULT_WORKLOAD = "six_sensors"
+# The reference arm's bounded sample: the first windows of every sensor.
+CPU_WINDOWS = {"six_sensors": 2, "runs_six_sensors": 2, "blobs_1280x720": 4, "runs_blobs_1280x720": 4}
+CPU_WINDOWS_DEFAULT = 40
+N_SMS, SCHEDULERS_PER_SM = 148, 4
 METRIC = "pixel-samples/s"
 SINKS = {"sink_evt3_1280x720": "evt3", "sink_evt21_1280x720": "evt21", "sink_evt2_1280x720": "evt2",
          "sink_dat_1280x720": "dat"}
 L2_BYTES = 126 * 1024 * 1024
-# DRAM bytes (read + write) of one launch of the engine kernel the autotuner picks, from an ncu capture of this
-# bench's own command (profiles/engine_kernel_coop_blobs16_346x260.md), per workload; other workloads report null.
-NCU_TRAFFIC_PER_LAUNCH = {"blobs16_346x260": 8.74e6 + 4.56e6}
+# Per workload, figures of one ncu capture of the dominant kernel of this bench's own command, kept beside the kernel
+# name and launch shape they were taken at (None where none was taken): DRAM bytes read + written per launch, warp
+# instructions issued per pixel-sample, and ncu's issue-slot activity. A run whose kernel or launch shape differs
+# from the capture's reports null for them.
+NCU = {
+    "blobs16_346x260": {"kernel": "engine_kernel_coop", "stage": 64, "tile_width": 8, "traffic": 8.74e6 + 4.56e6,
+                        "inst_per_sample": None, "issue_active": 0.285},
+}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -119,6 +139,31 @@ def b_sense(pixels: int, windows: int, samples: int, events: int) -> int:
     return samples * 12 + windows * pixels * (12 + 2 * 48 + 24) + events * 16
 
 
+def compute_fraction(wl_name: str, kernel: str, launch: dict, samples: float, kms: float, sm_mhz) -> dict:
+    """The issue-slot side of the roofline: warp instructions issued per launch (ncu's count per pixel-sample at the
+    captured launch shape, times this launch's pixel-samples) over the SMs' issue slots in the launch's duration at
+    the sampled median SM clock (148 SMs x 4 schedulers x cycles), with ncu's own issue-active beside it."""
+    cap = NCU.get(wl_name)
+    same = cap is not None and cap["kernel"] == kernel and cap.get("stage") == launch.get("stage") and \
+        cap.get("tile_width") == launch.get("tile_width")
+    out = {"ncu_capture": f"{cap['kernel']} stage {cap['stage']} tile {cap['tile_width']}" if cap else None,
+           "same_launch_shape": bool(same), "warp_inst_per_launch": None, "issue_slots_per_launch": None,
+           "issue_frac": None, "ncu_issue_active": cap.get("issue_active") if same else None}
+    if sm_mhz:
+        out["issue_slots_per_launch"] = N_SMS * SCHEDULERS_PER_SM * kms * 1e-3 * sm_mhz * 1e6
+    if same and cap.get("inst_per_sample") and sm_mhz:
+        out["warp_inst_per_launch"] = cap["inst_per_sample"] * samples
+        out["issue_frac"] = out["warp_inst_per_launch"] / out["issue_slots_per_launch"]
+    return out
+
+
+def engine_kernel_name(eng, cascade: bool, lattice: bool) -> str:
+    if cascade:
+        return "engine_lattice_kernel" if lattice else "engine_cascade_kernel"
+    return {64: "engine_kernel_coop", 16: "engine_kernel_staged<16>",
+            32: "engine_kernel_staged<32>"}.get(eng.launch["stage"], "engine_kernel")
+
+
 def run_ours(args, rank: int, world: int) -> dict | None:
     import torch
     import torch.distributed as dist
@@ -181,23 +226,31 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
     total_ms = float(sum(step_ms))
     total_ms_all, samples_all, events_all = reduce_step(total_ms, float(samples), float(events), world)
+    clocks = {k: v for k, v in clk.summary().items() if k != "samples"}
 
-    # e2e through the public API with host buffers: the initial frames from pinned host memory in, every event out
+    # e2e through the public API with host buffers: the initial frames from pinned host memory in, every event out;
+    # each phase timed on the host after a synchronize, for the split of the e2e step.
     frames = [torch.from_numpy(field_frame(s.field, 0)).pin_memory().numpy() for s in wl.sensors]
-    e2e_times, d2h = [], 0
+    e2e_times, d2h, split = [], 0, {"start_ms": 0.0, "run_ms": 0.0, "take_events_ms": 0.0}
     for k in range(0 if args.profile else args.warmup + args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         eng.start(0, sptr, frames=frames)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
         eng.run(wl.windows, sptr)
+        t2 = time.perf_counter()
         n_ev = 0
         for m in models:
             cols = m.take_events()
             n_ev += len(cols["t_cross_ns"])
         torch.cuda.synchronize()
+        t3 = time.perf_counter()
         if k >= args.warmup:
-            e2e_times.append(time.perf_counter() - t0)
+            e2e_times.append(t3 - t0)
             d2h = n_ev * 32
+            for key, v in zip(split, (t1 - t0, t2 - t1, t3 - t2)):
+                split[key] += 1e3 * v / args.steps
     e2e_s = reduce_max(sum(e2e_times), world)
     h2d = sum(int(f.nbytes) for f in frames)
 
@@ -210,6 +263,10 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     kms = statistics.mean(kernel_ms)
     alg = b_sense(pixels, wl.windows, int(per_step_samples), int(per_step_events))
     achieved = alg / (kms * 1e-3) / 1e9
+    kname = engine_kernel_name(eng, cascade, lattice)
+    cap = NCU.get(wl.name)
+    same_shape = cap is not None and cap["kernel"] == kname and cap.get("stage") == eng.launch["stage"] and \
+        cap.get("tile_width") == eng.launch["tile_width"]
     out = {
         "metric": METRIC,
         "value": samples_all / (total_ms_all * 1e-3),
@@ -228,26 +285,148 @@ def run_ours(args, rank: int, world: int) -> dict | None:
                    "events_per_step": int(per_step_events), "l2": "flushed between steps (256 MiB write)",
                    "sampler": {"tol": r.tol, "min_dt_ns": r.min_dt_ns, "max_refine_levels": r.max_refine_levels,
                                "levels": [r.l_min, r.l_max]},
-                   "parallelism": f"replicas x{world}",
+                   "parallelism": f"replicas x{world}", "path": "fused engine (runs kept on chip)",
                    "launch": {**eng.launch, "autotuned": tuned is not None, "cuda_graph": not args.no_graph,
                               "threads_per_pixel": 1}},
         "gpu_launches": 3 * args.steps,
-        "clocks": {k: v for k, v in clk.summary().items() if k != "samples"},
-        "e2e": {"value": samples_all / e2e_s if e2e_times else None, "unit": "pixel-samples/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
-        "roofline": {"kernel": (("engine_lattice_kernel" if lattice else "engine_cascade_kernel") if cascade
-                                else {64: "engine_kernel_coop", 16: "engine_kernel_staged<16>",
-                                      32: "engine_kernel_staged<32>"}.get(eng.launch["stage"], "engine_kernel")) +
-                               " (sampler + pixel model fused, runs kept on chip)", "bound": "hbm",
+        "clocks": clocks,
+        "e2e": {"value": samples_all / e2e_s if e2e_times else None, "unit": "pixel-samples/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "split_ms_per_step": {k: round(v, 3) for k, v in split.items()}},
+        "roofline": {"kernel": kname + " (sampler + pixel model fused, runs kept on chip)",
+                     "bound": "issue",
+                     "bound_note": "SIMT fp32 issue and latency (field exps, one log per sample, each crossing's "
+                                   "search and fire), not HBM; achieved/peak/frac are the algorithmic bytes of the "
+                                   "pixel model (B_sense) over the measured HBM copy bandwidth",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "peak_kind": hbm_kind, "traffic": NCU_TRAFFIC_PER_LAUNCH.get(wl.name), "algorithmic_bytes_per_launch": alg,
-                     "avg_launch_ms": kms, "runs_write_avoided_bytes": int(per_step_samples) * 12},
+                     "peak_kind": hbm_kind, "traffic": cap["traffic"] if same_shape else None,
+                     "algorithmic_bytes_per_launch": alg, "avg_launch_ms": kms,
+                     "runs_write_avoided_bytes": int(per_step_samples) * 12,
+                     "compute": compute_fraction(wl.name, kname, eng.launch, per_step_samples, kms,
+                                                 clocks.get("sm_mhz"))},
     }
     if world == 1 and not (args.no_cpu_baseline or args.profile):
-        out["cpu_baseline"] = cpu_baseline(wl, args.cpu_windows)
+        out["cpu_baseline"] = cpu_baseline(wl, cpu_windows(args))
     if rank == 0 and not (args.no_learned or args.profile):
         out["learned_vs_plain"] = learned_comparison()
     return out
+
+
+def run_runs(args, rank: int, world: int) -> dict | None:
+    """The reference engine's route with the runs in HBM (ballasim_b200.windows.DeviceWindows): per window and
+    sensor, the levels, sample_window on the device (count pass, scan, write pass) and advance_device (scatter of the
+    rows, advance_runs_kernel); the events stay on the device. Kernel time of the pixel model from CUDA events around
+    each advance_runs_kernel launch."""
+    import torch
+    import torch.distributed as dist
+
+    from ballasim_b200 import _lib
+    from ballasim_b200.params import resolve
+    from ballasim_b200.sensor import SensorModel
+    from ballasim_b200.windows import DeviceWindows
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    if not _lib.cuda_available():
+        raise RuntimeError("bench: no B200 visible")
+    wl = replica(RUNS[args.workload](), rank)
+    if args.windows:
+        wl.windows = min(wl.windows, args.windows)
+    r = wl.rules
+    models = [SensorModel(resolve(s.preset, s.overrides), s.width, s.height, s.seed, [{"type": "constant"}], s.camera)
+              for s in wl.sensors]
+    if args.block:
+        for m in models:
+            m.set_block(args.block)
+    dw = DeviceWindows([(m, s.field) for m, s in zip(models, wl.sensors)], tol=r.tol, dark=r.dark,
+                       min_dt_ns=r.min_dt_ns, max_refine_levels=r.max_refine_levels, l_min=r.l_min, l_max=r.l_max)
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        dw.start(0, sptr)
+        return dw.run(wl.windows, sptr)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    samples = events = 0
+    dw.launch_ms = 0.0
+    launches0 = sum(m.stats()["gpu_launches"] for m in models)
+    with Clocks(torch.cuda.current_device()) as clk:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.zero_()
+            starts[k].record(stream)
+            s_, e_ = step()
+            ends[k].record(stream)
+            samples += s_
+            events += e_
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+    advance_launches = sum(m.stats()["gpu_launches"] for m in models) - launches0
+    step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+    total_ms = float(sum(step_ms))
+    total_ms_all, samples_all, events_all = reduce_step(total_ms, float(samples), float(events), world)
+    clocks = {k: v for k, v in clk.summary().items() if k != "samples"}
+
+    # e2e through the public API with host buffers: the initial frames from pinned host memory in, per window and
+    # sensor every event downloaded to host columns.
+    from ballasim_b200.sampling import field_frame
+
+    frames = [torch.from_numpy(field_frame(s.field, 0)).pin_memory().numpy() for s in wl.sensors]
+    e2e_times, d2h = [], 0
+    for k in range(0 if args.profile else args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dw.start(0, sptr, frames=frames)
+        n_ev = [0]
+
+        def take(i, m, ev):
+            n_ev[0] += len(m.download_events(ev)["t_cross_ns"])
+
+        dw.run(wl.windows, sptr, on_events=take)
+        torch.cuda.synchronize()
+        if k >= args.warmup:
+            e2e_times.append(time.perf_counter() - t0)
+            d2h = n_ev[0] * 32
+    e2e_s = reduce_max(sum(e2e_times), world)
+    if rank != 0:
+        return None
+    per_step_samples = samples / args.steps
+    per_step_events = events / args.steps
+    hbm, hbm_kind = measured_hbm()
+    kms_total = dw.launch_ms / args.steps  # the pixel model's kernels, per step
+    n_launch = advance_launches / args.steps
+    alg = b_sense(wl.pixels, wl.windows, int(per_step_samples), int(per_step_events))
+    achieved = alg / (kms_total * 1e-3) / 1e9
+    cap = NCU.get("runs:" + wl.name)
+    calls = wl.windows * len(wl.sensors)
+    return {
+        "metric": METRIC, "value": samples_all / (total_ms_all * 1e-3), "unit": "pixel-samples/s",
+        "events_per_s": events_all / (total_ms_all * 1e-3), "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms_all / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+        "data": "synthetic (seeded analytic irradiance fields evaluated on the device)",
+        "config": {**wl.describe(), "pixel_samples_per_step": int(per_step_samples),
+                   "events_per_step": int(per_step_events), "l2": "flushed between steps (256 MiB write)",
+                   "path": "sample_window (device) -> runs in HBM -> advance_device, per sensor and window",
+                   "parallelism": f"replicas x{world}", "advance_block": args.block or "default"},
+        "gpu_launches": 9 * calls * args.steps + 2 * len(wl.sensors) * args.steps,
+        "clocks": clocks,
+        "e2e": {"value": samples_all / e2e_s if e2e_times else None, "unit": "pixel-samples/s",
+                "h2d_bytes_per_step": sum(int(f.nbytes) for f in frames), "d2h_bytes_per_step": d2h},
+        "roofline": {"kernel": "advance_runs_kernel (the pixel model on CSR runs read from HBM)", "bound": "hbm",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_kind": hbm_kind, "traffic": cap["traffic"] if cap else None,
+                     "algorithmic_bytes_per_step": alg, "launches_per_step": n_launch,
+                     "kernel_ms_per_step": kms_total, "share_of_step": kms_total / (total_ms_all / args.steps)},
+    }
 
 
 def _sink_writer(fmt: str, path: str, es):
@@ -417,21 +596,45 @@ def learned_comparison(train_stride: int = 4, steps: int = 9000, tau: float = 0.
     }
 
 
-def cpu_baseline(wl: W.Workload, windows: int) -> dict:
-    """The reference's own CPU path (oracle/_ref) on the first `windows` windows of the first sensor."""
+def cpu_windows(args) -> int:
+    return args.cpu_windows or CPU_WINDOWS.get(args.workload, CPU_WINDOWS_DEFAULT)
+
+
+def reference_sample(wl: W.Workload, windows: int, fp64: bool = False) -> dict:
+    """The reference's own CPU path (oracle/_ref) on a bounded sample of the workload: every sensor, its first
+    `windows` windows from t0 (WindowEngine<kHost>, serial by design, then SensorModel on every host thread).
+    The reference has no shot or background-activity noise: those rows are not passed, leak is."""
     from ballasim_b200.params import resolve
     from oracle.oracle import Ref
 
-    spec = wl.sensors[0]
     w = min(windows, wl.windows)
-    m = Ref.Model(resolve(spec.preset, spec.overrides), spec.width, spec.height, spec.seed, spec.camera)
-    t0 = time.perf_counter()
-    _, st = m.simulate(spec.field, wl.rules, w)
-    dt = time.perf_counter() - t0
-    return {"value": st["pixel_samples"] / dt, "unit": "pixel-samples/s", "cores": m.threads, "kind": "reference",
-            "sample": f"{spec.width}x{spec.height}, first {w} of {wl.windows} windows "
-                      f"({st['pixel_samples']} pixel-samples, {dt:.2f} s; sampler serial {st['sampler_s']:.2f} s, "
-                      f"pixel model on {m.threads} threads {st['sensor_s']:.2f} s)"}
+    samples, wall, sampler_s, sensor_s, threads = 0, 0.0, 0.0, 0.0, 0
+    for spec in wl.sensors:
+        m = Ref.Model(resolve(spec.preset, spec.overrides), spec.width, spec.height, spec.seed, spec.camera,
+                      fp64=fp64)
+        t0 = time.perf_counter()
+        _, st = m.simulate(spec.field, wl.rules, w)
+        wall += time.perf_counter() - t0
+        samples += st["pixel_samples"]
+        sampler_s += st["sampler_s"]
+        sensor_s += st["sensor_s"]
+        threads = m.threads
+    sizes = ", ".join(f"{s.width}x{s.height}" for s in wl.sensors)
+    return {"value": samples / wall, "unit": "pixel-samples/s", "cores": threads, "kind": "reference",
+            "precision": "fp64" if fp64 else "fp32", "pixel_samples": samples, "seconds": round(wall, 3),
+            "sample": f"every sensor ({sizes}), first {w} of {wl.windows} windows ({samples} pixel-samples, "
+                      f"{wall:.2f} s: the sampler, serial by design, {sampler_s:.2f} s; the pixel model on "
+                      f"{threads} threads {sensor_s:.2f} s); shot and background-activity noise have no reference "
+                      f"counterpart and are off there"}
+
+
+def cpu_baseline(wl: W.Workload, windows: int) -> dict:
+    """The reference CPU path's fp32 figure on the bounded sample, its fp64 kernel (the reference's default CPU
+    precision) on the same sample beside it."""
+    out = reference_sample(wl, windows)
+    f64 = reference_sample(wl, windows, fp64=True)
+    out["fp64"] = {"value": f64["value"], "seconds": f64["seconds"]}
+    return out
 
 
 def run_reference(args, rank: int) -> dict | None:
@@ -451,30 +654,25 @@ def run_reference(args, rank: int) -> dict | None:
                 "data": "synthetic (seeded event stream)", "config": {**es.describe(), "format": SINKS[args.workload]},
                 "cpu_baseline": {**cb, "value": value},
                 "e2e": {"value": value, "unit": "events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    wl = WORKLOADS[args.workload]()
-    from ballasim_b200.params import resolve
-    from oracle.oracle import Ref
-
-    spec = wl.sensors[0]
-    w = min(args.cpu_windows, wl.windows)
-    vals, threads, samples = [], 0, 0
+    wl = (RUNS.get(args.workload) or WORKLOADS[args.workload])()
+    w = cpu_windows(args)
+    secs, last = [], None
     for k in range(args.warmup + args.steps):
-        m = Ref.Model(resolve(spec.preset, spec.overrides), spec.width, spec.height, spec.seed, spec.camera)
-        t0 = time.perf_counter()
-        _, st = m.simulate(spec.field, wl.rules, w)
-        dt = time.perf_counter() - t0
-        threads, samples = m.threads, st["pixel_samples"]
+        last = reference_sample(wl, w)
         if k >= args.warmup:
-            vals.append(dt)
-    total = sum(vals)
-    value = samples * len(vals) / total
-    sample = f"{spec.width}x{spec.height}, first {w} of {wl.windows} windows per step ({samples} pixel-samples)"
+            secs.append(last["seconds"])
+    total = sum(secs)
+    value = last["pixel_samples"] * len(secs) / total
+    f64 = reference_sample(wl, w, fp64=True)
+    cb = {k: last[k] for k in ("unit", "cores", "kind", "sample", "precision")}
     return {"impl": "reference", "metric": METRIC, "value": value, "unit": "pixel-samples/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(vals),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(secs),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
-            "data": "synthetic (seeded analytic irradiance fields)", "config": {**wl.describe(), "bounded_windows": w},
-            "cpu_baseline": {"value": value, "unit": "pixel-samples/s", "cores": threads, "kind": "reference",
-                             "sample": sample},
+            "data": "synthetic (seeded analytic irradiance fields)",
+            "config": {**wl.describe(), "bounded_windows_per_sensor": min(w, wl.windows)},
+            "cpu_baseline": {**cb, "value": value},
+            "fp64": {"value": f64["value"], "unit": "pixel-samples/s", "seconds": f64["seconds"],
+                     "note": "the reference's fp64 CPU kernel (its default precision) on the same sample, once"},
             "e2e": {"value": value, "unit": "pixel-samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -484,8 +682,11 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(SINKS), default="blobs_346x260")
-    ap.add_argument("--cpu-windows", type=int, default=40)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(RUNS) + sorted(SINKS),
+                    default=DEFAULT_WORKLOAD)
+    ap.add_argument("--cpu-windows", type=int, default=0,
+                    help="windows of every sensor in the reference's bounded sample (0: the workload's default)")
+    ap.add_argument("--block", type=int, default=0, help="runs_* workloads: threads per block of advance_runs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--warps", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
@@ -509,7 +710,12 @@ def main():
 
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         try:
-            out = run_sink(args, rank, world) if args.workload in SINKS else run_ours(args, rank, world)
+            if args.workload in SINKS:
+                out = run_sink(args, rank, world)
+            elif args.workload in RUNS:
+                out = run_runs(args, rank, world)
+            else:
+                out = run_ours(args, rank, world)
         finally:
             if world > 1:
                 import torch.distributed as dist

@@ -200,8 +200,25 @@ bs_status bs_sampler_destroy(bs_sampler* s);
 bs_status bs_sample_window(bs_sampler* s, int64_t t_w, const uint32_t* pixel_ids, const uint8_t* levels, size_t n,
                            float* carried_irr, uint64_t* carried_sig, const bs_sample_rules* rules,
                            size_t* n_samples);
+/* sample_window with the inputs in device memory, as the reference's device window engine takes them
+ * (WindowEngine<Space::kDevice>::run, src/engine/window.h:133-174; its caller Camera::sample_and_sense,
+ * src/engine/engine_impl.h:1253-1343): pixel_ids, levels and the carried samples (carried_irr / carried_sig in,
+ * each pixel's last sample at t_w + W to carried_irr_out / carried_sig_out, arrays that must not alias the inputs)
+ * are the caller's device arrays, read on `stream` (NULL: the sampler's own stream). The ids and levels are checked
+ * on the device first (BS_EINVAL as bs_sample_window, nothing written). The runs stay in the sampler's memory for
+ * bs_sampler_device_runs -> bs_model_advance_device on the same stream; *n_samples gets their total. The call
+ * synchronizes `stream` twice (the check, the sample count) and leaves the write pass queued on it. */
+bs_status bs_sample_window_device(bs_sampler* s, int64_t t_w, const uint32_t* pixel_ids, const uint8_t* levels,
+                                  size_t n, const float* carried_irr, const uint64_t* carried_sig,
+                                  float* carried_irr_out, uint64_t* carried_sig_out, const bs_sample_rules* rules,
+                                  void* stream, size_t* n_samples);
+/* bs_field_levels and bs_field_frame into device arrays (width * height), queued on `stream`. */
+bs_status bs_field_levels_device(bs_sampler* s, int64_t t_w, int32_t l_min, int32_t l_max, uint8_t* out,
+                                 void* stream);
+bs_status bs_field_frame_device(bs_sampler* s, int64_t t_ns, float* out, void* stream);
 /* The last window's runs to host arrays (WindowRuns: offsets n + 1, t_ns, irradiance), or as device runs for
- * bs_model_advance_device (valid until the sampler runs again). */
+ * bs_model_advance_device (valid until the sampler runs again; after bs_sample_window_device the runs' pixel ids
+ * are the caller's array). */
 bs_status bs_sampler_download(bs_sampler* s, int64_t* offsets, int64_t* t_ns, float* irr);
 bs_status bs_sampler_device_runs(bs_sampler* s, bs_device_runs* out);
 /* sample_window for callers that cannot allocate device memory: code running under an external memory manager with
@@ -212,8 +229,9 @@ bs_status bs_sampler_device_runs(bs_sampler* s, bs_device_runs* out);
  * device array sized for at most 1,048,576 pixels (about 4 MiB, held by every GPU that loads the library until the
  * process exits); more pixels are refused (BS_EINVAL). It runs on the current device and on `stream` (NULL: the
  * default stream); its first call on a device looks up the array's device address, so make that first call before
- * any stream capture. *n_samples receives the window's sample count, also when it exceeds capacity (BS_EINVAL, the
- * outputs then unwritten). All calls share the one array: calls that overlap on the GPU (other streams, other host
+ * any stream capture. Each call synchronizes `stream` three times: it copies the input check's result and the
+ * window's sample count to the host, and returns once the runs are written. *n_samples receives the window's sample
+ * count, also when it exceeds capacity (BS_EINVAL, the outputs then unwritten). All calls share the one array: calls that overlap on the GPU (other streams, other host
  * threads) race and must be serialized by the caller. */
 bs_status bs_sample_window_static(const bs_field* field, int64_t t_w, const uint32_t* pixel_ids,
                                   const uint8_t* levels, size_t n, const float* carried_irr,

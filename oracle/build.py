@@ -3,8 +3,9 @@
 - ``build_port()``: the C restatement in oracle/port/ -> oracle/_build/liboracle.so (gcc, -ffp-contract=off).
 - ``build_ref()``: the reference's own CPU sources, compiled where they lie with the reference's floating-point
   policy (cmake/FloatingPoint.cmake:8-26: -ffp-contract=off -fno-fast-math, -march=x86-64-v3) and linked with
-  oracle/ref_harness.cpp into oracle/_ref/libballa_ref.so. It needs the reference tree (REFERENCE_ROOT, default
-  /root/reference); where that is absent the prebuilt library is used as it is. No reference source is copied.
+  oracle/ref_harness.cpp into oracle/_ref/libballa_ref.so. It needs the reference tree: REFERENCE_ROOT, else a
+  directory named ``reference`` beside this repository; where neither exists the prebuilt library is used as it
+  is. No reference source is copied.
 
 Run ``python -m oracle.build`` from the repository root, or call the functions.
 """
@@ -38,7 +39,8 @@ PORT_FLAGS = ["-std=c11", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC",
 
 
 def reference_root() -> Path:
-    return Path(os.environ.get("REFERENCE_ROOT", "/root/reference"))
+    env = os.environ.get("REFERENCE_ROOT")
+    return Path(env) if env else HERE.parent.parent / "reference"
 
 
 def _run(cmd: list[str]) -> None:

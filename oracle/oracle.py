@@ -378,6 +378,9 @@ class Ref:
             L.ref_model_create.restype = C.c_void_p
             L.ref_model_create.argtypes = [C.c_char_p, C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.c_int,
                                            C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, C.c_int]
+            L.ref_model_create_prec.restype = C.c_void_p
+            L.ref_model_create_prec.argtypes = [C.c_char_p, C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.c_int,
+                                                C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, C.c_int, C.c_int]
             L.ref_model_destroy.argtypes = [C.c_void_p]
             L.ref_model_init.argtypes = [C.c_void_p, C.c_int64, _f32p]
             L.ref_model_advance_runs.argtypes = [C.c_void_p, _u32p, C.c_size_t, _i64p, _f32p, C.c_size_t, _i64p,
@@ -561,7 +564,7 @@ class Ref:
                 "eps_L", "sigma_o", "noise_leaf_level", "noise_margin_z", "stationary_burnin_ns",
                 "stationary_probe_pixels")
 
-        def __init__(self, params, width, height, seed, camera=0, num_threads=0):
+        def __init__(self, params, width, height, seed, camera=0, num_threads=0, fp64=False):
             self.L = Ref.lib()
             self.width, self.height = width, height
             v = params.as_dict()
@@ -576,8 +579,8 @@ class Ref:
                                                         1.0 if v["noise_diffusion"] == "transient" else 0.0]
             ck = (C.c_char_p * len(keys))(*[k.encode() for k in keys])
             cv = (C.c_double * len(vals))(*vals)
-            self.h = self.L.ref_model_create(v["family"].encode(), ck, cv, len(keys), width, height, seed, camera,
-                                             num_threads)
+            self.h = self.L.ref_model_create_prec(v["family"].encode(), ck, cv, len(keys), width, height, seed,
+                                                  camera, num_threads, 1 if fp64 else 0)
             if not self.h:
                 raise ValueError(self.L.ref_last_error().decode())
 

@@ -1,5 +1,5 @@
 // A C-ABI harness around the reference's own CPU implementation of the path, compiled from its
-// sources in place by oracle/build_ref.sh into oracle/_ref/libballa_ref.so. TEST INFRASTRUCTURE
+// sources in place by oracle/build.py (build_ref) into oracle/_ref/libballa_ref.so. TEST INFRASTRUCTURE
 // ONLY: it pins the oracle port (oracle/port) and is the CPU baseline of bench.py's reference arm.
 //
 // It drives balla::sensor::SensorModel (src/sensor/sensor_model.h:98-320) on the fp32 precision
@@ -127,23 +127,29 @@ extern "C" {
 
 const char* ref_last_error() { return g_error.c_str(); }
 
-// preset: a family name; keys/values: n_over overrides (SensorParams field names).
-void* ref_model_create(const char* preset, const char* const* keys, const double* values, int n_over, uint32_t width,
-                       uint32_t height, uint64_t seed, uint32_t camera, int num_threads) {
+// preset: a family name; keys/values: n_over overrides (SensorParams field names); fp64 != 0: the reference's fp64
+// CPU kernel (its default precision, Precision::kFp64, src/sensor/sensor_model.h:30), else fp32.
+void* ref_model_create_prec(const char* preset, const char* const* keys, const double* values, int n_over,
+                            uint32_t width, uint32_t height, uint64_t seed, uint32_t camera, int num_threads,
+                            int fp64) {
   try {
     sensor::SensorParams p = sensor::preset(preset);
     for (int i = 0; i < n_over; ++i) set_field(p, keys[i], values[i]);
     p.validate();
     auto* m = new RefModel;
-    m->model = std::make_unique<sensor::SensorModel>(p, width, height, seed,
-                                                     std::vector<sensor::Waveform>{sensor::make_constant_waveform()},
-                                                     camera, num_threads, sensor::Precision::kFp32,
-                                                     sensor::Device::kCpu);
+    m->model = std::make_unique<sensor::SensorModel>(
+        p, width, height, seed, std::vector<sensor::Waveform>{sensor::make_constant_waveform()}, camera, num_threads,
+        fp64 ? sensor::Precision::kFp64 : sensor::Precision::kFp32, sensor::Device::kCpu);
     return m;
   } catch (const std::exception& e) {
     fail(e);
     return nullptr;
   }
+}
+
+void* ref_model_create(const char* preset, const char* const* keys, const double* values, int n_over, uint32_t width,
+                       uint32_t height, uint64_t seed, uint32_t camera, int num_threads) {
+  return ref_model_create_prec(preset, keys, values, n_over, width, height, seed, camera, num_threads, 0);
 }
 
 void ref_model_destroy(void* h) { delete static_cast<RefModel*>(h); }
