@@ -45,7 +45,7 @@ class Params(C.Structure):
                [(n, C.c_double) for n in ("k", "tau_o", "tau_sf", "eps_L")] + [("noise", C.c_int32)] + \
                [("sigma_o", C.c_double), ("noise_margin_z", C.c_double), ("noise_leaf_level", C.c_int32),
                 ("noise_diffusion", C.c_int32), ("initial_state", C.c_int32), ("stationary_probe_pixels", C.c_int32),
-                ("stationary_burnin_ns", C.c_int64)]
+                ("stationary_burnin_ns", C.c_int64), ("fingerprint", C.c_uint64)]
 
 
 class EventColumns(C.Structure):
@@ -123,6 +123,7 @@ _SIGS = {
     "bs_model_save_state": (C.c_int32, [_P, _P, C.c_size_t]),
     "bs_model_load_state": (C.c_int32, [_P, _P, C.c_size_t]),
     "bs_model_set_block": (C.c_int32, [_P, C.c_int32]),
+    "bs_model_set_long_run": (C.c_int32, [_P, C.c_int32]),
     "bs_sampler_create": (C.c_int32, [C.POINTER(Field), C.POINTER(_P)]),
     "bs_sampler_destroy": (C.c_int32, [_P]),
     "bs_sample_window": (C.c_int32, [_P, C.c_int64, _P, _P, C.c_size_t, _P, _P, C.POINTER(SampleRules),

@@ -118,6 +118,14 @@ void launch_advance_runs(const SensorConsts& k, const CascadeConsts& cc, const N
                          const int32_t* row_count, const int64_t* t, const float* irr, uint64_t n_samples,
                          int64_t t_state, int64_t t_end, EventBuf ev, unsigned long long* counters, int block,
                          cudaStream_t stream);
+// The instantaneous response on CSR runs, row-major (one warp per 32 runs; runs longer than long_row samples walked
+// by the whole warp, the others one per lane); listed: a bitmap of n_pixels bits, zeroed by the caller; the pixels
+// no run lists advance too.
+void launch_advance_rows(const SensorConsts& k, const MapSoA& map, StateSoA in, StateSoA out, uint32_t n_pixels,
+                         const uint32_t* pixel, uint32_t n_rows, const int64_t* row_start, const int32_t* row_count,
+                         const int64_t* t, const float* irr, uint64_t n_samples, int64_t t_state, int64_t t_end,
+                         int32_t long_row, uint32_t* listed, EventBuf ev, unsigned long long* counters,
+                         cudaStream_t stream);
 // sample_window: pass 0 counts, pass 1 writes at offsets.
 void launch_sample_window(const FieldDev& f, const SamplerRules& r, int64_t t_w, const uint32_t* pixel,
                           const uint8_t* level, uint32_t n, const float* carried_in, const uint64_t* sig_in,

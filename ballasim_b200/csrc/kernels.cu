@@ -288,6 +288,327 @@ __global__ void __launch_bounds__(128) advance_runs_kernel(RunArgs a) {
   warp_or(&a.counters[kCntErrors], err);
 }
 
+// ---------------------------------------------------------------------------------------------
+// CSR runs -> the instantaneous pixel model, row-major, long runs walked by the whole warp
+// ---------------------------------------------------------------------------------------------
+// A warp takes 32 consecutive runs (lane = run; its pixel p = pixel[run]): the run arrays and, for runs listed in
+// pixel order, the state and map planes are read as contiguous segments. A run's time is set by its serial chain
+// (each segment's comparator state depends on the one before), so the longest run of a window bounds the call; here
+// runs longer than long_row samples are walked by all 32 lanes together, one after another:
+//  - the lanes load 32 consecutive samples (coalesced) and each computes its sample's x = ln(I / i_scale), the
+//    pixel's state broadcast to every lane;
+//  - each lane tests its segment (from the previous sample) for the fast path's clean outcome: the pixel not blind,
+//    the search armed at or before the segment's start, no noise candidate before its end, Delta at its start below
+//    both levels and the rest of it excluded by the exact bound (PixelProc::segment_fast, whose only effects there are
+//    the search time and the piece / node counters);
+//  - a ballot finds the first segment that is not clean: those before it take their effects at once, it runs through
+//    the pixel model on every lane with the same values (the state stays warp-uniform; lane 0 alone appends its
+//    events), and the lanes after it are tested again with the new state.
+// So a run of n samples with d segments that can fire costs about n / 32 + d steps instead of n. Runs of at most
+// long_row samples are walked one per lane, as advance_runs_kernel does. Every lane then advances its own pixel on its
+// last sample to t_end.
+//
+// Listed pixels are marked in a bitmap (one bit per pixel, cleared per call): a pixel listed twice is refused
+// (kErrDuplicate) as the reference does; pixels no run lists are advanced to t_end by advance_unlisted_kernel.
+constexpr int kRowsWarps = 4;
+
+struct RowsArgs {
+  SensorConsts k;
+  MapSoA map;
+  StateSoA in, out;
+  uint32_t n_pixels;
+  const uint32_t* pixel;
+  uint32_t n_rows;
+  const int64_t* row_start;
+  const int32_t* row_count;
+  const int64_t* t;
+  const float* irr;
+  uint64_t n_samples;
+  int64_t t_state, t_end;
+  int32_t long_row;
+  uint32_t* listed;
+  EventBuf ev;
+  unsigned long long* counters;
+};
+
+// Marks the warp's pixels listed; returns kErrDuplicate if some pixel was listed before (in this warp or another).
+__device__ __forceinline__ unsigned long long mark_listed(uint32_t* listed, bool valid, uint32_t p) {
+  const unsigned full = 0xffffffffu;
+  unsigned long long err = 0;
+  const uint32_t key = valid ? p : 0xFFFFFFFFu;
+  const unsigned same = __match_any_sync(full, key);
+  if (valid && __popc(same) > 1) err |= kErrDuplicate;
+  const uint32_t word = valid ? (p >> 5) : 0xFFFFFFFFu;
+  const unsigned group = __match_any_sync(full, word);
+  const uint32_t bit = valid ? (1u << (p & 31u)) : 0u;
+  const uint32_t bits = __reduce_or_sync(group, bit);
+  if (valid && (threadIdx.x & 31u) == static_cast<uint32_t>(__ffs(group) - 1)) {
+    const uint32_t old = atomicOr(listed + word, bits);
+    if (old & bits) err |= kErrDuplicate;
+  }
+  return err;
+}
+
+// Inside warp-uniform processing every lane pushes the same event: lane 0 alone appends it.
+struct LaneZeroSink {
+  GlobalSink inner;
+  __device__ __forceinline__ void push(const RawEvent& e) {
+    if ((threadIdx.x & 31u) == 0u) inner.push(e);
+  }
+};
+
+__device__ __forceinline__ PixelRegs shfl_regs(const PixelRegs& s, int src) {
+  const unsigned full = 0xffffffffu;
+  PixelRegs o;
+  o.t_ref = __shfl_sync(full, s.t_ref, src);
+  o.t_search = __shfl_sync(full, s.t_search, src);
+  o.blind_until = __shfl_sync(full, s.blind_until, src);
+  o.s3_ref = __shfl_sync(full, s.s3_ref, src);
+  o.n3_ref = __shfl_sync(full, s.n3_ref, src);
+  o.dr_ref = __shfl_sync(full, s.dr_ref, src);
+  o.i_scale = __shfl_sync(full, s.i_scale, src);
+  o.held = __shfl_sync(full, s.held, src);
+  o.flags = __shfl_sync(full, s.flags, src);
+  o.t_shot = __shfl_sync(full, s.t_shot, src);
+  o.t_ba = __shfl_sync(full, s.t_ba, src);
+  o.n_shot = __shfl_sync(full, s.n_shot, src);
+  o.n_ba = __shfl_sync(full, s.n_ba, src);
+  return o;
+}
+
+__device__ __forceinline__ PixelMapRegs shfl_map(const PixelMapRegs& m, int src) {
+  const unsigned full = 0xffffffffu;
+  PixelMapRegs o;
+  o.theta_on = __shfl_sync(full, m.theta_on, src);
+  o.theta_off = __shfl_sync(full, m.theta_off, src);
+  o.leak = __shfl_sync(full, m.leak, src);
+  o.dark = __shfl_sync(full, m.dark, src);
+  o.scale = __shfl_sync(full, m.scale, src);
+  o.ba_rate_hz = __shfl_sync(full, m.ba_rate_hz, src);
+  o.shot_max_hz = __shfl_sync(full, m.shot_max_hz, src);
+  return o;
+}
+
+// Would PixelProc::segment_fast pass segment [t0, e) with nothing but its clean effects (the piece counted, the
+// search moved to e, a node counted when e - t0 > 2)? Only where it takes that branch: one 2^23 ns piece, the pixel
+// not blind, its search armed at or before t0, no noise candidate before e, Delta(t0) below both levels, and the
+// node (t0, e - 1] a single integer or excluded.
+template <class Sink>
+__device__ __forceinline__ bool clean_segment(const PixelProc<Sink>& proc, int64_t t0, int64_t e, float v0, float v1,
+                                              float x0, float x1) {
+  const PixelRegs& s = proc.s;
+  if (((e - 1) >> kWindowLog2) != (t0 >> kWindowLog2)) return false;
+  if (s.blind_until != kNotBlind || s.t_search > t0) return false;
+  const int64_t tn = proc.k.noise ? mini(s.t_shot, s.t_ba) : kForever;
+  if (tn < e) return false;
+  const float D0 = proc.delta(t0, x0);
+  if (D0 >= proc.m.theta_on || D0 <= -proc.m.theta_off) return false;
+  if (e - t0 == 1) return true;
+  return proc.excluded(Segment{t0, e, v0, v1}, t0, e, x0, x1);
+}
+
+// The warp-cooperative walk of one run (cnt samples at tp / vp) by a PixelProc whose state every lane holds alike.
+// prev_t / prev_v / x_prev: the last sample fed (at entry the held one at the model time, x_prev its x), updated.
+// Stops at the first sample out of order or after t_end (the call is refused then).
+__device__ __forceinline__ void coop_run(PixelProc<LaneZeroSink>& proc, const int64_t* tp, const float* vp,
+                                         int32_t cnt, const RowsArgs& a, uint32_t lane, int64_t& prev_t,
+                                         float& prev_v, float& x_prev, unsigned long long& err,
+                                         unsigned long long& clamps) {
+  const unsigned full = 0xffffffffu;
+  for (int32_t b = 0; b < cnt; b += 32) {
+    const int32_t i = b + static_cast<int32_t>(lane);
+    const bool in = i < cnt;
+    const int64_t ti = in ? __ldg(tp + i) : kForever;
+    const float raw = in ? __ldg(vp + i) : 0.0f;
+    if (in && !isfinite(raw)) err |= kErrNonFinite;
+    const float vi = clamp_irr(raw, a.k.irr_max);
+    if (in && !(vi == raw)) ++clamps;
+    const float xi = in ? proc.x_at_sample(vi) : 0.0f;
+    int64_t tq = __shfl_up_sync(full, ti, 1);
+    float vq = __shfl_up_sync(full, vi, 1), xq = __shfl_up_sync(full, xi, 1);
+    if (lane == 0u) {
+      tq = prev_t;
+      vq = prev_v;
+      xq = x_prev;
+    }
+    const bool bad_order = in && (i == 0 ? ti < a.t_state : ti <= tq);
+    const bool after = in && ti > a.t_end;
+    if (bad_order) err |= kErrOrder;
+    if (after) err |= kErrAfterEnd;
+    const unsigned bad = __ballot_sync(full, bad_order || after);
+    const int32_t left = cnt - b < 32 ? cnt - b : 32;
+    const int32_t limit = bad ? mini(__ffs(bad) - 1, left) : left;
+    int32_t j = 0;
+    // The run's first sample at the model time replaces the held one (pixel.h:777): no segment.
+    if (b == 0 && limit > 0 && __shfl_sync(full, ti, 0) == a.t_state) j = 1;
+    const unsigned upto = limit == 32 ? full : ((1u << limit) - 1u);
+    while (j < limit) {
+      const bool mine = static_cast<int32_t>(lane) >= j && static_cast<int32_t>(lane) < limit;
+      const bool clean = !mine || clean_segment(proc, tq, ti, vq, vi, xq, xi);
+      const unsigned range = upto & ~((1u << j) - 1u);
+      const unsigned dirty = __ballot_sync(full, !clean) & range;
+      const int32_t f = dirty ? __ffs(dirty) - 1 : limit;
+      if (f > j) {  // segments j .. f - 1 are clean: their effects at once
+        const unsigned cm = range & (f == 32 ? full : ((1u << f) - 1u));
+        proc.c.pieces += static_cast<uint32_t>(__popc(cm));
+        proc.c.leaves += static_cast<uint32_t>(__popc(__ballot_sync(full, ti - tq > 2) & cm));
+        proc.s.t_search = maxi(proc.s.t_search, __shfl_sync(full, ti, f - 1));
+      }
+      if (f < limit) {  // segment f through the pixel model, the same on every lane
+        const int64_t t0 = __shfl_sync(full, tq, f), e = __shfl_sync(full, ti, f);
+        const float v0 = __shfl_sync(full, vq, f), v1 = __shfl_sync(full, vi, f);
+        const float x0 = __shfl_sync(full, xq, f), x1 = __shfl_sync(full, xi, f);
+        if (((e - 1) >> kWindowLog2) == (t0 >> kWindowLog2)) {
+          proc.segment_fast(Segment{t0, e, v0, v1}, x0, x1);
+        } else {
+          proc.segment(Segment{t0, e, v0, v1}, t0, e);
+        }
+      }
+      j = f + 1;
+    }
+    if (limit > 0) {
+      prev_t = __shfl_sync(full, ti, limit - 1);
+      prev_v = __shfl_sync(full, vi, limit - 1);
+      x_prev = __shfl_sync(full, xi, limit - 1);
+    }
+    if (bad) break;
+  }
+}
+
+__global__ void __launch_bounds__(32 * kRowsWarps) advance_rows_kernel(RowsArgs a) {
+  const unsigned full = 0xffffffffu;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t row = (blockIdx.x * kRowsWarps + warp) * 32u + lane;
+  const bool in_rows = row < a.n_rows;
+  const uint32_t p = in_rows ? __ldg(a.pixel + row) : 0u;
+  unsigned long long err = 0, clamps = 0, samples = 0;
+  const bool valid = in_rows && p < a.n_pixels;
+  if (in_rows && !valid) err |= kErrPixelRange;
+  err |= mark_listed(a.listed, valid, p);
+  int64_t beg = 0;
+  int32_t cnt = 0;
+  if (valid) {
+    beg = __ldg(a.row_start + row);
+    cnt = __ldg(a.row_count + row);
+    if (cnt < 0 || beg < 0 || static_cast<uint64_t>(beg) + static_cast<uint64_t>(cnt) > a.n_samples) {
+      err |= kErrRunRange;
+      cnt = 0;
+      beg = 0;
+    }
+  }
+  const bool noise = a.k.noise != 0;
+  PixelRegs s{};
+  PixelMapRegs m{};
+  if (valid) {
+    load_state(a.in, p, noise, s);
+    load_map(a.map, p, m);
+  }
+  PixelCounters c;
+  GlobalSink sink{a.ev, &a.counters[kCntEvents]};
+  PixelProc<GlobalSink> proc{s, m, a.k, p, sink, c};
+  int64_t prev_t = a.t_state;
+  float prev_v = s.held;
+  const bool longrun = cnt > a.long_row;
+
+  // Short runs: one lane each.
+  if (cnt > 0 && !longrun) {
+    const int64_t* tp = a.t + beg;
+    const float* vp = a.irr + beg;
+    float x_prev = 0.0f;
+    bool have_x = false;
+    for (int32_t i = 0; i < cnt; ++i) {
+      const int64_t ti = __ldg(tp + i);
+      const float raw = __ldg(vp + i);
+      if (!isfinite(raw)) err |= kErrNonFinite;
+      const float vi = clamp_irr(raw, a.k.irr_max);
+      if (!(vi == raw)) ++clamps;
+      if (i == 0 ? ti < a.t_state : ti <= prev_t) {
+        err |= kErrOrder;
+        break;
+      }
+      if (ti > a.t_end) {
+        err |= kErrAfterEnd;
+        break;
+      }
+      if (i == 0 && ti == a.t_state) {  // a sample at the model time replaces the held one (pixel.h:777)
+        prev_v = vi;
+        continue;
+      }
+      if (((ti - 1) >> kWindowLog2) == (prev_t >> kWindowLog2)) {
+        if (!have_x) x_prev = proc.x_at_sample(prev_v);
+        const float x1 = proc.x_at_sample(vi);
+        proc.segment_fast(Segment{prev_t, ti, prev_v, vi}, x_prev, x1);
+        x_prev = x1;
+        have_x = true;
+      } else {
+        proc.segment(Segment{prev_t, ti, prev_v, vi}, prev_t, ti);
+        have_x = false;
+      }
+      prev_t = ti;
+      prev_v = vi;
+    }
+  }
+
+  // Long runs: the whole warp on each, one after another.
+  for (unsigned pend = __ballot_sync(full, longrun); pend != 0u; pend &= pend - 1u) {
+    const int r = __ffs(pend) - 1;
+    PixelRegs u = shfl_regs(s, r);
+    const PixelMapRegs um = shfl_map(m, r);
+    const uint32_t pr = __shfl_sync(full, p, r);
+    const int64_t br = __shfl_sync(full, beg, r);
+    const int32_t nr = __shfl_sync(full, cnt, r);
+    PixelCounters cu;
+    LaneZeroSink lz{sink};
+    PixelProc<LaneZeroSink> up{u, um, a.k, pr, lz, cu};
+    int64_t pt = a.t_state;
+    float pv = u.held, px = up.x_at_sample(u.held);
+    coop_run(up, a.t + br, a.irr + br, nr, a, lane, pt, pv, px, err, clamps);
+    if (static_cast<int>(lane) == r) {
+      s = u;
+      c.pieces += cu.pieces;
+      c.leaves += cu.leaves;
+      c.noise_candidates += cu.noise_candidates;
+      prev_t = pt;
+      prev_v = pv;
+    }
+  }
+
+  if (valid) {
+    samples = static_cast<unsigned long long>(cnt);
+    proc.segment(Segment{prev_t, kForever, prev_v, prev_v}, prev_t, a.t_end);
+    if (cnt > 0) s.held = prev_v;
+    store_state(a.out, p, noise, s);
+  }
+  __syncwarp();
+  warp_add(&a.counters[kCntClamps], clamps);
+  warp_add(&a.counters[kCntPieces], c.pieces);
+  warp_add(&a.counters[kCntLeaves], c.leaves);
+  warp_add(&a.counters[kCntSamples], samples);
+  warp_add(&a.counters[kCntNoise], c.noise_candidates);
+  warp_or(&a.counters[kCntErrors], err);
+}
+
+// The pixels no run lists: each advances on its held sample to t_end.
+__global__ void __launch_bounds__(128) advance_unlisted_kernel(RowsArgs a) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  PixelCounters c;
+  if (p < a.n_pixels && !((__ldg(a.listed + (p >> 5)) >> (p & 31u)) & 1u)) {
+    const bool noise = a.k.noise != 0;
+    PixelRegs s;
+    load_state(a.in, p, noise, s);
+    PixelMapRegs m;
+    load_map(a.map, p, m);
+    GlobalSink sink{a.ev, &a.counters[kCntEvents]};
+    PixelProc<GlobalSink> proc{s, m, a.k, p, sink, c};
+    proc.segment(Segment{a.t_state, kForever, s.held, s.held}, a.t_state, a.t_end);
+    store_state(a.out, p, noise, s);
+  }
+  __syncwarp();
+  warp_add(&a.counters[kCntPieces], c.pieces);
+  warp_add(&a.counters[kCntLeaves], c.leaves);
+  warp_add(&a.counters[kCntNoise], c.noise_candidates);
+}
+
 // The cascade with its noise lattice on CSR runs: the row is checked first (the same errors as advance_runs_kernel),
 // then the processor reads it with random access (the lattice's look-ahead).
 __global__ void __launch_bounds__(128) advance_runs_lattice_kernel(RunArgs a) {
@@ -1653,6 +1974,20 @@ void launch_advance_runs(const SensorConsts& k, const CascadeConsts& cc, const N
   if (k.cascade && tab.data != nullptr) advance_runs_lattice_kernel<<<grid, block, 0, stream>>>(a);
   else if (k.cascade) advance_runs_cascade_kernel<<<grid, block, 0, stream>>>(a);
   else advance_runs_kernel<<<grid, block, 0, stream>>>(a);
+}
+
+void launch_advance_rows(const SensorConsts& k, const MapSoA& map, StateSoA in, StateSoA out, uint32_t n_pixels,
+                         const uint32_t* pixel, uint32_t n_rows, const int64_t* row_start, const int32_t* row_count,
+                         const int64_t* t, const float* irr, uint64_t n_samples, int64_t t_state, int64_t t_end,
+                         int32_t long_row, uint32_t* listed, EventBuf ev, unsigned long long* counters,
+                         cudaStream_t stream) {
+  RowsArgs a{k, map, in, out, n_pixels, pixel, n_rows, row_start, row_count, t, irr, n_samples, t_state, t_end,
+             long_row, listed, ev, counters};
+  if (n_rows > 0) {
+    const unsigned grid = (n_rows + 32 * kRowsWarps - 1) / (32 * kRowsWarps);
+    advance_rows_kernel<<<grid, 32 * kRowsWarps, 0, stream>>>(a);
+  }
+  if (n_rows < n_pixels) advance_unlisted_kernel<<<(n_pixels + 127) / 128, 128, 0, stream>>>(a);
 }
 
 void launch_sample_window(const FieldDev& f, const SamplerRules& r, int64_t t_w, const uint32_t* pixel,

@@ -11,6 +11,7 @@
 #include <array>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -261,6 +262,7 @@ struct Model {
   StateSoA soa[2]{};
   int cur = 0;
   DevBuf<int32_t> row_of;
+  DevBuf<uint32_t> listed;  // the row-major CSR kernel's bitmap of listed pixels
   DevBuf<unsigned long long> counters;
   PinBuf<unsigned long long> counters_h;
   DevBuf<RawEvent> events;
@@ -274,7 +276,8 @@ struct Model {
   DevBuf<float> s_irr, s_frame;
   int64_t t_state = 0;
   bool initialized = false;
-  int block = 128;
+  int block = 0;  // 0: the row-major kernel (instantaneous response); else the per-pixel kernel's block
+  int32_t long_row = 32;  // the row-major kernel: runs longer than this are walked by the whole warp
   uint64_t stat_pieces = 0, stat_leaves = 0, stat_clamps = 0, stat_samples = 0, stat_noise = 0, stat_launches = 0,
            stat_reruns = 0;
   double launch_ms_total = 0, launch_ms_max = 0;
@@ -328,6 +331,7 @@ struct Model {
     soa[0] = st[0].soa(n, mode());
     soa[1] = st[1].soa(n, mode());
     row_of.ensure(n);
+    listed.ensure((n + 31) / 32);
     counters.ensure(kCntWords);
     counters_h.ensure(kCntWords);
     ensure_events(1 << 16);
@@ -597,12 +601,22 @@ struct Model {
     if (r.n > n) throw std::invalid_argument("SensorModel.advance: more runs than pixels");
     for (int attempt = 0;; ++attempt) {
       CK(cudaMemsetAsync(counters.p, 0, kCntWords * sizeof(unsigned long long), s));
-      CK(cudaMemsetAsync(row_of.p, 0xFF, n * sizeof(int32_t), s));
-      launch_scatter_rows(r.pixel, static_cast<uint32_t>(r.n), row_of.p, n, counters.p, s);
-      CK(cudaEventRecord(timer.a, s));
-      launch_advance_runs(k, cc, tab, map, soa[cur], soa[1 - cur], n, nullptr, r.n ? row_of.p : nullptr, r.row_start,
-                          r.row_count, r.t, r.irr, r.n_samples, t_state, t_end,
-                          EventBuf{events.p, static_cast<unsigned long long>(event_cap)}, counters.p, block, s);
+      const EventBuf evb{events.p, static_cast<unsigned long long>(event_cap)};
+      if (!k.cascade && block == 0) {
+        // The instantaneous response: row-major over the runs, the samples staged per warp.
+        CK(cudaMemsetAsync(listed.p, 0, ((n + 31) / 32) * sizeof(uint32_t), s));
+        CK(cudaEventRecord(timer.a, s));
+        launch_advance_rows(k, map, soa[cur], soa[1 - cur], n, r.pixel, static_cast<uint32_t>(r.n), r.row_start,
+                            r.row_count, r.t, r.irr, r.n_samples, t_state, t_end, long_row, listed.p, evb, counters.p,
+                            s);
+      } else {
+        CK(cudaMemsetAsync(row_of.p, 0xFF, n * sizeof(int32_t), s));
+        launch_scatter_rows(r.pixel, static_cast<uint32_t>(r.n), row_of.p, n, counters.p, s);
+        CK(cudaEventRecord(timer.a, s));
+        launch_advance_runs(k, cc, tab, map, soa[cur], soa[1 - cur], n, nullptr, r.n ? row_of.p : nullptr,
+                            r.row_start, r.row_count, r.t, r.irr, r.n_samples, t_state, t_end, evb, counters.p, block,
+                            s);
+      }
       CK(cudaGetLastError());
       CK(cudaEventRecord(timer.b, s));
       read_counters(s);
@@ -819,61 +833,180 @@ struct Model {
     }
   }
 
-  // save / load: header + the current state arrays.
-  struct Header {
-    uint32_t magic, version, width, height, camera, pad;
-    uint64_t seed, fingerprint;
+  // save / load in the reference's saved-state format (SensorModel::save_state / load_state,
+  // src/sensor/sensor_model.cpp:1198-1262): a StateHeader, then one 200-byte PixelState (src/sensor/pixel.h:105-121,
+  // fp64 fields) per pixel in pixel order. This model's fp32 state converts to and from the fp64 fields exactly, as
+  // the reference's fp32 kernel's load / store do (pixel.h:976-1041); the lattice's rho is stored as rho_m1 = rho - 1
+  // under transient diffusion and 0 under frozen (exact: rho is a float ratio). Fields a photoreceptor does not use
+  // are written 0 and not read. With this project's shot and background-activity noise on, one NoiseRecord per pixel
+  // follows (the two candidate chains' next times and counts; the reference has no such noise).
+  struct StateHeader {
+    uint32_t magic, version;
+    uint32_t width, height;
+    uint32_t groups, camera;
+    uint64_t seed;
+    uint64_t fingerprint;
     int64_t t_state;
-    uint32_t initialized, bytes_per_pixel;
+    uint32_t initialized;
+    uint32_t state_size;
   };
-  static constexpr uint32_t kMagic = 0x32304253;  // "SB02"
+  struct PixelStateRec {
+    double z, x1, s2, s3, i_scale, tv, nk[3], nk1[3], ln_a1;
+    int64_t cell, t_ref;
+    double s3_ref, n3_ref, dr_ref;
+    int64_t blind_until, t_search;
+    float held[8];
+    uint16_t flags;
+    uint8_t have_k1, reserved;
+    float rho_m1;
+  };
+  struct NoiseRecord {
+    int64_t t_shot, t_ba;
+    uint32_t n_shot, n_ba;
+    uint32_t pad[2];
+  };
+  static_assert(sizeof(StateHeader) == 56, "StateHeader layout is the reference's");
+  static_assert(sizeof(PixelStateRec) == 200, "PixelState layout is the reference's");
+  static_assert(sizeof(NoiseRecord) == 32, "NoiseRecord is 32 bytes");
+  static constexpr uint32_t kStateMagic = 0x534e5342;  // "BSNS" (sensor_model.cpp:28)
+  static constexpr uint32_t kStateVersion = 6, kStateVersionNoHpf = 5;
   int mode() const { return k.cascade == 0 ? 0 : (p.noise != 0 ? 2 : 1); }
   size_t i64_words() const { return StateBufs::i64_words(mode()); }
   size_t f32_words() const { return StateBufs::f32_words(mode()); }
   size_t u32_words() const { return StateBufs::u32_words(mode()); }
-  uint32_t bytes_per_pixel() const {
-    return static_cast<uint32_t>(i64_words() * 8 + f32_words() * 4 + u32_words() * 4);
+  bool noise_section() const { return k.noise != 0; }
+  size_t state_bytes() const {
+    return sizeof(StateHeader) + static_cast<size_t>(n) * sizeof(PixelStateRec) +
+           (noise_section() ? static_cast<size_t>(n) * sizeof(NoiseRecord) : 0);
   }
-  size_t state_bytes() const { return sizeof(Header) + static_cast<size_t>(n) * bytes_per_pixel(); }
-  // The parameters, and the gains when some gain is not 1 (src/sensor/sensor_model.cpp:53-66).
+  // state_fingerprint (sensor_model.cpp:53-66): the parameters' fingerprint, continued over the gains when some gain
+  // is not 1.
   uint64_t fingerprint() const {
-    const uint64_t h = fnv1a(&p, sizeof(p));
-    if (std::all_of(gain.begin(), gain.end(), [](float v) { return v == 1.0f; })) return h;
-    return fnv1a(gain.data(), gain.size() * sizeof(float), h);
+    if (std::all_of(gain.begin(), gain.end(), [](float v) { return v == 1.0f; })) return p.fingerprint;
+    return fnv1a(gain.data(), gain.size() * sizeof(float), p.fingerprint);
   }
 
   void save(uint8_t* out, size_t bytes) const {
     if (bytes != state_bytes()) throw std::invalid_argument("SensorModel.save_state: buffer size does not match");
-    Header h{kMagic, 1, width, height, camera, 0, seed, fingerprint(), t_state, initialized ? 1u : 0u, bytes_per_pixel()};
+    StateHeader h{kStateMagic, kStateVersion, width, height, 1u, camera, seed, fingerprint(), t_state,
+                  initialized ? 1u : 0u, static_cast<uint32_t>(sizeof(PixelStateRec))};
     std::memcpy(out, &h, sizeof(h));
-    uint8_t* q = out + sizeof(h);
     const StateBufs& b = st[cur];
-    CK(cudaMemcpy(q, b.i64.p, i64_words() * sizeof(int64_t) * n, cudaMemcpyDeviceToHost));
-    q += i64_words() * sizeof(int64_t) * n;
-    CK(cudaMemcpy(q, b.f32.p, f32_words() * sizeof(float) * n, cudaMemcpyDeviceToHost));
-    q += f32_words() * sizeof(float) * n;
-    CK(cudaMemcpy(q, b.u32.p, u32_words() * sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
+    const size_t ni = i64_words() * n, nf = f32_words() * n, nu = u32_words() * n;
+    std::vector<int64_t> i64(ni);
+    std::vector<float> f32(nf);
+    std::vector<uint32_t> u32(nu);
+    CK(cudaMemcpy(i64.data(), b.i64.p, ni * sizeof(int64_t), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(f32.data(), b.f32.p, nf * sizeof(float), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(u32.data(), b.u32.p, nu * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    const int md = mode();
+    const bool transient = md == 2 && p.noise_diffusion == 1;
+    uint8_t* q = out + sizeof(h);
+    for (size_t i = 0; i < n; ++i) {
+      PixelStateRec r{};
+      r.t_ref = i64[i];
+      r.t_search = i64[n + i];
+      r.blind_until = i64[2 * n + i];
+      r.s3_ref = f32[i];
+      r.n3_ref = f32[n + i];
+      r.dr_ref = f32[2 * n + i];
+      r.i_scale = f32[3 * n + i];
+      r.held[0] = f32[4 * n + i];
+      r.flags = static_cast<uint16_t>(u32[i]);
+      if (md >= 1) {
+        r.z = f32[5 * n + i];
+        r.x1 = f32[6 * n + i];
+        r.s2 = f32[7 * n + i];
+        r.s3 = f32[8 * n + i];
+        r.tv = f32[9 * n + i];
+      }
+      if (md == 2) {
+        for (int j = 0; j < 3; ++j) {
+          r.nk[j] = f32[(10 + j) * n + i];
+          r.nk1[j] = f32[(13 + j) * n + i];
+        }
+        r.ln_a1 = f32[16 * n + i];
+        r.rho_m1 = transient ? f32[17 * n + i] - 1.0f : 0.0f;
+        r.cell = i64[5 * n + i];
+        r.have_k1 = u32[3 * n + i] != 0u ? 1 : 0;
+      }
+      std::memcpy(q + i * sizeof(PixelStateRec), &r, sizeof(r));
+    }
+    if (noise_section()) {
+      uint8_t* z = q + n * sizeof(PixelStateRec);
+      for (size_t i = 0; i < n; ++i) {
+        const NoiseRecord r{i64[3 * n + i], i64[4 * n + i], u32[n + i], u32[2 * n + i], {0u, 0u}};
+        std::memcpy(z + i * sizeof(NoiseRecord), &r, sizeof(r));
+      }
+    }
   }
 
   void load(const uint8_t* data, size_t bytes) {
     if (bytes != state_bytes()) throw std::invalid_argument("SensorModel.load_state: size does not match this model");
-    Header h;
+    StateHeader h;
     std::memcpy(&h, data, sizeof(h));
-    if (h.magic != kMagic || h.version != 1 || h.bytes_per_pixel != bytes_per_pixel()) {
+    if (h.magic != kStateMagic || (h.version != kStateVersion && h.version != kStateVersionNoHpf) ||
+        h.state_size != sizeof(PixelStateRec)) {
       throw std::invalid_argument("SensorModel.load_state: not a sensor state of this version");
     }
-    if (h.width != width || h.height != height || h.camera != camera || h.seed != seed ||
+    if (h.width != width || h.height != height || h.groups != 1u || h.camera != camera || h.seed != seed ||
         h.fingerprint != fingerprint()) {
       throw std::invalid_argument("SensorModel.load_state: state was saved by a model with other parameters");
     }
-    initialized = false;
+    initialized = false;  // until the upload completes
+    const size_t ni = i64_words() * n, nf = f32_words() * n, nu = u32_words() * n;
+    std::vector<int64_t> i64(ni, 0);
+    std::vector<float> f32(nf, 0.0f);
+    std::vector<uint32_t> u32(nu, 0u);
+    const int md = mode();
     const uint8_t* q = data + sizeof(h);
+    for (size_t i = 0; i < n; ++i) {
+      PixelStateRec r;
+      std::memcpy(&r, q + i * sizeof(PixelStateRec), sizeof(r));
+      i64[i] = r.t_ref;
+      i64[n + i] = r.t_search;
+      i64[2 * n + i] = r.blind_until;
+      i64[3 * n + i] = kForever;  // the noise chains (the noise section below, when on)
+      i64[4 * n + i] = kForever;
+      f32[i] = static_cast<float>(r.s3_ref);
+      f32[n + i] = static_cast<float>(r.n3_ref);
+      f32[2 * n + i] = static_cast<float>(r.dr_ref);
+      f32[3 * n + i] = static_cast<float>(r.i_scale);
+      f32[4 * n + i] = r.held[0];
+      u32[i] = r.flags;
+      if (md >= 1) {
+        f32[5 * n + i] = static_cast<float>(r.z);
+        f32[6 * n + i] = static_cast<float>(r.x1);
+        f32[7 * n + i] = static_cast<float>(r.s2);
+        f32[8 * n + i] = static_cast<float>(r.s3);
+        f32[9 * n + i] = static_cast<float>(r.tv);
+      }
+      if (md == 2) {
+        for (int j = 0; j < 3; ++j) {
+          f32[(10 + j) * n + i] = static_cast<float>(r.nk[j]);
+          f32[(13 + j) * n + i] = static_cast<float>(r.nk1[j]);
+        }
+        f32[16 * n + i] = static_cast<float>(r.ln_a1);
+        f32[17 * n + i] = 1.0f + r.rho_m1;
+        i64[5 * n + i] = r.cell;
+        u32[3 * n + i] = r.have_k1 != 0 ? 1u : 0u;
+      }
+    }
+    if (noise_section()) {
+      const uint8_t* z = q + n * sizeof(PixelStateRec);
+      for (size_t i = 0; i < n; ++i) {
+        NoiseRecord r;
+        std::memcpy(&r, z + i * sizeof(NoiseRecord), sizeof(r));
+        i64[3 * n + i] = r.t_shot;
+        i64[4 * n + i] = r.t_ba;
+        u32[n + i] = r.n_shot;
+        u32[2 * n + i] = r.n_ba;
+      }
+    }
     StateBufs& b = st[cur];
-    CK(cudaMemcpy(b.i64.p, q, i64_words() * sizeof(int64_t) * n, cudaMemcpyHostToDevice));
-    q += i64_words() * sizeof(int64_t) * n;
-    CK(cudaMemcpy(b.f32.p, q, f32_words() * sizeof(float) * n, cudaMemcpyHostToDevice));
-    q += f32_words() * sizeof(float) * n;
-    CK(cudaMemcpy(b.u32.p, q, u32_words() * sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b.i64.p, i64.data(), ni * sizeof(int64_t), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b.f32.p, f32.data(), nf * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b.u32.p, u32.data(), nu * sizeof(uint32_t), cudaMemcpyHostToDevice));
     t_state = h.t_state;
     initialized = h.initialized != 0;
     last_events = 0;
@@ -1946,13 +2079,20 @@ bs_status bs_model_load_state(bs_model* m, const uint8_t* data, size_t n) {
     m->load(data, n);
   });
 }
+bs_status bs_model_set_long_run(bs_model* m, int32_t samples) {
+  return guarded([&] {
+    NEED(m);
+    if (samples < -1) throw std::invalid_argument("long run: -1 (none), 0 (the default) or a sample count");
+    m->long_row = samples == 0 ? 32 : (samples < 0 ? std::numeric_limits<int32_t>::max() : samples);
+  });
+}
 bs_status bs_model_set_block(bs_model* m, int32_t threads) {
   return guarded([&] {
     NEED(m);
     if (threads != 0 && (threads < 32 || threads > 128 || threads % 32 != 0)) {
       throw std::invalid_argument("threads per block must be 32, 64, 96 or 128");
     }
-    m->block = threads == 0 ? 128 : threads;
+    m->block = threads;
   });
 }
 

@@ -13,6 +13,7 @@ event rate at a photocurrent of 100 fA; the rate scales as 1/sqrt(I)), ``noise_b
 from __future__ import annotations
 
 import math
+import struct
 
 NAN = float("nan")
 
@@ -212,6 +213,56 @@ class SensorParams:
 
     def __repr__(self) -> str:
         return f"SensorParams(family={self._v['family']!r}, photoreceptor={self._v['photoreceptor']!r})"
+
+
+# The Value alternative of each row as the reference's row table yields it (config::Value, src/core/config/param.h:44:
+# null, bool, int64, double, string, ...): the family and the enums as their choice names, these rows as int64, the
+# noise switch as bool, every other row as double (limiter_phase_s: null while unset).
+_INT_ROWS = {"clock_offset_ns", "limiter_depth", "noise_leaf_level", "stationary_burnin_ns", "stationary_probe_pixels"}
+_STRING_ROWS = {"family", *ENUMS}
+_OWN_ROWS = ("noise_shot_rate_hz", "noise_ba_median_hz", "noise_ba_sigma_ln")
+_FNV_OFFSET, _FNV_PRIME, _MASK = 0xCBF29CE484222325, 0x100000001B3, (1 << 64) - 1
+
+
+def _fnv(h: int, data: bytes) -> int:
+    for b in data:
+        h = ((h ^ b) * _FNV_PRIME) & _MASK
+    return h
+
+
+def fingerprint(p: SensorParams) -> int:
+    """The reference's 64-bit fingerprint of the parameters and one constant light group (fingerprint,
+    src/sensor/params.cpp:214-263: FNV-1a over every row in row order, each as its Value index (a size_t) and its
+    value's bytes, a string as its length and characters; the high-pass filter's rows only while tau_hp > 0, the
+    limiter's only while it is on; then the waveform's fields, all zero for a constant group). It goes with saved
+    states, which load only into a model of the same fingerprint. This project's own noise rows follow, as doubles,
+    only while one of them is not zero, so that a sensor without them has the reference's fingerprint."""
+    v = p.as_dict()
+    h = _FNV_OFFSET
+    for name in ROW_NAMES:
+        if name in _OWN_ROWS:
+            continue
+        if v["tau_hp"] <= 0 and name in ("tau_hp", "tau_hp_sigma_ln"):
+            continue
+        if v["limiter"] == "off" and name.startswith("limiter"):
+            continue
+        x = v[name]
+        if x is None:
+            h = _fnv(h, struct.pack("<Q", 0))
+        elif name in _STRING_ROWS:
+            b = str(x).encode()
+            h = _fnv(h, struct.pack("<QQ", 4, len(b)) + b)
+        elif name == "noise":
+            h = _fnv(h, struct.pack("<Q?", 1, bool(x)))
+        elif name in _INT_ROWS:
+            h = _fnv(h, struct.pack("<Qq", 2, int(x)))
+        else:
+            h = _fnv(h, struct.pack("<Qd", 3, float(x)))
+    h = _fnv(h, bytes(4 + 4 + 8 + 2 * 8 * 8 + 6 * 8))  # the constant waveform: type, n_harmonics, f0, a/phi, pulse
+    if any(v[name] != 0 for name in _OWN_ROWS):
+        for name in _OWN_ROWS:
+            h = _fnv(h, struct.pack("<Qd", 3, float(v[name])))
+    return h
 
 
 def resolve(params, overrides: dict | None = None) -> SensorParams:

@@ -16,7 +16,7 @@ import threading
 import numpy as np
 
 from . import _lib
-from .params import SensorParams, preset_names, resolve  # noqa: F401  (re-exported: the reference's module API)
+from .params import SensorParams, fingerprint, preset_names, resolve  # noqa: F401  (re-exported: the reference's module API)
 
 cuda_available = _lib.cuda_available
 
@@ -45,6 +45,7 @@ def params_struct(p: SensorParams) -> _lib.Params:
     s.reset_mode = 1 if v["reset_mode"] == "ideal" else 0
     s.initial_phase = {"uniform": 0, "symmetric": 1, "zero": 2}[v["initial_phase"]]
     s.clock_offset_ns = int(v["clock_offset_ns"])
+    s.fingerprint = fingerprint(p)
     return s
 
 
@@ -356,6 +357,12 @@ class SensorModel:
         with self._lock:
             _lib.check(_lib.lib().bs_model_load_state(self._h, b.ctypes.data, len(b)))
 
+    def set_long_run(self, samples: int) -> None:
+        """Threads per pixel of the row-major kernel: runs longer than `samples` are walked by a whole warp (32 lanes,
+        32 samples at a time), the others one per lane (0: the default, 32; -1: every run by one lane)."""
+        _lib.check(_lib.lib().bs_model_set_long_run(self._h, int(samples)))
+
     def set_block(self, threads: int) -> None:
-        """Threads per block of the pixel-model kernel (32..128)."""
+        """Launch policy of the pixel model on runs: 0, the row-major kernel with staged samples (the default for
+        the instantaneous response); 32, 64, 96 or 128, one thread per pixel with that many threads per block."""
         _lib.check(_lib.lib().bs_model_set_block(self._h, int(threads)))

@@ -19,8 +19,20 @@ from . import _lib
 from .sampling import MidpointTest, rules_struct, sampler_for
 
 
+def _stream_handle(stream: int | None) -> int:
+    """The stream every call of a step goes to: the given handle, else torch's current stream (its legacy default
+    stream, handle 0, passed as cudaStreamLegacy: a NULL stream means each library object's own stream, and the
+    sampler's runs must be written on the stream that the pixel model then reads them on)."""
+    if stream:
+        return int(stream)
+    import torch
+
+    return int(torch.cuda.current_stream().cuda_stream) or 1  # 1: cudaStreamLegacy
+
+
 class DeviceWindows:
-    """Sensors (SensorModel, Field) sampled and sensed window by window through the C ABI's device boundary."""
+    """Sensors (SensorModel, Field) sampled and sensed window by window through the C ABI's device boundary, every
+    call of a step on one stream."""
 
     def __init__(self, sensors, *, tol: float = 0.01, dark: float = 0.01, min_dt_ns: int = 8192,
                  max_refine_levels: int = 10, l_min: int = 1, l_max: int = 10):
@@ -55,6 +67,7 @@ class DeviceWindows:
 
         if t0_ns % (1 << 23):
             raise ValueError("DeviceWindows.start: t0 must be a window start")
+        stream = _stream_handle(stream)
         for i, ((m, _), b) in enumerate(zip(self.sensors, self._bufs)):
             b["cur"] = 0
             b["sig"][0].zero_()
@@ -72,6 +85,7 @@ class DeviceWindows:
         next). on_events(i, model, events) sees each call's device events (valid until that model advances again).
         Returns the pixel-samples and events of the call; launch_ms accumulates the sensors' kernel times."""
         L = _lib.lib()
+        stream = _stream_handle(stream)
         samples = events = 0
         total = C.c_size_t()
         runs = _lib.DeviceRuns()

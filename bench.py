@@ -334,9 +334,11 @@ def run_runs(args, rank: int, world: int) -> dict | None:
     r = wl.rules
     models = [SensorModel(resolve(s.preset, s.overrides), s.width, s.height, s.seed, [{"type": "constant"}], s.camera)
               for s in wl.sensors]
-    if args.block:
-        for m in models:
+    for m in models:
+        if args.block:
             m.set_block(args.block)
+        if args.long_run:
+            m.set_long_run(args.long_run)
     dw = DeviceWindows([(m, s.field) for m, s in zip(models, wl.sensors)], tol=r.tol, dark=r.dark,
                        min_dt_ns=r.min_dt_ns, max_refine_levels=r.max_refine_levels, l_min=r.l_min, l_max=r.l_max)
     stream = torch.cuda.current_stream()
@@ -370,6 +372,7 @@ def run_runs(args, rank: int, world: int) -> dict | None:
         if world > 1:
             dist.barrier()
     advance_launches = sum(m.stats()["gpu_launches"] for m in models) - launches0
+    timed_launch_ms = dw.launch_ms
     step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
     total_ms = float(sum(step_ms))
     total_ms_all, samples_all, events_all = reduce_step(total_ms, float(samples), float(events), world)
@@ -401,7 +404,7 @@ def run_runs(args, rank: int, world: int) -> dict | None:
     per_step_samples = samples / args.steps
     per_step_events = events / args.steps
     hbm, hbm_kind = measured_hbm()
-    kms_total = dw.launch_ms / args.steps  # the pixel model's kernels, per step
+    kms_total = timed_launch_ms / args.steps  # the pixel model's kernels, per step
     n_launch = advance_launches / args.steps
     alg = b_sense(wl.pixels, wl.windows, int(per_step_samples), int(per_step_events))
     achieved = alg / (kms_total * 1e-3) / 1e9
@@ -416,7 +419,8 @@ def run_runs(args, rank: int, world: int) -> dict | None:
         "config": {**wl.describe(), "pixel_samples_per_step": int(per_step_samples),
                    "events_per_step": int(per_step_events), "l2": "flushed between steps (256 MiB write)",
                    "path": "sample_window (device) -> runs in HBM -> advance_device, per sensor and window",
-                   "parallelism": f"replicas x{world}", "advance_block": args.block or "default"},
+                   "parallelism": f"replicas x{world}", "advance_block": args.block or "row-major",
+                   "long_run": args.long_run or 32},
         "gpu_launches": 9 * calls * args.steps + 2 * len(wl.sensors) * args.steps,
         "clocks": clocks,
         "e2e": {"value": samples_all / e2e_s if e2e_times else None, "unit": "pixel-samples/s",
@@ -687,6 +691,8 @@ def main():
     ap.add_argument("--cpu-windows", type=int, default=0,
                     help="windows of every sensor in the reference's bounded sample (0: the workload's default)")
     ap.add_argument("--block", type=int, default=0, help="runs_* workloads: threads per block of advance_runs")
+    ap.add_argument("--long-run", type=int, default=0,
+                    help="runs_* workloads: runs longer than this are walked by a whole warp (-1: none)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--warps", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)

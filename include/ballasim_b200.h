@@ -61,6 +61,11 @@ typedef struct {
   int32_t noise_leaf_level, noise_diffusion;
   int32_t initial_state, stationary_probe_pixels;
   int64_t stationary_burnin_ns;
+  /* The parameter set's fingerprint as the reference computes it (fingerprint(params, light groups),
+   * src/sensor/params.cpp:246, over every SensorParams row), written into saved states and required of a state to
+   * load (the reference's own refusal); this library does not see every row, so the caller's parameter layer passes
+   * it (the Python shim restates the reference's function). */
+  uint64_t fingerprint;
 } bs_params;
 
 /* Event columns of the caller's arrays (count entries each; any pointer may be NULL to skip a column), sorted by
@@ -161,13 +166,24 @@ bs_status bs_model_set_photometry(bs_model* m, double illuminance_scale, const f
 bs_status bs_model_gain_map(const bs_model* m, float* out);
 /* time_ns, irr_max, initialized (sensor_model.h:212-236). */
 bs_status bs_model_info(const bs_model* m, int64_t* time_ns, float* irr_max, int32_t* initialized);
-/* save_state / load_state / state_bytes (sensor_model.h:175-178): this build's own blob (magic, version, shape,
- * seed, a parameter fingerprint, the model time, the per-pixel state). */
+/* save_state / load_state / state_bytes (sensor_model.h:175-178) in the reference's format
+ * (src/sensor/sensor_model.cpp:1198-1262): its 56-byte StateHeader (magic "BSNS", version 6, shape, groups, camera,
+ * seed, the state fingerprint: the parameters' fingerprint, continued over the gain map when some gain is not 1, the
+ * model time, initialized, 200), then one 200-byte PixelState (src/sensor/pixel.h:105-121) per pixel. A state saved
+ * by the reference's SensorModel loads here and the reverse, and each refuses a state of another shape, seed, camera
+ * or fingerprint. With this project's shot and background-activity noise on, 32 bytes per pixel follow (the noise
+ * chains' next candidate times and counts). */
 bs_status bs_model_state_bytes(const bs_model* m, size_t* n);
 bs_status bs_model_save_state(const bs_model* m, uint8_t* out, size_t n);
 bs_status bs_model_load_state(bs_model* m, const uint8_t* data, size_t n);
-/* Launch policy: threads per block of the pixel-model kernel (0: the default). */
+/* Launch policy of the pixel model on CSR runs. 0 (the default): the instantaneous response runs row-major, one warp
+ * per 32 runs with the runs' samples staged in shared memory (the cascade runs one thread per pixel, 128 per block);
+ * 32, 64, 96 or 128: one thread per pixel with that many threads per block, for every photoreceptor. */
 bs_status bs_model_set_block(bs_model* m, int32_t threads);
+/* The row-major kernel's threads per pixel: runs longer than `samples` are walked by all 32 lanes of a warp, 32
+ * consecutive samples at a time (their logs and exclusion tests in parallel, a ballot finding the first segment that
+ * can fire), the others by one lane each (0: the default, 32; -1: every run by one lane). */
+bs_status bs_model_set_long_run(bs_model* m, int32_t samples);
 
 /* ---- the window sampler: sample_window (src/engine/bindings/engine_module.cpp:311-355), MidpointTest ---- */
 

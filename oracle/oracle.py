@@ -382,6 +382,12 @@ class Ref:
             L.ref_model_create_prec.argtypes = [C.c_char_p, C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.c_int,
                                                 C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, C.c_int, C.c_int]
             L.ref_model_destroy.argtypes = [C.c_void_p]
+            L.ref_fingerprint.restype = C.c_uint64
+            L.ref_fingerprint.argtypes = [C.c_char_p, C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.c_int]
+            L.ref_model_state_bytes.restype = C.c_size_t
+            L.ref_model_state_bytes.argtypes = [C.c_void_p]
+            L.ref_model_save_state.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+            L.ref_model_load_state.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
             L.ref_model_init.argtypes = [C.c_void_p, C.c_int64, _f32p]
             L.ref_model_advance_runs.argtypes = [C.c_void_p, _u32p, C.c_size_t, _i64p, _f32p, C.c_size_t, _i64p,
                                                  _i32p, C.c_int64]
@@ -556,6 +562,17 @@ class Ref:
                 return t[:k], irr[:k * groups].reshape(k, groups), off, ci, cs, stats
             cap = -k
 
+    @classmethod
+    def fingerprint(cls, family: str, overrides: dict) -> int:
+        """The reference's fingerprint of preset(family) with numeric overrides (harness field names)."""
+        keys = list(overrides)
+        ck = (C.c_char_p * max(1, len(keys)))(*[k.encode() for k in keys])
+        cv = (C.c_double * max(1, len(keys)))(*[float(overrides[k]) for k in keys])
+        h = cls.lib().ref_fingerprint(family.encode(), ck, cv, len(keys))
+        if h == 0:
+            raise ValueError(cls.lib().ref_last_error().decode())
+        return int(h)
+
     class Model:
         # Overrides the harness understands (the SensorParams rows this path reads), from a resolved SensorParams.
         KEYS = ("theta_on", "theta_off", "sigma_theta_on", "sigma_theta_off", "theta_onoff_corr", "theta_floor",
@@ -588,6 +605,18 @@ class Ref:
             if getattr(self, "h", None):
                 self.L.ref_model_destroy(self.h)
                 self.h = None
+
+        def save_state(self) -> bytes:
+            n = self.L.ref_model_state_bytes(self.h)
+            buf = np.zeros(n, np.uint8)
+            if self.L.ref_model_save_state(self.h, buf.ctypes.data, n) != 0:
+                raise ValueError(self.L.ref_last_error().decode())
+            return buf.tobytes()
+
+        def load_state(self, blob: bytes) -> None:
+            b = np.frombuffer(blob, np.uint8)
+            if self.L.ref_model_load_state(self.h, b.ctypes.data, len(b)) != 0:
+                raise ValueError(self.L.ref_last_error().decode())
 
         @property
         def threads(self) -> int:

@@ -78,6 +78,13 @@ void set_field(sensor::SensorParams& p, const std::string& key, double v) {
     p.initial_state = v == 0.0 ? sensor::InitialState::kPhase : sensor::InitialState::kStationary;
   } else if (key == "stationary_burnin_ns") p.stationary_burnin_ns = static_cast<int64_t>(v);
   else if (key == "stationary_probe_pixels") p.stationary_probe_pixels = static_cast<int32_t>(v);
+  else if (key == "leak_ea_eV") p.leak_ea_eV = v;
+  else if (key == "dark_ea_eV") p.dark_ea_eV = v;
+  else if (key == "reference_temperature_K") p.reference_temperature_K = v;
+  else if (key == "clock_offset_ns") p.clock_offset_ns = static_cast<int64_t>(v);
+  else if (key == "clock_drift_ppm") p.clock_drift_ppm = v;
+  else if (key == "hot_fraction") p.hot_fraction = v;
+  else if (key == "veiling_glare") p.veiling_glare = v;
   else throw std::invalid_argument("ref harness: unknown field " + key);
 }
 
@@ -153,6 +160,40 @@ void* ref_model_create(const char* preset, const char* const* keys, const double
 }
 
 void ref_model_destroy(void* h) { delete static_cast<RefModel*>(h); }
+
+// The reference's parameter fingerprint (fingerprint, src/sensor/params.cpp:246) of a preset with overrides and one
+// constant light group; 0 with the message in ref_last_error on a refused parameter set.
+uint64_t ref_fingerprint(const char* preset, const char* const* keys, const double* values, int n_over) {
+  try {
+    sensor::SensorParams p = sensor::preset(preset);
+    for (int i = 0; i < n_over; ++i) set_field(p, keys[i], values[i]);
+    return sensor::fingerprint(p, std::vector<sensor::Waveform>{sensor::make_constant_waveform()});
+  } catch (const std::exception& e) {
+    fail(e);
+    return 0;
+  }
+}
+
+// SensorModel::state_bytes / save_state / load_state (src/sensor/sensor_model.cpp:1198-1262).
+size_t ref_model_state_bytes(void* h) { return static_cast<RefModel*>(h)->model->state_bytes(); }
+int ref_model_save_state(void* h, uint8_t* out, size_t n) {
+  try {
+    const std::vector<uint8_t> b = static_cast<RefModel*>(h)->model->save_state();
+    if (b.size() != n) throw std::invalid_argument("ref harness: state buffer size");
+    std::memcpy(out, b.data(), n);
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+int ref_model_load_state(void* h, const uint8_t* data, size_t n) {
+  try {
+    static_cast<RefModel*>(h)->model->load_state(data, n);
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
 
 int ref_model_init(void* h, int64_t t0, const float* irr0) {
   try {

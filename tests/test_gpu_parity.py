@@ -25,6 +25,7 @@ def same_events(dev: dict, ora: dict, width: int) -> None:
         assert np.array_equal(a, b), f"column {k} differs"
 
 
+@pytest.mark.parametrize("block", [0, 128])
 @pytest.mark.parametrize("overrides", [
     {},
     dict(W.MISMATCH),
@@ -32,7 +33,9 @@ def same_events(dev: dict, ora: dict, width: int) -> None:
     {"reset_mode": "physical", "refractory_s": 0.0, "eps_ci": 0.002, "initial_phase": "symmetric"},
     {**W.MISMATCH, **W.NOISE, "noise_shot_rate_hz": 50.0, "noise_ba_median_hz": 20.0},
 ])
-def test_pixel_model_on_random_runs(cuda_lib, oracle_port, overrides):
+def test_pixel_model_on_random_runs(cuda_lib, oracle_port, overrides, block):
+    """The pixel model on random ragged runs (random pixel subsets in random order) against the oracle: the
+    row-major kernel with staged samples (block 0) and the one-thread-per-pixel kernel (block 128)."""
     from ballasim_b200.sensor import SensorModel
 
     rng = np.random.default_rng(17 + len(overrides))
@@ -40,6 +43,7 @@ def test_pixel_model_on_random_runs(cuda_lib, oracle_port, overrides):
     n = Wd * Hd
     p = resolve("ideal", overrides)
     dev = SensorModel(p, Wd, Hd, 5, [{"type": "constant"}], 0)
+    dev.set_block(block)
     ora = oracle_port.Model(p, Wd, Hd, 5, 0)
     irr0 = rng.uniform(20, 200, n).astype(np.float32)
     dev.init(0, irr0.reshape(n, 1))
@@ -52,6 +56,69 @@ def test_pixel_model_on_random_runs(cuda_lib, oracle_port, overrides):
     same_events(merged, ora.take_events(), Wd)
     assert len(merged["t_cross_ns"]) > 10
     assert dev.time_ns == t_end
+
+
+@pytest.mark.parametrize("long_run", [0, 1, 5, -1])
+@pytest.mark.parametrize("layout", ["tiled", "long", "shuffled", "gaps", "sparse"])
+def test_row_major_kernel_on_every_run_layout(cuda_lib, oracle_port, layout, long_run):
+    """The row-major kernel against the oracle on every run layout (runs in pixel order tiling the sample arrays,
+    runs of hundreds to thousands of samples, runs whose starts are shuffled or leave gaps, a sparse listing whose
+    other pixels advance on their held sample) and split between its two walks: runs longer than long_run walked by
+    the whole warp (1: every run of two or more samples; 0: the default 32; -1: none)."""
+    from ballasim_b200.sensor import SensorModel
+
+    rng = np.random.default_rng({"tiled": 1, "long": 2, "shuffled": 3, "gaps": 4, "sparse": 5}[layout])
+    Wd, Hd = 40, 24
+    n = Wd * Hd
+    p = resolve("ideal", {**W.MISMATCH, **W.NOISE, "noise_shot_rate_hz": 20.0, "noise_ba_median_hz": 10.0,
+                          "leak_rate_hz": 1.0})
+    dev = SensorModel(p, Wd, Hd, 6, [{"type": "constant"}], 0)
+    dev.set_long_run(long_run)
+    ora = oracle_port.Model(p, Wd, Hd, 6, 0)
+    irr0 = rng.uniform(20, 300, n).astype(np.float32)
+    dev.init(0, irr0.reshape(n, 1))
+    ora.init(0, irr0)
+    got, t = [], 0
+    for call in range(4):
+        t_end = t + (1 << 23)
+        ids = np.arange(n, dtype=np.uint32)
+        if layout == "sparse":
+            ids = np.sort(rng.permutation(n)[: n // 7]).astype(np.uint32)
+        hi = 2000 if layout == "long" else 14
+        cnt = rng.integers(0, hi, len(ids)).astype(np.int32)
+        cnt[rng.random(len(ids)) < 0.2] = 0
+        runs = []
+        for k in cnt:
+            times = np.unique(rng.integers(t + 1, t_end + 1, int(k)))
+            if rng.random() < 0.3 and len(times):
+                times[0] = t
+                times = np.unique(times)
+            runs.append(times.astype(np.int64))
+        cnt = np.array([len(r) for r in runs], np.int32)
+        vals = [(100 * np.exp(np.cumsum(rng.normal(0, 0.05, len(r))))).astype(np.float32) for r in runs]
+        order = np.arange(len(ids))
+        if layout == "shuffled":
+            order = rng.permutation(len(ids))
+        pad = 3 if layout == "gaps" else 0
+        starts = np.zeros(len(ids), np.int64)
+        tt, vv, pos = [], [], 0
+        for i in order:
+            starts[i] = pos
+            tt.append(runs[i])
+            vv.append(vals[i])
+            pos += len(runs[i])
+            if pad:
+                tt.append(np.zeros(pad, np.int64))
+                vv.append(np.zeros(pad, np.float32))
+                pos += pad
+        tt = np.concatenate(tt) if tt else np.zeros(0, np.int64)
+        vv = np.concatenate(vv) if vv else np.zeros(0, np.float32)
+        got.append(dev.advance_runs(ids, tt, vv, t_end, starts, cnt))
+        ora.advance_runs(ids, tt, vv, starts, cnt, t_end)
+        t = t_end
+    merged = {k: np.concatenate([g[k] for g in got]) for k in got[0]}
+    same_events(merged, ora.take_events(), Wd)
+    assert len(merged["t_cross_ns"]) > 50
 
 
 def test_advance_rectangular_and_ragged_forms_agree(cuda_lib):
@@ -154,6 +221,68 @@ def test_save_and_load_state_resume_bitwise(cuda_lib, family, overrides):
     other = SensorModel(family, 10, 10, 5, [{"type": "constant"}], 0, overrides=overrides)
     with pytest.raises(ValueError):
         other.load_state(blob)
+
+
+STATE_CASES = [
+    ("ideal", dict(W.MISMATCH)),
+    ("ideal", {**W.MISMATCH, "leak_rate_hz": 2.0, "leak_sigma_log10": 0.1, "reset_mode": "ideal"}),
+    ("prophesee_gen3", {"noise": False}),
+    ("prophesee_gen3", {"noise": True}),
+    ("prophesee_gen3", {"noise": True, "noise_diffusion": "transient", "leak_rate_hz": 2.0}),
+]
+
+
+@pytest.mark.parametrize("family,overrides", STATE_CASES)
+def test_states_move_between_the_reference_and_this_model(cuda_lib, ref, family, overrides):
+    """save_state / load_state in the reference's format (src/sensor/sensor_model.cpp:1198-1262): a state the reference
+    saves after two calls resumes here, and one saved here resumes in the reference, each giving the events of an
+    uninterrupted reference run over the last two calls, bit for bit; the headers are equal, and a model of another
+    seed refuses either state."""
+    from ballasim_b200.sensor import SensorModel
+
+    p = resolve(family, overrides)
+    Wd, Hd, seed = 20, 16, 13
+    n = Wd * Hd
+    rng = np.random.default_rng(21)
+    irr0 = rng.uniform(10, 300, n).astype(np.float32)
+    calls = random_calls(rng, n, 0, 4)
+    full = ref.Model(p, Wd, Hd, seed, 0)
+    full.init(0, irr0)
+    for c in calls[:2]:
+        full.advance_runs(c[0], c[1], c[2], c[4], c[5], c[3])
+    full.take_events()
+    blob_ref = full.save_state()
+    for c in calls[2:]:
+        full.advance_runs(c[0], c[1], c[2], c[4], c[5], c[3])
+    want = full.take_events()
+    assert len(want["t_cross_ns"]) > 20
+
+    # reference -> here
+    dev = SensorModel(p, Wd, Hd, seed, [{"type": "constant"}], 0)
+    assert dev.state_bytes() == len(blob_ref)
+    dev.load_state(blob_ref)
+    got = [dev.advance_runs(c[0], c[1], c[2], c[3], c[4], c[5]) for c in calls[2:]]
+    same_events({k: np.concatenate([g[k] for g in got]) for k in got[0]}, want, Wd)
+
+    # here -> reference
+    mine = SensorModel(p, Wd, Hd, seed, [{"type": "constant"}], 0)
+    mine.init(0, irr0.reshape(n, 1))
+    for c in calls[:2]:
+        mine.advance_runs(c[0], c[1], c[2], c[3], c[4], c[5])
+    blob_mine = mine.save_state()
+    assert blob_mine[:56] == blob_ref[:56]  # the StateHeader: magic, version, shape, seed, fingerprint, time
+    back = ref.Model(p, Wd, Hd, seed, 0)
+    back.load_state(blob_mine)
+    for c in calls[2:]:
+        back.advance_runs(c[0], c[1], c[2], c[4], c[5], c[3])
+    same_events(back.take_events(), want, Wd)
+
+    other = SensorModel(p, Wd, Hd, seed + 1, [{"type": "constant"}], 0)
+    with pytest.raises(ValueError):
+        other.load_state(blob_ref)
+    other_ref = ref.Model(p, Wd, Hd, seed + 1, 0)
+    with pytest.raises(ValueError):
+        other_ref.load_state(blob_mine)
 
 
 @pytest.mark.parametrize("family,overrides,calls,t0", [

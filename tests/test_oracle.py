@@ -165,3 +165,27 @@ def test_port_refuses_what_the_reference_refuses(oracle_port, ref):
         for b in bad:
             with pytest.raises(ValueError):
                 m.advance_runs(*b)
+
+
+@pytest.mark.parametrize("family,overrides", [
+    ("ideal", {}), ("ideal", {"theta_on": 0.25, "sigma_theta_on": 0.03}), ("prophesee_gen3", {}),
+    ("samsung_gen3", {}), ("prophesee_gen3", {"noise": 0.0}), ("ideal", {"reset_mode": 0.0, "refractory_s": 1e-4}),
+    ("prophesee_gen3", {"noise_diffusion": 1.0, "initial_state": 1.0, "stationary_burnin_ns": 3e8}),
+    ("ideal", {"clock_offset_ns": 12345, "initial_phase": 1.0, "leak_rate_hz": 0.1, "leak_sigma_log10": 0.0}),
+    ("prophesee_gen3", {"noise_leaf_level": 3, "noise_margin_z": 5.0, "eps_L": 0.001, "hot_fraction": 0.0}),
+    ("samsung_gen3", {"photoreceptor": 1.0, "noise": 0.0, "dark_current_fA": 0.5, "temperature_K": 310.0}),
+])
+def test_parameter_fingerprint_equals_the_reference(ref, family, overrides):
+    """params.fingerprint restates the reference's fingerprint (src/sensor/params.cpp:246) bit for bit: saved states
+    carry it and a state loads only where it matches."""
+    from ballasim_b200.params import fingerprint
+
+    enums = {"reset_mode": ("physical", "ideal"), "initial_phase": ("uniform", "symmetric", "zero"),
+             "noise_diffusion": ("frozen", "transient"), "initial_state": ("phase", "stationary"),
+             "photoreceptor": ("cascade", "instantaneous")}
+    ints = {"clock_offset_ns", "noise_leaf_level", "stationary_burnin_ns"}
+    ours = {k: enums[k][int(v)] if k in enums else bool(v) if k == "noise" else int(v) if k in ints else v
+            for k, v in overrides.items()}
+    assert fingerprint(resolve(family, ours)) == ref.fingerprint(family, overrides)
+    # this project's own noise rows change it only when set
+    assert fingerprint(resolve(family, {**ours, "noise_shot_rate_hz": 0.5})) != fingerprint(resolve(family, ours))
