@@ -12,7 +12,7 @@ import numpy as np
 
 LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libballasim_b200.so"
 
-BS_OK, BS_EINVAL, BS_ELOGIC, BS_ENOMEM, BS_ECUDA, BS_EREFUSED, BS_EIO = 0, 1, 2, 3, 4, 5, 6
+BS_OK, BS_EINVAL, BS_ELOGIC, BS_ENOMEM, BS_ECUDA, BS_EREFUSED, BS_EIO, BS_ECANCELLED = 0, 1, 2, 3, 4, 5, 6, 7
 
 
 class FileInfo(C.Structure):
@@ -24,6 +24,10 @@ class FileInfo(C.Structure):
 class ExportError(ValueError):
     """An export refused its input or options; the message names the reason (the reference's
     ballasim.export.errors.ExportError, raised for the writers' Refused)."""
+
+
+class Cancelled(Exception):
+    """A window stopped by its CancelToken (the reference's _engine.Cancelled, src/engine/cancel.h:28-30)."""
 
 
 class MemoryBudgetError(MemoryError):
@@ -67,6 +71,21 @@ class DeviceRuns(C.Structure):
 
 class DeviceEvents(C.Structure):
     _fields_ = [("data", C.c_void_p), ("count", C.c_size_t)]
+
+
+class SampleRequest(C.Structure):
+    _fields_ = [("cam", C.c_uint16), ("flags", C.c_uint16), ("pixel", C.c_uint32), ("k_begin", C.c_uint32),
+                ("k_count", C.c_uint32), ("t_off_ns", C.c_int32), ("pose_slot", C.c_uint32)]
+
+
+RENDER_FN = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.POINTER(SampleRequest), C.c_size_t, C.POINTER(C.c_uint32),
+                        C.POINTER(C.c_float), C.POINTER(C.c_uint64), C.c_uint32)
+
+
+class WindowRules(C.Structure):
+    _fields_ = [("tol", C.c_float), ("dark", C.c_float), ("midpoint", C.c_int32), ("refine_signature", C.c_int32),
+                ("max_refine_levels", C.c_int32), ("min_dt_ns", C.c_int64), ("cam", C.c_uint16),
+                ("subsamples", C.c_uint32), ("cancel", C.c_void_p)]
 
 
 class Field(C.Structure):
@@ -124,6 +143,7 @@ _SIGS = {
     "bs_model_load_state": (C.c_int32, [_P, _P, C.c_size_t]),
     "bs_model_set_block": (C.c_int32, [_P, C.c_int32]),
     "bs_model_set_long_run": (C.c_int32, [_P, C.c_int32]),
+    "bs_model_take_timing": (C.c_int32, [_P, _P]),
     "bs_sampler_create": (C.c_int32, [C.POINTER(Field), C.POINTER(_P)]),
     "bs_sampler_destroy": (C.c_int32, [_P]),
     "bs_sample_window": (C.c_int32, [_P, C.c_int64, _P, _P, C.c_size_t, _P, _P, C.POINTER(SampleRules),
@@ -133,6 +153,12 @@ _SIGS = {
                                             C.POINTER(SampleRules), _P, _P, _P, C.c_size_t, _P, _P, _P,
                                             C.POINTER(C.c_size_t)]),
     "bs_sampler_device_runs": (C.c_int32, [_P, C.POINTER(DeviceRuns)]),
+    "bs_window_create": (C.c_int32, [C.c_int32, _P, _P, C.POINTER(_P)]),
+    "bs_window_destroy": (C.c_int32, [_P]),
+    "bs_window_run": (C.c_int32, [_P, C.c_int64, _P, _P, C.c_size_t, _P, _P, C.POINTER(WindowRules), RENDER_FN, _P,
+                                  C.POINTER(C.c_size_t)]),
+    "bs_window_runs": (C.c_int32, [_P, _P, _P, _P]),
+    "bs_window_stats": (C.c_int32, [_P, _P, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
     "bs_sample_window_device": (C.c_int32, [_P, C.c_int64, _P, _P, C.c_size_t, _P, _P, _P, _P,
                                             C.POINTER(SampleRules), _P, C.POINTER(C.c_size_t)]),
     "bs_field_levels_device": (C.c_int32, [_P, C.c_int64, C.c_int32, C.c_int32, _P, _P]),
@@ -204,6 +230,8 @@ def check(status: int) -> None:
         raise ExportError(msg)
     if status == BS_EIO:
         raise OSError(msg)
+    if status == BS_ECANCELLED:
+        raise Cancelled(msg)
     raise RuntimeError(msg)
 
 

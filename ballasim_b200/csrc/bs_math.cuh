@@ -13,12 +13,16 @@
 
 // BS_HD: shared host/device code, inlined where the compiler finds it worth it. BS_COLD: a rare path kept out of
 // line on the device, one copy per kernel, so that the hot loops' code stays small enough for the instruction cache.
+// BS_HOT: a small function of the per-sample path, always inlined: a call would need the caller's pixel state in
+// memory (a PixelProc holds references to it), which on the device means local memory on every access.
 #if defined(__CUDACC__)
 #define BS_HD __host__ __device__ inline
+#define BS_HOT __host__ __device__ __forceinline__
 #define BS_D __device__ __forceinline__
 #define BS_COLD __host__ __device__ __noinline__
 #else
 #define BS_HD inline
+#define BS_HOT inline
 #define BS_D inline
 #define BS_COLD
 #endif
@@ -90,17 +94,17 @@ BS_HD double rint_d(double x) {
 BS_HD float fabs_f(float x) { return u2f(f2u(x) & 0x7fffffffu); }
 
 // min / max with the reference's operand order (a NaN operand is not propagated symmetrically).
-BS_HD float minr(float a, float b) { return b < a ? b : a; }
-BS_HD float maxr(float a, float b) { return a < b ? b : a; }
-BS_HD int64_t mini(int64_t a, int64_t b) { return b < a ? b : a; }
-BS_HD int64_t maxi(int64_t a, int64_t b) { return a < b ? b : a; }
+BS_HOT float minr(float a, float b) { return b < a ? b : a; }
+BS_HOT float maxr(float a, float b) { return a < b ? b : a; }
+BS_HOT int64_t mini(int64_t a, int64_t b) { return b < a ? b : a; }
+BS_HOT int64_t maxi(int64_t a, int64_t b) { return a < b ? b : a; }
 
 constexpr float kInfF = __builtin_huge_valf();
 
 // ---------------------------------------------------------------------------------------------
 // fp32 natural logarithm
 // ---------------------------------------------------------------------------------------------
-BS_HD float log_f(float x) {
+BS_HOT float log_f(float x) {
   if (!(x > 0.0f)) return x == 0.0f ? -kInfF : u2f(0x7fc00000u);
   if (x == kInfF) return x;
   int bias = 0;
@@ -130,7 +134,7 @@ BS_HD float log_f(float x) {
 
 // fp32 e^x for the analytic fields: k = rint(x log2 e), Cody-Waite r, degree-7 Taylor, exact scaling by 2^k;
 // 0 below -87.33 (no subnormal results).
-BS_HD float exp_f(float x) {
+BS_HOT float exp_f(float x) {
   if (!(x >= -87.33f)) return x != x ? x : 0.0f;
   if (x > 88.72f) return kInfF;
   const float k = rint_f(x * 0x1.715476p+0f);

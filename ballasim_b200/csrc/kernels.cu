@@ -329,6 +329,7 @@ struct RowsArgs {
   uint32_t* listed;
   EventBuf ev;
   unsigned long long* counters;
+  const SensorConsts* kd;  // a device copy of k, for the cold calls (a kernel parameter's address is not taken)
 };
 
 // Marks the warp's pixels listed; returns kErrDuplicate if some pixel was listed before (in this warp or another).
@@ -392,26 +393,80 @@ __device__ __forceinline__ PixelMapRegs shfl_map(const PixelMapRegs& m, int src)
 // Would PixelProc::segment_fast pass segment [t0, e) with nothing but its clean effects (the piece counted, the
 // search moved to e, a node counted when e - t0 > 2)? Only where it takes that branch: one 2^23 ns piece, the pixel
 // not blind, its search armed at or before t0, no noise candidate before e, Delta(t0) below both levels, and the
-// node (t0, e - 1] a single integer or excluded.
-template <class Sink>
-__device__ __forceinline__ bool clean_segment(const PixelProc<Sink>& proc, int64_t t0, int64_t e, float v0, float v1,
-                                              float x0, float x1) {
-  const PixelRegs& s = proc.s;
+// node (t0, e - 1] a single integer or excluded. Inline code on the caller's registers.
+__device__ __forceinline__ bool clean_segment(const PixelRegs& s, const PixelMapRegs& m, const SensorConsts& k,
+                                              int64_t t0, int64_t e, float v0, float v1, float x0, float x1) {
   if (((e - 1) >> kWindowLog2) != (t0 >> kWindowLog2)) return false;
   if (s.blind_until != kNotBlind || s.t_search > t0) return false;
-  const int64_t tn = proc.k.noise ? mini(s.t_shot, s.t_ba) : kForever;
+  const int64_t tn = k.noise ? mini(s.t_shot, s.t_ba) : kForever;
   if (tn < e) return false;
-  const float D0 = proc.delta(t0, x0);
-  if (D0 >= proc.m.theta_on || D0 <= -proc.m.theta_off) return false;
+  NullSink ns;
+  PixelCounters nc;
+  const PixelProc<NullSink> hp{const_cast<PixelRegs&>(s), m, k, 0u, ns, nc};
+  const float D0 = hp.delta(t0, x0);
+  if (D0 >= m.theta_on || D0 <= -m.theta_off) return false;
   if (e - t0 == 1) return true;
-  return proc.excluded(Segment{t0, e, v0, v1}, t0, e, x0, x1);
+  return hp.excluded(Segment{t0, e, v0, v1}, t0, e, x0, x1);
 }
 
-// The warp-cooperative walk of one run (cnt samples at tp / vp) by a PixelProc whose state every lane holds alike.
+// x = ln(I / i_scale) at a sample of value v (PixelProc::x_at_sample on the caller's registers).
+__device__ __forceinline__ float x_sample(const PixelRegs& s, const PixelMapRegs& m, float v) {
+  return log_f((m.dark + m.scale * v) / s.i_scale);
+}
+
+// The pixel model's full path on a state in memory, out of line: the hot loops keep the state in registers and copy
+// it here only for a segment that is not clean. fast: PixelProc::segment_fast with x at both ends; else
+// PixelProc::segment over [from, to).
+template <class Sink>
+__device__ __noinline__ void cold_segment(PixelRegs* s, const PixelMapRegs* m, const SensorConsts* k, uint32_t pixel,
+                                          Sink sink, PixelCounters* c, Segment g, int64_t from, int64_t to, bool fast,
+                                          float x0, float x1) {
+  PixelProc<Sink> proc{*s, *m, *k, pixel, sink, *c};
+  if (fast) proc.segment_fast(g, x0, x1);
+  else proc.segment(g, from, to);
+}
+
+// One segment [t0, t1) of a pixel whose state is in registers: the clean outcome in place, anything else out of line.
+template <class Sink>
+__device__ __forceinline__ void feed_segment(PixelRegs& s, const PixelMapRegs& m, const SensorConsts& k,
+                                             const SensorConsts* kd, uint32_t pixel, const Sink& sink,
+                                             PixelCounters& c, int64_t t0, int64_t t1, float v0, float v1, float x0,
+                                             float x1) {
+  if (clean_segment(s, m, k, t0, t1, v0, v1, x0, x1)) {
+    ++c.pieces;
+    if (t1 - t0 > 2) ++c.leaves;
+    s.t_search = maxi(s.t_search, t1);
+    return;
+  }
+  PixelRegs ts = s;
+  PixelMapRegs tm = m;
+  PixelCounters tc = c;
+  const bool fast = ((t1 - 1) >> kWindowLog2) == (t0 >> kWindowLog2);
+  cold_segment(&ts, &tm, kd, pixel, sink, &tc, Segment{t0, t1, v0, v1}, t0, t1, fast, x0, x1);
+  s = ts;
+  c = tc;
+}
+
+// The held sample from t_from to t_end (the end of a call), out of line where there is such a stretch.
+template <class Sink>
+__device__ __forceinline__ void feed_held(PixelRegs& s, const PixelMapRegs& m, const SensorConsts* kd, uint32_t pixel,
+                                          const Sink& sink, PixelCounters& c, int64_t t_from, float v,
+                                          int64_t t_end) {
+  if (t_from >= t_end) return;
+  PixelRegs ts = s;
+  PixelMapRegs tm = m;
+  PixelCounters tc = c;
+  cold_segment(&ts, &tm, kd, pixel, sink, &tc, Segment{t_from, kForever, v, v}, t_from, t_end, false, 0.0f, 0.0f);
+  s = ts;
+  c = tc;
+}
+
+// The warp-cooperative walk of one run (cnt samples at tp / vp) of a pixel whose state u every lane holds alike.
 // prev_t / prev_v / x_prev: the last sample fed (at entry the held one at the model time, x_prev its x), updated.
 // Stops at the first sample out of order or after t_end (the call is refused then).
-__device__ __forceinline__ void coop_run(PixelProc<LaneZeroSink>& proc, const int64_t* tp, const float* vp,
-                                         int32_t cnt, const RowsArgs& a, uint32_t lane, int64_t& prev_t,
+__device__ __forceinline__ void coop_run(PixelRegs& u, const PixelMapRegs& um, const RowsArgs& a, uint32_t pixel,
+                                         const LaneZeroSink& lz, PixelCounters& cu, const int64_t* tp,
+                                         const float* vp, int32_t cnt, uint32_t lane, int64_t& prev_t,
                                          float& prev_v, float& x_prev, unsigned long long& err,
                                          unsigned long long& clamps) {
   const unsigned full = 0xffffffffu;
@@ -423,7 +478,7 @@ __device__ __forceinline__ void coop_run(PixelProc<LaneZeroSink>& proc, const in
     if (in && !isfinite(raw)) err |= kErrNonFinite;
     const float vi = clamp_irr(raw, a.k.irr_max);
     if (in && !(vi == raw)) ++clamps;
-    const float xi = in ? proc.x_at_sample(vi) : 0.0f;
+    const float xi = in ? x_sample(u, um, vi) : 0.0f;
     int64_t tq = __shfl_up_sync(full, ti, 1);
     float vq = __shfl_up_sync(full, vi, 1), xq = __shfl_up_sync(full, xi, 1);
     if (lane == 0u) {
@@ -444,25 +499,27 @@ __device__ __forceinline__ void coop_run(PixelProc<LaneZeroSink>& proc, const in
     const unsigned upto = limit == 32 ? full : ((1u << limit) - 1u);
     while (j < limit) {
       const bool mine = static_cast<int32_t>(lane) >= j && static_cast<int32_t>(lane) < limit;
-      const bool clean = !mine || clean_segment(proc, tq, ti, vq, vi, xq, xi);
+      const bool clean = !mine || clean_segment(u, um, a.k, tq, ti, vq, vi, xq, xi);
       const unsigned range = upto & ~((1u << j) - 1u);
       const unsigned dirty = __ballot_sync(full, !clean) & range;
       const int32_t f = dirty ? __ffs(dirty) - 1 : limit;
       if (f > j) {  // segments j .. f - 1 are clean: their effects at once
         const unsigned cm = range & (f == 32 ? full : ((1u << f) - 1u));
-        proc.c.pieces += static_cast<uint32_t>(__popc(cm));
-        proc.c.leaves += static_cast<uint32_t>(__popc(__ballot_sync(full, ti - tq > 2) & cm));
-        proc.s.t_search = maxi(proc.s.t_search, __shfl_sync(full, ti, f - 1));
+        cu.pieces += static_cast<uint32_t>(__popc(cm));
+        cu.leaves += static_cast<uint32_t>(__popc(__ballot_sync(full, ti - tq > 2) & cm));
+        u.t_search = maxi(u.t_search, __shfl_sync(full, ti, f - 1));
       }
       if (f < limit) {  // segment f through the pixel model, the same on every lane
         const int64_t t0 = __shfl_sync(full, tq, f), e = __shfl_sync(full, ti, f);
         const float v0 = __shfl_sync(full, vq, f), v1 = __shfl_sync(full, vi, f);
         const float x0 = __shfl_sync(full, xq, f), x1 = __shfl_sync(full, xi, f);
-        if (((e - 1) >> kWindowLog2) == (t0 >> kWindowLog2)) {
-          proc.segment_fast(Segment{t0, e, v0, v1}, x0, x1);
-        } else {
-          proc.segment(Segment{t0, e, v0, v1}, t0, e);
-        }
+        PixelRegs ts = u;
+        PixelMapRegs tm = um;
+        PixelCounters tc = cu;
+        const bool fast = ((e - 1) >> kWindowLog2) == (t0 >> kWindowLog2);
+        cold_segment(&ts, &tm, a.kd, pixel, lz, &tc, Segment{t0, e, v0, v1}, t0, e, fast, x0, x1);
+        u = ts;
+        cu = tc;
       }
       j = f + 1;
     }
@@ -504,8 +561,7 @@ __global__ void __launch_bounds__(32 * kRowsWarps) advance_rows_kernel(RowsArgs 
     load_map(a.map, p, m);
   }
   PixelCounters c;
-  GlobalSink sink{a.ev, &a.counters[kCntEvents]};
-  PixelProc<GlobalSink> proc{s, m, a.k, p, sink, c};
+  const GlobalSink sink{a.ev, &a.counters[kCntEvents]};
   int64_t prev_t = a.t_state;
   float prev_v = s.held;
   const bool longrun = cnt > a.long_row;
@@ -534,16 +590,11 @@ __global__ void __launch_bounds__(32 * kRowsWarps) advance_rows_kernel(RowsArgs 
         prev_v = vi;
         continue;
       }
-      if (((ti - 1) >> kWindowLog2) == (prev_t >> kWindowLog2)) {
-        if (!have_x) x_prev = proc.x_at_sample(prev_v);
-        const float x1 = proc.x_at_sample(vi);
-        proc.segment_fast(Segment{prev_t, ti, prev_v, vi}, x_prev, x1);
-        x_prev = x1;
-        have_x = true;
-      } else {
-        proc.segment(Segment{prev_t, ti, prev_v, vi}, prev_t, ti);
-        have_x = false;
-      }
+      if (!have_x) x_prev = x_sample(s, m, prev_v);
+      const float x1 = x_sample(s, m, vi);
+      feed_segment(s, m, a.k, a.kd, p, sink, c, prev_t, ti, prev_v, vi, x_prev, x1);
+      x_prev = x1;
+      have_x = true;
       prev_t = ti;
       prev_v = vi;
     }
@@ -558,11 +609,10 @@ __global__ void __launch_bounds__(32 * kRowsWarps) advance_rows_kernel(RowsArgs 
     const int64_t br = __shfl_sync(full, beg, r);
     const int32_t nr = __shfl_sync(full, cnt, r);
     PixelCounters cu;
-    LaneZeroSink lz{sink};
-    PixelProc<LaneZeroSink> up{u, um, a.k, pr, lz, cu};
+    const LaneZeroSink lz{sink};
     int64_t pt = a.t_state;
-    float pv = u.held, px = up.x_at_sample(u.held);
-    coop_run(up, a.t + br, a.irr + br, nr, a, lane, pt, pv, px, err, clamps);
+    float pv = u.held, px = x_sample(u, um, u.held);
+    coop_run(u, um, a, pr, lz, cu, a.t + br, a.irr + br, nr, lane, pt, pv, px, err, clamps);
     if (static_cast<int>(lane) == r) {
       s = u;
       c.pieces += cu.pieces;
@@ -575,7 +625,7 @@ __global__ void __launch_bounds__(32 * kRowsWarps) advance_rows_kernel(RowsArgs 
 
   if (valid) {
     samples = static_cast<unsigned long long>(cnt);
-    proc.segment(Segment{prev_t, kForever, prev_v, prev_v}, prev_t, a.t_end);
+    feed_held(s, m, a.kd, p, sink, c, prev_t, prev_v, a.t_end);
     if (cnt > 0) s.held = prev_v;
     store_state(a.out, p, noise, s);
   }
@@ -598,9 +648,8 @@ __global__ void __launch_bounds__(128) advance_unlisted_kernel(RowsArgs a) {
     load_state(a.in, p, noise, s);
     PixelMapRegs m;
     load_map(a.map, p, m);
-    GlobalSink sink{a.ev, &a.counters[kCntEvents]};
-    PixelProc<GlobalSink> proc{s, m, a.k, p, sink, c};
-    proc.segment(Segment{a.t_state, kForever, s.held, s.held}, a.t_state, a.t_end);
+    const GlobalSink sink{a.ev, &a.counters[kCntEvents]};
+    feed_held(s, m, a.kd, p, sink, c, a.t_state, s.held, a.t_end);
     store_state(a.out, p, noise, s);
   }
   __syncwarp();
@@ -924,6 +973,38 @@ struct WindowFeed {
   }
 };
 
+// WindowFeed for a pixel whose state stays in the caller's registers (s, m, c): each segment's clean outcome is taken
+// in place, anything else out of line (feed_segment); the same samples and state as WindowFeed's.
+struct RegFeed {
+  PixelRegs& s;
+  const PixelMapRegs& m;
+  PixelCounters& c;
+  const SensorConsts& k;
+  const SensorConsts* kd;
+  uint32_t pixel;
+  GlobalSink sink;
+  int64_t t_w;
+  int64_t prev_t;
+  float prev_v;
+  float last_raw;
+  float x_prev;
+  __device__ __forceinline__ void start(float carried) {
+    last_raw = carried;
+    prev_v = clamp_irr(carried, k.irr_max);
+    x_prev = x_sample(s, m, prev_v);
+  }
+  __device__ __forceinline__ void operator()(uint32_t dt, float v) {
+    last_raw = v;
+    const float vc = clamp_irr(v, k.irr_max);
+    const int64_t t = t_w + dt;
+    const float x1 = x_sample(s, m, vc);
+    feed_segment(s, m, k, kd, pixel, sink, c, prev_t, t, prev_v, vc, x_prev, x1);
+    prev_t = t;
+    prev_v = vc;
+    x_prev = x1;
+  }
+};
+
 __global__ void __launch_bounds__(128) engine_kernel(EngineArgs a) {
   const uint32_t lane = threadIdx.x & 31u;
   const int64_t t0 = *a.t0;
@@ -951,8 +1032,7 @@ __global__ void __launch_bounds__(128) engine_kernel(EngineArgs a) {
     }
     PixelCounters c;
     unsigned long long samples = 0;
-    GlobalSink sink{S.ev, &S.counters[kCntEvents]};
-    PixelProc<GlobalSink> proc{s, m, S.consts, p, sink, c};
+    const GlobalSink sink{S.ev, &S.counters[kCntEvents]};
     const FieldDev& f = S.field;
     __shared__ uint16_t lists[4][kMaxListed];
     uint16_t* my_list = lists[threadIdx.x >> 5];
@@ -961,7 +1041,7 @@ __global__ void __launch_bounds__(128) engine_kernel(EngineArgs a) {
       const BlobList list = warp_blob_list(f, have, x, y, t_w, t_w + kWindowNs, my_list);
       if (have) {
         const int level = field_level(f, list, x, y, t_w, a.r.l_min, a.r.l_max);
-        WindowFeed feed{&proc, t_w, S.consts.irr_max, t_w, s.held, carried, 0.0f};
+        RegFeed feed{s, m, c, S.consts, &S.consts, p, sink, t_w, t_w, s.held, carried, 0.0f};
         feed.start(carried);
         auto render = [&](uint32_t dt) { return field_eval(f, list, x, y, t_w + dt); };
         samples += sample_pixel_window(a.r, level, carried, false, render, feed);
@@ -1420,8 +1500,7 @@ __global__ void __launch_bounds__(128) engine_kernel_staged(EngineArgs a) {
     }
     PixelCounters c;
     unsigned long long samples = 0;
-    GlobalSink sink{S.ev, &S.counters[kCntEvents]};
-    PixelProc<GlobalSink> proc{s, m, S.consts, p, sink, c};
+    const GlobalSink sink{S.ev, &S.counters[kCntEvents]};
     const FieldDev& f = S.field;
     for (int32_t w = a.w0; w < a.w1; ++w) {
       const int64_t t_w = t0 + static_cast<int64_t>(w) * kWindowNs;
@@ -1444,7 +1523,7 @@ __global__ void __launch_bounds__(128) engine_kernel_staged(EngineArgs a) {
       __syncwarp();
       // Phase B: the pixel model over the staged samples.
       if (have) {
-        WindowFeed feed{&proc, t_w, S.consts.irr_max, t_w, s.held, carried, 0.0f};
+        RegFeed feed{s, m, c, S.consts, &S.consts, p, sink, t_w, t_w, s.held, carried, 0.0f};
         feed.start(carried);
         if (n - 1 <= static_cast<uint32_t>(kStage)) {
           for (uint32_t k = 0; k + 1 < n; ++k) feed(st_dt[warp][k][lane], st_v[warp][k][lane]);
@@ -1980,9 +2059,9 @@ void launch_advance_rows(const SensorConsts& k, const MapSoA& map, StateSoA in, 
                          const uint32_t* pixel, uint32_t n_rows, const int64_t* row_start, const int32_t* row_count,
                          const int64_t* t, const float* irr, uint64_t n_samples, int64_t t_state, int64_t t_end,
                          int32_t long_row, uint32_t* listed, EventBuf ev, unsigned long long* counters,
-                         cudaStream_t stream) {
+                         const SensorConsts* k_dev, cudaStream_t stream) {
   RowsArgs a{k, map, in, out, n_pixels, pixel, n_rows, row_start, row_count, t, irr, n_samples, t_state, t_end,
-             long_row, listed, ev, counters};
+             long_row, listed, ev, counters, k_dev};
   if (n_rows > 0) {
     const unsigned grid = (n_rows + 32 * kRowsWarps - 1) / (32 * kRowsWarps);
     advance_rows_kernel<<<grid, 32 * kRowsWarps, 0, stream>>>(a);

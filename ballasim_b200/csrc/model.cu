@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -263,6 +264,7 @@ struct Model {
   int cur = 0;
   DevBuf<int32_t> row_of;
   DevBuf<uint32_t> listed;  // the row-major CSR kernel's bitmap of listed pixels
+  DevBuf<SensorConsts> k_dev;  // a device copy of k (the row-major kernel's out-of-line calls read it)
   DevBuf<unsigned long long> counters;
   PinBuf<unsigned long long> counters_h;
   DevBuf<RawEvent> events;
@@ -283,6 +285,9 @@ struct Model {
   double launch_ms_total = 0, launch_ms_max = 0;
   int64_t readout_phase = 0;
   Timer timer;
+  mutable Timer take_timer;           // the last download's device part: sort + column split
+  mutable Timer take_timer_copy;      // and its device-to-host copy
+  mutable double take_ms[4] = {0, 0, 0, 0};  // sort + split, copy out, host column copies, whole call (ms)
 
   cudaStream_t stream_of(void* s) const { return s ? static_cast<cudaStream_t>(s) : own; }
 
@@ -605,10 +610,12 @@ struct Model {
       if (!k.cascade && block == 0) {
         // The instantaneous response: row-major over the runs, the samples staged per warp.
         CK(cudaMemsetAsync(listed.p, 0, ((n + 31) / 32) * sizeof(uint32_t), s));
+        k_dev.ensure(1);
+        CK(cudaMemcpyAsync(k_dev.p, &k, sizeof(SensorConsts), cudaMemcpyHostToDevice, s));
         CK(cudaEventRecord(timer.a, s));
         launch_advance_rows(k, map, soa[cur], soa[1 - cur], n, r.pixel, static_cast<uint32_t>(r.n), r.row_start,
                             r.row_count, r.t, r.irr, r.n_samples, t_state, t_end, long_row, listed.p, evb, counters.p,
-                            s);
+                            k_dev.p, s);
       } else {
         CK(cudaMemsetAsync(row_of.p, 0xFF, n * sizeof(int32_t), s));
         launch_scatter_rows(r.pixel, static_cast<uint32_t>(r.n), row_of.p, n, counters.p, s);
@@ -696,11 +703,14 @@ struct Model {
   // The events of a device buffer, sorted on the device, split there into the requested columns (256-byte aligned,
   // side by side), copied out in one transfer through pinned memory, then each column into the caller's array.
   void download_columns(const RawEvent* dev, size_t count, bs_event_columns* o, cudaStream_t s) const {
+    const auto w0 = std::chrono::steady_clock::now();
+    for (double& v : take_ms) v = 0.0;
     if (count == 0) return;
     if (count > 0x7fffffffull) throw std::invalid_argument("too many events in one call");
     const uint32_t n = static_cast<uint32_t>(count);
     sorted.ensure(count);
     sort_scratch.ensure(sort_events_scratch_bytes(n));
+    CK(cudaEventRecord(take_timer.a, s));
     CK(sort_events(dev, n, sorted.p, sort_scratch.p, s));
     struct Col {
       void* dst;
@@ -729,8 +739,16 @@ struct Model {
                             static_cast<float*>(at(8)),   static_cast<float*>(at(9)),
                             static_cast<float*>(at(10)),  static_cast<float*>(at(11))};
     CK(event_columns(sorted.p, n, width, readout(), d, s));
+    CK(cudaEventRecord(take_timer.b, s));
     CK(cudaMemcpyAsync(col_pin.p, col_dev.p, total, cudaMemcpyDeviceToHost, s));
+    CK(cudaEventRecord(take_timer_copy.b, s));
     CK(cudaStreamSynchronize(s));
+    const auto w1 = std::chrono::steady_clock::now();
+    float ms_split = 0.0f, ms_copy = 0.0f;
+    cudaEventElapsedTime(&ms_split, take_timer.a, take_timer.b);
+    cudaEventElapsedTime(&ms_copy, take_timer.b, take_timer_copy.b);
+    take_ms[0] = ms_split;
+    take_ms[1] = ms_copy;
     const auto copy = [&](const Col& c) { std::memcpy(c.dst, col_pin.p + c.at, c.elem * count); };
     if (count < 65536) {
       for (const Col& c : cols) {
@@ -743,6 +761,9 @@ struct Model {
       }
       for (std::thread& t : th) t.join();
     }
+    const auto w2 = std::chrono::steady_clock::now();
+    take_ms[2] = std::chrono::duration<double, std::milli>(w2 - w1).count();
+    take_ms[3] = std::chrono::duration<double, std::milli>(w2 - w0).count();
   }
 
   // ---- the output stage: events in output order, released at the model time's cut, the rest held ----
@@ -1445,6 +1466,9 @@ struct Engine {
   int warps_per_block = 4, blocks_per_sm = 0, stage = 0, tile_lw = 3;
   double last_ms = 0;
   Timer timer;
+  mutable Timer take_timer;           // the last download's device part: sort + column split
+  mutable Timer take_timer_copy;      // and its device-to-host copy
+  mutable double take_ms[4] = {0, 0, 0, 0};  // sort + split, copy out, host column copies, whole call (ms)
   cudaStream_t own = nullptr;
   cudaEvent_t order = nullptr;
   // The step as a CUDA graph (rebuilt when its launch shape, window count or proposal changes), fed from pinned
@@ -1946,6 +1970,13 @@ bs_status bs_model_download_events(bs_model* m, const bs_device_events* ev, bs_e
     NEED(ev);
     NEED(out);
     m->download_columns(static_cast<const bs::RawEvent*>(ev->data), ev->count, out, m->own);
+  });
+}
+bs_status bs_model_take_timing(const bs_model* m, double out[4]) {
+  return guarded([&] {
+    NEED(m);
+    NEED(out);
+    for (int i = 0; i < 4; ++i) out[i] = m->take_ms[i];
   });
 }
 bs_status bs_model_event_count(const bs_model* m, size_t* n) {

@@ -70,8 +70,8 @@ struct PixelCounters {
   uint32_t pieces = 0, leaves = 0, noise_candidates = 0;
 };
 
-BS_HD float clamp_irr(float v, float v_max) { return v >= 0.0f ? (v <= v_max ? v : v_max) : 0.0f; }
-BS_HD float since_ref(int64_t t, int64_t t_ref) { return static_cast<float>(static_cast<double>(t - t_ref) * 1e-9); }
+BS_HOT float clamp_irr(float v, float v_max) { return v >= 0.0f ? (v <= v_max ? v : v_max) : 0.0f; }
+BS_HOT float since_ref(int64_t t, int64_t t_ref) { return static_cast<float>(static_cast<double>(t - t_ref) * 1e-9); }
 
 BS_HD uint8_t split_label(float ds, float dl, float D, float cut) {
   const float a_s = ds / D, a_l = dl / D;
@@ -117,22 +117,22 @@ struct PixelProc {
   Segment pg{};
   int64_t p_t = 0, p_e = 0, p_lo = 0, p_stop = 0;
 
-  BS_HD float value(const Segment& g, int64_t t) const {
+  BS_HOT float value(const Segment& g, int64_t t) const {
     if (g.t1 == kForever) return g.v0;
     const float f = static_cast<float>(t - g.t0) / static_cast<float>(g.t1 - g.t0);
     return g.v0 + (g.v1 - g.v0) * f;
   }
-  BS_HD float current(const Segment& g, int64_t t) const { return m.dark + m.scale * value(g, t); }
-  BS_HD float log_ratio(float I) const { return log_f(I / s.i_scale); }
+  BS_HOT float current(const Segment& g, int64_t t) const { return m.dark + m.scale * value(g, t); }
+  BS_HOT float log_ratio(float I) const { return log_f(I / s.i_scale); }
 
-  BS_HD float delta(int64_t t, float x) const {
+  BS_HOT float delta(int64_t t, float x) const {
     const float ds = x - s.s3_ref;
     const float dn = 0.0f - s.n3_ref;
     const float dl = m.leak * since_ref(t, s.t_ref) + s.dr_ref;
     return ds + dn + dl;
   }
 
-  BS_HD void set_reference(int64_t t, float s3, float offset) {
+  BS_HOT void set_reference(int64_t t, float s3, float offset) {
     s.t_ref = t;
     s.s3_ref = s3;
     s.n3_ref = 0.0f;
@@ -179,7 +179,7 @@ struct PixelProc {
   // monotonically; so Delta over (a, c] lies between its value formed from min(x) and dl(a) and its value formed
   // from max(x) and dl(c), with no margin. It answers "no" only where no integer of (a, c] fires, and so prunes
   // at least what instant_may_fire prunes; the time-ordered search then finds the same first crossing.
-  BS_HD bool may_fire_exact(int64_t a, int64_t cc, float xa, float xc) const {
+  BS_HOT bool may_fire_exact(int64_t a, int64_t cc, float xa, float xc) const {
     const float dn = 0.0f - s.n3_ref;
     const float dl_a = m.leak * since_ref(a, s.t_ref) + s.dr_ref;
     const float dl_c = m.leak * since_ref(cc, s.t_ref) + s.dr_ref;
@@ -335,7 +335,7 @@ struct PixelProc {
   }
 
   // x(t) = ln(I / i_scale) at a sample of value v (the start of the segment it opens).
-  BS_HD float x_at_sample(float v) const { return log_ratio(m.dark + m.scale * v); }
+  BS_HOT float x_at_sample(float v) const { return log_ratio(m.dark + m.scale * v); }
 
   // A whole segment g = [t0, t1) that is one piece (no multiple of 2^23 ns inside), with x0 = x(t0) and
   // x1 = x(t1) (the next segment's start, x_at_sample(g.v1)). Bitwise piece(g, t0, t1): where the pixel is not
@@ -399,7 +399,7 @@ struct PixelProc {
   }
 
   // True when instant_may_fire(t0, t1 - 1, I(t0), I(t1 - 1)) and Delta(t1 - 1) are provably both false.
-  BS_HD bool excluded(const Segment& g, int64_t t0, int64_t e, float x0, float x1) const {
+  BS_HOT bool excluded(const Segment& g, int64_t t0, int64_t e, float x0, float x1) const {
     // The interpolation reaches v1 exactly (v0 + (v1 - v0) == v1 in fp32): I over [t0, t1] then lies between its
     // end values, and the exact bounds of may_fire_exact hold with x0, x1 (dl(t1) >= dl(t1 - 1)).
     if (g.v0 + (g.v1 - g.v0) == g.v1) {

@@ -21,19 +21,20 @@ from .fields import Field
 WINDOW_NS = 1 << 23
 
 
-class Cancelled(Exception):
-    """A window stopped by its CancelToken (the reference's _engine.Cancelled, src/engine/cancel.h:28-30)."""
+Cancelled = _lib.Cancelled
 
 
 class CancelToken:
     """A cooperative cancel (the reference's _engine.CancelToken, engine_module.cpp:1351-1357): set() from any
-    thread; sample_window checks it at each pixel batch and refinement round."""
+    thread; sample_window checks it at each pixel batch and refinement round (the flag the C window reads)."""
 
     def __init__(self):
         self._ev = threading.Event()
+        self._flag = C.c_int32(0)
 
     def set(self) -> None:
         """Requests the cancel (never cleared)."""
+        self._flag.value = 1
         self._ev.set()
 
     def is_set(self) -> bool:
@@ -191,96 +192,63 @@ def _render_batch(render, pixel: np.ndarray, t: np.ndarray, groups: int):
 
 
 def _host_window(t_w: int, ids: np.ndarray, lv: np.ndarray, ci: np.ndarray, cs: np.ndarray, render, midpoint,
-                 refine_signature: bool, max_refine_levels: int, min_split: int, cancel) -> tuple:
-    """The window with a Python callable as the renderer, breadth-first as the host WindowEngine runs it
-    (src/engine/window_impl.h:462-714): the lattice of every pixel rendered in one call (slot 0 is the carried
-    sample), round 0's flags (sampling.h:471-520), then up to max_refine_levels rounds, each rendering the listed
-    intervals' midpoints in one call and flagging their halves (sampling.h:612-660); the runs sorted by time per
-    pixel; ci / cs take each pixel's sample at t_w + 2^23. The midpoint triples of a round go to the device in one
-    launch (MidpointTest)."""
+                 refine_signature: bool, max_refine_levels: int, min_dt_ns: int, cancel) -> tuple:
+    """The window with a Python callable as the renderer, through the C ABI's render-hook window (bs_window_run: the
+    reference's host WindowEngine, src/engine/window_impl.h:462-714, breadth-first, one render call per round, the
+    midpoint tests on the device). The callable sees each call's requests as (pixel_ids, t_ns); ci / cs take each
+    pixel's sample at t_w + 2^23."""
     n, G = len(ids), ci.shape[1]
-    stats = {"pixels": n, "samples_by_round": [0], "flagged_signature": 0, "flagged_midpoint": 0,
-             "refine_cap_hits": 0, "band_samples_by_round": [0]}
-    if n == 0:
-        return np.zeros(0, np.int64), np.zeros((0, G), np.float32), np.zeros(1, np.int64), stats
-    _check_cancel(cancel, "window: batch")
-    count = (np.int64(1) << lv.astype(np.int64)) + 1
-    off0 = np.zeros(n + 1, np.int64)
-    np.cumsum(count, out=off0[1:])
-    s0 = int(off0[-1])
-    owner = np.repeat(np.arange(n, dtype=np.int64), count)
-    j = np.arange(s0, dtype=np.int64) - off0[owner]
-    dt = j << (23 - lv.astype(np.int64)[owner])
-    irr = np.zeros((s0, G), np.float32)
-    sig = np.zeros(s0, np.uint64)
-    irr[off0[:-1]] = ci
-    sig[off0[:-1]] = cs
-    req = np.nonzero(j != 0)[0]
-    irr[req], sig[req] = _render_batch(render, ids[owner[req]], t_w + dt[req], G)
-    rounds = [len(req)]
+    errors = []
 
-    def exceeds(a, m, b):
-        if midpoint is None or len(a) == 0:
-            return np.zeros(len(a), bool)
-        return midpoint.exceeds(irr[a], irr[m], irr[b])
+    def fn(_user, req, m, out_index, irr, sig, _subsamples):
+        try:
+            words = np.ctypeslib.as_array(C.cast(req, C.POINTER(C.c_uint32)), (m * 6,)).reshape(m, 6)
+            idx = np.ctypeslib.as_array(out_index, (m,)).astype(np.int64)
+            px = words[:, 1].copy()
+            t = int(t_w) + words[:, 4].view(np.int32).astype(np.int64)
+            e, s = _render_batch(render, px, t, G)
+            rows = int(idx.max()) + 1
+            np.ctypeslib.as_array(irr, (rows * G,)).reshape(rows, G)[idx] = e
+            np.ctypeslib.as_array(sig, (rows,))[idx] = s
+            return 0
+        except BaseException as ex:  # the callback cannot raise through C: kept, and raised after the call
+            errors.append(ex)
+            return 1
 
-    # Round 0: interval (i - 1, i) of every slot i past a pixel's first; node k tests the triple (k - 1, k, k + 1).
-    i = req
-    cnt_i = count[owner[i]]
-    flip = (sig[i] != sig[i - 1]) if refine_signature else np.zeros(len(i), bool)
-    node = np.zeros(s0, bool)
-    inner = i[j[i] + 1 < cnt_i]
-    node[inner] = exceeds(inner - 1, inner, inner + 1)
-    mid = ((j[i] + 1 < cnt_i) & node[i]) | ((j[i] >= 2) & node[i - 1])
-    want = flip | mid
-    split = want & (dt[i] - dt[i - 1] >= min_split)
-    words = [int(flip.sum()), int((mid & ~flip).sum()), int((want & ~split).sum())]
-    lo, hi = i[split] - 1, i[split]
-    parts_dt, parts_owner, parts_irr, parts_sig = [dt], [owner], [irr], [sig]
-    samples = s0
-    k = 0
-    while True:
-        stats["flagged_signature"] += words[0]
-        stats["flagged_midpoint"] += words[1]
-        if k == max_refine_levels:
-            stats["refine_cap_hits"] += words[2] + len(lo)
-            break
-        stats["refine_cap_hits"] += words[2]
-        if len(lo) == 0:
-            break
-        _check_cancel(cancel, "window: refinement round")
-        m = len(lo)
-        g = np.arange(samples, samples + m, dtype=np.int64)
-        d_g = (dt[lo] + dt[hi]) >> 1
-        o_g = owner[hi]
-        e_g, s_g = _render_batch(render, ids[o_g], t_w + d_g, G)
-        dt, owner = np.concatenate([dt, d_g]), np.concatenate([owner, o_g])
-        irr, sig = np.concatenate([irr, e_g]), np.concatenate([sig, s_g])
-        samples += m
-        s1 = (sig[lo] != sig[g]) if refine_signature else np.zeros(m, bool)
-        s2 = (sig[g] != sig[hi]) if refine_signature else np.zeros(m, bool)
-        bad = exceeds(lo, g, hi)
-        f1, f2 = s1 | bad, s2 | bad
-        p1 = f1 & (dt[g] - dt[lo] >= min_split)
-        p2 = f2 & (dt[hi] - dt[g] >= min_split)
-        words = [int(s1.sum() + s2.sum()), int((bad & ~s1).sum() + (bad & ~s2).sum()),
-                 int((f1 & ~p1).sum() + (f2 & ~p2).sum())]
-        # Candidates (lo, g), (g, hi) per listed interval, kept in order.
-        c_lo = np.stack([lo, g], 1).reshape(-1)
-        c_hi = np.stack([g, hi], 1).reshape(-1)
-        keep = np.stack([p1, p2], 1).reshape(-1)
-        lo, hi = c_lo[keep], c_hi[keep]
-        rounds.append(m)
-        k += 1
-    stats["samples_by_round"] = rounds
-    stats["band_samples_by_round"] = [0] * len(rounds)
-    order = np.lexsort((dt, owner))
-    last = off0[1:] - 1
-    ci[:] = irr[last]
-    cs[:] = sig[last]
-    off = np.zeros(n + 1, np.int64)
-    off[1:] = np.cumsum(np.bincount(owner, minlength=n))
-    return t_w + dt[order], irr[order], off, stats
+    cb = _lib.RENDER_FN(fn)
+    mn = np.ascontiguousarray(midpoint.m_min if midpoint is not None else [1.0] * G, np.float32)
+    mx = np.ascontiguousarray(midpoint.m_max if midpoint is not None else [1.0] * G, np.float32)
+    h = C.c_void_p()
+    _lib.check(_lib.lib().bs_window_create(G, mn.ctypes.data, mx.ctypes.data, C.byref(h)))
+    try:
+        rules = _lib.WindowRules(midpoint.tol if midpoint is not None else 0.0,
+                                 midpoint.dark if midpoint is not None else 0.0, 1 if midpoint is not None else 0,
+                                 1 if refine_signature else 0, int(max_refine_levels), int(min_dt_ns), 0, 64,
+                                 C.addressof(cancel._flag) if cancel is not None else None)
+        total = C.c_size_t()
+        st = _lib.lib().bs_window_run(h, int(t_w), _lib.ptr(ids), _lib.ptr(lv), n, _lib.ptr(ci), _lib.ptr(cs),
+                                      C.byref(rules), cb, None, C.byref(total))
+        if errors:
+            raise errors[0]
+        _lib.check(st)
+        S = total.value
+        off = np.zeros(n + 1, np.int64)
+        t = np.zeros(S, np.int64)
+        irr = np.zeros((S, G), np.float32)
+        _lib.check(_lib.lib().bs_window_runs(h, off.ctypes.data, t.ctypes.data if S else None,
+                                             irr.ctypes.data if S else None))
+        counters = np.zeros(4, np.uint64)
+        rounds = C.c_size_t()
+        by_round = np.zeros(64, np.uint64)
+        _lib.check(_lib.lib().bs_window_stats(h, counters.ctypes.data, by_round.ctypes.data, 64, C.byref(rounds)))
+    finally:
+        _lib.lib().bs_window_destroy(h)
+    k = min(rounds.value, 64)
+    stats = {"pixels": n, "samples_by_round": [int(v) for v in by_round[:k]],
+             "flagged_signature": int(counters[0]), "flagged_midpoint": int(counters[1]),
+             "refine_cap_hits": int(counters[2]), "render_calls": int(counters[3]),
+             "band_samples_by_round": [0] * k}
+    return t, irr, off, stats
 
 
 def sample_window(t_w: int, pixel_ids, levels, rank, carried_irr, carried_sig, render, *, refine_signature: bool,
@@ -324,7 +292,7 @@ def sample_window(t_w: int, pixel_ids, levels, rank, carried_irr, carried_sig, r
         if midpoint is not None and (len(midpoint.m_min) != G or len(midpoint.m_max) != G):
             raise ValueError("MidpointTest: one waveform range per light group is needed")
         t, irr, off, stats = _host_window(int(t_w), ids, lv, ci, cs, render, midpoint, bool(refine_signature),
-                                          int(max_refine_levels), 2 * int(min_dt_ns), cancel)
+                                          int(max_refine_levels), int(min_dt_ns), cancel)
         return WindowRuns(ids.copy(), t, irr, off, ci, cs, stats)
     if ci.shape[1] != 1:
         raise ValueError("sample_window: this build samples one light group")

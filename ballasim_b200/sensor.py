@@ -357,6 +357,13 @@ class SensorModel:
         with self._lock:
             _lib.check(_lib.lib().bs_model_load_state(self._h, b.ctypes.data, len(b)))
 
+    def take_timing(self) -> dict:
+        """The last download of device events, in parts (ms): the sort and column split on the device, the copy to
+        pinned host memory, the copies into the returned arrays, and the whole call."""
+        out = np.zeros(4)
+        _lib.check(_lib.lib().bs_model_take_timing(self._h, out.ctypes.data))
+        return dict(zip(("sort_split_ms", "copy_out_ms", "host_copy_ms", "total_ms"), out.tolist()))
+
     def set_long_run(self, samples: int) -> None:
         """Threads per pixel of the row-major kernel: runs longer than `samples` are walked by a whole warp (32 lanes,
         32 samples at a time), the others one per lane (0: the default, 32; -1: every run by one lane)."""

@@ -231,7 +231,9 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     # e2e through the public API with host buffers: the initial frames from pinned host memory in, every event out;
     # each phase timed on the host after a synchronize, for the split of the e2e step.
     frames = [torch.from_numpy(field_frame(s.field, 0)).pin_memory().numpy() for s in wl.sensors]
-    e2e_times, d2h, split = [], 0, {"start_ms": 0.0, "run_ms": 0.0, "take_events_ms": 0.0}
+    e2e_times, d2h = [], 0
+    split = {"start_ms": 0.0, "run_ms": 0.0, "take_events_ms": 0.0, "take_sort_split_ms": 0.0,
+             "take_copy_out_ms": 0.0, "take_host_copy_ms": 0.0, "take_download_ms": 0.0}
     for k in range(0 if args.profile else args.warmup + args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -240,17 +242,18 @@ def run_ours(args, rank: int, world: int) -> dict | None:
         t1 = time.perf_counter()
         eng.run(wl.windows, sptr)
         t2 = time.perf_counter()
-        n_ev = 0
+        n_ev, parts = 0, np.zeros(4)
         for m in models:
             cols = m.take_events()
             n_ev += len(cols["t_cross_ns"])
+            parts += np.array(list(m.take_timing().values()))
         torch.cuda.synchronize()
         t3 = time.perf_counter()
         if k >= args.warmup:
             e2e_times.append(t3 - t0)
             d2h = n_ev * 32
-            for key, v in zip(split, (t1 - t0, t2 - t1, t3 - t2)):
-                split[key] += 1e3 * v / args.steps
+            for key, v in zip(split, (1e3 * (t1 - t0), 1e3 * (t2 - t1), 1e3 * (t3 - t2), *parts)):
+                split[key] += v / args.steps
     e2e_s = reduce_max(sum(e2e_times), world)
     h2d = sum(int(f.nbytes) for f in frames)
 

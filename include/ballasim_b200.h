@@ -7,7 +7,7 @@
  *   BS_EINVAL -> ValueError (std::invalid_argument), BS_ELOGIC -> RuntimeError (std::logic_error),
  *   BS_ENOMEM -> MemoryError (MemoryBudgetError), BS_ECUDA -> RuntimeError (a CUDA failure or no device),
  *   BS_EREFUSED -> ExportError, a ValueError (the exporters' Refused), BS_EIO -> OSError (a file that cannot be
- *   created, written or read).
+ *   created, written or read), BS_ECANCELLED -> Cancelled (a window stopped by its cancel flag).
  * There is no CPU fallback: without a CUDA device every compute call returns BS_ECUDA.
  *
  * Citations are to the reference project's files; each entry point names the interface it replaces. */
@@ -29,6 +29,7 @@ typedef int32_t bs_status;
 #define BS_ECUDA 4
 #define BS_EREFUSED 5
 #define BS_EIO 6
+#define BS_ECANCELLED 7
 
 typedef struct bs_model bs_model;
 typedef struct bs_sampler bs_sampler;
@@ -130,6 +131,10 @@ bs_status bs_model_advance_device(bs_model* m, const bs_device_runs* runs, int64
  * and the kept events of bs_model_advance_runs / an engine run (then cleared). */
 bs_status bs_model_download_events(bs_model* m, const bs_device_events* ev, bs_event_columns* out);
 bs_status bs_model_event_count(const bs_model* m, size_t* n);
+/* The last device-event download's parts (ms; no reference counterpart): [0] the sort by (t_cross, pixel) and the
+ * split into columns on the device, [1] the columns' copy to pinned host memory (CUDA events on the model's stream),
+ * [2] the copies from pinned memory into the caller's arrays, [3] the whole download (host clock). */
+bs_status bs_model_take_timing(const bs_model* m, double out[4]);
 bs_status bs_model_take_events(bs_model* m, bs_event_columns* out);
 /* SensorModel::maps (sensor_model.h:180; sensor_module.cpp sensor_maps): the fp64 maps, width * height each. */
 bs_status bs_model_maps(const bs_model* m, double* theta_on, double* theta_off, double* leak, double* dark_fA,
@@ -254,6 +259,58 @@ bs_status bs_sample_window_static(const bs_field* field, int64_t t_w, const uint
                                   const uint64_t* carried_sig, const bs_sample_rules* rules, int64_t* offsets,
                                   int64_t* t_ns, float* irr, size_t capacity, float* carried_irr_out,
                                   uint64_t* carried_sig_out, void* stream, size_t* n_samples);
+/* ---- sample_window with a renderer behind a callback: the reference's host window engine (WindowEngine<kHost>,
+ * src/engine/window_impl.h:462-714) driving a RenderHook (src/engine/window.h:69-84) ---- */
+
+/* One pixel-sample request (render::SampleRequest, src/backend/api.h:25-34), 24 bytes: camera, flags (0: a regular
+ * lattice sample), pixel id, sub-sample range [k_begin, k_begin + k_count), time offset from the window start (ns),
+ * and the time slot t_off_ns >> log2(min_dt_ns) in pose_slot. */
+typedef struct {
+  uint16_t cam;
+  uint16_t flags;
+  uint32_t pixel;
+  uint32_t k_begin;
+  uint32_t k_count;
+  int32_t t_off_ns;
+  uint32_t pose_slot;
+} bs_sample_request;
+/* RenderHook::render as a C callback: request i's irradiance goes to row out_index[i] of irr (groups floats each) and
+ * its signature to sig[out_index[i]]; every request of a call has k_count == subsamples. Returns 0, or a non-zero
+ * status that stops the window (BS_EINVAL). Called on the calling thread, one call per render round. */
+typedef int32_t (*bs_render_fn)(void* user, bs_sample_request* requests, size_t n, const uint32_t* out_index,
+                                float* irr, uint64_t* sig, uint32_t subsamples);
+/* The window's rules (SampleConfig, src/engine/window.h:98-110, with the Phase 1 sample rules): the eta_L midpoint
+ * test (tol, dark) when midpoint != 0, refine_signature, max_refine_levels, min_dt_ns (a power of two in [1, 2^23]),
+ * the camera and sub-samples of the requests; cancel (may be NULL): a flag another thread may set, checked before the
+ * window and at every refinement round (the reference's CancelToken; BS_ECANCELLED). */
+typedef struct {
+  float tol, dark;
+  int32_t midpoint, refine_signature, max_refine_levels;
+  int64_t min_dt_ns;
+  uint16_t cam;
+  uint32_t subsamples;
+  const volatile int32_t* cancel;
+} bs_window_rules;
+typedef struct bs_window bs_window;
+/* groups light groups (1 to 8) with their waveform ranges m_min / m_max (NULL: 1), the midpoint test's MidpointTest
+ * (tol, dark, m_min, m_max) (engine_module.cpp:1363-1411). */
+bs_status bs_window_create(int32_t groups, const float* m_min, const float* m_max, bs_window** out);
+bs_status bs_window_destroy(bs_window* w);
+/* One window at t_w (a multiple of 2^23) of n listed pixels (ids in render order, lattice levels in [0, 23 -
+ * log2(min_dt_ns)]) with their carried samples (host, n x groups irradiance and n signatures, in and out: each pixel's
+ * sample at t_w + 2^23): the lattice in one render call, round 0's flags, then the refinement rounds, one render call
+ * each; each round's midpoint tests run on the device (no device call without the midpoint test). *n_samples receives
+ * the runs' total. */
+bs_status bs_window_run(bs_window* w, int64_t t_w, const uint32_t* pixel_ids, const uint8_t* levels, size_t n,
+                        float* carried_irr, uint64_t* carried_sig, const bs_window_rules* rules, bs_render_fn render,
+                        void* user, size_t* n_samples);
+/* The last window's runs (WindowRuns: offsets n + 1, t_ns, irradiance n_samples x groups), host arrays. */
+bs_status bs_window_runs(const bs_window* w, int64_t* offsets, int64_t* t_ns, float* irr);
+/* Its WindowStats (src/engine/window.h:111-131): counters [flagged_signature, flagged_midpoint, refine_cap_hits,
+ * render_calls], samples_by_round (up to cap rounds) and *rounds their number. */
+bs_status bs_window_stats(const bs_window* w, uint64_t counters[4], uint64_t* samples_by_round, size_t cap,
+                          size_t* rounds);
+
 /* The field's level rule per pixel at t_w, and the field itself at t (width * height, host outputs). */
 bs_status bs_field_levels(bs_sampler* s, int64_t t_w, int32_t l_min, int32_t l_max, uint8_t* out);
 bs_status bs_field_frame(bs_sampler* s, int64_t t_ns, float* out);

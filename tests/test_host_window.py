@@ -203,3 +203,91 @@ def test_fixed_rate_window_equals_the_reference_engine(oracle_port, ref, period_
     runs = fixed_rate_window(t_w, ids, np.arange(len(ids)), period_ns, carried, sig, render)
     _same_runs(runs, want)
     assert runs.stats["samples_by_round"] == [len(ids) * fixed_rate_samples(t_w, period_ns)]
+
+
+@pytest.mark.parametrize("max_refine_levels,min_dt_ns", [(4, 8192), (10, 2048)])
+def test_render_calls_follow_the_reference_order(oracle_port, ref, max_refine_levels, min_dt_ns):
+    """The render-hook window makes the reference engine's render calls (WindowEngine<kHost>, window_impl.h:462-714):
+    the same number of calls, each with the same requests in the same order (the lattice pixel-major and by time,
+    then each round's midpoints in interval order), signature refinement with non-zero signatures."""
+    from ballasim_b200.sampling import sample_window
+
+    f = _fast_blobs()
+    ids = np.random.default_rng(9).permutation(f.width * f.height)[:150].astype(np.uint32)
+    base = _field_render(oracle_port, f, 1, 9.0)
+    lv = (1 + ids % 4).astype(np.uint8)
+    carried, sig = base(ids, np.zeros(len(ids), np.int64))
+    assert np.count_nonzero(sig) > 0
+    seen = {"ours": [], "ref": []}
+
+    def recorder(key):
+        def render(p, t):
+            seen[key].append((p.copy(), t.copy()))
+            return base(p, t)
+        return render
+
+    want = ref.sample_window_cb(recorder("ref"), 1, None, True, max_refine_levels, min_dt_ns, 3 << 23, ids, lv,
+                                carried.copy(), sig.copy())
+    runs = sample_window(3 << 23, ids, lv, np.arange(len(ids)), carried, sig, recorder("ours"), refine_signature=True,
+                         midpoint=None, max_refine_levels=max_refine_levels, min_dt_ns=min_dt_ns)
+    _same_runs(runs, want)
+    assert len(seen["ours"]) == len(seen["ref"]) == want[5]["render_calls"] >= 2
+    for (pa, ta), (pb, tb) in zip(seen["ours"], seen["ref"]):
+        assert np.array_equal(pa, pb) and np.array_equal(ta, tb)
+
+
+def test_window_requests_through_the_c_abi():
+    """bs_window_run's requests as a C renderer sees them: 24-byte rows with the camera, flags 0, the pixel, the
+    sub-sample range [0, subsamples), the time offset from the window start and the time slot t_off >> log2(min_dt);
+    each row's irradiance and signature written at out_index go into the runs; a failing renderer stops the window."""
+    import ctypes as C
+
+    from ballasim_b200 import _lib
+
+    L = _lib.lib()
+    rows = []
+
+    def fn(_user, req, n, out_index, irr, sig, subsamples):
+        idx = np.ctypeslib.as_array(out_index, (n,))
+        m = int(idx.max()) + 1
+        e = np.ctypeslib.as_array(irr, (m,))
+        s = np.ctypeslib.as_array(sig, (m,))
+        for i in range(n):
+            r = req[i]
+            rows.append((r.cam, r.flags, r.pixel, r.k_begin, r.k_count, r.t_off_ns, r.pose_slot, subsamples))
+            e[idx[i]] = float(r.pixel) + r.t_off_ns * 1e-6
+            s[idx[i]] = r.pixel * 1000 + r.pose_slot
+        return 0
+
+    cb = _lib.RENDER_FN(fn)
+    h = C.c_void_p()
+    _lib.check(L.bs_window_create(1, None, None, C.byref(h)))
+    ids = np.array([7, 3, 12], np.uint32)
+    lv = np.array([1, 2, 0], np.uint8)
+    ci = np.array([1.5, 2.5, 3.5], np.float32)
+    cs = np.array([70, 30, 120], np.uint64)
+    rules = _lib.WindowRules(0.0, 0.0, 0, 0, 0, 1 << 16, 5, 16, None)
+    n_s = C.c_size_t()
+    _lib.check(L.bs_window_run(h, 2 << 23, ids.ctypes.data, lv.ctypes.data, 3, ci.ctypes.data, cs.ctypes.data,
+                               C.byref(rules), cb, None, C.byref(n_s)))
+    assert n_s.value == 3 + 5 + 2 and len(rows) == 2 + 4 + 1
+    for cam, flags, px, k0, kn, t_off, slot, sub in rows:
+        assert (cam, flags, k0, kn, sub) == (5, 0, 0, 16, 16) and slot == t_off >> 16
+    assert [r[2] for r in rows] == [7, 7, 3, 3, 3, 3, 12]
+    assert [r[5] for r in rows] == [1 << 22, 1 << 23, 1 << 21, 2 << 21, 3 << 21, 4 << 21, 1 << 23]
+    off = np.zeros(4, np.int64)
+    t = np.zeros(10, np.int64)
+    irr = np.zeros(10, np.float32)
+    _lib.check(L.bs_window_runs(h, off.ctypes.data, t.ctypes.data, irr.ctypes.data))
+    assert list(off) == [0, 3, 8, 10]
+    assert t[0] == 2 << 23 and irr[0] == np.float32(1.5) and t[2] == (2 << 23) + (1 << 23)
+    assert irr[2] == np.float32(7 + 8.388608) and ci[0] == irr[2] and cs[0] == 7000 + (1 << 23 >> 16)
+
+    def failing(*_):
+        return 3
+
+    bad = _lib.RENDER_FN(failing)
+    with pytest.raises(ValueError, match="render callback failed"):
+        _lib.check(L.bs_window_run(h, 0, ids.ctypes.data, lv.ctypes.data, 3, ci.ctypes.data, cs.ctypes.data,
+                                   C.byref(rules), bad, None, C.byref(n_s)))
+    L.bs_window_destroy(h)
