@@ -409,6 +409,88 @@ __device__ __forceinline__ bool clean_segment(const PixelRegs& s, const PixelMap
   return hp.excluded(Segment{t0, e, v0, v1}, t0, e, x0, x1);
 }
 
+// The noise candidates of a stretch [t_from, t_end) of every lane's pixel, computed with all 32 lanes together.
+// A candidate that thinning rejects changes nothing but its chain (PixelProc::noise_candidate), and its acceptance
+// depends only on its draw and the irradiance at its time, which the stretch's samples give: so each lane's chains
+// move past their rejected candidates here, and stop at their first accepted candidate in the stretch (or at their
+// first candidate after it). The pixel model then meets only accepted candidates, at which it runs its own noise
+// path (the draw and the thinning test again, the refractory drop, the event) and follows the chains from there as
+// usual. Events and the chains' end state are those of the pixel model meeting every candidate; only the count of
+// the crossing search's nodes differs, since the search is no longer cut at rejected candidates (the first crossing
+// is the same: a time-ordered search over [lo, e) finds what searches over [lo, tn) then [tn, e) find).
+// active: this lane's stretch is in `run` (run.n samples after the one held at t_from, run.t(j) / run.v_at(j), raw
+// values clamped here as the pixel model clamps them). All lanes of the warp call it.
+template <class Run>
+__device__ __forceinline__ void noise_ahead(PixelRegs& s, const PixelMapRegs& m, const SensorConsts& k,
+                                            uint32_t pixel, bool active, int64_t t_from, float v_held,
+                                            int64_t t_end, const Run& run, PixelCounters& c) {
+  bool done_shot = !active, done_ba = !active;
+  for (;;) {
+    const bool p_shot = !done_shot && s.t_shot < t_end, p_ba = !done_ba && s.t_ba < t_end;
+    if (!__any_sync(0xffffffffu, p_shot || p_ba)) break;
+    if (!(p_shot || p_ba)) continue;
+    const bool shot = p_shot && (!p_ba || s.t_shot <= s.t_ba);
+    const int64_t tn = shot ? s.t_shot : s.t_ba;
+    const uint32_t purpose = shot ? kPurposeShot : kPurposeBackground;
+    const uint32_t nidx = shot ? s.n_shot : s.n_ba;
+    // The segment holding tn: [t_a, t_b) between consecutive samples, or held after the last one.
+    int64_t ta = t_from;
+    float va = v_held;
+    int64_t tb = kForever;
+    float vb = va;
+    for (int j = 0; j < run.n; ++j) {
+      const int64_t tj = run.t(j);
+      const float vj = clamp_irr(run.v_at(j), k.irr_max);
+      if (tj > tn) {
+        tb = tj;
+        vb = vj;
+        break;
+      }
+      ta = tj;
+      va = vj;
+    }
+    if (tb == kForever) vb = va;
+    const U4 w = draw(k.seed, purpose, k.camera, pixel, nidx);
+    NullSink ns;
+    PixelCounters nc;
+    const PixelProc<NullSink> hp{s, m, k, pixel, ns, nc};
+    const float I = hp.current(Segment{ta, tb, va, vb}, tn);
+    const double accept = shot ? sqrt(static_cast<double>(m.dark) / static_cast<double>(I)) : 1.0;
+    if (open_uniform_d(w.v[1]) < accept) {
+      if (shot) done_shot = true;
+      else done_ba = true;
+      continue;
+    }
+    ++c.noise_candidates;
+    const int64_t next = noise_next(k.seed, purpose, k.camera, pixel, nidx + 1, tn, shot ? m.shot_max_hz : m.ba_rate_hz);
+    if (shot) {
+      s.n_shot = nidx + 1;
+      s.t_shot = next;
+    } else {
+      s.n_ba = nidx + 1;
+      s.t_ba = next;
+    }
+  }
+}
+
+// A lane's window staged in shared memory (dt / v strided by 32 lanes) as noise_ahead's run.
+struct StagedRun {
+  int64_t t_w;
+  const uint32_t* dt;
+  const float* v;
+  int n;
+  __device__ __forceinline__ int64_t t(int j) const { return t_w + dt[j * 32]; }
+  __device__ __forceinline__ float v_at(int j) const { return v[j * 32]; }
+};
+// A CSR run in device memory as noise_ahead's run.
+struct GlobalRun {
+  const int64_t* tp;
+  const float* vp;
+  int n;
+  __device__ __forceinline__ int64_t t(int j) const { return __ldg(tp + j); }
+  __device__ __forceinline__ float v_at(int j) const { return __ldg(vp + j); }
+};
+
 // x = ln(I / i_scale) at a sample of value v (PixelProc::x_at_sample on the caller's registers).
 __device__ __forceinline__ float x_sample(const PixelRegs& s, const PixelMapRegs& m, float v) {
   return log_f((m.dark + m.scale * v) / s.i_scale);
@@ -438,11 +520,12 @@ __device__ __forceinline__ void feed_segment(PixelRegs& s, const PixelMapRegs& m
     s.t_search = maxi(s.t_search, t1);
     return;
   }
+  const Segment g{t0, t1, v0, v1};
+  const bool fast = ((t1 - 1) >> kWindowLog2) == (t0 >> kWindowLog2);
   PixelRegs ts = s;
   PixelMapRegs tm = m;
   PixelCounters tc = c;
-  const bool fast = ((t1 - 1) >> kWindowLog2) == (t0 >> kWindowLog2);
-  cold_segment(&ts, &tm, kd, pixel, sink, &tc, Segment{t0, t1, v0, v1}, t0, t1, fast, x0, x1);
+  cold_segment(&ts, &tm, kd, pixel, sink, &tc, g, t0, t1, fast, x0, x1);
   s = ts;
   c = tc;
 }
@@ -566,6 +649,11 @@ __global__ void __launch_bounds__(32 * kRowsWarps) advance_rows_kernel(RowsArgs 
   float prev_v = s.held;
   const bool longrun = cnt > a.long_row;
 
+  // The short runs' noise candidates, all lanes together (a long run meets its candidates in the pixel model).
+  if (noise) {
+    const GlobalRun run{a.t + beg, a.irr + beg, cnt};
+    noise_ahead(s, m, a.k, p, valid && !longrun, a.t_state, s.held, a.t_end, run, c);
+  }
   // Short runs: one lane each.
   if (cnt > 0 && !longrun) {
     const int64_t* tp = a.t + beg;
@@ -1521,6 +1609,12 @@ __global__ void __launch_bounds__(128) engine_kernel_staged(EngineArgs a) {
         });
       }
       __syncwarp();
+      // Phase N: the window's noise candidates of all lanes together; the rejected ones leave the pixel model.
+      if (noise) {
+        const StagedRun run{t_w, &st_dt[warp][0][lane], &st_v[warp][0][lane], static_cast<int>(n) - 1};
+        noise_ahead(s, m, S.consts, p, have && n - 1 <= static_cast<uint32_t>(kStage), t_w,
+                    clamp_irr(carried, S.consts.irr_max), t_w + kWindowNs, run, c);
+      }
       // Phase B: the pixel model over the staged samples.
       if (have) {
         RegFeed feed{s, m, c, S.consts, &S.consts, p, sink, t_w, t_w, s.held, carried, 0.0f};
