@@ -499,17 +499,25 @@ __device__ __forceinline__ float x_sample(const PixelRegs& s, const PixelMapRegs
 // The pixel model's full path on a state in memory, out of line: the hot loops keep the state in registers and copy
 // it here only for a segment that is not clean. fast: PixelProc::segment_fast with x at both ends; else
 // PixelProc::segment over [from, to).
-template <class Sink>
+// kFlat: the processor's rare paths inline here, on copies the compiler can keep in registers (one large function:
+// the CSR kernel and the streaming engine); else they stay separate out-of-line functions working on the state in
+// memory (smaller code: the staged engine, whose instruction footprint sets its speed).
+template <class Sink, bool kFlat>
 __device__ __noinline__ void cold_segment(PixelRegs* s, const PixelMapRegs* m, const SensorConsts* k, uint32_t pixel,
                                           Sink sink, PixelCounters* c, Segment g, int64_t from, int64_t to, bool fast,
                                           float x0, float x1) {
-  PixelProc<Sink> proc{*s, *m, *k, pixel, sink, *c};
+  PixelRegs sl = *s;
+  const PixelMapRegs ml = *m;
+  PixelCounters cl = *c;
+  PixelProc<Sink, kFlat> proc{sl, ml, *k, pixel, sink, cl};
   if (fast) proc.segment_fast(g, x0, x1);
   else proc.segment(g, from, to);
+  *s = sl;
+  *c = cl;
 }
 
 // One segment [t0, t1) of a pixel whose state is in registers: the clean outcome in place, anything else out of line.
-template <class Sink>
+template <bool kFlat = true, class Sink>
 __device__ __forceinline__ void feed_segment(PixelRegs& s, const PixelMapRegs& m, const SensorConsts& k,
                                              const SensorConsts* kd, uint32_t pixel, const Sink& sink,
                                              PixelCounters& c, int64_t t0, int64_t t1, float v0, float v1, float x0,
@@ -525,7 +533,7 @@ __device__ __forceinline__ void feed_segment(PixelRegs& s, const PixelMapRegs& m
   PixelRegs ts = s;
   PixelMapRegs tm = m;
   PixelCounters tc = c;
-  cold_segment(&ts, &tm, kd, pixel, sink, &tc, g, t0, t1, fast, x0, x1);
+  cold_segment<Sink, kFlat>(&ts, &tm, kd, pixel, sink, &tc, g, t0, t1, fast, x0, x1);
   s = ts;
   c = tc;
 }
@@ -539,7 +547,8 @@ __device__ __forceinline__ void feed_held(PixelRegs& s, const PixelMapRegs& m, c
   PixelRegs ts = s;
   PixelMapRegs tm = m;
   PixelCounters tc = c;
-  cold_segment(&ts, &tm, kd, pixel, sink, &tc, Segment{t_from, kForever, v, v}, t_from, t_end, false, 0.0f, 0.0f);
+  cold_segment<Sink, true>(&ts, &tm, kd, pixel, sink, &tc, Segment{t_from, kForever, v, v}, t_from, t_end, false, 0.0f,
+                           0.0f);
   s = ts;
   c = tc;
 }
@@ -600,7 +609,7 @@ __device__ __forceinline__ void coop_run(PixelRegs& u, const PixelMapRegs& um, c
         PixelMapRegs tm = um;
         PixelCounters tc = cu;
         const bool fast = ((e - 1) >> kWindowLog2) == (t0 >> kWindowLog2);
-        cold_segment(&ts, &tm, a.kd, pixel, lz, &tc, Segment{t0, e, v0, v1}, t0, e, fast, x0, x1);
+        cold_segment<LaneZeroSink, true>(&ts, &tm, a.kd, pixel, lz, &tc, Segment{t0, e, v0, v1}, t0, e, fast, x0, x1);
         u = ts;
         cu = tc;
       }
@@ -1062,7 +1071,8 @@ struct WindowFeed {
 };
 
 // WindowFeed for a pixel whose state stays in the caller's registers (s, m, c): each segment's clean outcome is taken
-// in place, anything else out of line (feed_segment); the same samples and state as WindowFeed's.
+// in place, anything else out of line (feed_segment<kFlat>); the same samples and state as WindowFeed's.
+template <bool kFlat>
 struct RegFeed {
   PixelRegs& s;
   const PixelMapRegs& m;
@@ -1086,7 +1096,7 @@ struct RegFeed {
     const float vc = clamp_irr(v, k.irr_max);
     const int64_t t = t_w + dt;
     const float x1 = x_sample(s, m, vc);
-    feed_segment(s, m, k, kd, pixel, sink, c, prev_t, t, prev_v, vc, x_prev, x1);
+    feed_segment<kFlat>(s, m, k, kd, pixel, sink, c, prev_t, t, prev_v, vc, x_prev, x1);
     prev_t = t;
     prev_v = vc;
     x_prev = x1;
@@ -1129,7 +1139,7 @@ __global__ void __launch_bounds__(128) engine_kernel(EngineArgs a) {
       const BlobList list = warp_blob_list(f, have, x, y, t_w, t_w + kWindowNs, my_list);
       if (have) {
         const int level = field_level(f, list, x, y, t_w, a.r.l_min, a.r.l_max);
-        RegFeed feed{s, m, c, S.consts, &S.consts, p, sink, t_w, t_w, s.held, carried, 0.0f};
+        RegFeed<true> feed{s, m, c, S.consts, &S.consts, p, sink, t_w, t_w, s.held, carried, 0.0f};
         feed.start(carried);
         auto render = [&](uint32_t dt) { return field_eval(f, list, x, y, t_w + dt); };
         samples += sample_pixel_window(a.r, level, carried, false, render, feed);
@@ -1617,7 +1627,7 @@ __global__ void __launch_bounds__(128) engine_kernel_staged(EngineArgs a) {
       }
       // Phase B: the pixel model over the staged samples.
       if (have) {
-        RegFeed feed{s, m, c, S.consts, &S.consts, p, sink, t_w, t_w, s.held, carried, 0.0f};
+        RegFeed<false> feed{s, m, c, S.consts, &S.consts, p, sink, t_w, t_w, s.held, carried, 0.0f};
         feed.start(carried);
         if (n - 1 <= static_cast<uint32_t>(kStage)) {
           for (uint32_t k = 0; k + 1 < n; ++k) feed(st_dt[warp][k][lane], st_v[warp][k][lane]);

@@ -84,15 +84,20 @@ BS_HD uint8_t first_label(bool on, float ds, float dn, float l, float cut) {
   return (on ? D > 0.0f : D < 0.0f) ? split_label(ds, l, D, cut) : kLabelNoise;
 }
 
-// The next candidate of a noise chain after t (kForever without a rate).
-static BS_COLD int64_t noise_next(uint64_t seed, uint32_t purpose, uint32_t camera, uint32_t pixel, uint32_t n,
-                                  int64_t t, double rate_hz) {
+// The candidate after one at t whose successor's draw is w (word 0 its gap): kForever without a rate.
+BS_HD int64_t noise_after(const U4& w, int64_t t, double rate_hz) {
   if (!(rate_hz > 0.0)) return kForever;
-  const U4 w = draw(seed, purpose, camera, pixel, n);
   const double dt = -log_d(open_uniform_d(w.v[0])) / rate_hz * 1e9;
   const double step = ceil(dt);
   if (!(step < 9.0e18)) return kForever;
   return t + static_cast<int64_t>(step < 1.0 ? 1.0 : step);
+}
+
+// The next candidate of a noise chain after t (kForever without a rate): candidate n's draw gives its gap.
+static BS_COLD int64_t noise_next(uint64_t seed, uint32_t purpose, uint32_t camera, uint32_t pixel, uint32_t n,
+                                  int64_t t, double rate_hz) {
+  if (!(rate_hz > 0.0)) return kForever;
+  return noise_after(draw(seed, purpose, camera, pixel, n), t, rate_hz);
 }
 
 // One linear sample segment: [t0, t1) between two samples, or held from t0 on (t1 = kForever).
@@ -101,7 +106,16 @@ struct Segment {
   float v0, v1;
 };
 
-template <class Sink>
+// kFlat: the rare paths (fire, the search, the noise candidates, piece) inline into the caller, for a caller that is
+// itself out of line (cold_segment): there the state can stay in registers. Otherwise each is one out-of-line copy.
+// The input at t on segment g: linear between its samples in that operation order, held after the last one.
+BS_HOT float segment_value(const Segment& g, int64_t t) {
+  if (g.t1 == kForever) return g.v0;
+  const float f = static_cast<float>(t - g.t0) / static_cast<float>(g.t1 - g.t0);
+  return g.v0 + (g.v1 - g.v0) * f;
+}
+
+template <class Sink, bool kFlat = false>
 struct PixelProc {
   PixelRegs& s;
   const PixelMapRegs& m;
@@ -117,11 +131,7 @@ struct PixelProc {
   Segment pg{};
   int64_t p_t = 0, p_e = 0, p_lo = 0, p_stop = 0;
 
-  BS_HOT float value(const Segment& g, int64_t t) const {
-    if (g.t1 == kForever) return g.v0;
-    const float f = static_cast<float>(t - g.t0) / static_cast<float>(g.t1 - g.t0);
-    return g.v0 + (g.v1 - g.v0) * f;
-  }
+  BS_HOT float value(const Segment& g, int64_t t) const { return segment_value(g, t); }
   BS_HOT float current(const Segment& g, int64_t t) const { return m.dark + m.scale * value(g, t); }
   BS_HOT float log_ratio(float I) const { return log_f(I / s.i_scale); }
 
@@ -140,7 +150,15 @@ struct PixelProc {
   }
 
   // The event and the reset (pixel.h:1534-1588); label_override >= 0 labels a noise event.
-  BS_COLD void fire(int64_t t, bool on, float x, int label_override) {
+  BS_HD void fire(int64_t t, bool on, float x, int label_override) {
+    if constexpr (kFlat) {
+      fire_body(t, on, x, label_override);
+    } else {
+      fire_out(t, on, x, label_override);
+    }
+  }
+  BS_COLD void fire_out(int64_t t, bool on, float x, int label_override) { fire_body(t, on, x, label_override); }
+  BS_HD void fire_body(int64_t t, bool on, float x, int label_override) {
     const float ds = x - s.s3_ref;
     const float dn = 0.0f - s.n3_ref;
     const float l = m.leak * since_ref(t, s.t_ref);
@@ -190,7 +208,15 @@ struct PixelProc {
 
   // The first integer t in [lo, hi) where Delta fires (instant_search's time-ordered depth-first bisection,
   // pixel.h:1886-1916, with the exact node test above; each node carries x at its ends, one log per split).
-  BS_COLD bool search(const Segment& g, int64_t lo, int64_t hi, int64_t& t_hit, bool& on, float& x_hit) {
+  BS_HD bool search(const Segment& g, int64_t lo, int64_t hi, int64_t& t_hit, bool& on, float& x_hit) {
+    if constexpr (kFlat) {
+      return search_body(g, lo, hi, t_hit, on, x_hit);
+    } else {
+      return search_out(g, lo, hi, t_hit, on, x_hit);
+    }
+  }
+  BS_COLD bool search_out(const Segment& g, int64_t lo, int64_t hi, int64_t& t_hit, bool& on, float& x_hit) { return search_body(g, lo, hi, t_hit, on, x_hit); }
+  BS_HD bool search_body(const Segment& g, int64_t lo, int64_t hi, int64_t& t_hit, bool& on, float& x_hit) {
     float x = log_ratio(current(g, lo));
     float D = delta(lo, x);
     if (D >= m.theta_on || D <= -m.theta_off) {
@@ -241,7 +267,15 @@ struct PixelProc {
 
   // Is the earliest noise candidate (at tn) accepted by thinning (u1 < lambda(t) / lambda_max)? on: its polarity,
   // I: the photocurrent at tn. No side effects.
-  BS_COLD bool candidate_accepted(const Segment& g, int64_t tn, bool& on, float& I) const {
+  BS_HD bool candidate_accepted(const Segment& g, int64_t tn, bool& on, float& I) const {
+    if constexpr (kFlat) {
+      return candidate_accepted_body(g, tn, on, I);
+    } else {
+      return candidate_accepted_out(g, tn, on, I);
+    }
+  }
+  BS_COLD bool candidate_accepted_out(const Segment& g, int64_t tn, bool& on, float& I) const { return candidate_accepted_body(g, tn, on, I); }
+  BS_HD bool candidate_accepted_body(const Segment& g, int64_t tn, bool& on, float& I) const {
     const bool shot = s.t_shot <= s.t_ba;
     const U4 w = draw(k.seed, shot ? kPurposeShot : kPurposeBackground, k.camera, pixel, shot ? s.n_shot : s.n_ba);
     I = current(g, tn);
@@ -251,7 +285,15 @@ struct PixelProc {
   }
 
   // Moves the earliest candidate's chain (the one at tn) on to its next candidate.
-  BS_COLD void advance_chain(int64_t tn) {
+  BS_HD void advance_chain(int64_t tn) {
+    if constexpr (kFlat) {
+      advance_chain_body(tn);
+    } else {
+      advance_chain_out(tn);
+    }
+  }
+  BS_COLD void advance_chain_out(int64_t tn) { advance_chain_body(tn); }
+  BS_HD void advance_chain_body(int64_t tn) {
     ++c.noise_candidates;
     const bool shot = s.t_shot <= s.t_ba;
     const uint32_t purpose = shot ? kPurposeShot : kPurposeBackground;
@@ -268,7 +310,15 @@ struct PixelProc {
   }
 
   // Drops the earliest noise candidate (refractory or dead time) or tests and fires it; advances its chain.
-  BS_COLD void noise_candidate(const Segment& g, int64_t tn, bool blind) {
+  BS_HD void noise_candidate(const Segment& g, int64_t tn, bool blind) {
+    if constexpr (kFlat) {
+      noise_candidate_body(g, tn, blind);
+    } else {
+      noise_candidate_out(g, tn, blind);
+    }
+  }
+  BS_COLD void noise_candidate_out(const Segment& g, int64_t tn, bool blind) { noise_candidate_body(g, tn, blind); }
+  BS_HD void noise_candidate_body(const Segment& g, int64_t tn, bool blind) {
     bool on = false;
     float I = 0.0f;
     const bool fires = !blind && candidate_accepted(g, tn, on, I);
@@ -277,7 +327,15 @@ struct PixelProc {
   }
 
   // One piece [t, e) inside segment g (advance_instant's inner loop), with the noise candidates it holds.
-  BS_COLD void piece(const Segment& g, int64_t t, int64_t e) {
+  BS_HD void piece(const Segment& g, int64_t t, int64_t e) {
+    if constexpr (kFlat) {
+      piece_body(g, t, e);
+    } else {
+      piece_out(g, t, e);
+    }
+  }
+  BS_COLD void piece_out(const Segment& g, int64_t t, int64_t e) { piece_body(g, t, e); }
+  BS_HD void piece_body(const Segment& g, int64_t t, int64_t e) {
     ++c.pieces;
     for (;;) {
       const int64_t tn = k.noise ? mini(s.t_shot, s.t_ba) : kForever;

@@ -66,7 +66,8 @@ def _check_light_groups(light_groups) -> int:
 
 
 def new_columns(n: int) -> dict:
-    return {name: np.zeros(n, dt) for name, dt in EVENT_COLUMNS}
+    """Fresh host columns for n events; every element is written by the library (so not zero-filled first)."""
+    return {name: np.empty(n, dt) for name, dt in EVENT_COLUMNS}
 
 
 def column_struct(cols: dict, with_pixel: np.ndarray | None = None) -> _lib.EventColumns:
