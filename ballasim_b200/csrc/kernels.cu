@@ -1860,9 +1860,14 @@ __global__ void __launch_bounds__(128) engine_kernel_coop(EngineArgs a) {
         });
       }
       __syncwarp();
+      const bool staged = have && n - 1 <= static_cast<uint32_t>(kStage);
+      // The window's noise candidates of all lanes together; the rejected ones leave the pixel model.
+      if (noise) {
+        const StagedRun run{t_w, &st_dt[warp][0][lane], &st_v[warp][0][lane], static_cast<int>(n) - 1};
+        noise_ahead(s, m, S.consts, p, staged, t_w, clamp_irr(carried, S.consts.irr_max), t_w + kWindowNs, run, c);
+      }
       // Phase B, the warp together.
       WindowFeed feed{&proc, t_w, S.consts.irr_max, t_w, s.held, carried, 0.0f};
-      const bool staged = have && n - 1 <= static_cast<uint32_t>(kStage);
       if (staged) feed.start(carried);
       proc.defer = true;
       uint32_t next = 0;

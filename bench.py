@@ -14,7 +14,8 @@ time.
 
 The runs_* workloads take the reference engine's own two-kernel route instead (Camera::sample_and_sense): per
 sensor and window, sample_window on the device writes CSR runs to HBM and SensorModel::advance_device reads them
-(ballasim_b200.windows); the roofline line is then the pixel model on the runs (advance_runs_kernel).
+(ballasim_b200.windows); the roofline line is then the pixel model on the runs (advance_rows_kernel, or
+advance_runs_kernel with --block).
 
 --impl reference times the reference's own CPU implementation (oracle/_ref: WindowEngine<kHost> and
 SensorModel fp32 on every host core) on a bounded sample of the same workload (the first windows of every
@@ -72,6 +73,15 @@ L2_BYTES = 126 * 1024 * 1024
 NCU = {
     "blobs16_346x260": {"kernel": "engine_kernel_coop", "stage": 64, "tile_width": 8, "traffic": 8.74e6 + 4.56e6,
                         "inst_per_sample": None, "issue_active": 0.285},
+    # traffic: one pass on the full 60-window launch; instructions and issue-active: the full set on its first 4
+    # windows (74,251,870 pixel-samples, 3.329e9 warp instructions).
+    "six_sensors_4.6Mpx": {"kernel": "engine_kernel_staged<16>", "stage": 16, "tile_width": 8,
+                           "traffic": 690.74e6 + 3.59e9, "inst_per_sample": 3.329e9 / 74251870,
+                           "issue_active": 0.209},
+    # The runs path: its six advance_rows_kernel launches of one window (one per sensor), DRAM bytes against the
+    # window's algorithmic bytes (836.3 MB read + 325.6 MB written; 833.9 MB).
+    "runs:six_sensors_4.6Mpx": {"kernel": "advance_rows_kernel", "dram_per_alg_byte": (836.32e6 + 325.60e6) / 833.92e6,
+                                "capture": "advance_rows_kernel, the six sensors' first window (6 launches, one pass)"},
 }
 FALLBACK_HBM_GBS = 6650.0
 
@@ -318,8 +328,8 @@ def run_ours(args, rank: int, world: int) -> dict | None:
 def run_runs(args, rank: int, world: int) -> dict | None:
     """The reference engine's route with the runs in HBM (ballasim_b200.windows.DeviceWindows): per window and
     sensor, the levels, sample_window on the device (count pass, scan, write pass) and advance_device (scatter of the
-    rows, advance_runs_kernel); the events stay on the device. Kernel time of the pixel model from CUDA events around
-    each advance_runs_kernel launch."""
+    rows, advance_rows_kernel); the events stay on the device. Kernel time of the pixel model from CUDA events around
+    each advance launch."""
     import torch
     import torch.distributed as dist
 
@@ -411,7 +421,10 @@ def run_runs(args, rank: int, world: int) -> dict | None:
     n_launch = advance_launches / args.steps
     alg = b_sense(wl.pixels, wl.windows, int(per_step_samples), int(per_step_events))
     achieved = alg / (kms_total * 1e-3) / 1e9
+    kname = "advance_runs_kernel" if args.block else "advance_rows_kernel"
     cap = NCU.get("runs:" + wl.name)
+    if cap is not None and cap["kernel"] != kname:
+        cap = None
     calls = wl.windows * len(wl.sensors)
     return {
         "metric": METRIC, "value": samples_all / (total_ms_all * 1e-3), "unit": "pixel-samples/s",
@@ -424,13 +437,20 @@ def run_runs(args, rank: int, world: int) -> dict | None:
                    "path": "sample_window (device) -> runs in HBM -> advance_device, per sensor and window",
                    "parallelism": f"replicas x{world}", "advance_block": args.block or "row-major",
                    "long_run": args.long_run or 32},
-        "gpu_launches": 9 * calls * args.steps + 2 * len(wl.sensors) * args.steps,
+        # Per sensor and window: levels, the input check, two sample_window passes, three scan kernels and the pixel
+        # model (advance_rows_kernel; every pixel is listed, so no advance_unlisted_kernel; --block adds the scatter);
+        # per sensor and step the first frame and init.
+        "gpu_launches": (8 + (1 if args.block else 0)) * calls * args.steps + 2 * len(wl.sensors) * args.steps,
         "clocks": clocks,
         "e2e": {"value": samples_all / e2e_s if e2e_times else None, "unit": "pixel-samples/s",
                 "h2d_bytes_per_step": sum(int(f.nbytes) for f in frames), "d2h_bytes_per_step": d2h},
-        "roofline": {"kernel": "advance_runs_kernel (the pixel model on CSR runs read from HBM)", "bound": "hbm",
+        "roofline": {"kernel": kname + " (the pixel model on CSR runs read from HBM)", "bound": "hbm",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "peak_kind": hbm_kind, "traffic": cap["traffic"] if cap else None,
+                     "peak_kind": hbm_kind,
+                     # DRAM bytes of an average launch: the capture's DRAM bytes per algorithmic byte (its launches
+                     # summed) times this run's algorithmic bytes per launch.
+                     "traffic": cap["dram_per_alg_byte"] * alg / n_launch if cap and n_launch else None,
+                     "traffic_capture": cap["capture"] if cap else None,
                      "algorithmic_bytes_per_step": alg, "launches_per_step": n_launch,
                      "kernel_ms_per_step": kms_total, "share_of_step": kms_total / (total_ms_all / args.steps)},
     }
