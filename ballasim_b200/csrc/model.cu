@@ -608,7 +608,7 @@ struct Model {
       CK(cudaMemsetAsync(counters.p, 0, kCntWords * sizeof(unsigned long long), s));
       const EventBuf evb{events.p, static_cast<unsigned long long>(event_cap)};
       if (!k.cascade && block == 0) {
-        // The instantaneous response: row-major over the runs, the samples staged per warp.
+        // The instantaneous response: row-major over the runs, long runs walked by the whole warp.
         CK(cudaMemsetAsync(listed.p, 0, ((n + 31) / 32) * sizeof(uint32_t), s));
         k_dev.ensure(1);
         CK(cudaMemcpyAsync(k_dev.p, &k, sizeof(SensorConsts), cudaMemcpyHostToDevice, s));

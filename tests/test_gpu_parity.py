@@ -35,7 +35,7 @@ def same_events(dev: dict, ora: dict, width: int) -> None:
 ])
 def test_pixel_model_on_random_runs(cuda_lib, oracle_port, overrides, block):
     """The pixel model on random ragged runs (random pixel subsets in random order) against the oracle: the
-    row-major kernel with staged samples (block 0) and the one-thread-per-pixel kernel (block 128)."""
+    row-major kernel (block 0) and the one-thread-per-pixel kernel (block 128)."""
     from ballasim_b200.sensor import SensorModel
 
     rng = np.random.default_rng(17 + len(overrides))
@@ -119,6 +119,54 @@ def test_row_major_kernel_on_every_run_layout(cuda_lib, oracle_port, layout, lon
     merged = {k: np.concatenate([g[k] for g in got]) for k in got[0]}
     same_events(merged, ora.take_events(), Wd)
     assert len(merged["t_cross_ns"]) > 50
+
+
+@pytest.mark.parametrize("t_off,v_off", [(0, 0), (1, 1), (0, 2), (1, 3)])
+def test_row_major_kernel_reads_device_runs_at_any_alignment(cuda_lib, oracle_port, t_off, v_off):
+    """advance_device on CSR arrays that start t_off int64 and v_off float elements past a 16-byte boundary (a
+    caller's sub-buffers) against the oracle."""
+    import torch
+
+    from ballasim_b200 import _lib
+    from ballasim_b200.sensor import SensorModel
+
+    rng = np.random.default_rng(40 + 4 * t_off + v_off)
+    Wd, Hd = 36, 20
+    n = Wd * Hd
+    p = resolve("ideal", {**W.MISMATCH, **W.NOISE, "noise_shot_rate_hz": 20.0, "leak_rate_hz": 1.0})
+    dev = SensorModel(p, Wd, Hd, 8, [{"type": "constant"}], 0)
+    ora = oracle_port.Model(p, Wd, Hd, 8, 0)
+    irr0 = rng.uniform(20, 300, n).astype(np.float32)
+    dev.init(0, irr0.reshape(n, 1))
+    ora.init(0, irr0)
+    got, t = [], 0
+    ids = np.arange(n, dtype=np.uint32)
+    for call in range(3):
+        t_end = t + (1 << 23)
+        runs = [np.unique(rng.integers(t + 1, t_end + 1, int(k))).astype(np.int64)
+                for k in rng.integers(0, 12, n)]
+        cnt = np.array([len(r) for r in runs], np.int32)
+        starts = np.concatenate([[0], np.cumsum(cnt)[:-1]]).astype(np.int64)
+        tt = np.concatenate(runs)
+        vv = np.concatenate([(100 * np.exp(np.cumsum(rng.normal(0, 0.08, len(r))))).astype(np.float32)
+                             for r in runs])
+        d_t = torch.zeros(len(tt) + 2, dtype=torch.int64, device="cuda")
+        d_v = torch.zeros(len(vv) + 4, dtype=torch.float32, device="cuda")
+        d_t[t_off:t_off + len(tt)] = torch.from_numpy(tt).cuda()
+        d_v[v_off:v_off + len(vv)] = torch.from_numpy(vv).cuda()
+        d_ids = torch.from_numpy(ids.astype(np.int32)).cuda()
+        d_start = torch.from_numpy(starts).cuda()
+        d_cnt = torch.from_numpy(cnt).cuda()
+        r = _lib.DeviceRuns(d_ids.data_ptr(), d_start.data_ptr(), d_cnt.data_ptr(), n,
+                            d_t.data_ptr() + 8 * t_off, d_v.data_ptr() + 4 * v_off, len(tt))
+        torch.cuda.synchronize()
+        ev = dev.advance_device(r, t_end, 1)
+        got.append(dev.download_events(ev))
+        ora.advance_runs(ids, tt, vv, starts, cnt, t_end)
+        t = t_end
+    merged = {k: np.concatenate([g[k] for g in got]) for k in got[0]}
+    same_events(merged, ora.take_events(), Wd)
+    assert len(merged["t_cross_ns"]) > 20
 
 
 def test_advance_rectangular_and_ragged_forms_agree(cuda_lib):
