@@ -265,6 +265,7 @@ struct TrainArgs {
   // Expectile weight tau: a row's squared error counts 2 tau when the net predicts below its target and
   // 2 (1 - tau) above it (0.5: the plain mean squared error).
   float tau;
+  unsigned int* err;  // set when a tensor-core chain's completion was not seen within the wait's bound
 };
 int train_grid(uint32_t rows);
 void launch_train_partials(const TrainArgs& a, cudaStream_t stream);

@@ -1,10 +1,11 @@
 // Training of the learned step proposal on the GPU: the walk that turns the plain sampler's runs into
-// (history, step) pairs, the fused forward + backward pass on the tensor cores (mma.sync m16n8k16, BF16 operands,
-// FP32 accumulators), Adam, and the batch forward pass. No reference counterpart (this project's own method).
+// (history, step) pairs, the fused forward + backward pass on the 5th-generation tensor cores (tcgen05.mma, BF16
+// operands from shared memory, FP32 accumulators in tensor memory), Adam, and the batch forward pass. No reference
+// counterpart (this project's own method).
 //
-// One training step = train_partials_kernel (grid = rows / 128 CTAs of 4 warps; each warp runs 32 rows forward
-// and back, then the CTA forms its weight gradients over its 128 rows with two more mma passes and writes them as
-// one partial row) + adam_kernel (sums the partial rows in a fixed order, so a step is deterministic, and updates
+// One training step = train_partials_kernel (grid = rows / 128 CTAs of 4 warps, one thread per row; the CTA runs
+// its 128 rows forward and back and forms its weight gradients over them, five tcgen05 chains in all, and writes them
+// as one partial row) + adam_kernel (sums the partial rows in a fixed order, so a step is deterministic, and updates
 // the FP32 masters and their BF16 operand copies). The step counter lives in device memory, so a run of steps can
 // be replayed from a CUDA graph.
 #include <cooperative_groups.h>
@@ -99,48 +100,203 @@ __global__ void __launch_bounds__(128) walk_pairs_kernel(WalkArgs a) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// training step
+// training step on the 5th-generation tensor cores
 // ---------------------------------------------------------------------------------------------
+// A CTA takes 128 rows of the batch, one thread per row; each of its five contractions is one tcgen05.mma chain of
+// M = 128 (the rows, or for the weight gradients the weight's rows padded to 128), N = 64, K = 16 per instruction,
+// BF16 operands from shared memory and an FP32 accumulator in tensor memory (TMEM lane t = the tile's row t, so
+// thread t reads its own row back with tcgen05.ld):
+//   H1 = relu(X W1 + b1)          X [128 x 16],   W1^T [64 x 16]   (both K-major)
+//   H2 = relu(H1 W2 + b2)         H1 [128 x 64],  W2^T [64 x 64]   (K-major); y = H2 w3 + b3 per thread
+//   dH1 = (dH2 W2^T) * [H1 > 0]   dH2 [128 x 64], W2 [64 x 64]     (K-major)
+//   dW2 = H1^T dH2, dW1 = X^T dH1 over the 128 rows               (the same tiles read MN-major)
+// One thread (tid 0) issues each chain and commits it to an mbarrier that the CTA waits on; the bias and w3
+// gradients and the loss are column sums over the rows, taken in a fixed order (shuffles within each warp, then
+// the four warps), so a step is deterministic. BF16 rounding happens where the mma.sync form rounded (X, H1, dH2, dH1 and the weights).
+//
+// Tiles use the tensor core's canonical no-swizzle layout: a [rows][cols] BF16 matrix in core matrices of 8 rows x 8
+// columns (16 bytes a row, 128 contiguous bytes), core (rb, cb) at byte (rb * cols / 8 + cb) * 128. Read with K
+// along the columns (K-major) the descriptor's leading offset is 128 (the next 8 columns) and its stride offset
+// cols * 16 (the next 8 rows); read with K along the rows (MN-major, for the transposed operands) the same bytes have
+// stride offset 128 and leading offset cols * 16.
 constexpr int kRowsPerCta = 128;
-constexpr int kST = kRowsPerCta + 8;  // stride (u16) of the transposed activation tiles [feature][row]
+constexpr int kMmaWaitLimit = 1 << 20;  // mbarrier polls before a wait gives up (the step's error word is set)
 
-struct TrainShared {
-  uint16_t w1t[kMlpHid * kSW1];
-  uint16_t w2t[kMlpHid * kSW2];
-  uint16_t w2n[kMlpHid * kSW2];
+__host__ __device__ constexpr uint32_t tile_off(int r, int c, int cols) {
+  return static_cast<uint32_t>(((r >> 3) * (cols >> 3) + (c >> 3)) * 128 + (r & 7) * 16 + (c & 7) * 2);
+}
+
+// The transposed reads with M = 128 run past a tile whose M is smaller (X^T: 16 rows, H1^T: 64 rows) into the next
+// member, which is why x is followed by w1t and h1 by dh2; those accumulator rows are never read.
+struct __align__(128) TrainTiles {
+  uint8_t x[kRowsPerCta * kMlpIn * 2];    // X [r][f]
+  uint8_t w1t[kMlpHid * kMlpIn * 2];      // W1^T [h][f]
+  uint8_t h1[kRowsPerCta * kMlpHid * 2];  // H1 [r][h]
+  uint8_t dh2[kRowsPerCta * kMlpHid * 2]; // dH2 [r][o]
+  uint8_t dh1[kRowsPerCta * kMlpHid * 2]; // dH1 [r][h]
+  uint8_t w2t[kMlpHid * kMlpHid * 2];     // W2^T [o][h]
+  uint8_t w2n[kMlpHid * kMlpHid * 2];     // W2 [h][o]
+  float part[3][4][kMlpHid];             // per warp: the db2, dW3 and db1 column sums of its 32 rows
   float b1[kMlpHid], b2[kMlpHid], w3[kMlpHid];
   float b3;
-  uint16_t xt[kMlpIn * kST];
-  uint16_t h1t[kMlpHid * kST];
-  uint16_t dh2t[kMlpHid * kST];
-  uint16_t dh1t[kMlpHid * kST];
-  float wsum[4][3][kMlpHid];  // per warp: db1, db2, dW3 column sums
   float wdb3[4];
   double wloss[4];
+  unsigned long long bar;
+  uint32_t tmem;
 };
+static_assert(offsetof(TrainTiles, w1t) == sizeof(TrainTiles::x) && offsetof(TrainTiles, dh2) ==
+              offsetof(TrainTiles, h1) + sizeof(TrainTiles::h1), "the transposed reads' overrun targets");
+static_assert(offsetof(TrainTiles, w1t) + sizeof(TrainTiles::w1t) >= 15 * 128 + 7 * 512 + 256 + 128,
+              "X^T's overrun stays inside w1t");
+static_assert(offsetof(TrainTiles, h1) % 128 == 0 && offsetof(TrainTiles, dh1) % 128 == 0 &&
+              offsetof(TrainTiles, w2t) % 128 == 0 && offsetof(TrainTiles, w2n) % 128 == 0 &&
+              offsetof(TrainTiles, bar) % 8 == 0, "tile alignment");
 
-__device__ __forceinline__ uint16_t lo16(uint32_t r) { return static_cast<uint16_t>(r & 0xffffu); }
-__device__ __forceinline__ uint16_t hi16(uint32_t r) { return static_cast<uint16_t>(r >> 16); }
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
 
-__global__ void __launch_bounds__(128) train_partials_kernel(TrainArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  TrainShared& S = *reinterpret_cast<TrainShared*>(smem_raw);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, q = lane & 3;
-  for (int i = tid; i < kMlpHid * kMlpIn; i += blockDim.x) S.w1t[(i / kMlpIn) * kSW1 + i % kMlpIn] = a.ops[kOpW1t + i];
-  for (int i = tid; i < kMlpHid * kMlpHid; i += blockDim.x) {
-    S.w2t[(i / kMlpHid) * kSW2 + i % kMlpHid] = a.ops[kOpW2t + i];
-    S.w2n[(i / kMlpHid) * kSW2 + i % kMlpHid] = a.ops[kOpW2n + i];
+// A shared-memory matrix descriptor: no swizzle, version 1 (bits 46-47), the start and both offsets in 16-byte
+// units.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16) |
+         (static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32) | (uint64_t{1} << 46);
+}
+
+// The instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1), BF16 A and B (bits 7-9, 10-12 = 1),
+// A and B major (bits 15, 16: 0 K-major, 1 MN-major), N / 8 (bits 17-22), M / 16 (bits 24-28); M = 128, N = 64.
+__host__ __device__ constexpr uint32_t umma_idesc(bool mn_major) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (mn_major ? (1u << 15) | (1u << 16) : 0u) | ((64u >> 3) << 17) |
+         ((128u >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      :
+      : "r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(unsigned long long* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// This thread's shared-memory writes made visible to the tensor core (the async proxy).
+__device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Polls the barrier's phase of the given parity; false after kMmaWaitLimit polls.
+__device__ __forceinline__ bool bar_wait(unsigned long long* bar, uint32_t parity) {
+  const uint32_t b = smem_u32(bar);
+  for (int i = 0; i < kMmaWaitLimit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(b), "r"(parity)
+        : "memory");
+    if (done) return true;
   }
-  for (int i = tid; i < kMlpHid; i += blockDim.x) {
-    S.b1[i] = a.params[kOffB1 + i];
-    S.b2[i] = a.params[kOffB2 + i];
-    S.w3[i] = bf16_f(a.ops[kOpW3 + i]);
-  }
-  if (tid == 0) S.b3 = a.params[kOffB3];
-  __syncthreads();
+  return false;
+}
 
-  // This lane's row: local row 32 warp + lane of the CTA.
-  const uint32_t gi = blockIdx.x * kRowsPerCta + warp * 32 + lane;
+// Waits for the chain committed to the barrier's phase; a wait that gives up sets the error word and waits once more
+// (the chain's TMEM must not be freed under it).
+__device__ __forceinline__ void chain_wait(unsigned long long* bar, uint32_t parity, unsigned int* err) {
+  if (!bar_wait(bar, parity)) {
+    if (threadIdx.x == 0) atomicOr(err, 1u);
+    bar_wait(bar, parity);
+  }
+  tc_fence_after();
+}
+
+// 16 FP32 columns of this thread's TMEM lane (the warp's 32 lanes, starting at column col of taddr).
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+      "[%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+// 64 FP32 columns of this thread's lane.
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float (&v)[64]) {
+  tmem_ld16(taddr, v);
+  tmem_ld16(taddr + 16, v + 16);
+  tmem_ld16(taddr + 32, v + 32);
+  tmem_ld16(taddr + 48, v + 48);
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Row t of a [rows][64] tile from 32 packed BF16 pairs.
+__device__ __forceinline__ void store_row64(uint8_t* tile, int t, const uint32_t (&p)[32]) {
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    *reinterpret_cast<uint4*>(tile + tile_off(t, 8 * j, kMlpHid)) =
+        make_uint4(p[4 * j], p[4 * j + 1], p[4 * j + 2], p[4 * j + 3]);
+  }
+}
+
+// The warp's column sums of v (64 columns, one row per lane), reduced and scattered: halving exchanges with the
+// lanes 16, 8, 4, 2 and 1 apart, each lane keeping the half its lane bit selects, leave lane l the sums of columns
+// 2l and 2l + 1 in v[0] and v[1] (a fixed order, so the sums are deterministic).
+__device__ __forceinline__ void warp_column_sums(float (&v)[64], int lane) {
+#pragma unroll
+  for (int s = 16, n = 64; s >= 1; s >>= 1, n >>= 1) {
+    const bool up = (lane & s) != 0;
+#pragma unroll
+    for (int i = 0; i < n / 2; ++i) {
+      const float keep = up ? v[i + n / 2] : v[i], send = up ? v[i] : v[i + n / 2];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, s);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128, 1) train_partials_kernel(TrainArgs a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  TrainTiles& S = *reinterpret_cast<TrainTiles*>(smem_raw);
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  if (warp == 0) {  // 128 TMEM columns: two 64-column accumulators
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem)),
+                 "r"(128u)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&S.bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // The operands of the weights (BF16, row-major in ops) into their tiles.
+  {
+    const int h = t >> 1, j = t & 1;
+    *reinterpret_cast<uint4*>(S.w1t + tile_off(h, 8 * j, kMlpIn)) =
+        *reinterpret_cast<const uint4*>(a.ops + kOpW1t + h * kMlpIn + 8 * j);
+  }
+  for (int q = t; q < kMlpHid * 8; q += kRowsPerCta) {
+    const int r = q >> 3, j = q & 7;
+    *reinterpret_cast<uint4*>(S.w2t + tile_off(r, 8 * j, kMlpHid)) =
+        *reinterpret_cast<const uint4*>(a.ops + kOpW2t + r * kMlpHid + 8 * j);
+    *reinterpret_cast<uint4*>(S.w2n + tile_off(r, 8 * j, kMlpHid)) =
+        *reinterpret_cast<const uint4*>(a.ops + kOpW2n + r * kMlpHid + 8 * j);
+  }
+  if (t < kMlpHid) {
+    S.b1[t] = a.params[kOffB1 + t];
+    S.b2[t] = a.params[kOffB2 + t];
+    S.w3[t] = bf16_f(a.ops[kOpW3 + t]);
+  }
+  if (t == 0) S.b3 = a.params[kOffB3];
+
+  // This thread's row.
+  const uint32_t gi = blockIdx.x * kRowsPerCta + t;
   uint64_t idx = 0;
   bool valid = false;
   if (a.sampled) {
@@ -153,201 +309,178 @@ __global__ void __launch_bounds__(128) train_partials_kernel(TrainArgs a) {
     valid = gi < a.n;
     idx = gi;
   }
-  float dw3[8][2], db2[8][2], db1[8][2];
+  {
+    uint32_t xw[8];
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    dw3[j][0] = dw3[j][1] = db2[j][0] = db2[j][1] = db1[j][0] = db1[j][1] = 0.0f;
+    for (int k = 0; k < 8; ++k) xw[k] = valid ? ld32(a.x + idx * kMlpIn + 2 * k) : 0u;
+    *reinterpret_cast<uint4*>(S.x + tile_off(t, 0, kMlpIn)) = make_uint4(xw[0], xw[1], xw[2], xw[3]);
+    *reinterpret_cast<uint4*>(S.x + tile_off(t, 8, kMlpIn)) = make_uint4(xw[4], xw[5], xw[6], xw[7]);
   }
-  float sdy = 0.0f;
-  double sloss = 0.0;
-#pragma unroll 1
-  for (int mt = 0; mt < 2; ++mt) {
-    const int r0 = mt * 16 + g, r1 = r0 + 8;  // warp-local rows
-    const uint64_t i0 = __shfl_sync(0xffffffffu, idx, r0), i1 = __shfl_sync(0xffffffffu, idx, r1);
-    const bool v0 = __shfl_sync(0xffffffffu, valid, r0), v1 = __shfl_sync(0xffffffffu, valid, r1);
-    const int c0 = warp * 32 + r0, c1 = warp * 32 + r1;  // CTA-local rows
-    uint32_t ax[4];
-    ax[0] = v0 ? ld32(a.x + i0 * kMlpIn + 2 * q) : 0u;
-    ax[1] = v1 ? ld32(a.x + i1 * kMlpIn + 2 * q) : 0u;
-    ax[2] = v0 ? ld32(a.x + i0 * kMlpIn + 2 * q + 8) : 0u;
-    ax[3] = v1 ? ld32(a.x + i1 * kMlpIn + 2 * q + 8) : 0u;
-    S.xt[(2 * q) * kST + c0] = lo16(ax[0]);
-    S.xt[(2 * q + 1) * kST + c0] = hi16(ax[0]);
-    S.xt[(2 * q) * kST + c1] = lo16(ax[1]);
-    S.xt[(2 * q + 1) * kST + c1] = hi16(ax[1]);
-    S.xt[(2 * q + 8) * kST + c0] = lo16(ax[2]);
-    S.xt[(2 * q + 9) * kST + c0] = hi16(ax[2]);
-    S.xt[(2 * q + 8) * kST + c1] = lo16(ax[3]);
-    S.xt[(2 * q + 9) * kST + c1] = hi16(ax[3]);
-    // layer 1
-    uint32_t h1[4][4];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const float bb0 = S.b1[8 * j + 2 * q], bb1 = S.b1[8 * j + 2 * q + 1];
-      float c[4] = {bb0, bb1, bb0, bb1};
-      mma_bf16(c, ax, ld32(S.w1t + (8 * j + g) * kSW1 + 2 * q), ld32(S.w1t + (8 * j + g) * kSW1 + 2 * q + 8));
-      const uint32_t top = pack2(fmaxf(c[0], 0.0f), fmaxf(c[1], 0.0f));
-      const uint32_t bot = pack2(fmaxf(c[2], 0.0f), fmaxf(c[3], 0.0f));
-      h1[j >> 1][(j & 1) * 2 + 0] = top;
-      h1[j >> 1][(j & 1) * 2 + 1] = bot;
-      S.h1t[(8 * j + 2 * q) * kST + c0] = lo16(top);
-      S.h1t[(8 * j + 2 * q + 1) * kST + c0] = hi16(top);
-      S.h1t[(8 * j + 2 * q) * kST + c1] = lo16(bot);
-      S.h1t[(8 * j + 2 * q + 1) * kST + c1] = hi16(bot);
-    }
-    // layer 2 and the output
-    uint32_t h2[8][2];
-    float y0 = 0.0f, y1 = 0.0f;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const float bb0 = S.b2[8 * j + 2 * q], bb1 = S.b2[8 * j + 2 * q + 1];
-      float c[4] = {bb0, bb1, bb0, bb1};
-#pragma unroll
-      for (int kk = 0; kk < 4; ++kk) {
-        mma_bf16(c, h1[kk], ld32(S.w2t + (8 * j + g) * kSW2 + 16 * kk + 2 * q),
-                 ld32(S.w2t + (8 * j + g) * kSW2 + 16 * kk + 2 * q + 8));
-      }
-      h2[j][0] = pack2(fmaxf(c[0], 0.0f), fmaxf(c[1], 0.0f));
-      h2[j][1] = pack2(fmaxf(c[2], 0.0f), fmaxf(c[3], 0.0f));
-      const float w30 = S.w3[8 * j + 2 * q], w31 = S.w3[8 * j + 2 * q + 1];
-      y0 = y0 + lo_f(h2[j][0]) * w30;
-      y0 = y0 + hi_f(h2[j][0]) * w31;
-      y1 = y1 + lo_f(h2[j][1]) * w30;
-      y1 = y1 + hi_f(h2[j][1]) * w31;
-    }
-    y0 += __shfl_xor_sync(0xffffffffu, y0, 1);
-    y1 += __shfl_xor_sync(0xffffffffu, y1, 1);
-    y0 += __shfl_xor_sync(0xffffffffu, y0, 2);
-    y1 += __shfl_xor_sync(0xffffffffu, y1, 2);
-    y0 += S.b3;
-    y1 += S.b3;
-    const float e0 = v0 ? y0 - a.y[i0] : 0.0f, e1 = v1 ? y1 - a.y[i1] : 0.0f;
-    const float w0 = 2.0f * (e0 < 0.0f ? a.tau : 1.0f - a.tau), w1 = 2.0f * (e1 < 0.0f ? a.tau : 1.0f - a.tau);
-    const float dy0 = w0 * e0 * a.inv_rows, dy1 = w1 * e1 * a.inv_rows;
-    if (q == 0) {
-      sloss += static_cast<double>(w0) * e0 * e0 + static_cast<double>(w1) * e1 * e1;
-      sdy += dy0 + dy1;
-    }
-    // dH2 = dy W3^T masked by ReLU; the dW3 and db2 column sums
-    uint32_t da[4][4];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const float w30 = S.w3[8 * j + 2 * q], w31 = S.w3[8 * j + 2 * q + 1];
-      const float h00 = lo_f(h2[j][0]), h01 = hi_f(h2[j][0]), h10 = lo_f(h2[j][1]), h11 = hi_f(h2[j][1]);
-      const float d00 = h00 > 0.0f ? dy0 * w30 : 0.0f, d01 = h01 > 0.0f ? dy0 * w31 : 0.0f;
-      const float d10 = h10 > 0.0f ? dy1 * w30 : 0.0f, d11 = h11 > 0.0f ? dy1 * w31 : 0.0f;
-      dw3[j][0] += h00 * dy0 + h10 * dy1;
-      dw3[j][1] += h01 * dy0 + h11 * dy1;
-      db2[j][0] += d00 + d10;
-      db2[j][1] += d01 + d11;
-      const uint32_t top = pack2(d00, d01), bot = pack2(d10, d11);
-      da[j >> 1][(j & 1) * 2 + 0] = top;
-      da[j >> 1][(j & 1) * 2 + 1] = bot;
-      S.dh2t[(8 * j + 2 * q) * kST + c0] = lo16(top);
-      S.dh2t[(8 * j + 2 * q + 1) * kST + c0] = hi16(top);
-      S.dh2t[(8 * j + 2 * q) * kST + c1] = lo16(bot);
-      S.dh2t[(8 * j + 2 * q + 1) * kST + c1] = hi16(bot);
-    }
-    // dH1 = dH2 W2^T masked by ReLU; the db1 column sums
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-#pragma unroll
-      for (int kk = 0; kk < 4; ++kk) {
-        mma_bf16(c, da[kk], ld32(S.w2n + (8 * j + g) * kSW2 + 16 * kk + 2 * q),
-                 ld32(S.w2n + (8 * j + g) * kSW2 + 16 * kk + 2 * q + 8));
-      }
-      const uint32_t ht = h1[j >> 1][(j & 1) * 2 + 0], hb = h1[j >> 1][(j & 1) * 2 + 1];
-      const float m00 = lo_f(ht) > 0.0f ? c[0] : 0.0f, m01 = hi_f(ht) > 0.0f ? c[1] : 0.0f;
-      const float m10 = lo_f(hb) > 0.0f ? c[2] : 0.0f, m11 = hi_f(hb) > 0.0f ? c[3] : 0.0f;
-      db1[j][0] += m00 + m10;
-      db1[j][1] += m01 + m11;
-      S.dh1t[(8 * j + 2 * q) * kST + c0] = bf16_rn(m00);
-      S.dh1t[(8 * j + 2 * q + 1) * kST + c0] = bf16_rn(m01);
-      S.dh1t[(8 * j + 2 * q) * kST + c1] = bf16_rn(m10);
-      S.dh1t[(8 * j + 2 * q + 1) * kST + c1] = bf16_rn(m11);
-    }
+  proxy_fence();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = S.tmem;
+  const uint32_t lane_base = static_cast<uint32_t>(32 * warp) << 16;  // this warp's TMEM lanes
+  const uint32_t acc_a = tmem, acc_b = tmem + 64;                      // the two accumulators (columns)
+  constexpr uint32_t kK = umma_idesc(false), kMN = umma_idesc(true);
+  const uint32_t sx = smem_u32(S.x), sw1 = smem_u32(S.w1t), sh1 = smem_u32(S.h1), sdh2 = smem_u32(S.dh2),
+                 sdh1 = smem_u32(S.dh1), sw2t = smem_u32(S.w2t), sw2n = smem_u32(S.w2n);
+
+  // Layer 1 into accumulator a.
+  if (t == 0) {
+    umma_bf16(acc_a, umma_desc(sx, 128, 256), umma_desc(sw1, 128, 256), kK, 0u);
+    umma_commit(&S.bar);
   }
-  // Column sums over the warp's rows: reduce over g (lanes q, q + 4, ..., q + 28).
+  chain_wait(&S.bar, 0, a.err);
+  float acc[64];
+  uint32_t h1p[32];
+  tmem_ld64(acc_a + lane_base, acc);
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      float s0 = db1[j][h], s1 = db2[j][h], s2 = dw3[j][h];
-#pragma unroll
-      for (int o = 4; o < 32; o <<= 1) {
-        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-      }
-      if (g == 0) {
-        S.wsum[warp][0][8 * j + 2 * q + h] = s0;
-        S.wsum[warp][1][8 * j + 2 * q + h] = s1;
-        S.wsum[warp][2][8 * j + 2 * q + h] = s2;
-      }
-    }
+  for (int j = 0; j < 32; ++j) {
+    h1p[j] = pack2(fmaxf(acc[2 * j] + S.b1[2 * j], 0.0f), fmaxf(acc[2 * j + 1] + S.b1[2 * j + 1], 0.0f));
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    sdy += __shfl_xor_sync(0xffffffffu, sdy, o);
-    sloss += __shfl_xor_sync(0xffffffffu, sloss, o);
-  }
-  if (lane == 0) {
-    S.wdb3[warp] = sdy;
-    S.wloss[warp] = sloss;
-  }
+  store_row64(S.h1, t, h1p);
+  proxy_fence();
+  tc_fence_before();
   __syncthreads();
 
+  // Layer 2 into accumulator b.
+  if (t == 0) {
+    tc_fence_after();
+#pragma unroll
+    for (int s = 0; s < kMlpHid / 16; ++s) {
+      umma_bf16(acc_b, umma_desc(sh1 + 256 * s, 128, 1024), umma_desc(sw2t + 256 * s, 128, 1024), kK, s > 0);
+    }
+    umma_commit(&S.bar);
+  }
+  chain_wait(&S.bar, 1, a.err);
+  tmem_ld64(acc_b + lane_base, acc);
+  float y = 0.0f;
+#pragma unroll
+  for (int o = 0; o < kMlpHid; ++o) y = y + bf16_round(fmaxf(acc[o] + S.b2[o], 0.0f)) * S.w3[o];
+  y += S.b3;
+  const float e = valid ? y - a.y[idx] : 0.0f;
+  const float wgt = 2.0f * (e < 0.0f ? a.tau : 1.0f - a.tau);
+  const float dy = wgt * e * a.inv_rows;
+  // dH2 = dy w3 masked by ReLU: the tile (BF16); its FP32 values summed down the columns for db2.
+  {
+    uint32_t dp[32];
+    float v[64];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const float h0 = bf16_round(fmaxf(acc[2 * j] + S.b2[2 * j], 0.0f));
+      const float h1v = bf16_round(fmaxf(acc[2 * j + 1] + S.b2[2 * j + 1], 0.0f));
+      const float d0 = h0 > 0.0f ? dy * S.w3[2 * j] : 0.0f, d1 = h1v > 0.0f ? dy * S.w3[2 * j + 1] : 0.0f;
+      v[2 * j] = d0;
+      v[2 * j + 1] = d1;
+      dp[j] = pack2(d0, d1);
+    }
+    store_row64(S.dh2, t, dp);
+    warp_column_sums(v, lane);
+    S.part[0][warp][2 * lane] = v[0];
+    S.part[0][warp][2 * lane + 1] = v[1];
+  }
+  // db3 and the loss: the warp's rows, then the warps in order.
+  {
+    float sdy = dy;
+    double sl = static_cast<double>(wgt) * e * e;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sdy += __shfl_xor_sync(0xffffffffu, sdy, o);
+      sl += __shfl_xor_sync(0xffffffffu, sl, o);
+    }
+    if (lane == 0) {
+      S.wdb3[warp] = sdy;
+      S.wloss[warp] = sl;
+    }
+  }
+  proxy_fence();
+  tc_fence_before();
+  __syncthreads();
+
+  // dH1 into accumulator a, while the CTA sums db2 and dW3.
+  if (t == 0) {
+    tc_fence_after();
+#pragma unroll
+    for (int s = 0; s < kMlpHid / 16; ++s) {
+      umma_bf16(acc_a, umma_desc(sdh2 + 256 * s, 128, 1024), umma_desc(sw2n + 256 * s, 128, 1024), kK, s > 0);
+    }
+    umma_commit(&S.bar);
+  }
+#pragma unroll
+  for (int o = 0; o < kMlpHid; ++o) acc[o] = bf16_round(fmaxf(acc[o] + S.b2[o], 0.0f)) * dy;
+  warp_column_sums(acc, lane);
+  S.part[1][warp][2 * lane] = acc[0];
+  S.part[1][warp][2 * lane + 1] = acc[1];
+  chain_wait(&S.bar, 0, a.err);
+  tmem_ld64(acc_a + lane_base, acc);
+  {
+    uint32_t dp[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const float m0 = lo_f(h1p[j]) > 0.0f ? acc[2 * j] : 0.0f, m1 = hi_f(h1p[j]) > 0.0f ? acc[2 * j + 1] : 0.0f;
+      acc[2 * j] = m0;
+      acc[2 * j + 1] = m1;
+      dp[j] = pack2(m0, m1);
+    }
+    store_row64(S.dh1, t, dp);
+  }
+  proxy_fence();
+  tc_fence_before();
+  __syncthreads();
+
+  // dW2 = H1^T dH2 into accumulator b, dW1 = X^T dH1 into accumulator a (K = the 128 rows, MN-major reads).
+  if (t == 0) {
+    tc_fence_after();
+#pragma unroll
+    for (int s = 0; s < kRowsPerCta / 16; ++s) {
+      umma_bf16(acc_b, umma_desc(sh1 + 2048 * s, 1024, 128), umma_desc(sdh2 + 2048 * s, 1024, 128), kMN, s > 0);
+    }
+#pragma unroll
+    for (int s = 0; s < kRowsPerCta / 16; ++s) {
+      umma_bf16(acc_a, umma_desc(sx + 512 * s, 256, 128), umma_desc(sdh1 + 2048 * s, 1024, 128), kMN, s > 0);
+    }
+    umma_commit(&S.bar);
+  }
+  warp_column_sums(acc, lane);
+  S.part[2][warp][2 * lane] = acc[0];
+  S.part[2][warp][2 * lane + 1] = acc[1];
+  __syncthreads();
   float* out = a.partial + static_cast<size_t>(blockIdx.x) * kMlpParamsPad;
-  // dW2 [i][o] = sum_r H1[r][i] dH2[r][o]: warp w takes rows i in [16w, 16w + 16).
-#pragma unroll 1
-  for (int j = 0; j < 8; ++j) {
-    float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  if (t < kMlpHid) {  // the column sums: the four warps' in order
+    out[kOffB2 + t] = ((S.part[0][0][t] + S.part[0][1][t]) + S.part[0][2][t]) + S.part[0][3][t];
+    out[kOffW3 + t] = ((S.part[1][0][t] + S.part[1][1][t]) + S.part[1][2][t]) + S.part[1][3][t];
+    out[kOffB1 + t] = ((S.part[2][0][t] + S.part[2][1][t]) + S.part[2][2][t]) + S.part[2][3][t];
+  }
+  chain_wait(&S.bar, 1, a.err);
+  if (warp < 2) {  // dW2 [h][o]: rows 0-63 of accumulator b
+    tmem_ld64(acc_b + lane_base, acc);
+    float4* dst = reinterpret_cast<float4*>(out + kOffW2 + t * kMlpHid);
 #pragma unroll
-    for (int kk = 0; kk < kRowsPerCta / 16; ++kk) {
-      uint32_t aa[4];
-      aa[0] = ld32(S.h1t + (16 * warp + g) * kST + 16 * kk + 2 * q);
-      aa[1] = ld32(S.h1t + (16 * warp + g + 8) * kST + 16 * kk + 2 * q);
-      aa[2] = ld32(S.h1t + (16 * warp + g) * kST + 16 * kk + 2 * q + 8);
-      aa[3] = ld32(S.h1t + (16 * warp + g + 8) * kST + 16 * kk + 2 * q + 8);
-      mma_bf16(c, aa, ld32(S.dh2t + (8 * j + g) * kST + 16 * kk + 2 * q),
-               ld32(S.dh2t + (8 * j + g) * kST + 16 * kk + 2 * q + 8));
+    for (int o = 0; o < kMlpHid / 4; ++o) {
+      dst[o] = make_float4(acc[4 * o], acc[4 * o + 1], acc[4 * o + 2], acc[4 * o + 3]);
     }
-    const int i0 = 16 * warp + g, o0 = 8 * j + 2 * q;
-    out[kOffW2 + i0 * kMlpHid + o0] = c[0];
-    out[kOffW2 + i0 * kMlpHid + o0 + 1] = c[1];
-    out[kOffW2 + (i0 + 8) * kMlpHid + o0] = c[2];
-    out[kOffW2 + (i0 + 8) * kMlpHid + o0 + 1] = c[3];
   }
-  // dW1 [f][h] = sum_r X[r][f] dH1[r][h]: warp w takes columns h in [16w, 16w + 16).
-#pragma unroll 1
-  for (int jj = 0; jj < 2; ++jj) {
-    const int j = 2 * warp + jj;
-    float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  if (warp == 0) {  // dW1 [f][h]: rows 0-15 of accumulator a
+    tmem_ld64(acc_a + lane_base, acc);
+    if (lane < kMlpIn) {
+      float4* dst = reinterpret_cast<float4*>(out + kOffW1 + lane * kMlpHid);
 #pragma unroll
-    for (int kk = 0; kk < kRowsPerCta / 16; ++kk) {
-      uint32_t aa[4];
-      aa[0] = ld32(S.xt + g * kST + 16 * kk + 2 * q);
-      aa[1] = ld32(S.xt + (g + 8) * kST + 16 * kk + 2 * q);
-      aa[2] = ld32(S.xt + g * kST + 16 * kk + 2 * q + 8);
-      aa[3] = ld32(S.xt + (g + 8) * kST + 16 * kk + 2 * q + 8);
-      mma_bf16(c, aa, ld32(S.dh1t + (8 * j + g) * kST + 16 * kk + 2 * q),
-               ld32(S.dh1t + (8 * j + g) * kST + 16 * kk + 2 * q + 8));
+      for (int h = 0; h < kMlpHid / 4; ++h) {
+        dst[h] = make_float4(acc[4 * h], acc[4 * h + 1], acc[4 * h + 2], acc[4 * h + 3]);
+      }
     }
-    const int h0 = 8 * j + 2 * q;
-    out[kOffW1 + g * kMlpHid + h0] = c[0];
-    out[kOffW1 + g * kMlpHid + h0 + 1] = c[1];
-    out[kOffW1 + (g + 8) * kMlpHid + h0] = c[2];
-    out[kOffW1 + (g + 8) * kMlpHid + h0 + 1] = c[3];
   }
-  if (tid < kMlpHid) {
-    out[kOffB1 + tid] = ((S.wsum[0][0][tid] + S.wsum[1][0][tid]) + S.wsum[2][0][tid]) + S.wsum[3][0][tid];
-    out[kOffB2 + tid] = ((S.wsum[0][1][tid] + S.wsum[1][1][tid]) + S.wsum[2][1][tid]) + S.wsum[3][1][tid];
-    out[kOffW3 + tid] = ((S.wsum[0][2][tid] + S.wsum[1][2][tid]) + S.wsum[2][2][tid]) + S.wsum[3][2][tid];
-  }
-  if (tid == 0) {
+  if (t == 0) {
     out[kOffB3] = ((S.wdb3[0] + S.wdb3[1]) + S.wdb3[2]) + S.wdb3[3];
     a.partial_loss[blockIdx.x] = ((S.wloss[0] + S.wloss[1]) + S.wloss[2]) + S.wloss[3];
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128u) : "memory");
   }
 }
 
@@ -457,7 +590,7 @@ int train_grid(uint32_t rows) { return static_cast<int>((rows + kRowsPerCta - 1)
 
 void launch_train_partials(const TrainArgs& a, cudaStream_t stream) {
   static bool configured = false;
-  const int bytes = static_cast<int>(sizeof(TrainShared));
+  const int bytes = static_cast<int>(sizeof(TrainTiles));
   if (!configured) {
     cudaFuncSetAttribute(train_partials_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     configured = true;

@@ -1217,7 +1217,7 @@ struct Mlp {
   DevBuf<uint16_t> ops;
   DevBuf<double> partial_loss, grad, loss;
   DevBuf<int64_t> step;
-  DevBuf<unsigned int> done;
+  DevBuf<unsigned int> done;  // [0]: Adam's block counter; [1]: the training kernel's error word
   cudaStream_t own = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -1243,7 +1243,7 @@ struct Mlp {
     v.ensure(kMlpParams);
     ops.ensure(kOpWords);
     step.ensure(1);
-    done.ensure(1);
+    done.ensure(2);
     grad.ensure(kMlpParams);
     loss.ensure(1);
     losses.ensure(kLossCap);
@@ -1269,7 +1269,7 @@ struct Mlp {
     CK(cudaMemsetAsync(v.p, 0, kMlpParams * sizeof(float), own));
     CK(cudaMemsetAsync(ops.p, 0, kOpWords * sizeof(uint16_t), own));
     CK(cudaMemsetAsync(step.p, 0, sizeof(int64_t), own));
-    CK(cudaMemsetAsync(done.p, 0, sizeof(unsigned int), own));
+    CK(cudaMemsetAsync(done.p, 0, 2 * sizeof(unsigned int), own));
     launch_operands(params.p, ops.p, own);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(own));
@@ -1297,13 +1297,24 @@ struct Mlp {
     partial.ensure(static_cast<size_t>(ctas) * kMlpParamsPad);
     partial_loss.ensure(ctas);
     TrainArgs a{x, y, n, static_cast<uint32_t>(n), 0, 0, step.p, ops.p, params.p, partial.p, partial_loss.p,
-                1.0f / static_cast<float>(n), 0.5f};
+                1.0f / static_cast<float>(n), 0.5f, done.p + 1};
     launch_train_partials(a, s);
     launch_reduce_partials(partial.p, partial_loss.p, ctas, a.inv_rows, grad.p, loss.p, s);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(g_host, grad.p, kMlpParams * sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(loss_host, loss.p, sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    check_chains();
+  }
+
+  // The training kernel's error word: a tensor-core chain whose completion it did not see in time.
+  void check_chains() {
+    unsigned int e = 0;
+    CK(cudaMemcpy(&e, done.p + 1, sizeof(e), cudaMemcpyDeviceToHost));
+    if (e != 0) {
+      CK(cudaMemset(done.p + 1, 0, sizeof(e)));
+      throw CudaError("mlp: a tensor-core chain of the training step did not complete within its wait bound");
+    }
   }
 
   // `steps` Adam steps on batches of `batch` rows drawn with replacement from the n pairs. The steps run from a
@@ -1320,7 +1331,7 @@ struct Mlp {
     partial_loss.ensure(ctas);
     const int64_t s0 = steps_from_device(s);
     const TrainArgs a{x, y, n, static_cast<uint32_t>(batch), 1, seed, step.p, ops.p, params.p, partial.p,
-                      partial_loss.p, 1.0f / static_cast<float>(batch), tau};
+                      partial_loss.p, 1.0f / static_cast<float>(batch), tau, done.p + 1};
     auto one = [&](cudaStream_t st) {
       launch_train_partials(a, st);
       launch_adam(params.p, m.p, v.p, ops.p, partial.p, partial_loss.p, ctas, lr, a.inv_rows, step.p, losses.p,
@@ -1371,6 +1382,7 @@ struct Mlp {
       }
     }
     CK(cudaStreamSynchronize(s));
+    check_chains();
   }
 
   int64_t steps_from_device(cudaStream_t s) {

@@ -321,7 +321,7 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     if world == 1 and not (args.no_cpu_baseline or args.profile):
         out["cpu_baseline"] = cpu_baseline(wl, cpu_windows(args))
     if rank == 0 and not (args.no_learned or args.profile):
-        out["learned_vs_plain"] = learned_comparison()
+        out["learned_vs_plain"] = learned_comparison(steps=args.learned_steps)
     return out
 
 
@@ -726,10 +726,18 @@ def main():
     ap.add_argument("--windows", type=int, default=0, help="run only the first windows (profiling a reduced case)")
     ap.add_argument("--profile", action="store_true", help="no e2e, CPU or learned legs (fewest launches, for ncu)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal comparison")
+    ap.add_argument("--learned-only", action="store_true",
+                    help="run the learned-proposal comparison alone (its training and both samplers) and print it")
+    ap.add_argument("--learned-steps", type=int, default=9000, help="Adam steps of the learned proposal's training")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
-    if args.impl == "reference":
+    if args.learned_only:
+        import torch
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        out = {"learned_vs_plain": learned_comparison(steps=args.learned_steps)} if rank == 0 else None
+    elif args.impl == "reference":
         out = run_reference(args, rank)
     else:
         if world > 1:
