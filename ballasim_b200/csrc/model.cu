@@ -749,16 +749,30 @@ struct Model {
     cudaEventElapsedTime(&ms_copy, take_timer.b, take_timer_copy.b);
     take_ms[0] = ms_split;
     take_ms[1] = ms_copy;
-    const auto copy = [&](const Col& c) { std::memcpy(c.dst, col_pin.p + c.at, c.elem * count); };
-    if (count < 65536) {
+    // The columns into the caller's arrays: up to 8 threads, each over an equal share of all the columns' bytes
+    // (a share can span columns; the caller's fresh pages are first touched here, so the shares fault in parallel).
+    size_t bytes = 0;
+    for (const Col& c : cols) {
+      if (c.dst) bytes += c.elem * count;
+    }
+    const auto copy_range = [&](size_t lo, size_t hi) {
+      size_t base_at = 0;
       for (const Col& c : cols) {
-        if (c.dst) copy(c);
+        if (!c.dst) continue;
+        const size_t len = c.elem * count, a = std::max(lo, base_at), b = std::min(hi, base_at + len);
+        if (a < b) {
+          std::memcpy(static_cast<unsigned char*>(c.dst) + (a - base_at), col_pin.p + c.at + (a - base_at), b - a);
+        }
+        base_at += len;
       }
+    };
+    const size_t hw = std::max<size_t>(1, std::thread::hardware_concurrency());
+    const size_t k = bytes < (size_t{4} << 20) ? 1 : std::min<size_t>({8, hw, bytes >> 20});
+    if (k == 1) {
+      copy_range(0, bytes);
     } else {
       std::vector<std::thread> th;
-      for (const Col& c : cols) {
-        if (c.dst) th.emplace_back(copy, c);
-      }
+      for (size_t i = 0; i < k; ++i) th.emplace_back(copy_range, bytes * i / k, bytes * (i + 1) / k);
       for (std::thread& t : th) t.join();
     }
     const auto w2 = std::chrono::steady_clock::now();

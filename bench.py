@@ -66,23 +66,36 @@ METRIC = "pixel-samples/s"
 SINKS = {"sink_evt3_1280x720": "evt3", "sink_evt21_1280x720": "evt21", "sink_evt2_1280x720": "evt2",
          "sink_dat_1280x720": "dat"}
 L2_BYTES = 126 * 1024 * 1024
-# Per workload, figures of one ncu capture of the dominant kernel of this bench's own command, kept beside the kernel
-# name and launch shape they were taken at (None where none was taken): DRAM bytes read + written per launch, warp
-# instructions issued per pixel-sample, and ncu's issue-slot activity. A run whose kernel or launch shape differs
-# from the capture's reports null for them.
+# Per workload, figures of ncu captures of the dominant kernel of this bench's own command, each kept beside the
+# kernel name and launch shape it was taken at: DRAM bytes read + written per launch, warp instructions issued per
+# pixel-sample, and ncu's issue-slot activity. A run whose kernel or launch shape matches no capture reports null.
 NCU = {
-    "blobs16_346x260": {"kernel": "engine_kernel_coop", "stage": 64, "tile_width": 8, "traffic": 8.74e6 + 4.56e6,
-                        "inst_per_sample": None, "issue_active": 0.285},
+    "blobs16_346x260": [{"kernel": "engine_kernel_coop", "stage": 64, "tile_width": 8,
+                         "traffic": 8.74e6 + 4.56e6, "inst_per_sample": None, "issue_active": 0.285}],
     # traffic: one pass on the full 60-window launch; instructions and issue-active: the full set on its first 4
-    # windows (74,251,870 pixel-samples, 3.329e9 warp instructions).
-    "six_sensors_4.6Mpx": {"kernel": "engine_kernel_staged<16>", "stage": 16, "tile_width": 8,
-                           "traffic": 690.74e6 + 3.59e9, "inst_per_sample": 3.329e9 / 74251870,
-                           "issue_active": 0.209},
+    # windows (74,251,870 pixel-samples).
+    "six_sensors_4.6Mpx": [
+        {"kernel": "engine_kernel_staged<16>", "stage": 16, "tile_width": 8, "traffic": 690.74e6 + 3.59e9,
+         "inst_per_sample": 3.329e9 / 74251870, "issue_active": 0.209},
+        {"kernel": "engine_kernel_staged<16>", "stage": 16, "tile_width": 4, "traffic": 694.48e6 + 3.67e9,
+         "inst_per_sample": 3.3297e9 / 74251870, "issue_active": 0.210},
+    ],
     # The runs path: its six advance_rows_kernel launches of one window (one per sensor), DRAM bytes against the
     # window's algorithmic bytes (836.3 MB read + 325.6 MB written; 833.9 MB).
-    "runs:six_sensors_4.6Mpx": {"kernel": "advance_rows_kernel", "dram_per_alg_byte": (836.32e6 + 325.60e6) / 833.92e6,
-                                "capture": "advance_rows_kernel, the six sensors' first window (6 launches, one pass)"},
+    "runs:six_sensors_4.6Mpx": [{"kernel": "advance_rows_kernel", "dram_per_alg_byte": (836.32e6 + 325.60e6) / 833.92e6,
+                                 "capture": "advance_rows_kernel, the six sensors' first window (6 launches, one pass)"}],
 }
+
+
+def ncu_capture(name: str, kernel: str, stage=None, tile_width=None):
+    """The capture of NCU[name] taken at this kernel and launch shape (stage and tile width where given), or None."""
+    for cap in NCU.get(name, []):
+        if cap["kernel"] == kernel and (stage is None or cap.get("stage") == stage) and \
+                (tile_width is None or cap.get("tile_width") == tile_width):
+            return cap
+    return None
+
+
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -153,9 +166,8 @@ def compute_fraction(wl_name: str, kernel: str, launch: dict, samples: float, km
     """The issue-slot side of the roofline: warp instructions issued per launch (ncu's count per pixel-sample at the
     captured launch shape, times this launch's pixel-samples) over the SMs' issue slots in the launch's duration at
     the sampled median SM clock (148 SMs x 4 schedulers x cycles), with ncu's own issue-active beside it."""
-    cap = NCU.get(wl_name)
-    same = cap is not None and cap["kernel"] == kernel and cap.get("stage") == launch.get("stage") and \
-        cap.get("tile_width") == launch.get("tile_width")
+    cap = ncu_capture(wl_name, kernel, launch.get("stage"), launch.get("tile_width"))
+    same = cap is not None
     out = {"ncu_capture": f"{cap['kernel']} stage {cap['stage']} tile {cap['tile_width']}" if cap else None,
            "same_launch_shape": bool(same), "warp_inst_per_launch": None, "issue_slots_per_launch": None,
            "issue_frac": None, "ncu_issue_active": cap.get("issue_active") if same else None}
@@ -277,9 +289,8 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     alg = b_sense(pixels, wl.windows, int(per_step_samples), int(per_step_events))
     achieved = alg / (kms * 1e-3) / 1e9
     kname = engine_kernel_name(eng, cascade, lattice)
-    cap = NCU.get(wl.name)
-    same_shape = cap is not None and cap["kernel"] == kname and cap.get("stage") == eng.launch["stage"] and \
-        cap.get("tile_width") == eng.launch["tile_width"]
+    cap = ncu_capture(wl.name, kname, eng.launch["stage"], eng.launch["tile_width"])
+    same_shape = cap is not None
     out = {
         "metric": METRIC,
         "value": samples_all / (total_ms_all * 1e-3),
@@ -422,9 +433,7 @@ def run_runs(args, rank: int, world: int) -> dict | None:
     alg = b_sense(wl.pixels, wl.windows, int(per_step_samples), int(per_step_events))
     achieved = alg / (kms_total * 1e-3) / 1e9
     kname = "advance_runs_kernel" if args.block else "advance_rows_kernel"
-    cap = NCU.get("runs:" + wl.name)
-    if cap is not None and cap["kernel"] != kname:
-        cap = None
+    cap = ncu_capture("runs:" + wl.name, kname)
     calls = wl.windows * len(wl.sensors)
     return {
         "metric": METRIC, "value": samples_all / (total_ms_all * 1e-3), "unit": "pixel-samples/s",
