@@ -58,6 +58,7 @@ enum ErrorBit : unsigned long long {
   kErrAfterEnd = 16ull,
   kErrNonFinite = 32ull,
   kErrSearchBound = 64ull,  // a warp-cooperative crossing search or its warp loop ran past its bound
+  kErrRestList = 128ull,    // the split engine's list of posted pixels overflowed (it holds every pixel: not reached)
 };
 
 struct EventBuf {
@@ -150,6 +151,16 @@ void launch_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t tota
                    int32_t w0, int32_t w1, const SamplerRules& r, unsigned int* tile_counter, int blocks,
                    int warps_per_block, int stage, int tile_lw, int cascade, cudaStream_t stream);
 int engine_max_blocks_per_sm(int warps_per_block, int stage, int cascade);
+// The split engine (stage kStageSplit): window w as engine_window_kernel (blocks x warps_per_block warps, persistent
+// over the tiles) then engine_rest_kernel (rest_blocks x 128 threads) over the pixels the first posted to `rest`
+// (rest_capacity records of rest_record_bytes(); *rest_count and *tile_counter zero before the launch).
+constexpr int kStageSplit = 1;
+void launch_engine_split(const EngineSensor* sensors_dev, int n_sensors, uint32_t total_tiles, const int64_t* t0,
+                         int32_t w, const SamplerRules& r, unsigned int* tile_counter, void* rest, unsigned int* rest_count,
+                         unsigned int rest_capacity, int blocks, int warps_per_block, int tile_lw, int rest_blocks,
+                         cudaStream_t stream);
+size_t rest_record_bytes();
+int engine_rest_blocks_per_sm();
 // The fused engine with the learned step proposal (BF16 MLP operands and FP32 parameters in device memory):
 // the same tiles and pixel model, each window sampled by proposed power-of-two steps judged by the plain rule.
 // rec_samples / rec_steps (capacity 0: off) record every sample and every proposed step.

@@ -16,6 +16,8 @@ namespace bs {
 
 namespace {
 
+// Appends events to one sensor's buffer; the lanes of a warp that push together share one atomic, so every lane of
+// the warp must push to the same buffer (a warp works on one tile of one sensor).
 struct GlobalSink {
   EventBuf ev;
   unsigned long long* count;
@@ -25,6 +27,22 @@ struct GlobalSink {
     if (g.thread_rank() == 0) base = atomicAdd(count, static_cast<unsigned long long>(g.size()));
     base = g.shfl(base, 0);
     const unsigned long long i = base + g.thread_rank();
+    if (i < ev.capacity) {
+      const uint4* src = reinterpret_cast<const uint4*>(&e);
+      uint4* dst = reinterpret_cast<uint4*>(ev.data + i);
+      dst[0] = src[0];
+      dst[1] = src[1];
+    }
+  }
+};
+
+// Appends each event with the pushing thread's own atomic: for a kernel whose lanes serve pixels of different
+// sensors (engine_rest_kernel).
+struct ThreadSink {
+  EventBuf ev;
+  unsigned long long* count;
+  __device__ __forceinline__ void push(const RawEvent& e) {
+    const unsigned long long i = atomicAdd(count, 1ull);
     if (i < ev.capacity) {
       const uint4* src = reinterpret_cast<const uint4*>(&e);
       uint4* dst = reinterpret_cast<uint4*>(ev.data + i);
@@ -406,6 +424,22 @@ __device__ __forceinline__ bool clean_segment(const PixelRegs& s, const PixelMap
   const float D0 = hp.delta(t0, x0);
   if (D0 >= m.theta_on || D0 <= -m.theta_off) return false;
   if (e - t0 == 1) return true;
+  return hp.excluded(Segment{t0, e, v0, v1}, t0, e, x0, x1);
+}
+
+// clean_segment's other case, for a segment it refused: the search armed after t0 (the first segment after init, or
+// the segment of an event), where PixelProc::piece searches [t_search, e) alone, without Delta(t0); clean when
+// nothing is left to search or the node (t0, e - 1] around it is excluded (the same effects).
+__device__ __forceinline__ bool clean_after_start(const PixelRegs& s, const PixelMapRegs& m, const SensorConsts& k,
+                                                  int64_t t0, int64_t e, float v0, float v1, float x0, float x1) {
+  if (((e - 1) >> kWindowLog2) != (t0 >> kWindowLog2)) return false;
+  if (s.blind_until != kNotBlind || s.t_search <= t0) return false;
+  const int64_t tn = k.noise ? mini(s.t_shot, s.t_ba) : kForever;
+  if (tn < e) return false;
+  if (s.t_search >= e) return true;
+  NullSink ns;
+  PixelCounters nc;
+  const PixelProc<NullSink> hp{const_cast<PixelRegs&>(s), m, k, 0u, ns, nc};
   return hp.excluded(Segment{t0, e, v0, v1}, t0, e, x0, x1);
 }
 
@@ -1072,7 +1106,7 @@ struct WindowFeed {
 
 // WindowFeed for a pixel whose state stays in the caller's registers (s, m, c): each segment's clean outcome is taken
 // in place, anything else out of line (feed_segment<kFlat>); the same samples and state as WindowFeed's.
-template <bool kFlat>
+template <bool kFlat, class Sink = GlobalSink>
 struct RegFeed {
   PixelRegs& s;
   const PixelMapRegs& m;
@@ -1080,7 +1114,7 @@ struct RegFeed {
   const SensorConsts& k;
   const SensorConsts* kd;
   uint32_t pixel;
-  GlobalSink sink;
+  Sink sink;
   int64_t t_w;
   int64_t prev_t;
   float prev_v;
@@ -1648,6 +1682,217 @@ __global__ void __launch_bounds__(128) engine_kernel_staged(EngineArgs a) {
     warp_add(&S.counters[kCntLeaves], c.leaves);
     warp_add(&S.counters[kCntSamples], samples);
     warp_add(&S.counters[kCntNoise], c.noise_candidates);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// The split engine: per window, the common path in one kernel and the rare one in another
+// ---------------------------------------------------------------------------------------------
+// A pixel's rare paths (a segment where a crossing may occur, an accepted noise candidate, the refractory interval,
+// the first segment after the start) run one or two lanes at a time while the rest of the warp waits, and their code
+// competes with the hot loop's for the instruction cache: on the six sensors they took most of the staged engine's
+// time. Here each window is two launches. engine_window_kernel runs the staged engine's phases for every pixel (the
+// walk with its first kSplitStage samples staged, the noise pass, the pixel model's clean segments in registers)
+// and, at a pixel's first segment that is not clean, stops that pixel and posts it (its state, its feed and the
+// staged samples left) to a list; a window that overflows the stage is posted whole. engine_rest_kernel then
+// finishes the posted pixels' windows, one thread per pixel, through the full pixel model, so its lanes all run the
+// rare paths together. A pixel's samples are fed in the same order to the same state either way, so events and
+// state are the staged engine's; the state passes from one window to the next through HBM.
+constexpr int kSplitStage = 16;
+constexpr uint8_t kRestWhole = 0xFF;  // RestRecord::n of a window that overflowed the stage
+
+struct RestRecord {
+  PixelRegs s;        // the state where the pixel stopped (after the noise pass and its clean segments)
+  int64_t prev_t;     // the feed: the last sample fed (time, clamped value, x) and the last raw value
+  float prev_v, x_prev, last_raw;
+  uint32_t pixel;
+  uint16_t sensor;
+  uint8_t n;          // samples left in dt / v (kRestWhole: the window from its start, the carried sample in last_raw)
+  uint8_t level;      // the window's lattice level (for a whole window)
+  uint32_t dt[kSplitStage];
+  float v[kSplitStage];
+};
+
+struct RestList {
+  RestRecord* rec;
+  unsigned int* count;
+  unsigned int capacity;
+};
+
+// Window a.w0 of every tile (a.t0 the model time at the call's start). kFirst: the call's first window, where the
+// pixels' searches can be armed after their first segment's start (after init): such a segment is also taken in
+// place when clean (clean_after_start), instead of being posted; the other windows' kernel leaves that test out (in
+// the hot loop it cost more than it saves there).
+template <bool kFirst>
+__global__ void __launch_bounds__(128) engine_window_kernel(EngineArgs a, RestList rl) {
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const int64_t t_w = *a.t0 + static_cast<int64_t>(a.w0) * kWindowNs;
+  __shared__ uint16_t lists[4][kMaxListed];
+  __shared__ uint32_t st_dt[4][kSplitStage][32];
+  __shared__ float st_v[4][kSplitStage][32];
+  uint16_t* my_list = lists[warp];
+  for (;;) {
+    uint32_t tile = 0;
+    if (lane == 0) tile = atomicAdd(a.tile_counter, 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if (tile >= a.total_tiles) break;
+    int si = 0;
+    while (si + 1 < a.n_sensors && a.sensors[si + 1].tile0 <= tile) ++si;
+    const EngineSensor& S = a.sensors[si];
+    const uint32_t local = tile - S.tile0;
+    uint32_t x, y;
+    tile_xy(local, S.tiles_x, a.tile_lw, lane, x, y);
+    const bool have = x < S.width && y < S.height;
+    const uint32_t p = have ? y * S.width + x : 0u;
+    const bool noise = S.consts.noise != 0;
+    const float irr_max = S.consts.irr_max;
+    PixelRegs s;
+    PixelMapRegs m;
+    float carried = 0.0f;
+    if (have) {
+      load_state(S.in, p, noise, s);
+      load_map(S.map, p, m);
+      carried = S.carried_in[p];
+    }
+    PixelCounters c;
+    const FieldDev& f = S.field;
+    const BlobList list = warp_blob_list(f, have, x, y, t_w, t_w + kWindowNs, my_list);
+    auto render = [&](uint32_t dt) { return field_eval(f, list, x, y, t_w + dt); };
+    // The walk, its first kSplitStage samples after slot 0 staged.
+    uint32_t n = 0;
+    int level = 0;
+    if (have) {
+      level = field_level(f, list, x, y, t_w, a.r.l_min, a.r.l_max);
+      uint32_t k = 0;
+      n = sample_pixel_window(a.r, level, carried, false, render, [&](uint32_t dt, float v) {
+        if (k < static_cast<uint32_t>(kSplitStage)) {
+          st_dt[warp][k][lane] = dt;
+          st_v[warp][k][lane] = v;
+        }
+        ++k;
+      });
+    }
+    __syncwarp();
+    const bool staged = have && n - 1 <= static_cast<uint32_t>(kSplitStage);
+    // The window's noise candidates of all lanes together; the rejected ones leave the pixel model.
+    if (noise) {
+      const StagedRun run{t_w, &st_dt[warp][0][lane], &st_v[warp][0][lane], static_cast<int>(n) - 1};
+      noise_ahead(s, m, S.consts, p, staged, t_w, clamp_irr(carried, irr_max), t_w + kWindowNs, run, c);
+    }
+    // The clean segments in place; the first other one stops the pixel there (a window that overflowed the stage
+    // stops at its start).
+    bool post = have && !staged;
+    uint32_t j = 0;
+    int64_t prev_t = t_w;
+    float prev_v = 0.0f, last_raw = carried, x_prev = 0.0f;
+    if (staged) {
+      prev_v = clamp_irr(carried, irr_max);
+      x_prev = x_sample(s, m, prev_v);
+      for (; j + 1 < n; ++j) {
+        const float v = st_v[warp][j][lane];
+        const int64_t t = t_w + st_dt[warp][j][lane];
+        const float vc = clamp_irr(v, irr_max);
+        const float x1 = x_sample(s, m, vc);
+        if (!clean_segment(s, m, S.consts, prev_t, t, prev_v, vc, x_prev, x1) &&
+            !(kFirst && clean_after_start(s, m, S.consts, prev_t, t, prev_v, vc, x_prev, x1))) {
+          break;
+        }
+        ++c.pieces;
+        if (t - prev_t > 2) ++c.leaves;
+        s.t_search = maxi(s.t_search, t);
+        last_raw = v;
+        prev_t = t;
+        prev_v = vc;
+        x_prev = x1;
+      }
+      post = j + 1 < n;
+      if (!post) {
+        s.held = prev_v;
+        store_state(S.out, p, noise, s);
+        S.carried_out[p] = last_raw;
+      }
+    }
+    // One record per stopped pixel, the warp's records reserved together.
+    __syncwarp();
+    const unsigned posting = __ballot_sync(0xffffffffu, post);
+    if (posting != 0u) {
+      const int leader = __ffs(posting) - 1;
+      unsigned int base = 0;
+      if (static_cast<int>(lane) == leader) base = atomicAdd(rl.count, static_cast<unsigned int>(__popc(posting)));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (post) {
+        const unsigned int i = base + static_cast<unsigned int>(__popc(posting & ((1u << lane) - 1u)));
+        if (i >= rl.capacity) {
+          atomicOr(&S.counters[kCntErrors], kErrRestList);
+        } else {
+          RestRecord& r = rl.rec[i];
+          r.s = s;
+          r.prev_t = prev_t;
+          r.prev_v = prev_v;
+          r.x_prev = x_prev;
+          r.last_raw = last_raw;
+          r.pixel = p;
+          r.sensor = static_cast<uint16_t>(si);
+          r.level = static_cast<uint8_t>(level);
+          if (!staged) {
+            r.n = kRestWhole;
+          } else {
+            r.n = static_cast<uint8_t>(n - 1 - j);
+            for (uint32_t q = j; q + 1 < n; ++q) {
+              r.dt[q - j] = st_dt[warp][q][lane];
+              r.v[q - j] = st_v[warp][q][lane];
+            }
+          }
+        }
+      }
+    }
+    __syncwarp();
+    warp_add(&S.counters[kCntPieces], c.pieces);
+    warp_add(&S.counters[kCntLeaves], c.leaves);
+    warp_add(&S.counters[kCntSamples], have ? n : 0u);
+    warp_add(&S.counters[kCntNoise], c.noise_candidates);
+  }
+}
+
+// The posted pixels of window a.w0, one thread each: the rest of the window through the full pixel model (a window
+// posted whole is walked again from its start, every blob of the field evaluated: the same values as the warp's
+// culled list gives), then the state and the carried sample stored.
+__global__ void __launch_bounds__(128) engine_rest_kernel(EngineArgs a, RestList rl) {
+  const int64_t t_w = *a.t0 + static_cast<int64_t>(a.w0) * kWindowNs;
+  const unsigned int count = min(*rl.count, rl.capacity);
+  for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const RestRecord& r = rl.rec[i];
+    const EngineSensor& S = a.sensors[r.sensor];
+    PixelRegs s = r.s;
+    PixelMapRegs m;
+    load_map(S.map, r.pixel, m);
+    PixelCounters c;
+    const ThreadSink sink{S.ev, &S.counters[kCntEvents]};
+    float held, last_raw;
+    if (r.n == kRestWhole) {
+      const FieldDev& f = S.field;
+      const BlobList all{nullptr, f.n_blobs};
+      const uint32_t x = r.pixel % S.width, y = r.pixel / S.width;
+      auto render = [&](uint32_t dt) { return field_eval(f, all, x, y, t_w + dt); };
+      RegFeed<true, ThreadSink> feed{s,   m,   c,      S.consts,   &S.consts, r.pixel,
+                                     sink, t_w, t_w, s.held, r.last_raw, 0.0f};
+      feed.start(r.last_raw);
+      sample_pixel_window(a.r, r.level, r.last_raw, false, render, feed);
+      held = feed.prev_v;
+      last_raw = feed.last_raw;
+    } else {
+      RegFeed<true, ThreadSink> feed{s, m, c, S.consts, &S.consts, r.pixel, sink, t_w, r.prev_t, r.prev_v, r.last_raw,
+                                     r.x_prev};
+      for (int q = 0; q < r.n; ++q) feed(r.dt[q], r.v[q]);
+      held = feed.prev_v;
+      last_raw = feed.last_raw;
+    }
+    s.held = held;
+    store_state(S.out, r.pixel, S.consts.noise != 0, s);
+    S.carried_out[r.pixel] = last_raw;
+    if (c.pieces) atomicAdd(&S.counters[kCntPieces], static_cast<unsigned long long>(c.pieces));
+    if (c.leaves) atomicAdd(&S.counters[kCntLeaves], static_cast<unsigned long long>(c.leaves));
+    if (c.noise_candidates) atomicAdd(&S.counters[kCntNoise], static_cast<unsigned long long>(c.noise_candidates));
   }
 }
 
@@ -2239,8 +2484,31 @@ void launch_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t tota
   else engine_kernel<<<blocks, warps_per_block * 32, 0, stream>>>(a);
 }
 
+void launch_engine_split(const EngineSensor* sensors_dev, int n_sensors, uint32_t total_tiles, const int64_t* t0,
+                         int32_t w, const SamplerRules& r, unsigned int* tile_counter, void* rest, unsigned int* rest_count,
+                         unsigned int rest_capacity, int blocks, int warps_per_block, int tile_lw, int rest_blocks,
+                         cudaStream_t stream) {
+  const EngineArgs a{sensors_dev, n_sensors, total_tiles, t0, w, w + 1, r, tile_counter, static_cast<uint32_t>(tile_lw)};
+  const RestList rl{static_cast<RestRecord*>(rest), rest_count, rest_capacity};
+  if (w == 0) engine_window_kernel<true><<<blocks, warps_per_block * 32, 0, stream>>>(a, rl);
+  else engine_window_kernel<false><<<blocks, warps_per_block * 32, 0, stream>>>(a, rl);
+  engine_rest_kernel<<<rest_blocks, 128, 0, stream>>>(a, rl);
+}
+
+size_t rest_record_bytes() { return sizeof(RestRecord); }
+
+int engine_rest_blocks_per_sm() {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_rest_kernel, 128, 0);
+  return n;
+}
+
 int engine_max_blocks_per_sm(int warps_per_block, int stage, int cascade) {
   int n = 0;
+  if (stage == kStageSplit) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_window_kernel<false>, warps_per_block * 32, 0);
+    return n;
+  }
   if (cascade == 2 && stage != 0) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_lattice_kernel_staged, warps_per_block * 32, 0);
   } else if (cascade == 2) {

@@ -597,6 +597,7 @@ struct Model {
     if (e & kErrAfterEnd) return "SensorModel.advance: sample after t_end_ns";
     if (e & kErrNonFinite) return "SensorModel.advance: non-finite irradiance";
     if (e & kErrSearchBound) return "engine: a crossing search ran past its bound";
+    if (e & kErrRestList) return "engine: the split engine's list of posted pixels overflowed";
     return "SensorModel.advance: refused input";
   }
 
@@ -1516,6 +1517,16 @@ struct Engine {
   DevBuf<unsigned long long> rec_count;
   size_t rec_cap = 0;
   unsigned long long rec_n[2] = {0, 0};
+  // The split engine (stage kStageSplit): two scratch states and carried frames per sensor that the windows between
+  // a call's first and last pass the state through, the per-window descriptors, the posted-pixel list (room for every
+  // pixel), and per window a tile counter and a list count.
+  std::vector<std::unique_ptr<StateBufs>> split_state;
+  std::vector<std::unique_ptr<DevBuf<float>>> split_carried;
+  DevBuf<EngineSensor> split_desc;
+  PinBuf<EngineSensor> split_desc_pin;
+  DevBuf<unsigned char> rest;
+  DevBuf<unsigned int> split_counts;
+  unsigned int rest_capacity = 0;
 
   static int32_t models_cascade(bs_model* m) { return m ? reinterpret_cast<Model*>(m)->mode() : 0; }
   // 0 the instantaneous response, 1 the cascade, 2 the cascade with its noise lattice (every sensor alike).
@@ -1650,6 +1661,12 @@ struct Engine {
   }
 
   int block_warps() const { return mlp ? 4 : warps_per_block; }
+  static int sm_count() {
+    int dev = 0, sms = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    return sms;
+  }
   int grid_blocks() const {
     int dev = 0, sms = 0;
     CK(cudaGetDevice(&dev));
@@ -1688,6 +1705,47 @@ struct Engine {
     t0_pin.p[0] = t0;
   }
 
+  // The split engine's descriptors, window-major: window w reads what w - 1 wrote (the call's input state for the
+  // first window), and writes a scratch state (the call's output state for the last one).
+  void describe_split(int32_t windows) {
+    const size_t ns = models.size();
+    if (split_state.size() < 2 * ns) {
+      split_state.clear();
+      split_carried.clear();
+      for (size_t i = 0; i < 2 * ns; ++i) {
+        split_state.push_back(std::make_unique<StateBufs>());
+        split_carried.push_back(std::make_unique<DevBuf<float>>());
+      }
+    }
+    unsigned int pixels = 0;
+    for (Model* m : models) pixels += m->n;
+    if (rest_capacity < pixels) {
+      rest.ensure(static_cast<size_t>(pixels) * rest_record_bytes());
+      rest_capacity = pixels;
+    }
+    const size_t nw = static_cast<size_t>(std::max(windows, 1));
+    split_desc_pin.ensure(nw * ns);
+    split_desc.ensure(nw * ns);
+    split_counts.ensure(2 * nw);
+    for (size_t i = 0; i < ns; ++i) {
+      Model* m = models[i];
+      const StateSoA tmp[2] = {split_state[2 * i]->soa(m->n, m->mode()), split_state[2 * i + 1]->soa(m->n, m->mode())};
+      float* tmp_c[2] = {split_carried[2 * i]->ensure(m->n), split_carried[2 * i + 1]->ensure(m->n)};
+      for (size_t w = 0; w < nw; ++w) {
+        EngineSensor e = host_pin.p[i];
+        if (w > 0) {
+          e.in = tmp[(w - 1) % 2];
+          e.carried_in = tmp_c[(w - 1) % 2];
+        }
+        if (w + 1 < nw) {
+          e.out = tmp[w % 2];
+          e.carried_out = tmp_c[w % 2];
+        }
+        split_desc_pin.p[w * ns + i] = e;
+      }
+    }
+  }
+
   // One step's device work, in stream order (what the CUDA graph holds): counters cleared, descriptors and the
   // model time uploaded from pinned memory, the persistent kernel between two timing events, counters read back.
   void enqueue(int32_t windows, int blocks, cudaStream_t st, bool capturing) {
@@ -1707,6 +1765,17 @@ struct Engine {
                               RecBuf{rec[0].p, rec_count.p, rec_cap}, RecBuf{rec[1].p, rec_count.p + 1, rec_cap}};
         launch_learned_engine(sensors_dev.p, static_cast<int>(host.size()), total_tiles, t0_dev.p, 0, windows,
                               rules, l, tile_counter.p, blocks, block_warps(), tile_lw, st);
+      } else if (stage == kStageSplit) {
+        const size_t ns = host.size();
+        CK(cudaMemcpyAsync(split_desc.p, split_desc_pin.p, static_cast<size_t>(windows) * ns * sizeof(EngineSensor),
+                           cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(split_counts.p, 0, 2 * static_cast<size_t>(windows) * sizeof(unsigned int), st));
+        const int rest_blocks = sm_count() * std::max(1, engine_rest_blocks_per_sm());
+        for (int32_t w = 0; w < windows; ++w) {
+          launch_engine_split(split_desc.p + static_cast<size_t>(w) * ns, static_cast<int>(ns), total_tiles, t0_dev.p,
+                              w, rules, split_counts.p + 2 * w, rest.p, split_counts.p + 2 * w + 1, rest_capacity,
+                              blocks, warps_per_block, tile_lw, rest_blocks, st);
+        }
       } else {
         launch_engine(sensors_dev.p, static_cast<int>(host.size()), total_tiles, t0_dev.p, 0, windows, rules,
                       tile_counter.p, blocks, warps_per_block, stage, tile_lw, cascade(), st);
@@ -1744,6 +1813,7 @@ struct Engine {
     rec_n_pin.ensure(2);
     for (;;) {
       describe(t0);
+      if (stage == kStageSplit) describe_split(windows);
       if (use_graph && rec_cap == 0) {
         const uint64_t key[8] = {static_cast<uint64_t>(windows), static_cast<uint64_t>(blocks),
                                  static_cast<uint64_t>(block_warps()), static_cast<uint64_t>(stage),
@@ -1787,6 +1857,10 @@ struct Engine {
         }
       }
       if (rerun) continue;
+      for (Model* m : models) {
+        const unsigned long long e = m->counters_h.p[kCntErrors];
+        if (e != 0) throw std::runtime_error(std::string("engine: ") + Model::error_text(e));
+      }
       if (rec_cap) {
         rec_n[0] = rec_n_pin.p[0];
         rec_n[1] = rec_n_pin.p[1];
@@ -1828,8 +1902,12 @@ struct Engine {
   void set_launch(int32_t warps, int32_t per_sm, int32_t stg, int32_t lw) {
     if (warps < 0 || warps > 4) throw std::invalid_argument("engine: warps per block must lie in [1, 4]");
     if (per_sm < 0 || per_sm > 32) throw std::invalid_argument("engine: blocks_per_sm in [0, 32]");
-    if (stg != 0 && stg != 16 && stg != 32 && stg != 64) {
-      throw std::invalid_argument("engine: stage 0, 16, 32 or 64 (32 deep with the warp-cooperative search)");
+    if (stg != 0 && stg != kStageSplit && stg != 16 && stg != 32 && stg != 64) {
+      throw std::invalid_argument(
+          "engine: stage 0, 1 (the split engine), 16, 32 or 64 (32 deep with the warp-cooperative search)");
+    }
+    if (stg == kStageSplit && (cascade() != 0 || mlp)) {
+      throw std::invalid_argument("engine: the split engine (stage 1) is the instantaneous response's");
     }
     if (stg == 64 && (cascade() != 0 || mlp)) {
       throw std::invalid_argument("engine: the warp-cooperative search (stage 64) is the instantaneous response's");
@@ -1859,9 +1937,9 @@ struct Engine {
     int bl = keep[0], bw = keep[1], bs = keep[2];
     for (int lw : {2, 3, 4}) {
       for (int w : {2, 4}) {
-        for (int st : {0, 16, 64}) {
+        for (int st : {0, kStageSplit, 16, 64}) {
           if ((mlp && (w != 4 || st != 0)) || (cascade() == 1 && st != 0)) continue;
-          if (cascade() == 2 && st == 64) continue;
+          if (cascade() == 2 && (st == 64 || st == kStageSplit)) continue;
           if (cascade() == 2 && st != 0) st = 32;
           set_launch(w, 0, st, lw);
           step(windows, s, false, nullptr, nullptr);

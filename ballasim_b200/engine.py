@@ -74,8 +74,10 @@ class Engine:
 
     def set_launch(self, warps_per_block: int = 0, blocks_per_sm: int = 0, stage: int = 0,
                    tile_width: int = 0) -> None:
-        """Launch shape of the persistent grid, the staging depth (0, 16 or 32) and the tile width (4, 8, 16 or 32
-        px; the tile is 32 / width px high)."""
+        """Launch shape of the persistent grid, the stage (0 streaming; 16 or 32 staged in shared memory; 64 staged
+        with the warp's crossing search; 1 the split engine: per window one launch for every pixel's common path and
+        one for the pixels posted at a segment that is not clean) and the tile width (4, 8, 16 or 32 px; the tile is
+        32 / width px high)."""
         _lib.check(_lib.lib().bs_engine_set_launch(self._h, int(warps_per_block), int(blocks_per_sm), int(stage),
                                                    int(tile_width)))
 

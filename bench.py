@@ -182,8 +182,13 @@ def compute_fraction(wl_name: str, kernel: str, launch: dict, samples: float, km
 def engine_kernel_name(eng, cascade: bool, lattice: bool) -> str:
     if cascade:
         return "engine_lattice_kernel" if lattice else "engine_cascade_kernel"
-    return {64: "engine_kernel_coop", 16: "engine_kernel_staged<16>",
-            32: "engine_kernel_staged<32>"}.get(eng.launch["stage"], "engine_kernel")
+    return {64: "engine_kernel_coop", 16: "engine_kernel_staged<16>", 32: "engine_kernel_staged<32>",
+            1: "engine_window_kernel+engine_rest_kernel"}.get(eng.launch["stage"], "engine_kernel")
+
+
+def engine_launches(eng, windows: int) -> int:
+    """The engine's kernel launches in one step: one persistent launch, or two per window for the split engine."""
+    return 2 * windows if eng.launch["stage"] == 1 else 1
 
 
 def run_ours(args, rank: int, world: int) -> dict | None:
@@ -312,12 +317,15 @@ def run_ours(args, rank: int, world: int) -> dict | None:
                    "parallelism": f"replicas x{world}", "path": "fused engine (runs kept on chip)",
                    "launch": {**eng.launch, "autotuned": tuned is not None, "cuda_graph": not args.no_graph,
                               "threads_per_pixel": 1}},
-        "gpu_launches": 3 * args.steps,
+        # Per step: the first frame and init of every sensor (field_frame_kernel, init_kernel), then the engine.
+        "gpu_launches": (2 * len(wl.sensors) + engine_launches(eng, wl.windows)) * args.steps,
         "clocks": clocks,
         "e2e": {"value": samples_all / e2e_s if e2e_times else None, "unit": "pixel-samples/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "split_ms_per_step": {k: round(v, 3) for k, v in split.items()}},
-        "roofline": {"kernel": kname + " (sampler + pixel model fused, runs kept on chip)",
+        "roofline": {"kernel": kname + " (sampler + pixel model fused, runs kept on chip)"
+                     + (" (per window: the common path, then the posted pixels' rare paths; avg_launch_ms is the "
+                        "step's engine time, all windows)" if eng.launch["stage"] == 1 else ""),
                      "bound": "issue",
                      "bound_note": "SIMT fp32 issue and latency (field exps, one log per sample, each crossing's "
                                    "search and fire), not HBM; achieved/peak/frac are the algorithmic bytes of the "

@@ -182,7 +182,8 @@ bs_status bs_model_state_bytes(const bs_model* m, size_t* n);
 bs_status bs_model_save_state(const bs_model* m, uint8_t* out, size_t n);
 bs_status bs_model_load_state(bs_model* m, const uint8_t* data, size_t n);
 /* Launch policy of the pixel model on CSR runs. 0 (the default): the instantaneous response runs row-major, one warp
- * per 32 runs with the runs' samples staged in shared memory (the cascade runs one thread per pixel, 128 per block);
+ * per 32 runs, runs longer than the long-run threshold walked by the whole warp (the cascade runs one thread per
+ * pixel, 128 per block);
  * 32, 64, 96 or 128: one thread per pixel with that many threads per block, for every photoreceptor. */
 bs_status bs_model_set_block(bs_model* m, int32_t threads);
 /* The row-major kernel's threads per pixel: runs longer than `samples` are walked by all 32 lanes of a warp, 32
@@ -338,8 +339,12 @@ bs_status bs_engine_start_frames(bs_engine* e, int64_t t0_ns, const float* const
 bs_status bs_engine_run(bs_engine* e, int32_t windows, void* stream, uint64_t* pixel_samples, uint64_t* events);
 /* Launch shape: warps per block and blocks per SM of the persistent grid (0: the defaults, 4 and as many as fit),
  * the staging depth (0: the sampler feeds the pixel model sample by sample; 16 or 32: per window each lane's samples
- * are staged in shared memory between a sampling phase and a sensing phase) and the tile width in pixels (4, 8, 16
- * or 32; the tile is 32 / width pixels high, one warp per tile; 0: 8). The learned engine runs 4 warps per block. */
+ * are staged in shared memory between a sampling phase and a sensing phase; 64: staged 32 deep with the crossing
+ * search taken by the whole warp; 1: the split engine, two launches per window, the first running the staged phases
+ * and the pixel model's clean segments for every pixel and posting each pixel at its first other segment, the second
+ * finishing the posted pixels' windows one thread per pixel; the instantaneous response only) and the tile width in
+ * pixels (4, 8, 16 or 32; the tile is 32 / width pixels high, one warp per tile; 0: 8). The learned engine runs 4 warps
+ * per block. */
 bs_status bs_engine_set_launch(bs_engine* e, int32_t warps_per_block, int32_t blocks_per_sm, int32_t stage,
                                int32_t tile_width);
 /* The current launch shape: warps per block, blocks per SM, staging depth, tile width. */
@@ -349,7 +354,7 @@ bs_status bs_engine_get_launch(const bs_engine* e, int32_t out[4]);
  * rebuilt when the window count, launch shape or proposal changes. */
 bs_status bs_engine_set_graph(bs_engine* e, int32_t on);
 /* The autotuner: times trial steps of `windows` windows from the current state for each candidate launch shape
- * (tile width 4, 8, 16 x warps per block 2, 4 x staging depth 0, 16; the learned engine: tile widths) without
+ * (tile width 4, 8, 16 x warps per block 2, 4 x stage 0, 1, 16, 64; the learned engine: tile widths) without
  * moving the models, and keeps the fastest. rows (cap x 4 doubles: tile width, warps, stage, ms) receives the
  * candidates tried, *n their number. */
 bs_status bs_engine_autotune(bs_engine* e, int32_t windows, void* stream, double* rows, size_t cap, size_t* n);

@@ -74,7 +74,7 @@ def mixed_sensors():
     return [a, b, c]
 
 
-@pytest.mark.parametrize("stage,tile", [(0, 8), (16, 8), (64, 8), (0, 4), (64, 16), (32, 32)])
+@pytest.mark.parametrize("stage,tile", [(0, 8), (16, 8), (64, 8), (0, 4), (64, 16), (32, 32), (1, 8), (1, 16)])
 def test_several_sensors_in_one_launch_equal_each_sensor_alone(cuda_lib, stage, tile):
     """A launch over three sensors of different sizes, seeds, thresholds and laws: each sensor's events and the
     total samples equal the oracle chain of each sensor run alone, bit for bit, over two calls."""
@@ -145,7 +145,7 @@ def test_blobs_1280x720_noise_first_windows_equal_the_oracle(cuda_lib):
     spec = wl.sensors[0]
     windows = 8
     want, st = simulate_port(spec, wl.rules, windows)
-    for stage in (0, 64):
+    for stage in (0, 64, 1):
         eng, models = make_engine(wl.sensors, wl.rules, stage, 8)
         got, samples = run_engine(eng, models, [windows])
         assert samples == st["pixel_samples"]
@@ -162,11 +162,12 @@ def test_six_sensors_first_windows_equal_the_oracle(cuda_lib):
     wl = W.six_sensors()
     windows = 2
     want = [simulate_port(s, wl.rules, windows) for s in wl.sensors]
-    eng, models = make_engine(wl.sensors, wl.rules)
-    got, samples = run_engine(eng, models, [windows])
-    assert samples == sum(st["pixel_samples"] for _, st in want)
-    for i, (s, (ev, _)) in enumerate(zip(wl.sensors, want)):
-        same_events(got[i], ev, s.width, f"sensor {i} ({s.width}x{s.height})")
+    for stage in (None, 1):
+        eng, models = make_engine(wl.sensors, wl.rules, stage, 8 if stage else None)
+        got, samples = run_engine(eng, models, [windows])
+        assert samples == sum(st["pixel_samples"] for _, st in want)
+        for i, (s, (ev, _)) in enumerate(zip(wl.sensors, want)):
+            same_events(got[i], ev, s.width, f"stage {stage}, sensor {i} ({s.width}x{s.height})")
     assert sum(len(ev["t_cross_ns"]) for ev, _ in want) > 10_000
 
 

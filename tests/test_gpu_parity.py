@@ -444,12 +444,14 @@ def test_midpoint_test_matches_numpy_fp32(cuda_lib):
 
 @pytest.mark.parametrize("stage,tile,graph", [(0, 8, True), (16, 8, True), (32, 8, True), (0, 4, True),
                                               (16, 16, True), (0, 32, True), (0, 8, False), (64, 8, True),
-                                              (64, 4, True), (64, 16, False)])
+                                              (64, 4, True), (64, 16, False), (1, 8, True), (1, 4, False),
+                                              (1, 32, True)])
 @pytest.mark.parametrize("case", ["edge", "blobs", "noise"])
 def test_engine_equals_the_oracle_chain(cuda_lib, case, stage, tile, graph):
     """The fused engine (sampler and pixel model on one thread, all windows in one launch; streamed, or staged in
-    shared memory per window, stage 64 with the warp-cooperative crossing search; any tile shape; from a CUDA graph
-    or not) gives the oracle chain's events (sample_window, then advance, per window) bit for bit."""
+    shared memory per window, stage 64 with the warp-cooperative crossing search, stage 1 split into two launches per
+    window; any tile shape; from a CUDA graph or not) gives the oracle chain's events (sample_window, then advance,
+    per window) bit for bit."""
     from ballasim_b200.engine import Engine
     from ballasim_b200.sensor import SensorModel
     from oracle.oracle import simulate_port
@@ -481,6 +483,33 @@ def test_engine_equals_the_oracle_chain(cuda_lib, case, stage, tile, graph):
         assert np.count_nonzero(ev["label"] == 1) > 5
 
 
+@pytest.mark.parametrize("l_min,windows", [(5, 6), (3, 10)])
+def test_split_engine_where_windows_overflow_the_stage(cuda_lib, l_min, windows):
+    """The split engine where every window (lattice level 5: 32 slots) or some windows overflow its 16-sample stage:
+    those are posted whole and walked again by the rest kernel; the events equal the oracle chain's."""
+    from dataclasses import replace
+
+    from ballasim_b200.engine import Engine
+    from ballasim_b200.sensor import SensorModel
+    from oracle.oracle import simulate_port
+
+    wl = W.small("noise", 40, 30, windows)
+    spec = wl.sensors[0]
+    r = replace(wl.rules, l_min=l_min, l_max=max(l_min, wl.rules.l_max))
+    p = resolve(resolve("ideal", spec.overrides), {"noise_shot_rate_hz": 40.0, "noise_ba_median_hz": 30.0,
+                                                   "leak_rate_hz": 3.0})
+    ora, st = simulate_port(spec, r, windows, params=p)
+    m = SensorModel(p, spec.width, spec.height, spec.seed, [{"type": "constant"}], spec.camera)
+    eng = Engine([(m, spec.field)], tol=r.tol, dark=r.dark, min_dt_ns=r.min_dt_ns,
+                 max_refine_levels=r.max_refine_levels, l_min=r.l_min, l_max=r.l_max)
+    eng.set_launch(0, 0, 1, 8)
+    eng.start(0)
+    s, _ = eng.run(windows)
+    assert s == st["pixel_samples"]
+    same_events(m.take_events(), ora, spec.width)
+    assert len(ora["t_cross_ns"]) > 20
+
+
 @pytest.mark.gpu
 def test_autotune_keeps_the_state_and_the_events(cuda_lib):
     """The autotuner's trial steps leave the models as they were: the run after it gives the events of a run
@@ -499,7 +528,7 @@ def test_autotune_keeps_the_state_and_the_events(cuda_lib):
         eng.start(0)
         if tune:
             rows = eng.autotune(4)
-            assert len(rows) == 18 and all(x["ms"] > 0 for x in rows)  # 3 tile widths x 2 warps x stage 0, 16, 64
+            assert len(rows) == 24 and all(x["ms"] > 0 for x in rows)  # 3 tile widths x 2 warps x stage 0, 1, 16, 64
             best = min(rows, key=lambda x: x["ms"])
             assert eng.launch["tile_width"] == best["tile_width"] and eng.launch["stage"] == best["stage"]
         s, e = eng.run(wl.windows)
