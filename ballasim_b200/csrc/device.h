@@ -126,7 +126,13 @@ void launch_advance_rows(const SensorConsts& k, const MapSoA& map, StateSoA in, 
                          const uint32_t* pixel, uint32_t n_rows, const int64_t* row_start, const int32_t* row_count,
                          const int64_t* t, const float* irr, uint64_t n_samples, int64_t t_state, int64_t t_end,
                          int32_t long_row, uint32_t* listed, EventBuf ev, unsigned long long* counters,
-                         const SensorConsts* k_dev, cudaStream_t stream);
+                         const SensorConsts* k_dev, void* rest, unsigned int* rest_count, int rest_blocks,
+                         cudaStream_t stream);
+// With `rest` (room for n_rows records of row_rest_bytes(); *rest_count zero before the launch), the row-major kernel
+// runs split: advance_rows_split_kernel stops a short run at its first segment that is not clean (or before its held
+// stretch to t_end) and advance_rows_rest_kernel (rest_blocks x 128 threads) finishes those rows one thread each.
+size_t row_rest_bytes();
+int rows_rest_blocks_per_sm();
 // sample_window: pass 0 counts, pass 1 writes at offsets.
 void launch_sample_window(const FieldDev& f, const SamplerRules& r, int64_t t_w, const uint32_t* pixel,
                           const uint8_t* level, uint32_t n, const float* carried_in, const uint64_t* sig_in,

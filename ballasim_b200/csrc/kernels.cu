@@ -769,6 +769,234 @@ __global__ void __launch_bounds__(32 * kRowsWarps) advance_rows_kernel(RowsArgs 
   warp_or(&a.counters[kCntErrors], err);
 }
 
+// The row-major kernel split like the split engine: advance_rows_split_kernel runs what advance_rows_kernel runs
+// except the pixel model's paths for a short run's segment that is not clean (and the held stretch after its last
+// sample): there the lane stops and posts its row (the state, the feed, the next sample's index), and
+// advance_rows_rest_kernel finishes the posted rows one thread each, reading their samples in place with the same
+// checks. A row's samples meet the same state in the same order, so the events and the refusals are the same.
+struct RowRest {
+  PixelRegs s;
+  int64_t prev_t;
+  float prev_v, x_prev;
+  uint32_t row;
+  int32_t next;     // the first sample not yet fed (cnt: only the held stretch to t_end is left)
+  uint32_t have_x;  // x_prev holds x at prev_v
+};
+
+struct RowRestList {
+  RowRest* rec;
+  unsigned int* count;
+  unsigned int capacity;
+};
+
+__global__ void __launch_bounds__(32 * kRowsWarps) advance_rows_split_kernel(RowsArgs a, RowRestList rl) {
+  const unsigned full = 0xffffffffu;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t row = (blockIdx.x * kRowsWarps + warp) * 32u + lane;
+  const bool in_rows = row < a.n_rows;
+  const uint32_t p = in_rows ? __ldg(a.pixel + row) : 0u;
+  unsigned long long err = 0, clamps = 0, samples = 0;
+  const bool valid = in_rows && p < a.n_pixels;
+  if (in_rows && !valid) err |= kErrPixelRange;
+  err |= mark_listed(a.listed, valid, p);
+  int64_t beg = 0;
+  int32_t cnt = 0;
+  if (valid) {
+    beg = __ldg(a.row_start + row);
+    cnt = __ldg(a.row_count + row);
+    if (cnt < 0 || beg < 0 || static_cast<uint64_t>(beg) + static_cast<uint64_t>(cnt) > a.n_samples) {
+      err |= kErrRunRange;
+      cnt = 0;
+      beg = 0;
+    }
+  }
+  const bool noise = a.k.noise != 0;
+  PixelRegs s{};
+  PixelMapRegs m{};
+  if (valid) {
+    load_state(a.in, p, noise, s);
+    load_map(a.map, p, m);
+  }
+  PixelCounters c;
+  const GlobalSink sink{a.ev, &a.counters[kCntEvents]};
+  int64_t prev_t = a.t_state;
+  float prev_v = s.held;
+  const bool longrun = cnt > a.long_row;
+
+  // The short runs' noise candidates, all lanes together (a long run meets its candidates in the pixel model).
+  if (noise) {
+    const GlobalRun run{a.t + beg, a.irr + beg, cnt};
+    noise_ahead(s, m, a.k, p, valid && !longrun, a.t_state, s.held, a.t_end, run, c);
+  }
+  // Short runs: one lane each, the clean segments in place; the first other one stops the lane there.
+  bool post = false;
+  int32_t next = 0;
+  float x_prev = 0.0f;
+  bool have_x = false;
+  if (cnt > 0 && !longrun) {
+    const int64_t* tp = a.t + beg;
+    const float* vp = a.irr + beg;
+    for (int32_t i = 0; i < cnt; ++i) {
+      const int64_t ti = __ldg(tp + i);
+      const float raw = __ldg(vp + i);
+      if (!isfinite(raw)) err |= kErrNonFinite;
+      const float vi = clamp_irr(raw, a.k.irr_max);
+      if (!(vi == raw)) ++clamps;
+      if (i == 0 ? ti < a.t_state : ti <= prev_t) {
+        err |= kErrOrder;
+        break;
+      }
+      if (ti > a.t_end) {
+        err |= kErrAfterEnd;
+        break;
+      }
+      if (i == 0 && ti == a.t_state) {  // a sample at the model time replaces the held one (pixel.h:777)
+        prev_v = vi;
+        continue;
+      }
+      if (!have_x) x_prev = x_sample(s, m, prev_v);
+      const float x1 = x_sample(s, m, vi);
+      have_x = true;
+      if (!clean_segment(s, m, a.k, prev_t, ti, prev_v, vi, x_prev, x1)) {
+        if (!(vi == raw)) --clamps;  // the rest kernel counts this sample's clamp (and checks it) again
+        post = true;
+        next = i;
+        break;
+      }
+      ++c.pieces;
+      if (ti - prev_t > 2) ++c.leaves;
+      s.t_search = maxi(s.t_search, ti);
+      x_prev = x1;
+      prev_t = ti;
+      prev_v = vi;
+    }
+  }
+
+  // Long runs: the whole warp on each, one after another.
+  for (unsigned pend = __ballot_sync(full, longrun); pend != 0u; pend &= pend - 1u) {
+    const int r = __ffs(pend) - 1;
+    PixelRegs u = shfl_regs(s, r);
+    const PixelMapRegs um = shfl_map(m, r);
+    const uint32_t pr = __shfl_sync(full, p, r);
+    const int64_t br = __shfl_sync(full, beg, r);
+    const int32_t nr = __shfl_sync(full, cnt, r);
+    PixelCounters cu;
+    const LaneZeroSink lz{sink};
+    int64_t pt = a.t_state;
+    float pv = u.held, px = x_sample(u, um, u.held);
+    coop_run(u, um, a, pr, lz, cu, a.t + br, a.irr + br, nr, lane, pt, pv, px, err, clamps);
+    if (static_cast<int>(lane) == r) {
+      s = u;
+      c.pieces += cu.pieces;
+      c.leaves += cu.leaves;
+      c.noise_candidates += cu.noise_candidates;
+      prev_t = pt;
+      prev_v = pv;
+    }
+  }
+
+  if (valid) {
+    samples = static_cast<unsigned long long>(cnt);
+    if (!post && prev_t < a.t_end) {  // the held stretch to t_end goes to the rest kernel
+      post = true;
+      next = cnt;
+    }
+    if (!post) {
+      if (cnt > 0) s.held = prev_v;
+      store_state(a.out, p, noise, s);
+    }
+  }
+  // One record per stopped row, the warp's records reserved together.
+  __syncwarp();
+  const unsigned posting = __ballot_sync(full, post);
+  if (posting != 0u) {
+    const int leader = __ffs(posting) - 1;
+    unsigned int base = 0;
+    if (static_cast<int>(lane) == leader) base = atomicAdd(rl.count, static_cast<unsigned int>(__popc(posting)));
+    base = __shfl_sync(full, base, leader);
+    if (post) {
+      const unsigned int i = base + static_cast<unsigned int>(__popc(posting & ((1u << lane) - 1u)));
+      if (i >= rl.capacity) {
+        err |= kErrRestList;
+      } else {
+        RowRest& r = rl.rec[i];
+        r.s = s;
+        r.prev_t = prev_t;
+        r.prev_v = prev_v;
+        r.x_prev = x_prev;
+        r.row = row;
+        r.next = next;
+        r.have_x = have_x ? 1u : 0u;
+      }
+    }
+  }
+  __syncwarp();
+  warp_add(&a.counters[kCntClamps], clamps);
+  warp_add(&a.counters[kCntPieces], c.pieces);
+  warp_add(&a.counters[kCntLeaves], c.leaves);
+  warp_add(&a.counters[kCntSamples], samples);
+  warp_add(&a.counters[kCntNoise], c.noise_candidates);
+  warp_or(&a.counters[kCntErrors], err);
+}
+
+// The posted rows, one thread each: the rest of the row through the full pixel model with advance_rows_kernel's
+// checks, the held stretch to t_end, the state stored.
+__global__ void __launch_bounds__(128) advance_rows_rest_kernel(RowsArgs a, RowRestList rl) {
+  const unsigned int count = min(*rl.count, rl.capacity);
+  const bool noise = a.k.noise != 0;
+  for (unsigned int q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
+    const RowRest& r = rl.rec[q];
+    const uint32_t p = __ldg(a.pixel + r.row);
+    const int64_t beg = __ldg(a.row_start + r.row);
+    const int32_t cnt = __ldg(a.row_count + r.row);
+    PixelRegs s = r.s;
+    PixelMapRegs m;
+    load_map(a.map, p, m);
+    PixelCounters c;
+    const ThreadSink sink{a.ev, &a.counters[kCntEvents]};
+    unsigned long long err = 0, clamps = 0;
+    int64_t prev_t = r.prev_t;
+    float prev_v = r.prev_v, x_prev = r.x_prev;
+    bool have_x = r.have_x != 0u;
+    const int64_t* tp = a.t + beg;
+    const float* vp = a.irr + beg;
+    for (int32_t i = r.next; i < cnt; ++i) {
+      const int64_t ti = __ldg(tp + i);
+      const float raw = __ldg(vp + i);
+      if (!isfinite(raw)) err |= kErrNonFinite;
+      const float vi = clamp_irr(raw, a.k.irr_max);
+      if (!(vi == raw)) ++clamps;
+      if (i == 0 ? ti < a.t_state : ti <= prev_t) {
+        err |= kErrOrder;
+        break;
+      }
+      if (ti > a.t_end) {
+        err |= kErrAfterEnd;
+        break;
+      }
+      if (i == 0 && ti == a.t_state) {
+        prev_v = vi;
+        continue;
+      }
+      if (!have_x) x_prev = x_sample(s, m, prev_v);
+      const float x1 = x_sample(s, m, vi);
+      feed_segment(s, m, a.k, a.kd, p, sink, c, prev_t, ti, prev_v, vi, x_prev, x1);
+      x_prev = x1;
+      have_x = true;
+      prev_t = ti;
+      prev_v = vi;
+    }
+    feed_held(s, m, a.kd, p, sink, c, prev_t, prev_v, a.t_end);
+    if (cnt > 0) s.held = prev_v;
+    store_state(a.out, p, noise, s);
+    if (clamps) atomicAdd(&a.counters[kCntClamps], clamps);
+    if (c.pieces) atomicAdd(&a.counters[kCntPieces], static_cast<unsigned long long>(c.pieces));
+    if (c.leaves) atomicAdd(&a.counters[kCntLeaves], static_cast<unsigned long long>(c.leaves));
+    if (c.noise_candidates) atomicAdd(&a.counters[kCntNoise], static_cast<unsigned long long>(c.noise_candidates));
+    if (err) atomicOr(&a.counters[kCntErrors], err);
+  }
+}
+
 // The pixels no run lists: each advances on its held sample to t_end.
 __global__ void __launch_bounds__(128) advance_unlisted_kernel(RowsArgs a) {
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2413,12 +2641,19 @@ void launch_advance_rows(const SensorConsts& k, const MapSoA& map, StateSoA in, 
                          const uint32_t* pixel, uint32_t n_rows, const int64_t* row_start, const int32_t* row_count,
                          const int64_t* t, const float* irr, uint64_t n_samples, int64_t t_state, int64_t t_end,
                          int32_t long_row, uint32_t* listed, EventBuf ev, unsigned long long* counters,
-                         const SensorConsts* k_dev, cudaStream_t stream) {
+                         const SensorConsts* k_dev, void* rest, unsigned int* rest_count, int rest_blocks,
+                         cudaStream_t stream) {
   RowsArgs a{k, map, in, out, n_pixels, pixel, n_rows, row_start, row_count, t, irr, n_samples, t_state, t_end,
              long_row, listed, ev, counters, k_dev};
   if (n_rows > 0) {
     const unsigned grid = (n_rows + 32 * kRowsWarps - 1) / (32 * kRowsWarps);
-    advance_rows_kernel<<<grid, 32 * kRowsWarps, 0, stream>>>(a);
+    if (rest != nullptr) {
+      const RowRestList rl{static_cast<RowRest*>(rest), rest_count, n_rows};
+      advance_rows_split_kernel<<<grid, 32 * kRowsWarps, 0, stream>>>(a, rl);
+      advance_rows_rest_kernel<<<rest_blocks, 128, 0, stream>>>(a, rl);
+    } else {
+      advance_rows_kernel<<<grid, 32 * kRowsWarps, 0, stream>>>(a);
+    }
   }
   if (n_rows < n_pixels) advance_unlisted_kernel<<<(n_pixels + 127) / 128, 128, 0, stream>>>(a);
 }
@@ -2496,6 +2731,12 @@ void launch_engine_split(const EngineSensor* sensors_dev, int n_sensors, uint32_
 }
 
 size_t rest_record_bytes() { return sizeof(RestRecord); }
+size_t row_rest_bytes() { return sizeof(RowRest); }
+int rows_rest_blocks_per_sm() {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, advance_rows_rest_kernel, 128, 0);
+  return n;
+}
 
 int engine_rest_blocks_per_sm() {
   int n = 0;

@@ -278,7 +278,11 @@ struct Model {
   DevBuf<float> s_irr, s_frame;
   int64_t t_state = 0;
   bool initialized = false;
-  int block = 0;  // 0: the row-major kernel (instantaneous response); else the per-pixel kernel's block
+  // 0: the row-major kernel split in two (instantaneous response); 1: the row-major kernel in one launch; else the
+  // per-pixel kernel's block.
+  int block = 0;
+  DevBuf<unsigned char> row_rest;  // the split row-major kernel's posted rows (room for every pixel) and their count
+  DevBuf<unsigned int> row_rest_count;
   int32_t long_row = 32;  // the row-major kernel: runs longer than this are walked by the whole warp
   uint64_t stat_pieces = 0, stat_leaves = 0, stat_clamps = 0, stat_samples = 0, stat_noise = 0, stat_launches = 0,
            stat_reruns = 0;
@@ -608,15 +612,27 @@ struct Model {
     for (int attempt = 0;; ++attempt) {
       CK(cudaMemsetAsync(counters.p, 0, kCntWords * sizeof(unsigned long long), s));
       const EventBuf evb{events.p, static_cast<unsigned long long>(event_cap)};
-      if (!k.cascade && block == 0) {
-        // The instantaneous response: row-major over the runs, long runs walked by the whole warp.
+      if (!k.cascade && (block == 0 || block == 1)) {
+        // The instantaneous response: row-major over the runs, long runs walked by the whole warp; split (block 0):
+        // a row stopped at its first segment that is not clean is finished by a second kernel, one thread per row.
         CK(cudaMemsetAsync(listed.p, 0, ((n + 31) / 32) * sizeof(uint32_t), s));
         k_dev.ensure(1);
         CK(cudaMemcpyAsync(k_dev.p, &k, sizeof(SensorConsts), cudaMemcpyHostToDevice, s));
+        void* rest = nullptr;
+        int rest_blocks = 0;
+        if (block == 0) {
+          rest = row_rest.ensure(static_cast<size_t>(n) * row_rest_bytes());
+          row_rest_count.ensure(1);
+          CK(cudaMemsetAsync(row_rest_count.p, 0, sizeof(unsigned int), s));
+          int dev = 0, sms = 0;
+          CK(cudaGetDevice(&dev));
+          CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+          rest_blocks = sms * std::max(1, rows_rest_blocks_per_sm());
+        }
         CK(cudaEventRecord(timer.a, s));
         launch_advance_rows(k, map, soa[cur], soa[1 - cur], n, r.pixel, static_cast<uint32_t>(r.n), r.row_start,
                             r.row_count, r.t, r.irr, r.n_samples, t_state, t_end, long_row, listed.p, evb, counters.p,
-                            k_dev.p, s);
+                            k_dev.p, rest, row_rest_count.p, rest_blocks, s);
       } else {
         CK(cudaMemsetAsync(row_of.p, 0xFF, n * sizeof(int32_t), s));
         launch_scatter_rows(r.pixel, static_cast<uint32_t>(r.n), row_of.p, n, counters.p, s);
@@ -2224,8 +2240,8 @@ bs_status bs_model_set_long_run(bs_model* m, int32_t samples) {
 bs_status bs_model_set_block(bs_model* m, int32_t threads) {
   return guarded([&] {
     NEED(m);
-    if (threads != 0 && (threads < 32 || threads > 128 || threads % 32 != 0)) {
-      throw std::invalid_argument("threads per block must be 32, 64, 96 or 128");
+    if (threads != 0 && threads != 1 && (threads < 32 || threads > 128 || threads % 32 != 0)) {
+      throw std::invalid_argument("threads per block must be 32, 64, 96 or 128 (0, 1: the row-major kernel)");
     }
     m->block = threads;
   });

@@ -371,6 +371,8 @@ class SensorModel:
         _lib.check(_lib.lib().bs_model_set_long_run(self._h, int(samples)))
 
     def set_block(self, threads: int) -> None:
-        """Launch policy of the pixel model on runs: 0, the row-major kernel with staged samples (the default for
-        the instantaneous response); 32, 64, 96 or 128, one thread per pixel with that many threads per block."""
+        """Launch policy of the pixel model on runs: 0, the row-major kernel split in two launches (the default for
+        the instantaneous response: runs stopped at a segment that is not clean are finished one thread each by a
+        second kernel); 1, the row-major kernel in one launch; 32, 64, 96 or 128, one thread per pixel with that many
+        threads per block."""
         _lib.check(_lib.lib().bs_model_set_block(self._h, int(threads)))

@@ -445,7 +445,8 @@ def run_runs(args, rank: int, world: int) -> dict | None:
     n_launch = advance_launches / args.steps
     alg = b_sense(wl.pixels, wl.windows, int(per_step_samples), int(per_step_events))
     achieved = alg / (kms_total * 1e-3) / 1e9
-    kname = "advance_runs_kernel" if args.block else "advance_rows_kernel"
+    kname = {0: "advance_rows_split_kernel+advance_rows_rest_kernel", 1: "advance_rows_kernel"}.get(
+        args.block, "advance_runs_kernel")
     cap = ncu_capture("runs:" + wl.name, kname)
     calls = wl.windows * len(wl.sensors)
     return {
@@ -460,9 +461,9 @@ def run_runs(args, rank: int, world: int) -> dict | None:
                    "parallelism": f"replicas x{world}", "advance_block": args.block or "row-major",
                    "long_run": args.long_run or 32},
         # Per sensor and window: levels, the input check, two sample_window passes, three scan kernels and the pixel
-        # model (advance_rows_kernel; every pixel is listed, so no advance_unlisted_kernel; --block adds the scatter);
-        # per sensor and step the first frame and init.
-        "gpu_launches": (8 + (1 if args.block else 0)) * calls * args.steps + 2 * len(wl.sensors) * args.steps,
+        # model (the split row-major kernel's two launches, --block 1 one, --block n > 1 the scatter and one; every
+        # pixel is listed, so no advance_unlisted_kernel); per sensor and step the first frame and init.
+        "gpu_launches": (7 + (1 if args.block == 1 else 2)) * calls * args.steps + 2 * len(wl.sensors) * args.steps,
         "clocks": clocks,
         "e2e": {"value": samples_all / e2e_s if e2e_times else None, "unit": "pixel-samples/s",
                 "h2d_bytes_per_step": sum(int(f.nbytes) for f in frames), "d2h_bytes_per_step": d2h},
@@ -735,7 +736,8 @@ def main():
                     default=DEFAULT_WORKLOAD)
     ap.add_argument("--cpu-windows", type=int, default=0,
                     help="windows of every sensor in the reference's bounded sample (0: the workload's default)")
-    ap.add_argument("--block", type=int, default=0, help="runs_* workloads: threads per block of advance_runs")
+    ap.add_argument("--block", type=int, default=0,
+                    help="runs_* workloads: 0 the split row-major kernel, 1 unsplit, n > 1 advance_runs_kernel's block")
     ap.add_argument("--long-run", type=int, default=0,
                     help="runs_* workloads: runs longer than this are walked by a whole warp (-1: none)")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -182,8 +182,9 @@ bs_status bs_model_state_bytes(const bs_model* m, size_t* n);
 bs_status bs_model_save_state(const bs_model* m, uint8_t* out, size_t n);
 bs_status bs_model_load_state(bs_model* m, const uint8_t* data, size_t n);
 /* Launch policy of the pixel model on CSR runs. 0 (the default): the instantaneous response runs row-major, one warp
- * per 32 runs, runs longer than the long-run threshold walked by the whole warp (the cascade runs one thread per
- * pixel, 128 per block);
+ * per 32 runs, runs longer than the long-run threshold walked by the whole warp, split in two launches: a run stopped
+ * at its first segment that is not clean (or before its held stretch to t_end) is finished by a second kernel, one
+ * thread per run (the cascade runs one thread per pixel, 128 per block); 1: the same row-major kernel in one launch;
  * 32, 64, 96 or 128: one thread per pixel with that many threads per block, for every photoreceptor. */
 bs_status bs_model_set_block(bs_model* m, int32_t threads);
 /* The row-major kernel's threads per pixel: runs longer than `samples` are walked by all 32 lanes of a warp, 32

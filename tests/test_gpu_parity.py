@@ -25,7 +25,7 @@ def same_events(dev: dict, ora: dict, width: int) -> None:
         assert np.array_equal(a, b), f"column {k} differs"
 
 
-@pytest.mark.parametrize("block", [0, 128])
+@pytest.mark.parametrize("block", [0, 1, 128])
 @pytest.mark.parametrize("overrides", [
     {},
     dict(W.MISMATCH),
@@ -35,7 +35,8 @@ def same_events(dev: dict, ora: dict, width: int) -> None:
 ])
 def test_pixel_model_on_random_runs(cuda_lib, oracle_port, overrides, block):
     """The pixel model on random ragged runs (random pixel subsets in random order) against the oracle: the
-    row-major kernel (block 0) and the one-thread-per-pixel kernel (block 128)."""
+    row-major kernel split in two launches (block 0) and in one (block 1), and the one-thread-per-pixel kernel
+    (block 128)."""
     from ballasim_b200.sensor import SensorModel
 
     rng = np.random.default_rng(17 + len(overrides))
@@ -58,9 +59,10 @@ def test_pixel_model_on_random_runs(cuda_lib, oracle_port, overrides, block):
     assert dev.time_ns == t_end
 
 
+@pytest.mark.parametrize("block", [0, 1])
 @pytest.mark.parametrize("long_run", [0, 1, 5, -1])
 @pytest.mark.parametrize("layout", ["tiled", "long", "shuffled", "gaps", "sparse"])
-def test_row_major_kernel_on_every_run_layout(cuda_lib, oracle_port, layout, long_run):
+def test_row_major_kernel_on_every_run_layout(cuda_lib, oracle_port, layout, long_run, block):
     """The row-major kernel against the oracle on every run layout (runs in pixel order tiling the sample arrays,
     runs of hundreds to thousands of samples, runs whose starts are shuffled or leave gaps, a sparse listing whose
     other pixels advance on their held sample) and split between its two walks: runs longer than long_run walked by
@@ -74,6 +76,7 @@ def test_row_major_kernel_on_every_run_layout(cuda_lib, oracle_port, layout, lon
                           "leak_rate_hz": 1.0})
     dev = SensorModel(p, Wd, Hd, 6, [{"type": "constant"}], 0)
     dev.set_long_run(long_run)
+    dev.set_block(block)
     ora = oracle_port.Model(p, Wd, Hd, 6, 0)
     irr0 = rng.uniform(20, 300, n).astype(np.float32)
     dev.init(0, irr0.reshape(n, 1))
