@@ -127,10 +127,12 @@ void launch_advance_rows(const SensorConsts& k, const MapSoA& map, StateSoA in, 
                          const int64_t* t, const float* irr, uint64_t n_samples, int64_t t_state, int64_t t_end,
                          int32_t long_row, uint32_t* listed, EventBuf ev, unsigned long long* counters,
                          const SensorConsts* k_dev, void* rest, unsigned int* rest_count, int rest_blocks,
-                         cudaStream_t stream);
+                         bool first_call, cudaStream_t stream);
 // With `rest` (room for n_rows records of row_rest_bytes(); *rest_count zero before the launch), the row-major kernel
 // runs split: advance_rows_split_kernel stops a short run at its first segment that is not clean (or before its held
 // stretch to t_end) and advance_rows_rest_kernel (rest_blocks x 128 threads) finishes those rows one thread each.
+// first_call: the model's first call since init (its first segments are then also tested with the search armed
+// after their start).
 size_t row_rest_bytes();
 int rows_rest_blocks_per_sm();
 // sample_window: pass 0 counts, pass 1 writes at offsets.

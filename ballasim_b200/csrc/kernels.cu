@@ -789,6 +789,10 @@ struct RowRestList {
   unsigned int capacity;
 };
 
+// kFirst: the model's first call after init, where every pixel's search is armed after its first segment's start:
+// such a segment is also taken in place when clean (clean_after_start) rather than posted; the other calls' kernel
+// leaves that test out of its loop.
+template <bool kFirst>
 __global__ void __launch_bounds__(32 * kRowsWarps) advance_rows_split_kernel(RowsArgs a, RowRestList rl) {
   const unsigned full = 0xffffffffu;
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
@@ -857,7 +861,8 @@ __global__ void __launch_bounds__(32 * kRowsWarps) advance_rows_split_kernel(Row
       if (!have_x) x_prev = x_sample(s, m, prev_v);
       const float x1 = x_sample(s, m, vi);
       have_x = true;
-      if (!clean_segment(s, m, a.k, prev_t, ti, prev_v, vi, x_prev, x1)) {
+      if (!clean_segment(s, m, a.k, prev_t, ti, prev_v, vi, x_prev, x1) &&
+          !(kFirst && clean_after_start(s, m, a.k, prev_t, ti, prev_v, vi, x_prev, x1))) {
         if (!(vi == raw)) --clamps;  // the rest kernel counts this sample's clamp (and checks it) again
         post = true;
         next = i;
@@ -2642,14 +2647,15 @@ void launch_advance_rows(const SensorConsts& k, const MapSoA& map, StateSoA in, 
                          const int64_t* t, const float* irr, uint64_t n_samples, int64_t t_state, int64_t t_end,
                          int32_t long_row, uint32_t* listed, EventBuf ev, unsigned long long* counters,
                          const SensorConsts* k_dev, void* rest, unsigned int* rest_count, int rest_blocks,
-                         cudaStream_t stream) {
+                         bool first_call, cudaStream_t stream) {
   RowsArgs a{k, map, in, out, n_pixels, pixel, n_rows, row_start, row_count, t, irr, n_samples, t_state, t_end,
              long_row, listed, ev, counters, k_dev};
   if (n_rows > 0) {
     const unsigned grid = (n_rows + 32 * kRowsWarps - 1) / (32 * kRowsWarps);
     if (rest != nullptr) {
       const RowRestList rl{static_cast<RowRest*>(rest), rest_count, n_rows};
-      advance_rows_split_kernel<<<grid, 32 * kRowsWarps, 0, stream>>>(a, rl);
+      if (first_call) advance_rows_split_kernel<true><<<grid, 32 * kRowsWarps, 0, stream>>>(a, rl);
+      else advance_rows_split_kernel<false><<<grid, 32 * kRowsWarps, 0, stream>>>(a, rl);
       advance_rows_rest_kernel<<<rest_blocks, 128, 0, stream>>>(a, rl);
     } else {
       advance_rows_kernel<<<grid, 32 * kRowsWarps, 0, stream>>>(a);

@@ -278,6 +278,7 @@ struct Model {
   DevBuf<float> s_irr, s_frame;
   int64_t t_state = 0;
   bool initialized = false;
+  bool fresh = false;  // no call has advanced the model since init (every pixel's search armed at t0 + 1)
   // 0: the row-major kernel split in two (instantaneous response); 1: the row-major kernel in one launch; else the
   // per-pixel kernel's block.
   int block = 0;
@@ -485,6 +486,7 @@ struct Model {
     if (mode() == 2 && p.initial_state == 1) stationary(t0, irr0_dev, host_copy, s);
     t_state = t0;
     initialized = true;
+    fresh = true;
     last_events = 0;
     kept.clear();
     n_held = n_ready = 0;  // a new run: nothing held by the output stage
@@ -632,7 +634,7 @@ struct Model {
         CK(cudaEventRecord(timer.a, s));
         launch_advance_rows(k, map, soa[cur], soa[1 - cur], n, r.pixel, static_cast<uint32_t>(r.n), r.row_start,
                             r.row_count, r.t, r.irr, r.n_samples, t_state, t_end, long_row, listed.p, evb, counters.p,
-                            k_dev.p, rest, row_rest_count.p, rest_blocks, s);
+                            k_dev.p, rest, row_rest_count.p, rest_blocks, fresh, s);
       } else {
         CK(cudaMemsetAsync(row_of.p, 0xFF, n * sizeof(int32_t), s));
         launch_scatter_rows(r.pixel, static_cast<uint32_t>(r.n), row_of.p, n, counters.p, s);
@@ -664,6 +666,7 @@ struct Model {
       last_events = static_cast<size_t>(c[kCntEvents]);
       cur = 1 - cur;
       t_state = t_end;
+      fresh = false;
       return;
     }
   }
@@ -1061,6 +1064,7 @@ struct Model {
     CK(cudaMemcpy(b.u32.p, u32.data(), nu * sizeof(uint32_t), cudaMemcpyHostToDevice));
     t_state = h.t_state;
     initialized = h.initialized != 0;
+    fresh = false;
     last_events = 0;
     kept.clear();
   }
@@ -1904,6 +1908,7 @@ struct Engine {
         m->kept.clear();
         m->cur = 1 - m->cur;
         m->t_state = t0 + static_cast<int64_t>(windows) * kWindowNs;
+        m->fresh = false;
         carried_cur[i] = 1 - carried_cur[i];
         if (mlp) lcur[i] = 1 - lcur[i];
       }
