@@ -172,6 +172,7 @@ _SIGS = {
     "bs_engine_start": (C.c_int32, [_P, C.c_int64, _P]),
     "bs_engine_start_frames": (C.c_int32, [_P, C.c_int64, _P, _P]),
     "bs_engine_run": (C.c_int32, [_P, C.c_int32, _P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "bs_engine_take_events": (C.c_int32, [_P, _P]),
     "bs_engine_set_launch": (C.c_int32, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "bs_engine_get_launch": (C.c_int32, [_P, _P]),
     "bs_engine_set_graph": (C.c_int32, [_P, C.c_int32]),

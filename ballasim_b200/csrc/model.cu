@@ -720,23 +720,37 @@ struct Model {
   mutable DevBuf<unsigned char> col_dev;
   mutable PinBuf<unsigned char> col_pin;
 
+  // A download's columns: the caller's array, the element size and the column's offset in the pinned buffer.
+  struct Col {
+    void* dst;
+    size_t elem;
+    size_t at;
+  };
+  mutable Col pend_cols[12] = {};
+  mutable size_t pend_count = 0;
+  mutable std::chrono::steady_clock::time_point pend_w0;
+
   // The events of a device buffer, sorted on the device, split there into the requested columns (256-byte aligned,
   // side by side), copied out in one transfer through pinned memory, then each column into the caller's array.
   void download_columns(const RawEvent* dev, size_t count, bs_event_columns* o, cudaStream_t s) const {
-    const auto w0 = std::chrono::steady_clock::now();
+    if (!download_enqueue(dev, count, o, s)) return;
+    CK(cudaStreamSynchronize(s));
+    download_finish();
+  }
+
+  // The download's device part queued on stream s (the sort, the column split, the copy out, with the timing events;
+  // take_timer_copy.b marks the copy's end); false when there is nothing to copy.
+  bool download_enqueue(const RawEvent* dev, size_t count, const bs_event_columns* o, cudaStream_t s) const {
+    pend_w0 = std::chrono::steady_clock::now();
+    pend_count = 0;
     for (double& v : take_ms) v = 0.0;
-    if (count == 0) return;
+    if (count == 0) return false;
     if (count > 0x7fffffffull) throw std::invalid_argument("too many events in one call");
     const uint32_t n = static_cast<uint32_t>(count);
     sorted.ensure(count);
     sort_scratch.ensure(sort_events_scratch_bytes(n));
     CK(cudaEventRecord(take_timer.a, s));
     CK(sort_events(dev, n, sorted.p, sort_scratch.p, s));
-    struct Col {
-      void* dst;
-      size_t elem;
-      size_t at;
-    };
     Col cols[12] = {{o->pixel, 4, 0},      {o->x, 2, 0},     {o->y, 2, 0},  {o->p, 1, 0},
                     {o->t_cross_ns, 8, 0}, {o->t_reported_ns, 8, 0},        {o->label, 1, 0},
                     {o->flags, 2, 0},      {o->ds, 4, 0},    {o->dn, 4, 0}, {o->dl, 4, 0},
@@ -747,7 +761,7 @@ struct Model {
       c.at = total;
       total += (c.elem * count + 255) & ~size_t{255};
     }
-    if (total == 0) return;
+    if (total == 0) return false;
     col_dev.ensure(total);
     col_pin.ensure(total);
     unsigned char* base = col_dev.p;
@@ -762,22 +776,30 @@ struct Model {
     CK(cudaEventRecord(take_timer.b, s));
     CK(cudaMemcpyAsync(col_pin.p, col_dev.p, total, cudaMemcpyDeviceToHost, s));
     CK(cudaEventRecord(take_timer_copy.b, s));
-    CK(cudaStreamSynchronize(s));
+    std::copy(cols, cols + 12, pend_cols);
+    pend_count = count;
+    return true;
+  }
+
+  // The download's host part, once its copy out has completed: the columns into the caller's arrays, up to 8
+  // threads, each over an equal share of all the columns' bytes (a share can span columns; the caller's fresh pages
+  // are first touched here, so the shares fault in parallel).
+  void download_finish() const {
+    const size_t count = pend_count;
+    if (count == 0) return;
     const auto w1 = std::chrono::steady_clock::now();
     float ms_split = 0.0f, ms_copy = 0.0f;
     cudaEventElapsedTime(&ms_split, take_timer.a, take_timer.b);
     cudaEventElapsedTime(&ms_copy, take_timer.b, take_timer_copy.b);
     take_ms[0] = ms_split;
     take_ms[1] = ms_copy;
-    // The columns into the caller's arrays: up to 8 threads, each over an equal share of all the columns' bytes
-    // (a share can span columns; the caller's fresh pages are first touched here, so the shares fault in parallel).
     size_t bytes = 0;
-    for (const Col& c : cols) {
+    for (const Col& c : pend_cols) {
       if (c.dst) bytes += c.elem * count;
     }
     const auto copy_range = [&](size_t lo, size_t hi) {
       size_t base_at = 0;
-      for (const Col& c : cols) {
+      for (const Col& c : pend_cols) {
         if (!c.dst) continue;
         const size_t len = c.elem * count, a = std::max(lo, base_at), b = std::min(hi, base_at + len);
         if (a < b) {
@@ -797,7 +819,8 @@ struct Model {
     }
     const auto w2 = std::chrono::steady_clock::now();
     take_ms[2] = std::chrono::duration<double, std::milli>(w2 - w1).count();
-    take_ms[3] = std::chrono::duration<double, std::milli>(w2 - w0).count();
+    take_ms[3] = std::chrono::duration<double, std::milli>(w2 - pend_w0).count();
+    pend_count = 0;
   }
 
   // ---- the output stage: events in output order, released at the model time's cut, the rest held ----
@@ -1920,6 +1943,30 @@ struct Engine {
     step(windows, s, true, samples_out, events_out);
   }
 
+  // Every sensor's events as bs_model_take_events gives them, into outs[i] for sensor i: the sensors' device parts
+  // (sort, column split, copy out) are queued on their own streams first, then each sensor's host copies run as soon
+  // as its copy out has completed, while the device works on the sensors after it.
+  void take_events(bs_event_columns* outs) {
+    std::vector<char> queued(models.size(), 0);
+    for (size_t i = 0; i < models.size(); ++i) {
+      Model* m = models[i];
+      if (m->kept.empty() && m->last_events > 0) {
+        queued[i] = m->download_enqueue(m->events.p, m->last_events, &outs[i], m->own) ? 1 : 0;
+      }
+    }
+    for (size_t i = 0; i < models.size(); ++i) {
+      Model* m = models[i];
+      if (queued[i]) {
+        CK(cudaEventSynchronize(m->take_timer_copy.b));
+        m->download_finish();
+      } else if (!m->kept.empty()) {
+        m->columns(m->kept, &outs[i]);
+      }
+      m->kept.clear();
+      m->last_events = 0;
+    }
+  }
+
   void set_launch(int32_t warps, int32_t per_sm, int32_t stg, int32_t lw) {
     if (warps < 0 || warps > 4) throw std::invalid_argument("engine: warps per block must lie in [1, 4]");
     if (per_sm < 0 || per_sm > 32) throw std::invalid_argument("engine: blocks_per_sm in [0, 32]");
@@ -2461,6 +2508,13 @@ bs_status bs_engine_run(bs_engine* e, int32_t windows, void* stream, uint64_t* p
   return guarded([&] {
     NEED(e);
     e->run(windows, stream ? static_cast<cudaStream_t>(stream) : e->own, pixel_samples, events);
+  });
+}
+bs_status bs_engine_take_events(bs_engine* e, bs_event_columns* out) {
+  return guarded([&] {
+    NEED(e);
+    NEED(out);
+    e->take_events(out);
   });
 }
 bs_status bs_engine_set_launch(bs_engine* e, int32_t warps_per_block, int32_t blocks_per_sm, int32_t stage,

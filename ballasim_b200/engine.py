@@ -72,6 +72,32 @@ class Engine:
         _lib.check(_lib.lib().bs_engine_run(self._h, int(windows), stream, C.byref(s), C.byref(e)))
         return s.value, e.value
 
+    def take_events(self, with_pixel: bool = False) -> list[dict]:
+        """Every sensor's events, as SensorModel.take_events gives them, in the engine's sensor order; the models'
+        lists are cleared. The sensors' device sorts and copies are queued together, and each sensor's host copies
+        run while the device works on the sensors after it."""
+        import contextlib
+
+        from .sensor import column_struct, new_columns
+
+        models = [m for m, _ in self.sensors]
+        with contextlib.ExitStack() as stack:
+            for m in models:
+                stack.enter_context(m._lock)
+            out, structs = [], []
+            for m in models:
+                n = C.c_size_t()
+                _lib.check(_lib.lib().bs_model_event_count(m._h, C.byref(n)))
+                cols = new_columns(n.value)
+                px = np.zeros(n.value, np.uint32) if with_pixel else None
+                structs.append(column_struct(cols, px))
+                if with_pixel:
+                    cols["pixel"] = px
+                out.append(cols)
+            arr = (_lib.EventColumns * len(structs))(*structs)
+            _lib.check(_lib.lib().bs_engine_take_events(self._h, arr))
+        return out
+
     def set_launch(self, warps_per_block: int = 0, blocks_per_sm: int = 0, stage: int = 0,
                    tile_width: int = 0) -> None:
         """Launch shape of the persistent grid, the stage (0 streaming; 16 or 32 staged in shared memory; 64 staged

@@ -338,6 +338,11 @@ bs_status bs_engine_start_frames(bs_engine* e, int64_t t0_ns, const float* const
 /* Samples and senses `windows` whole windows of every sensor from the current model time; the events are kept in
  * each model (bs_model_take_events). *pixel_samples and *events receive the totals of the call. */
 bs_status bs_engine_run(bs_engine* e, int32_t windows, void* stream, uint64_t* pixel_samples, uint64_t* events);
+/* bs_model_take_events for every sensor of the engine at once (out[i]: sensor i's columns, sized by
+ * bs_model_event_count): the sensors' device sorts, column splits and copies out are queued together, and each
+ * sensor's copies into the caller's arrays run while the device works on the sensors after it. No counterpart in the
+ * reference, whose engine takes one camera's events at a time; the columns and the order are bs_model_take_events'. */
+bs_status bs_engine_take_events(bs_engine* e, bs_event_columns* out);
 /* Launch shape: warps per block and blocks per SM of the persistent grid (0: the defaults, 4 and as many as fit),
  * the staging depth (0: the sampler feeds the pixel model sample by sample; 16 or 32: per window each lane's samples
  * are staged in shared memory between a sampling phase and a sensing phase; 64: staged 32 deep with the crossing

@@ -93,6 +93,32 @@ def test_several_sensors_in_one_launch_equal_each_sensor_alone(cuda_lib, stage, 
     assert np.count_nonzero(got[1]["label"] == 1) > 5  # sensor 1's noise events are there
 
 
+def test_engine_take_of_every_sensor_equals_each_model_take(cuda_lib):
+    """Engine.take_events (every sensor's sort and copy queued together, the host copies overlapped) gives each
+    sensor the columns SensorModel.take_events gives, over two calls, with and without the pixel column."""
+    specs = mixed_sensors()
+    rules = W.Rules()
+    got = []
+    for batched in (False, True):
+        eng, models = make_engine(specs, rules, 1, 8)
+        eng.start(0)
+        calls = []
+        for chunk, with_pixel in ((5, True), (9, False)):
+            eng.run(chunk)
+            if batched:
+                calls.append(eng.take_events(with_pixel=with_pixel))
+            else:
+                calls.append([m.take_events(with_pixel=with_pixel) for m in models])
+            assert all(m.take_events()["t_cross_ns"].size == 0 for m in models)  # the lists are cleared
+        got.append(calls)
+    for call_a, call_b in zip(*got):
+        for a, b in zip(call_a, call_b):
+            assert a.keys() == b.keys()
+            for k in a:
+                assert np.array_equal(np.asarray(a[k]).view(np.uint8), np.asarray(b[k]).view(np.uint8)), k
+    assert sum(len(c["t_cross_ns"]) for c in got[1][0]) > 100
+
+
 def test_sensor_order_in_the_launch_does_not_matter(cuda_lib):
     """The same three sensors listed in reverse order give each sensor the same events."""
     specs = mixed_sensors()
