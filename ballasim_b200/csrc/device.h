@@ -135,6 +135,16 @@ void launch_advance_rows(const SensorConsts& k, const MapSoA& map, StateSoA in, 
 // after their start).
 size_t row_rest_bytes();
 int rows_rest_blocks_per_sm();
+// sample_window in one walk: pass 0 walks, counts, writes the carried samples and stages each pixel's samples in a
+// scratch list (stage_dt / stage_v, stage_cap entries, *stage_used zero before; stage_at[i] the pixel's start or
+// 0xFFFFFFFF); pass 1, after the scan of the counts, writes every row at its offset from the list, walking again a
+// pixel the list does not hold.
+void launch_sample_window_staged(const FieldDev& f, const SamplerRules& r, int64_t t_w, const uint32_t* pixel,
+                                 const uint8_t* level, uint32_t n, const float* carried_in, const uint64_t* sig_in,
+                                 uint32_t* counts, const int64_t* offsets, int64_t* t_out, float* irr_out,
+                                 float* carried_out, uint64_t* sig_out, uint32_t* stage_dt, float* stage_v,
+                                 uint32_t* stage_at, unsigned int* stage_used, uint32_t stage_cap, int pass,
+                                 cudaStream_t stream);
 // sample_window: pass 0 counts, pass 1 writes at offsets.
 void launch_sample_window(const FieldDev& f, const SamplerRules& r, int64_t t_w, const uint32_t* pixel,
                           const uint8_t* level, uint32_t n, const float* carried_in, const uint64_t* sig_in,

@@ -1207,6 +1207,122 @@ __global__ void __launch_bounds__(128) sample_window_kernel(WindowArgs a) {
   }
 }
 
+// sample_window in one walk (the device-runs path): sample_window_stage_kernel walks every pixel once, stages its
+// samples after slot 0 in shared memory (up to kSampStage), writes its count, its carried sample and signature, and
+// copies the staged samples to a scratch list (each warp's reserved with one atomic; stage_at[i] their start, or
+// kStageNone); after the scan of the counts, sample_window_place_kernel writes each row at its offset from the list,
+// or walks a pixel whose window overflowed the stage (or the list) again. The runs equal the two-pass form's.
+constexpr int kSampStage = 32;
+constexpr uint32_t kStageNone = 0xFFFFFFFFu;
+
+struct StageArgs {
+  WindowArgs w;
+  uint32_t* stage_dt;
+  float* stage_v;
+  uint32_t* stage_at;
+  unsigned int* stage_used;
+  uint32_t stage_cap;
+};
+
+__global__ void __launch_bounds__(128) sample_window_stage_kernel(StageArgs sa) {
+  const WindowArgs& a = sa.w;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool have = i < a.n;
+  const uint32_t px = have ? a.pixel[i] : 0u;
+  const uint32_t x = a.f.width > 0 ? px % a.f.width : 0u, y = a.f.width > 0 ? px / a.f.width : 0u;
+  __shared__ uint16_t lists[4][kMaxListed];
+  __shared__ uint32_t st_dt[4][kSampStage][32];
+  __shared__ float st_v[4][kSampStage][32];
+  const BlobList list = warp_blob_list(a.f, have, x, y, a.t_w, a.t_w + kWindowNs, lists[warp]);
+  uint32_t n = 0;
+  if (have) {
+    const float carried = a.carried_in[i];
+    const bool flip = a.sig_in[i] != 0ull;
+    const FieldDev& f = a.f;
+    const int64_t t_w = a.t_w;
+    auto render = [&](uint32_t dt) { return field_eval(f, list, x, y, t_w + dt); };
+    uint32_t k = 0;
+    float last = carried;
+    n = sample_pixel_window(a.r, a.level[i], carried, flip, render, [&](uint32_t dt, float v) {
+      if (k < static_cast<uint32_t>(kSampStage)) {
+        st_dt[warp][k][lane] = dt;
+        st_v[warp][k][lane] = v;
+      }
+      ++k;
+      last = v;
+    });
+    a.counts[i] = n;
+    a.carried_out[i] = last;
+    a.sig_out[i] = 0ull;
+  }
+  __syncwarp();
+  const uint32_t m = have && n >= 1u && n - 1u <= static_cast<uint32_t>(kSampStage) ? n - 1u : 0u;
+  const bool staged = have && n >= 1u && n - 1u <= static_cast<uint32_t>(kSampStage);
+  // The warp's staged samples reserved together: lane l's start is the base plus the lanes before it.
+  uint32_t before = m;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y2 = __shfl_up_sync(0xffffffffu, before, o);
+    if (static_cast<int>(lane) >= o) before += y2;
+  }
+  const uint32_t total = __shfl_sync(0xffffffffu, before, 31);
+  before -= m;
+  unsigned int base = 0;
+  if (lane == 0u && total > 0u) base = atomicAdd(sa.stage_used, total);
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (have) {
+    const bool fits = staged && static_cast<uint64_t>(base) + total <= sa.stage_cap;
+    if (fits) {
+      const uint32_t at = base + before;
+      for (uint32_t q = 0; q < m; ++q) {
+        sa.stage_dt[at + q] = st_dt[warp][q][lane];
+        sa.stage_v[at + q] = st_v[warp][q][lane];
+      }
+      sa.stage_at[i] = at;
+    } else {
+      sa.stage_at[i] = kStageNone;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128) sample_window_place_kernel(StageArgs sa) {
+  const WindowArgs& a = sa.w;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool have = i < a.n;
+  const uint32_t at = have ? sa.stage_at[i] : 0u;
+  const bool walk = have && at == kStageNone;
+  const uint32_t px = have ? a.pixel[i] : 0u;
+  const uint32_t x = a.f.width > 0 ? px % a.f.width : 0u, y = a.f.width > 0 ? px / a.f.width : 0u;
+  __shared__ uint16_t lists[4][kMaxListed];
+  BlobList list{nullptr, a.f.n_blobs};
+  if (__any_sync(0xffffffffu, walk)) {
+    list = warp_blob_list(a.f, have, x, y, a.t_w, a.t_w + kWindowNs, lists[threadIdx.x >> 5]);
+  }
+  if (!have) return;
+  const int64_t t_w = a.t_w;
+  const float carried = a.carried_in[i];
+  int64_t* t_out = a.t_out + a.offsets[i];
+  float* irr_out = a.irr_out + a.offsets[i];
+  t_out[0] = t_w;  // slot 0: the carried sample
+  irr_out[0] = carried;
+  if (!walk) {
+    const uint32_t m = a.counts[i] - 1u;
+    for (uint32_t q = 0; q < m; ++q) {
+      t_out[1 + q] = t_w + sa.stage_dt[at + q];
+      irr_out[1 + q] = sa.stage_v[at + q];
+    }
+    return;
+  }
+  const FieldDev& f = a.f;
+  auto render = [&](uint32_t dt) { return field_eval(f, list, x, y, t_w + dt); };
+  uint32_t k = 1;
+  sample_pixel_window(a.r, a.level[i], carried, a.sig_in[i] != 0ull, render, [&](uint32_t dt, float v) {
+    t_out[k] = t_w + dt;
+    irr_out[k] = v;
+    ++k;
+  });
+}
+
 __global__ void levels_kernel(FieldDev f, int64_t t_w, int32_t l_min, int32_t l_max, uint32_t n_pixels,
                               uint8_t* level) {
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2674,6 +2790,21 @@ void launch_sample_window(const FieldDev& f, const SamplerRules& r, int64_t t_w,
   const unsigned grid = (n + 127) / 128;
   if (pass == 0) sample_window_kernel<0><<<grid, 128, 0, stream>>>(a);
   else sample_window_kernel<1><<<grid, 128, 0, stream>>>(a);
+}
+
+void launch_sample_window_staged(const FieldDev& f, const SamplerRules& r, int64_t t_w, const uint32_t* pixel,
+                                 const uint8_t* level, uint32_t n, const float* carried_in, const uint64_t* sig_in,
+                                 uint32_t* counts, const int64_t* offsets, int64_t* t_out, float* irr_out,
+                                 float* carried_out, uint64_t* sig_out, uint32_t* stage_dt, float* stage_v,
+                                 uint32_t* stage_at, unsigned int* stage_used, uint32_t stage_cap, int pass,
+                                 cudaStream_t stream) {
+  if (n == 0) return;
+  const StageArgs a{WindowArgs{f, r, t_w, pixel, level, n, carried_in, sig_in, counts, offsets, t_out, irr_out,
+                               carried_out, sig_out},
+                    stage_dt, stage_v, stage_at, stage_used, stage_cap};
+  const unsigned grid = (n + 127) / 128;
+  if (pass == 0) sample_window_stage_kernel<<<grid, 128, 0, stream>>>(a);
+  else sample_window_place_kernel<<<grid, 128, 0, stream>>>(a);
 }
 
 size_t scan_scratch_words(uint32_t n) { return (n + kScanBlock - 1) / kScanBlock + 1; }

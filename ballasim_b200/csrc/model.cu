@@ -1237,8 +1237,17 @@ struct Sampler {
     CK(cudaStreamSynchronize(s));
     if (info.p[0] & 1ull) throw std::invalid_argument("levels must lie in [0, 23 - log2(min_dt_ns)]");
     if (info.p[0] & 2ull) throw std::invalid_argument("pixel id outside the field");
-    launch_sample_window(field.f, r, t_w, ids, lv, nn, c_in, s_in, counts.p, nullptr, nullptr, nullptr, nullptr,
-                         nullptr, 0, s);
+    // One walk: the samples staged in a scratch list (room for the last window's total and a quarter, at least
+    // 8 a pixel; a pixel that does not fit is walked again when its row is written).
+    const size_t cap = std::min<size_t>(std::max<size_t>(np * 8, stage_want), 0xFFFFFFF0ull);
+    stage_dt.ensure(cap);
+    stage_v.ensure(cap);
+    stage_at.ensure(np);
+    stage_used.ensure(1);
+    CK(cudaMemsetAsync(stage_used.p, 0, sizeof(unsigned int), s));
+    launch_sample_window_staged(field.f, r, t_w, ids, lv, nn, c_in, s_in, counts.p, nullptr, nullptr, nullptr, c_out,
+                                s_out, stage_dt.p, stage_v.p, stage_at.p, stage_used.p, static_cast<uint32_t>(cap), 0,
+                                s);
     launch_scan(counts.p, nn, offsets.p, scratch.p, s);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(info.p + 1, offsets.p + np, 8, cudaMemcpyDeviceToHost, s));
@@ -1246,12 +1255,19 @@ struct Sampler {
     n = np;
     dev_ids = ids;
     samples = static_cast<size_t>(info.p[1]);
+    stage_want = samples + samples / 4;
     t.ensure(samples);
     irr.ensure(samples);
-    launch_sample_window(field.f, r, t_w, ids, lv, nn, c_in, s_in, counts.p, offsets.p, t.p, irr.p, c_out, s_out, 1,
-                         s);
+    launch_sample_window_staged(field.f, r, t_w, ids, lv, nn, c_in, s_in, counts.p, offsets.p, t.p, irr.p, c_out,
+                                s_out, stage_dt.p, stage_v.p, stage_at.p, stage_used.p, static_cast<uint32_t>(cap), 1,
+                                s);
     CK(cudaGetLastError());
   }
+  DevBuf<uint32_t> stage_dt;  // the one-walk path's scratch list of staged samples, and each pixel's start in it
+  DevBuf<float> stage_v;
+  DevBuf<uint32_t> stage_at;
+  DevBuf<unsigned int> stage_used;
+  size_t stage_want = 0;
   DevBuf<unsigned long long> err;
   PinBuf<unsigned long long> info;
   const uint32_t* dev_ids = nullptr;  // the last device window's ids (the caller's array), null after a host window
