@@ -135,16 +135,18 @@ void launch_advance_rows(const SensorConsts& k, const MapSoA& map, StateSoA in, 
 // after their start).
 size_t row_rest_bytes();
 int rows_rest_blocks_per_sm();
-// sample_window in one walk: pass 0 walks, counts, writes the carried samples and stages each pixel's samples in a
-// scratch list (stage_dt / stage_v, stage_cap entries, *stage_used zero before; stage_at[i] the pixel's start or
-// 0xFFFFFFFF); pass 1, after the scan of the counts, writes every row at its offset from the list, walking again a
-// pixel the list does not hold.
+// sample_window in one walk: pass 0 checks the ids (< n_field) and levels (<= max_level; a bad one ORed into *err,
+// 1 level, 2 id, and not walked), walks, counts, and stages each pixel's carried sample, signature and samples in
+// scratch (stage_dt / stage_v, stage_cap entries, *stage_used zero before; stage_at[i] the pixel's start or
+// 0xFFFFFFFF); pass 1, after the scan of the counts and only if *err is clear, writes every row at its offset from
+// the list (walking again a pixel the list does not hold) and the carried samples and signatures.
 void launch_sample_window_staged(const FieldDev& f, const SamplerRules& r, int64_t t_w, const uint32_t* pixel,
                                  const uint8_t* level, uint32_t n, const float* carried_in, const uint64_t* sig_in,
                                  uint32_t* counts, const int64_t* offsets, int64_t* t_out, float* irr_out,
                                  float* carried_out, uint64_t* sig_out, uint32_t* stage_dt, float* stage_v,
-                                 uint32_t* stage_at, unsigned int* stage_used, uint32_t stage_cap, int pass,
-                                 cudaStream_t stream);
+                                 uint32_t* stage_at, unsigned int* stage_used, uint32_t stage_cap, float* stage_carried,
+                                 uint64_t* stage_sig, uint32_t n_field, int max_level, unsigned long long* err,
+                                 int pass, cudaStream_t stream);
 // sample_window: pass 0 counts, pass 1 writes at offsets.
 void launch_sample_window(const FieldDev& f, const SamplerRules& r, int64_t t_w, const uint32_t* pixel,
                           const uint8_t* level, uint32_t n, const float* carried_in, const uint64_t* sig_in,
@@ -156,9 +158,6 @@ void launch_scan(const uint32_t* counts, uint32_t n, int64_t* offsets, int64_t* 
 void launch_levels(const FieldDev& f, int64_t t_w, int32_t l_min, int32_t l_max, uint32_t n_pixels, uint8_t* level,
                    cudaStream_t stream);
 void launch_field_frame(const FieldDev& f, int64_t t, uint32_t n_pixels, float* out, cudaStream_t stream);
-// ORs into *err: bit 0 where a level exceeds max_level, bit 1 where a pixel id is outside the field.
-void launch_check_window(const uint32_t* pixel, const uint8_t* level, uint32_t n, uint32_t n_field, int max_level,
-                         unsigned long long* err, cudaStream_t stream);
 // The fused engine: windows [w0, w1) of every sensor, one warp per 8 x 4 pixel tile, tiles taken from a global
 // counter (work stealing) by a persistent grid. stage 0: the sampler feeds the pixel model sample by sample;
 // 16 or 32: per window the samples are staged in shared memory (that many per lane) between the two phases.

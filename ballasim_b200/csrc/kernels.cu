@@ -1207,11 +1207,13 @@ __global__ void __launch_bounds__(128) sample_window_kernel(WindowArgs a) {
   }
 }
 
-// sample_window in one walk (the device-runs path): sample_window_stage_kernel walks every pixel once, stages its
-// samples after slot 0 in shared memory (up to kSampStage), writes its count, its carried sample and signature, and
+// sample_window in one walk (the device-runs path): sample_window_stage_kernel checks each pixel's id and level (a
+// bad one is flagged in *err, 1: level, 2: id, and not walked), walks every pixel once, stages its samples after slot
+// 0 in shared memory (up to kSampStage), writes its count and keeps its carried sample and signature in scratch, and
 // copies the staged samples to a scratch list (each warp's reserved with one atomic; stage_at[i] their start, or
-// kStageNone); after the scan of the counts, sample_window_place_kernel writes each row at its offset from the list,
-// or walks a pixel whose window overflowed the stage (or the list) again. The runs equal the two-pass form's.
+// kStageNone). After the scan of the counts (and only when nothing was flagged), sample_window_place_kernel writes
+// each row at its offset from the list, or walks a pixel whose window overflowed the stage (or the list) again, and
+// the carried samples and signatures. The runs equal the two-pass form's.
 constexpr int kSampStage = 32;
 constexpr uint32_t kStageNone = 0xFFFFFFFFu;
 
@@ -1222,6 +1224,11 @@ struct StageArgs {
   uint32_t* stage_at;
   unsigned int* stage_used;
   uint32_t stage_cap;
+  float* stage_carried;  // each pixel's carried sample and signature, written out by the place kernel
+  uint64_t* stage_sig;
+  uint32_t n_field;
+  int max_level;
+  unsigned long long* err;
 };
 
 __global__ void __launch_bounds__(128) sample_window_stage_kernel(StageArgs sa) {
@@ -1234,9 +1241,16 @@ __global__ void __launch_bounds__(128) sample_window_stage_kernel(StageArgs sa) 
   __shared__ uint16_t lists[4][kMaxListed];
   __shared__ uint32_t st_dt[4][kSampStage][32];
   __shared__ float st_v[4][kSampStage][32];
-  const BlobList list = warp_blob_list(a.f, have, x, y, a.t_w, a.t_w + kWindowNs, lists[warp]);
+  unsigned long long bad = 0;
+  if (have && px >= sa.n_field) bad |= 2ull;
+  if (have && a.level[i] > sa.max_level) bad |= 1ull;
+  const BlobList list = warp_blob_list(a.f, have && bad == 0ull, x, y, a.t_w, a.t_w + kWindowNs, lists[warp]);
+  warp_or(sa.err, bad);
   uint32_t n = 0;
-  if (have) {
+  if (have && bad != 0ull) {
+    n = 1;
+    a.counts[i] = n;
+  } else if (have) {
     const float carried = a.carried_in[i];
     const bool flip = a.sig_in[i] != 0ull;
     const FieldDev& f = a.f;
@@ -1253,8 +1267,8 @@ __global__ void __launch_bounds__(128) sample_window_stage_kernel(StageArgs sa) 
       last = v;
     });
     a.counts[i] = n;
-    a.carried_out[i] = last;
-    a.sig_out[i] = 0ull;
+    sa.stage_carried[i] = last;
+    sa.stage_sig[i] = 0ull;
   }
   __syncwarp();
   const uint32_t m = have && n >= 1u && n - 1u <= static_cast<uint32_t>(kSampStage) ? n - 1u : 0u;
@@ -1301,6 +1315,8 @@ __global__ void __launch_bounds__(128) sample_window_place_kernel(StageArgs sa) 
   if (!have) return;
   const int64_t t_w = a.t_w;
   const float carried = a.carried_in[i];
+  a.carried_out[i] = sa.stage_carried[i];
+  a.sig_out[i] = sa.stage_sig[i];
   int64_t* t_out = a.t_out + a.offsets[i];
   float* irr_out = a.irr_out + a.offsets[i];
   t_out[0] = t_w;  // slot 0: the carried sample
@@ -2796,12 +2812,14 @@ void launch_sample_window_staged(const FieldDev& f, const SamplerRules& r, int64
                                  const uint8_t* level, uint32_t n, const float* carried_in, const uint64_t* sig_in,
                                  uint32_t* counts, const int64_t* offsets, int64_t* t_out, float* irr_out,
                                  float* carried_out, uint64_t* sig_out, uint32_t* stage_dt, float* stage_v,
-                                 uint32_t* stage_at, unsigned int* stage_used, uint32_t stage_cap, int pass,
-                                 cudaStream_t stream) {
+                                 uint32_t* stage_at, unsigned int* stage_used, uint32_t stage_cap, float* stage_carried,
+                                 uint64_t* stage_sig, uint32_t n_field, int max_level, unsigned long long* err,
+                                 int pass, cudaStream_t stream) {
   if (n == 0) return;
   const StageArgs a{WindowArgs{f, r, t_w, pixel, level, n, carried_in, sig_in, counts, offsets, t_out, irr_out,
                                carried_out, sig_out},
-                    stage_dt, stage_v, stage_at, stage_used, stage_cap};
+                    stage_dt, stage_v, stage_at, stage_used, stage_cap, stage_carried, stage_sig, n_field, max_level,
+                    err};
   const unsigned grid = (n + 127) / 128;
   if (pass == 0) sample_window_stage_kernel<<<grid, 128, 0, stream>>>(a);
   else sample_window_place_kernel<<<grid, 128, 0, stream>>>(a);
@@ -2823,25 +2841,6 @@ void launch_levels(const FieldDev& f, int64_t t_w, int32_t l_min, int32_t l_max,
 
 void launch_field_frame(const FieldDev& f, int64_t t, uint32_t n_pixels, float* out, cudaStream_t stream) {
   field_frame_kernel<<<(n_pixels + 255) / 256, 256, 0, stream>>>(f, t, n_pixels, out);
-}
-
-namespace {
-// The window inputs' checks on the device (bit 0: a level above max_level, bit 1: an id outside the field).
-__global__ void check_window_kernel(const uint32_t* pixel, const uint8_t* level, uint32_t n, uint32_t n_field,
-                                    int max_level, unsigned long long* err) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned long long bits = 0;
-  if (i < n) {
-    if (level[i] > max_level) bits |= 1ull;
-    if (pixel[i] >= n_field) bits |= 2ull;
-  }
-  warp_or(err, bits);
-}
-}  // namespace
-
-void launch_check_window(const uint32_t* pixel, const uint8_t* level, uint32_t n, uint32_t n_field, int max_level,
-                         unsigned long long* err, cudaStream_t stream) {
-  if (n > 0) check_window_kernel<<<(n + 255) / 256, 256, 0, stream>>>(pixel, level, n, n_field, max_level, err);
 }
 
 void launch_engine(const EngineSensor* sensors_dev, int n_sensors, uint32_t total_tiles, const int64_t* t0,

@@ -1227,31 +1227,30 @@ struct Sampler {
     counts.ensure(np);
     offsets.ensure(np + 1);
     scratch.ensure(scan_scratch_words(nn));
-    err.ensure(1);
     info.ensure(2);
-    // The inputs are checked before the walk runs on them (a lattice level sets the walk's length).
-    CK(cudaMemsetAsync(err.p, 0, sizeof(unsigned long long), s));
-    launch_check_window(ids, lv, nn, field.f.width * field.f.height, kWindowLog2 - shift, err.p, s);
-    CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(info.p, err.p, 8, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    if (info.p[0] & 1ull) throw std::invalid_argument("levels must lie in [0, 23 - log2(min_dt_ns)]");
-    if (info.p[0] & 2ull) throw std::invalid_argument("pixel id outside the field");
     // One walk: the samples staged in a scratch list (room for the last window's total and a quarter, at least
-    // 8 a pixel; a pixel that does not fit is walked again when its row is written).
+    // 8 a pixel; a pixel that does not fit is walked again when its row is written). The walk checks each pixel's
+    // id and level first (a lattice level sets the walk's length); the flags come back with the total, and nothing
+    // the caller passed is written unless both are clear.
     const size_t cap = std::min<size_t>(std::max<size_t>(np * 8, stage_want), 0xFFFFFFF0ull);
     stage_dt.ensure(cap);
     stage_v.ensure(cap);
     stage_at.ensure(np);
-    stage_used.ensure(1);
-    CK(cudaMemsetAsync(stage_used.p, 0, sizeof(unsigned int), s));
+    stage_c.ensure(np);
+    stage_s.ensure(np);
+    stage_used.ensure(4);  // [0] the list's use, [2..3] the flags
+    unsigned long long* flags = reinterpret_cast<unsigned long long*>(stage_used.p + 2);
+    CK(cudaMemsetAsync(stage_used.p, 0, 4 * sizeof(unsigned int), s));
     launch_sample_window_staged(field.f, r, t_w, ids, lv, nn, c_in, s_in, counts.p, nullptr, nullptr, nullptr, c_out,
-                                s_out, stage_dt.p, stage_v.p, stage_at.p, stage_used.p, static_cast<uint32_t>(cap), 0,
-                                s);
+                                s_out, stage_dt.p, stage_v.p, stage_at.p, stage_used.p, static_cast<uint32_t>(cap),
+                                stage_c.p, stage_s.p, field.f.width * field.f.height, kWindowLog2 - shift, flags, 0, s);
     launch_scan(counts.p, nn, offsets.p, scratch.p, s);
     CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(info.p, flags, 8, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(info.p + 1, offsets.p + np, 8, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    if (info.p[0] & 1ull) throw std::invalid_argument("levels must lie in [0, 23 - log2(min_dt_ns)]");
+    if (info.p[0] & 2ull) throw std::invalid_argument("pixel id outside the field");
     n = np;
     dev_ids = ids;
     samples = static_cast<size_t>(info.p[1]);
@@ -1259,16 +1258,17 @@ struct Sampler {
     t.ensure(samples);
     irr.ensure(samples);
     launch_sample_window_staged(field.f, r, t_w, ids, lv, nn, c_in, s_in, counts.p, offsets.p, t.p, irr.p, c_out,
-                                s_out, stage_dt.p, stage_v.p, stage_at.p, stage_used.p, static_cast<uint32_t>(cap), 1,
-                                s);
+                                s_out, stage_dt.p, stage_v.p, stage_at.p, stage_used.p, static_cast<uint32_t>(cap),
+                                stage_c.p, stage_s.p, field.f.width * field.f.height, kWindowLog2 - shift, flags, 1, s);
     CK(cudaGetLastError());
   }
   DevBuf<uint32_t> stage_dt;  // the one-walk path's scratch list of staged samples, and each pixel's start in it
   DevBuf<float> stage_v;
   DevBuf<uint32_t> stage_at;
   DevBuf<unsigned int> stage_used;
+  DevBuf<float> stage_c;  // each pixel's carried sample and signature until the rows are placed
+  DevBuf<uint64_t> stage_s;
   size_t stage_want = 0;
-  DevBuf<unsigned long long> err;
   PinBuf<unsigned long long> info;
   const uint32_t* dev_ids = nullptr;  // the last device window's ids (the caller's array), null after a host window
 };
