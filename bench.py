@@ -463,10 +463,11 @@ def run_runs(args, rank: int, world: int) -> dict | None:
                    "path": "sample_window (device) -> runs in HBM -> advance_device, per sensor and window",
                    "parallelism": f"replicas x{world}", "advance_block": args.block or "row-major",
                    "long_run": args.long_run or 32},
-        # Per sensor and window: levels, the input check, two sample_window passes, three scan kernels and the pixel
-        # model (the split row-major kernel's two launches, --block 1 one, --block n > 1 the scatter and one; every
-        # pixel is listed, so no advance_unlisted_kernel); per sensor and step the first frame and init.
-        "gpu_launches": (7 + (1 if args.block == 1 else 2)) * calls * args.steps + 2 * len(wl.sensors) * args.steps,
+        # Per sensor and window: levels, two sample_window passes (the walk, which also checks the inputs, and the
+        # placement), three scan kernels and the pixel model (the split row-major kernel's two launches, --block 1
+        # one, --block n > 1 the scatter and one; every pixel is listed, so no advance_unlisted_kernel); per sensor
+        # and step the first frame and init.
+        "gpu_launches": (6 + (1 if args.block == 1 else 2)) * calls * args.steps + 2 * len(wl.sensors) * args.steps,
         "clocks": clocks,
         "e2e": {"value": samples_all / e2e_s if e2e_times else None, "unit": "pixel-samples/s",
                 "h2d_bytes_per_step": sum(int(f.nbytes) for f in frames), "d2h_bytes_per_step": d2h},
