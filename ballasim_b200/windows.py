@@ -5,13 +5,15 @@ bs_sample_window_device), then SensorModel::advance_device on those runs (src/se
 events stay on the device.
 
 This is the two-kernel form of what the fused engine (engine.Engine) does in one launch: it writes and re-reads the
-runs (12 B per pixel-sample each way) and synchronizes three times per sensor and window (the window's input check,
-its sample count, the sensor's counters), as the reference's engine synchronizes per window. Device buffers are torch
-tensors.
+runs (12 B per pixel-sample each way) and synchronizes twice per sensor and window (the window's sample count with
+its input flags, the sensor's counters), as the reference's engine synchronizes per window. The sensors are
+independent, so by default each sensor's windows run in order on a stream of its own, driven from a host thread of
+its own: one sensor's synchronizations and host work overlap the others' kernels. Device buffers are torch tensors.
 """
 from __future__ import annotations
 
 import ctypes as C
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -59,6 +61,8 @@ class DeviceWindows:
             })
         self.t_ns = 0
         self.launch_ms = 0.0
+        self._streams = None  # the sensors' own streams and their host threads, made at the first concurrent run
+        self._pool = None
 
     def start(self, t0_ns: int = 0, stream: int | None = None, frames=None) -> None:
         """Renders every field at t0 on the device (or copies frames[i], sensor i's host frame of height * width
@@ -80,35 +84,78 @@ class DeviceWindows:
             m.init_device(int(t0_ns), b["carried"][0].data_ptr(), stream)
         self.t_ns = int(t0_ns)
 
-    def run(self, windows: int, stream: int | None = None, on_events=None) -> tuple[int, int]:
-        """Samples and senses `windows` windows of every sensor, window-major (each window of every sensor, then the
-        next). on_events(i, model, events) sees each call's device events (valid until that model advances again).
-        Returns the pixel-samples and events of the call; launch_ms accumulates the sensors' kernel times."""
-        L = _lib.lib()
+    def run(self, windows: int, stream: int | None = None, on_events=None, concurrent: bool = True) -> tuple[int, int]:
+        """Samples and senses `windows` windows of every sensor. on_events(i, model, events) sees each call's device
+        events (valid until that model advances again), in window order for each sensor. Returns the pixel-samples and
+        events of the call; launch_ms accumulates the sensors' kernel times.
+
+        concurrent (with more than one sensor): each sensor's windows on its own stream from its own host thread,
+        those streams starting after the work already queued on `stream` and `stream` waiting for them at the end
+        (on_events is then called from those threads, each sensor's calls from one). Otherwise window-major on
+        `stream` (each window of every sensor, then the next), as the reference's engine runs its cameras."""
         stream = _stream_handle(stream)
-        samples = events = 0
+        t0 = self.t_ns
+        n_sensors = len(self.sensors)
+        if concurrent and n_sensors > 1:
+            import torch
+
+            dev = torch.cuda.current_device()
+            if self._streams is None:
+                self._streams = [torch.cuda.Stream(device=dev) for _ in range(n_sensors)]
+                self._pool = ThreadPoolExecutor(max_workers=n_sensors, thread_name_prefix="bs-sensor")
+            caller = (torch.cuda.current_stream(dev) if stream == 1
+                      else torch.cuda.ExternalStream(stream, device=dev))
+            ready = torch.cuda.Event()
+            ready.record(caller)
+            for st in self._streams:
+                st.wait_event(ready)
+
+            def one(i):
+                torch.cuda.set_device(dev)
+                return self._sensor_windows(i, t0, windows, self._streams[i].cuda_stream, on_events)
+
+            parts = [f.result() for f in [self._pool.submit(one, i) for i in range(n_sensors)]]
+            for st in self._streams:
+                done = torch.cuda.Event()
+                done.record(st)
+                caller.wait_event(done)
+        else:
+            parts = [[0, 0, 0.0] for _ in range(n_sensors)]
+            for w in range(int(windows)):
+                for i in range(n_sensors):
+                    got = self._sensor_windows(i, t0 + w * (1 << 23), 1, stream, on_events)
+                    parts[i] = [a + b for a, b in zip(parts[i], got)]
+        self.launch_ms += sum(p[2] for p in parts)
+        self.t_ns = t0 + int(windows) * (1 << 23)
+        return sum(p[0] for p in parts), sum(p[1] for p in parts)
+
+    def _sensor_windows(self, i: int, t_w: int, windows: int, stream: int, on_events) -> list:
+        """Sensor i's windows [t_w, t_w + windows * 2^23) on `stream`: [pixel-samples, events, kernel ms]."""
+        L = _lib.lib()
+        (m, _), b = self.sensors[i], self._bufs[i]
+        s, n = b["sampler"], m.width * m.height
         total = C.c_size_t()
         runs = _lib.DeviceRuns()
+        samples = events = 0
+        ms = 0.0
         for _ in range(int(windows)):
-            t_w = self.t_ns
-            for i, ((m, _), b) in enumerate(zip(self.sensors, self._bufs)):
-                s, n, cur = b["sampler"], m.width * m.height, b["cur"]
-                _lib.check(L.bs_field_levels_device(s.h, t_w, self.l_min, self.l_max, b["level"].data_ptr(), stream))
-                _lib.check(L.bs_sample_window_device(
-                    s.h, t_w, b["ids"].data_ptr(), b["level"].data_ptr(), n, b["carried"][cur].data_ptr(),
-                    b["sig"][cur].data_ptr(), b["carried"][1 - cur].data_ptr(), b["sig"][1 - cur].data_ptr(),
-                    C.byref(self.rules), stream, C.byref(total)))
-                _lib.check(L.bs_sampler_device_runs(s.h, C.byref(runs)))
-                ms0 = m.stats()["gpu_launch_ms_total"]
-                ev = m.advance_device(runs, t_w + (1 << 23), stream)
-                self.launch_ms += m.stats()["gpu_launch_ms_total"] - ms0
-                if on_events is not None:
-                    on_events(i, m, ev)
-                samples += int(total.value)
-                events += int(ev.count)
-                b["cur"] = 1 - cur
-            self.t_ns = t_w + (1 << 23)
-        return samples, events
+            cur = b["cur"]
+            _lib.check(L.bs_field_levels_device(s.h, t_w, self.l_min, self.l_max, b["level"].data_ptr(), stream))
+            _lib.check(L.bs_sample_window_device(
+                s.h, t_w, b["ids"].data_ptr(), b["level"].data_ptr(), n, b["carried"][cur].data_ptr(),
+                b["sig"][cur].data_ptr(), b["carried"][1 - cur].data_ptr(), b["sig"][1 - cur].data_ptr(),
+                C.byref(self.rules), stream, C.byref(total)))
+            _lib.check(L.bs_sampler_device_runs(s.h, C.byref(runs)))
+            ms0 = m.stats()["gpu_launch_ms_total"]
+            ev = m.advance_device(runs, t_w + (1 << 23), stream)
+            ms += m.stats()["gpu_launch_ms_total"] - ms0
+            if on_events is not None:
+                on_events(i, m, ev)
+            samples += int(total.value)
+            events += int(ev.count)
+            b["cur"] = 1 - cur
+            t_w += 1 << 23
+        return [samples, events, ms]
 
 
 def carried_samples(dw: DeviceWindows, i: int) -> np.ndarray:

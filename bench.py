@@ -353,10 +353,11 @@ def run_ours(args, rank: int, world: int) -> dict | None:
 
 
 def run_runs(args, rank: int, world: int) -> dict | None:
-    """The reference engine's route with the runs in HBM (ballasim_b200.windows.DeviceWindows): per window and
-    sensor, the levels, sample_window on the device (count pass, scan, write pass) and advance_device (scatter of the
-    rows, advance_rows_kernel); the events stay on the device. Kernel time of the pixel model from CUDA events around
-    each advance launch."""
+    """The reference engine's route with the runs in HBM (ballasim_b200.windows.DeviceWindows): per sensor and
+    window, the levels, sample_window on the device (the walk, the scan, the placement) and advance_device (the split
+    row-major kernel); the events stay on the device. The sensors run each on its own stream and host thread (or,
+    with --window-major, in turn on one stream). Kernel time of the pixel model from CUDA events around each advance
+    launch, in window-major steps."""
     import torch
     import torch.distributed as dist
 
@@ -385,9 +386,9 @@ def run_runs(args, rank: int, world: int) -> dict | None:
     sptr = stream.cuda_stream
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
 
-    def step():
+    def step(concurrent=not args.window_major):
         dw.start(0, sptr)
-        return dw.run(wl.windows, sptr)
+        return dw.run(wl.windows, sptr, concurrent=concurrent)
 
     for _ in range(args.warmup):
         step()
@@ -413,6 +414,14 @@ def run_runs(args, rank: int, world: int) -> dict | None:
             dist.barrier()
     advance_launches = sum(m.stats()["gpu_launches"] for m in models) - launches0
     timed_launch_ms = dw.launch_ms
+    if not args.window_major:
+        # The pixel model's kernel times for the roofline from window-major steps on one stream (the sensors'
+        # streams overlap their kernels, so each launch's events would also time the other sensors' work).
+        dw.launch_ms = 0.0
+        for _ in range(args.steps):
+            step(concurrent=False)
+        torch.cuda.synchronize()
+        timed_launch_ms = dw.launch_ms
     step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
     total_ms = float(sum(step_ms))
     total_ms_all, samples_all, events_all = reduce_step(total_ms, float(samples), float(events), world)
@@ -428,16 +437,16 @@ def run_runs(args, rank: int, world: int) -> dict | None:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         dw.start(0, sptr, frames=frames)
-        n_ev = [0]
+        n_ev = [0] * len(models)  # one count per sensor: each sensor's calls come from one thread
 
         def take(i, m, ev):
-            n_ev[0] += len(m.download_events(ev)["t_cross_ns"])
+            n_ev[i] += len(m.download_events(ev)["t_cross_ns"])
 
-        dw.run(wl.windows, sptr, on_events=take)
+        dw.run(wl.windows, sptr, on_events=take, concurrent=not args.window_major)
         torch.cuda.synchronize()
         if k >= args.warmup:
             e2e_times.append(time.perf_counter() - t0)
-            d2h = n_ev[0] * 32
+            d2h = sum(n_ev) * 32
     e2e_s = reduce_max(sum(e2e_times), world)
     if rank != 0:
         return None
@@ -461,6 +470,8 @@ def run_runs(args, rank: int, world: int) -> dict | None:
         "config": {**wl.describe(), "pixel_samples_per_step": int(per_step_samples),
                    "events_per_step": int(per_step_events), "l2": "flushed between steps (256 MiB write)",
                    "path": "sample_window (device) -> runs in HBM -> advance_device, per sensor and window",
+                   "sensors_run": "window-major on one stream" if args.window_major
+                   else "each on its own stream and host thread",
                    "parallelism": f"replicas x{world}", "advance_block": args.block or "row-major",
                    "long_run": args.long_run or 32},
         # Per sensor and window: levels, two sample_window passes (the walk, which also checks the inputs, and the
@@ -479,7 +490,8 @@ def run_runs(args, rank: int, world: int) -> dict | None:
                      "traffic": cap["dram_per_alg_byte"] * alg / n_launch if cap and n_launch else None,
                      "traffic_capture": cap["capture"] if cap else None,
                      "algorithmic_bytes_per_step": alg, "launches_per_step": n_launch,
-                     "kernel_ms_per_step": kms_total, "share_of_step": kms_total / (total_ms_all / args.steps)},
+                     "kernel_ms_per_step": kms_total, "kernel_ms_from": "window-major steps on one stream",
+                     "share_of_step": kms_total / (total_ms_all / args.steps)},
     }
 
 
@@ -742,6 +754,9 @@ def main():
                     help="windows of every sensor in the reference's bounded sample (0: the workload's default)")
     ap.add_argument("--block", type=int, default=0,
                     help="runs_* workloads: 0 the split row-major kernel, 1 unsplit, n > 1 advance_runs_kernel's block")
+    ap.add_argument("--window-major", action="store_true",
+                    help="runs_* workloads: every sensor's windows in turn on one stream (default: each sensor on a "
+                         "stream and host thread of its own)")
     ap.add_argument("--long-run", type=int, default=0,
                     help="runs_* workloads: runs longer than this are walked by a whole warp (-1: none)")
     ap.add_argument("--no-cpu-baseline", action="store_true")

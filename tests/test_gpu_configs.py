@@ -294,10 +294,11 @@ def test_o13_ramp_event_count_on_the_device(cuda_lib, sigma):
 
 # ---- the reference engine's per-window loop with the runs in HBM (sample_window on the device, advance_device) ----
 
-@pytest.mark.parametrize("case", ["blobs", "noise", "mixed"])
-def test_device_windows_equal_the_oracle(cuda_lib, case):
+@pytest.mark.parametrize("case,concurrent", [("blobs", True), ("noise", True), ("mixed", True), ("mixed", False)])
+def test_device_windows_equal_the_oracle(cuda_lib, case, concurrent):
     """Levels, sample_window on device-resident inputs and advance_device on the runs, window by window and sensor by
-    sensor: each sensor's events (downloaded per call) and the samples equal the oracle chain, bit for bit."""
+    sensor (each sensor on its own stream and host thread, or all window-major on one stream): each sensor's events
+    (downloaded per call) and the samples equal the oracle chain, bit for bit."""
     from ballasim_b200.sensor import SensorModel
     from ballasim_b200.windows import DeviceWindows
     from oracle.oracle import simulate_port
@@ -316,7 +317,8 @@ def test_device_windows_equal_the_oracle(cuda_lib, case):
                        l_max=rules.l_max)
     dw.start(0)
     parts = [[] for _ in specs]
-    samples, events = dw.run(windows, on_events=lambda i, m, ev: parts[i].append(m.download_events(ev)))
+    samples, events = dw.run(windows, on_events=lambda i, m, ev: parts[i].append(m.download_events(ev)),
+                             concurrent=concurrent)
     assert samples == sum(st["pixel_samples"] for _, st in want)
     for i, (s, (ev, _)) in enumerate(zip(specs, want)):
         got = {k: np.concatenate([p[k] for p in parts[i]]) for k in parts[i][0]}
