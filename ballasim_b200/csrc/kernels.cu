@@ -2064,24 +2064,64 @@ __global__ void __launch_bounds__(128) engine_kernel_staged(EngineArgs a) {
 // rare paths together. A pixel's samples are fed in the same order to the same state either way, so events and
 // state are the staged engine's; the state passes from one window to the next through HBM.
 constexpr int kSplitStage = 16;
-constexpr uint8_t kRestWhole = 0xFF;  // RestRecord::n of a window that overflowed the stage
+constexpr uint32_t kRestWhole = 0xFF;  // the samples left of a window that overflowed the stage
 
-struct RestRecord {
-  PixelRegs s;        // the state where the pixel stopped (after the noise pass and its clean segments)
-  int64_t prev_t;     // the feed: the last sample fed (time, clamped value, x) and the last raw value
-  float prev_v, x_prev, last_raw;
-  uint32_t pixel;
-  uint16_t sensor;
-  uint8_t n;          // samples left in dt / v (kRestWhole: the window from its start, the carried sample in last_raw)
-  uint8_t level;      // the window's lattice level (for a whole window)
-  uint32_t dt[kSplitStage];
-  float v[kSplitStage];
+// The posted pixels, as planes (structure of arrays): field k of record i at plane k, entry i, so that the window
+// kernel's posting lanes (consecutive records) store and the rest kernel's threads load with coalesced accesses.
+// Per record: the state where the pixel stopped (after the noise pass and its clean segments); the feed (the last
+// sample fed: time, clamped value, x; the last raw value); the pixel, its sensor, the samples left in dt / v
+// (kRestWhole: the window from its start, the carried sample in last_raw) and the window's lattice level (for a
+// whole window); the staged samples left.
+enum : int { kR64TRef, kR64TSearch, kR64Blind, kR64TShot, kR64TBa, kR64PrevT, kRest64 };
+enum : int {
+  kR32S3Ref, kR32N3Ref, kR32DrRef, kR32IScale, kR32Held, kR32Flags, kR32NShot, kR32NBa, kR32PrevV, kR32XPrev,
+  kR32LastRaw, kR32Pixel, kR32Tag, kR32Dt, kR32V = kR32Dt + kSplitStage, kRest32 = kR32V + kSplitStage
 };
+constexpr size_t kRestRecordBytes = kRest64 * 8 + kRest32 * 4;
 
 struct RestList {
-  RestRecord* rec;
+  unsigned char* base;  // kRest64 planes of 8 bytes, then kRest32 planes of 4, each `capacity` entries
   unsigned int* count;
   unsigned int capacity;
+  __device__ __forceinline__ int64_t* p64(int k) const {
+    return reinterpret_cast<int64_t*>(base) + static_cast<size_t>(k) * capacity;
+  }
+  __device__ __forceinline__ uint32_t* p32(int k) const {
+    return reinterpret_cast<uint32_t*>(base + static_cast<size_t>(kRest64) * 8 * capacity) +
+           static_cast<size_t>(k) * capacity;
+  }
+  __device__ __forceinline__ void put_state(unsigned int i, const PixelRegs& s) const {
+    p64(kR64TRef)[i] = s.t_ref;
+    p64(kR64TSearch)[i] = s.t_search;
+    p64(kR64Blind)[i] = s.blind_until;
+    p64(kR64TShot)[i] = s.t_shot;
+    p64(kR64TBa)[i] = s.t_ba;
+    p32(kR32S3Ref)[i] = __float_as_uint(s.s3_ref);
+    p32(kR32N3Ref)[i] = __float_as_uint(s.n3_ref);
+    p32(kR32DrRef)[i] = __float_as_uint(s.dr_ref);
+    p32(kR32IScale)[i] = __float_as_uint(s.i_scale);
+    p32(kR32Held)[i] = __float_as_uint(s.held);
+    p32(kR32Flags)[i] = s.flags;
+    p32(kR32NShot)[i] = s.n_shot;
+    p32(kR32NBa)[i] = s.n_ba;
+  }
+  __device__ __forceinline__ PixelRegs state(unsigned int i) const {
+    PixelRegs s;
+    s.t_ref = p64(kR64TRef)[i];
+    s.t_search = p64(kR64TSearch)[i];
+    s.blind_until = p64(kR64Blind)[i];
+    s.t_shot = p64(kR64TShot)[i];
+    s.t_ba = p64(kR64TBa)[i];
+    s.s3_ref = __uint_as_float(p32(kR32S3Ref)[i]);
+    s.n3_ref = __uint_as_float(p32(kR32N3Ref)[i]);
+    s.dr_ref = __uint_as_float(p32(kR32DrRef)[i]);
+    s.i_scale = __uint_as_float(p32(kR32IScale)[i]);
+    s.held = __uint_as_float(p32(kR32Held)[i]);
+    s.flags = p32(kR32Flags)[i];
+    s.n_shot = p32(kR32NShot)[i];
+    s.n_ba = p32(kR32NBa)[i];
+    return s;
+  }
 };
 
 // Window a.w0 of every tile (a.t0 the model time at the call's start). kFirst: the call's first window, where the
@@ -2190,22 +2230,18 @@ __global__ void __launch_bounds__(128) engine_window_kernel(EngineArgs a, RestLi
         if (i >= rl.capacity) {
           atomicOr(&S.counters[kCntErrors], kErrRestList);
         } else {
-          RestRecord& r = rl.rec[i];
-          r.s = s;
-          r.prev_t = prev_t;
-          r.prev_v = prev_v;
-          r.x_prev = x_prev;
-          r.last_raw = last_raw;
-          r.pixel = p;
-          r.sensor = static_cast<uint16_t>(si);
-          r.level = static_cast<uint8_t>(level);
-          if (!staged) {
-            r.n = kRestWhole;
-          } else {
-            r.n = static_cast<uint8_t>(n - 1 - j);
+          rl.put_state(i, s);
+          rl.p64(kR64PrevT)[i] = prev_t;
+          rl.p32(kR32PrevV)[i] = __float_as_uint(prev_v);
+          rl.p32(kR32XPrev)[i] = __float_as_uint(x_prev);
+          rl.p32(kR32LastRaw)[i] = __float_as_uint(last_raw);
+          rl.p32(kR32Pixel)[i] = p;
+          const uint32_t left = staged ? n - 1 - j : kRestWhole;
+          rl.p32(kR32Tag)[i] = static_cast<uint32_t>(si) | left << 16 | static_cast<uint32_t>(level) << 24;
+          if (staged) {
             for (uint32_t q = j; q + 1 < n; ++q) {
-              r.dt[q - j] = st_dt[warp][q][lane];
-              r.v[q - j] = st_v[warp][q][lane];
+              rl.p32(kR32Dt + static_cast<int>(q - j))[i] = st_dt[warp][q][lane];
+              rl.p32(kR32V + static_cast<int>(q - j))[i] = __float_as_uint(st_v[warp][q][lane]);
             }
           }
         }
@@ -2227,35 +2263,39 @@ __global__ void __launch_bounds__(128, 4) engine_rest_kernel(EngineArgs a, RestL
   const int64_t t_w = *a.t0 + static_cast<int64_t>(a.w0) * kWindowNs;
   const unsigned int count = min(*rl.count, rl.capacity);
   for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-    const RestRecord& r = rl.rec[i];
-    const EngineSensor& S = a.sensors[r.sensor];
-    PixelRegs s = r.s;
+    const uint32_t tag = rl.p32(kR32Tag)[i], pixel = rl.p32(kR32Pixel)[i];
+    const uint32_t left = tag >> 16 & 0xFFu;
+    const float raw0 = __uint_as_float(rl.p32(kR32LastRaw)[i]);
+    const EngineSensor& S = a.sensors[tag & 0xFFFFu];
+    PixelRegs s = rl.state(i);
     PixelMapRegs m;
-    load_map(S.map, r.pixel, m);
+    load_map(S.map, pixel, m);
     PixelCounters c;
     const ThreadSink sink{S.ev, &S.counters[kCntEvents]};
     float held, last_raw;
-    if (r.n == kRestWhole) {
+    if (left == kRestWhole) {
       const FieldDev& f = S.field;
       const BlobList all{nullptr, f.n_blobs};
-      const uint32_t x = r.pixel % S.width, y = r.pixel / S.width;
+      const uint32_t x = pixel % S.width, y = pixel / S.width;
       auto render = [&](uint32_t dt) { return field_eval(f, all, x, y, t_w + dt); };
-      RegFeed<true, ThreadSink> feed{s,   m,   c,      S.consts,   &S.consts, r.pixel,
-                                     sink, t_w, t_w, s.held, r.last_raw, 0.0f};
-      feed.start(r.last_raw);
-      sample_pixel_window(a.r, r.level, r.last_raw, false, render, feed);
+      RegFeed<true, ThreadSink> feed{s, m, c, S.consts, &S.consts, pixel, sink, t_w, t_w, s.held, raw0, 0.0f};
+      feed.start(raw0);
+      sample_pixel_window(a.r, static_cast<int>(tag >> 24), raw0, false, render, feed);
       held = feed.prev_v;
       last_raw = feed.last_raw;
     } else {
-      RegFeed<true, ThreadSink> feed{s, m, c, S.consts, &S.consts, r.pixel, sink, t_w, r.prev_t, r.prev_v, r.last_raw,
-                                     r.x_prev};
-      for (int q = 0; q < r.n; ++q) feed(r.dt[q], r.v[q]);
+      RegFeed<true, ThreadSink> feed{s, m, c, S.consts, &S.consts, pixel, sink, t_w, rl.p64(kR64PrevT)[i],
+                                     __uint_as_float(rl.p32(kR32PrevV)[i]), raw0,
+                                     __uint_as_float(rl.p32(kR32XPrev)[i])};
+      for (uint32_t q = 0; q < left; ++q) {
+        feed(rl.p32(kR32Dt + static_cast<int>(q))[i], __uint_as_float(rl.p32(kR32V + static_cast<int>(q))[i]));
+      }
       held = feed.prev_v;
       last_raw = feed.last_raw;
     }
     s.held = held;
-    store_state(S.out, r.pixel, S.consts.noise != 0, s);
-    S.carried_out[r.pixel] = last_raw;
+    store_state(S.out, pixel, S.consts.noise != 0, s);
+    S.carried_out[pixel] = last_raw;
     if (c.pieces) atomicAdd(&S.counters[kCntPieces], static_cast<unsigned long long>(c.pieces));
     if (c.leaves) atomicAdd(&S.counters[kCntLeaves], static_cast<unsigned long long>(c.leaves));
     if (c.noise_candidates) atomicAdd(&S.counters[kCntNoise], static_cast<unsigned long long>(c.noise_candidates));
@@ -2861,13 +2901,13 @@ void launch_engine_split(const EngineSensor* sensors_dev, int n_sensors, uint32_
                          unsigned int rest_capacity, int blocks, int warps_per_block, int tile_lw, int rest_blocks,
                          cudaStream_t stream) {
   const EngineArgs a{sensors_dev, n_sensors, total_tiles, t0, w, w + 1, r, tile_counter, static_cast<uint32_t>(tile_lw)};
-  const RestList rl{static_cast<RestRecord*>(rest), rest_count, rest_capacity};
+  const RestList rl{static_cast<unsigned char*>(rest), rest_count, rest_capacity};
   if (w == 0) engine_window_kernel<true><<<blocks, warps_per_block * 32, 0, stream>>>(a, rl);
   else engine_window_kernel<false><<<blocks, warps_per_block * 32, 0, stream>>>(a, rl);
   engine_rest_kernel<<<rest_blocks, 128, 0, stream>>>(a, rl);
 }
 
-size_t rest_record_bytes() { return sizeof(RestRecord); }
+size_t rest_record_bytes() { return kRestRecordBytes; }
 size_t row_rest_bytes() { return sizeof(RowRest); }
 int rows_rest_blocks_per_sm() {
   int n = 0;

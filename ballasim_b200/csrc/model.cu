@@ -1594,6 +1594,7 @@ struct Engine {
   Engine(bs_model* const* ms, const bs_field* fs, int32_t cnt, const bs_sample_rules& r) {
     require_device();
     if (cnt < 1) throw std::invalid_argument("engine: at least one sensor");
+    if (cnt > 65535) throw std::invalid_argument("engine: at most 65535 sensors");
     rules = make_rules(r);
     uint32_t tile0 = 0;
     for (int32_t i = 0; i < cnt; ++i) {
