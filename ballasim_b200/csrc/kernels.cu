@@ -840,9 +840,15 @@ __global__ void __launch_bounds__(32 * kRowsWarps) advance_rows_split_kernel(Row
   if (cnt > 0 && !longrun) {
     const int64_t* tp = a.t + beg;
     const float* vp = a.irr + beg;
+    int64_t t_next = __ldg(tp);  // each sample loaded one iteration ahead of its use
+    float v_next = __ldg(vp);
     for (int32_t i = 0; i < cnt; ++i) {
-      const int64_t ti = __ldg(tp + i);
-      const float raw = __ldg(vp + i);
+      const int64_t ti = t_next;
+      const float raw = v_next;
+      if (i + 1 < cnt) {
+        t_next = __ldg(tp + i + 1);
+        v_next = __ldg(vp + i + 1);
+      }
       if (!isfinite(raw)) err |= kErrNonFinite;
       const float vi = clamp_irr(raw, a.k.irr_max);
       if (!(vi == raw)) ++clamps;
