@@ -2244,10 +2244,10 @@ __global__ void __launch_bounds__(128) engine_window_kernel(EngineArgs a, RestLi
           rl.p32(kR32Pixel)[i] = p;
           const uint32_t left = staged ? n - 1 - j : kRestWhole;
           rl.p32(kR32Tag)[i] = static_cast<uint32_t>(si) | left << 16 | static_cast<uint32_t>(level) << 24;
-          if (staged) {
-            for (uint32_t q = j; q + 1 < n; ++q) {
-              rl.p32(kR32Dt + static_cast<int>(q - j))[i] = st_dt[warp][q][lane];
-              rl.p32(kR32V + static_cast<int>(q - j))[i] = __float_as_uint(st_v[warp][q][lane]);
+          if (staged) {  // by plane, so that the posting lanes write each plane together
+            for (uint32_t u = 0; u < left; ++u) {
+              rl.p32(kR32Dt + static_cast<int>(u))[i] = st_dt[warp][j + u][lane];
+              rl.p32(kR32V + static_cast<int>(u))[i] = __float_as_uint(st_v[warp][j + u][lane]);
             }
           }
         }
