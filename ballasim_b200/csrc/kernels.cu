@@ -1219,8 +1219,9 @@ __global__ void __launch_bounds__(128) sample_window_kernel(WindowArgs a) {
 // copies the staged samples to a scratch list (each warp's reserved with one atomic; stage_at[i] their start, or
 // kStageNone). After the scan of the counts (and only when nothing was flagged), sample_window_place_kernel writes
 // each row at its offset from the list, or walks a pixel whose window overflowed the stage (or the list) again, and
-// the carried samples and signatures. The runs equal the two-pass form's.
-constexpr int kSampStage = 32;
+// the carried samples and signatures. The runs equal the two-pass form's. 16 staged samples a lane (18 KB of shared
+// memory a block) leave the registers to bound the blocks per SM; 32 (35 KB) held them to 6 and measured slower.
+constexpr int kSampStage = 16;
 constexpr uint32_t kStageNone = 0xFFFFFFFFu;
 
 struct StageArgs {
