@@ -75,11 +75,12 @@ NCU = {
     # traffic: one pass on the full 60-window launch; instructions and issue-active: the full set on its first 4
     # windows (74,251,870 pixel-samples).
     "six_sensors_4.6Mpx": [
-        # The split engine: one pass over all 120 launches of a step (traffic, instructions: the step's sums;
-        # issue-active: the two kernels' full-set figures weighted by their time).
+        # The split engine: one pass over all 120 launches of a step (traffic, instructions: the step's sums);
+        # issue-active: the two kernels' full-set figures on one window, weighted by their time (that full set was
+        # taken while the posted records were one struct per pixel rather than planes).
         {"kernel": "engine_window_kernel+engine_rest_kernel", "stage": 1, "tile_width": 8,
-         "traffic": (32.68e9 + 0.549e9 + 6.656e9) + (19.56e9 + 0.331e9 + 3.102e9),
-         "inst_per_sample": (3.472e10 + 5.999e8 + 1.772e9) / 1103436116, "issue_active": 0.471},
+         "traffic": (32.41e9 + 0.5452e9 + 6.498e9) + (19.34e9 + 0.3281e9 + 3.512e9),
+         "inst_per_sample": (3.488e10 + 6.022e8 + 1.819e9) / 1103436116, "issue_active": 0.471},
         {"kernel": "engine_kernel_staged<16>", "stage": 16, "tile_width": 8, "traffic": 690.74e6 + 3.59e9,
          "inst_per_sample": 3.329e9 / 74251870, "issue_active": 0.209},
         {"kernel": "engine_kernel_staged<16>", "stage": 16, "tile_width": 4, "traffic": 694.48e6 + 3.67e9,
