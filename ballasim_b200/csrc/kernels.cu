@@ -793,7 +793,10 @@ struct RowRestList {
 // such a segment is also taken in place when clean (clean_after_start) rather than posted; the other calls' kernel
 // leaves that test out of its loop.
 template <bool kFirst>
-__global__ void __launch_bounds__(32 * kRowsWarps) advance_rows_split_kernel(RowsArgs a, RowRestList rl) {
+// At most 64 registers (8 blocks of 4 warps per SM): the kernel waits on its rows' loads, and the extra warps hide
+// more than the spills cost (pixel-model kernels 97.0 ms per six-sensor runs step at 128 registers, 82.0 at 80,
+// 78.1 at 64).
+__global__ void __launch_bounds__(32 * kRowsWarps, 8) advance_rows_split_kernel(RowsArgs a, RowRestList rl) {
   const unsigned full = 0xffffffffu;
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t row = (blockIdx.x * kRowsWarps + warp) * 32u + lane;
