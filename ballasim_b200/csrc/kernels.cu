@@ -2268,9 +2268,10 @@ __global__ void __launch_bounds__(128) engine_window_kernel(EngineArgs a, RestLi
 
 // The posted pixels of window a.w0, one thread each: the rest of the window through the full pixel model (a window
 // posted whole is walked again from its start, every blob of the field evaluated: the same values as the warp's
-// culled list gives), then the state and the carried sample stored. Capped at 128 registers (4 blocks per SM): a few
-// spills, but 16 warps per SM instead of 12 measured 0.5 % faster on the six sensors.
-__global__ void __launch_bounds__(128, 4) engine_rest_kernel(EngineArgs a, RestList rl) {
+// culled list gives), then the state and the carried sample stored. Capped for 5 blocks per SM (at most 102
+// registers): more spills, but 20 warps per SM; on the six sensors 68.5 ms per step against 70.1 at 4 blocks (128
+// registers) and 69.0 at 6 (4 blocks had measured 0.5 % faster than 3, uncapped).
+__global__ void __launch_bounds__(128, 5) engine_rest_kernel(EngineArgs a, RestList rl) {
   const int64_t t_w = *a.t0 + static_cast<int64_t>(a.w0) * kWindowNs;
   const unsigned int count = min(*rl.count, rl.capacity);
   for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
