@@ -2643,7 +2643,9 @@ __global__ void learned_reset_kernel(LearnedSoA st, uint32_t n, const float* irr
 // Per window and warp: every lane with its walk inside the window writes its 16 features, the warp runs the MLP on
 // the tensor cores (32 rows), and each lane takes its proposed step (judge, fallback and pixel model on its own);
 // the loop ends when every lane has reached the window's end.
-__global__ void __launch_bounds__(128) learned_engine_kernel(EngineArgs a, LearnedLaunch l) {
+// At most 64 registers (8 blocks per SM; 128 uncapped held it to 4): on the 1280x720 held-out field 170.5 against
+// 198.7 ms (186.3 at 6 blocks, 177.2 at 7), the proposals and the events unchanged.
+__global__ void __launch_bounds__(128, 8) learned_engine_kernel(EngineArgs a, LearnedLaunch l) {
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const int64_t t0 = *a.t0;
   __shared__ MlpShared W;
