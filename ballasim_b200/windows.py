@@ -13,7 +13,7 @@ its own: one sensor's synchronizations and host work overlap the others' kernels
 from __future__ import annotations
 
 import ctypes as C
-from concurrent.futures import ThreadPoolExecutor
+from concurrent.futures import ThreadPoolExecutor, wait
 
 import numpy as np
 
@@ -114,7 +114,9 @@ class DeviceWindows:
                 torch.cuda.set_device(dev)
                 return self._sensor_windows(i, t0, windows, self._streams[i].cuda_stream, on_events)
 
-            parts = [f.result() for f in [self._pool.submit(one, i) for i in range(n_sensors)]]
+            futures = [self._pool.submit(one, i) for i in range(n_sensors)]
+            wait(futures)  # every sensor's thread done before any error reaches the caller
+            parts = [f.result() for f in futures]
             for st in self._streams:
                 done = torch.cuda.Event()
                 done.record(st)

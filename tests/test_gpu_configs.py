@@ -326,6 +326,32 @@ def test_device_windows_equal_the_oracle(cuda_lib, case, concurrent):
     assert events == sum(len(ev["t_cross_ns"]) for ev, _ in want) > 50
 
 
+def test_device_windows_finish_every_sensor_before_an_error(cuda_lib):
+    """With each sensor on its own thread, an error in one sensor's call (here its events callback) reaches the caller
+    only after every other sensor has run all its windows."""
+    from ballasim_b200.sensor import SensorModel
+    from ballasim_b200.windows import DeviceWindows
+
+    specs, rules, windows = mixed_sensors(), W.Rules(), 4
+    models = [SensorModel(resolve(s.preset, s.overrides), s.width, s.height, s.seed, [{"type": "constant"}], s.camera)
+              for s in specs]
+    dw = DeviceWindows([(m, s.field) for m, s in zip(models, specs)], tol=rules.tol, dark=rules.dark,
+                       min_dt_ns=rules.min_dt_ns, max_refine_levels=rules.max_refine_levels, l_min=rules.l_min,
+                       l_max=rules.l_max)
+    dw.start(0)
+    calls = [0] * len(specs)
+
+    def on_events(i, m, ev):
+        calls[i] += 1
+        if i == 1 and calls[i] == 2:
+            raise RuntimeError("stop sensor 1")
+
+    with pytest.raises(RuntimeError, match="stop sensor 1"):
+        dw.run(windows, on_events=on_events)
+    assert calls[1] == 2
+    assert all(c == windows for i, c in enumerate(calls) if i != 1)
+
+
 def test_device_window_refuses_bad_inputs_and_recovers(cuda_lib):
     """bs_sample_window_device checks the device ids and levels before it samples: a level above the finest or an id
     outside the field is refused (ValueError) with nothing written, and the next valid call samples as usual."""
